@@ -1,0 +1,230 @@
+/*
+ * dmph.h — C ABI of the B200 DEM-MPH explicit-timestep library (libdmph.so).
+ *
+ * The reference solver (Ryo1011gd/DEM_MPH) has no plugin or FFI layer: its
+ * physics are file-static functions over file-scope globals in
+ * source/DEM-MPH.cpp, called from main (source/DEM-MPH.cpp:350-617), and its
+ * external contract is the process CLI plus the text formats dem.data, .grid
+ * and .prof.  This header is the boundary that replaces that path: a host
+ * driver (the `dem_mph` executable built from dem_mph_b200/host/, or any
+ * caller over ctypes / cgo / JNI) reads the same files and calls the GPU only
+ * through these entry points.  Each function below cites the reference code
+ * it stands in for.
+ *
+ * Conventions
+ *   - All arrays are caller-owned host memory, copied in or out; device
+ *     buffers are owned by the context.
+ *   - Vectors are interleaved x,y,z per particle (the reference's
+ *     double[N][3] layout).
+ *   - Every function returns 0 on success or a negative DMPH_E* code; the
+ *     message is available from dmph_last_error().
+ *   - One host thread per context.  Contexts are independent (re-entrant
+ *     across contexts), each with its own CUDA stream.
+ */
+#ifndef DMPH_H_INCLUDED
+#define DMPH_H_INCLUDED
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DMPH_ABI_VERSION 1
+#define DMPH_TYPE_COUNT 6 /* source/DEM-MPH.cpp:46 */
+
+/* particle classes by type (source/DEM-MPH.cpp:46-52) */
+#define DMPH_FLUID_BEGIN 0
+#define DMPH_FLUID_END 2
+#define DMPH_SOLID_BEGIN 2
+#define DMPH_SOLID_END 4
+#define DMPH_WALL_BEGIN 4
+#define DMPH_WALL_END 6
+
+/* error codes */
+#define DMPH_OK 0
+#define DMPH_EINVAL (-1)   /* bad argument or inconsistent parameters */
+#define DMPH_ECUDA (-2)    /* CUDA runtime error */
+#define DMPH_ENOMEM (-3)   /* device allocation failed */
+#define DMPH_EIO (-4)      /* file could not be read or written */
+#define DMPH_ENAN (-5)     /* non-finite state detected */
+#define DMPH_ETIMEOUT (-6) /* a bounded device wait ran out */
+#define DMPH_ERANGE (-7)   /* a size limit was exceeded */
+
+/* precision of the pair kernels */
+#define DMPH_PRECISION_FP64 0       /* parity build: FP64 everywhere */
+#define DMPH_PRECISION_FP32_SPLIT 1 /* FP32 pair math on cell-relative positions */
+
+/* flags */
+#define DMPH_FLAG_SURFACE_TENSION_AUTO 0u /* default: on iff an InteractionRatio != 0 */
+#define DMPH_FLAG_SURFACE_TENSION_ON (1u << 0)
+#define DMPH_FLAG_SURFACE_TENSION_OFF (1u << 1)
+#define DMPH_FLAG_WALL_DEM_COEFFS (1u << 2) /* also compute the (output-only) DEM constants of wall particles */
+#define DMPH_FLAG_RIGID_CLUMPS (1u << 3)    /* debris bodies move as rigid clumps (no reference counterpart) */
+#define DMPH_FLAG_ALL_NEIGHBOR_COUNTS (1u << 4) /* keep NeighborCount for every particle (VTK "neighbor") */
+
+/*
+ * Simulation parameters: the keywords of dem.data
+ * (readDataFile, source/DEM-MPH.cpp:621-679) plus the grid header
+ * (readGridFile, source/DEM-MPH.cpp:689-702).  RadiusRatioG is forced equal
+ * to RadiusRatioA as in the reference (source/DEM-MPH.cpp:1009).
+ */
+typedef struct dmph_params {
+    int32_t dim;       /* 2: the reference's TWO_DIMENSIONAL build (source/DEM-MPH.cpp:39); 3: the 3D branches */
+    int32_t precision; /* DMPH_PRECISION_* */
+    uint32_t flags;    /* DMPH_FLAG_* */
+    int32_t reserved0;
+    double dt;
+    double dem_dt;
+    double output_interval;
+    double vtk_output_interval;
+    double end_time;
+    double radius_ratio_a;
+    double radius_ratio_p;
+    double radius_ratio_v;
+    double density[DMPH_TYPE_COUNT];
+    double bulk_modulus[DMPH_TYPE_COUNT];
+    double bulk_viscosity[DMPH_TYPE_COUNT];
+    double shear_viscosity[DMPH_TYPE_COUNT];
+    double surface_tension[DMPH_TYPE_COUNT];
+    double interaction_ratio[DMPH_TYPE_COUNT][DMPH_TYPE_COUNT];
+    double gravity[3];
+    double young_modulus[DMPH_TYPE_COUNT];
+    double poisson_ratio[DMPH_TYPE_COUNT];
+    double restitution_coefficient[DMPH_TYPE_COUNT];
+    double viscous_friction_coefficient[DMPH_TYPE_COUNT];
+    double wall_center[DMPH_TYPE_COUNT][3];
+    double wall_velocity[DMPH_TYPE_COUNT][3];
+    double wall_omega[DMPH_TYPE_COUNT][3];
+    /* grid-file header */
+    double time;
+    double particle_spacing;
+    double domain_min[3];
+    double domain_max[3];
+} dmph_params;
+
+typedef struct dmph_ctx dmph_ctx;
+
+/* ---------------------------------------------------------------- host I/O */
+
+/* Fill defaults (the reference's static initialisers, source/DEM-MPH.cpp:61-75,
+ * 159, 238-250) into *p: dt = dem_dt = 1e100, everything else 0, dim = 3. */
+void dmph_params_default(dmph_params *p);
+
+/* Parse a dem.data keyword file into *p (readDataFile, source/DEM-MPH.cpp:621-679).
+ * '#' lines are comments; unknown lines are reported through
+ * dmph_io_last_message() and ignored, like the reference. */
+int dmph_read_data_file(const char *path, dmph_params *p);
+
+/* Read a .grid / .prof file (readGridFile, source/DEM-MPH.cpp:681-851).
+ * First call with type == NULL to get *n; then call again with arrays of n
+ * (type) and 3n (x3, v3) elements.  The header fills p->time,
+ * p->particle_spacing, p->domain_min/max. */
+int dmph_read_grid_file(const char *path, dmph_params *p, int *n, int *type, double *x3, double *v3);
+
+/* Write a .prof file (writeProfFile, source/DEM-MPH.cpp:853-877): same
+ * header and "%d %e %e %e  %e %e %e" rows, particles in the solver's current
+ * (sorted) order. */
+int dmph_write_prof_file(const char *path, const dmph_params *p, int n, const int *type, const double *x3,
+                         const double *v3);
+
+/* Last informational message of the I/O layer (invalid data-file lines). */
+const char *dmph_io_last_message(void);
+
+/* ------------------------------------------------------------ solver context */
+
+/*
+ * Create a solver on the current CUDA device and upload the particles.
+ * Replaces the initialisation of main (source/DEM-MPH.cpp:370-426):
+ * initializeWeight :1007, initializeFluid :1128, initializeWall :1166,
+ * initializeDomain :1207, then the first cell sort, neighbour build and
+ * density evaluation (:419-425).
+ */
+int dmph_create(const dmph_params *p, int n, const int *type, const double *x3, const double *v3, dmph_ctx **out);
+
+/* Advance nsteps explicit steps: one iteration of the reference main loop
+ * (source/DEM-MPH.cpp:450-579) each, without file output. */
+int dmph_step(dmph_ctx *ctx, int nsteps);
+
+/* Same as dmph_step, and report the device time of the nsteps as measured by
+ * CUDA events recorded on the context's stream. */
+int dmph_step_timed(dmph_ctx *ctx, int nsteps, float *device_ms);
+
+/* Copy the particle state to host arrays in the solver's current (sorted)
+ * order.  Any pointer may be NULL.  orig_id is the reference's ParticleIndex
+ * (source/DEM-MPH.cpp:82): the row of the particle in the input grid. */
+int dmph_get_state(dmph_ctx *ctx, int *type, double *x3, double *v3, int *orig_id);
+
+/* Overwrite positions and velocities (current order, 3n each).  Used by
+ * host-driven coupling loops; takes effect at the next step. */
+int dmph_set_state(dmph_ctx *ctx, const double *x3, const double *v3);
+
+/* Per-particle fields, current order; `out` holds n (scalars) or 3n (vectors)
+ * values of the type given beside each id. */
+enum dmph_field {
+    DMPH_FIELD_FORCE = 0,               /* double[3n]  Force :87 */
+    DMPH_FIELD_VOL_STRAIN_P = 1,        /* double[n]   VolStrainP :141 */
+    DMPH_FIELD_DIVERGENCE_P = 2,        /* double[n]   DivergenceP :142 */
+    DMPH_FIELD_PRESSURE_P = 3,          /* double[n]   PressureP :143 */
+    DMPH_FIELD_DENSITY_A = 4,           /* double[n]   DensityA :138 */
+    DMPH_FIELD_GRAVITY_CENTER = 5,      /* double[3n]  GravityCenter :139 */
+    DMPH_FIELD_PRESSURE_A = 6,          /* double[n]   PressureA :140 */
+    DMPH_FIELD_NORMAL_SPRING = 7,       /* double[n]   NormalSpringConstant :190 */
+    DMPH_FIELD_NORMAL_DAMPING = 8,      /* double[n]   NormalViscousDampingConstant :192 */
+    DMPH_FIELD_TANGENTIAL_SPRING = 9,   /* double[n]   TangentialSpringConstant :191 */
+    DMPH_FIELD_TANGENTIAL_DAMPING = 10, /* double[n]   TangentialViscousDampingConstant :193 */
+    DMPH_FIELD_ALPHA = 11,              /* double[n]   alpha (solid volume fraction) :194 */
+    DMPH_FIELD_DRAG_C = 12,             /* double[n]   DragC :195 */
+    DMPH_FIELD_NEIGHBOR_COUNT = 13,     /* int32[n]    NeighborCount :88 (rebuild time) */
+    DMPH_FIELD_SOLID_NEIGHBOR_COUNT = 14, /* int32[n]  SolidNeighborCount :94 (rebuild time) */
+    DMPH_FIELD_CELL_INDEX = 15,         /* int32[n]    sorted cell key CellIndex :121 */
+    DMPH_FIELD_MASS = 16,               /* double[n]   Mass :84 */
+    DMPH_FIELD_COUNT_ = 17
+};
+int dmph_get_field(dmph_ctx *ctx, int field_id, void *out);
+
+/* Scalars of the context. */
+typedef struct dmph_info {
+    int32_t n;                 /* ParticleCount */
+    int32_t n_fluid, n_solid, n_wall;
+    int32_t cell_count[3];     /* CellCount :116 */
+    int32_t total_cell_count;  /* TotalCellCount :117 */
+    int32_t power_count;       /* PowerParticleCount :113 */
+    int32_t dem_substeps;      /* (int)(Dt/DEMDt) :434 */
+    int64_t steps;             /* steps advanced since create */
+    int64_t rebuilds;          /* neighbour rebuilds since create (the initial one excluded) */
+    double time;               /* Time :69 */
+    double cell_width[3];      /* CellWidth :115 */
+    double n0a, n0p, r2g;      /* :248-250 */
+    double max_radius;         /* MaxRadius :238 */
+    int32_t num_bodies;        /* rigid clumps (0 unless DMPH_FLAG_RIGID_CLUMPS) */
+    int32_t surface_tension;   /* 1 if the surface-tension passes run */
+} dmph_info;
+int dmph_get_info(dmph_ctx *ctx, dmph_info *info);
+
+/*
+ * Neighbour list in the reference's CSR form (calculateNeighbor,
+ * source/DEM-MPH.cpp:1521-1851): for every particle, all particles within
+ * MaxRadius+MARGIN at the last rebuild, fluid then solid then wall cells of
+ * the periodic 3x3(x3) stencil; ptr has n+1 entries.  Call first with
+ * ind == NULL to get the total count in *ptr[n].  The timestep path never
+ * materialises this list (it traverses the same cells directly); this entry
+ * point exists so the neighbour sets can be checked against the reference.
+ */
+int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind, int64_t capacity);
+
+/* Release the context and its device memory. */
+int dmph_destroy(dmph_ctx *ctx);
+
+/* Message of the last failing call on ctx (or of the last failing
+ * dmph_create when ctx is NULL).  Never NULL. */
+const char *dmph_last_error(dmph_ctx *ctx);
+
+/* Library build string (compiler, arch), never NULL. */
+const char *dmph_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DMPH_H_INCLUDED */

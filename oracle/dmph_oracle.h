@@ -1,0 +1,40 @@
+/*
+ * dmph_oracle.h — CPU restatement of the reference DEM-MPH explicit step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker the GPU library is compared
+ * against; it is never linked into libdmph.so, the `dem_mph` executable or
+ * anything the timestep path calls.  Only tests/, __graft_entry__.smoke() and
+ * the cpu_baseline leg of bench.py load it.
+ *
+ * It restates, in plain C with OpenMP, the FP64 algorithm of
+ * source/DEM-MPH.cpp (Ryo1011gd/DEM_MPH), including its quirks (see the
+ * comments at each function).  It is pinned against the reference itself:
+ * oracle/Makefile builds the reference's own source into oracle/_ref/, and
+ * tests/test_oracle_pin.py and the committed golden fixtures under
+ * tests/golden/ check that this restatement reproduces it bit for bit.
+ */
+#ifndef DMPH_ORACLE_H
+#define DMPH_ORACLE_H
+
+#include "../include/dmph.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dmph_oracle dmph_oracle;
+
+dmph_oracle *dmph_oracle_create(const dmph_params *p, int n, const int *type, const double *x3, const double *v3);
+int dmph_oracle_step(dmph_oracle *o, int nsteps);
+/* number of elements of a named array (see dmph_oracle_get) or -1 */
+long dmph_oracle_size(dmph_oracle *o, const char *name);
+/* copy a named array (names as in the reference: "Position", "Force", ...) */
+int dmph_oracle_get(dmph_oracle *o, const char *name, void *out);
+/* scalar by name ("Time", "N0a", "Rebuilds", ...) */
+double dmph_oracle_scalar(dmph_oracle *o, const char *name);
+void dmph_oracle_destroy(dmph_oracle *o);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

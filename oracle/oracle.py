@@ -1,0 +1,112 @@
+"""ctypes wrapper of liboracle.so, the CPU restatement of the reference step.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py, never by the dem_mph_b200 package.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+_lib = None
+
+INT_FIELDS = {"ParticleIndex", "Property", "NeighborCount", "FluidNeighborCount",
+              "SolidNeighborCount", "CellIndex", "CellParticle", "NeighborInd",
+              "CellFluidParticleBegin", "CellFluidParticleEnd", "CellSolidParticleBegin",
+              "CellSolidParticleEnd", "CellWallParticleBegin", "CellWallParticleEnd"}
+VEC_FIELDS = {"Position", "Velocity", "Force", "GravityCenter", "NeighborCalculatedPosition"}
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("oracle/liboracle.so is not built (make -C oracle oracle)")
+        L = C.CDLL(LIB_PATH)
+        L.dmph_oracle_create.restype = C.c_void_p
+        L.dmph_oracle_create.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dmph_oracle_step.argtypes = [C.c_void_p, C.c_int]
+        L.dmph_oracle_size.restype = C.c_long
+        L.dmph_oracle_size.argtypes = [C.c_void_p, C.c_char_p]
+        L.dmph_oracle_get.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+        L.dmph_oracle_scalar.restype = C.c_double
+        L.dmph_oracle_scalar.argtypes = [C.c_void_p, C.c_char_p]
+        L.dmph_oracle_destroy.argtypes = [C.c_void_p]
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """FP64 CPU restatement of the reference solver on one scene."""
+
+    def __init__(self, params, typ, x, v):
+        L = lib()
+        self._typ = np.ascontiguousarray(typ, dtype=np.int32)
+        xx = np.ascontiguousarray(x, dtype=np.float64)
+        vv = np.ascontiguousarray(v, dtype=np.float64)
+        self.n = len(self._typ)
+        self._h = L.dmph_oracle_create(C.byref(params), self.n, self._typ.ctypes.data,
+                                       xx.ctypes.data, vv.ctypes.data)
+        if not self._h:
+            raise ValueError("dmph_oracle_create rejected the scene")
+
+    def step(self, n=1):
+        rc = lib().dmph_oracle_step(self._h, n)
+        if rc != 0:
+            raise RuntimeError("dmph_oracle_step failed (%d)" % rc)
+
+    def get(self, name):
+        L = lib()
+        size = L.dmph_oracle_size(self._h, name.encode())
+        if size < 0:
+            raise KeyError(name)
+        if name == "NeighborPtr":
+            out = np.empty(size, dtype=np.int64)
+        elif name in INT_FIELDS:
+            out = np.empty(size, dtype=np.int32)
+        else:
+            out = np.empty(size, dtype=np.float64)
+        L.dmph_oracle_get(self._h, name.encode(), out.ctypes.data)
+        if name in VEC_FIELDS:
+            out = out.reshape(-1, 3)
+        return out
+
+    def scalar(self, name):
+        return lib().dmph_oracle_scalar(self._h, name.encode())
+
+    def close(self):
+        if self._h:
+            lib().dmph_oracle_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def read_ref_dump(d):
+    """Read one step directory written by oracle/_ref/ref_dump*."""
+    out = {}
+    for fn in os.listdir(d):
+        base, ext = os.path.splitext(fn)
+        path = os.path.join(d, fn)
+        if ext == ".f64":
+            a = np.fromfile(path, dtype=np.float64)
+            out[base] = a.reshape(-1, 3) if base in VEC_FIELDS else a
+        elif ext == ".i32":
+            out[base] = np.fromfile(path, dtype=np.int32)
+        elif ext == ".i64":
+            out[base] = np.fromfile(path, dtype=np.int64)
+        elif fn == "meta.txt":
+            meta = {}
+            for line in open(path):
+                k, *vals = line.split()
+                meta[k] = [float(s) for s in vals] if len(vals) > 1 else float(vals[0])
+            out["meta"] = meta
+    return out
