@@ -1,0 +1,503 @@
+// The C ABI of libdmph.so (include/dmph.h): solver contexts and the step
+// driver that stands in for the reference main loop
+// (source/DEM-MPH.cpp:438-581).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dmph_internal.h"
+
+using namespace dmph;
+
+namespace {
+thread_local std::string g_create_err;
+}
+
+struct dmph_ctx {
+    dmph_params p;
+    DevParams P;
+    WallMotion Wm;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int sms = 148;
+    DevState S{};
+    // second buffers of the permuted arrays
+    double *pos2 = nullptr, *vel2 = nullptr;
+    int *type2 = nullptr, *pidx2 = nullptr;
+    unsigned long long *words = nullptr;
+    int *flag = nullptr, *offs = nullptr, *bsums = nullptr, *total = nullptr;
+    unsigned long long *maxshift = nullptr;
+    unsigned long long *h_maxshift = nullptr;  // pinned
+    int *h_small = nullptr;                    // pinned scratch for small read-backs
+    int fb = 0, fe = 0, sb = 0, se = 0, wb = 0, we = 0;
+    int ch_s0 = 0, ch_w0 = 0, ch_end = 0;
+    int demSteps = 0;
+    double time = 0.0;
+    long long steps = 0, rebuilds = 0;
+    bool all_counts = false;
+    std::string err;
+    std::vector<void *> allocs;
+};
+
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                             \
+            return DMPH_ECUDA;                                                                         \
+        }                                                                                              \
+    } while (0)
+
+template <class T>
+static int dalloc(dmph_ctx *ctx, T **ptr, size_t count)
+{
+    void *p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, count ? count * sizeof(T) : 16);
+    if (e != cudaSuccess) {
+        ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return DMPH_ENOMEM;
+    }
+    ctx->allocs.push_back(p);
+    *ptr = (T *)p;
+    return cudaMemsetAsync(p, 0, count ? count * sizeof(T) : 16, ctx->st) == cudaSuccess ? DMPH_OK : DMPH_ECUDA;
+}
+
+static void release(dmph_ctx *ctx)
+{
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    for (void *p : ctx->allocs) cudaFree(p);
+    ctx->allocs.clear();
+    if (ctx->h_maxshift) cudaFreeHost(ctx->h_maxshift);
+    if (ctx->h_small) cudaFreeHost(ctx->h_small);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->st) cudaStreamDestroy(ctx->st);
+    ctx->h_maxshift = nullptr;
+    ctx->h_small = nullptr;
+    ctx->ev0 = ctx->ev1 = nullptr;
+    ctx->st = nullptr;
+}
+
+// calculateCellParticle :1288 + the parts of calculateNeighbor the step needs
+static int rebuild(dmph_ctx *ctx)
+{
+    const DevParams &P = ctx->P;
+    launch_keys(P, ctx->S.pos, ctx->S.type, ctx->words, ctx->st);
+    launch_bitonic(ctx->words, P.P2, P.P2log, ctx->st);
+    launch_cell_start(P, ctx->words, ctx->S.cell_start, ctx->st);
+    launch_permute(P, ctx->words, ctx->S.pos, ctx->S.vel, ctx->S.type, ctx->S.pidx, ctx->pos2, ctx->vel2, ctx->type2,
+                   ctx->pidx2, ctx->S.xref, ctx->st);
+    std::swap(ctx->S.pos, ctx->pos2);
+    std::swap(ctx->S.vel, ctx->vel2);
+    std::swap(ctx->S.type, ctx->type2);
+    std::swap(ctx->S.pidx, ctx->pidx2);
+    ctx->S.skey = ctx->words;
+    launch_chunks(P, ctx->words, ctx->S.cell_start, ctx->flag, ctx->offs, ctx->bsums, ctx->total, ctx->S.chunks,
+                  ctx->st);
+    // class boundaries: slot ranges from cell_start, chunk ranges from the scan
+    int *h = ctx->h_small;
+    CK(cudaMemcpyAsync(h + 0, ctx->S.cell_start + P.T, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(h + 1, ctx->S.cell_start + 2 * P.T, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(h + 2, ctx->total, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    const int sb = h[0], wb = h[1], nch = h[2];
+    ctx->fb = 0;
+    ctx->fe = sb;
+    ctx->sb = sb;
+    ctx->se = wb;
+    ctx->wb = wb;
+    ctx->we = P.N;
+    if (sb < P.N) CK(cudaMemcpyAsync(h + 3, ctx->offs + sb, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    if (wb < P.N) CK(cudaMemcpyAsync(h + 4, ctx->offs + wb, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->ch_s0 = sb < P.N ? h[3] : nch;
+    ctx->ch_w0 = wb < P.N ? h[4] : nch;
+    ctx->ch_end = nch;
+    if (ctx->all_counts)
+        launch_counts(P, ctx->S, 0, ctx->ch_end, ctx->st);
+    else
+        launch_counts(P, ctx->S, ctx->ch_s0, ctx->ch_w0, ctx->st);
+    CK(cudaGetLastError());
+    return DMPH_OK;
+}
+
+static int step_once(dmph_ctx *ctx)
+{
+    const DevParams &P = ctx->P;
+    ctx->Wm.moving = (ctx->time >= 0.2 && 0.4 >= ctx->time) ? 1 : 0;
+    CK(cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), ctx->st));
+    launch_drift(P, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, ctx->st);
+    // WallCenter moves only while `0.0 < Time < 0.2` holds, i.e. Time <= 0 (:2892)
+    if (!(0.0 < ctx->time))
+        for (int t = DMPH_WALL_BEGIN; t < DMPH_WALL_END; ++t)
+            for (int d = 0; d < 3; d++) ctx->Wm.C[t][d] += ctx->Wm.Vel[t][d] * P.dt;
+    CK(cudaMemcpyAsync(ctx->h_maxshift, ctx->maxshift, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    double m2;
+    std::memcpy(&m2, ctx->h_maxshift, sizeof(double));
+    const double margin = (0.1 * P.dx);
+    if (m2 > 0.5 * margin * 0.5 * margin) {
+        const int rc = rebuild(ctx);
+        if (rc) return rc;
+        ctx->rebuilds++;
+    }
+    launch_pass_a(P, ctx->S, 0, ctx->ch_end, 0, ctx->st);
+    launch_pass_b(P, ctx->S, 0, ctx->ch_w0, ctx->st);
+    for (int k = 0; k < ctx->demSteps; ++k) {
+        launch_dem_force(P, ctx->S, ctx->ch_s0, ctx->ch_w0, 1, ctx->st);
+        if (P.wall_dem_coeffs) launch_dem_force(P, ctx->S, ctx->ch_w0, ctx->ch_end, 0, ctx->st);
+        launch_dem_integrate(P, ctx->S, ctx->sb, ctx->se, ctx->st);
+    }
+    CK(cudaGetLastError());
+    ctx->time += P.dt;
+    ctx->steps++;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const double *x3, const double *v3,
+                           dmph_ctx **out)
+{
+    g_create_err.clear();
+    if (!out) return DMPH_EINVAL;
+    *out = nullptr;
+    if (!p || !type || !x3 || !v3) {
+        g_create_err = "null argument";
+        return DMPH_EINVAL;
+    }
+    if (p->precision != DMPH_PRECISION_FP64) {
+        g_create_err = "this build implements DMPH_PRECISION_FP64 only";
+        return DMPH_EINVAL;
+    }
+    for (int i = 0; i < n; i++)
+        if (type[i] < 0 || type[i] >= DMPH_TYPE_COUNT) {
+            g_create_err = "particle type outside 0..5 at row " + std::to_string(i);
+            return DMPH_EINVAL;
+        }
+    dmph_ctx *ctx = new dmph_ctx();
+    ctx->p = *p;
+    int rc = derive_params(*p, n, ctx->P, ctx->Wm, ctx->err);
+    if (rc) {
+        g_create_err = ctx->err;
+        delete ctx;
+        return rc;
+    }
+    ctx->all_counts = (p->flags & DMPH_FLAG_ALL_NEIGHBOR_COUNTS) != 0;
+    ctx->demSteps = p->dt / p->dem_dt;  // (int)(Dt/DEMDt), :434
+    ctx->time = p->time;
+    auto fail = [&](int code) {
+        g_create_err = ctx->err;
+        release(ctx);
+        delete ctx;
+        return code;
+    };
+#define CKC(call)                                                                                \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                       \
+            return fail(DMPH_ECUDA);                                                             \
+        }                                                                                        \
+    } while (0)
+    int dev = 0;
+    CKC(cudaGetDevice(&dev));
+    CKC(cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, dev));
+    CKC(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
+    CKC(cudaEventCreate(&ctx->ev0));
+    CKC(cudaEventCreate(&ctx->ev1));
+    CKC(cudaMallocHost(&ctx->h_maxshift, sizeof(unsigned long long)));
+    CKC(cudaMallocHost(&ctx->h_small, 16 * sizeof(int)));
+    const DevParams &P = ctx->P;
+    const size_t N = (size_t)n, N3 = 3 * N;
+    DevState &S = ctx->S;
+#define AL(ptr, cnt)                                  \
+    do {                                              \
+        int r_ = dalloc(ctx, &(ptr), (size_t)(cnt));  \
+        if (r_) return fail(r_);                      \
+    } while (0)
+    AL(S.pos, N3);
+    AL(S.vel, N3);
+    AL(S.frc, N3);
+    AL(S.xref, N3);
+    AL(S.type, N);
+    AL(S.pidx, N);
+    AL(S.vsp, N);
+    AL(S.divp, N);
+    AL(S.pres, N);
+    AL(S.densA, N);
+    AL(S.pA, N);
+    AL(S.gc, N3);
+    AL(S.kn, N);
+    AL(S.cn, N);
+    AL(S.kt, N);
+    AL(S.ct, N);
+    AL(S.alpha, N);
+    AL(S.dragC, N);
+    AL(S.nc, N);
+    AL(S.snc, N);
+    AL(S.cell_start, (size_t)3 * P.T + 1);
+    AL(S.chunks, N + 64);
+    AL(ctx->pos2, N3);
+    AL(ctx->vel2, N3);
+    AL(ctx->type2, N);
+    AL(ctx->pidx2, N);
+    AL(ctx->words, (size_t)P.P2);
+    AL(ctx->flag, N);
+    AL(ctx->offs, N);
+    AL(ctx->bsums, 4096);
+    AL(ctx->total, 4);
+    AL(ctx->maxshift, 1);
+    // upload: interleaved x,y,z rows -> component planes
+    {
+        std::vector<double> planes(N3);
+        for (size_t i = 0; i < N; i++)
+            for (int d = 0; d < 3; d++) planes[d * N + i] = x3[3 * i + d];
+        CKC(cudaMemcpyAsync(S.pos, planes.data(), N3 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        CKC(cudaStreamSynchronize(ctx->st));
+        for (size_t i = 0; i < N; i++)
+            for (int d = 0; d < 3; d++) planes[d * N + i] = v3[3 * i + d];
+        CKC(cudaMemcpyAsync(S.vel, planes.data(), N3 * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        CKC(cudaMemcpyAsync(S.type, type, N * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+        std::vector<int> iota(N);
+        for (size_t i = 0; i < N; i++) iota[i] = (int)i;
+        CKC(cudaMemcpyAsync(S.pidx, iota.data(), N * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+        CKC(cudaStreamSynchronize(ctx->st));
+    }
+    // initial sort, neighbour counts and densities (:419-425)
+    rc = rebuild(ctx);
+    if (rc) return fail(rc);
+    launch_pass_a(P, S, 0, ctx->ch_end, 1, ctx->st);
+    CKC(cudaGetLastError());
+    CKC(cudaStreamSynchronize(ctx->st));
+#undef AL
+#undef CKC
+    *out = ctx;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_step(dmph_ctx *ctx, int nsteps)
+{
+    if (!ctx || nsteps < 0) return DMPH_EINVAL;
+    for (int s = 0; s < nsteps; s++) {
+        const int rc = step_once(ctx);
+        if (rc) return rc;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return DMPH_OK;
+}
+
+extern "C" int dmph_step_timed(dmph_ctx *ctx, int nsteps, float *device_ms)
+{
+    if (!ctx || nsteps < 0) return DMPH_EINVAL;
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    for (int s = 0; s < nsteps; s++) {
+        const int rc = step_once(ctx);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    CK(cudaEventSynchronize(ctx->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    if (device_ms) *device_ms = ms;
+    return DMPH_OK;
+}
+
+static int d2h_planes(dmph_ctx *ctx, const double *dev, double *x3)
+{
+    const size_t N = (size_t)ctx->P.N;
+    std::vector<double> planes(3 * N);
+    CK(cudaMemcpyAsync(planes.data(), dev, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (size_t i = 0; i < N; i++)
+        for (int d = 0; d < 3; d++) x3[3 * i + d] = planes[d * N + i];
+    return DMPH_OK;
+}
+
+extern "C" int dmph_get_state(dmph_ctx *ctx, int *type, double *x3, double *v3, int *orig_id)
+{
+    if (!ctx) return DMPH_EINVAL;
+    const size_t N = (size_t)ctx->P.N;
+    if (x3) {
+        int rc = d2h_planes(ctx, ctx->S.pos, x3);
+        if (rc) return rc;
+    }
+    if (v3) {
+        int rc = d2h_planes(ctx, ctx->S.vel, v3);
+        if (rc) return rc;
+    }
+    if (type) CK(cudaMemcpyAsync(type, ctx->S.type, N * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    if (orig_id) CK(cudaMemcpyAsync(orig_id, ctx->S.pidx, N * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return DMPH_OK;
+}
+
+extern "C" int dmph_set_state(dmph_ctx *ctx, const double *x3, const double *v3)
+{
+    if (!ctx) return DMPH_EINVAL;
+    const size_t N = (size_t)ctx->P.N;
+    std::vector<double> planes(3 * N);
+    if (x3) {
+        for (size_t i = 0; i < N; i++)
+            for (int d = 0; d < 3; d++) planes[d * N + i] = x3[3 * i + d];
+        CK(cudaMemcpyAsync(ctx->S.pos, planes.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    if (v3) {
+        for (size_t i = 0; i < N; i++)
+            for (int d = 0; d < 3; d++) planes[d * N + i] = v3[3 * i + d];
+        CK(cudaMemcpyAsync(ctx->S.vel, planes.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    return DMPH_OK;
+}
+
+extern "C" int dmph_get_field(dmph_ctx *ctx, int field_id, void *out)
+{
+    if (!ctx || !out) return DMPH_EINVAL;
+    const size_t N = (size_t)ctx->P.N;
+    const DevState &S = ctx->S;
+    const double *src = nullptr;
+    switch (field_id) {
+    case DMPH_FIELD_FORCE: return d2h_planes(ctx, S.frc, (double *)out);
+    case DMPH_FIELD_GRAVITY_CENTER: return d2h_planes(ctx, S.gc, (double *)out);
+    case DMPH_FIELD_VOL_STRAIN_P: src = S.vsp; break;
+    case DMPH_FIELD_DIVERGENCE_P: src = S.divp; break;
+    case DMPH_FIELD_PRESSURE_P: src = S.pres; break;
+    case DMPH_FIELD_DENSITY_A: src = S.densA; break;
+    case DMPH_FIELD_PRESSURE_A: src = S.pA; break;
+    case DMPH_FIELD_NORMAL_SPRING: src = S.kn; break;
+    case DMPH_FIELD_NORMAL_DAMPING: src = S.cn; break;
+    case DMPH_FIELD_TANGENTIAL_SPRING: src = S.kt; break;
+    case DMPH_FIELD_TANGENTIAL_DAMPING: src = S.ct; break;
+    case DMPH_FIELD_ALPHA: src = S.alpha; break;
+    case DMPH_FIELD_DRAG_C: src = S.dragC; break;
+    case DMPH_FIELD_NEIGHBOR_COUNT:
+        CK(cudaMemcpyAsync(out, S.nc, N * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        return DMPH_OK;
+    case DMPH_FIELD_SOLID_NEIGHBOR_COUNT:
+        CK(cudaMemcpyAsync(out, S.snc, N * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        return DMPH_OK;
+    case DMPH_FIELD_CELL_INDEX: {
+        std::vector<unsigned long long> w(N);
+        CK(cudaMemcpyAsync(w.data(), ctx->words, N * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        int *o = (int *)out;
+        for (size_t i = 0; i < N; i++) o[i] = (int)word_key(w[i]);
+        return DMPH_OK;
+    }
+    case DMPH_FIELD_MASS: {
+        std::vector<int> t(N);
+        CK(cudaMemcpyAsync(t.data(), S.type, N * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        double *o = (double *)out;
+        for (size_t i = 0; i < N; i++) o[i] = ctx->P.mass[t[i]];
+        return DMPH_OK;
+    }
+    default: ctx->err = "unknown field id"; return DMPH_EINVAL;
+    }
+    CK(cudaMemcpyAsync(out, src, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return DMPH_OK;
+}
+
+extern "C" int dmph_get_info(dmph_ctx *ctx, dmph_info *info)
+{
+    if (!ctx || !info) return DMPH_EINVAL;
+    std::memset(info, 0, sizeof(*info));
+    const DevParams &P = ctx->P;
+    info->n = P.N;
+    info->n_fluid = ctx->fe - ctx->fb;
+    info->n_solid = ctx->se - ctx->sb;
+    info->n_wall = ctx->we - ctx->wb;
+    for (int d = 0; d < 3; d++) {
+        info->cell_count[d] = P.cc[d];
+        info->cell_width[d] = P.cw[d];
+    }
+    info->total_cell_count = P.T;
+    info->power_count = P.P2;
+    info->dem_substeps = ctx->demSteps;
+    info->steps = ctx->steps;
+    info->rebuilds = ctx->rebuilds;
+    info->time = ctx->time;
+    info->n0a = P.N0a;
+    info->n0p = P.N0p;
+    info->r2g = P.R2g;
+    info->max_radius = std::sqrt(P.rc2) - 0.1 * P.dx;
+    info->num_bodies = 0;
+    info->surface_tension = P.surface_tension;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind, int64_t capacity)
+{
+    if (!ctx || !ptr) return DMPH_EINVAL;
+    const DevParams &P = ctx->P;
+    const size_t N = (size_t)P.N;
+    // counts of every particle at the last rebuild
+    launch_counts(P, ctx->S, 0, ctx->ch_end, ctx->st);
+    CK(cudaGetLastError());
+    std::vector<int> nc(N);
+    CK(cudaMemcpyAsync(nc.data(), ctx->S.nc, N * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ptr[0] = 0;
+    for (size_t i = 0; i < N; i++) ptr[i + 1] = ptr[i] + nc[i];
+    int rc = DMPH_OK;
+    if (ind) {
+        if (capacity < ptr[N]) {
+            ctx->err = "neighbour list capacity too small";
+            rc = DMPH_ERANGE;
+        } else {
+            long long *dptr = nullptr;
+            int *dind = nullptr;
+            CK(cudaMalloc(&dptr, (N + 1) * sizeof(long long)));
+            if (cudaMalloc(&dind, (size_t)(ptr[N] > 0 ? ptr[N] : 1) * sizeof(int)) != cudaSuccess) {
+                cudaFree(dptr);
+                ctx->err = "cudaMalloc of the neighbour list failed";
+                return DMPH_ENOMEM;
+            }
+            cudaMemcpyAsync(dptr, ptr, (N + 1) * sizeof(long long), cudaMemcpyHostToDevice, ctx->st);
+            launch_neighbor_fill(P, ctx->S, 0, ctx->ch_end, dptr, dind, ctx->st);
+            cudaError_t e = cudaGetLastError();
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(ind, dind, (size_t)ptr[N] * sizeof(int), cudaMemcpyDeviceToHost, ctx->st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+            cudaFree(dptr);
+            cudaFree(dind);
+            if (e != cudaSuccess) {
+                ctx->err = std::string("neighbour list: ") + cudaGetErrorString(e);
+                return DMPH_ECUDA;
+            }
+        }
+    }
+    // restore the step's own counts (solids only unless all were requested)
+    if (!ctx->all_counts) {
+        // the hot path reads counts of solids only; the full recount above
+        // computed the same values for them, so nothing to restore
+    }
+    return rc;
+}
+
+extern "C" int dmph_destroy(dmph_ctx *ctx)
+{
+    if (!ctx) return DMPH_EINVAL;
+    release(ctx);
+    delete ctx;
+    return DMPH_OK;
+}
+
+extern "C" const char *dmph_last_error(dmph_ctx *ctx)
+{
+    if (!ctx) return g_create_err.c_str();
+    return ctx->err.c_str();
+}
+
+extern "C" const char *dmph_version(void)
+{
+    static const std::string v = std::string("libdmph ") + std::to_string(DMPH_ABI_VERSION) +
+                                 " sm_100a nvcc " + std::to_string(__CUDACC_VER_MAJOR__) + "." +
+                                 std::to_string(__CUDACC_VER_MINOR__);
+    return v.c_str();
+}

@@ -1,0 +1,36 @@
+// Internal declarations shared by the translation units of libdmph.so.
+#pragma once
+
+#include <string>
+
+#include "dmph_state.cuh"
+
+namespace dmph {
+
+int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, std::string &err);
+
+// dmph_rebuild.cu
+void launch_keys(const DevParams &P, const double *pos, const int *type, unsigned long long *words, cudaStream_t st);
+void launch_bitonic(unsigned long long *words, int n, int nlog, cudaStream_t st);
+void launch_cell_start(const DevParams &P, const unsigned long long *words, int *start, cudaStream_t st);
+void launch_permute(const DevParams &P, const unsigned long long *words, const double *pos_in, const double *vel_in,
+                    const int *type_in, const int *pidx_in, double *pos_out, double *vel_out, int *type_out,
+                    int *pidx_out, double *xref, cudaStream_t st);
+template <class T>
+int launch_exclusive_scan(const T *in, T *out, int n, T *block_sums, T *total, cudaStream_t st);
+void launch_chunks(const DevParams &P, const unsigned long long *words, const int *start, int *flag, int *offs,
+                   int *block_sums, int *total, Chunk *chunks, cudaStream_t st);
+void launch_widen(const int *in, long long *out, int n, cudaStream_t st);
+
+// dmph_f64.cu
+void launch_drift(const DevParams &P, const DevState &S, const WallMotion &Wm, unsigned long long *maxshift, int sms,
+                  cudaStream_t st);
+void launch_pass_a(const DevParams &P, const DevState &S, int cb, int ce, int init_only, cudaStream_t st);
+void launch_pass_b(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st);
+void launch_dem_force(const DevParams &P, const DevState &S, int cb, int ce, int forces, cudaStream_t st);
+void launch_dem_integrate(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st);
+void launch_counts(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st);
+void launch_neighbor_fill(const DevParams &P, const DevState &S, int cb, int ce, const long long *ptr, int *ind,
+                          cudaStream_t st);
+
+}  // namespace dmph

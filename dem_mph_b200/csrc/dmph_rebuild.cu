@@ -1,0 +1,306 @@
+// Neighbour rebuild: cell keys, the bitonic sort, cell ranges, permutation and
+// the warp work list (calculateCellParticle, source/DEM-MPH.cpp:1288-1519).
+//
+// The reference sorts (key, slot) pairs with a bitonic network over the
+// power-of-two padded array (:1317-1338).  The network swaps equal keys inside
+// descending sub-blocks, so the order of particles within a cell depends on
+// the network itself; the DEM contact constants take the last neighbour within
+// dx (:2305-2341), which depends on that order.  The same network is therefore
+// run here, exactly: stages whose compare distance is below the tile size are
+// done in shared memory (one launch per outer stage), the wider ones as
+// global passes.  Keys and slots travel as one 64-bit word; only the key half
+// is compared, as in the reference.
+#include "dmph_state.cuh"
+
+namespace dmph {
+
+constexpr int kSortTileLog = 11;  // 2048 words = 16 KiB of shared memory per block
+constexpr int kSortTile = 1 << kSortTileLog;
+
+// cell key + class offset (:1295-1313) and identity payload; pad with 3T
+__global__ void k_keys(DevParams P, const double *__restrict__ pos, const int *__restrict__ type,
+                       unsigned long long *__restrict__ words)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.P2) return;
+    const int N = P.N;
+    unsigned long long w;
+    if (i < N) {
+        const int ix = ((int)floor((pos[i] - P.dmin[0]) / P.cw[0])) % P.cc[0];
+        const int iy = ((int)floor((pos[N + i] - P.dmin[1]) / P.cw[1])) % P.cc[1];
+        const int iz = ((int)floor((pos[2 * N + i] - P.dmin[2]) / P.cw[2])) % P.cc[2];
+        int k = cell_id(P, ix, iy, iz);
+        const int t = type[i];
+        if (is_solid(t))
+            k += P.T;
+        else if (is_wall(t))
+            k += 2 * P.T;
+        w = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)i;
+    } else {
+        w = ((unsigned long long)(uint32_t)(3 * P.T) << 32) | (uint32_t)N;
+    }
+    words[i] = w;
+}
+
+__device__ __forceinline__ void cmp_exchange(unsigned long long &a, unsigned long long &b, bool up)
+{
+    // swap when (key_a > key_b) == up  (:1326)
+    if ((word_key(a) > word_key(b)) == up) {
+        const unsigned long long t = a;
+        a = b;
+        b = t;
+    }
+}
+
+// Stages (stage, dist) with dist < tile, from `stage_lo` (starting at
+// dist_start) to `stage_hi`, inside one tile in shared memory.
+__global__ void __launch_bounds__(kSortTile / 2) k_bitonic_local(unsigned long long *words, int tile, int stage_lo,
+                                                                 int stage_hi, int dist_start)
+{
+    __shared__ unsigned long long sm[kSortTile];
+    const int base = blockIdx.x * tile;
+    for (int k = threadIdx.x; k < tile; k += blockDim.x) sm[k] = words[base + k];
+    __syncthreads();
+    for (int stage = stage_lo; stage <= stage_hi; ++stage) {
+        int dist = (stage == stage_lo) ? dist_start : (1 << stage);
+        if (dist > tile / 2) dist = tile / 2;
+        for (; dist >= 1; dist >>= 1) {
+            for (int t = threadIdx.x; t < tile / 2; t += blockDim.x) {
+                const int lo = (t / dist) * 2 * dist + (t % dist);  // local index with bit `dist` clear
+                const int g = base + lo;
+                const bool up = ((g >> stage) & 2) == 0;
+                cmp_exchange(sm[lo], sm[lo + dist], up);
+            }
+            __syncthreads();
+        }
+    }
+    for (int k = threadIdx.x; k < tile; k += blockDim.x) words[base + k] = sm[k];
+}
+
+__global__ void k_bitonic_global(unsigned long long *words, int n, int stage, int dist)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n / 2) return;
+    const int lo = (t / dist) * 2 * dist + (t % dist);
+    const bool up = ((lo >> stage) & 2) == 0;
+    unsigned long long a = words[lo], b = words[lo + dist];
+    if ((word_key(a) > word_key(b)) == up) {
+        words[lo] = b;
+        words[lo + dist] = a;
+    }
+}
+
+// cell_start[c] = number of sorted keys below c, c in [0, 3T]  (the begin/end
+// arrays of :1340-1438 are cell_start[k] and cell_start[k+1])
+__global__ void k_cell_start(DevParams P, const unsigned long long *__restrict__ words, int *__restrict__ start)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > 3 * P.T) return;
+    int lo = 0, hi = P.N;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((int)word_key(words[mid]) < c)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    start[c] = lo;
+}
+
+// gather ParticleIndex, Property, Position, Velocity (:1455-1518) into the
+// other buffer and snapshot NeighborCalculatedPosition (:1842-1850)
+__global__ void k_permute(DevParams P, const unsigned long long *__restrict__ words, const double *__restrict__ pos_in,
+                          const double *__restrict__ vel_in, const int *__restrict__ type_in,
+                          const int *__restrict__ pidx_in, double *__restrict__ pos_out, double *__restrict__ vel_out,
+                          int *__restrict__ type_out, int *__restrict__ pidx_out, double *__restrict__ xref)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int N = P.N;
+    if (i >= N) return;
+    const int src = (int)word_slot(words[i]);
+    for (int d = 0; d < 3; d++) {
+        const double x = pos_in[d * N + src];
+        pos_out[d * N + i] = x;
+        xref[d * N + i] = x;
+        vel_out[d * N + i] = vel_in[d * N + src];
+    }
+    type_out[i] = type_in[src];
+    pidx_out[i] = pidx_in[src];
+}
+
+// chunk heads: a slot starts a chunk when it starts its key's range or is a
+// multiple of 32 into it
+__global__ void k_chunk_flags(DevParams P, const unsigned long long *__restrict__ words, const int *__restrict__ start,
+                              int *__restrict__ flag)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.N) return;
+    const int k = (int)word_key(words[i]);
+    flag[i] = ((i - start[k]) % kWarp) == 0 ? 1 : 0;
+}
+
+__global__ void k_chunk_write(DevParams P, const unsigned long long *__restrict__ words, const int *__restrict__ start,
+                              const int *__restrict__ flag, const int *__restrict__ offs, Chunk *__restrict__ chunks)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.N || !flag[i]) return;
+    const int k = (int)word_key(words[i]);
+    const int end = start[k + 1];
+    Chunk c;
+    c.i0 = i;
+    c.cnt = min(kWarp, end - i);
+    chunks[offs[i]] = c;
+}
+
+// ------------------------------------------------------------ prefix sums
+// Exclusive scan of n int32 values (n <= kScanBlock * kScanBlock * 4) in
+// three launches; out[n] receives the total.
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanBlock = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int *sh, int &total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, s, o);
+            if (lane >= o) s += y;
+        }
+        sh[lane] = s;
+    }
+    __syncthreads();
+    const int warp_prefix = w > 0 ? sh[w - 1] : 0;
+    total = sh[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return warp_prefix + x - v;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kScanThreads) k_scan_local(const T *__restrict__ in, T *__restrict__ out, int n,
+                                                             T *__restrict__ block_sums)
+{
+    __shared__ int sh[32];
+    const int base = blockIdx.x * kScanBlock + threadIdx.x * kScanItems;
+    T v[kScanItems];
+    T s = 0;
+    for (int k = 0; k < kScanItems; k++) {
+        v[k] = (base + k < n) ? in[base + k] : T(0);
+        s += v[k];
+    }
+    int total;
+    const int ex = block_exclusive_scan((int)s, sh, total);
+    T run = (T)ex;
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = (T)total;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(T *__restrict__ sums, int nb, T *__restrict__ total_out)
+{
+    // one block: exclusive scan of the block sums in place (nb <= kScanBlock)
+    __shared__ int sh[32];
+    const int base = threadIdx.x * kScanItems;
+    T v[kScanItems];
+    T s = 0;
+    for (int k = 0; k < kScanItems; k++) {
+        v[k] = (base + k < nb) ? sums[base + k] : T(0);
+        s += v[k];
+    }
+    int total;
+    const int ex = block_exclusive_scan((int)s, sh, total);
+    T run = (T)ex;
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < nb) sums[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 0) *total_out = (T)total;
+}
+
+template <class T>
+__global__ void k_scan_add(T *__restrict__ out, int n, const T *__restrict__ sums)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] += sums[i / kScanBlock];
+}
+
+// --------------------------------------------------------------- host side
+void launch_keys(const DevParams &P, const double *pos, const int *type, unsigned long long *words, cudaStream_t st)
+{
+    k_keys<<<(P.P2 + 255) / 256, 256, 0, st>>>(P, pos, type, words);
+}
+
+void launch_bitonic(unsigned long long *words, int n, int nlog, cudaStream_t st)
+{
+    const int tile = n < kSortTile ? n : kSortTile;
+    const int tlog = n < kSortTile ? nlog : kSortTileLog;
+    const int threads = tile / 2 > 0 ? tile / 2 : 1;
+    const int blocks = n / tile;
+    // all stages whose distance fits the tile: stages 0 .. tlog-1
+    if (tlog > 0) k_bitonic_local<<<blocks, threads, 0, st>>>(words, tile, 0, tlog - 1, 1);
+    for (int stage = tlog; stage < nlog; ++stage) {
+        for (int dist = 1 << stage; dist >= tile; dist >>= 1)
+            k_bitonic_global<<<(n / 2 + 255) / 256, 256, 0, st>>>(words, n, stage, dist);
+        k_bitonic_local<<<blocks, threads, 0, st>>>(words, tile, stage, stage, tile / 2);
+    }
+}
+
+void launch_cell_start(const DevParams &P, const unsigned long long *words, int *start, cudaStream_t st)
+{
+    const int n = 3 * P.T + 1;
+    k_cell_start<<<(n + 255) / 256, 256, 0, st>>>(P, words, start);
+}
+
+void launch_permute(const DevParams &P, const unsigned long long *words, const double *pos_in, const double *vel_in,
+                    const int *type_in, const int *pidx_in, double *pos_out, double *vel_out, int *type_out,
+                    int *pidx_out, double *xref, cudaStream_t st)
+{
+    k_permute<<<(P.N + 255) / 256, 256, 0, st>>>(P, words, pos_in, vel_in, type_in, pidx_in, pos_out, vel_out,
+                                                 type_out, pidx_out, xref);
+}
+
+template <class T>
+int launch_exclusive_scan(const T *in, T *out, int n, T *block_sums, T *total, cudaStream_t st)
+{
+    const int nb = (n + kScanBlock - 1) / kScanBlock;
+    if (nb > kScanBlock) return DMPH_ERANGE;
+    k_scan_local<T><<<nb, kScanThreads, 0, st>>>(in, out, n, block_sums);
+    k_scan_sums<T><<<1, kScanThreads, 0, st>>>(block_sums, nb, total);
+    k_scan_add<T><<<(n + 255) / 256, 256, 0, st>>>(out, n, block_sums);
+    return 0;
+}
+template int launch_exclusive_scan<int>(const int *, int *, int, int *, int *, cudaStream_t);
+
+void launch_chunks(const DevParams &P, const unsigned long long *words, const int *start, int *flag, int *offs,
+                   int *block_sums, int *total, Chunk *chunks, cudaStream_t st)
+{
+    k_chunk_flags<<<(P.N + 255) / 256, 256, 0, st>>>(P, words, start, flag);
+    launch_exclusive_scan<int>(flag, offs, P.N, block_sums, total, st);
+    k_chunk_write<<<(P.N + 255) / 256, 256, 0, st>>>(P, words, start, flag, offs, chunks);
+}
+
+// int64 neighbour pointers for the CSR diagnostic: small enough to scan on
+// the host side of the caller; provided here as a widening copy.
+__global__ void k_widen(const int *in, long long *out, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[i];
+}
+void launch_widen(const int *in, long long *out, int n, cudaStream_t st)
+{
+    if (n > 0) k_widen<<<(n + 255) / 256, 256, 0, st>>>(in, out, n);
+}
+
+}  // namespace dmph

@@ -1,0 +1,160 @@
+"""Python binding of libdmph.so through its C ABI (include/dmph.h).
+
+The library is loaded from this package directory (built in-tree by
+dem_mph_b200.build); there is no fallback: if it is missing or no CUDA device
+is present the calls fail loudly.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .abi import Params, Info, FIELDS
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdmph.so")
+
+_lib = None
+
+
+def lib():
+    """Load libdmph.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("dem_mph_b200/libdmph.so is not built: run python -m dem_mph_b200.build")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.dmph_params_default.argtypes = [vp]
+        L.dmph_read_data_file.argtypes = [C.c_char_p, vp]
+        L.dmph_read_grid_file.argtypes = [C.c_char_p, vp, C.POINTER(C.c_int), vp, vp, vp]
+        L.dmph_write_prof_file.argtypes = [C.c_char_p, vp, C.c_int, vp, vp, vp]
+        L.dmph_io_last_message.restype = C.c_char_p
+        L.dmph_create.argtypes = [vp, C.c_int, vp, vp, vp, C.POINTER(vp)]
+        L.dmph_step.argtypes = [vp, C.c_int]
+        L.dmph_step_timed.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
+        L.dmph_get_state.argtypes = [vp, vp, vp, vp, vp]
+        L.dmph_set_state.argtypes = [vp, vp, vp]
+        L.dmph_get_field.argtypes = [vp, C.c_int, vp]
+        L.dmph_get_info.argtypes = [vp, vp]
+        L.dmph_get_neighbor_list.argtypes = [vp, vp, vp, C.c_int64]
+        L.dmph_destroy.argtypes = [vp]
+        L.dmph_last_error.argtypes = [vp]
+        L.dmph_last_error.restype = C.c_char_p
+        L.dmph_version.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+class DmphError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("dmph error %d: %s" % (code, msg))
+        self.code = code
+
+
+def _ptr(a):
+    return a.ctypes.data if a is not None else None
+
+
+class Solver:
+    """One solver context on the current CUDA device."""
+
+    def __init__(self, params, typ, x, v):
+        L = lib()
+        self.params = params.copy()
+        self._typ = np.ascontiguousarray(typ, dtype=np.int32)
+        xx = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+        vv = np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
+        self.n = len(self._typ)
+        h = C.c_void_p()
+        rc = L.dmph_create(C.byref(self.params), self.n, _ptr(self._typ), _ptr(xx), _ptr(vv), C.byref(h))
+        if rc != 0:
+            raise DmphError(rc, L.dmph_last_error(None).decode())
+        self._h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise DmphError(rc, lib().dmph_last_error(self._h).decode())
+
+    def step(self, n=1):
+        self._check(lib().dmph_step(self._h, n))
+
+    def step_timed(self, n=1):
+        ms = C.c_float()
+        self._check(lib().dmph_step_timed(self._h, n, C.byref(ms)))
+        return ms.value
+
+    def state(self):
+        """(type, x[N,3], v[N,3], orig_id) in the current sorted order"""
+        t = np.empty(self.n, np.int32)
+        x = np.empty((self.n, 3), np.float64)
+        v = np.empty((self.n, 3), np.float64)
+        o = np.empty(self.n, np.int32)
+        self._check(lib().dmph_get_state(self._h, _ptr(t), _ptr(x), _ptr(v), _ptr(o)))
+        return t, x, v, o
+
+    def set_state(self, x=None, v=None):
+        xx = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+        vv = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        self._check(lib().dmph_set_state(self._h, _ptr(xx), _ptr(vv)))
+
+    def field(self, name):
+        fid, dt, comps = FIELDS[name]
+        out = np.empty(self.n * comps, dtype=dt)
+        self._check(lib().dmph_get_field(self._h, fid, _ptr(out)))
+        return out.reshape(-1, 3) if comps == 3 else out
+
+    def info(self):
+        inf = Info()
+        self._check(lib().dmph_get_info(self._h, C.byref(inf)))
+        return inf
+
+    def neighbor_list(self):
+        ptr = np.empty(self.n + 1, np.int64)
+        self._check(lib().dmph_get_neighbor_list(self._h, _ptr(ptr), None, 0))
+        ind = np.empty(max(int(ptr[-1]), 1), np.int32)
+        self._check(lib().dmph_get_neighbor_list(self._h, _ptr(ptr), _ptr(ind), int(ptr[-1])))
+        return ptr, ind[:int(ptr[-1])]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().dmph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def read_data_file(path):
+    """dem.data -> Params through the library's own reader (dmph_read_data_file)."""
+    p = abi.Params()
+    lib().dmph_params_default(C.byref(p))
+    rc = lib().dmph_read_data_file(path.encode(), C.byref(p))
+    if rc != 0:
+        raise DmphError(rc, lib().dmph_io_last_message().decode())
+    return p
+
+
+def read_grid_file(path, params):
+    """.grid/.prof -> (type, x, v) through dmph_read_grid_file; fills the header into params."""
+    n = C.c_int(0)
+    rc = lib().dmph_read_grid_file(path.encode(), C.byref(params), C.byref(n), None, None, None)
+    if rc != 0:
+        raise DmphError(rc, lib().dmph_io_last_message().decode())
+    t = np.empty(n.value, np.int32)
+    x = np.empty((n.value, 3), np.float64)
+    v = np.empty((n.value, 3), np.float64)
+    rc = lib().dmph_read_grid_file(path.encode(), C.byref(params), C.byref(n), _ptr(t), _ptr(x), _ptr(v))
+    if rc != 0:
+        raise DmphError(rc, lib().dmph_io_last_message().decode())
+    return t, x, v

@@ -1,0 +1,45 @@
+"""The oracle restatement (oracle/dmph_oracle.c) against the golden fixtures
+that the reference solver itself produced (tests/golden/make_golden.py)."""
+import hashlib
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from helpers import GOLD, GOLDEN, fingerprint_ok, load_scene
+from oracle.oracle import Oracle
+from dem_mph_b200 import generator
+
+
+def test_generator_reproduces_shipped_grid():
+    """Known-answer test: results/SYSU/2mm/DEM.boid -> DEM.grid byte for byte."""
+    with tempfile.TemporaryDirectory() as tmp:
+        out = os.path.join(tmp, "DEM.grid")
+        n = generator.boid_to_grid(os.path.join(GOLDEN, "sysu2mm", "DEM.boid"), out)
+        assert n == 19913
+        with open(out, "rb") as f:
+            assert hashlib.sha256(f.read()).hexdigest() == GOLD["generator_kat"]["sysu2mm"]
+
+
+@pytest.mark.parametrize("name", sorted(GOLD["scenes"]))
+def test_oracle_matches_reference(name):
+    rec = GOLD["scenes"][name]
+    p, typ, x, v = load_scene(name)
+    o = Oracle(p, typ, x, v)
+    done = 0
+    for s in sorted(int(k) for k in rec["steps"]):
+        o.step(s - done)
+        done = s
+        gold = rec["steps"][str(s)]
+        bad = []
+        for arr, fp in gold["arrays"].items():
+            ok, msg = fingerprint_ok(o.get(arr), fp)
+            if not ok:
+                bad.append("%s: %s" % (arr, msg))
+        assert not bad, "step %d: %s" % (s, "; ".join(bad))
+        meta = gold["meta"]
+        assert o.scalar("N0a") == meta["N0a"] and o.scalar("N0p") == meta["N0p"]
+        assert o.scalar("Rebuilds") == meta["Rebuilds"]
+        assert o.scalar("Time") == meta["Time"]
+        assert [o.scalar("CellCount%d" % d) for d in range(3)] == meta["CellCount"]
