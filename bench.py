@@ -1,0 +1,311 @@
+"""Benchmark of the DEM-MPH explicit timestep on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload config2|config1] [--precision fp64|fp32]
+
+One "step" is one explicit timestep of the whole scene (the reference main
+loop body, source/DEM-MPH.cpp:450-579): drift, walls, periodic wrap, the
+rebuild trigger (and a neighbour rebuild when it fires), the density and
+pressure pass, the force pass with drag/buoyancy/gravity and the fluid
+update, and the DEM substeps.  The workload is the 3D dam break with debris
+of dem_mph_b200.scenes (config2: 3.2 x 1.0 x 1.0 m tank at 5 mm, ~1.2 M
+fluid + ~1.4 M wall particles + 200 debris bodies; seeded synthetic
+particles, since the reference ships no such scene).
+
+Metric: particle-steps/s = N_total x steps / device seconds (whole job, all
+ranks; inputs resident in HBM).  Multi-GPU: every rank advances its own
+independent seeded replica (weak scaling, no data-path collective); time is
+the max over ranks.  Rank 0 prints one JSON line.
+
+`--impl reference` times the reference's own CPU implementation (built from
+its source into oracle/_ref/ by oracle/Makefile) on this machine's host cores
+with all OpenMP threads, on a bounded number of steps of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d, "measured"
+    except Exception:
+        return PEAKS_FALLBACK, "fallback"
+
+
+def make_scene(workload, rank):
+    from dem_mph_b200 import scenes
+    seed = 1234 + rank
+    if workload == "config1":
+        return scenes.config1(seed=seed)
+    if workload == "config2":
+        return scenes.config2(seed=seed)
+    raise ValueError(workload)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region"""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        try:
+            for line in open(self.path):
+                f = [s.strip() for s in line.split(",")]
+                if len(f) < 9:
+                    continue
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+                for name, val in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                      "sw_power_cap"), f[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(name)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def reference_time(scene, steps, warmup, threads=None):
+    """Time the reference's own step (oracle/_ref/ref_dump3d --bench: the
+    reference's functions called in its main-loop order) on the host cores."""
+    from dem_mph_b200 import files
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_dump3d")
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/ref_dump3d not built"
+    with tempfile.TemporaryDirectory() as tmp:
+        data, grid = os.path.join(tmp, "dem.data"), os.path.join(tmp, "scene.grid")
+        files.write_data_file(data, scene.params)
+        files.write_grid(grid, scene.params, scene.type, scene.x, scene.v)
+        env = dict(os.environ)
+        if threads:
+            env["OMP_NUM_THREADS"] = str(threads)
+        r = subprocess.run([exe, "--bench", data, grid, str(steps), str(warmup)], capture_output=True, text=True,
+                           env=env)
+        if r.returncode != 0:
+            return None, "reference run failed: " + r.stderr[-200:]
+        line = [l for l in r.stdout.splitlines() if l.startswith("{")][-1]
+        return json.loads(line), None
+
+
+def algorithmic_bytes(prec):
+    """Compulsory HBM bytes per particle of the dominant kernel (pass B) with
+    neighbour re-reads served on chip: read position, velocity, pressure and
+    type, write force and (fluid) velocity."""
+    if prec == "fp64":
+        return 24 + 24 + 8 + 4 + 24 + 24
+    return 16 + 16 + 4 + 16 + 16
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config1"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from dem_mph_b200 import solver
+    from dem_mph_b200.abi import PRECISION_FP64, PRECISION_FP32_SPLIT
+
+    scene = make_scene(args.workload, rank)
+    p = scene.params.copy()
+    p.precision = PRECISION_FP64 if args.precision == "fp64" else PRECISION_FP32_SPLIT
+    g = solver.Solver(p, scene.type, scene.x, scene.v)
+    n = scene.n
+    g.step(args.warmup)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- timed region: K steps, device time on the solver's stream
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms = g.step_timed(args.steps)
+        torch.cuda.synchronize()
+    barrier()
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    inf = g.info()
+    value = n * world * args.steps / (ms_max / 1e3)
+
+    # ---- per-phase device times (separate pass, events around each phase)
+    g.set_profiling(True)
+    g.step(args.steps)
+    ph = g.phase_times()
+    g.set_profiling(False)
+    pb_ms, pb_n = ph["pass_b"]
+    pa_ms, pa_n = ph["pass_a"]
+    top = "pass_b" if pb_ms >= pa_ms else "pass_a"
+    inf = g.info()
+    n_fs = inf.n_fluid + inf.n_solid
+    peaks, peak_src = load_peaks()
+    bpp = algorithmic_bytes(args.precision)
+    if top == "pass_b":
+        bytes_launch = n_fs * bpp
+        dur = pb_ms / max(pb_n, 1)
+    else:
+        bytes_launch = n * (bpp - 24)
+        dur = pa_ms / max(pa_n, 1)
+    achieved = bytes_launch / (dur / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_" + top, "achieved": achieved, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                "peak_source": peak_src, "launch_ms": dur,
+                "phase_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in ph.items()}}
+
+    # ---- end to end through the C ABI with host buffers: every step uploads
+    # the particle state from pinned host memory, steps, reads it back
+    x_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    v_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    _, x0, v0, _ = g.state()
+    x_h[:] = x0
+    v_h[:] = v0
+    e2e_steps = max(3, min(args.steps, 10))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        g.set_state(x_h, v_h)
+        g.step(1)
+        _, xs, vs, _ = g.state()
+        x_h[:] = xs
+        v_h[:] = vs
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e = {"value": n * world * e2e_steps / float(e2e_t.item()), "unit": "particle-steps/s",
+           "h2d_bytes_per_step": int(n * 48), "d2h_bytes_per_step": int(n * 48 + n * 8),
+           "steps": e2e_steps}
+    g.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res, why = reference_time(scene, 1, 0)
+        if res:
+            cpu = {"value": res["particles"] * res["steps"] / res["seconds"], "unit": "particle-steps/s",
+                   "cores": res["threads"], "kind": "reference",
+                   "sample": "1 step of the same scene after initialisation (reference init incl. its serial "
+                             "neighbour build excluded), %d rebuilds" % res["rebuilds"]}
+        else:
+            cpu = {"value": None, "unit": "particle-steps/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": why}
+
+    counts = scene.counts()
+    out = {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic (seeded dam break with debris, dem_mph_b200.scenes)",
+        "config": {"workload": scene.name, "n_particles": counts["total"], "n_fluid": counts["fluid"],
+                   "n_solid": counts["solid"], "n_wall": counts["wall"], "n_debris_bodies": len(scene.body_density),
+                   "precision": args.precision, "dt": p.dt, "dem_substeps": inf.dem_substeps,
+                   "rebuilds_in_timed_steps": None, "parallelism": "replicas x%d" % world,
+                   "l2": "inputs larger than L2 (particle state alone %.0f MB)" % (n * 60 / 1e6)},
+        "sim_s_per_hour": p.dt * args.steps / (ms_max / 1e3) * 3600.0,
+        "clocks": clk.summary(),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": None,
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU step on this box's cores."""
+    if rank != 0:
+        return
+    scene = make_scene(args.workload, 0)
+    steps = max(1, min(args.steps, 3))
+    warm = min(args.warmup, 1)
+    res, why = reference_time(scene, steps, warm)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return
+    v = res["particles"] * res["steps"] / res["seconds"]
+    out = {"impl": "reference", "metric": "particle-steps/s", "value": v, "unit": "particle-steps/s",
+           "n_gpus": world, "steps": res["steps"], "warmup": warm, "ms_per_step": res["seconds"] * 1e3 / res["steps"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded dam break with debris, dem_mph_b200.scenes)",
+           "config": {"workload": scene.name, "n_particles": scene.n, "parallelism": "cpu openmp"},
+           "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": res["threads"], "kind": "reference",
+                            "sample": "%d steps after %d warm-up of the same scene (bounded sample; reference "
+                                      "initialisation excluded), %d rebuilds" % (res["steps"], warm,
+                                                                                res["rebuilds"])},
+           "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -40,6 +40,7 @@ CU_SOURCES = [
     ("dmph_f64.cu", ["-fmad=false"]),
     ("dmph_rebuild.cu", ["-fmad=false"]),
     ("dmph_api.cu", ["-fmad=false"]),
+    ("dmph_f32.cu", []),
 ]
 CPP_SOURCES = ["dmph_params.cpp", "dmph_io.cpp"]
 HEADERS = ["dmph_device.cuh", "dmph_state.cuh", "dmph_traverse.cuh", "dmph_internal.h"]

@@ -18,6 +18,8 @@ thread_local std::string g_create_err;
 struct dmph_ctx {
     dmph_params p;
     DevParams P;
+    DevParams32 Q;
+    bool fp32 = false;
     WallMotion Wm;
     cudaStream_t st = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -26,6 +28,7 @@ struct dmph_ctx {
     // second buffers of the permuted arrays
     double *pos2 = nullptr, *vel2 = nullptr;
     int *type2 = nullptr, *pidx2 = nullptr;
+    float4 *p4b = nullptr, *v4b = nullptr;  // second buffers of the FP32 state
     unsigned long long *words = nullptr;
     int *flag = nullptr, *offs = nullptr, *bsums = nullptr, *total = nullptr;
     unsigned long long *maxshift = nullptr;
@@ -37,6 +40,10 @@ struct dmph_ctx {
     double time = 0.0;
     long long steps = 0, rebuilds = 0;
     bool all_counts = false;
+    bool prof = false;
+    cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+    double phase_ms[DMPH_PHASE_COUNT] = {0};
+    long long phase_n[DMPH_PHASE_COUNT] = {0};
     std::string err;
     std::vector<void *> allocs;
 };
@@ -73,6 +80,8 @@ static void release(dmph_ctx *ctx)
     if (ctx->h_small) cudaFreeHost(ctx->h_small);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->pe0) cudaEventDestroy(ctx->pe0);
+    if (ctx->pe1) cudaEventDestroy(ctx->pe1);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     ctx->h_maxshift = nullptr;
     ctx->h_small = nullptr;
@@ -81,16 +90,26 @@ static void release(dmph_ctx *ctx)
 }
 
 // calculateCellParticle :1288 + the parts of calculateNeighbor the step needs
-static int rebuild(dmph_ctx *ctx)
+static int rebuild(dmph_ctx *ctx, bool first = false)
 {
     const DevParams &P = ctx->P;
+    // FP32 split state: absolute FP64 positions are rebuilt into the FP64
+    // planes first (unless they already hold them, at creation)
+    if (ctx->fp32 && !first) launch_export32(P, ctx->S, ctx->S.pos, nullptr, ctx->st);
     launch_keys(P, ctx->S.pos, ctx->S.type, ctx->words, ctx->st);
     launch_bitonic(ctx->words, P.P2, P.P2log, ctx->st);
     launch_cell_start(P, ctx->words, ctx->S.cell_start, ctx->st);
-    launch_permute(P, ctx->words, ctx->S.pos, ctx->S.vel, ctx->S.type, ctx->S.pidx, ctx->pos2, ctx->vel2, ctx->type2,
-                   ctx->pidx2, ctx->S.xref, ctx->st);
-    std::swap(ctx->S.pos, ctx->pos2);
-    std::swap(ctx->S.vel, ctx->vel2);
+    if (ctx->fp32) {
+        launch_permute32(P, ctx->words, ctx->S.pos, ctx->S.v4, ctx->S.type, ctx->S.pidx, ctx->p4b, ctx->v4b,
+                         ctx->type2, ctx->pidx2, ctx->S.xref, ctx->S.xref4, ctx->st);
+        std::swap(ctx->S.p4, ctx->p4b);
+        std::swap(ctx->S.v4, ctx->v4b);
+    } else {
+        launch_permute(P, ctx->words, ctx->S.pos, ctx->S.vel, ctx->S.type, ctx->S.pidx, ctx->pos2, ctx->vel2,
+                       ctx->type2, ctx->pidx2, ctx->S.xref, ctx->st);
+        std::swap(ctx->S.pos, ctx->pos2);
+        std::swap(ctx->S.vel, ctx->vel2);
+    }
     std::swap(ctx->S.type, ctx->type2);
     std::swap(ctx->S.pidx, ctx->pidx2);
     ctx->S.skey = ctx->words;
@@ -123,12 +142,33 @@ static int rebuild(dmph_ctx *ctx)
     return DMPH_OK;
 }
 
+// phase timing (dmph_set_profiling): events around one phase, synchronised
+static void phase_begin(dmph_ctx *ctx)
+{
+    if (ctx->prof) cudaEventRecord(ctx->pe0, ctx->st);
+}
+static void phase_end(dmph_ctx *ctx, int ph)
+{
+    if (!ctx->prof) return;
+    cudaEventRecord(ctx->pe1, ctx->st);
+    cudaEventSynchronize(ctx->pe1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->pe0, ctx->pe1);
+    ctx->phase_ms[ph] += ms;
+    ctx->phase_n[ph] += 1;
+}
+
 static int step_once(dmph_ctx *ctx)
 {
     const DevParams &P = ctx->P;
     ctx->Wm.moving = (ctx->time >= 0.2 && 0.4 >= ctx->time) ? 1 : 0;
     CK(cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), ctx->st));
-    launch_drift(P, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, ctx->st);
+    phase_begin(ctx);
+    if (ctx->fp32)
+        launch_drift32(P, ctx->Q, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, ctx->st);
+    else
+        launch_drift(P, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, ctx->st);
+    phase_end(ctx, 0);
     // WallCenter moves only while `0.0 < Time < 0.2` holds, i.e. Time <= 0 (:2892)
     if (!(0.0 < ctx->time))
         for (int t = DMPH_WALL_BEGIN; t < DMPH_WALL_END; ++t)
@@ -139,16 +179,43 @@ static int step_once(dmph_ctx *ctx)
     std::memcpy(&m2, ctx->h_maxshift, sizeof(double));
     const double margin = (0.1 * P.dx);
     if (m2 > 0.5 * margin * 0.5 * margin) {
+        phase_begin(ctx);
         const int rc = rebuild(ctx);
         if (rc) return rc;
+        phase_end(ctx, 1);
         ctx->rebuilds++;
     }
-    launch_pass_a(P, ctx->S, 0, ctx->ch_end, 0, ctx->st);
-    launch_pass_b(P, ctx->S, 0, ctx->ch_w0, ctx->st);
-    for (int k = 0; k < ctx->demSteps; ++k) {
-        launch_dem_force(P, ctx->S, ctx->ch_s0, ctx->ch_w0, 1, ctx->st);
-        if (P.wall_dem_coeffs) launch_dem_force(P, ctx->S, ctx->ch_w0, ctx->ch_end, 0, ctx->st);
-        launch_dem_integrate(P, ctx->S, ctx->sb, ctx->se, ctx->st);
+    if (ctx->fp32) {
+        const DevParams32 &Q = ctx->Q;
+        phase_begin(ctx);
+        launch_pass_a32(P, Q, ctx->S, 0, ctx->ch_end, ctx->st);
+        phase_end(ctx, 2);
+        phase_begin(ctx);
+        launch_pass_b32(P, Q, ctx->S, 0, ctx->ch_w0, ctx->st);
+        launch_fluid_accel32(Q, ctx->S, ctx->fb, ctx->fe, ctx->st);
+        phase_end(ctx, 3);
+        phase_begin(ctx);
+        for (int k = 0; k < ctx->demSteps; ++k) {
+            launch_dem_force32(P, Q, ctx->S, ctx->ch_s0, ctx->ch_w0, 1, ctx->st);
+            if (P.wall_dem_coeffs) launch_dem_force32(P, Q, ctx->S, ctx->ch_w0, ctx->ch_end, 0, ctx->st);
+            launch_dem_integrate32(Q, ctx->S, ctx->sb, ctx->se, ctx->st);
+        }
+        phase_end(ctx, 4);
+    } else {
+        phase_begin(ctx);
+        launch_pass_a(P, ctx->S, 0, ctx->ch_end, 0, ctx->st);
+        phase_end(ctx, 2);
+        phase_begin(ctx);
+        launch_pass_b(P, ctx->S, 0, ctx->ch_w0, ctx->st);
+        launch_fluid_accel(P, ctx->S, ctx->fb, ctx->fe, ctx->st);
+        phase_end(ctx, 3);
+        phase_begin(ctx);
+        for (int k = 0; k < ctx->demSteps; ++k) {
+            launch_dem_force(P, ctx->S, ctx->ch_s0, ctx->ch_w0, 1, ctx->st);
+            if (P.wall_dem_coeffs) launch_dem_force(P, ctx->S, ctx->ch_w0, ctx->ch_end, 0, ctx->st);
+            launch_dem_integrate(P, ctx->S, ctx->sb, ctx->se, ctx->st);
+        }
+        phase_end(ctx, 4);
     }
     CK(cudaGetLastError());
     ctx->time += P.dt;
@@ -166,8 +233,8 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         g_create_err = "null argument";
         return DMPH_EINVAL;
     }
-    if (p->precision != DMPH_PRECISION_FP64) {
-        g_create_err = "this build implements DMPH_PRECISION_FP64 only";
+    if (p->precision != DMPH_PRECISION_FP64 && p->precision != DMPH_PRECISION_FP32_SPLIT) {
+        g_create_err = "unknown precision";
         return DMPH_EINVAL;
     }
     for (int i = 0; i < n; i++)
@@ -184,6 +251,18 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         return rc;
     }
     ctx->all_counts = (p->flags & DMPH_FLAG_ALL_NEIGHBOR_COUNTS) != 0;
+    ctx->fp32 = p->precision == DMPH_PRECISION_FP32_SPLIT;
+    if (ctx->fp32) {
+        const int *cc = ctx->P.cc;
+        const bool fits = cc[0] <= 1024 && cc[1] <= 1024 && cc[2] <= 512;
+        const bool wide = cc[0] >= 3 && cc[1] >= 3 && (p->dim == 2 ? cc[2] == 1 : cc[2] >= 3);
+        if (!fits || !wide) {
+            g_create_err = "FP32 split precision needs 3..1024 cells along x and y and 3..512 along z (1 in 2D)";
+            delete ctx;
+            return DMPH_EINVAL;
+        }
+        ctx->Q = make_params32(ctx->P);
+    }
     ctx->demSteps = p->dt / p->dem_dt;  // (int)(Dt/DEMDt), :434
     ctx->time = p->time;
     auto fail = [&](int code) {
@@ -206,6 +285,8 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     CKC(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
     CKC(cudaEventCreate(&ctx->ev0));
     CKC(cudaEventCreate(&ctx->ev1));
+    CKC(cudaEventCreate(&ctx->pe0));
+    CKC(cudaEventCreate(&ctx->pe1));
     CKC(cudaMallocHost(&ctx->h_maxshift, sizeof(unsigned long long)));
     CKC(cudaMallocHost(&ctx->h_small, 16 * sizeof(int)));
     const DevParams &P = ctx->P;
@@ -243,6 +324,26 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     AL(ctx->type2, N);
     AL(ctx->pidx2, N);
     AL(ctx->words, (size_t)P.P2);
+    if (ctx->fp32) {
+        AL(S.p4, N);
+        AL(S.v4, N);
+        AL(S.f4, N);
+        AL(S.xref4, N);
+        AL(S.gc4, N);
+        AL(ctx->p4b, N);
+        AL(ctx->v4b, N);
+        AL(S.pres32, N);
+        AL(S.vsp32, N);
+        AL(S.div32, N);
+        AL(S.densA32, N);
+        AL(S.pA32, N);
+        AL(S.kn32, N);
+        AL(S.cn32, N);
+        AL(S.kt32, N);
+        AL(S.ct32, N);
+        AL(S.alpha32, N);
+        AL(S.dragC32, N);
+    }
     AL(ctx->flag, N);
     AL(ctx->offs, N);
     AL(ctx->bsums, 4096);
@@ -264,10 +365,21 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         CKC(cudaMemcpyAsync(S.pidx, iota.data(), N * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
         CKC(cudaStreamSynchronize(ctx->st));
     }
+    if (ctx->fp32) {
+        // velocities of the FP32 state (positions are set by the first rebuild)
+        std::vector<float4> v4(N);
+        for (size_t i = 0; i < N; i++)
+            v4[i] = make_float4((float)v3[3 * i], (float)v3[3 * i + 1], (float)v3[3 * i + 2], 0.f);
+        CKC(cudaMemcpyAsync(S.v4, v4.data(), N * sizeof(float4), cudaMemcpyHostToDevice, ctx->st));
+        CKC(cudaStreamSynchronize(ctx->st));
+    }
     // initial sort, neighbour counts and densities (:419-425)
-    rc = rebuild(ctx);
+    rc = rebuild(ctx, true);
     if (rc) return fail(rc);
-    launch_pass_a(P, S, 0, ctx->ch_end, 1, ctx->st);
+    if (ctx->fp32)
+        launch_pass_a32(P, ctx->Q, ctx->S, 0, ctx->ch_end, ctx->st);
+    else
+        launch_pass_a(P, S, 0, ctx->ch_end, 1, ctx->st);
     CKC(cudaGetLastError());
     CKC(cudaStreamSynchronize(ctx->st));
 #undef AL
@@ -318,6 +430,7 @@ extern "C" int dmph_get_state(dmph_ctx *ctx, int *type, double *x3, double *v3, 
 {
     if (!ctx) return DMPH_EINVAL;
     const size_t N = (size_t)ctx->P.N;
+    if (ctx->fp32) launch_export32(ctx->P, ctx->S, ctx->S.pos, ctx->S.vel, ctx->st);
     if (x3) {
         int rc = d2h_planes(ctx, ctx->S.pos, x3);
         if (rc) return rc;
@@ -349,6 +462,12 @@ extern "C" int dmph_set_state(dmph_ctx *ctx, const double *x3, const double *v3)
         CK(cudaMemcpyAsync(ctx->S.vel, planes.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
     }
+    if (ctx->fp32) {
+        if (!x3) launch_export32(ctx->P, ctx->S, ctx->S.pos, nullptr, ctx->st);
+        launch_import32(ctx->P, ctx->S, ctx->S.pos, v3 ? ctx->S.vel : nullptr, ctx->st);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->st));
+    }
     return DMPH_OK;
 }
 
@@ -358,6 +477,27 @@ extern "C" int dmph_get_field(dmph_ctx *ctx, int field_id, void *out)
     const size_t N = (size_t)ctx->P.N;
     const DevState &S = ctx->S;
     const double *src = nullptr;
+    if (ctx->fp32) {
+        // widen the FP32 field into its FP64 twin, then copy as in FP64 mode
+        const int n = (int)N;
+        switch (field_id) {
+        case DMPH_FIELD_FORCE: launch_widen_f4(S.f4, S.frc, n, ctx->st); break;
+        case DMPH_FIELD_GRAVITY_CENTER: launch_widen_f4(S.gc4, S.gc, n, ctx->st); break;
+        case DMPH_FIELD_VOL_STRAIN_P: launch_widen_f(S.vsp32, S.vsp, n, ctx->st); break;
+        case DMPH_FIELD_DIVERGENCE_P: launch_widen_f(S.div32, S.divp, n, ctx->st); break;
+        case DMPH_FIELD_PRESSURE_P: launch_widen_f(S.pres32, S.pres, n, ctx->st); break;
+        case DMPH_FIELD_DENSITY_A: launch_widen_f(S.densA32, S.densA, n, ctx->st); break;
+        case DMPH_FIELD_PRESSURE_A: launch_widen_f(S.pA32, S.pA, n, ctx->st); break;
+        case DMPH_FIELD_NORMAL_SPRING: launch_widen_f(S.kn32, S.kn, n, ctx->st); break;
+        case DMPH_FIELD_NORMAL_DAMPING: launch_widen_f(S.cn32, S.cn, n, ctx->st); break;
+        case DMPH_FIELD_TANGENTIAL_SPRING: launch_widen_f(S.kt32, S.kt, n, ctx->st); break;
+        case DMPH_FIELD_TANGENTIAL_DAMPING: launch_widen_f(S.ct32, S.ct, n, ctx->st); break;
+        case DMPH_FIELD_ALPHA: launch_widen_f(S.alpha32, S.alpha, n, ctx->st); break;
+        case DMPH_FIELD_DRAG_C: launch_widen_f(S.dragC32, S.dragC, n, ctx->st); break;
+        default: break;
+        }
+        CK(cudaGetLastError());
+    }
     switch (field_id) {
     case DMPH_FIELD_FORCE: return d2h_planes(ctx, S.frc, (double *)out);
     case DMPH_FIELD_GRAVITY_CENTER: return d2h_planes(ctx, S.gc, (double *)out);
@@ -478,6 +618,27 @@ extern "C" int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind,
         // computed the same values for them, so nothing to restore
     }
     return rc;
+}
+
+extern "C" int dmph_set_profiling(dmph_ctx *ctx, int enable)
+{
+    if (!ctx) return DMPH_EINVAL;
+    ctx->prof = enable != 0;
+    for (int k = 0; k < DMPH_PHASE_COUNT; k++) {
+        ctx->phase_ms[k] = 0.0;
+        ctx->phase_n[k] = 0;
+    }
+    return DMPH_OK;
+}
+
+extern "C" int dmph_get_phase_times(dmph_ctx *ctx, double *ms, int64_t *launches, int n)
+{
+    if (!ctx || n < 0) return DMPH_EINVAL;
+    for (int k = 0; k < n && k < DMPH_PHASE_COUNT; k++) {
+        if (ms) ms[k] = ctx->phase_ms[k];
+        if (launches) launches[k] = ctx->phase_n[k];
+    }
+    return DMPH_OK;
 }
 
 extern "C" int dmph_destroy(dmph_ctx *ctx)

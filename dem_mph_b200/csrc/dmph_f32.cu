@@ -1,0 +1,670 @@
+// FP32 split-precision timestep kernels (DMPH_PRECISION_FP32_SPLIT).
+//
+// Same step structure, pair sets and per-particle semantics as the FP64
+// kernels in dmph_f64.cu (which restate the reference, source/DEM-MPH.cpp),
+// but the pair arithmetic runs in FP32 on positions stored relative to the
+// origin of each particle's rebuild-time cell:  when a warp stages a
+// neighbour j it shifts j into the frame of the warp's cell by the
+// minimum-image cell offset times the cell width, so every difference is
+// formed between numbers of a few particle spacings.  Reciprocal square roots
+// and fused multiply-adds are used freely; accuracy is checked against the
+// FP64 oracle with a 1e-5 bound on forces relative to their field maximum.
+#include "dmph_state.cuh"
+#include "dmph_traverse.cuh"
+
+namespace dmph {
+
+
+
+struct Tile32 {
+    float4 p[kWarp];  // position in the frame of the warp's cell; .w = type as float bits
+    float4 v[kWarp];  // velocity; .w = pressure (pass B)
+};
+struct TileST {
+    float4 g[kWarp];  // gravity centre; .w = attractive pressure
+};
+
+constexpr int kWarpsPerBlock32 = 8;
+
+__device__ __forceinline__ int min_image_cell(int d, int c)
+{
+    return d > 1 ? d - c : (d < -1 ? d + c : d);
+}
+
+// stage particle j into the tile in the frame of cell (ci)
+__device__ __forceinline__ void stage32(const DevParams &P, const DevParams32 &Q, const DevState &S, Tile32 &tl,
+                                        int j, int slot, int cix, int ciy, int ciz, bool with_pressure)
+{
+    const float4 pj = S.p4[j];
+    const unsigned w = __float_as_uint(pj.w);
+    const int dx = min_image_cell(unpack_cx(w) - cix, P.cc[0]);
+    const int dy = min_image_cell(unpack_cy(w) - ciy, P.cc[1]);
+    const int dz = min_image_cell(unpack_cz(w) - ciz, P.cc[2]);
+    tl.p[slot] = make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
+                             fmaf((float)dz, Q.cw[2], pj.z), __int_as_float(unpack_type(w)));
+    float4 vj = S.v4[j];
+    if (with_pressure) vj.w = S.pres32[j];
+    tl.v[slot] = vj;
+}
+
+__device__ __forceinline__ void chunk_cell(const DevParams &P, int key_cell, int &cx, int &cy, int &cz)
+{
+    cx = key_cell / (P.cc[1] * P.cc[2]);
+    cy = (key_cell / P.cc[2]) % P.cc[1];
+    cz = key_cell % P.cc[2];
+}
+
+// ---------------------------------------------------------------- drift
+__global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm, unsigned long long *maxshift)
+{
+    const int N = P.N;
+    float m2 = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        float4 p = S.p4[i];
+        float4 v = S.v4[i];
+        const unsigned w = __float_as_uint(p.w);
+        const int t = unpack_type(w);
+        if (is_fluid(t)) {
+            p.x = fmaf(v.x, Q.dt, p.x);
+            p.y = fmaf(v.y, Q.dt, p.y);
+            p.z = fmaf(v.z, Q.dt, p.z);
+        } else if (is_wall(t)) {
+            if (Wm.moving) {
+                const double o[3] = {P.dmin[0] + unpack_cx(w) * P.cw[0], P.dmin[1] + unpack_cy(w) * P.cw[1],
+                                     P.dmin[2] + unpack_cz(w) * P.cw[2]};
+                double x[3] = {o[0] + p.x, o[1] + p.y, o[2] + p.z}, vv[3];
+                double r[3] = {x[0] - Wm.C[t][0], x[1] - Wm.C[t][1], x[2] - Wm.C[t][2]};
+                const double(*R)[3] = Wm.R[t];
+                const double *om = Wm.Om[t];
+                r[0] = R[0][0] * r[0] + R[0][1] * r[1] + R[0][2] * r[2];
+                r[1] = R[1][0] * r[0] + R[1][1] * r[1] + R[1][2] * r[2];
+                r[2] = R[2][0] * r[0] + R[2][1] * r[1] + R[2][2] * r[2];
+                vv[0] = om[1] * r[2] - om[2] * r[1] + Wm.Vel[t][0];
+                vv[1] = om[2] * r[0] - om[0] * r[2] + Wm.Vel[t][1];
+                vv[2] = om[0] * r[1] - om[1] * r[0] + Wm.Vel[t][2];
+                for (int d = 0; d < 3; d++) x[d] = r[d] + Wm.C[t][d] + Wm.Vel[t][d] * P.dt;
+                p.x = (float)(x[0] - o[0]);
+                p.y = (float)(x[1] - o[1]);
+                p.z = (float)(x[2] - o[2]);
+                v = make_float4((float)vv[0], (float)vv[1], (float)vv[2], 0.f);
+            } else {
+                v = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+        S.p4[i] = p;
+        S.v4[i] = v;
+        S.f4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 r = S.xref4[i];
+        const float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
+        m2 = fmaxf(m2, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+    }
+    // reduce as double bits so the host compares like the FP64 path
+    unsigned long long b = __double_as_longlong((double)m2);
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long ob = __shfl_down_sync(kFull, b, o);
+        b = ob > b ? ob : b;
+    }
+    __shared__ unsigned long long red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long mx = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) mx = red[k] > mx ? red[k] : mx;
+        atomicMax(maxshift, mx);
+    }
+}
+
+// ---------------------------------------------------------------- pass A
+__global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_a32(DevParams P, DevParams32 Q, DevState S,
+                                                                       int chunk_begin, int chunk_end)
+{
+    __shared__ Tile32 tiles[kWarpsPerBlock32];
+    Tile32 &tl = tiles[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int cidx = chunk_begin + blockIdx.x * kWarpsPerBlock32 + (threadIdx.x >> 5);
+    if (cidx >= chunk_end) return;
+    const Chunk ch = S.chunks[cidx];
+    const int i = ch.i0 + lane;
+    const bool active = lane < ch.cnt;
+    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+    int cix, ciy, ciz;
+    chunk_cell(P, key_cell, cix, ciy, ciz);
+    const int ii = active ? i : ch.i0;
+    const float4 pi = S.p4[ii];
+    const float4 vi = S.v4[ii];
+    const int ti = unpack_type(__float_as_uint(pi.w));
+    const bool st = P.surface_tension;
+    float vsp = 0.f, div = 0.f, dA = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
+    traverse_stencil(
+        P, S.cell_start, key_cell, lane, active, 7u,
+        [&](int j, int slot) { stage32(P, Q, S, tl, j, slot, cix, ciy, ciz, false); },
+        [&](int j, int s) {
+            const float4 pj = tl.p[s];
+            const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+            const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
+            if (j == i) return;
+            const int tj = __float_as_int(pj.w);
+            if (r2 <= Q.RP2) {
+                const float ir = rsqrtf(r2);
+                const float r = r2 * ir;
+                const float a = fmaf(-r, Q.iRP, 1.f);  // 1 - r/h
+                vsp = fmaf(Q.Bp * a, a, vsp);
+                const bool skip = (is_solid(ti) && is_wall(tj)) || (is_solid(tj) && is_wall(ti)) ||
+                                  (is_solid(tj) && is_solid(ti));
+                if (!skip) {
+                    const float4 vj = tl.v[s];
+                    const float uq = fmaf(vj.x - vi.x, q0, fmaf(vj.y - vi.y, q1, (vj.z - vi.z) * q2));
+                    div = fmaf(-uq * ir, Q.dwp * a, div);  // -(u.e) dw
+                }
+            }
+            if (st && !(is_solid(ti) && is_wall(tj))) {
+                const float ratio = Q.ratio[ti][tj];
+                if (r2 <= Q.RA2) {
+                    const float r = sqrtf(r2);
+                    const float x = r * Q.iRA;
+                    dA = fmaf(ratio * Q.Ba * x * (1.f - x), (1.f - x), dA);
+                }
+                if (r2 <= Q.RG2) {
+                    const float r = sqrtf(r2);
+                    const float a = fmaf(-r, Q.iRG, 1.f);
+                    const float w = ratio * Q.Bg * a * a * Q.R2g_inv_RG;
+                    g0 = fmaf(q0, w, g0);
+                    g1 = fmaf(q1, w, g1);
+                    g2 = fmaf(q2, w, g2);
+                }
+            }
+        });
+    if (!active) return;
+    const float volstrain = vsp - Q.N0p;
+    S.vsp32[i] = volstrain;
+    S.div32[i] = div;
+    const float kappa = volstrain < 0.f ? 0.f : Q.bulk[ti];
+    if (!is_solid(ti)) S.pres32[i] = fmaf(-Q.bvisc[ti], div, kappa * volstrain);
+    if (st) {
+        S.densA32[i] = dA;
+        float pa = Q.CofA[ti] * (dA - Q.N0a) / Q.dx;
+        if (Q.N0a <= dA) pa = 0.f;
+        S.pA32[i] = pa;
+        S.gc4[i] = make_float4(g0, g1, g2, 0.f);
+    }
+}
+
+// ---------------------------------------------------------------- pass B
+__global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_b32(DevParams P, DevParams32 Q, DevState S,
+                                                                       int chunk_begin, int chunk_end)
+{
+    __shared__ Tile32 tiles[kWarpsPerBlock32];
+    __shared__ TileST tst[kWarpsPerBlock32];
+    Tile32 &tl = tiles[threadIdx.x >> 5];
+    TileST &ts = tst[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int cidx = chunk_begin + blockIdx.x * kWarpsPerBlock32 + (threadIdx.x >> 5);
+    if (cidx >= chunk_end) return;
+    const Chunk ch = S.chunks[cidx];
+    const int i = ch.i0 + lane;
+    const bool active = lane < ch.cnt;
+    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+    int cix, ciy, ciz;
+    chunk_cell(P, key_cell, cix, ciy, ciz);
+    const int ii = active ? i : ch.i0;
+    const float4 pi = S.p4[ii];
+    const float4 vi = S.v4[ii];
+    const int ti = unpack_type(__float_as_uint(pi.w));
+    const bool sol = is_solid(ti);
+    const float Pi = S.pres32[ii];
+    const float mui = Q.svisc[ti];
+    const float rhoi = Q.density[ti];
+    const bool st = P.surface_tension;
+    float4 gi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (st) {
+        gi = S.gc4[ii];
+        gi.w = S.pA32[ii];
+    }
+    float alpha = 0.f;
+    if (sol) {
+        const int nci = S.nc[ii];
+        alpha = nci > 0 ? (float)S.snc[ii] / (float)nci : 0.f;
+    }
+    float3 fP = make_float3(0.f, 0.f, 0.f), fV = fP, fD = fP, fB = fP, fS = fP;
+    float dragc = 0.f;
+    bool have_drag = false;
+    traverse_stencil(
+        P, S.cell_start, key_cell, lane, active, 7u,
+        [&](int j, int slot) {
+            stage32(P, Q, S, tl, j, slot, cix, ciy, ciz, true);
+            if (st) {
+                float4 g = S.gc4[j];
+                g.w = S.pA32[j];
+                ts.g[slot] = g;
+            }
+        },
+        [&](int j, int s) {
+            const float4 pj = tl.p[s];
+            const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+            const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
+            if (j == i || r2 >= Q.RV2 && r2 >= Q.RP2 && (!st || (r2 >= Q.RA2 && r2 >= Q.RG2))) return;
+            const int tj = __float_as_int(pj.w);
+            const float4 vj = tl.v[s];
+            const float u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
+            const float ir = rsqrtf(r2);
+            const float r = r2 * ir;
+            if (!sol && r2 < Q.RP2) {
+                const float a = fmaf(-r, Q.iRP, 1.f);
+                const float c = (Pi + vj.w) * Q.dwp * a * ir * Q.V;  // (Pi+Pj) dw/r V
+                fP.x = fmaf(c, q0, fP.x);
+                fP.y = fmaf(c, q1, fP.y);
+                fP.z = fmaf(c, q2, fP.z);
+            }
+            if (!(sol && is_wall(tj)) && r2 < Q.RV2) {
+                const float a = fmaf(-r, Q.iRV, 1.f);
+                const float muj = Q.svisc[tj];
+                const float muij = 2.f * (mui * muj) / (mui + muj);
+                const float uq = fmaf(u0, q0, fmaf(u1, q1, u2 * q2));
+                // C mu (u.e) e (-dw)/r V  with e = q/r
+                const float c = Q.viscC * muij * uq * (-Q.dwv * a) * ir * ir * ir * Q.V;
+                fV.x = fmaf(c, q0, fV.x);
+                fV.y = fmaf(c, q1, fV.y);
+                fV.z = fmaf(c, q2, fV.z);
+            }
+            if (sol && r2 < Q.RP2 && is_fluid(tj)) {
+                const float Vs = sqrtf(fmaf(u0, u0, fmaf(u1, u1, u2 * u2)));
+                const float Re = alpha * rhoi * Vs * Q.dx / Q.svisc[tj];
+                float cd;
+                if (alpha < 0.8f)
+                    cd = (4.f / 3.f) * (150.f * (1.f - alpha) / (alpha * Re) + 1.75f);
+                else if (Re <= 1000.f)
+                    cd = 24.f * (1.f + 0.15f * powf(Re, 0.687f)) / (alpha * Re) * powf(alpha, -2.65f);
+                else
+                    cd = 0.44f;
+                dragc = cd;
+                have_drag = true;
+                const float c = cd * rhoi * Q.drag_pref * Vs;
+                fD.x = fmaf(c, u0, fD.x);
+                fD.y = fmaf(c, u1, fD.y);
+                fD.z = fmaf(c, u2, fD.z);
+                const float a = fmaf(-r, Q.iRP, 1.f);
+                const float wb = Q.density[tj] * Q.V * Q.Bp * a * a;
+                fB.x = fmaf(wb, Q.g[0], fB.x);
+                fB.y = fmaf(wb, Q.g[1], fB.y);
+                fB.z = fmaf(wb, Q.g[2], fB.z);
+            }
+            if (st && !((sol && is_wall(tj)) || (is_solid(tj) && is_wall(ti)))) {
+                const float rij_ = Q.ratio[ti][tj], rji_ = Q.ratio[tj][ti];
+                const float4 gj = ts.g[s];
+                if (r2 < Q.RA2) {
+                    const float x = r * Q.iRA;
+                    const float dwa = Q.Ba * (1.f - x) * (1.f - 3.f * x) * Q.iRA;
+                    const float c = (gi.w * rij_ + gj.w * rji_) * dwa * ir * Q.V;
+                    fS.x = fmaf(c, q0, fS.x);
+                    fS.y = fmaf(c, q1, fS.y);
+                    fS.z = fmaf(c, q2, fS.z);
+                }
+                if (r2 < Q.RG2) {
+                    const float a = fmaf(-r, Q.iRG, 1.f);
+                    const float w2 = Q.Bg * a * a, dw2 = Q.dwg * a;
+                    const float ai = Q.ai[ti];
+                    const float k = Q.R2g_inv_RG * Q.Vdx;
+                    fS.x -= (ai * gj.x * rji_ * w2 - ai * gi.x * rij_ * w2) * k;
+                    fS.y -= (ai * gj.y * rji_ * w2 - ai * gi.y * rij_ * w2) * k;
+                    fS.z -= (ai * gj.z * rji_ * w2 - ai * gi.z * rij_ * w2) * k;
+                    const float gr = (ai * gj.x * rji_ * dw2 - ai * gi.x * rij_ * dw2) * q0 +
+                                     (ai * gj.y * rji_ * dw2 - ai * gi.y * rij_ * dw2) * q1 +
+                                     (ai * gj.z * rji_ * dw2 - ai * gi.z * rij_ * dw2) * q2;
+                    const float c = gr * ir * k;
+                    fS.x -= c * q0;
+                    fS.y -= c * q1;
+                    fS.z -= c * q2;
+                }
+            }
+        });
+    if (!active) return;
+    const float m = Q.mass[ti];
+    float4 F;
+    if (sol) {
+        F.x = 2.f * fD.x + fS.x + fV.x - fB.x + m * Q.g[0];
+        F.y = 2.f * fD.y + fS.y + fV.y - fB.y + m * Q.g[1];
+        F.z = 2.f * fD.z + fS.z + fV.z - fB.z + m * Q.g[2];
+        S.alpha32[i] = alpha;
+        if (have_drag) S.dragC32[i] = dragc;
+    } else {
+        F.x = fP.x + fS.x + fV.x + m * Q.g[0];
+        F.y = fP.y + fS.y + fV.y + m * Q.g[1];
+        F.z = fP.z + fS.z + fV.z + m * Q.g[2];
+    }
+    F.w = 0.f;
+    S.f4[i] = F;
+}
+
+__global__ void k_fluid_accel32(DevParams32 Q, DevState S, int b, int e)
+{
+    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= e) return;
+    const float4 f = S.f4[i];
+    float4 v = S.v4[i];
+    const float k = Q.dt / Q.mass[unpack_type(__float_as_uint(S.p4[i].w))];
+    v.x = fmaf(f.x, k, v.x);
+    v.y = fmaf(f.y, k, v.y);
+    v.z = fmaf(f.z, k, v.z);
+    S.v4[i] = v;
+}
+
+// ---------------------------------------------------------------- DEM
+__global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_dem_force32(DevParams P, DevParams32 Q, DevState S,
+                                                                          int chunk_begin, int chunk_end, int forces)
+{
+    __shared__ Tile32 tiles[kWarpsPerBlock32];
+    Tile32 &tl = tiles[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int cidx = chunk_begin + blockIdx.x * kWarpsPerBlock32 + (threadIdx.x >> 5);
+    if (cidx >= chunk_end) return;
+    const Chunk ch = S.chunks[cidx];
+    const int i = ch.i0 + lane;
+    const bool active = lane < ch.cnt;
+    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+    int cix, ciy, ciz;
+    chunk_cell(P, key_cell, cix, ciy, ciz);
+    const int ii = active ? i : ch.i0;
+    const float4 pi = S.p4[ii];
+    const float4 vi = S.v4[ii];
+    const int ti = unpack_type(__float_as_uint(pi.w));
+    auto stage = [&](int j, int slot) { stage32(P, Q, S, tl, j, slot, cix, ciy, ciz, false); };
+    int tlast = -1;
+    float r2last = 0.f;
+    traverse_stencil(P, S.cell_start, key_cell, lane, active, 7u, stage, [&](int j, int s) {
+        if (j == i) return;
+        const float4 pj = tl.p[s];
+        const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+        const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
+        if (r2 <= Q.dx2) {
+            tlast = __float_as_int(pj.w);
+            r2last = r2;
+        }
+    });
+    float kn = 0.f, cn = 0.f, kt = 0.f, ct = 0.f;
+    if (active) {
+        if (tlast >= 0) {
+            const float ov = fmaxf(0.f, Q.dx - sqrtf(r2last));
+            kn = (4.f / 3.f) * Q.Eeff[ti][tlast] * sqrtf(Q.Reff * ov);
+            const float mi = Q.mass[ti], mj = Q.mass[tlast];
+            const float mij = mi * mj / (mi + mj);
+            cn = -2.f * sqrtf(mij * kn) * Q.logE[ti] / Q.cnDen[ti];
+            kt = Q.KtFac[ti][tlast] * sqrtf(Q.Reff * sqrtf(ov));
+            ct = Q.ctFac[ti] * sqrtf(mij * kt);
+            S.kn32[i] = kn;
+            S.cn32[i] = cn;
+            S.kt32[i] = kt;
+            S.ct32[i] = ct;
+        } else {
+            kn = S.kn32[i];
+            cn = S.cn32[i];
+            kt = S.kt32[i];
+            ct = S.ct32[i];
+        }
+    }
+    if (!forces) return;
+    float3 fN = make_float3(0.f, 0.f, 0.f), fT = fN;
+    const float muf = Q.friction[ti];
+    traverse_stencil(P, S.cell_start, key_cell, lane, active, 6u, stage, [&](int j, int s) {
+        if (j == i) return;
+        const float4 pj = tl.p[s];
+        const float q[3] = {pj.x - pi.x, pj.y - pi.y, pj.z - pi.z};
+        const float r2 = fmaf(q[0], q[0], fmaf(q[1], q[1], q[2] * q[2]));
+        if (r2 > Q.dx2) return;
+        const float r = sqrtf(r2);
+        const float e[3] = {q[0] / r, q[1] / r, q[2] / r};
+        const float4 vj = tl.v[s];
+        const float u[3] = {vj.x - vi.x, vj.y - vi.y, vj.z - vi.z};
+        float vn[3], vt[3], dtv[3], sN[3], sT[3];
+        for (int d = 0; d < 3; d++) vn[d] = u[d] * e[d];  // component-wise, as the reference (:2648)
+        for (int d = 0; d < 3; d++) vt[d] = u[d] - vn[d] * e[d];
+        for (int d = 0; d < 3; d++) dtv[d] = vt[d] * Q.ddt;
+        for (int d = 0; d < 3; d++) sN[d] = -kn * (Q.dx - r) * e[d] - (cn * vn[d] * e[d] * Q.dt);
+        const float aFn = muf * sqrtf(sN[0] * sN[0] + sN[1] * sN[1] + sN[2] * sN[2]);
+        for (int d = 0; d < 3; d++) sT[d] = -kt * dtv[d] - (ct * vt[d]);
+        const float aFt = sqrtf(sT[0] * sT[0] + sT[1] * sT[1] + sT[2] * sT[2]);
+        fN.x += sN[0];
+        fN.y += sN[1];
+        fN.z += sN[2];
+        if (aFn > aFt) {
+            fT.x += sT[0];
+            fT.y += sT[1];
+            fT.z += sT[2];
+        } else {
+            const float avt = sqrtf(vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]);
+            if (avt != 0.f) {
+                const float c = aFn / avt;
+                fT.x += c * vt[0];
+                fT.y += c * vt[1];
+                fT.z += c * vt[2];
+            }
+        }
+    });
+    if (!active) return;
+    float4 F = S.f4[i];
+    F.x += fN.x + fT.x;
+    F.y += fN.y + fT.y;
+    F.z += fN.z + fT.z;
+    S.f4[i] = F;
+}
+
+__global__ void k_dem_integrate32(DevParams32 Q, DevState S, int b, int e)
+{
+    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= e) return;
+    float4 p = S.p4[i];
+    float4 v = S.v4[i];
+    const float4 f = S.f4[i];
+    const float k = Q.ddt / Q.mass[unpack_type(__float_as_uint(p.w))];
+    v.x = fmaf(f.x, k, v.x);
+    v.y = fmaf(f.y, k, v.y);
+    v.z = fmaf(f.z, k, v.z);
+    p.x = fmaf(v.x, Q.ddt, p.x);
+    p.y = fmaf(v.y, Q.ddt, p.y);
+    p.z = fmaf(v.z, Q.ddt, p.z);
+    S.v4[i] = v;
+    S.p4[i] = p;
+}
+
+// ------------------------------------------------------- layout conversion
+// FP32 split state -> FP64 absolute positions (wrapped into the periodic
+// domain like calculatePeriodicBoundary :3153) and velocities, into the FP64
+// planes; used by the rebuild (cell keys) and by the state getters.
+__global__ void k_export32(DevParams P, DevState S, double *pos, double *vel)
+{
+    const int N = P.N;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float4 p = S.p4[i];
+    const float4 v = S.v4[i];
+    const unsigned w = __float_as_uint(p.w);
+    const int c[3] = {unpack_cx(w), unpack_cy(w), unpack_cz(w)};
+    const float pr[3] = {p.x, p.y, p.z};
+    const float vr[3] = {v.x, v.y, v.z};
+    for (int d = 0; d < 3; d++) {
+        const double a = P.dmin[d] + c[d] * P.cw[d] + (double)pr[d];
+        const double t = a - P.dmin[d];
+        pos[d * N + i] = (t - P.W[d] * floor(t / P.W[d])) + P.dmin[d];
+        if (vel) vel[d * N + i] = (double)vr[d];
+    }
+}
+
+// permutation of the FP32 state at a rebuild: the new slot's cell comes from
+// its sorted key, its position is re-expressed relative to that cell
+__global__ void k_permute32(DevParams P, const unsigned long long *__restrict__ words, const double *__restrict__ xabs,
+                            const float4 *__restrict__ v_in, const int *__restrict__ type_in,
+                            const int *__restrict__ pidx_in, float4 *__restrict__ p_out, float4 *__restrict__ v_out,
+                            int *__restrict__ type_out, int *__restrict__ pidx_out, double *__restrict__ xref,
+                            float4 *__restrict__ xref4)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int N = P.N;
+    if (i >= N) return;
+    const unsigned long long wd = words[i];
+    const int src = (int)word_slot(wd);
+    const int kc = (int)(word_key(wd) % (unsigned)P.T);
+    int c[3];
+    c[0] = kc / (P.cc[1] * P.cc[2]);
+    c[1] = (kc / P.cc[2]) % P.cc[1];
+    c[2] = kc % P.cc[2];
+    const int t = type_in[src];
+    float r[3];
+    for (int d = 0; d < 3; d++) {
+        const double x = xabs[d * N + src];
+        xref[d * N + i] = x;
+        r[d] = (float)(x - (P.dmin[d] + c[d] * P.cw[d]));
+    }
+    const float4 p = make_float4(r[0], r[1], r[2], __uint_as_float(pack_cell(t, c[0], c[1], c[2])));
+    p_out[i] = p;
+    xref4[i] = p;
+    v_out[i] = v_in[src];
+    type_out[i] = t;
+    pidx_out[i] = pidx_in[src];
+}
+
+// FP64 planes -> FP32 split state in the current cells (dmph_set_state, create)
+__global__ void k_import32(DevParams P, DevState S, const double *pos, const double *vel)
+{
+    const int N = P.N;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float4 p = S.p4[i];
+    const unsigned w = __float_as_uint(p.w);
+    const int c[3] = {unpack_cx(w), unpack_cy(w), unpack_cz(w)};
+    float r[3];
+    for (int d = 0; d < 3; d++) {
+        double a = pos[d * N + i] - (P.dmin[d] + c[d] * P.cw[d]);
+        // nearest periodic image of the cell origin
+        a -= P.W[d] * rint(a / P.W[d]);
+        r[d] = (float)a;
+    }
+    S.p4[i] = make_float4(r[0], r[1], r[2], p.w);
+    if (vel) S.v4[i] = make_float4((float)vel[i], (float)vel[N + i], (float)vel[2 * N + i], 0.f);
+}
+
+// widen an FP32 field to FP64 (getters)
+__global__ void k_widen_f(const float *in, double *out, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (double)in[i];
+}
+__global__ void k_widen_f4(const float4 *in, double *out, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 v = in[i];
+    out[i] = v.x;
+    out[n + i] = v.y;
+    out[2 * n + i] = v.z;
+}
+
+// ---------------------------------------------------------------- host side
+DevParams32 make_params32(const DevParams &P)
+{
+    DevParams32 Q;
+    for (int d = 0; d < 3; d++) {
+        Q.cw[d] = (float)P.cw[d];
+        Q.g[d] = (float)P.g[d];
+    }
+    Q.dx = (float)P.dx;
+    Q.V = (float)P.V;
+    Q.dt = (float)P.dt;
+    Q.ddt = (float)P.ddt;
+    Q.dx2 = (float)P.dx2;
+    Q.RP2 = (float)P.RP2;
+    Q.RV2 = (float)P.RV2;
+    Q.RA2 = (float)P.RA2;
+    Q.RG2 = (float)P.RG2;
+    Q.iRP = (float)(1.0 / P.RP);
+    Q.iRV = (float)(1.0 / P.RV);
+    Q.iRA = (float)(1.0 / P.RA);
+    Q.iRG = (float)(1.0 / P.RG);
+    Q.Bp = (float)P.Bp;
+    Q.Bv = (float)P.Bv;
+    Q.Ba = (float)P.Ba;
+    Q.Bg = (float)P.Bg;
+    Q.dwp = (float)(-2.0 * P.Bp / P.RP);
+    Q.dwv = (float)(-2.0 * P.Bv / P.RV);
+    Q.dwg = (float)(-2.0 * P.Bg / P.RG);
+    Q.N0p = (float)P.N0p;
+    Q.N0a = (float)P.N0a;
+    Q.R2g_inv_RG = (float)(P.RG / P.R2g);
+    Q.viscC = (float)P.viscC;
+    Q.Reff = (float)P.Reff;
+    Q.Vdx = (float)(P.V / P.dx);
+    Q.drag_pref = (float)(0.5 * P.dx * P.dx * P.dx);
+    for (int t = 0; t < kTypes; t++) {
+        Q.mass[t] = (float)P.mass[t];
+        Q.density[t] = (float)P.density[t];
+        Q.bulk[t] = (float)P.bulk[t];
+        Q.bvisc[t] = (float)P.bvisc[t];
+        Q.svisc[t] = (float)P.svisc[t];
+        Q.friction[t] = (float)P.friction[t];
+        Q.CofA[t] = (float)P.CofA[t];
+        Q.ai[t] = (float)P.ai[t];
+        Q.logE[t] = (float)P.logE[t];
+        Q.cnDen[t] = (float)P.cnDen[t];
+        Q.ctFac[t] = (float)P.ctFac[t];
+        for (int u = 0; u < kTypes; u++) {
+            Q.ratio[t][u] = (float)P.ratio[t][u];
+            Q.Eeff[t][u] = (float)P.Eeff[t][u];
+            Q.KtFac[t][u] = (float)P.KtFac[t][u];
+        }
+    }
+    return Q;
+}
+
+static inline int blocks32(int b, int e) { return (e - b + kWarpsPerBlock32 - 1) / kWarpsPerBlock32; }
+
+void launch_drift32(const DevParams &P, const DevParams32 &Q, const DevState &S, const WallMotion &Wm,
+                    unsigned long long *maxshift, int sms, cudaStream_t st)
+{
+    int blocks = (P.N + 255) / 256;
+    if (blocks > sms * 8) blocks = sms * 8;
+    k_drift32<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(P, Q, S, Wm, maxshift);
+}
+void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, cudaStream_t st)
+{
+    if (ce > cb) k_pass_a32<<<blocks32(cb, ce), kWarpsPerBlock32 * kWarp, 0, st>>>(P, Q, S, cb, ce);
+}
+void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, cudaStream_t st)
+{
+    if (ce > cb) k_pass_b32<<<blocks32(cb, ce), kWarpsPerBlock32 * kWarp, 0, st>>>(P, Q, S, cb, ce);
+}
+void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, int b, int e, cudaStream_t st)
+{
+    if (e > b) k_fluid_accel32<<<(e - b + 255) / 256, 256, 0, st>>>(Q, S, b, e);
+}
+void launch_dem_force32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, int forces,
+                        cudaStream_t st)
+{
+    if (ce > cb) k_dem_force32<<<blocks32(cb, ce), kWarpsPerBlock32 * kWarp, 0, st>>>(P, Q, S, cb, ce, forces);
+}
+void launch_dem_integrate32(const DevParams32 &Q, const DevState &S, int b, int e, cudaStream_t st)
+{
+    if (e > b) k_dem_integrate32<<<(e - b + 127) / 128, 128, 0, st>>>(Q, S, b, e);
+}
+void launch_export32(const DevParams &P, const DevState &S, double *pos, double *vel, cudaStream_t st)
+{
+    k_export32<<<(P.N + 255) / 256, 256, 0, st>>>(P, S, pos, vel);
+}
+void launch_import32(const DevParams &P, const DevState &S, const double *pos, const double *vel, cudaStream_t st)
+{
+    k_import32<<<(P.N + 255) / 256, 256, 0, st>>>(P, S, pos, vel);
+}
+void launch_permute32(const DevParams &P, const unsigned long long *words, const double *xabs, const float4 *v_in,
+                      const int *type_in, const int *pidx_in, float4 *p_out, float4 *v_out, int *type_out,
+                      int *pidx_out, double *xref, float4 *xref4, cudaStream_t st)
+{
+    k_permute32<<<(P.N + 255) / 256, 256, 0, st>>>(P, words, xabs, v_in, type_in, pidx_in, p_out, v_out, type_out,
+                                                   pidx_out, xref, xref4);
+}
+void launch_widen_f(const float *in, double *out, int n, cudaStream_t st)
+{
+    if (n > 0) k_widen_f<<<(n + 255) / 256, 256, 0, st>>>(in, out, n);
+}
+void launch_widen_f4(const float4 *in, double *out, int n, cudaStream_t st)
+{
+    if (n > 0) k_widen_f4<<<(n + 255) / 256, 256, 0, st>>>(in, out, n);
+}
+
+}  // namespace dmph

@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, 
 // :512), calculatePressureP :2210-2245, calculatePressureA :2033-2070,
 // calculateDiffuseInterface :2074-2126, calculateViscosityV :2248-2292,
 // calculateBuoyancyForce :2699-2737, calculateGravity :2811 and
-// calculateAcceleration :2832.  Each reference kernel's per-particle sum is
+// (calculateAcceleration :2832 follows in k_fluid_accel).  Each reference kernel's per-particle sum is
 // kept in its own accumulator and added to Force in the reference's call
 // order, so the sums are bit-identical.  Wall particles are not visited:
 // their forces are reset at the next step without ever being read.
@@ -358,7 +358,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, 
             for (int d = 0; d < 3; d++) F[d] += fI[d];
         for (int d = 0; d < 3; d++) F[d] += fV[d];
         for (int d = 0; d < 3; d++) F[d] += m * P.g[d];
-        for (int d = 0; d < 3; d++) S.vel[d * N + i] = (d == 0 ? vxi : d == 1 ? vyi : vzi) + F[d] / m * P.dt;
     }
     for (int d = 0; d < 3; d++) S.frc[d * N + i] = F[d];
 }
@@ -475,6 +474,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_dem_force(DevParams 
         F += fT[d];
         S.frc[d * N + i] = F;
     }
+}
+
+// calculateAcceleration :2832-2843 over the fluid slots [b, e).  A kernel of
+// its own: pass B reads the velocities of neighbouring particles, so they may
+// only change once every force of the step is known.
+__global__ void k_fluid_accel(DevParams P, DevState S, int b, int e)
+{
+    const int N = P.N;
+    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= e) return;
+    const double m = P.mass[S.type[i]];
+    for (int d = 0; d < 3; d++) S.vel[d * N + i] += S.frc[d * N + i] / m * P.dt;
 }
 
 // calculateDEMconvection :1872-1891 over the solid slots [b, e)
@@ -596,6 +607,10 @@ void launch_pass_b(const DevParams &P, const DevState &S, int cb, int ce, cudaSt
 void launch_dem_force(const DevParams &P, const DevState &S, int cb, int ce, int forces, cudaStream_t st)
 {
     if (ce > cb) k_dem_force<<<chunk_blocks(cb, ce), kWarpsPerBlock * kWarp, 0, st>>>(P, S, cb, ce, forces);
+}
+void launch_fluid_accel(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st)
+{
+    if (e > b) k_fluid_accel<<<(e - b + 255) / 256, 256, 0, st>>>(P, S, b, e);
 }
 void launch_dem_integrate(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st)
 {

@@ -27,10 +27,29 @@ void launch_drift(const DevParams &P, const DevState &S, const WallMotion &Wm, u
                   cudaStream_t st);
 void launch_pass_a(const DevParams &P, const DevState &S, int cb, int ce, int init_only, cudaStream_t st);
 void launch_pass_b(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st);
+void launch_fluid_accel(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st);
 void launch_dem_force(const DevParams &P, const DevState &S, int cb, int ce, int forces, cudaStream_t st);
 void launch_dem_integrate(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st);
 void launch_counts(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st);
 void launch_neighbor_fill(const DevParams &P, const DevState &S, int cb, int ce, const long long *ptr, int *ind,
                           cudaStream_t st);
+
+// dmph_f32.cu
+DevParams32 make_params32(const DevParams &P);
+void launch_drift32(const DevParams &P, const DevParams32 &Q, const DevState &S, const WallMotion &Wm,
+                    unsigned long long *maxshift, int sms, cudaStream_t st);
+void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, cudaStream_t st);
+void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, cudaStream_t st);
+void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, int b, int e, cudaStream_t st);
+void launch_dem_force32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, int forces,
+                        cudaStream_t st);
+void launch_dem_integrate32(const DevParams32 &Q, const DevState &S, int b, int e, cudaStream_t st);
+void launch_export32(const DevParams &P, const DevState &S, double *pos, double *vel, cudaStream_t st);
+void launch_import32(const DevParams &P, const DevState &S, const double *pos, const double *vel, cudaStream_t st);
+void launch_permute32(const DevParams &P, const unsigned long long *words, const double *xabs, const float4 *v_in,
+                      const int *type_in, const int *pidx_in, float4 *p_out, float4 *v_out, int *type_out,
+                      int *pidx_out, double *xref, float4 *xref4, cudaStream_t st);
+void launch_widen_f(const float *in, double *out, int n, cudaStream_t st);
+void launch_widen_f4(const float4 *in, double *out, int n, cudaStream_t st);
 
 }  // namespace dmph

@@ -20,6 +20,42 @@ struct DevState {
     unsigned long long *skey;       // sorted (key << 32 | slot), P2 entries
     int *cell_start;                // 3T + 1 entries
     Chunk *chunks;
+    // FP32 split-precision state (DMPH_PRECISION_FP32_SPLIT): positions relative
+    // to the origin of the particle's rebuild-time cell, the cell coordinates
+    // and type packed in .w (pack_cell), so every pair is formed in the frame
+    // of one cell with FP32 magnitudes of a few particle spacings
+    float4 *p4, *v4, *f4, *xref4, *gc4;
+    float *pres32, *vsp32, *div32, *densA32, *pA32;
+    float *kn32, *cn32, *kt32, *ct32, *alpha32, *dragC32;
+};
+
+// .w of the FP32 position: type (3 bits) | cx (10) | cy (10) | cz (9)
+__host__ __device__ inline unsigned pack_cell(int t, int cx, int cy, int cz)
+{
+    return (unsigned)t | ((unsigned)cx << 3) | ((unsigned)cy << 13) | ((unsigned)cz << 23);
+}
+__host__ __device__ inline int unpack_type(unsigned w) { return (int)(w & 7u); }
+__host__ __device__ inline int unpack_cx(unsigned w) { return (int)((w >> 3) & 1023u); }
+__host__ __device__ inline int unpack_cy(unsigned w) { return (int)((w >> 13) & 1023u); }
+__host__ __device__ inline int unpack_cz(unsigned w) { return (int)((w >> 23) & 511u); }
+
+// FP32 copies of the scene constants used by the split-precision kernels
+struct DevParams32 {
+    float cw[3];
+    float dx, V, dt, ddt, dx2;
+    float RP2, RV2, RA2, RG2;
+    float iRP, iRV, iRA, iRG;            // 1/h
+    float Bp, Bv, Ba, Bg;                // (1/Sw)/h^dim
+    float dwp, dwv, dwg;                 // -2 B / h of the quadratic kernels
+    float N0p, N0a, R2g_inv_RG;          // RG / R2g
+    float viscC, Reff, Vdx;              // V/dx
+    float g[3];
+    float mass[kTypes], density[kTypes], bulk[kTypes], bvisc[kTypes], svisc[kTypes], friction[kTypes];
+    float CofA[kTypes], ai[kTypes];
+    float ratio[kTypes][kTypes];
+    float Eeff[kTypes][kTypes], KtFac[kTypes][kTypes];
+    float logE[kTypes], cnDen[kTypes], ctFac[kTypes];
+    float drag_pref;                     // 0.5 dx^3
 };
 
 // Moving-wall constants (calculateWall, source/DEM-MPH.cpp:2846-2900)

@@ -39,6 +39,8 @@ def lib():
         L.dmph_get_field.argtypes = [vp, C.c_int, vp]
         L.dmph_get_info.argtypes = [vp, vp]
         L.dmph_get_neighbor_list.argtypes = [vp, vp, vp, C.c_int64]
+        L.dmph_set_profiling.argtypes = [vp, C.c_int]
+        L.dmph_get_phase_times.argtypes = [vp, vp, vp, C.c_int]
         L.dmph_destroy.argtypes = [vp]
         L.dmph_last_error.argtypes = [vp]
         L.dmph_last_error.restype = C.c_char_p
@@ -116,6 +118,18 @@ class Solver:
         ind = np.empty(max(int(ptr[-1]), 1), np.int32)
         self._check(lib().dmph_get_neighbor_list(self._h, _ptr(ptr), _ptr(ind), int(ptr[-1])))
         return ptr, ind[:int(ptr[-1])]
+
+    PHASES = ("drift", "rebuild", "pass_a", "pass_b", "dem", "bodies")
+
+    def set_profiling(self, on=True):
+        self._check(lib().dmph_set_profiling(self._h, 1 if on else 0))
+
+    def phase_times(self):
+        """{phase: (total_ms, count)} accumulated since set_profiling(True)"""
+        ms = np.zeros(len(self.PHASES), np.float64)
+        n = np.zeros(len(self.PHASES), np.int64)
+        self._check(lib().dmph_get_phase_times(self._h, _ptr(ms), _ptr(n), len(self.PHASES)))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.PHASES)}
 
     def close(self):
         if getattr(self, "_h", None):

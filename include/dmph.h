@@ -214,6 +214,16 @@ int dmph_get_info(dmph_ctx *ctx, dmph_info *info);
  */
 int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind, int64_t capacity);
 
+/* Per-phase device timing.  With enable != 0, every following step records
+ * CUDA events on the context's stream around each phase (this adds event
+ * overhead, so time throughput with it off); dmph_get_phase_times returns the
+ * accumulated milliseconds and launch counts per phase since it was enabled:
+ * index 0 drift, 1 rebuild, 2 pass A, 3 pass B, 4 DEM substeps, 5 rigid
+ * bodies. */
+#define DMPH_PHASE_COUNT 6
+int dmph_set_profiling(dmph_ctx *ctx, int enable);
+int dmph_get_phase_times(dmph_ctx *ctx, double *ms, int64_t *launches, int n);
+
 /* Release the context and its device memory. */
 int dmph_destroy(dmph_ctx *ctx);
 
