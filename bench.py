@@ -183,10 +183,15 @@ def main():
     # ---- timed region: K steps, device time on the solver's stream
     barrier()
     torch.cuda.synchronize()
+    l0 = g.info().kernel_launches
+    rebuilds_before = int(g.info().rebuilds)
     with ClockSampler(torch.cuda.current_device()) as clk:
         ms = g.step_timed(args.steps)
         torch.cuda.synchronize()
     barrier()
+    inf_t = g.info()
+    launches = int(inf_t.kernel_launches - l0)
+    rebuilds_timed = int(inf_t.rebuilds)
     ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
@@ -267,14 +272,14 @@ def main():
         "config": {"workload": scene.name, "n_particles": counts["total"], "n_fluid": counts["fluid"],
                    "n_solid": counts["solid"], "n_wall": counts["wall"], "n_debris_bodies": len(scene.body_density),
                    "precision": args.precision, "dt": p.dt, "dem_substeps": inf.dem_substeps,
-                   "rebuilds_in_timed_steps": None, "parallelism": "replicas x%d" % world,
+                   "rebuilds_in_timed_steps": rebuilds_timed - rebuilds_before, "parallelism": "replicas x%d" % world,
                    "l2": "inputs larger than L2 (particle state alone %.0f MB)" % (n * 60 / 1e6)},
         "sim_s_per_hour": p.dt * args.steps / (ms_max / 1e3) * 3600.0,
         "clocks": clk.summary(),
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": None,
+        "gpu_launches": launches,
     }
     if rank == 0:
         print(json.dumps(out))

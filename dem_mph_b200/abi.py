@@ -108,6 +108,7 @@ class Info(C.Structure):
         ("max_radius", C.c_double),
         ("num_bodies", C.c_int32),
         ("surface_tension", C.c_int32),
+        ("kernel_launches", C.c_int64),
     ]
 
 

@@ -41,6 +41,7 @@ CU_SOURCES = [
     ("dmph_rebuild.cu", ["-fmad=false"]),
     ("dmph_api.cu", ["-fmad=false"]),
     ("dmph_f32.cu", []),
+    ("dmph_bodies.cu", []),
 ]
 CPP_SOURCES = ["dmph_params.cpp", "dmph_io.cpp"]
 HEADERS = ["dmph_device.cuh", "dmph_state.cuh", "dmph_traverse.cuh", "dmph_internal.h"]
@@ -91,8 +92,10 @@ def build(force=False, verbose=False):
         _run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
     host_src = os.path.join(HOST, "dem_mph.cpp")
     if os.path.exists(host_src) and (force or _newer(EXE, [host_src, LIB, os.path.join(ROOT, "include", "dmph.h")])):
-        _run(["g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), host_src,
-              "-o", EXE, "-L", HERE, "-ldmph", "-Wl,-rpath,$ORIGIN"])
+        _run(["g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"),
+              "-I", os.path.join(cuda, "include"), host_src, "-o", EXE, "-L", HERE, "-ldmph",
+              "-L", os.path.join(cuda, "lib64"), "-lcudart", "-Wl,-rpath,$ORIGIN",
+              "-Wl,-rpath," + os.path.join(cuda, "lib64")])
     if verbose:
         for l in logs:
             sys.stdout.write(l)

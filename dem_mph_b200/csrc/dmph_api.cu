@@ -29,6 +29,8 @@ struct dmph_ctx {
     double *pos2 = nullptr, *vel2 = nullptr;
     int *type2 = nullptr, *pidx2 = nullptr;
     float4 *p4b = nullptr, *v4b = nullptr;  // second buffers of the FP32 state
+    int *bid2 = nullptr;                     // second buffer of the body ids
+    DevBodies Bd{};                          // rigid clumps (B = 0: off)
     unsigned long long *words = nullptr;
     int *flag = nullptr, *offs = nullptr, *bsums = nullptr, *total = nullptr;
     unsigned long long *maxshift = nullptr;
@@ -39,6 +41,7 @@ struct dmph_ctx {
     int demSteps = 0;
     double time = 0.0;
     long long steps = 0, rebuilds = 0;
+    long long launches = 0;  // kernels launched by dmph_step
     bool all_counts = false;
     bool prof = false;
     cudaEvent_t pe0 = nullptr, pe1 = nullptr;
@@ -89,6 +92,15 @@ static void release(dmph_ctx *ctx)
     ctx->st = nullptr;
 }
 
+// number of kernels launch_bitonic issues for n = 2^nlog words
+static long long bitonic_launches(int n, int nlog)
+{
+    const int tlog = n < 2048 ? nlog : 11;
+    long long c = tlog > 0 ? 1 : 0;
+    for (int stage = tlog; stage < nlog; ++stage) c += (stage - tlog + 1) + 1;
+    return c;
+}
+
 // calculateCellParticle :1288 + the parts of calculateNeighbor the step needs
 static int rebuild(dmph_ctx *ctx, bool first = false)
 {
@@ -101,17 +113,24 @@ static int rebuild(dmph_ctx *ctx, bool first = false)
     launch_cell_start(P, ctx->words, ctx->S.cell_start, ctx->st);
     if (ctx->fp32) {
         launch_permute32(P, ctx->words, ctx->S.pos, ctx->S.v4, ctx->S.type, ctx->S.pidx, ctx->p4b, ctx->v4b,
-                         ctx->type2, ctx->pidx2, ctx->S.xref, ctx->S.xref4, ctx->st);
+                         ctx->type2, ctx->pidx2, ctx->S.xref, ctx->S.xref4, ctx->S.bid, ctx->bid2, ctx->S.vel,
+                         ctx->pos2, ctx->vel2, ctx->st);
         std::swap(ctx->S.p4, ctx->p4b);
         std::swap(ctx->S.v4, ctx->v4b);
+        std::swap(ctx->S.pos, ctx->pos2);
+        std::swap(ctx->S.vel, ctx->vel2);
     } else {
         launch_permute(P, ctx->words, ctx->S.pos, ctx->S.vel, ctx->S.type, ctx->S.pidx, ctx->pos2, ctx->vel2,
-                       ctx->type2, ctx->pidx2, ctx->S.xref, ctx->st);
+                       ctx->type2, ctx->pidx2, ctx->S.xref, ctx->S.bid, ctx->bid2, ctx->st);
         std::swap(ctx->S.pos, ctx->pos2);
         std::swap(ctx->S.vel, ctx->vel2);
     }
     std::swap(ctx->S.type, ctx->type2);
     std::swap(ctx->S.pidx, ctx->pidx2);
+    if (ctx->S.bid) {
+        std::swap(ctx->S.bid, ctx->bid2);
+        launch_slot_of_row(P, ctx->S.pidx, ctx->Bd.slot_of_row, ctx->st);
+    }
     ctx->S.skey = ctx->words;
     launch_chunks(P, ctx->words, ctx->S.cell_start, ctx->flag, ctx->offs, ctx->bsums, ctx->total, ctx->S.chunks,
                   ctx->st);
@@ -139,6 +158,10 @@ static int rebuild(dmph_ctx *ctx, bool first = false)
     else
         launch_counts(P, ctx->S, ctx->ch_s0, ctx->ch_w0, ctx->st);
     CK(cudaGetLastError());
+    // keys, sort, cell starts, permute, (export), chunk flags + 3 scan + write, counts
+    ctx->launches += 1 + bitonic_launches(P.P2, P.P2log) + 1 + 1 + (ctx->fp32 && !first ? 1 : 0) + 5 +
+                     (ctx->S.bid ? 1 : 0) +
+                     ((ctx->all_counts ? ctx->ch_end > 0 : ctx->ch_w0 > ctx->ch_s0) ? 1 : 0);
     return DMPH_OK;
 }
 
@@ -194,13 +217,21 @@ static int step_once(dmph_ctx *ctx)
         launch_pass_b32(P, Q, ctx->S, 0, ctx->ch_w0, ctx->st);
         launch_fluid_accel32(Q, ctx->S, ctx->fb, ctx->fe, ctx->st);
         phase_end(ctx, 3);
+        // DEM and rigid bodies in FP64 on the solids' and walls' master state
         phase_begin(ctx);
+        launch_solid_force_to64(P, ctx->S, ctx->sb, ctx->se, ctx->st);
         for (int k = 0; k < ctx->demSteps; ++k) {
-            launch_dem_force32(P, Q, ctx->S, ctx->ch_s0, ctx->ch_w0, 1, ctx->st);
-            if (P.wall_dem_coeffs) launch_dem_force32(P, Q, ctx->S, ctx->ch_w0, ctx->ch_end, 0, ctx->st);
-            launch_dem_integrate32(Q, ctx->S, ctx->sb, ctx->se, ctx->st);
+            if (ctx->Bd.B > 0) {
+                launch_clump_dem(P, ctx->S, ctx->ch_s0, ctx->ch_w0, ctx->st);
+                launch_body_step(P, ctx->S, ctx->Bd, true, ctx->st);
+                continue;
+            }
+            launch_dem_force(P, ctx->S, ctx->ch_s0, ctx->ch_w0, 1, ctx->st, true);
+            if (P.wall_dem_coeffs) launch_dem_force(P, ctx->S, ctx->ch_w0, ctx->ch_end, 0, ctx->st, true);
+            launch_dem_integrate(P, ctx->S, ctx->sb, ctx->se, ctx->st);
         }
-        phase_end(ctx, 4);
+        launch_sync_solids32(P, ctx->S, ctx->sb, ctx->se, ctx->st);
+        phase_end(ctx, ctx->Bd.B > 0 ? 5 : 4);
     } else {
         phase_begin(ctx);
         launch_pass_a(P, ctx->S, 0, ctx->ch_end, 0, ctx->st);
@@ -211,13 +242,29 @@ static int step_once(dmph_ctx *ctx)
         phase_end(ctx, 3);
         phase_begin(ctx);
         for (int k = 0; k < ctx->demSteps; ++k) {
+            if (ctx->Bd.B > 0) {
+                launch_clump_dem(P, ctx->S, ctx->ch_s0, ctx->ch_w0, ctx->st);
+                launch_body_step(P, ctx->S, ctx->Bd, false, ctx->st);
+                continue;
+            }
             launch_dem_force(P, ctx->S, ctx->ch_s0, ctx->ch_w0, 1, ctx->st);
             if (P.wall_dem_coeffs) launch_dem_force(P, ctx->S, ctx->ch_w0, ctx->ch_end, 0, ctx->st);
             launch_dem_integrate(P, ctx->S, ctx->sb, ctx->se, ctx->st);
         }
-        phase_end(ctx, 4);
+        phase_end(ctx, ctx->Bd.B > 0 ? 5 : 4);
     }
     CK(cudaGetLastError());
+    {
+        long long l = 1;  // drift
+        l += ctx->ch_end > 0 ? 1 : 0;                       // pass A
+        l += ctx->ch_w0 > 0 ? 1 : 0;                        // pass B
+        l += ctx->fe > ctx->fb ? 1 : 0;                     // fluid velocity update
+        const long long dem =
+            ctx->Bd.B > 0 ? (ctx->ch_w0 > ctx->ch_s0 ? 1 : 0) + 1
+                          : (ctx->ch_w0 > ctx->ch_s0 ? 1 : 0) + (P.wall_dem_coeffs && ctx->ch_end > ctx->ch_w0 ? 1 : 0) +
+                                (ctx->se > ctx->sb ? 1 : 0);
+        ctx->launches += l + ctx->demSteps * dem + (ctx->fp32 && ctx->se > ctx->sb ? 2 : 0);
+    }
     ctx->time += P.dt;
     ctx->steps++;
     return DMPH_OK;
@@ -337,10 +384,6 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         AL(S.div32, N);
         AL(S.densA32, N);
         AL(S.pA32, N);
-        AL(S.kn32, N);
-        AL(S.cn32, N);
-        AL(S.kt32, N);
-        AL(S.ct32, N);
         AL(S.alpha32, N);
         AL(S.dragC32, N);
     }
@@ -384,6 +427,7 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     CKC(cudaStreamSynchronize(ctx->st));
 #undef AL
 #undef CKC
+    ctx->launches = 0;
     *out = ctx;
     return DMPH_OK;
 }
@@ -481,17 +525,13 @@ extern "C" int dmph_get_field(dmph_ctx *ctx, int field_id, void *out)
         // widen the FP32 field into its FP64 twin, then copy as in FP64 mode
         const int n = (int)N;
         switch (field_id) {
-        case DMPH_FIELD_FORCE: launch_widen_f4(S.f4, S.frc, n, ctx->st); break;
-        case DMPH_FIELD_GRAVITY_CENTER: launch_widen_f4(S.gc4, S.gc, n, ctx->st); break;
+        case DMPH_FIELD_FORCE: launch_widen_f4(S.f4, S.frc, ctx->fe, n, ctx->st); break;  // solids: FP64 already
+        case DMPH_FIELD_GRAVITY_CENTER: launch_widen_f4(S.gc4, S.gc, n, n, ctx->st); break;
         case DMPH_FIELD_VOL_STRAIN_P: launch_widen_f(S.vsp32, S.vsp, n, ctx->st); break;
         case DMPH_FIELD_DIVERGENCE_P: launch_widen_f(S.div32, S.divp, n, ctx->st); break;
         case DMPH_FIELD_PRESSURE_P: launch_widen_f(S.pres32, S.pres, n, ctx->st); break;
         case DMPH_FIELD_DENSITY_A: launch_widen_f(S.densA32, S.densA, n, ctx->st); break;
         case DMPH_FIELD_PRESSURE_A: launch_widen_f(S.pA32, S.pA, n, ctx->st); break;
-        case DMPH_FIELD_NORMAL_SPRING: launch_widen_f(S.kn32, S.kn, n, ctx->st); break;
-        case DMPH_FIELD_NORMAL_DAMPING: launch_widen_f(S.cn32, S.cn, n, ctx->st); break;
-        case DMPH_FIELD_TANGENTIAL_SPRING: launch_widen_f(S.kt32, S.kt, n, ctx->st); break;
-        case DMPH_FIELD_TANGENTIAL_DAMPING: launch_widen_f(S.ct32, S.ct, n, ctx->st); break;
         case DMPH_FIELD_ALPHA: launch_widen_f(S.alpha32, S.alpha, n, ctx->st); break;
         case DMPH_FIELD_DRAG_C: launch_widen_f(S.dragC32, S.dragC, n, ctx->st); break;
         default: break;
@@ -566,8 +606,9 @@ extern "C" int dmph_get_info(dmph_ctx *ctx, dmph_info *info)
     info->n0p = P.N0p;
     info->r2g = P.R2g;
     info->max_radius = std::sqrt(P.rc2) - 0.1 * P.dx;
-    info->num_bodies = 0;
+    info->num_bodies = ctx->Bd.B;
     info->surface_tension = P.surface_tension;
+    info->kernel_launches = ctx->launches;
     return DMPH_OK;
 }
 
@@ -618,6 +659,186 @@ extern "C" int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind,
         // computed the same values for them, so nothing to restore
     }
     return rc;
+}
+
+// 3x3 inverse (FP64, host)
+static bool inverse3(const double a[9], double o[9])
+{
+    const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+    const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+    if (!(std::fabs(det) > 0.0)) return false;
+    const double id = 1.0 / det;
+    o[0] = c00 * id;
+    o[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+    o[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    o[3] = c01 * id;
+    o[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    o[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    o[6] = c02 * id;
+    o[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+    o[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+    return true;
+}
+
+extern "C" int dmph_set_bodies(dmph_ctx *ctx, int nbodies, const int *body_of_row, const double *body_density)
+{
+    if (!ctx || nbodies <= 0 || !body_of_row || !body_density) return DMPH_EINVAL;
+    if (ctx->Bd.B > 0 || ctx->steps > 0) {
+        ctx->err = "dmph_set_bodies must be called once, before the first step";
+        return DMPH_EINVAL;
+    }
+    const DevParams &P = ctx->P;
+    const int N = P.N;
+    std::vector<int> type(N), pidx(N);
+    std::vector<double> x(3 * (size_t)N), v(3 * (size_t)N);
+    int rc = dmph_get_state(ctx, type.data(), x.data(), v.data(), pidx.data());
+    if (rc) return rc;
+    // rows -> current data
+    std::vector<int> slot_of_row(N);
+    for (int i = 0; i < N; i++) slot_of_row[pidx[i]] = i;
+    std::vector<std::vector<int>> members(nbodies);
+    for (int r = 0; r < N; r++) {
+        const int b = body_of_row[r];
+        const int t = type[slot_of_row[r]];
+        if (b < -1 || b >= nbodies) return ctx->err = "body index out of range", DMPH_EINVAL;
+        if (b >= 0 && !is_solid(t)) return ctx->err = "a body member is not a solid particle", DMPH_EINVAL;
+        if (b < 0 && is_solid(t)) return ctx->err = "every solid particle must belong to a body", DMPH_EINVAL;
+        if (b >= 0) members[b].push_back(r);
+    }
+    for (int b = 0; b < nbodies; b++) {
+        if (members[b].empty()) return ctx->err = "empty body", DMPH_EINVAL;
+        if (!(body_density[b] > 0.0)) return ctx->err = "body density must be positive", DMPH_EINVAL;
+    }
+    std::vector<int> ptr(nbodies + 1, 0), mrow;
+    std::vector<double> r0, X(3 * nbodies), V(3 * nbodies), L(3 * nbodies), q(4 * nbodies), M(nbodies),
+        Iinv(9 * nbodies);
+    for (int b = 0; b < nbodies; b++) {
+        const double m = body_density[b] * P.V;
+        const auto &mb = members[b];
+        // unwrap the members around the first one (periodic domain)
+        const double *x0 = &x[3 * (size_t)slot_of_row[mb[0]]];
+        double c[3] = {0, 0, 0}, vc[3] = {0, 0, 0};
+        std::vector<double> xu(3 * mb.size());
+        for (size_t k = 0; k < mb.size(); k++) {
+            const int i = slot_of_row[mb[k]];
+            for (int d = 0; d < 3; d++) {
+                double dd = x[3 * (size_t)i + d] - x0[d];
+                dd -= P.W[d] * std::nearbyint(dd / P.W[d]);
+                xu[3 * k + d] = x0[d] + dd;
+                c[d] += xu[3 * k + d];
+                vc[d] += v[3 * (size_t)i + d];
+            }
+        }
+        for (int d = 0; d < 3; d++) {
+            c[d] /= (double)mb.size();
+            vc[d] /= (double)mb.size();
+        }
+        const double a = 0.4 * m * (0.5 * P.dx) * (0.5 * P.dx);  // solid-sphere inertia of each particle
+        double I[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, Lb[3] = {0, 0, 0};
+        for (size_t k = 0; k < mb.size(); k++) {
+            const int i = slot_of_row[mb[k]];
+            const double r[3] = {xu[3 * k] - c[0], xu[3 * k + 1] - c[1], xu[3 * k + 2] - c[2]};
+            const double rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+            for (int p = 0; p < 3; p++)
+                for (int qq = 0; qq < 3; qq++) I[3 * p + qq] += m * ((p == qq ? rr : 0.0) - r[p] * r[qq]);
+            for (int p = 0; p < 3; p++) I[4 * p] += a;
+            const double u[3] = {v[3 * (size_t)i] - vc[0], v[3 * (size_t)i + 1] - vc[1], v[3 * (size_t)i + 2] - vc[2]};
+            Lb[0] += m * (r[1] * u[2] - r[2] * u[1]);
+            Lb[1] += m * (r[2] * u[0] - r[0] * u[2]);
+            Lb[2] += m * (r[0] * u[1] - r[1] * u[0]);
+            mrow.push_back(mb[k]);
+            for (int d = 0; d < 3; d++) r0.push_back(r[d]);
+        }
+        ptr[b + 1] = (int)mrow.size();
+        if (!inverse3(I, &Iinv[9 * b])) return ctx->err = "singular body inertia", DMPH_EINVAL;
+        for (int d = 0; d < 3; d++) {
+            X[3 * b + d] = c[d];
+            V[3 * b + d] = vc[d];
+            L[3 * b + d] = Lb[d];
+        }
+        q[4 * b] = 1.0;
+        q[4 * b + 1] = q[4 * b + 2] = q[4 * b + 3] = 0.0;
+        M[b] = m * (double)mb.size();
+    }
+    // device arrays
+    const size_t nm = mrow.size();
+    DevBodies &Bd = ctx->Bd;
+    int *dptr = nullptr, *dmrow = nullptr, *dsor = nullptr, *dbid = nullptr, *dbid2 = nullptr;
+    double *dr0 = nullptr, *dX = nullptr, *dV = nullptr, *dL = nullptr, *dq = nullptr, *dM = nullptr, *dI = nullptr,
+           *dF = nullptr, *dT = nullptr, *drho = nullptr, *dfd = nullptr;
+#define AB(ptr_, cnt_)                                      \
+    do {                                                    \
+        int r_ = dalloc(ctx, &(ptr_), (size_t)(cnt_));      \
+        if (r_) return r_;                                  \
+    } while (0)
+    AB(dptr, nbodies + 1);
+    AB(dmrow, nm);
+    AB(dsor, N);
+    AB(dbid, N);
+    AB(dbid2, N);
+    AB(dr0, 3 * nm);
+    AB(dX, 3 * nbodies);
+    AB(dV, 3 * nbodies);
+    AB(dL, 3 * nbodies);
+    AB(dq, 4 * nbodies);
+    AB(dM, nbodies);
+    AB(dI, 9 * nbodies);
+    AB(dF, 3 * nbodies);
+    AB(dT, 3 * nbodies);
+    AB(drho, nbodies);
+    AB(dfd, 6 * (size_t)N);
+#undef AB
+    std::vector<int> bid(N);
+    for (int i = 0; i < N; i++) bid[i] = body_of_row[pidx[i]];
+    CK(cudaMemcpyAsync(dptr, ptr.data(), (nbodies + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dmrow, mrow.data(), nm * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dsor, slot_of_row.data(), N * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dbid, bid.data(), N * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dr0, r0.data(), 3 * nm * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dX, X.data(), 3 * nbodies * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dV, V.data(), 3 * nbodies * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dL, L.data(), 3 * nbodies * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dq, q.data(), 4 * nbodies * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dM, M.data(), nbodies * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(dI, Iinv.data(), 9 * nbodies * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(drho, body_density, nbodies * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    Bd.B = nbodies;
+    Bd.ptr = dptr;
+    Bd.member_row = dmrow;
+    Bd.slot_of_row = dsor;
+    Bd.r0 = dr0;
+    Bd.X = dX;
+    Bd.V = dV;
+    Bd.L = dL;
+    Bd.q = dq;
+    Bd.M = dM;
+    Bd.Iinv0 = dI;
+    Bd.Fsum = dF;
+    Bd.Tsum = dT;
+    ctx->S.bid = dbid;
+    ctx->bid2 = dbid2;
+    ctx->S.body_rho = drho;
+    ctx->S.frc_dem = dfd;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_get_bodies(dmph_ctx *ctx, double *X, double *V, double *q, double *L, double *mass, double *F,
+                               double *T)
+{
+    if (!ctx) return DMPH_EINVAL;
+    const DevBodies &Bd = ctx->Bd;
+    const size_t B = (size_t)Bd.B;
+    if (B == 0) return DMPH_OK;
+    if (X) CK(cudaMemcpyAsync(X, Bd.X, 3 * B * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    if (V) CK(cudaMemcpyAsync(V, Bd.V, 3 * B * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    if (q) CK(cudaMemcpyAsync(q, Bd.q, 4 * B * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    if (L) CK(cudaMemcpyAsync(L, Bd.L, 3 * B * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    if (mass) CK(cudaMemcpyAsync(mass, Bd.M, B * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    if (F) CK(cudaMemcpyAsync(F, Bd.Fsum, 3 * B * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    if (T) CK(cudaMemcpyAsync(T, Bd.Tsum, 3 * B * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return DMPH_OK;
 }
 
 extern "C" int dmph_set_profiling(dmph_ctx *ctx, int enable)

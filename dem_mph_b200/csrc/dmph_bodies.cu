@@ -1,0 +1,305 @@
+// Rigid debris clumps (DMPH_FLAG_RIGID_CLUMPS).  No counterpart in the
+// reference: there, debris particles move individually (calculateDEMconvection,
+// source/DEM-MPH.cpp:1872-1891) and the torque/inertia code
+// (:2402-2557) feeds nothing.  Here each debris body is rigid:
+//
+//   1. k_clump_dem: for every body particle, the spring-dashpot contact force
+//      from particles of OTHER bodies, free debris and walls within dx.  The
+//      pair constants follow the reference's Hertz-type formulas (effective
+//      modulus, overlap, restitution damping; :2318-2338, :2374-2396) but are
+//      evaluated per pair with pair-symmetric restitution and friction, the
+//      normal damping is the projection c_n (u.e) e, and the tangential force
+//      opposes sliding and is capped by Coulomb friction.  The force acts at
+//      the contact midpoint, so the offset torque 0.5 q x F is kept too; pair
+//      forces are antisymmetric and total linear and angular momentum of
+//      colliding bodies are conserved.
+//   2. k_body_step: one warp per body reduces, in FP64 with warp shuffles,
+//      the total force F = sum(fluid + contact) and torque
+//      T = sum(R r0 x f + contact offset torques) over its members (gathered
+//      through slot_of_row, so the reduction order is the body's fixed member
+//      order, independent of the cell sort), then advances the body in FP64:
+//      V += F/M dt, X += V dt, L += T dt, q <- exp(w dt / 2) q with
+//      w = R I0^-1 R^T L, and places every member at X + R r0 with velocity
+//      V + w x (R r0).
+#include "dmph_internal.h"
+#include "dmph_traverse.cuh"
+
+namespace dmph {
+
+__global__ void k_slot_of_row(int N, const int *__restrict__ pidx, int *__restrict__ slot_of_row)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) slot_of_row[pidx[i]] = i;
+}
+
+struct ClumpTile {
+    double x[kWarp], y[kWarp], z[kWarp], vx[kWarp], vy[kWarp], vz[kWarp];
+    int t[kWarp], b[kWarp];
+};
+
+// position of slot j in FP64: absolute (FP64 mode) or in the frame of cell
+// (cix, ciy, ciz) (FP32 split mode)
+template <bool F32>
+__device__ __forceinline__ void load_xv(const DevParams &P, const DevState &S, int j, int cix, int ciy, int ciz,
+                                        double *x, double *v, int *t)
+{
+    const int N = P.N;
+    if (F32) {
+        const float4 p = S.p4[j];
+        const float4 vv = S.v4[j];
+        const unsigned w = __float_as_uint(p.w);
+        int d[3] = {unpack_cx(w) - cix, unpack_cy(w) - ciy, unpack_cz(w) - ciz};
+        for (int k = 0; k < 3; k++) d[k] = d[k] > 1 ? d[k] - P.cc[k] : (d[k] < -1 ? d[k] + P.cc[k] : d[k]);
+        x[0] = d[0] * P.cw[0] + (double)p.x;
+        x[1] = d[1] * P.cw[1] + (double)p.y;
+        x[2] = d[2] * P.cw[2] + (double)p.z;
+        v[0] = vv.x;
+        v[1] = vv.y;
+        v[2] = vv.z;
+        *t = unpack_type(w);
+    } else {
+        for (int k = 0; k < 3; k++) {
+            x[k] = S.pos[k * N + j];
+            v[k] = S.vel[k * N + j];
+        }
+        *t = S.type[j];
+    }
+}
+
+template <bool F32>
+__global__ void __launch_bounds__(4 * kWarp) k_clump_dem(DevParams P, DevState S, int chunk_begin, int chunk_end)
+{
+    __shared__ ClumpTile tiles[4];
+    ClumpTile &tl = tiles[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int N = P.N;
+    const int cidx = chunk_begin + blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (cidx >= chunk_end) return;
+    const Chunk ch = S.chunks[cidx];
+    const int i = ch.i0 + lane;
+    const bool active = lane < ch.cnt;
+    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+    const int cix = key_cell / (P.cc[1] * P.cc[2]), ciy = (key_cell / P.cc[2]) % P.cc[1], ciz = key_cell % P.cc[2];
+    const int ii = active ? i : ch.i0;
+    double xi[3], vi[3];
+    int ti;
+    load_xv<F32>(P, S, ii, cix, ciy, ciz, xi, vi, &ti);
+    const int bi = S.bid[ii];
+    const double mi = particle_density(S, P, ii, ti) * P.V;
+    double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
+    traverse_stencil(
+        P, S.cell_start, key_cell, lane, active, 6u,
+        [&](int j, int slot) {
+            double x[3], v[3];
+            int t;
+            load_xv<F32>(P, S, j, cix, ciy, ciz, x, v, &t);
+            tl.x[slot] = x[0];
+            tl.y[slot] = x[1];
+            tl.z[slot] = x[2];
+            tl.vx[slot] = v[0];
+            tl.vy[slot] = v[1];
+            tl.vz[slot] = v[2];
+            tl.t[slot] = t;
+            tl.b[slot] = S.bid[j];
+        },
+        [&](int j, int s) {
+            if (j == i || (bi >= 0 && tl.b[s] == bi)) return;
+            double q[3] = {tl.x[s] - xi[0], tl.y[s] - xi[1], tl.z[s] - xi[2]};
+            if (!F32)
+                for (int k = 0; k < 3; k++) q[k] -= P.W[k] * rint(q[k] / P.W[k]);
+            const double r2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+            if (r2 > P.dx2 || r2 <= 0.0) return;
+            const int tj = tl.t[s];
+            const double r = sqrt(r2);
+            const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
+            const double ov = P.dx - r;
+            const double u[3] = {tl.vx[s] - vi[0], tl.vy[s] - vi[1], tl.vz[s] - vi[2]};
+            const double un = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
+            const int bj = tl.b[s];
+            const double mj = (bj >= 0 ? S.body_rho[bj] : P.density[tj]) * P.V;
+            const double mij = mi * mj / (mi + mj);
+            const double kn = (4.0 / 3.0) * P.Eeff[ti][tj] * sqrt(P.Reff * ov);
+            const double cn = sqrt(mij * kn) * P.pairDamp[ti][tj];
+            const double kt = P.KtFac[ti][tj] * sqrt(P.Reff * sqrt(ov));
+            const double ct = sqrt(mij * kt) * P.pairDamp[ti][tj];
+            double f[3], ut[3];
+            const double fnm = fmin(-kn * ov + cn * un, 0.0);  // no adhesion
+            for (int k = 0; k < 3; k++) {
+                f[k] = fnm * e[k];
+                ut[k] = u[k] - un * e[k];
+            }
+            const double ctot = ct + kt * P.ddt;
+            const double aut = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
+            const double cap = P.pairFric[ti][tj] * fabs(fnm);
+            const double ft = ctot * aut > cap && aut > 0.0 ? cap / aut : ctot;
+            for (int k = 0; k < 3; k++) f[k] += ft * ut[k];
+            for (int k = 0; k < 3; k++) F[k] += f[k];
+            // offset of the contact midpoint from the particle centre: 0.5 q
+            T[0] += 0.5 * (q[1] * f[2] - q[2] * f[1]);
+            T[1] += 0.5 * (q[2] * f[0] - q[0] * f[2]);
+            T[2] += 0.5 * (q[0] * f[1] - q[1] * f[0]);
+        });
+    if (!active) return;
+    for (int k = 0; k < 3; k++) {
+        S.frc_dem[k * N + i] = F[k];
+        S.frc_dem[(3 + k) * N + i] = T[k];
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ void quat_to_R(const double *q, double R[3][3])
+{
+    const double w = q[0], x = q[1], y = q[2], z = q[3];
+    R[0][0] = 1.0 - 2.0 * (y * y + z * z);
+    R[0][1] = 2.0 * (x * y - w * z);
+    R[0][2] = 2.0 * (x * z + w * y);
+    R[1][0] = 2.0 * (x * y + w * z);
+    R[1][1] = 1.0 - 2.0 * (x * x + z * z);
+    R[1][2] = 2.0 * (y * z - w * x);
+    R[2][0] = 2.0 * (x * z - w * y);
+    R[2][1] = 2.0 * (y * z + w * x);
+    R[2][2] = 1.0 - 2.0 * (x * x + y * y);
+}
+
+// w = R I0^-1 R^T L
+__device__ __forceinline__ void omega_of(const double R[3][3], const double *Ii, const double *L, double *w)
+{
+    double a[3], b[3];
+    for (int r = 0; r < 3; r++) a[r] = R[0][r] * L[0] + R[1][r] * L[1] + R[2][r] * L[2];  // R^T L
+    for (int r = 0; r < 3; r++) b[r] = Ii[3 * r] * a[0] + Ii[3 * r + 1] * a[1] + Ii[3 * r + 2] * a[2];
+    for (int r = 0; r < 3; r++) w[r] = R[r][0] * b[0] + R[r][1] * b[1] + R[r][2] * b[2];
+}
+
+template <bool F32>
+__global__ void k_body_step(DevParams P, DevState S, DevBodies Bd)
+{
+    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (b >= Bd.B) return;
+    const int N = P.N;
+    const int m0 = Bd.ptr[b], m1 = Bd.ptr[b + 1];
+    double q[4] = {Bd.q[4 * b], Bd.q[4 * b + 1], Bd.q[4 * b + 2], Bd.q[4 * b + 3]};
+    double R[3][3];
+    quat_to_R(q, R);
+    double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
+    for (int m = m0 + lane; m < m1; m += kWarp) {
+        const int i = Bd.slot_of_row[Bd.member_row[m]];
+        double f[3];
+        if (F32) {
+            const float4 ff = S.f4[i];
+            f[0] = ff.x;
+            f[1] = ff.y;
+            f[2] = ff.z;
+        } else {
+            for (int k = 0; k < 3; k++) f[k] = S.frc[k * N + i];
+        }
+        for (int k = 0; k < 3; k++) f[k] += S.frc_dem[k * N + i];
+        const double *r0 = Bd.r0 + 3 * m;
+        double r[3];
+        for (int k = 0; k < 3; k++) r[k] = R[k][0] * r0[0] + R[k][1] * r0[1] + R[k][2] * r0[2];
+        for (int k = 0; k < 3; k++) F[k] += f[k];
+        T[0] += r[1] * f[2] - r[2] * f[1] + S.frc_dem[3 * N + i];
+        T[1] += r[2] * f[0] - r[0] * f[2] + S.frc_dem[4 * N + i];
+        T[2] += r[0] * f[1] - r[1] * f[0] + S.frc_dem[5 * N + i];
+    }
+    for (int k = 0; k < 3; k++) {
+        F[k] = warp_sum(F[k]);
+        T[k] = warp_sum(T[k]);
+    }
+    // integrate (every lane holds the same values)
+    const double dt = P.ddt, M = Bd.M[b];
+    double X[3], V[3], L[3];
+    for (int k = 0; k < 3; k++) {
+        V[k] = Bd.V[3 * b + k] + F[k] / M * dt;
+        X[k] = Bd.X[3 * b + k] + V[k] * dt;
+        L[k] = Bd.L[3 * b + k] + T[k] * dt;
+    }
+    const double *Ii = Bd.Iinv0 + 9 * b;
+    double w[3];
+    omega_of(R, Ii, L, w);
+    const double wn = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    if (wn > 0.0) {
+        const double h = 0.5 * wn * dt;
+        const double c = cos(h), sn = sin(h) / wn;
+        const double d[4] = {c, w[0] * sn, w[1] * sn, w[2] * sn};
+        const double nq[4] = {d[0] * q[0] - d[1] * q[1] - d[2] * q[2] - d[3] * q[3],
+                              d[0] * q[1] + d[1] * q[0] + d[2] * q[3] - d[3] * q[2],
+                              d[0] * q[2] - d[1] * q[3] + d[2] * q[0] + d[3] * q[1],
+                              d[0] * q[3] + d[1] * q[2] - d[2] * q[1] + d[3] * q[0]};
+        const double inv = 1.0 / sqrt(nq[0] * nq[0] + nq[1] * nq[1] + nq[2] * nq[2] + nq[3] * nq[3]);
+        for (int k = 0; k < 4; k++) q[k] = nq[k] * inv;
+    }
+    quat_to_R(q, R);
+    omega_of(R, Ii, L, w);
+    if (lane == 0) {
+        for (int k = 0; k < 3; k++) {
+            Bd.X[3 * b + k] = X[k];
+            Bd.V[3 * b + k] = V[k];
+            Bd.L[3 * b + k] = L[k];
+            Bd.Fsum[3 * b + k] = F[k];
+            Bd.Tsum[3 * b + k] = T[k];
+        }
+        for (int k = 0; k < 4; k++) Bd.q[4 * b + k] = q[k];
+    }
+    // place the members
+    for (int m = m0 + lane; m < m1; m += kWarp) {
+        const int i = Bd.slot_of_row[Bd.member_row[m]];
+        const double *r0 = Bd.r0 + 3 * m;
+        double r[3], x[3], v[3];
+        for (int k = 0; k < 3; k++) r[k] = R[k][0] * r0[0] + R[k][1] * r0[1] + R[k][2] * r0[2];
+        for (int k = 0; k < 3; k++) x[k] = X[k] + r[k];
+        v[0] = V[0] + w[1] * r[2] - w[2] * r[1];
+        v[1] = V[1] + w[2] * r[0] - w[0] * r[2];
+        v[2] = V[2] + w[0] * r[1] - w[1] * r[0];
+        if (F32) {
+            float4 p = S.p4[i];
+            const unsigned pw = __float_as_uint(p.w);
+            const int c[3] = {unpack_cx(pw), unpack_cy(pw), unpack_cz(pw)};
+            float rr[3];
+            for (int k = 0; k < 3; k++) {
+                double a = x[k] - (P.dmin[k] + c[k] * P.cw[k]);
+                a -= P.W[k] * rint(a / P.W[k]);
+                rr[k] = (float)a;
+            }
+            S.p4[i] = make_float4(rr[0], rr[1], rr[2], p.w);
+            S.v4[i] = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
+        } else {
+            for (int k = 0; k < 3; k++) {
+                const double t = x[k] - P.dmin[k];
+                S.pos[k * N + i] = (t - P.W[k] * floor(t / P.W[k])) + P.dmin[k];
+                S.vel[k * N + i] = v[k];
+            }
+        }
+    }
+}
+
+void launch_slot_of_row(const DevParams &P, const int *pidx, int *slot_of_row, cudaStream_t st)
+{
+    k_slot_of_row<<<(P.N + 255) / 256, 256, 0, st>>>(P.N, pidx, slot_of_row);
+}
+
+// Both precisions run the clump contacts and the body update in FP64 on the
+// FP64 state of solids and walls (in the FP32 split mode these planes are the
+// solids' and walls' master copies, refreshed into the FP32 arrays after the
+// substeps), so the template's FP32 branches are not instantiated.
+void launch_clump_dem(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st)
+{
+    if (ce <= cb) return;
+    k_clump_dem<false><<<(ce - cb + 3) / 4, 4 * kWarp, 0, st>>>(P, S, cb, ce);
+}
+
+void launch_body_step(const DevParams &P, const DevState &S, const DevBodies &Bd, bool f32, cudaStream_t st)
+{
+    (void)f32;
+    if (Bd.B <= 0) return;
+    const int threads = 128;
+    const int blocks = (Bd.B * kWarp + threads - 1) / threads;
+    k_body_step<false><<<blocks, threads, 0, st>>>(P, S, Bd);
+}
+
+}  // namespace dmph

@@ -64,6 +64,9 @@ struct DevParams {
     double logE[kTypes];              // log(RestitutionCoefficient)
     double cnDen[kTypes];             // sqrt(pi^2 + log(e)^2)
     double ctFac[kTypes];             // -2 log(e) / sqrt(pi^2 + log(e)^2)
+    // pair-symmetric contact constants of the rigid-clump mode
+    double pairDamp[kTypes][kTypes];  // -2 log(e_ij) / sqrt(pi^2 + log(e_ij)^2), e_ij = (e_i + e_j)/2
+    double pairFric[kTypes][kTypes];  // (mu_i + mu_j)/2
 };
 
 struct Chunk {

@@ -87,8 +87,14 @@ __global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm,
                 p.y = (float)(x[1] - o[1]);
                 p.z = (float)(x[2] - o[2]);
                 v = make_float4((float)vv[0], (float)vv[1], (float)vv[2], 0.f);
+                for (int d = 0; d < 3; d++) {
+                    const double t0 = x[d] - P.dmin[d];
+                    S.pos[d * N + i] = (t0 - P.W[d] * floor(t0 / P.W[d])) + P.dmin[d];
+                    S.vel[d * N + i] = vv[d];
+                }
             } else {
                 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                for (int d = 0; d < 3; d++) S.vel[d * N + i] = 0.0;
             }
         }
         S.p4[i] = p;
@@ -213,7 +219,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_b32(DevParams
     const bool sol = is_solid(ti);
     const float Pi = S.pres32[ii];
     const float mui = Q.svisc[ti];
-    const float rhoi = Q.density[ti];
+    const float rhoi = (float)particle_density(S, P, ii, ti);
     const bool st = P.surface_tension;
     float4 gi = make_float4(0.f, 0.f, 0.f, 0.f);
     if (st) {
@@ -318,7 +324,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_b32(DevParams
             }
         });
     if (!active) return;
-    const float m = Q.mass[ti];
+    const float m = sol ? rhoi * Q.V : Q.mass[ti];
     float4 F;
     if (sol) {
         F.x = 2.f * fD.x + fS.x + fV.x - fB.x + m * Q.g[0];
@@ -348,128 +354,11 @@ __global__ void k_fluid_accel32(DevParams32 Q, DevState S, int b, int e)
     S.v4[i] = v;
 }
 
-// ---------------------------------------------------------------- DEM
-__global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_dem_force32(DevParams P, DevParams32 Q, DevState S,
-                                                                          int chunk_begin, int chunk_end, int forces)
-{
-    __shared__ Tile32 tiles[kWarpsPerBlock32];
-    Tile32 &tl = tiles[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    const int cidx = chunk_begin + blockIdx.x * kWarpsPerBlock32 + (threadIdx.x >> 5);
-    if (cidx >= chunk_end) return;
-    const Chunk ch = S.chunks[cidx];
-    const int i = ch.i0 + lane;
-    const bool active = lane < ch.cnt;
-    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-    int cix, ciy, ciz;
-    chunk_cell(P, key_cell, cix, ciy, ciz);
-    const int ii = active ? i : ch.i0;
-    const float4 pi = S.p4[ii];
-    const float4 vi = S.v4[ii];
-    const int ti = unpack_type(__float_as_uint(pi.w));
-    auto stage = [&](int j, int slot) { stage32(P, Q, S, tl, j, slot, cix, ciy, ciz, false); };
-    int tlast = -1;
-    float r2last = 0.f;
-    traverse_stencil(P, S.cell_start, key_cell, lane, active, 7u, stage, [&](int j, int s) {
-        if (j == i) return;
-        const float4 pj = tl.p[s];
-        const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-        const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
-        if (r2 <= Q.dx2) {
-            tlast = __float_as_int(pj.w);
-            r2last = r2;
-        }
-    });
-    float kn = 0.f, cn = 0.f, kt = 0.f, ct = 0.f;
-    if (active) {
-        if (tlast >= 0) {
-            const float ov = fmaxf(0.f, Q.dx - sqrtf(r2last));
-            kn = (4.f / 3.f) * Q.Eeff[ti][tlast] * sqrtf(Q.Reff * ov);
-            const float mi = Q.mass[ti], mj = Q.mass[tlast];
-            const float mij = mi * mj / (mi + mj);
-            cn = -2.f * sqrtf(mij * kn) * Q.logE[ti] / Q.cnDen[ti];
-            kt = Q.KtFac[ti][tlast] * sqrtf(Q.Reff * sqrtf(ov));
-            ct = Q.ctFac[ti] * sqrtf(mij * kt);
-            S.kn32[i] = kn;
-            S.cn32[i] = cn;
-            S.kt32[i] = kt;
-            S.ct32[i] = ct;
-        } else {
-            kn = S.kn32[i];
-            cn = S.cn32[i];
-            kt = S.kt32[i];
-            ct = S.ct32[i];
-        }
-    }
-    if (!forces) return;
-    float3 fN = make_float3(0.f, 0.f, 0.f), fT = fN;
-    const float muf = Q.friction[ti];
-    traverse_stencil(P, S.cell_start, key_cell, lane, active, 6u, stage, [&](int j, int s) {
-        if (j == i) return;
-        const float4 pj = tl.p[s];
-        const float q[3] = {pj.x - pi.x, pj.y - pi.y, pj.z - pi.z};
-        const float r2 = fmaf(q[0], q[0], fmaf(q[1], q[1], q[2] * q[2]));
-        if (r2 > Q.dx2) return;
-        const float r = sqrtf(r2);
-        const float e[3] = {q[0] / r, q[1] / r, q[2] / r};
-        const float4 vj = tl.v[s];
-        const float u[3] = {vj.x - vi.x, vj.y - vi.y, vj.z - vi.z};
-        float vn[3], vt[3], dtv[3], sN[3], sT[3];
-        for (int d = 0; d < 3; d++) vn[d] = u[d] * e[d];  // component-wise, as the reference (:2648)
-        for (int d = 0; d < 3; d++) vt[d] = u[d] - vn[d] * e[d];
-        for (int d = 0; d < 3; d++) dtv[d] = vt[d] * Q.ddt;
-        for (int d = 0; d < 3; d++) sN[d] = -kn * (Q.dx - r) * e[d] - (cn * vn[d] * e[d] * Q.dt);
-        const float aFn = muf * sqrtf(sN[0] * sN[0] + sN[1] * sN[1] + sN[2] * sN[2]);
-        for (int d = 0; d < 3; d++) sT[d] = -kt * dtv[d] - (ct * vt[d]);
-        const float aFt = sqrtf(sT[0] * sT[0] + sT[1] * sT[1] + sT[2] * sT[2]);
-        fN.x += sN[0];
-        fN.y += sN[1];
-        fN.z += sN[2];
-        if (aFn > aFt) {
-            fT.x += sT[0];
-            fT.y += sT[1];
-            fT.z += sT[2];
-        } else {
-            const float avt = sqrtf(vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]);
-            if (avt != 0.f) {
-                const float c = aFn / avt;
-                fT.x += c * vt[0];
-                fT.y += c * vt[1];
-                fT.z += c * vt[2];
-            }
-        }
-    });
-    if (!active) return;
-    float4 F = S.f4[i];
-    F.x += fN.x + fT.x;
-    F.y += fN.y + fT.y;
-    F.z += fN.z + fT.z;
-    S.f4[i] = F;
-}
-
-__global__ void k_dem_integrate32(DevParams32 Q, DevState S, int b, int e)
-{
-    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= e) return;
-    float4 p = S.p4[i];
-    float4 v = S.v4[i];
-    const float4 f = S.f4[i];
-    const float k = Q.ddt / Q.mass[unpack_type(__float_as_uint(p.w))];
-    v.x = fmaf(f.x, k, v.x);
-    v.y = fmaf(f.y, k, v.y);
-    v.z = fmaf(f.z, k, v.z);
-    p.x = fmaf(v.x, Q.ddt, p.x);
-    p.y = fmaf(v.y, Q.ddt, p.y);
-    p.z = fmaf(v.z, Q.ddt, p.z);
-    S.v4[i] = v;
-    S.p4[i] = p;
-}
-
 // ------------------------------------------------------- layout conversion
 // FP32 split state -> FP64 absolute positions (wrapped into the periodic
 // domain like calculatePeriodicBoundary :3153) and velocities, into the FP64
 // planes; used by the rebuild (cell keys) and by the state getters.
-__global__ void k_export32(DevParams P, DevState S, double *pos, double *vel)
+__global__ void k_export32(DevParams P, DevState S, double *pos, double *vel, int fluid_only)
 {
     const int N = P.N;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -477,6 +366,8 @@ __global__ void k_export32(DevParams P, DevState S, double *pos, double *vel)
     const float4 p = S.p4[i];
     const float4 v = S.v4[i];
     const unsigned w = __float_as_uint(p.w);
+    // solids and walls keep their FP64 master state in the planes
+    if (fluid_only && !is_fluid(unpack_type(w))) return;
     const int c[3] = {unpack_cx(w), unpack_cy(w), unpack_cz(w)};
     const float pr[3] = {p.x, p.y, p.z};
     const float vr[3] = {v.x, v.y, v.z};
@@ -494,7 +385,8 @@ __global__ void k_permute32(DevParams P, const unsigned long long *__restrict__ 
                             const float4 *__restrict__ v_in, const int *__restrict__ type_in,
                             const int *__restrict__ pidx_in, float4 *__restrict__ p_out, float4 *__restrict__ v_out,
                             int *__restrict__ type_out, int *__restrict__ pidx_out, double *__restrict__ xref,
-                            float4 *__restrict__ xref4)
+                            float4 *__restrict__ xref4, const int *__restrict__ bid_in, int *__restrict__ bid_out,
+                            const double *__restrict__ vabs, double *__restrict__ pos_out, double *__restrict__ vel_out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int N = P.N;
@@ -511,6 +403,8 @@ __global__ void k_permute32(DevParams P, const unsigned long long *__restrict__ 
     for (int d = 0; d < 3; d++) {
         const double x = xabs[d * N + src];
         xref[d * N + i] = x;
+        pos_out[d * N + i] = x;
+        vel_out[d * N + i] = vabs[d * N + src];
         r[d] = (float)(x - (P.dmin[d] + c[d] * P.cw[d]));
     }
     const float4 p = make_float4(r[0], r[1], r[2], __uint_as_float(pack_cell(t, c[0], c[1], c[2])));
@@ -519,6 +413,7 @@ __global__ void k_permute32(DevParams P, const unsigned long long *__restrict__ 
     v_out[i] = v_in[src];
     type_out[i] = t;
     pidx_out[i] = pidx_in[src];
+    if (bid_in) bid_out[i] = bid_in[src];
 }
 
 // FP64 planes -> FP32 split state in the current cells (dmph_set_state, create)
@@ -541,20 +436,60 @@ __global__ void k_import32(DevParams P, DevState S, const double *pos, const dou
     if (vel) S.v4[i] = make_float4((float)vel[i], (float)vel[N + i], (float)vel[2 * N + i], 0.f);
 }
 
+// FP32 mode: the DEM and the rigid bodies run in FP64 on the solids' FP64
+// master state (the planes S.pos/S.vel), so contacts see exact lattice
+// spacings.  Before the substeps, the solids' FP32 fluid forces seed the FP64
+// force planes; after them, the FP32 positions and velocities of the solids
+// are refreshed from the masters.
+__global__ void k_solid_force_to64(DevParams P, DevState S, int b, int e)
+{
+    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= e) return;
+    const float4 f = S.f4[i];
+    S.frc[i] = f.x;
+    S.frc[P.N + i] = f.y;
+    S.frc[2 * P.N + i] = f.z;
+}
+__global__ void k_sync_solids32(DevParams P, DevState S, int b, int e)
+{
+    const int N = P.N;
+    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= e) return;
+    const float4 p = S.p4[i];
+    const unsigned w = __float_as_uint(p.w);
+    const int c[3] = {unpack_cx(w), unpack_cy(w), unpack_cz(w)};
+    float r[3];
+    for (int d = 0; d < 3; d++) {
+        double a = S.pos[d * N + i] - (P.dmin[d] + c[d] * P.cw[d]);
+        a -= P.W[d] * rint(a / P.W[d]);
+        r[d] = (float)a;
+    }
+    S.p4[i] = make_float4(r[0], r[1], r[2], p.w);
+    S.v4[i] = make_float4((float)S.vel[i], (float)S.vel[N + i], (float)S.vel[2 * N + i], 0.f);
+}
+void launch_solid_force_to64(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st)
+{
+    if (e > b) k_solid_force_to64<<<(e - b + 255) / 256, 256, 0, st>>>(P, S, b, e);
+}
+void launch_sync_solids32(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st)
+{
+    if (e > b) k_sync_solids32<<<(e - b + 255) / 256, 256, 0, st>>>(P, S, b, e);
+}
+
 // widen an FP32 field to FP64 (getters)
 __global__ void k_widen_f(const float *in, double *out, int n)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = (double)in[i];
 }
-__global__ void k_widen_f4(const float4 *in, double *out, int n)
+__global__ void k_widen_f4(const float4 *in, double *out, int count, int stride)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= count) return;
     const float4 v = in[i];
     out[i] = v.x;
-    out[n + i] = v.y;
-    out[2 * n + i] = v.z;
+    out[stride + i] = v.y;
+    out[2 * stride + i] = v.z;
 }
 
 // ---------------------------------------------------------------- host side
@@ -634,18 +569,9 @@ void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, int b, int e,
 {
     if (e > b) k_fluid_accel32<<<(e - b + 255) / 256, 256, 0, st>>>(Q, S, b, e);
 }
-void launch_dem_force32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, int forces,
-                        cudaStream_t st)
-{
-    if (ce > cb) k_dem_force32<<<blocks32(cb, ce), kWarpsPerBlock32 * kWarp, 0, st>>>(P, Q, S, cb, ce, forces);
-}
-void launch_dem_integrate32(const DevParams32 &Q, const DevState &S, int b, int e, cudaStream_t st)
-{
-    if (e > b) k_dem_integrate32<<<(e - b + 127) / 128, 128, 0, st>>>(Q, S, b, e);
-}
 void launch_export32(const DevParams &P, const DevState &S, double *pos, double *vel, cudaStream_t st)
 {
-    k_export32<<<(P.N + 255) / 256, 256, 0, st>>>(P, S, pos, vel);
+    k_export32<<<(P.N + 255) / 256, 256, 0, st>>>(P, S, pos, vel, 1);
 }
 void launch_import32(const DevParams &P, const DevState &S, const double *pos, const double *vel, cudaStream_t st)
 {
@@ -653,18 +579,19 @@ void launch_import32(const DevParams &P, const DevState &S, const double *pos, c
 }
 void launch_permute32(const DevParams &P, const unsigned long long *words, const double *xabs, const float4 *v_in,
                       const int *type_in, const int *pidx_in, float4 *p_out, float4 *v_out, int *type_out,
-                      int *pidx_out, double *xref, float4 *xref4, cudaStream_t st)
+                      int *pidx_out, double *xref, float4 *xref4, const int *bid_in, int *bid_out, const double *vabs,
+                      double *pos_out, double *vel_out, cudaStream_t st)
 {
     k_permute32<<<(P.N + 255) / 256, 256, 0, st>>>(P, words, xabs, v_in, type_in, pidx_in, p_out, v_out, type_out,
-                                                   pidx_out, xref, xref4);
+                                                   pidx_out, xref, xref4, bid_in, bid_out, vabs, pos_out, vel_out);
 }
 void launch_widen_f(const float *in, double *out, int n, cudaStream_t st)
 {
     if (n > 0) k_widen_f<<<(n + 255) / 256, 256, 0, st>>>(in, out, n);
 }
-void launch_widen_f4(const float4 *in, double *out, int n, cudaStream_t st)
+void launch_widen_f4(const float4 *in, double *out, int count, int stride, cudaStream_t st)
 {
-    if (n > 0) k_widen_f4<<<(n + 255) / 256, 256, 0, st>>>(in, out, n);
+    if (count > 0) k_widen_f4<<<(count + 255) / 256, 256, 0, st>>>(in, out, count, stride);
 }
 
 }  // namespace dmph

@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, 
         gci2 = S.gc[2 * N + ii];
     }
     const double mui = P.svisc[ti];
-    const double rhoi = P.density[ti];
+    const double rhoi = particle_density(S, P, ii, ti);
     double alpha = 0.0;
     if (sol) {
         const int nci = S.nc[ii];
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, 
         });
     if (!active) return;
     double F[3] = {0.0, 0.0, 0.0};
-    const double m = P.mass[ti];
+    const double m = sol ? rhoi * P.V : P.mass[ti];
     if (sol) {
         for (int d = 0; d < 3; d++) F[d] += fD[d];
         if (st)
@@ -372,6 +372,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, 
 // calculateNormalDirectionForce :2560 and calculateTangentialDirectionForce
 // :2614 add their sums to Force in that order.  calculateInertialTensor and
 // calculateTorque only feed arrays nothing reads and are not run.
+// MIXED: FP32 split mode, where solids and walls keep FP64 master positions in
+// S.pos/S.vel but fluid particles live in the FP32 arrays p4/v4.
+template <bool MIXED>
 __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_dem_force(DevParams P, DevState S, int chunk_begin,
                                                                       int chunk_end, int forces)
 {
@@ -390,13 +393,26 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_dem_force(DevParams 
     const double xi = S.pos[ii], yi = S.pos[N + ii], zi = S.pos[2 * N + ii];
     const double vxi = S.vel[ii], vyi = S.vel[N + ii], vzi = S.vel[2 * N + ii];
     auto stage = [&](int j, int slot) {
-        tl.x[slot] = S.pos[j];
-        tl.y[slot] = S.pos[N + j];
-        tl.z[slot] = S.pos[2 * N + j];
-        tl.vx[slot] = S.vel[j];
-        tl.vy[slot] = S.vel[N + j];
-        tl.vz[slot] = S.vel[2 * N + j];
-        tl.t[slot] = S.type[j];
+        const int t = S.type[j];
+        if (MIXED && is_fluid(t)) {
+            const float4 p = S.p4[j];
+            const float4 v = S.v4[j];
+            const unsigned w = __float_as_uint(p.w);
+            tl.x[slot] = P.dmin[0] + unpack_cx(w) * P.cw[0] + (double)p.x;
+            tl.y[slot] = P.dmin[1] + unpack_cy(w) * P.cw[1] + (double)p.y;
+            tl.z[slot] = P.dmin[2] + unpack_cz(w) * P.cw[2] + (double)p.z;
+            tl.vx[slot] = v.x;
+            tl.vy[slot] = v.y;
+            tl.vz[slot] = v.z;
+        } else {
+            tl.x[slot] = S.pos[j];
+            tl.y[slot] = S.pos[N + j];
+            tl.z[slot] = S.pos[2 * N + j];
+            tl.vx[slot] = S.vel[j];
+            tl.vy[slot] = S.vel[N + j];
+            tl.vz[slot] = S.vel[2 * N + j];
+        }
+        tl.t[slot] = t;
     };
     // 1) last neighbour within dx
     int tlast = -1;
@@ -604,9 +620,13 @@ void launch_pass_b(const DevParams &P, const DevState &S, int cb, int ce, cudaSt
 {
     if (ce > cb) k_pass_b<<<chunk_blocks(cb, ce), kWarpsPerBlock * kWarp, 0, st>>>(P, S, cb, ce);
 }
-void launch_dem_force(const DevParams &P, const DevState &S, int cb, int ce, int forces, cudaStream_t st)
+void launch_dem_force(const DevParams &P, const DevState &S, int cb, int ce, int forces, cudaStream_t st, bool mixed)
 {
-    if (ce > cb) k_dem_force<<<chunk_blocks(cb, ce), kWarpsPerBlock * kWarp, 0, st>>>(P, S, cb, ce, forces);
+    if (ce <= cb) return;
+    if (mixed)
+        k_dem_force<true><<<chunk_blocks(cb, ce), kWarpsPerBlock * kWarp, 0, st>>>(P, S, cb, ce, forces);
+    else
+        k_dem_force<false><<<chunk_blocks(cb, ce), kWarpsPerBlock * kWarp, 0, st>>>(P, S, cb, ce, forces);
 }
 void launch_fluid_accel(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st)
 {

@@ -15,7 +15,7 @@ void launch_bitonic(unsigned long long *words, int n, int nlog, cudaStream_t st)
 void launch_cell_start(const DevParams &P, const unsigned long long *words, int *start, cudaStream_t st);
 void launch_permute(const DevParams &P, const unsigned long long *words, const double *pos_in, const double *vel_in,
                     const int *type_in, const int *pidx_in, double *pos_out, double *vel_out, int *type_out,
-                    int *pidx_out, double *xref, cudaStream_t st);
+                    int *pidx_out, double *xref, const int *bid_in, int *bid_out, cudaStream_t st);
 template <class T>
 int launch_exclusive_scan(const T *in, T *out, int n, T *block_sums, T *total, cudaStream_t st);
 void launch_chunks(const DevParams &P, const unsigned long long *words, const int *start, int *flag, int *offs,
@@ -28,7 +28,8 @@ void launch_drift(const DevParams &P, const DevState &S, const WallMotion &Wm, u
 void launch_pass_a(const DevParams &P, const DevState &S, int cb, int ce, int init_only, cudaStream_t st);
 void launch_pass_b(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st);
 void launch_fluid_accel(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st);
-void launch_dem_force(const DevParams &P, const DevState &S, int cb, int ce, int forces, cudaStream_t st);
+void launch_dem_force(const DevParams &P, const DevState &S, int cb, int ce, int forces, cudaStream_t st,
+                      bool mixed = false);
 void launch_dem_integrate(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st);
 void launch_counts(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st);
 void launch_neighbor_fill(const DevParams &P, const DevState &S, int cb, int ce, const long long *ptr, int *ind,
@@ -41,15 +42,20 @@ void launch_drift32(const DevParams &P, const DevParams32 &Q, const DevState &S,
 void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, cudaStream_t st);
 void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, cudaStream_t st);
 void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, int b, int e, cudaStream_t st);
-void launch_dem_force32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, int forces,
-                        cudaStream_t st);
-void launch_dem_integrate32(const DevParams32 &Q, const DevState &S, int b, int e, cudaStream_t st);
 void launch_export32(const DevParams &P, const DevState &S, double *pos, double *vel, cudaStream_t st);
 void launch_import32(const DevParams &P, const DevState &S, const double *pos, const double *vel, cudaStream_t st);
 void launch_permute32(const DevParams &P, const unsigned long long *words, const double *xabs, const float4 *v_in,
                       const int *type_in, const int *pidx_in, float4 *p_out, float4 *v_out, int *type_out,
-                      int *pidx_out, double *xref, float4 *xref4, cudaStream_t st);
+                      int *pidx_out, double *xref, float4 *xref4, const int *bid_in, int *bid_out, const double *vabs,
+                      double *pos_out, double *vel_out, cudaStream_t st);
+void launch_solid_force_to64(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st);
+void launch_sync_solids32(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st);
 void launch_widen_f(const float *in, double *out, int n, cudaStream_t st);
-void launch_widen_f4(const float4 *in, double *out, int n, cudaStream_t st);
+void launch_widen_f4(const float4 *in, double *out, int count, int stride, cudaStream_t st);
+
+// dmph_bodies.cu
+void launch_slot_of_row(const DevParams &P, const int *pidx, int *slot_of_row, cudaStream_t st);
+void launch_clump_dem(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st);
+void launch_body_step(const DevParams &P, const DevState &S, const DevBodies &Bd, bool f32, cudaStream_t st);
 
 }  // namespace dmph

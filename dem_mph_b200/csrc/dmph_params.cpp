@@ -118,6 +118,10 @@ int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, std
             const double pi_ = p.poisson_ratio[ti], pj = p.poisson_ratio[tj];
             P.Eeff[ti][tj] = (yi * yj) / ((1 - pi_ * pi_) * yj + (1 - pj * pj) * yi);
             P.KtFac[ti][tj] = 8.0 * yi * yj / (((1 + pi_) * (2 - pi_) * yj) + ((1 + pj) * (2 - pj) * yi));
+            const double eij = 0.5 * (p.restitution_coefficient[ti] + p.restitution_coefficient[tj]);
+            const double lij = eij > 0.0 ? std::log(eij) : 0.0;
+            P.pairDamp[ti][tj] = eij > 0.0 ? -2.0 * lij / std::sqrt(M_PI * M_PI + lij * lij) : 0.0;
+            P.pairFric[ti][tj] = 0.5 * (p.viscous_friction_coefficient[ti] + p.viscous_friction_coefficient[tj]);
         }
     }
     P.Reff = dx * dx / (dx + dx);

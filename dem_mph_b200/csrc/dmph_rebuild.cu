@@ -112,7 +112,8 @@ __global__ void k_cell_start(DevParams P, const unsigned long long *__restrict__
 __global__ void k_permute(DevParams P, const unsigned long long *__restrict__ words, const double *__restrict__ pos_in,
                           const double *__restrict__ vel_in, const int *__restrict__ type_in,
                           const int *__restrict__ pidx_in, double *__restrict__ pos_out, double *__restrict__ vel_out,
-                          int *__restrict__ type_out, int *__restrict__ pidx_out, double *__restrict__ xref)
+                          int *__restrict__ type_out, int *__restrict__ pidx_out, double *__restrict__ xref,
+                          const int *__restrict__ bid_in, int *__restrict__ bid_out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int N = P.N;
@@ -126,6 +127,7 @@ __global__ void k_permute(DevParams P, const unsigned long long *__restrict__ wo
     }
     type_out[i] = type_in[src];
     pidx_out[i] = pidx_in[src];
+    if (bid_in) bid_out[i] = bid_in[src];
 }
 
 // chunk heads: a slot starts a chunk when it starts its key's range or is a
@@ -265,10 +267,10 @@ void launch_cell_start(const DevParams &P, const unsigned long long *words, int 
 
 void launch_permute(const DevParams &P, const unsigned long long *words, const double *pos_in, const double *vel_in,
                     const int *type_in, const int *pidx_in, double *pos_out, double *vel_out, int *type_out,
-                    int *pidx_out, double *xref, cudaStream_t st)
+                    int *pidx_out, double *xref, const int *bid_in, int *bid_out, cudaStream_t st)
 {
     k_permute<<<(P.N + 255) / 256, 256, 0, st>>>(P, words, pos_in, vel_in, type_in, pidx_in, pos_out, vel_out,
-                                                 type_out, pidx_out, xref);
+                                                 type_out, pidx_out, xref, bid_in, bid_out);
 }
 
 template <class T>

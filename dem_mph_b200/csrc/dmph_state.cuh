@@ -26,7 +26,39 @@ struct DevState {
     // of one cell with FP32 magnitudes of a few particle spacings
     float4 *p4, *v4, *f4, *xref4, *gc4;
     float *pres32, *vsp32, *div32, *densA32, *pA32;
-    float *kn32, *cn32, *kt32, *ct32, *alpha32, *dragC32;
+    float *alpha32, *dragC32;
+    // rigid clumps (DMPH_FLAG_RIGID_CLUMPS): body of each slot (-1: none) and
+    // the density of each body; null when the mode is off
+    int *bid;
+    const double *body_rho;
+    double *frc_dem;  // FP64 planes: DEM contact force of the current substep (clump mode)
+};
+
+// per-particle density: a debris body's own density when the particle belongs
+// to one, else the density of its type
+__device__ __forceinline__ double particle_density(const DevState &S, const DevParams &P, int i, int t)
+{
+    if (S.bid) {
+        const int b = S.bid[i];
+        if (b >= 0) return S.body_rho[b];
+    }
+    return P.density[t];
+}
+
+// Rigid debris bodies, FP64 (no counterpart in the reference).  Members are
+// stored in body order (CSR over bodies) by their input row; slot_of_row maps
+// a row to its current sorted slot and is refreshed at every rebuild.
+struct DevBodies {
+    int B;
+    const int *ptr;         // B+1
+    const int *member_row;  // members, by body
+    int *slot_of_row;       // N
+    const double *r0;       // 3 per member: offset from the centre of mass, body frame
+    double *X, *V, *L;      // 3 per body: centre of mass, velocity, angular momentum (world)
+    double *q;              // 4 per body: orientation (w, x, y, z), body -> world
+    const double *M;        // mass
+    const double *Iinv0;    // 9 per body: inverse inertia tensor, body frame
+    double *Fsum, *Tsum;    // 3 per body: last substep's total force and torque (diagnostics)
 };
 
 // .w of the FP32 position: type (3 bits) | cx (10) | cy (10) | cz (9)

@@ -1,0 +1,142 @@
+// dem_mph — drop-in replacement of the reference solver executable.
+//
+//   dem_mph [--dim 2|3] [--fp32] [--gpu N] data grid prof_pattern vtk_pattern log
+//
+// Same positional arguments, defaults and output cadence as the reference's
+// main (source/DEM-MPH.cpp:350-617): it reads dem.data and the .grid file,
+// writes a .prof (positions and velocities in the solver's sorted order) at
+// the top of every step whose time reaches the next OutputInterval boundary
+// and advances until EndTime.  All computation happens in libdmph.so through
+// the C ABI of include/dmph.h.  The reference is compiled 2D by default
+// (source/DEM-MPH.cpp:39); --dim 3 selects its 3D branches.  The reference
+// also writes a sixth argument-free VTK output; this build's VTK writer is not
+// implemented, and a non-default VTK pattern is reported and ignored.
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime_api.h>
+
+#include "dmph.h"
+
+static FILE *g_log = nullptr;
+
+static void log_printf(const char *fmt, ...)
+{
+    va_list a, b;
+    va_start(a, fmt);
+    va_copy(b, a);
+    if (g_log) vfprintf(g_log, fmt, a);
+    vfprintf(stderr, fmt, b);
+    va_end(a);
+    va_end(b);
+}
+
+static int fail(const char *what, int rc, dmph_ctx *ctx)
+{
+    log_printf("%s failed (%d): %s\n", what, rc, dmph_last_error(ctx));
+    return 1;
+}
+
+int main(int argc, char **argv)
+{
+    // defaults of the reference (:54-58)
+    std::string logf = "sample.log", dataf = "sample.data", gridf = "sample.grid", proff = "sample%03d.prof",
+                vtkf = "sample%03d.vtk";
+    int dim = 2, fp32 = 0, gpu = 0;
+    std::vector<std::string> pos;
+    for (int a = 1; a < argc; a++) {
+        if (!std::strcmp(argv[a], "--dim") && a + 1 < argc)
+            dim = std::atoi(argv[++a]);
+        else if (!std::strcmp(argv[a], "--fp32"))
+            fp32 = 1;
+        else if (!std::strcmp(argv[a], "--gpu") && a + 1 < argc)
+            gpu = std::atoi(argv[++a]);
+        else
+            pos.push_back(argv[a]);
+    }
+    if (pos.size() > 0) dataf = pos[0];
+    if (pos.size() > 1) gridf = pos[1];
+    if (pos.size() > 2) proff = pos[2];
+    if (pos.size() > 3) vtkf = pos[3];
+    if (pos.size() > 4) logf = pos[4];
+    g_log = std::fopen(logf.c_str(), "w");
+    if (!g_log) std::fprintf(stderr, "error in open %s\n", logf.c_str());
+    {
+        time_t t = time(NULL);
+        log_printf("start reading files at %s\n", ctime(&t));
+    }
+    dmph_params p;
+    dmph_params_default(&p);
+    int rc = dmph_read_data_file(dataf.c_str(), &p);
+    if (rc) return log_printf("cannot read %s: %s\n", dataf.c_str(), dmph_io_last_message()), 1;
+    if (*dmph_io_last_message()) log_printf("%s", dmph_io_last_message());
+    int n = 0;
+    rc = dmph_read_grid_file(gridf.c_str(), &p, &n, nullptr, nullptr, nullptr);
+    if (rc) return log_printf("cannot read %s: %s\n", gridf.c_str(), dmph_io_last_message()), 1;
+    std::vector<int> type(n);
+    std::vector<double> x(3 * (size_t)n), v(3 * (size_t)n);
+    rc = dmph_read_grid_file(gridf.c_str(), &p, &n, type.data(), x.data(), v.data());
+    if (rc) return log_printf("cannot read %s: %s\n", gridf.c_str(), dmph_io_last_message()), 1;
+    p.dim = dim;
+    p.precision = fp32 ? DMPH_PRECISION_FP32_SPLIT : DMPH_PRECISION_FP64;
+    p.flags |= DMPH_FLAG_ALL_NEIGHBOR_COUNTS;
+    if (cudaSetDevice(gpu) != cudaSuccess) return log_printf("cannot select GPU %d\n", gpu), 1;
+    {
+        time_t t = time(NULL);
+        log_printf("start initialization at %s\n", ctime(&t));
+    }
+    dmph_ctx *ctx = nullptr;
+    rc = dmph_create(&p, n, type.data(), x.data(), v.data(), &ctx);
+    if (rc) return fail("dmph_create", rc, nullptr);
+    dmph_info info;
+    dmph_get_info(ctx, &info);
+    log_printf("N0a = %e\nN0p = %e\n", info.n0a, info.n0p);
+    log_printf("CellCount[DIM]: %d %d %d\nTotalCellCount: %d\n", info.cell_count[0], info.cell_count[1],
+               info.cell_count[2], info.total_cell_count);
+    log_printf("CellWidth[DIM]: %e %e %e\n", info.cell_width[0], info.cell_width[1], info.cell_width[2]);
+    log_printf("Using GPU %d (%s)\n", gpu, dmph_version());
+    if (vtkf != "sample%03d.vtk") log_printf("VTK output (%s) is not produced by this build\n", vtkf.c_str());
+
+    double Time = p.time, OutputNext = 0.0;
+    const double Dt = p.dt;
+    int iStep = (int)(Time / Dt);
+    {
+        time_t t = time(NULL);
+        log_printf("start main roop at %s\n", ctime(&t));
+    }
+    const clock_t c0 = clock();
+    while (Time < p.end_time + 1.0e-5 * Dt) {
+        if (Time + 1.0e-5 * Dt >= OutputNext) {
+            char fn[1024];
+            std::snprintf(fn, sizeof(fn), proff.c_str(), iStep);
+            dmph_params hp = p;
+            hp.time = Time;
+            rc = dmph_get_state(ctx, type.data(), x.data(), v.data(), nullptr);
+            if (rc) return fail("dmph_get_state", rc, ctx);
+            rc = dmph_write_prof_file(fn, &hp, n, type.data(), x.data(), v.data());
+            if (rc) return log_printf("cannot write %s\n", fn), 1;
+            log_printf("@ Prof Output Time : %e\n", Time);
+            OutputNext += p.output_interval;
+        }
+        rc = dmph_step(ctx, 1);
+        if (rc) return fail("dmph_step", rc, ctx);
+        Time += Dt;
+        iStep++;
+    }
+    const clock_t c1 = clock();
+    dmph_get_info(ctx, &info);
+    {
+        time_t t = time(NULL);
+        log_printf("end main roop at %s\n", ctime(&t));
+    }
+    log_printf("steps %lld, rebuilds %lld\n", (long long)info.steps, (long long)info.rebuilds);
+    log_printf("total:                   %lf [CPU sec]\n", (double)(c1 - c0) / CLOCKS_PER_SEC);
+    dmph_destroy(ctx);
+    if (g_log) std::fclose(g_log);
+    return 0;
+}

@@ -39,6 +39,8 @@ def lib():
         L.dmph_get_field.argtypes = [vp, C.c_int, vp]
         L.dmph_get_info.argtypes = [vp, vp]
         L.dmph_get_neighbor_list.argtypes = [vp, vp, vp, C.c_int64]
+        L.dmph_set_bodies.argtypes = [vp, C.c_int, vp, vp]
+        L.dmph_get_bodies.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
         L.dmph_set_profiling.argtypes = [vp, C.c_int]
         L.dmph_get_phase_times.argtypes = [vp, vp, vp, C.c_int]
         L.dmph_destroy.argtypes = [vp]
@@ -118,6 +120,24 @@ class Solver:
         ind = np.empty(max(int(ptr[-1]), 1), np.int32)
         self._check(lib().dmph_get_neighbor_list(self._h, _ptr(ptr), _ptr(ind), int(ptr[-1])))
         return ptr, ind[:int(ptr[-1])]
+
+    def set_bodies(self, body_of_row, body_density):
+        """Make debris bodies rigid (see dmph_set_bodies): body_of_row[r] is the
+        body of input row r (-1 none), body_density[b] its density."""
+        b = np.ascontiguousarray(body_of_row, dtype=np.int32)
+        rho = np.ascontiguousarray(body_density, dtype=np.float64)
+        self._check(lib().dmph_set_bodies(self._h, len(rho), _ptr(b), _ptr(rho)))
+        self.nbodies = len(rho)
+
+    def bodies(self):
+        """dict of body arrays: X, V, L (B,3), q (B,4), M (B,), F, T (B,3)"""
+        B = getattr(self, "nbodies", 0)
+        out = {k: np.zeros((B, 3)) for k in ("X", "V", "L", "F", "T")}
+        out["q"] = np.zeros((B, 4))
+        out["M"] = np.zeros(B)
+        self._check(lib().dmph_get_bodies(self._h, _ptr(out["X"]), _ptr(out["V"]), _ptr(out["q"]), _ptr(out["L"]),
+                                          _ptr(out["M"]), _ptr(out["F"]), _ptr(out["T"])))
+        return out
 
     PHASES = ("drift", "rebuild", "pass_a", "pass_b", "dem", "bodies")
 

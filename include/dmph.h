@@ -200,6 +200,7 @@ typedef struct dmph_info {
     double max_radius;         /* MaxRadius :238 */
     int32_t num_bodies;        /* rigid clumps (0 unless DMPH_FLAG_RIGID_CLUMPS) */
     int32_t surface_tension;   /* 1 if the surface-tension passes run */
+    int64_t kernel_launches;   /* kernels this library launched in dmph_step calls since create */
 } dmph_info;
 int dmph_get_info(dmph_ctx *ctx, dmph_info *info);
 
@@ -214,6 +215,24 @@ int dmph_get_info(dmph_ctx *ctx, dmph_info *info);
  */
 int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind, int64_t capacity);
 
+/*
+ * Rigid debris bodies (no counterpart in the reference, whose debris particles
+ * move individually, source/DEM-MPH.cpp:1872-1891).  body_of_row[r] is the body
+ * of input-grid row r (-1: none); every solid particle must belong to a body.
+ * body_density[b] replaces the type density for the particles of body b.
+ * Mass, centre of mass, inertia tensor, velocity and angular momentum of each
+ * body are computed from its particles' current state (FP64); from the next
+ * step on, DEM substeps move each body rigidly (translation + quaternion
+ * rotation in FP64) under the sum of its particles' fluid and contact forces.
+ * Call once, before the first dmph_step.
+ */
+int dmph_set_bodies(dmph_ctx *ctx, int nbodies, const int *body_of_row, const double *body_density);
+
+/* Body state, each pointer optional: X,V,L 3 per body (centre of mass,
+ * velocity, angular momentum), q 4 per body (w,x,y,z), mass 1 per body,
+ * F,T 3 per body (total force and torque of the last substep). */
+int dmph_get_bodies(dmph_ctx *ctx, double *X, double *V, double *q, double *L, double *mass, double *F, double *T);
+
 /* Per-phase device timing.  With enable != 0, every following step records
  * CUDA events on the context's stream around each phase (this adds event
  * overhead, so time throughput with it off); dmph_get_phase_times returns the
@@ -223,6 +242,7 @@ int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind, int64_t ca
 #define DMPH_PHASE_COUNT 6
 int dmph_set_profiling(dmph_ctx *ctx, int enable);
 int dmph_get_phase_times(dmph_ctx *ctx, double *ms, int64_t *launches, int n);
+
 
 /* Release the context and its device memory. */
 int dmph_destroy(dmph_ctx *ctx);

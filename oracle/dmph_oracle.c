@@ -42,6 +42,7 @@ struct dmph_oracle {
     double *mass, *kappa, *lambda, *mu;
     double *densA, *gc, *pA, *vsp, *div, *P;
     double *kn, *cn, *kt, *ct, *alpha, *dragC;
+    double *fsc; /* per particle: sum of |pair force| terms of the step (test scale, not a reference array) */
     int *nc, *fnc, *snc;
     long *nptr;
     int *nind;
@@ -49,6 +50,13 @@ struct dmph_oracle {
     int *key, *payload;
     int *cfb, *cfe, *csb, *cse, *cwb, *cwe;
     int fb, fe, sb, se, wb, we;
+    /* rigid bodies (0 = off) */
+    int B;
+    int *bid;          /* body of each slot, permuted with the sort */
+    double *brho;      /* density of each body */
+    int *bptr, *bmrow; /* members (input rows) by body */
+    double *br0, *bX, *bV, *bL, *bq, *bM, *bIi;
+    double *fdem;      /* 6 per particle: contact force and offset torque */
 };
 
 /* Mod macro, :76 */
@@ -60,6 +68,7 @@ static inline void rel(const dmph_oracle *o, const double *xi, const double *xj,
     for (int d = 0; d < 3; d++) q[d] = pmod(xj[d] - xi[d] + 0.5 * o->W[d], o->W[d]) - 0.5 * o->W[d];
 }
 static inline double sq3(const double *q) { return (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]); }
+static inline double nrm3(double a, double b, double c) { return sqrt(a * a + b * b + c * c); }
 
 /* smoothing kernels, :272-342 ; B = (1/Sw)/h^dim */
 static inline double k_wa(double r, double B, double h) { return B * (r / h) * (1.0 - (r / h)) * (1.0 - (r / h)); }
@@ -286,6 +295,10 @@ static void cell_sort(dmph_oracle *o)
     memcpy(o->pidx, ti, sizeof(int) * N);
     for (int i = 0; i < N; i++) ti[i] = o->prop[pay[i]];
     memcpy(o->prop, ti, sizeof(int) * N);
+    if (o->bid) {
+        for (int i = 0; i < N; i++) ti[i] = o->bid[pay[i]];
+        memcpy(o->bid, ti, sizeof(int) * N);
+    }
     for (int i = 0; i < N; i++)
         for (int d = 0; d < 3; d++) td[3 * i + d] = o->x[3 * (size_t)pay[i] + d];
     memcpy(o->x, td, sizeof(double) * 3 * N);
@@ -470,6 +483,7 @@ static void physical_coefficients(dmph_oracle *o)
     for (int i = 0; i < o->N; i++) {
         const int t = o->prop[i];
         o->mass[i] = o->p.density[t] * o->V;
+        if (o->bid && o->bid[i] >= 0) o->mass[i] = o->brho[o->bid[i]] * o->V;
         o->kappa[i] = o->p.bulk_modulus[t];
         if (o->vsp[i] < 0.0) o->kappa[i] = 0.0;
         o->lambda[i] = o->p.bulk_viscosity[t];
@@ -488,7 +502,7 @@ static void drag_force(dmph_oracle *o)
             o->alpha[i] = (double)(o->snc[i]) / (o->nc[i]);
         else
             o->alpha[i] = 0.0;
-        const double rho = o->p.density[o->prop[i]];
+        const double rho = (o->bid && o->bid[i] >= 0) ? o->brho[o->bid[i]] : o->p.density[o->prop[i]];
         FOR_NEIGHBORS(o, i, j)
         {
             if (i == j) continue;
@@ -510,6 +524,7 @@ static void drag_force(dmph_oracle *o)
                     cd = 0.44;
                 o->dragC[i] = cd;
                 for (int d = 0; d < 3; d++) f[d] += 0.5 * cd * rho * o->dx * o->dx * o->dx * u[d] * Vs;
+                o->fsc[i] += fabs(0.5 * cd * rho * o->dx * o->dx * o->dx * Vs * Vs);
             }
         }
         for (int d = 0; d < 3; d++) o->F[3 * i + d] += f[d];
@@ -545,6 +560,7 @@ static void pressure_p(dmph_oracle *o)
                 const double dw = k_dw(r, o->Bp, o->RP);
                 const double g[3] = {dw * q[0] / r, dw * q[1] / r, dw * q[2] / r};
                 for (int d = 0; d < 3; d++) f[d] += (o->P[i] + o->P[j]) * g[d] * o->V;
+                o->fsc[i] += fabs((o->P[i] + o->P[j]) * dw * o->V);
             }
         }
         for (int d = 0; d < 3; d++) o->F[3 * i + d] += f[d];
@@ -580,6 +596,7 @@ static void pressure_a(dmph_oracle *o)
                 const double dwji = rji_ * k_dwa(r, o->Ba, o->RA);
                 const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
                 for (int d = 0; d < 3; d++) f[d] += (o->pA[i] * dwij + o->pA[j] * dwji) * e[d] * o->V;
+                o->fsc[i] += fabs((o->pA[i] * dwij + o->pA[j] * dwji) * o->V);
             }
         }
         for (int d = 0; d < 3; d++) o->F[3 * i + d] += f[d];
@@ -620,6 +637,9 @@ static void diffuse_interface(dmph_oracle *o)
                 double gr = 0.0;
                 for (int d = 0; d < 3; d++) gr += (aj * gj[d] * dwji - ai * gi[d] * dwij) * q[d];
                 for (int d = 0; d < 3; d++) f[d] -= (gr)*e[d] / o->R2g * o->RG * (o->V / o->dx);
+                o->fsc[i] += (fabs(gr) + nrm3(aj * gj[0] * wji - ai * gi[0] * wij, aj * gj[1] * wji - ai * gi[1] * wij,
+                                              aj * gj[2] * wji - ai * gi[2] * wij)) /
+                             o->R2g * o->RG * (o->V / o->dx);
             }
         }
         for (int d = 0; d < 3; d++) o->F[3 * i + d] += f[d];
@@ -650,6 +670,7 @@ static void viscosity_v(dmph_oracle *o)
                 const double muij = 2.0 * (o->mu[i] * o->mu[j]) / (o->mu[i] + o->mu[j]);
                 for (int d = 0; d < 3; d++)
                     f[d] += C * muij * (u[0] * e[0] + u[1] * e[1] + u[2] * e[2]) * e[d] * dwij / r * o->V;
+                o->fsc[i] += fabs(C * muij * nrm3(u[0], u[1], u[2]) * dwij / r * o->V);
             }
         }
         for (int d = 0; d < 3; d++) o->F[3 * i + d] += f[d];
@@ -671,6 +692,8 @@ static void buoyancy_force(dmph_oracle *o)
             if (o->RP * o->RP - r2 > 0 && is_fluid(o->prop[j])) {
                 const double w = k_w(sqrt(r2), o->Bp, o->RP);
                 for (int d = 0; d < 3; d++) f[d] += o->p.density[o->prop[j]] * o->V * o->p.gravity[d] * w;
+                o->fsc[i] += fabs(o->p.density[o->prop[j]] * o->V * w) *
+                             nrm3(o->p.gravity[0], o->p.gravity[1], o->p.gravity[2]);
             }
         }
         for (int d = 0; d < 3; d++) o->F[3 * i + d] -= f[d];
@@ -879,6 +902,152 @@ static int need_rebuild(dmph_oracle *o)
     return m > 0.5 * o->margin * 0.5 * o->margin;
 }
 
+/* ---- rigid debris bodies (no reference counterpart; the library's
+ * DMPH_FLAG_RIGID_CLUMPS mode restated in FP64).  Contact force per pair of
+ * particles of different bodies (or a body and a wall) within dx: Hertz-type
+ * normal spring with the pair's effective modulus, projected normal damping,
+ * tangential viscous force capped by Coulomb friction, acting at the contact
+ * midpoint; then per body: total force and torque, semi-implicit Euler for the
+ * centre of mass and angular momentum, exact quaternion rotation by w dt. */
+static void clump_dem(dmph_oracle *o)
+{
+    const double dx = o->dx, Reff = dx * dx / (dx + dx);
+#pragma omp parallel for
+    for (int i = o->sb; i < o->se; ++i) {
+        const int ti = o->prop[i], bi = o->bid[i];
+        const double mi = o->mass[i];
+        double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+        FOR_NEIGHBORS(o, i, j)
+        {
+            const int tj = o->prop[j];
+            if (j == i || is_fluid(tj) || (bi >= 0 && o->bid[j] == bi)) continue;
+            double q[3];
+            for (int d = 0; d < 3; d++) {
+                q[d] = o->x[3 * j + d] - o->x[3 * i + d];
+                q[d] -= o->W[d] * nearbyint(q[d] / o->W[d]);
+            }
+            const double r2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+            if (r2 > dx * dx || r2 <= 0.0) continue;
+            const double r = sqrt(r2), ov = dx - r;
+            const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
+            const double u[3] = {o->v[3 * j] - o->v[3 * i], o->v[3 * j + 1] - o->v[3 * i + 1],
+                                 o->v[3 * j + 2] - o->v[3 * i + 2]};
+            const double un = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
+            const double mj = (o->bid[j] >= 0 ? o->brho[o->bid[j]] : o->p.density[tj]) * o->V;
+            const double mij = mi * mj / (mi + mj);
+            const double yi = o->p.young_modulus[ti], yj = o->p.young_modulus[tj];
+            const double pi_ = o->p.poisson_ratio[ti], pj = o->p.poisson_ratio[tj];
+            const double Eeff = (yi * yj) / ((1 - pi_ * pi_) * yj + (1 - pj * pj) * yi);
+            const double ktf = 8.0 * yi * yj / (((1 + pi_) * (2 - pi_) * yj) + ((1 + pj) * (2 - pj) * yi));
+            const double eij = 0.5 * (o->p.restitution_coefficient[ti] + o->p.restitution_coefficient[tj]);
+            const double lij = eij > 0.0 ? log(eij) : 0.0;
+            const double damp = eij > 0.0 ? -2.0 * lij / sqrt(M_PI * M_PI + lij * lij) : 0.0;
+            const double fric =
+                0.5 * (o->p.viscous_friction_coefficient[ti] + o->p.viscous_friction_coefficient[tj]);
+            const double kn = (4.0 / 3.0) * Eeff * sqrt(Reff * ov);
+            const double cn = sqrt(mij * kn) * damp;
+            const double kt = ktf * sqrt(Reff * sqrt(ov));
+            const double ct = sqrt(mij * kt) * damp;
+            double f[3], ut[3];
+            const double fnm = fmin(-kn * ov + cn * un, 0.0);
+            for (int d = 0; d < 3; d++) {
+                f[d] = fnm * e[d];
+                ut[d] = u[d] - un * e[d];
+            }
+            const double ctot = ct + kt * o->p.dem_dt;
+            const double aut = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
+            const double cap = fric * fabs(fnm);
+            const double ft = ctot * aut > cap && aut > 0.0 ? cap / aut : ctot;
+            for (int d = 0; d < 3; d++) f[d] += ft * ut[d];
+            for (int d = 0; d < 3; d++) F[d] += f[d];
+            T[0] += 0.5 * (q[1] * f[2] - q[2] * f[1]);
+            T[1] += 0.5 * (q[2] * f[0] - q[0] * f[2]);
+            T[2] += 0.5 * (q[0] * f[1] - q[1] * f[0]);
+        }
+        for (int d = 0; d < 3; d++) {
+            o->fdem[6 * (size_t)i + d] = F[d];
+            o->fdem[6 * (size_t)i + 3 + d] = T[d];
+        }
+    }
+}
+
+static void quat_R(const double *q, double R[3][3])
+{
+    const double w = q[0], x = q[1], y = q[2], z = q[3];
+    R[0][0] = 1.0 - 2.0 * (y * y + z * z);
+    R[0][1] = 2.0 * (x * y - w * z);
+    R[0][2] = 2.0 * (x * z + w * y);
+    R[1][0] = 2.0 * (x * y + w * z);
+    R[1][1] = 1.0 - 2.0 * (x * x + z * z);
+    R[1][2] = 2.0 * (y * z - w * x);
+    R[2][0] = 2.0 * (x * z - w * y);
+    R[2][1] = 2.0 * (y * z + w * x);
+    R[2][2] = 1.0 - 2.0 * (x * x + y * y);
+}
+
+static void body_omega(const double R[3][3], const double *Ii, const double *L, double *w)
+{
+    double a[3], b[3];
+    for (int r = 0; r < 3; r++) a[r] = R[0][r] * L[0] + R[1][r] * L[1] + R[2][r] * L[2];
+    for (int r = 0; r < 3; r++) b[r] = Ii[3 * r] * a[0] + Ii[3 * r + 1] * a[1] + Ii[3 * r + 2] * a[2];
+    for (int r = 0; r < 3; r++) w[r] = R[r][0] * b[0] + R[r][1] * b[1] + R[r][2] * b[2];
+}
+
+static void body_step(dmph_oracle *o)
+{
+    int *slot = xcalloc((size_t)o->N, sizeof(int));
+    for (int i = 0; i < o->N; i++) slot[o->pidx[i]] = i;
+    const double dt = o->p.dem_dt;
+    for (int b = 0; b < o->B; b++) {
+        double *q = o->bq + 4 * b, R[3][3];
+        quat_R(q, R);
+        double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+        for (int m = o->bptr[b]; m < o->bptr[b + 1]; m++) {
+            const int i = slot[o->bmrow[m]];
+            const double *r0 = o->br0 + 3 * m;
+            double r[3], f[3];
+            for (int k = 0; k < 3; k++) r[k] = R[k][0] * r0[0] + R[k][1] * r0[1] + R[k][2] * r0[2];
+            for (int k = 0; k < 3; k++) f[k] = o->F[3 * i + k] + o->fdem[6 * (size_t)i + k];
+            for (int k = 0; k < 3; k++) F[k] += f[k];
+            T[0] += r[1] * f[2] - r[2] * f[1] + o->fdem[6 * (size_t)i + 3];
+            T[1] += r[2] * f[0] - r[0] * f[2] + o->fdem[6 * (size_t)i + 4];
+            T[2] += r[0] * f[1] - r[1] * f[0] + o->fdem[6 * (size_t)i + 5];
+        }
+        double *X = o->bX + 3 * b, *V = o->bV + 3 * b, *L = o->bL + 3 * b, w[3];
+        for (int k = 0; k < 3; k++) {
+            V[k] += F[k] / o->bM[b] * dt;
+            X[k] += V[k] * dt;
+            L[k] += T[k] * dt;
+        }
+        const double *Ii = o->bIi + 9 * b;
+        body_omega(R, Ii, L, w);
+        const double wn = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+        if (wn > 0.0) {
+            const double h = 0.5 * wn * dt, c = cos(h), sn = sin(h) / wn;
+            const double d[4] = {c, w[0] * sn, w[1] * sn, w[2] * sn};
+            const double nq[4] = {d[0] * q[0] - d[1] * q[1] - d[2] * q[2] - d[3] * q[3],
+                                  d[0] * q[1] + d[1] * q[0] + d[2] * q[3] - d[3] * q[2],
+                                  d[0] * q[2] - d[1] * q[3] + d[2] * q[0] + d[3] * q[1],
+                                  d[0] * q[3] + d[1] * q[2] - d[2] * q[1] + d[3] * q[0]};
+            const double inv = 1.0 / sqrt(nq[0] * nq[0] + nq[1] * nq[1] + nq[2] * nq[2] + nq[3] * nq[3]);
+            for (int k = 0; k < 4; k++) q[k] = nq[k] * inv;
+        }
+        quat_R(q, R);
+        body_omega(R, Ii, L, w);
+        for (int m = o->bptr[b]; m < o->bptr[b + 1]; m++) {
+            const int i = slot[o->bmrow[m]];
+            const double *r0 = o->br0 + 3 * m;
+            double r[3];
+            for (int k = 0; k < 3; k++) r[k] = R[k][0] * r0[0] + R[k][1] * r0[1] + R[k][2] * r0[2];
+            for (int k = 0; k < 3; k++) o->x[3 * i + k] = pmod(X[k] + r[k] - o->p.domain_min[k], o->W[k]) + o->p.domain_min[k];
+            o->v[3 * i] = V[0] + w[1] * r[2] - w[2] * r[1];
+            o->v[3 * i + 1] = V[1] + w[2] * r[0] - w[0] * r[2];
+            o->v[3 * i + 2] = V[2] + w[0] * r[1] - w[1] * r[0];
+        }
+    }
+    free(slot);
+}
+
 /* one iteration of the main loop, :450-579 */
 static void step_once(dmph_oracle *o)
 {
@@ -890,6 +1059,7 @@ static void step_once(dmph_oracle *o)
         for (int d = 0; d < 3; d++)
             o->x[3 * i + d] = pmod(o->x[3 * i + d] - o->p.domain_min[d], o->W[d]) + o->p.domain_min[d];
     memset(o->F, 0, sizeof(double) * 3 * N); /* resetForce :1894 */
+    memset(o->fsc, 0, sizeof(double) * N);
     if (need_rebuild(o)) {
         cell_sort(o);
         build_neighbors(o);
@@ -909,6 +1079,11 @@ static void step_once(dmph_oracle *o)
     buoyancy_force(o);
     gravity_and_acceleration(o);
     for (int s = 0; s < o->demSteps; s++) {
+        if (o->B > 0) {
+            clump_dem(o);
+            body_step(o);
+            continue;
+        }
         dem_coefficients(o);
         dem_forces(o);
         dem_convection(o);
@@ -955,6 +1130,7 @@ dmph_oracle *dmph_oracle_create(const dmph_params *p, int n, const int *type, co
     o->ct = xcalloc(N, sizeof(double));
     o->alpha = xcalloc(N, sizeof(double));
     o->dragC = xcalloc(N, sizeof(double));
+    o->fsc = xcalloc(N, sizeof(double));
     o->nc = xcalloc(N, sizeof(int));
     o->fnc = xcalloc(N, sizeof(int));
     o->snc = xcalloc(N, sizeof(int));
@@ -1027,6 +1203,7 @@ static const field_t FIELDS[] = {
     {"TangentialViscousDampingConstant", FO(ct), 1},
     {"alpha", FO(alpha), 1},
     {"DragC", FO(dragC), 1},
+    {"ForceScale", FO(fsc), 1},
     {"NeighborCount", FO(nc), 0},
     {"FluidNeighborCount", FO(fnc), 0},
     {"SolidNeighborCount", FO(snc), 0},
@@ -1118,15 +1295,154 @@ double dmph_oracle_scalar(dmph_oracle *o, const char *name)
     return NAN;
 }
 
+static int inv3(const double *a, double *out)
+{
+    const double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+    const double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+    if (!(fabs(det) > 0.0)) return -1;
+    const double id = 1.0 / det;
+    out[0] = c00 * id;
+    out[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+    out[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    out[3] = c01 * id;
+    out[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    out[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    out[6] = c02 * id;
+    out[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+    out[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+    return 0;
+}
+
+int dmph_oracle_set_bodies(dmph_oracle *o, int nb, const int *body_of_row, const double *rho)
+{
+    if (!o || nb <= 0 || !body_of_row || !rho || o->B > 0 || o->steps > 0) return DMPH_EINVAL;
+    const int N = o->N;
+    int *slot = xcalloc((size_t)N, sizeof(int));
+    for (int i = 0; i < N; i++) slot[o->pidx[i]] = i;
+    int *cnt = xcalloc((size_t)nb + 1, sizeof(int));
+    for (int r = 0; r < N; r++) {
+        const int b = body_of_row[r], t = o->prop[slot[r]];
+        if (b < -1 || b >= nb || (b >= 0) != is_solid(t)) {
+            free(slot);
+            free(cnt);
+            return DMPH_EINVAL;
+        }
+        if (b >= 0) cnt[b + 1]++;
+    }
+    o->B = nb;
+    o->bptr = xcalloc((size_t)nb + 1, sizeof(int));
+    for (int b = 0; b < nb; b++) o->bptr[b + 1] = o->bptr[b] + cnt[b + 1];
+    const int nm = o->bptr[nb];
+    o->bmrow = xcalloc((size_t)nm, sizeof(int));
+    o->br0 = xcalloc(3 * (size_t)nm, sizeof(double));
+    o->bX = xcalloc(3 * (size_t)nb, sizeof(double));
+    o->bV = xcalloc(3 * (size_t)nb, sizeof(double));
+    o->bL = xcalloc(3 * (size_t)nb, sizeof(double));
+    o->bq = xcalloc(4 * (size_t)nb, sizeof(double));
+    o->bM = xcalloc((size_t)nb, sizeof(double));
+    o->bIi = xcalloc(9 * (size_t)nb, sizeof(double));
+    o->brho = xcalloc((size_t)nb, sizeof(double));
+    o->bid = xcalloc((size_t)N, sizeof(int));
+    o->fdem = xcalloc(6 * (size_t)N, sizeof(double));
+    for (int i = 0; i < N; i++) o->bid[i] = body_of_row[o->pidx[i]];
+    int *fill = xcalloc((size_t)nb, sizeof(int));
+    for (int r = 0; r < N; r++)
+        if (body_of_row[r] >= 0) {
+            const int b = body_of_row[r];
+            o->bmrow[o->bptr[b] + fill[b]++] = r;
+        }
+    for (int b = 0; b < nb; b++) {
+        o->brho[b] = rho[b];
+        const double m = rho[b] * o->V;
+        const int m0 = o->bptr[b], m1 = o->bptr[b + 1], n = m1 - m0;
+        const double *x0 = o->x + 3 * (size_t)slot[o->bmrow[m0]];
+        double c[3] = {0, 0, 0}, vc[3] = {0, 0, 0};
+        double *xu = xcalloc(3 * (size_t)n, sizeof(double));
+        for (int k = 0; k < n; k++) {
+            const int i = slot[o->bmrow[m0 + k]];
+            for (int d = 0; d < 3; d++) {
+                double dd = o->x[3 * (size_t)i + d] - x0[d];
+                dd -= o->W[d] * nearbyint(dd / o->W[d]);
+                xu[3 * k + d] = x0[d] + dd;
+                c[d] += xu[3 * k + d];
+                vc[d] += o->v[3 * (size_t)i + d];
+            }
+        }
+        for (int d = 0; d < 3; d++) {
+            c[d] /= (double)n;
+            vc[d] /= (double)n;
+        }
+        const double a = 0.4 * m * (0.5 * o->dx) * (0.5 * o->dx);
+        double I[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, L[3] = {0, 0, 0};
+        for (int k = 0; k < n; k++) {
+            const int i = slot[o->bmrow[m0 + k]];
+            const double r[3] = {xu[3 * k] - c[0], xu[3 * k + 1] - c[1], xu[3 * k + 2] - c[2]};
+            const double rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+            for (int p = 0; p < 3; p++)
+                for (int q = 0; q < 3; q++) I[3 * p + q] += m * ((p == q ? rr : 0.0) - r[p] * r[q]);
+            for (int p = 0; p < 3; p++) I[4 * p] += a;
+            const double u[3] = {o->v[3 * (size_t)i] - vc[0], o->v[3 * (size_t)i + 1] - vc[1],
+                                 o->v[3 * (size_t)i + 2] - vc[2]};
+            L[0] += m * (r[1] * u[2] - r[2] * u[1]);
+            L[1] += m * (r[2] * u[0] - r[0] * u[2]);
+            L[2] += m * (r[0] * u[1] - r[1] * u[0]);
+            for (int d = 0; d < 3; d++) o->br0[3 * (m0 + k) + d] = r[d];
+        }
+        free(xu);
+        if (inv3(I, o->bIi + 9 * b)) {
+            free(slot);
+            free(cnt);
+            free(fill);
+            return DMPH_EINVAL;
+        }
+        for (int d = 0; d < 3; d++) {
+            o->bX[3 * b + d] = c[d];
+            o->bV[3 * b + d] = vc[d];
+            o->bL[3 * b + d] = L[d];
+        }
+        o->bq[4 * b] = 1.0;
+        o->bM[b] = m * (double)n;
+    }
+    free(slot);
+    free(cnt);
+    free(fill);
+    return 0;
+}
+
+int dmph_oracle_get_bodies(dmph_oracle *o, double *X, double *V, double *q, double *L, double *M)
+{
+    if (!o) return DMPH_EINVAL;
+    const size_t B = (size_t)o->B;
+    if (X) memcpy(X, o->bX, 3 * B * sizeof(double));
+    if (V) memcpy(V, o->bV, 3 * B * sizeof(double));
+    if (q) memcpy(q, o->bq, 4 * B * sizeof(double));
+    if (L) memcpy(L, o->bL, 3 * B * sizeof(double));
+    if (M) memcpy(M, o->bM, B * sizeof(double));
+    return 0;
+}
+
 void dmph_oracle_destroy(dmph_oracle *o)
 {
     if (!o) return;
+    free(o->bid);
+    free(o->brho);
+    free(o->bptr);
+    free(o->bmrow);
+    free(o->br0);
+    free(o->bX);
+    free(o->bV);
+    free(o->bL);
+    free(o->bq);
+    free(o->bM);
+    free(o->bIi);
+    free(o->fdem);
     void **ptrs[] = {(void **)&o->pidx,  (void **)&o->prop,  (void **)&o->x,      (void **)&o->v,
                      (void **)&o->F,     (void **)&o->xref,  (void **)&o->mass,   (void **)&o->kappa,
                      (void **)&o->lambda, (void **)&o->mu,   (void **)&o->densA,  (void **)&o->gc,
                      (void **)&o->pA,    (void **)&o->vsp,   (void **)&o->div,    (void **)&o->P,
                      (void **)&o->kn,    (void **)&o->cn,    (void **)&o->kt,     (void **)&o->ct,
-                     (void **)&o->alpha, (void **)&o->dragC, (void **)&o->nc,     (void **)&o->fnc,
+                     (void **)&o->alpha, (void **)&o->dragC, (void **)&o->fsc,    (void **)&o->nc,
+                     (void **)&o->fnc,
                      (void **)&o->snc,   (void **)&o->nptr,  (void **)&o->nind,   (void **)&o->key,
                      (void **)&o->payload, (void **)&o->cfb, (void **)&o->cfe,    (void **)&o->csb,
                      (void **)&o->cse,   (void **)&o->cwb,   (void **)&o->cwe};

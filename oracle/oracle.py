@@ -36,6 +36,8 @@ def lib():
         L.dmph_oracle_scalar.restype = C.c_double
         L.dmph_oracle_scalar.argtypes = [C.c_void_p, C.c_char_p]
         L.dmph_oracle_destroy.argtypes = [C.c_void_p]
+        L.dmph_oracle_set_bodies.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.dmph_oracle_get_bodies.argtypes = [C.c_void_p] + [C.c_void_p] * 5
         _lib = L
     return _lib
 
@@ -73,6 +75,23 @@ class Oracle:
         L.dmph_oracle_get(self._h, name.encode(), out.ctypes.data)
         if name in VEC_FIELDS:
             out = out.reshape(-1, 3)
+        return out
+
+    def set_bodies(self, body_of_row, body_density):
+        b = np.ascontiguousarray(body_of_row, dtype=np.int32)
+        rho = np.ascontiguousarray(body_density, dtype=np.float64)
+        rc = lib().dmph_oracle_set_bodies(self._h, len(rho), b.ctypes.data, rho.ctypes.data)
+        if rc != 0:
+            raise ValueError("dmph_oracle_set_bodies rejected the bodies")
+        self.nbodies = len(rho)
+
+    def bodies(self):
+        B = getattr(self, "nbodies", 0)
+        out = {k: np.zeros((B, 3)) for k in ("X", "V", "L")}
+        out["q"] = np.zeros((B, 4))
+        out["M"] = np.zeros(B)
+        lib().dmph_oracle_get_bodies(self._h, out["X"].ctypes.data, out["V"].ctypes.data, out["q"].ctypes.data,
+                                     out["L"].ctypes.data, out["M"].ctypes.data)
         return out
 
     def scalar(self, name):
