@@ -41,6 +41,7 @@ CU_SOURCES = [
     ("dmph_rebuild.cu", ["-fmad=false"]),
     ("dmph_api.cu", ["-fmad=false"]),
     ("dmph_f32.cu", []),
+    ("dmph_noalloc.cu", ["-fmad=false"]),
     ("dmph_bodies.cu", []),
 ]
 CPP_SOURCES = ["dmph_params.cpp", "dmph_io.cpp"]

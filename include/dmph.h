@@ -243,6 +243,32 @@ int dmph_get_bodies(dmph_ctx *ctx, double *X, double *V, double *q, double *L, d
 int dmph_set_profiling(dmph_ctx *ctx, int enable);
 int dmph_get_phase_times(dmph_ctx *ctx, double *ms, int64_t *launches, int n);
 
+/*
+ * Allocation-free cell sort.  No counterpart in the reference: it serves
+ * callers that cannot call cudaMalloc (work recorded while a stream is being
+ * captured into a CUDA graph, hosts whose framework owns every device
+ * allocation, real-time loops that must not enter the allocator).  It runs the
+ * neighbour-rebuild sort of calculateCellParticle (cell key with class offset
+ * and the reference's bitonic network) on the caller's stream and allocates
+ * nothing: its scratch space is a file-scope device array of
+ * DMPH_NOALLOC_MAX_WORDS 64-bit words (4 MiB) that every GPU loading the
+ * library keeps until the process exits, so n must stay below
+ * DMPH_NOALLOC_MAX_WORDS (n <= 524287).
+ *   pos_planes  device, 3n doubles: x[0..n), y[0..n), z[0..n)
+ *   type        device, n ints
+ *   sorted_key  device, n ints out: the sorted keys (CellIndex)
+ *   perm        device, n ints out: input row of each sorted slot
+ *   stream      cudaStream_t (NULL = legacy default stream)
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the one array and it keeps the
+ * last call's contents, so calls whose work overlaps on the GPU (other
+ * streams, other host threads) race; serialise them.  Returns DMPH_ERANGE
+ * when n is too large.
+ */
+#define DMPH_NOALLOC_MAX_WORDS (1 << 19)
+int dmph_cell_sort_noalloc(const dmph_params *p, int n, const double *pos_planes, const int *type,
+                           int32_t *sorted_key, int32_t *perm, void *stream);
 
 /* Release the context and its device memory. */
 int dmph_destroy(dmph_ctx *ctx);
