@@ -143,12 +143,17 @@ def algorithmic_bytes(prec):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="config2", choices=["config2", "config1"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--settle", type=int, default=200,
+                    help="untimed steps run before warm-up so the flow is moving and rebuilds fire in the timed steps")
+    ap.add_argument("--no-graph", action="store_true", help="launch kernels one by one instead of graph replay")
+    ap.add_argument("--no-bodies", action="store_true",
+                    help="move debris particles individually (reference DEM) instead of as rigid bodies")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -173,7 +178,13 @@ def main():
     p = scene.params.copy()
     p.precision = PRECISION_FP64 if args.precision == "fp64" else PRECISION_FP32_SPLIT
     g = solver.Solver(p, scene.type, scene.x, scene.v)
+    bodies = not args.no_bodies and len(scene.body_density) > 0
+    if bodies:
+        g.set_bodies(scene.body, scene.body_density)
     n = scene.n
+    g.step(args.settle)
+    if not args.no_graph:
+        g.set_graph(True)
     g.step(args.warmup)
 
     def barrier():
@@ -225,11 +236,11 @@ def main():
 
     # ---- end to end through the C ABI with host buffers: every step uploads
     # the particle state from pinned host memory, steps, reads it back
-    x_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
-    v_h = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
-    _, x0, v0, _ = g.state()
-    x_h[:] = x0
-    v_h[:] = v0
+    host = (torch.empty(n, dtype=torch.int32, pin_memory=True).numpy(),
+            torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy(),
+            torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy(),
+            torch.empty(n, dtype=torch.int32, pin_memory=True).numpy())
+    _, x_h, v_h, _ = g.state(out=host)
     e2e_steps = max(3, min(args.steps, 10))
     barrier()
     torch.cuda.synchronize()
@@ -237,9 +248,7 @@ def main():
     for _ in range(e2e_steps):
         g.set_state(x_h, v_h)
         g.step(1)
-        _, xs, vs, _ = g.state()
-        x_h[:] = xs
-        v_h[:] = vs
+        g.state(out=host)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
@@ -271,8 +280,10 @@ def main():
         "data": "synthetic (seeded dam break with debris, dem_mph_b200.scenes)",
         "config": {"workload": scene.name, "n_particles": counts["total"], "n_fluid": counts["fluid"],
                    "n_solid": counts["solid"], "n_wall": counts["wall"], "n_debris_bodies": len(scene.body_density),
+                   "debris": "rigid bodies (FP64)" if bodies else "individual DEM particles",
                    "precision": args.precision, "dt": p.dt, "dem_substeps": inf.dem_substeps,
                    "rebuilds_in_timed_steps": rebuilds_timed - rebuilds_before, "parallelism": "replicas x%d" % world,
+                   "settle_steps": args.settle, "graph_replay": not args.no_graph,
                    "l2": "inputs larger than L2 (particle state alone %.0f MB)" % (n * 60 / 1e6)},
         "sim_s_per_hour": p.dt * args.steps / (ms_max / 1e3) * 3600.0,
         "clocks": clk.summary(),

@@ -36,8 +36,13 @@ struct dmph_ctx {
     unsigned long long *maxshift = nullptr;
     unsigned long long *h_maxshift = nullptr;  // pinned
     int *h_small = nullptr;                    // pinned scratch for small read-backs
-    int fb = 0, fe = 0, sb = 0, se = 0, wb = 0, we = 0;
-    int ch_s0 = 0, ch_w0 = 0, ch_end = 0;
+    int *dB = nullptr;         // device bounds (DevBound)
+    cudaStream_t st2 = nullptr;      // capture stream of the rebuild body
+    bool use_graph = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    long long graph_steps = 0, host_rebuilds = 0;
+    Chunk *chunks2 = nullptr;  // partition scratch
     int demSteps = 0;
     double time = 0.0;
     long long steps = 0, rebuilds = 0;
@@ -77,6 +82,12 @@ static int dalloc(dmph_ctx *ctx, T **ptr, size_t count)
 static void release(dmph_ctx *ctx)
 {
     if (ctx->st) cudaStreamSynchronize(ctx->st);
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    if (ctx->graph) cudaGraphDestroy(ctx->graph);
+    ctx->gexec = nullptr;
+    ctx->graph = nullptr;
+    if (ctx->st2) cudaStreamDestroy(ctx->st2);
+    ctx->st2 = nullptr;
     for (void *p : ctx->allocs) cudaFree(p);
     ctx->allocs.clear();
     if (ctx->h_maxshift) cudaFreeHost(ctx->h_maxshift);
@@ -101,68 +112,50 @@ static long long bitonic_launches(int n, int nlog)
     return c;
 }
 
-// calculateCellParticle :1288 + the parts of calculateNeighbor the step needs
-static int rebuild(dmph_ctx *ctx, bool first = false)
+// calculateCellParticle :1288 + the parts of calculateNeighbor the step needs.
+// Every launch has a static shape and every range lives in ctx->dB, so the
+// sequence can be recorded into a CUDA graph; permuted arrays are written to
+// the second buffers and copied back, so device pointers never change.
+static void enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
 {
     const DevParams &P = ctx->P;
-    // FP32 split state: absolute FP64 positions are rebuilt into the FP64
-    // planes first (unless they already hold them, at creation)
-    if (ctx->fp32 && !first) launch_export32(P, ctx->S, ctx->S.pos, nullptr, ctx->st);
-    launch_keys(P, ctx->S.pos, ctx->S.type, ctx->words, ctx->st);
-    launch_bitonic(ctx->words, P.P2, P.P2log, ctx->st);
-    launch_cell_start(P, ctx->words, ctx->S.cell_start, ctx->st);
+    const size_t N = (size_t)P.N;
+    DevState &S = ctx->S;
+    if (ctx->fp32 && !first) launch_export32(P, S, S.pos, nullptr, st);
+    launch_keys(P, S.pos, S.type, ctx->words, st);
+    launch_bitonic(ctx->words, P.P2, P.P2log, st);
+    launch_cell_start(P, ctx->words, S.cell_start, st);
     if (ctx->fp32) {
-        launch_permute32(P, ctx->words, ctx->S.pos, ctx->S.v4, ctx->S.type, ctx->S.pidx, ctx->p4b, ctx->v4b,
-                         ctx->type2, ctx->pidx2, ctx->S.xref, ctx->S.xref4, ctx->S.bid, ctx->bid2, ctx->S.vel,
-                         ctx->pos2, ctx->vel2, ctx->st);
-        std::swap(ctx->S.p4, ctx->p4b);
-        std::swap(ctx->S.v4, ctx->v4b);
-        std::swap(ctx->S.pos, ctx->pos2);
-        std::swap(ctx->S.vel, ctx->vel2);
+        launch_permute32(P, ctx->words, S.pos, S.v4, S.type, S.pidx, ctx->p4b, ctx->v4b, ctx->type2, ctx->pidx2,
+                         S.xref, S.xref4, S.bid, ctx->bid2, S.vel, ctx->pos2, ctx->vel2, st);
+        cudaMemcpyAsync(S.p4, ctx->p4b, N * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(S.v4, ctx->v4b, N * sizeof(float4), cudaMemcpyDeviceToDevice, st);
     } else {
-        launch_permute(P, ctx->words, ctx->S.pos, ctx->S.vel, ctx->S.type, ctx->S.pidx, ctx->pos2, ctx->vel2,
-                       ctx->type2, ctx->pidx2, ctx->S.xref, ctx->S.bid, ctx->bid2, ctx->st);
-        std::swap(ctx->S.pos, ctx->pos2);
-        std::swap(ctx->S.vel, ctx->vel2);
+        launch_permute(P, ctx->words, S.pos, S.vel, S.type, S.pidx, ctx->pos2, ctx->vel2, ctx->type2, ctx->pidx2,
+                       S.xref, S.bid, ctx->bid2, st);
     }
-    std::swap(ctx->S.type, ctx->type2);
-    std::swap(ctx->S.pidx, ctx->pidx2);
-    if (ctx->S.bid) {
-        std::swap(ctx->S.bid, ctx->bid2);
-        launch_slot_of_row(P, ctx->S.pidx, ctx->Bd.slot_of_row, ctx->st);
+    cudaMemcpyAsync(S.pos, ctx->pos2, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(S.vel, ctx->vel2, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(S.type, ctx->type2, N * sizeof(int), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(S.pidx, ctx->pidx2, N * sizeof(int), cudaMemcpyDeviceToDevice, st);
+    if (S.bid) {
+        cudaMemcpyAsync(S.bid, ctx->bid2, N * sizeof(int), cudaMemcpyDeviceToDevice, st);
+        launch_slot_of_row(P, S.pidx, ctx->Bd.slot_of_row, st);
     }
-    ctx->S.skey = ctx->words;
-    launch_chunks(P, ctx->words, ctx->S.cell_start, ctx->flag, ctx->offs, ctx->bsums, ctx->total, ctx->S.chunks,
-                  ctx->st);
-    // class boundaries: slot ranges from cell_start, chunk ranges from the scan
-    int *h = ctx->h_small;
-    CK(cudaMemcpyAsync(h + 0, ctx->S.cell_start + P.T, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(h + 1, ctx->S.cell_start + 2 * P.T, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaMemcpyAsync(h + 2, ctx->total, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    const int sb = h[0], wb = h[1], nch = h[2];
-    ctx->fb = 0;
-    ctx->fe = sb;
-    ctx->sb = sb;
-    ctx->se = wb;
-    ctx->wb = wb;
-    ctx->we = P.N;
-    if (sb < P.N) CK(cudaMemcpyAsync(h + 3, ctx->offs + sb, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
-    if (wb < P.N) CK(cudaMemcpyAsync(h + 4, ctx->offs + wb, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    ctx->ch_s0 = sb < P.N ? h[3] : nch;
-    ctx->ch_w0 = wb < P.N ? h[4] : nch;
-    ctx->ch_end = nch;
-    if (ctx->all_counts)
-        launch_counts(P, ctx->S, 0, ctx->ch_end, ctx->st);
-    else
-        launch_counts(P, ctx->S, ctx->ch_s0, ctx->ch_w0, ctx->st);
-    CK(cudaGetLastError());
-    // keys, sort, cell starts, permute, (export), chunk flags + 3 scan + write, counts
-    ctx->launches += 1 + bitonic_launches(P.P2, P.P2log) + 1 + 1 + (ctx->fp32 && !first ? 1 : 0) + 5 +
-                     (ctx->S.bid ? 1 : 0) +
-                     ((ctx->all_counts ? ctx->ch_end > 0 : ctx->ch_w0 > ctx->ch_s0) ? 1 : 0);
-    return DMPH_OK;
+    S.skey = ctx->words;
+    launch_chunks(P, ctx->words, S.cell_start, ctx->flag, ctx->offs, ctx->bsums, ctx->total, S.chunks, st);
+    launch_bounds(P, S.cell_start, ctx->offs, ctx->total, ctx->dB, st);
+    if (ctx->fp32)
+        launch_wet_partition(P, ctx->words, S.cell_start, S.chunks, ctx->chunks2, ctx->dB, ctx->flag, ctx->offs,
+                             ctx->bsums, ctx->total, st);
+    launch_counts(P, S, ctx->dB, ctx->all_counts ? CR_ALL : CR_SOLID, st);
+}
+
+static long long rebuild_launches(const dmph_ctx *ctx, bool first)
+{
+    const DevParams &P = ctx->P;
+    return 1 + bitonic_launches(P.P2, P.P2log) + 1 + 1 + (ctx->fp32 && !first ? 1 : 0) + 5 + 1 +
+           (ctx->fp32 ? 6 : 0) + 1 + (ctx->S.bid ? 1 : 0);
 }
 
 // phase timing (dmph_set_profiling): events around one phase, synchronised
@@ -181,92 +174,167 @@ static void phase_end(dmph_ctx *ctx, int ph)
     ctx->phase_n[ph] += 1;
 }
 
-static int step_once(dmph_ctx *ctx)
+// drift + rebuild decision (first part of a step)
+static void enqueue_head(dmph_ctx *ctx, unsigned long long graph_cond, cudaStream_t st)
 {
     const DevParams &P = ctx->P;
-    ctx->Wm.moving = (ctx->time >= 0.2 && 0.4 >= ctx->time) ? 1 : 0;
-    CK(cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), ctx->st));
-    phase_begin(ctx);
+    cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), st);
     if (ctx->fp32)
-        launch_drift32(P, ctx->Q, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, ctx->st);
+        launch_drift32(P, ctx->Q, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, st);
     else
-        launch_drift(P, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, ctx->st);
-    phase_end(ctx, 0);
-    // WallCenter moves only while `0.0 < Time < 0.2` holds, i.e. Time <= 0 (:2892)
-    if (!(0.0 < ctx->time))
-        for (int t = DMPH_WALL_BEGIN; t < DMPH_WALL_END; ++t)
-            for (int d = 0; d < 3; d++) ctx->Wm.C[t][d] += ctx->Wm.Vel[t][d] * P.dt;
-    CK(cudaMemcpyAsync(ctx->h_maxshift, ctx->maxshift, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    double m2;
-    std::memcpy(&m2, ctx->h_maxshift, sizeof(double));
-    const double margin = (0.1 * P.dx);
-    if (m2 > 0.5 * margin * 0.5 * margin) {
-        phase_begin(ctx);
-        const int rc = rebuild(ctx);
-        if (rc) return rc;
-        phase_end(ctx, 1);
-        ctx->rebuilds++;
-    }
+        launch_drift(P, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, st);
+    launch_decide(P, ctx->maxshift, ctx->dB, graph_cond, st);
+}
+
+// the force passes and the DEM substeps (second part of a step)
+static void enqueue_tail(dmph_ctx *ctx, cudaStream_t st)
+{
+    const DevParams &P = ctx->P;
+    DevState &S = ctx->S;
+    const int *dB = ctx->dB;
     if (ctx->fp32) {
         const DevParams32 &Q = ctx->Q;
         phase_begin(ctx);
-        launch_pass_a32(P, Q, ctx->S, 0, ctx->ch_end, ctx->st);
+        launch_pass_a32(P, Q, S, dB, CR_WET, st);
         phase_end(ctx, 2);
         phase_begin(ctx);
-        launch_pass_b32(P, Q, ctx->S, 0, ctx->ch_w0, ctx->st);
-        launch_fluid_accel32(Q, ctx->S, ctx->fb, ctx->fe, ctx->st);
+        launch_pass_b32(P, Q, S, dB, st);
+        launch_fluid_accel32(Q, S, dB, st);
         phase_end(ctx, 3);
         // DEM and rigid bodies in FP64 on the solids' and walls' master state
         phase_begin(ctx);
-        launch_solid_force_to64(P, ctx->S, ctx->sb, ctx->se, ctx->st);
+        launch_solid_force_to64(P, S, dB, st);
         for (int k = 0; k < ctx->demSteps; ++k) {
             if (ctx->Bd.B > 0) {
-                launch_clump_dem(P, ctx->S, ctx->ch_s0, ctx->ch_w0, ctx->st);
-                launch_body_step(P, ctx->S, ctx->Bd, true, ctx->st);
+                launch_clump_dem(P, S, dB, st);
+                launch_body_step(P, S, ctx->Bd, true, st);
                 continue;
             }
-            launch_dem_force(P, ctx->S, ctx->ch_s0, ctx->ch_w0, 1, ctx->st, true);
-            if (P.wall_dem_coeffs) launch_dem_force(P, ctx->S, ctx->ch_w0, ctx->ch_end, 0, ctx->st, true);
-            launch_dem_integrate(P, ctx->S, ctx->sb, ctx->se, ctx->st);
+            launch_dem_force(P, S, dB, CR_SOLID, 1, st, true);
+            if (P.wall_dem_coeffs) launch_dem_force(P, S, dB, CR_WALL, 0, st, true);
+            launch_dem_integrate(P, S, dB, st);
         }
-        launch_sync_solids32(P, ctx->S, ctx->sb, ctx->se, ctx->st);
+        launch_sync_solids32(P, S, dB, st);
         phase_end(ctx, ctx->Bd.B > 0 ? 5 : 4);
     } else {
         phase_begin(ctx);
-        launch_pass_a(P, ctx->S, 0, ctx->ch_end, 0, ctx->st);
+        launch_pass_a(P, S, dB, CR_ALL, 0, st);
         phase_end(ctx, 2);
         phase_begin(ctx);
-        launch_pass_b(P, ctx->S, 0, ctx->ch_w0, ctx->st);
-        launch_fluid_accel(P, ctx->S, ctx->fb, ctx->fe, ctx->st);
+        launch_pass_b(P, S, dB, st);
+        launch_fluid_accel(P, S, dB, st);
         phase_end(ctx, 3);
         phase_begin(ctx);
         for (int k = 0; k < ctx->demSteps; ++k) {
             if (ctx->Bd.B > 0) {
-                launch_clump_dem(P, ctx->S, ctx->ch_s0, ctx->ch_w0, ctx->st);
-                launch_body_step(P, ctx->S, ctx->Bd, false, ctx->st);
+                launch_clump_dem(P, S, dB, st);
+                launch_body_step(P, S, ctx->Bd, false, st);
                 continue;
             }
-            launch_dem_force(P, ctx->S, ctx->ch_s0, ctx->ch_w0, 1, ctx->st);
-            if (P.wall_dem_coeffs) launch_dem_force(P, ctx->S, ctx->ch_w0, ctx->ch_end, 0, ctx->st);
-            launch_dem_integrate(P, ctx->S, ctx->sb, ctx->se, ctx->st);
+            launch_dem_force(P, S, dB, CR_SOLID, 1, st);
+            if (P.wall_dem_coeffs) launch_dem_force(P, S, dB, CR_WALL, 0, st);
+            launch_dem_integrate(P, S, dB, st);
         }
         phase_end(ctx, ctx->Bd.B > 0 ? 5 : 4);
     }
-    CK(cudaGetLastError());
-    {
-        long long l = 1;  // drift
-        l += ctx->ch_end > 0 ? 1 : 0;                       // pass A
-        l += ctx->ch_w0 > 0 ? 1 : 0;                        // pass B
-        l += ctx->fe > ctx->fb ? 1 : 0;                     // fluid velocity update
-        const long long dem =
-            ctx->Bd.B > 0 ? (ctx->ch_w0 > ctx->ch_s0 ? 1 : 0) + 1
-                          : (ctx->ch_w0 > ctx->ch_s0 ? 1 : 0) + (P.wall_dem_coeffs && ctx->ch_end > ctx->ch_w0 ? 1 : 0) +
-                                (ctx->se > ctx->sb ? 1 : 0);
-        ctx->launches += l + ctx->demSteps * dem + (ctx->fp32 && ctx->se > ctx->sb ? 2 : 0);
-    }
-    ctx->time += P.dt;
+}
+
+static long long tail_launches(const dmph_ctx *ctx)
+{
+    const long long dem = ctx->Bd.B > 0 ? 2 : 2 + (ctx->P.wall_dem_coeffs ? 1 : 0);
+    return 3 + ctx->demSteps * dem + (ctx->fp32 ? 2 : 0);
+}
+
+static void advance_host_clock(dmph_ctx *ctx)
+{
+    // WallCenter moves only while `0.0 < Time < 0.2` holds, i.e. Time <= 0 (:2892)
+    if (!(0.0 < ctx->time))
+        for (int t = DMPH_WALL_BEGIN; t < DMPH_WALL_END; ++t)
+            for (int d = 0; d < 3; d++) ctx->Wm.C[t][d] += ctx->Wm.Vel[t][d] * ctx->P.dt;
+    ctx->time += ctx->P.dt;
     ctx->steps++;
+}
+
+// One step recorded as a CUDA graph: head, an IF node whose body is the
+// rebuild (its condition set on the device by the decision kernel), tail.
+// Valid while the head's parameters do not change: no moving-wall window and
+// Time > 0 (the wall centres move only while Time <= 0).
+static int build_graph(dmph_ctx *ctx)
+{
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle cond;
+    CK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+    CK(cudaStreamBeginCaptureToGraph(ctx->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_head(ctx, (unsigned long long)cond, ctx->st);
+    cudaStreamCaptureStatus status;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraph_t cg = nullptr;
+    CK(cudaStreamGetCaptureInfo(ctx->st, &status, nullptr, &cg, &deps, &ndeps));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CK(cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(ctx->st, &cnode, 1, cudaStreamSetCaptureDependencies));
+    CK(cudaStreamBeginCaptureToGraph(ctx->st2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_rebuild(ctx, false, ctx->st2);
+    CK(cudaStreamEndCapture(ctx->st2, &body));
+    enqueue_tail(ctx, ctx->st);
+    CK(cudaStreamEndCapture(ctx->st, &g));
+    CK(cudaGraphInstantiate(&ctx->gexec, g, 0));
+    ctx->graph = g;
+    return DMPH_OK;
+}
+
+static bool graph_usable(const dmph_ctx *ctx)
+{
+    return ctx->use_graph && !ctx->prof && 0.0 < ctx->time && !(ctx->time >= 0.2 && 0.4 >= ctx->time);
+}
+
+static int step_once(dmph_ctx *ctx)
+{
+    ctx->Wm.moving = (ctx->time >= 0.2 && 0.4 >= ctx->time) ? 1 : 0;
+    if (graph_usable(ctx)) {
+        if (!ctx->gexec) {
+            const int rc = build_graph(ctx);
+            if (rc) return rc;
+        }
+        CK(cudaGraphLaunch(ctx->gexec, ctx->st));
+        ctx->graph_steps++;
+        advance_host_clock(ctx);
+        return DMPH_OK;
+    }
+    phase_begin(ctx);
+    enqueue_head(ctx, 0, ctx->st);
+    phase_end(ctx, 0);
+    CK(cudaMemcpyAsync(ctx->h_small, ctx->dB + B_NEED, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->launches += 2;
+    if (ctx->h_small[0]) {
+        phase_begin(ctx);
+        enqueue_rebuild(ctx, false, ctx->st);
+        phase_end(ctx, 1);
+        ctx->launches += rebuild_launches(ctx, false);
+        ctx->host_rebuilds++;
+    }
+    enqueue_tail(ctx, ctx->st);
+    ctx->launches += tail_launches(ctx);
+    CK(cudaGetLastError());
+    advance_host_clock(ctx);
+    return DMPH_OK;
+}
+
+// host copy of the device bounds (synchronises the stream)
+static int read_bounds(dmph_ctx *ctx, int *b)
+{
+    CK(cudaMemcpyAsync(ctx->h_small, ctx->dB, B_COUNT * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (int k = 0; k < B_COUNT; k++) b[k] = ctx->h_small[k];
     return DMPH_OK;
 }
 
@@ -330,12 +398,13 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     CKC(cudaGetDevice(&dev));
     CKC(cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, dev));
     CKC(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
+    CKC(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
     CKC(cudaEventCreate(&ctx->ev0));
     CKC(cudaEventCreate(&ctx->ev1));
     CKC(cudaEventCreate(&ctx->pe0));
     CKC(cudaEventCreate(&ctx->pe1));
     CKC(cudaMallocHost(&ctx->h_maxshift, sizeof(unsigned long long)));
-    CKC(cudaMallocHost(&ctx->h_small, 16 * sizeof(int)));
+    CKC(cudaMallocHost(&ctx->h_small, 2 * B_COUNT * sizeof(int)));
     const DevParams &P = ctx->P;
     const size_t N = (size_t)n, N3 = 3 * N;
     DevState &S = ctx->S;
@@ -366,6 +435,7 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     AL(S.snc, N);
     AL(S.cell_start, (size_t)3 * P.T + 1);
     AL(S.chunks, N + 64);
+    AL(ctx->chunks2, N + 64);
     AL(ctx->pos2, N3);
     AL(ctx->vel2, N3);
     AL(ctx->type2, N);
@@ -392,6 +462,7 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     AL(ctx->bsums, 4096);
     AL(ctx->total, 4);
     AL(ctx->maxshift, 1);
+    AL(ctx->dB, B_COUNT);
     // upload: interleaved x,y,z rows -> component planes
     {
         std::vector<double> planes(N3);
@@ -417,12 +488,12 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         CKC(cudaStreamSynchronize(ctx->st));
     }
     // initial sort, neighbour counts and densities (:419-425)
-    rc = rebuild(ctx, true);
-    if (rc) return fail(rc);
+    if (ctx->fp32) ctx->Q.N0p32 = lattice_n0p32(P, ctx->Q, ctx->st);
+    enqueue_rebuild(ctx, true, ctx->st);
     if (ctx->fp32)
-        launch_pass_a32(P, ctx->Q, ctx->S, 0, ctx->ch_end, ctx->st);
+        launch_pass_a32(P, ctx->Q, ctx->S, ctx->dB, CR_ALL, ctx->st);
     else
-        launch_pass_a(P, S, 0, ctx->ch_end, 1, ctx->st);
+        launch_pass_a(P, S, ctx->dB, CR_ALL, 1, ctx->st);
     CKC(cudaGetLastError());
     CKC(cudaStreamSynchronize(ctx->st));
 #undef AL
@@ -459,14 +530,22 @@ extern "C" int dmph_step_timed(dmph_ctx *ctx, int nsteps, float *device_ms)
     return DMPH_OK;
 }
 
-static int d2h_planes(dmph_ctx *ctx, const double *dev, double *x3)
+// device planes -> caller's x,y,z buffer through a staging buffer (pos2 or
+// vel2, free between steps); the copy is enqueued, the caller synchronises
+static int d2h_planes_async(dmph_ctx *ctx, const double *dev, double *stage, double *x3)
 {
     const size_t N = (size_t)ctx->P.N;
-    std::vector<double> planes(3 * N);
-    CK(cudaMemcpyAsync(planes.data(), dev, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    launch_planes_to_xyz(dev, stage, (int)N, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(x3, stage, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    return DMPH_OK;
+}
+
+static int d2h_planes(dmph_ctx *ctx, const double *dev, double *x3)
+{
+    const int rc = d2h_planes_async(ctx, dev, ctx->pos2, x3);
+    if (rc) return rc;
     CK(cudaStreamSynchronize(ctx->st));
-    for (size_t i = 0; i < N; i++)
-        for (int d = 0; d < 3; d++) x3[3 * i + d] = planes[d * N + i];
     return DMPH_OK;
 }
 
@@ -474,13 +553,13 @@ extern "C" int dmph_get_state(dmph_ctx *ctx, int *type, double *x3, double *v3, 
 {
     if (!ctx) return DMPH_EINVAL;
     const size_t N = (size_t)ctx->P.N;
-    if (ctx->fp32) launch_export32(ctx->P, ctx->S, ctx->S.pos, ctx->S.vel, ctx->st);
+    if (ctx->fp32 && (x3 || v3)) launch_export32(ctx->P, ctx->S, ctx->S.pos, ctx->S.vel, ctx->st);
     if (x3) {
-        int rc = d2h_planes(ctx, ctx->S.pos, x3);
+        int rc = d2h_planes_async(ctx, ctx->S.pos, ctx->pos2, x3);
         if (rc) return rc;
     }
     if (v3) {
-        int rc = d2h_planes(ctx, ctx->S.vel, v3);
+        int rc = d2h_planes_async(ctx, ctx->S.vel, ctx->vel2, v3);
         if (rc) return rc;
     }
     if (type) CK(cudaMemcpyAsync(type, ctx->S.type, N * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
@@ -493,25 +572,20 @@ extern "C" int dmph_set_state(dmph_ctx *ctx, const double *x3, const double *v3)
 {
     if (!ctx) return DMPH_EINVAL;
     const size_t N = (size_t)ctx->P.N;
-    std::vector<double> planes(3 * N);
     if (x3) {
-        for (size_t i = 0; i < N; i++)
-            for (int d = 0; d < 3; d++) planes[d * N + i] = x3[3 * i + d];
-        CK(cudaMemcpyAsync(ctx->S.pos, planes.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
+        CK(cudaMemcpyAsync(ctx->pos2, x3, 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        launch_xyz_to_planes(ctx->pos2, ctx->S.pos, (int)N, ctx->st);
     }
     if (v3) {
-        for (size_t i = 0; i < N; i++)
-            for (int d = 0; d < 3; d++) planes[d * N + i] = v3[3 * i + d];
-        CK(cudaMemcpyAsync(ctx->S.vel, planes.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
+        CK(cudaMemcpyAsync(ctx->vel2, v3, 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+        launch_xyz_to_planes(ctx->vel2, ctx->S.vel, (int)N, ctx->st);
     }
     if (ctx->fp32) {
         if (!x3) launch_export32(ctx->P, ctx->S, ctx->S.pos, nullptr, ctx->st);
         launch_import32(ctx->P, ctx->S, ctx->S.pos, v3 ? ctx->S.vel : nullptr, ctx->st);
-        CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(ctx->st));
     }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
     return DMPH_OK;
 }
 
@@ -525,7 +599,13 @@ extern "C" int dmph_get_field(dmph_ctx *ctx, int field_id, void *out)
         // widen the FP32 field into its FP64 twin, then copy as in FP64 mode
         const int n = (int)N;
         switch (field_id) {
-        case DMPH_FIELD_FORCE: launch_widen_f4(S.f4, S.frc, ctx->fe, n, ctx->st); break;  // solids: FP64 already
+        case DMPH_FIELD_FORCE: {  // fluid slots only: the solids' FP64 forces include their contacts
+            int b[B_COUNT];
+            const int rc = read_bounds(ctx, b);
+            if (rc) return rc;
+            launch_widen_f4(S.f4, S.frc, b[B_FE], n, ctx->st);
+            break;
+        }
         case DMPH_FIELD_GRAVITY_CENTER: launch_widen_f4(S.gc4, S.gc, n, n, ctx->st); break;
         case DMPH_FIELD_VOL_STRAIN_P: launch_widen_f(S.vsp32, S.vsp, n, ctx->st); break;
         case DMPH_FIELD_DIVERGENCE_P: launch_widen_f(S.div32, S.divp, n, ctx->st); break;
@@ -589,9 +669,12 @@ extern "C" int dmph_get_info(dmph_ctx *ctx, dmph_info *info)
     std::memset(info, 0, sizeof(*info));
     const DevParams &P = ctx->P;
     info->n = P.N;
-    info->n_fluid = ctx->fe - ctx->fb;
-    info->n_solid = ctx->se - ctx->sb;
-    info->n_wall = ctx->we - ctx->wb;
+    int b[B_COUNT];
+    const int rc = read_bounds(ctx, b);
+    if (rc) return rc;
+    info->n_fluid = b[B_FE];
+    info->n_solid = b[B_SE] - b[B_SB];
+    info->n_wall = P.N - b[B_SE];
     for (int d = 0; d < 3; d++) {
         info->cell_count[d] = P.cc[d];
         info->cell_width[d] = P.cw[d];
@@ -600,7 +683,7 @@ extern "C" int dmph_get_info(dmph_ctx *ctx, dmph_info *info)
     info->power_count = P.P2;
     info->dem_substeps = ctx->demSteps;
     info->steps = ctx->steps;
-    info->rebuilds = ctx->rebuilds;
+    info->rebuilds = b[B_REBUILDS];
     info->time = ctx->time;
     info->n0a = P.N0a;
     info->n0p = P.N0p;
@@ -608,7 +691,11 @@ extern "C" int dmph_get_info(dmph_ctx *ctx, dmph_info *info)
     info->max_radius = std::sqrt(P.rc2) - 0.1 * P.dx;
     info->num_bodies = ctx->Bd.B;
     info->surface_tension = P.surface_tension;
-    info->kernel_launches = ctx->launches;
+    {
+        const long long graph_rebuilds = b[B_REBUILDS] - ctx->host_rebuilds;
+        info->kernel_launches = ctx->launches + ctx->graph_steps * (2 + tail_launches(ctx)) +
+                                graph_rebuilds * rebuild_launches(ctx, false);
+    }
     return DMPH_OK;
 }
 
@@ -618,7 +705,7 @@ extern "C" int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind,
     const DevParams &P = ctx->P;
     const size_t N = (size_t)P.N;
     // counts of every particle at the last rebuild
-    launch_counts(P, ctx->S, 0, ctx->ch_end, ctx->st);
+    launch_counts(P, ctx->S, ctx->dB, CR_ALL, ctx->st);
     CK(cudaGetLastError());
     std::vector<int> nc(N);
     CK(cudaMemcpyAsync(nc.data(), ctx->S.nc, N * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
@@ -640,7 +727,7 @@ extern "C" int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind,
                 return DMPH_ENOMEM;
             }
             cudaMemcpyAsync(dptr, ptr, (N + 1) * sizeof(long long), cudaMemcpyHostToDevice, ctx->st);
-            launch_neighbor_fill(P, ctx->S, 0, ctx->ch_end, dptr, dind, ctx->st);
+            launch_neighbor_fill(P, ctx->S, ctx->dB, dptr, dind, ctx->st);
             cudaError_t e = cudaGetLastError();
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(ind, dind, (size_t)ptr[N] * sizeof(int), cudaMemcpyDeviceToHost, ctx->st);
@@ -838,6 +925,13 @@ extern "C" int dmph_get_bodies(dmph_ctx *ctx, double *X, double *V, double *q, d
     if (F) CK(cudaMemcpyAsync(F, Bd.Fsum, 3 * B * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     if (T) CK(cudaMemcpyAsync(T, Bd.Tsum, 3 * B * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    return DMPH_OK;
+}
+
+extern "C" int dmph_set_graph(dmph_ctx *ctx, int enable)
+{
+    if (!ctx) return DMPH_EINVAL;
+    ctx->use_graph = enable != 0;
     return DMPH_OK;
 }
 

@@ -67,82 +67,83 @@ __device__ __forceinline__ void load_xv(const DevParams &P, const DevState &S, i
 }
 
 template <bool F32>
-__global__ void __launch_bounds__(4 * kWarp) k_clump_dem(DevParams P, DevState S, int chunk_begin, int chunk_end)
+__global__ void __launch_bounds__(4 * kWarp) k_clump_dem(DevParams P, DevState S, const int *dB, int range)
 {
     __shared__ ClumpTile tiles[4];
     ClumpTile &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int N = P.N;
-    const int cidx = chunk_begin + blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (cidx >= chunk_end) return;
-    const Chunk ch = S.chunks[cidx];
-    const int i = ch.i0 + lane;
-    const bool active = lane < ch.cnt;
-    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-    const int cix = key_cell / (P.cc[1] * P.cc[2]), ciy = (key_cell / P.cc[2]) % P.cc[1], ciz = key_cell % P.cc[2];
-    const int ii = active ? i : ch.i0;
-    double xi[3], vi[3];
-    int ti;
-    load_xv<F32>(P, S, ii, cix, ciy, ciz, xi, vi, &ti);
-    const int bi = S.bid[ii];
-    const double mi = particle_density(S, P, ii, ti) * P.V;
-    double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
-    traverse_stencil(
-        P, S.cell_start, key_cell, lane, active, 6u,
-        [&](int j, int slot) {
-            double x[3], v[3];
-            int t;
-            load_xv<F32>(P, S, j, cix, ciy, ciz, x, v, &t);
-            tl.x[slot] = x[0];
-            tl.y[slot] = x[1];
-            tl.z[slot] = x[2];
-            tl.vx[slot] = v[0];
-            tl.vy[slot] = v[1];
-            tl.vz[slot] = v[2];
-            tl.t[slot] = t;
-            tl.b[slot] = S.bid[j];
-        },
-        [&](int j, int s) {
-            if (j == i || (bi >= 0 && tl.b[s] == bi)) return;
-            double q[3] = {tl.x[s] - xi[0], tl.y[s] - xi[1], tl.z[s] - xi[2]};
-            if (!F32)
-                for (int k = 0; k < 3; k++) q[k] -= P.W[k] * rint(q[k] / P.W[k]);
-            const double r2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
-            if (r2 > P.dx2 || r2 <= 0.0) return;
-            const int tj = tl.t[s];
-            const double r = sqrt(r2);
-            const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
-            const double ov = P.dx - r;
-            const double u[3] = {tl.vx[s] - vi[0], tl.vy[s] - vi[1], tl.vz[s] - vi[2]};
-            const double un = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
-            const int bj = tl.b[s];
-            const double mj = (bj >= 0 ? S.body_rho[bj] : P.density[tj]) * P.V;
-            const double mij = mi * mj / (mi + mj);
-            const double kn = (4.0 / 3.0) * P.Eeff[ti][tj] * sqrt(P.Reff * ov);
-            const double cn = sqrt(mij * kn) * P.pairDamp[ti][tj];
-            const double kt = P.KtFac[ti][tj] * sqrt(P.Reff * sqrt(ov));
-            const double ct = sqrt(mij * kt) * P.pairDamp[ti][tj];
-            double f[3], ut[3];
-            const double fnm = fmin(-kn * ov + cn * un, 0.0);  // no adhesion
-            for (int k = 0; k < 3; k++) {
-                f[k] = fnm * e[k];
-                ut[k] = u[k] - un * e[k];
-            }
-            const double ctot = ct + kt * P.ddt;
-            const double aut = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
-            const double cap = P.pairFric[ti][tj] * fabs(fnm);
-            const double ft = ctot * aut > cap && aut > 0.0 ? cap / aut : ctot;
-            for (int k = 0; k < 3; k++) f[k] += ft * ut[k];
-            for (int k = 0; k < 3; k++) F[k] += f[k];
-            // offset of the contact midpoint from the particle centre: 0.5 q
-            T[0] += 0.5 * (q[1] * f[2] - q[2] * f[1]);
-            T[1] += 0.5 * (q[2] * f[0] - q[0] * f[2]);
-            T[2] += 0.5 * (q[0] * f[1] - q[1] * f[0]);
-        });
-    if (!active) return;
-    for (int k = 0; k < 3; k++) {
-        S.frc_dem[k * N + i] = F[k];
-        S.frc_dem[(3 + k) * N + i] = T[k];
+    FOR_EACH_CHUNK(dB, range, 4, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        const int cix = key_cell / (P.cc[1] * P.cc[2]), ciy = (key_cell / P.cc[2]) % P.cc[1], ciz = key_cell % P.cc[2];
+        const int ii = active ? i : ch.i0;
+        double xi[3], vi[3];
+        int ti;
+        load_xv<F32>(P, S, ii, cix, ciy, ciz, xi, vi, &ti);
+        const int bi = S.bid[ii];
+        const double mi = particle_density(S, P, ii, ti) * P.V;
+        double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
+        traverse_stencil(
+            P, S.cell_start, key_cell, lane, active, 6u,
+            [&](int j, int slot) {
+                double x[3], v[3];
+                int t;
+                load_xv<F32>(P, S, j, cix, ciy, ciz, x, v, &t);
+                tl.x[slot] = x[0];
+                tl.y[slot] = x[1];
+                tl.z[slot] = x[2];
+                tl.vx[slot] = v[0];
+                tl.vy[slot] = v[1];
+                tl.vz[slot] = v[2];
+                tl.t[slot] = t;
+                tl.b[slot] = S.bid[j];
+            },
+            [&](int j, int s) {
+                if (j == i || (bi >= 0 && tl.b[s] == bi)) return;
+                double q[3] = {tl.x[s] - xi[0], tl.y[s] - xi[1], tl.z[s] - xi[2]};
+                if (!F32)
+                    for (int k = 0; k < 3; k++) q[k] -= P.W[k] * rint(q[k] / P.W[k]);
+                const double r2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+                if (r2 > P.dx2 || r2 <= 0.0) return;
+                const int tj = tl.t[s];
+                const double r = sqrt(r2);
+                const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
+                const double ov = P.dx - r;
+                const double u[3] = {tl.vx[s] - vi[0], tl.vy[s] - vi[1], tl.vz[s] - vi[2]};
+                const double un = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
+                const int bj = tl.b[s];
+                const double mj = (bj >= 0 ? S.body_rho[bj] : P.density[tj]) * P.V;
+                const double mij = mi * mj / (mi + mj);
+                const double kn = (4.0 / 3.0) * P.Eeff[ti][tj] * sqrt(P.Reff * ov);
+                const double cn = sqrt(mij * kn) * P.pairDamp[ti][tj];
+                const double kt = P.KtFac[ti][tj] * sqrt(P.Reff * sqrt(ov));
+                const double ct = sqrt(mij * kt) * P.pairDamp[ti][tj];
+                double f[3], ut[3];
+                const double fnm = fmin(-kn * ov + cn * un, 0.0);  // no adhesion
+                for (int k = 0; k < 3; k++) {
+                    f[k] = fnm * e[k];
+                    ut[k] = u[k] - un * e[k];
+                }
+                const double ctot = ct + kt * P.ddt;
+                const double aut = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
+                const double cap = P.pairFric[ti][tj] * fabs(fnm);
+                const double ft = ctot * aut > cap && aut > 0.0 ? cap / aut : ctot;
+                for (int k = 0; k < 3; k++) f[k] += ft * ut[k];
+                for (int k = 0; k < 3; k++) F[k] += f[k];
+                // offset of the contact midpoint from the particle centre: 0.5 q
+                T[0] += 0.5 * (q[1] * f[2] - q[2] * f[1]);
+                T[1] += 0.5 * (q[2] * f[0] - q[0] * f[2]);
+                T[2] += 0.5 * (q[0] * f[1] - q[1] * f[0]);
+            });
+        if (!active) continue;
+        for (int k = 0; k < 3; k++) {
+            S.frc_dem[k * N + i] = F[k];
+            S.frc_dem[(3 + k) * N + i] = T[k];
+        }
     }
 }
 
@@ -287,10 +288,10 @@ void launch_slot_of_row(const DevParams &P, const int *pidx, int *slot_of_row, c
 // FP64 state of solids and walls (in the FP32 split mode these planes are the
 // solids' and walls' master copies, refreshed into the FP32 arrays after the
 // substeps), so the template's FP32 branches are not instantiated.
-void launch_clump_dem(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st)
+void launch_clump_dem(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
 {
-    if (ce <= cb) return;
-    k_clump_dem<false><<<(ce - cb + 3) / 4, 4 * kWarp, 0, st>>>(P, S, cb, ce);
+    static const int g = persistent_grid((const void *)k_clump_dem<false>, 4 * kWarp);
+    k_clump_dem<false><<<g, 4 * kWarp, 0, st>>>(P, S, dB, CR_SOLID);
 }
 
 void launch_body_step(const DevParams &P, const DevState &S, const DevBodies &Bd, bool f32, cudaStream_t st)

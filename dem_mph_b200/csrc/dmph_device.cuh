@@ -74,6 +74,66 @@ struct Chunk {
     int cnt;  // 1..32 particles
 };
 
+// Device-resident bounds of the current cell sort, written by the rebuild
+// kernels and read by every kernel that walks chunks or slot ranges, so that
+// launch shapes never depend on host-side values (a step can be captured in a
+// CUDA graph and replayed).
+enum DevBound {
+    B_CH_S0 = 0,    // first solid chunk
+    B_CH_W0 = 1,    // first wall chunk
+    B_CH_END = 2,   // number of chunks
+    B_CH_WET = 3,   // end of the wall chunks with fluid in reach (FP32 pass A)
+    B_FE = 4,       // fluid slots [0, fe)
+    B_SB = 5,       // solid slots [sb, se)
+    B_SE = 6,
+    B_NEED = 7,     // rebuild decided for this step
+    B_REBUILDS = 8, // rebuilds since creation
+    B_COUNT = 16
+};
+
+enum ChunkRange { CR_ALL = 0, CR_FLUID_SOLID = 1, CR_SOLID = 2, CR_WALL = 3, CR_WET = 4 };
+
+__device__ __forceinline__ void chunk_range(const int *dB, int kind, int &b, int &e)
+{
+    switch (kind) {
+    case CR_FLUID_SOLID: b = 0; e = dB[B_CH_W0]; break;
+    case CR_SOLID: b = dB[B_CH_S0]; e = dB[B_CH_W0]; break;
+    case CR_WALL: b = dB[B_CH_W0]; e = dB[B_CH_END]; break;
+    case CR_WET: b = 0; e = dB[B_CH_WET]; break;
+    default: b = 0; e = dB[B_CH_END]; break;
+    }
+}
+
+// Grid of a persistent kernel: as many blocks as can be resident at once on
+// the device (queried once per kernel through the occupancy API).
+inline int persistent_grid(const void *kernel, int block_threads)
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block_threads, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return sms * per_sm;
+}
+
+// elementwise slot loop over [dB[kb], dB[ke]) (kb < 0: from 0)
+#define FOR_EACH_SLOT(dB, kb, ke, i)                                                                   \
+    const int sb_ = (kb) < 0 ? 0 : dB[kb], se_ = dB[ke];                                              \
+    for (int i = sb_ + blockIdx.x * blockDim.x + threadIdx.x; i < se_; i += gridDim.x * blockDim.x)
+
+// persistent warp loop over the chunks of a range: every warp of the grid
+// takes chunks b + w, b + w + W, ...
+#define FOR_EACH_CHUNK(dB, kind, WARPS_PER_BLOCK, cidx)                                        \
+    int cb_, ce_;                                                                            \
+    chunk_range(dB, kind, cb_, ce_);                                                         \
+    for (int cidx = cb_ + blockIdx.x * (WARPS_PER_BLOCK) + (int)(threadIdx.x >> 5); cidx < ce_; \
+         cidx += gridDim.x * (WARPS_PER_BLOCK))
+
 // 64-bit sort word: key in the high half, payload (slot) in the low half
 __host__ __device__ inline uint32_t word_key(unsigned long long w) { return (uint32_t)(w >> 32); }
 __host__ __device__ inline uint32_t word_slot(unsigned long long w) { return (uint32_t)(w & 0xffffffffull); }

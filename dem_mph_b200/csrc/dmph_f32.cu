@@ -121,237 +121,291 @@ __global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm,
 }
 
 // ---------------------------------------------------------------- pass A
+// Densities, divergence and pressures (the FP32 counterpart of k_pass_a in
+// dmph_f64.cu).  Each staged batch of 32 candidates is first reduced to a
+// per-lane bitmask of the candidates within the cut-off (a branch-free,
+// fully unrolled distance test), then each lane walks its own set bits, so
+// the kernel-weight arithmetic runs only for pairs that contribute.
+template <bool ST>
 __global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_a32(DevParams P, DevParams32 Q, DevState S,
-                                                                       int chunk_begin, int chunk_end)
+                                                                       const int *dB, int range)
 {
     __shared__ Tile32 tiles[kWarpsPerBlock32];
     Tile32 &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
-    const int cidx = chunk_begin + blockIdx.x * kWarpsPerBlock32 + (threadIdx.x >> 5);
-    if (cidx >= chunk_end) return;
-    const Chunk ch = S.chunks[cidx];
-    const int i = ch.i0 + lane;
-    const bool active = lane < ch.cnt;
-    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-    int cix, ciy, ciz;
-    chunk_cell(P, key_cell, cix, ciy, ciz);
-    const int ii = active ? i : ch.i0;
-    const float4 pi = S.p4[ii];
-    const float4 vi = S.v4[ii];
-    const int ti = unpack_type(__float_as_uint(pi.w));
-    const bool st = P.surface_tension;
-    float vsp = 0.f, div = 0.f, dA = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
-    traverse_stencil(
-        P, S.cell_start, key_cell, lane, active, 7u,
-        [&](int j, int slot) { stage32(P, Q, S, tl, j, slot, cix, ciy, ciz, false); },
-        [&](int j, int s) {
-            const float4 pj = tl.p[s];
-            const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-            const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
-            if (j == i) return;
-            const int tj = __float_as_int(pj.w);
-            if (r2 <= Q.RP2) {
-                const float ir = rsqrtf(r2);
-                const float r = r2 * ir;
-                const float a = fmaf(-r, Q.iRP, 1.f);  // 1 - r/h
-                vsp = fmaf(Q.Bp * a, a, vsp);
-                const bool skip = (is_solid(ti) && is_wall(tj)) || (is_solid(tj) && is_wall(ti)) ||
-                                  (is_solid(tj) && is_solid(ti));
-                if (!skip) {
-                    const float4 vj = tl.v[s];
-                    const float uq = fmaf(vj.x - vi.x, q0, fmaf(vj.y - vi.y, q1, (vj.z - vi.z) * q2));
-                    div = fmaf(-uq * ir, Q.dwp * a, div);  // -(u.e) dw
+    FOR_EACH_CHUNK(dB, range, kWarpsPerBlock32, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        int cix, ciy, ciz;
+        chunk_cell(P, key_cell, cix, ciy, ciz);
+        const int ii = active ? i : ch.i0;
+        const float4 pi = S.p4[ii];
+        const float4 vi = S.v4[ii];
+        const int ti = unpack_type(__float_as_uint(pi.w));
+        const bool si = is_solid(ti), wi = is_wall(ti);
+        const float cut2 = ST ? fmaxf(Q.RP2, fmaxf(Q.RA2, Q.RG2)) : Q.RP2;
+        // VolStrainP = sum(w) - N0p cancels to ~1e-3 of the sum, so the sums are
+        // carried in FP64 (one add per pair); the pair terms stay FP32
+        double vsp = 0.0, div = 0.0;
+        float dA = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
+        traverse_stencil_batched(
+            P, S.cell_start, key_cell, lane, 7u,
+            [&](int j, int slot) { stage32(P, Q, S, tl, j, slot, cix, ciy, ciz, false); },
+            [&](int base, int nb) {
+                if (!active) return;
+                unsigned m = 0;
+    #pragma unroll
+                for (int s = 0; s < kWarp; ++s) {
+                    const float4 pj = tl.p[s];
+                    const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+                    const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
+                    m |= (s < nb && r2 <= cut2) ? (1u << s) : 0u;
                 }
-            }
-            if (st && !(is_solid(ti) && is_wall(tj))) {
-                const float ratio = Q.ratio[ti][tj];
-                if (r2 <= Q.RA2) {
+                const int self = i - base;
+                if (self >= 0 && self < kWarp) m &= ~(1u << self);
+                while (m) {
+                    const int s = __ffs(m) - 1;
+                    m &= m - 1;
+                    const float4 pj = tl.p[s];
+                    const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+                    const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
+                    const int tj = __float_as_int(pj.w);
+                    // correctly rounded sqrt: the approximate reciprocal square
+                    // root has a bias that would add up over ~100 neighbours
                     const float r = sqrtf(r2);
-                    const float x = r * Q.iRA;
-                    dA = fmaf(ratio * Q.Ba * x * (1.f - x), (1.f - x), dA);
+                    const float ir = __frcp_rn(r);
+                    if (!ST || r2 <= Q.RP2) {
+                        const float a = fmaf(-r, Q.iRP, 1.f);  // 1 - r/h
+                        vsp += (double)(Q.Bp * a * a);
+                        const bool sj = is_solid(tj);
+                        if (!((si && is_wall(tj)) || (sj && wi) || (sj && si))) {
+                            const float4 vj = tl.v[s];
+                            const float uq = fmaf(vj.x - vi.x, q0, fmaf(vj.y - vi.y, q1, (vj.z - vi.z) * q2));
+                            div -= (double)(uq * ir * Q.dwp * a);  // -(u.e) dw
+                        }
+                    }
+                    if (ST && !(si && is_wall(tj))) {
+                        const float ratio = Q.ratio[ti][tj];
+                        if (r2 <= Q.RA2) {
+                            const float x = r * Q.iRA;
+                            dA = fmaf(ratio * Q.Ba * x * (1.f - x), (1.f - x), dA);
+                        }
+                        if (r2 <= Q.RG2) {
+                            const float a = fmaf(-r, Q.iRG, 1.f);
+                            const float w = ratio * Q.Bg * a * a * Q.R2g_inv_RG;
+                            g0 = fmaf(q0, w, g0);
+                            g1 = fmaf(q1, w, g1);
+                            g2 = fmaf(q2, w, g2);
+                        }
+                    }
                 }
-                if (r2 <= Q.RG2) {
-                    const float r = sqrtf(r2);
-                    const float a = fmaf(-r, Q.iRG, 1.f);
-                    const float w = ratio * Q.Bg * a * a * Q.R2g_inv_RG;
-                    g0 = fmaf(q0, w, g0);
-                    g1 = fmaf(q1, w, g1);
-                    g2 = fmaf(q2, w, g2);
-                }
-            }
-        });
-    if (!active) return;
-    const float volstrain = vsp - Q.N0p;
-    S.vsp32[i] = volstrain;
-    S.div32[i] = div;
-    const float kappa = volstrain < 0.f ? 0.f : Q.bulk[ti];
-    if (!is_solid(ti)) S.pres32[i] = fmaf(-Q.bvisc[ti], div, kappa * volstrain);
-    if (st) {
-        S.densA32[i] = dA;
-        float pa = Q.CofA[ti] * (dA - Q.N0a) / Q.dx;
-        if (Q.N0a <= dA) pa = 0.f;
-        S.pA32[i] = pa;
-        S.gc4[i] = make_float4(g0, g1, g2, 0.f);
+            });
+        if (!active) continue;
+        const double volstrain = vsp - Q.N0p32;
+        S.vsp32[i] = (float)volstrain;
+        S.div32[i] = (float)div;
+        const double kappa = volstrain < 0.0 ? 0.0 : P.bulk[ti];
+        if (!si) S.pres32[i] = (float)(-P.bvisc[ti] * div + kappa * volstrain);
+        if (ST) {
+            S.densA32[i] = dA;
+            float pa = Q.CofA[ti] * (dA - Q.N0a) / Q.dx;
+            if (Q.N0a <= dA) pa = 0.f;
+            S.pA32[i] = pa;
+            S.gc4[i] = make_float4(g0, g1, g2, 0.f);
+        }
     }
 }
 
 // ---------------------------------------------------------------- pass B
+// All fluid forces (the FP32 counterpart of k_pass_b), same two-phase batch
+// scheme.  Chunks hold one particle class, so the fluid/solid split below is
+// uniform across the warp.
+template <bool ST>
 __global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_b32(DevParams P, DevParams32 Q, DevState S,
-                                                                       int chunk_begin, int chunk_end)
+                                                                       const int *dB, int range)
 {
     __shared__ Tile32 tiles[kWarpsPerBlock32];
-    __shared__ TileST tst[kWarpsPerBlock32];
+    __shared__ TileST tst[ST ? kWarpsPerBlock32 : 1];
     Tile32 &tl = tiles[threadIdx.x >> 5];
-    TileST &ts = tst[threadIdx.x >> 5];
+    TileST &ts = tst[ST ? (threadIdx.x >> 5) : 0];
     const int lane = threadIdx.x & 31;
-    const int cidx = chunk_begin + blockIdx.x * kWarpsPerBlock32 + (threadIdx.x >> 5);
-    if (cidx >= chunk_end) return;
-    const Chunk ch = S.chunks[cidx];
-    const int i = ch.i0 + lane;
-    const bool active = lane < ch.cnt;
-    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-    int cix, ciy, ciz;
-    chunk_cell(P, key_cell, cix, ciy, ciz);
-    const int ii = active ? i : ch.i0;
-    const float4 pi = S.p4[ii];
-    const float4 vi = S.v4[ii];
-    const int ti = unpack_type(__float_as_uint(pi.w));
-    const bool sol = is_solid(ti);
-    const float Pi = S.pres32[ii];
-    const float mui = Q.svisc[ti];
-    const float rhoi = (float)particle_density(S, P, ii, ti);
-    const bool st = P.surface_tension;
-    float4 gi = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (st) {
-        gi = S.gc4[ii];
-        gi.w = S.pA32[ii];
-    }
-    float alpha = 0.f;
-    if (sol) {
-        const int nci = S.nc[ii];
-        alpha = nci > 0 ? (float)S.snc[ii] / (float)nci : 0.f;
-    }
-    float3 fP = make_float3(0.f, 0.f, 0.f), fV = fP, fD = fP, fB = fP, fS = fP;
-    float dragc = 0.f;
-    bool have_drag = false;
-    traverse_stencil(
-        P, S.cell_start, key_cell, lane, active, 7u,
-        [&](int j, int slot) {
-            stage32(P, Q, S, tl, j, slot, cix, ciy, ciz, true);
-            if (st) {
-                float4 g = S.gc4[j];
-                g.w = S.pA32[j];
-                ts.g[slot] = g;
-            }
-        },
-        [&](int j, int s) {
-            const float4 pj = tl.p[s];
-            const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-            const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
-            if (j == i || r2 >= Q.RV2 && r2 >= Q.RP2 && (!st || (r2 >= Q.RA2 && r2 >= Q.RG2))) return;
-            const int tj = __float_as_int(pj.w);
-            const float4 vj = tl.v[s];
-            const float u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
-            const float ir = rsqrtf(r2);
-            const float r = r2 * ir;
-            if (!sol && r2 < Q.RP2) {
-                const float a = fmaf(-r, Q.iRP, 1.f);
-                const float c = (Pi + vj.w) * Q.dwp * a * ir * Q.V;  // (Pi+Pj) dw/r V
-                fP.x = fmaf(c, q0, fP.x);
-                fP.y = fmaf(c, q1, fP.y);
-                fP.z = fmaf(c, q2, fP.z);
-            }
-            if (!(sol && is_wall(tj)) && r2 < Q.RV2) {
-                const float a = fmaf(-r, Q.iRV, 1.f);
-                const float muj = Q.svisc[tj];
-                const float muij = 2.f * (mui * muj) / (mui + muj);
-                const float uq = fmaf(u0, q0, fmaf(u1, q1, u2 * q2));
-                // C mu (u.e) e (-dw)/r V  with e = q/r
-                const float c = Q.viscC * muij * uq * (-Q.dwv * a) * ir * ir * ir * Q.V;
-                fV.x = fmaf(c, q0, fV.x);
-                fV.y = fmaf(c, q1, fV.y);
-                fV.z = fmaf(c, q2, fV.z);
-            }
-            if (sol && r2 < Q.RP2 && is_fluid(tj)) {
-                const float Vs = sqrtf(fmaf(u0, u0, fmaf(u1, u1, u2 * u2)));
-                const float Re = alpha * rhoi * Vs * Q.dx / Q.svisc[tj];
-                float cd;
-                if (alpha < 0.8f)
-                    cd = (4.f / 3.f) * (150.f * (1.f - alpha) / (alpha * Re) + 1.75f);
-                else if (Re <= 1000.f)
-                    cd = 24.f * (1.f + 0.15f * powf(Re, 0.687f)) / (alpha * Re) * powf(alpha, -2.65f);
-                else
-                    cd = 0.44f;
-                dragc = cd;
-                have_drag = true;
-                const float c = cd * rhoi * Q.drag_pref * Vs;
-                fD.x = fmaf(c, u0, fD.x);
-                fD.y = fmaf(c, u1, fD.y);
-                fD.z = fmaf(c, u2, fD.z);
-                const float a = fmaf(-r, Q.iRP, 1.f);
-                const float wb = Q.density[tj] * Q.V * Q.Bp * a * a;
-                fB.x = fmaf(wb, Q.g[0], fB.x);
-                fB.y = fmaf(wb, Q.g[1], fB.y);
-                fB.z = fmaf(wb, Q.g[2], fB.z);
-            }
-            if (st && !((sol && is_wall(tj)) || (is_solid(tj) && is_wall(ti)))) {
-                const float rij_ = Q.ratio[ti][tj], rji_ = Q.ratio[tj][ti];
-                const float4 gj = ts.g[s];
-                if (r2 < Q.RA2) {
-                    const float x = r * Q.iRA;
-                    const float dwa = Q.Ba * (1.f - x) * (1.f - 3.f * x) * Q.iRA;
-                    const float c = (gi.w * rij_ + gj.w * rji_) * dwa * ir * Q.V;
-                    fS.x = fmaf(c, q0, fS.x);
-                    fS.y = fmaf(c, q1, fS.y);
-                    fS.z = fmaf(c, q2, fS.z);
+    FOR_EACH_CHUNK(dB, range, kWarpsPerBlock32, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        int cix, ciy, ciz;
+        chunk_cell(P, key_cell, cix, ciy, ciz);
+        const int ii = active ? i : ch.i0;
+        const float4 pi = S.p4[ii];
+        const float4 vi = S.v4[ii];
+        const int ti = unpack_type(__float_as_uint(pi.w));
+        const bool sol = is_solid(ti);
+        const float Pi = S.pres32[ii];
+        const float rhoi = (float)particle_density(S, P, ii, ti);
+        float4 gi = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ST) {
+            gi = S.gc4[ii];
+            gi.w = S.pA32[ii];
+        }
+        float alpha = 0.f;
+        if (sol) {
+            const int nci = S.nc[ii];
+            alpha = nci > 0 ? (float)S.snc[ii] / (float)nci : 0.f;
+        }
+        const float cut2 = ST ? fmaxf(fmaxf(Q.RP2, Q.RV2), fmaxf(Q.RA2, Q.RG2)) : fmaxf(Q.RP2, Q.RV2);
+        // the pressure and viscous pair terms nearly cancel: their sums are FP64
+        double3 fP = make_double3(0.0, 0.0, 0.0), fV = fP;
+        float3 fD = make_float3(0.f, 0.f, 0.f), fB = fD, fS = fD;
+        float dragc = 0.f;
+        bool have_drag = false;
+        traverse_stencil_batched(
+            P, S.cell_start, key_cell, lane, 7u,
+            [&](int j, int slot) {
+                stage32(P, Q, S, tl, j, slot, cix, ciy, ciz, true);
+                if (ST) {
+                    float4 g = S.gc4[j];
+                    g.w = S.pA32[j];
+                    ts.g[slot] = g;
                 }
-                if (r2 < Q.RG2) {
-                    const float a = fmaf(-r, Q.iRG, 1.f);
-                    const float w2 = Q.Bg * a * a, dw2 = Q.dwg * a;
-                    const float ai = Q.ai[ti];
-                    const float k = Q.R2g_inv_RG * Q.Vdx;
-                    fS.x -= (ai * gj.x * rji_ * w2 - ai * gi.x * rij_ * w2) * k;
-                    fS.y -= (ai * gj.y * rji_ * w2 - ai * gi.y * rij_ * w2) * k;
-                    fS.z -= (ai * gj.z * rji_ * w2 - ai * gi.z * rij_ * w2) * k;
-                    const float gr = (ai * gj.x * rji_ * dw2 - ai * gi.x * rij_ * dw2) * q0 +
-                                     (ai * gj.y * rji_ * dw2 - ai * gi.y * rij_ * dw2) * q1 +
-                                     (ai * gj.z * rji_ * dw2 - ai * gi.z * rij_ * dw2) * q2;
-                    const float c = gr * ir * k;
-                    fS.x -= c * q0;
-                    fS.y -= c * q1;
-                    fS.z -= c * q2;
+            },
+            [&](int base, int nb) {
+                if (!active) return;
+                unsigned m = 0;
+    #pragma unroll
+                for (int s = 0; s < kWarp; ++s) {
+                    const float4 pj = tl.p[s];
+                    const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+                    const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
+                    m |= (s < nb && r2 < cut2) ? (1u << s) : 0u;
                 }
-            }
-        });
-    if (!active) return;
-    const float m = sol ? rhoi * Q.V : Q.mass[ti];
-    float4 F;
-    if (sol) {
-        F.x = 2.f * fD.x + fS.x + fV.x - fB.x + m * Q.g[0];
-        F.y = 2.f * fD.y + fS.y + fV.y - fB.y + m * Q.g[1];
-        F.z = 2.f * fD.z + fS.z + fV.z - fB.z + m * Q.g[2];
-        S.alpha32[i] = alpha;
-        if (have_drag) S.dragC32[i] = dragc;
-    } else {
-        F.x = fP.x + fS.x + fV.x + m * Q.g[0];
-        F.y = fP.y + fS.y + fV.y + m * Q.g[1];
-        F.z = fP.z + fS.z + fV.z + m * Q.g[2];
+                const int self = i - base;
+                if (self >= 0 && self < kWarp) m &= ~(1u << self);
+                while (m) {
+                    const int s = __ffs(m) - 1;
+                    m &= m - 1;
+                    const float4 pj = tl.p[s];
+                    const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+                    const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
+                    const int tj = __float_as_int(pj.w);
+                    const float4 vj = tl.v[s];
+                    const float u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
+                    const float ir = rsqrtf(r2);
+                    const float r = r2 * ir;
+                    if (!sol) {
+                        if (r2 < Q.RP2) {
+                            const float a = fmaf(-r, Q.iRP, 1.f);
+                            const float c = (Pi + vj.w) * Q.dwpV * a * ir;  // (Pi+Pj) dw/r V
+                            fP.x += (double)(c * q0);
+                            fP.y += (double)(c * q1);
+                            fP.z += (double)(c * q2);
+                        }
+                        if (r2 < Q.RV2) {
+                            const float a = fmaf(-r, Q.iRV, 1.f);
+                            const float uq = fmaf(u0, q0, fmaf(u1, q1, u2 * q2));
+                            // C mu (u.e) e (-dw)/r V with e = q/r
+                            const float c = Q.muij[ti][tj] * uq * a * (ir * ir * ir);
+                            fV.x += (double)(c * q0);
+                            fV.y += (double)(c * q1);
+                            fV.z += (double)(c * q2);
+                        }
+                    } else {
+                        if (!is_wall(tj) && r2 < Q.RV2) {
+                            const float a = fmaf(-r, Q.iRV, 1.f);
+                            const float uq = fmaf(u0, q0, fmaf(u1, q1, u2 * q2));
+                            const float c = Q.muij[ti][tj] * uq * a * (ir * ir * ir);
+                            fV.x += (double)(c * q0);
+                            fV.y += (double)(c * q1);
+                            fV.z += (double)(c * q2);
+                        }
+                        if (r2 < Q.RP2 && is_fluid(tj)) {
+                            const float Vs = sqrtf(fmaf(u0, u0, fmaf(u1, u1, u2 * u2)));
+                            const float Re = alpha * rhoi * Vs * Q.dx / Q.svisc[tj];
+                            float cd;
+                            if (alpha < 0.8f)
+                                cd = (4.f / 3.f) * (150.f * (1.f - alpha) / (alpha * Re) + 1.75f);
+                            else if (Re <= 1000.f)
+                                cd = 24.f * (1.f + 0.15f * powf(Re, 0.687f)) / (alpha * Re) * powf(alpha, -2.65f);
+                            else
+                                cd = 0.44f;
+                            dragc = cd;
+                            have_drag = true;
+                            const float c = cd * rhoi * Q.drag_pref * Vs;
+                            fD.x = fmaf(c, u0, fD.x);
+                            fD.y = fmaf(c, u1, fD.y);
+                            fD.z = fmaf(c, u2, fD.z);
+                            const float a = fmaf(-r, Q.iRP, 1.f);
+                            const float wb = Q.density[tj] * Q.V * Q.Bp * a * a;
+                            fB.x = fmaf(wb, Q.g[0], fB.x);
+                            fB.y = fmaf(wb, Q.g[1], fB.y);
+                            fB.z = fmaf(wb, Q.g[2], fB.z);
+                        }
+                    }
+                    if (ST && !((sol && is_wall(tj)) || (is_solid(tj) && is_wall(ti)))) {
+                        const float rij_ = Q.ratio[ti][tj], rji_ = Q.ratio[tj][ti];
+                        const float4 gj = ts.g[s];
+                        if (r2 < Q.RA2) {
+                            const float x = r * Q.iRA;
+                            const float dwa = Q.Ba * (1.f - x) * (1.f - 3.f * x) * Q.iRA;
+                            const float c = (gi.w * rij_ + gj.w * rji_) * dwa * ir * Q.V;
+                            fS.x = fmaf(c, q0, fS.x);
+                            fS.y = fmaf(c, q1, fS.y);
+                            fS.z = fmaf(c, q2, fS.z);
+                        }
+                        if (r2 < Q.RG2) {
+                            const float a = fmaf(-r, Q.iRG, 1.f);
+                            const float w2 = Q.Bg * a * a, dw2 = Q.dwg * a;
+                            const float ai = Q.ai[ti];
+                            const float k = Q.R2g_inv_RG * Q.Vdx;
+                            fS.x -= (ai * gj.x * rji_ * w2 - ai * gi.x * rij_ * w2) * k;
+                            fS.y -= (ai * gj.y * rji_ * w2 - ai * gi.y * rij_ * w2) * k;
+                            fS.z -= (ai * gj.z * rji_ * w2 - ai * gi.z * rij_ * w2) * k;
+                            const float gr = (ai * gj.x * rji_ * dw2 - ai * gi.x * rij_ * dw2) * q0 +
+                                             (ai * gj.y * rji_ * dw2 - ai * gi.y * rij_ * dw2) * q1 +
+                                             (ai * gj.z * rji_ * dw2 - ai * gi.z * rij_ * dw2) * q2;
+                            const float c = gr * ir * k;
+                            fS.x -= c * q0;
+                            fS.y -= c * q1;
+                            fS.z -= c * q2;
+                        }
+                    }
+                }
+            });
+        if (!active) continue;
+        const float m = sol ? rhoi * Q.V : Q.mass[ti];
+        float4 F;
+        if (sol) {
+            F.x = (float)(2.0 * fD.x + fS.x + fV.x - fB.x + (double)m * P.g[0]);
+            F.y = (float)(2.0 * fD.y + fS.y + fV.y - fB.y + (double)m * P.g[1]);
+            F.z = (float)(2.0 * fD.z + fS.z + fV.z - fB.z + (double)m * P.g[2]);
+            S.alpha32[i] = alpha;
+            if (have_drag) S.dragC32[i] = dragc;
+        } else {
+            F.x = (float)(fP.x + fS.x + fV.x + (double)m * P.g[0]);
+            F.y = (float)(fP.y + fS.y + fV.y + (double)m * P.g[1]);
+            F.z = (float)(fP.z + fS.z + fV.z + (double)m * P.g[2]);
+        }
+        F.w = 0.f;
+        S.f4[i] = F;
     }
-    F.w = 0.f;
-    S.f4[i] = F;
 }
 
-__global__ void k_fluid_accel32(DevParams32 Q, DevState S, int b, int e)
+__global__ void k_fluid_accel32(DevParams32 Q, DevState S, const int *dB)
 {
-    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= e) return;
-    const float4 f = S.f4[i];
-    float4 v = S.v4[i];
-    const float k = Q.dt / Q.mass[unpack_type(__float_as_uint(S.p4[i].w))];
-    v.x = fmaf(f.x, k, v.x);
-    v.y = fmaf(f.y, k, v.y);
-    v.z = fmaf(f.z, k, v.z);
-    S.v4[i] = v;
+    FOR_EACH_SLOT(dB, -1, B_FE, i)
+    {
+        const float4 f = S.f4[i];
+        float4 v = S.v4[i];
+        const float k = Q.dt / Q.mass[unpack_type(__float_as_uint(S.p4[i].w))];
+        v.x = fmaf(f.x, k, v.x);
+        v.y = fmaf(f.y, k, v.y);
+        v.z = fmaf(f.z, k, v.z);
+        S.v4[i] = v;
+    }
 }
 
 // ------------------------------------------------------- layout conversion
@@ -441,39 +495,77 @@ __global__ void k_import32(DevParams P, DevState S, const double *pos, const dou
 // spacings.  Before the substeps, the solids' FP32 fluid forces seed the FP64
 // force planes; after them, the FP32 positions and velocities of the solids
 // are refreshed from the masters.
-__global__ void k_solid_force_to64(DevParams P, DevState S, int b, int e)
+__global__ void k_solid_force_to64(DevParams P, DevState S, const int *dB)
 {
-    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= e) return;
-    const float4 f = S.f4[i];
-    S.frc[i] = f.x;
-    S.frc[P.N + i] = f.y;
-    S.frc[2 * P.N + i] = f.z;
+    FOR_EACH_SLOT(dB, B_SB, B_SE, i)
+    {
+        const float4 f = S.f4[i];
+        S.frc[i] = f.x;
+        S.frc[P.N + i] = f.y;
+        S.frc[2 * P.N + i] = f.z;
+    }
 }
-__global__ void k_sync_solids32(DevParams P, DevState S, int b, int e)
+__global__ void k_sync_solids32(DevParams P, DevState S, const int *dB)
 {
     const int N = P.N;
-    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= e) return;
-    const float4 p = S.p4[i];
-    const unsigned w = __float_as_uint(p.w);
-    const int c[3] = {unpack_cx(w), unpack_cy(w), unpack_cz(w)};
-    float r[3];
-    for (int d = 0; d < 3; d++) {
-        double a = S.pos[d * N + i] - (P.dmin[d] + c[d] * P.cw[d]);
-        a -= P.W[d] * rint(a / P.W[d]);
-        r[d] = (float)a;
+    FOR_EACH_SLOT(dB, B_SB, B_SE, i)
+    {
+        const float4 p = S.p4[i];
+        const unsigned w = __float_as_uint(p.w);
+        const int c[3] = {unpack_cx(w), unpack_cy(w), unpack_cz(w)};
+        float r[3];
+        for (int d = 0; d < 3; d++) {
+            double a = S.pos[d * N + i] - (P.dmin[d] + c[d] * P.cw[d]);
+            a -= P.W[d] * rint(a / P.W[d]);
+            r[d] = (float)a;
+        }
+        S.p4[i] = make_float4(r[0], r[1], r[2], p.w);
+        S.v4[i] = make_float4((float)S.vel[i], (float)S.vel[N + i], (float)S.vel[2 * N + i], 0.f);
     }
-    S.p4[i] = make_float4(r[0], r[1], r[2], p.w);
-    S.v4[i] = make_float4((float)S.vel[i], (float)S.vel[N + i], (float)S.vel[2 * N + i], 0.f);
 }
-void launch_solid_force_to64(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st)
+void launch_solid_force_to64(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
 {
-    if (e > b) k_solid_force_to64<<<(e - b + 255) / 256, 256, 0, st>>>(P, S, b, e);
+    k_solid_force_to64<<<148, 256, 0, st>>>(P, S, dB);
 }
-void launch_sync_solids32(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st)
+void launch_sync_solids32(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
 {
-    if (e > b) k_sync_solids32<<<(e - b + 255) / 256, 256, 0, st>>>(P, S, b, e);
+    k_sync_solids32<<<148, 256, 0, st>>>(P, S, dB);
+}
+
+// The lattice sum N0p (initializeWeight :1078-1119) evaluated with exactly
+// the FP32 arithmetic of pass A.  VolStrainP = sum(w) - N0p cancels; any
+// rounding bias of the FP32 kernel evaluation (constants 1/h and B are
+// rounded once) then appears identically in both terms and drops out.
+__global__ void k_lattice32(DevParams P, DevParams32 Q, double *out)
+{
+    const int range = (int)(P.RP / P.dx + 3.0);
+    const int zr = P.dim == 2 ? 0 : range;
+    double sum = 0.0;
+    for (int ix = -range; ix <= range; ++ix)
+        for (int iy = -range; iy <= range; ++iy)
+            for (int iz = -zr; iz <= zr; ++iz) {
+                if (ix == 0 && iy == 0 && iz == 0) continue;
+                const float q0 = (float)(P.dx * ix), q1 = (float)(P.dx * iy), q2 = (float)(P.dx * iz);
+                const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
+                if (r2 <= Q.RP2) {
+                    const float r = sqrtf(r2);
+                    const float a = fmaf(-r, Q.iRP, 1.f);
+                    sum += (double)(Q.Bp * a * a);
+                }
+            }
+    *out = sum;
+}
+
+double lattice_n0p32(const DevParams &P, const DevParams32 &Q, cudaStream_t st)
+{
+    double *d = nullptr, h = P.N0p;
+    if (cudaMalloc(&d, sizeof(double)) != cudaSuccess) return h;
+    k_lattice32<<<1, 1, 0, st>>>(P, Q, d);
+    if (cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        h = P.N0p;
+    cudaFree(d);
+    return h;
 }
 
 // widen an FP32 field to FP64 (getters)
@@ -527,6 +619,7 @@ DevParams32 make_params32(const DevParams &P)
     Q.Reff = (float)P.Reff;
     Q.Vdx = (float)(P.V / P.dx);
     Q.drag_pref = (float)(0.5 * P.dx * P.dx * P.dx);
+    Q.dwpV = (float)(-2.0 * P.Bp / P.RP * P.V);
     for (int t = 0; t < kTypes; t++) {
         Q.mass[t] = (float)P.mass[t];
         Q.density[t] = (float)P.density[t];
@@ -543,12 +636,13 @@ DevParams32 make_params32(const DevParams &P)
             Q.ratio[t][u] = (float)P.ratio[t][u];
             Q.Eeff[t][u] = (float)P.Eeff[t][u];
             Q.KtFac[t][u] = (float)P.KtFac[t][u];
+            // C mu_ij (-dw/da) V / h-free part of the viscous pair term: C * harmonic-mean mu * 2B/h * V
+            const double mu = (P.svisc[t] + P.svisc[u]) > 0.0 ? 2.0 * (P.svisc[t] * P.svisc[u]) / (P.svisc[t] + P.svisc[u]) : 0.0;
+            Q.muij[t][u] = (float)(P.viscC * mu * (2.0 * P.Bv / P.RV) * P.V);
         }
     }
     return Q;
 }
-
-static inline int blocks32(int b, int e) { return (e - b + kWarpsPerBlock32 - 1) / kWarpsPerBlock32; }
 
 void launch_drift32(const DevParams &P, const DevParams32 &Q, const DevState &S, const WallMotion &Wm,
                     unsigned long long *maxshift, int sms, cudaStream_t st)
@@ -557,17 +651,32 @@ void launch_drift32(const DevParams &P, const DevParams32 &Q, const DevState &S,
     if (blocks > sms * 8) blocks = sms * 8;
     k_drift32<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(P, Q, S, Wm, maxshift);
 }
-void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, cudaStream_t st)
+void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int range,
+                     cudaStream_t st)
 {
-    if (ce > cb) k_pass_a32<<<blocks32(cb, ce), kWarpsPerBlock32 * kWarp, 0, st>>>(P, Q, S, cb, ce);
+    constexpr int B = kWarpsPerBlock32 * kWarp;
+    if (P.surface_tension) {
+        static const int g = persistent_grid((const void *)k_pass_a32<true>, B);
+        k_pass_a32<true><<<g, B, 0, st>>>(P, Q, S, dB, range);
+    } else {
+        static const int g = persistent_grid((const void *)k_pass_a32<false>, B);
+        k_pass_a32<false><<<g, B, 0, st>>>(P, Q, S, dB, range);
+    }
 }
-void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, cudaStream_t st)
+void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st)
 {
-    if (ce > cb) k_pass_b32<<<blocks32(cb, ce), kWarpsPerBlock32 * kWarp, 0, st>>>(P, Q, S, cb, ce);
+    constexpr int B = kWarpsPerBlock32 * kWarp;
+    if (P.surface_tension) {
+        static const int g = persistent_grid((const void *)k_pass_b32<true>, B);
+        k_pass_b32<true><<<g, B, 0, st>>>(P, Q, S, dB, CR_FLUID_SOLID);
+    } else {
+        static const int g = persistent_grid((const void *)k_pass_b32<false>, B);
+        k_pass_b32<false><<<g, B, 0, st>>>(P, Q, S, dB, CR_FLUID_SOLID);
+    }
 }
-void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, int b, int e, cudaStream_t st)
+void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st)
 {
-    if (e > b) k_fluid_accel32<<<(e - b + 255) / 256, 256, 0, st>>>(Q, S, b, e);
+    k_fluid_accel32<<<148 * 4, 256, 0, st>>>(Q, S, dB);
 }
 void launch_export32(const DevParams &P, const DevState &S, double *pos, double *vel, cudaStream_t st)
 {

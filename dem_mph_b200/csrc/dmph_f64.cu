@@ -117,86 +117,86 @@ __global__ void k_drift(DevParams P, DevState S, WallMotion Wm, unsigned long lo
 // :2129, calculateDivergenceP :2158, calculatePhysicalCoefficients :1918 and
 // the pressures of calculatePressureP :2203-2208 and calculatePressureA
 // :2026-2031, for every particle.
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, DevState S, int chunk_begin,
-                                                                   int chunk_end, int init_only)
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, DevState S, const int *dB, int range, int init_only)
 {
     __shared__ TileA tiles[kWarpsPerBlock];
     TileA &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int N = P.N;
-    const int cidx = chunk_begin + blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-    if (cidx >= chunk_end) return;
-    const Chunk ch = S.chunks[cidx];
-    const int i = ch.i0 + lane;
-    const bool active = lane < ch.cnt;
-    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-    const int ii = active ? i : ch.i0;
-    const int ti = S.type[ii];
-    const double xi = S.pos[ii], yi = S.pos[N + ii], zi = S.pos[2 * N + ii];
-    const double vxi = S.vel[ii], vyi = S.vel[N + ii], vzi = S.vel[2 * N + ii];
-    double vsp = 0.0, div = 0.0, dA = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0;
-    const bool st = P.surface_tension;
-    traverse_stencil(
-        P, S.cell_start, key_cell, lane, active, 7u,
-        [&](int j, int slot) {
-            tl.x[slot] = S.pos[j];
-            tl.y[slot] = S.pos[N + j];
-            tl.z[slot] = S.pos[2 * N + j];
-            tl.vx[slot] = S.vel[j];
-            tl.vy[slot] = S.vel[N + j];
-            tl.vz[slot] = S.vel[2 * N + j];
-            tl.t[slot] = S.type[j];
-        },
-        [&](int j, int s) {
-            if (j == i) return;
-            const double q0 = rel1(tl.x[s], xi, P.W[0], P.hW[0]);
-            const double q1 = rel1(tl.y[s], yi, P.W[1], P.hW[1]);
-            const double q2 = rel1(tl.z[s], zi, P.W[2], P.hW[2]);
-            const double r2 = (q0 * q0 + q1 * q1 + q2 * q2);
-            const int tj = tl.t[s];
-            if (st && !(is_solid(ti) && is_wall(tj))) {
-                const double ratio = P.ratio[ti][tj];
-                if (r2 <= P.RA2) dA += ratio * k_wa(sqrt(r2), P.Ba, P.RA);
-                if (r2 <= P.RG2) {
-                    const double w = ratio * k_w(sqrt(r2), P.Bg, P.RG);
-                    g0 += q0 * w / P.R2g * P.RG;
-                    g1 += q1 * w / P.R2g * P.RG;
-                    g2 += q2 * w / P.R2g * P.RG;
+    FOR_EACH_CHUNK(dB, range, kWarpsPerBlock, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        const int ii = active ? i : ch.i0;
+        const int ti = S.type[ii];
+        const double xi = S.pos[ii], yi = S.pos[N + ii], zi = S.pos[2 * N + ii];
+        const double vxi = S.vel[ii], vyi = S.vel[N + ii], vzi = S.vel[2 * N + ii];
+        double vsp = 0.0, div = 0.0, dA = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0;
+        const bool st = P.surface_tension;
+        traverse_stencil(
+            P, S.cell_start, key_cell, lane, active, 7u,
+            [&](int j, int slot) {
+                tl.x[slot] = S.pos[j];
+                tl.y[slot] = S.pos[N + j];
+                tl.z[slot] = S.pos[2 * N + j];
+                tl.vx[slot] = S.vel[j];
+                tl.vy[slot] = S.vel[N + j];
+                tl.vz[slot] = S.vel[2 * N + j];
+                tl.t[slot] = S.type[j];
+            },
+            [&](int j, int s) {
+                if (j == i) return;
+                const double q0 = rel1(tl.x[s], xi, P.W[0], P.hW[0]);
+                const double q1 = rel1(tl.y[s], yi, P.W[1], P.hW[1]);
+                const double q2 = rel1(tl.z[s], zi, P.W[2], P.hW[2]);
+                const double r2 = (q0 * q0 + q1 * q1 + q2 * q2);
+                const int tj = tl.t[s];
+                if (st && !(is_solid(ti) && is_wall(tj))) {
+                    const double ratio = P.ratio[ti][tj];
+                    if (r2 <= P.RA2) dA += ratio * k_wa(sqrt(r2), P.Ba, P.RA);
+                    if (r2 <= P.RG2) {
+                        const double w = ratio * k_w(sqrt(r2), P.Bg, P.RG);
+                        g0 += q0 * w / P.R2g * P.RG;
+                        g1 += q1 * w / P.R2g * P.RG;
+                        g2 += q2 * w / P.R2g * P.RG;
+                    }
                 }
-            }
-            if (r2 <= P.RP2) {
-                const double r = sqrt(r2);
-                vsp += k_w(r, P.Bp, P.RP);
-                const bool skip = (is_solid(ti) && is_wall(tj)) || (is_solid(tj) && is_wall(ti)) ||
-                                  (is_solid(tj) && is_solid(ti));
-                if (!skip) {
-                    const double dw = k_dw(r, P.Bp, P.RP);
-                    const double e0 = q0 / r, e1 = q1 / r, e2 = q2 / r;
-                    const double u0 = tl.vx[s] - vxi, u1 = tl.vy[s] - vyi, u2 = tl.vz[s] - vzi;
-                    div -= u0 * e0 * dw;
-                    div -= u1 * e1 * dw;
-                    div -= u2 * e2 * dw;
+                if (r2 <= P.RP2) {
+                    const double r = sqrt(r2);
+                    vsp += k_w(r, P.Bp, P.RP);
+                    const bool skip = (is_solid(ti) && is_wall(tj)) || (is_solid(tj) && is_wall(ti)) ||
+                                      (is_solid(tj) && is_solid(ti));
+                    if (!skip) {
+                        const double dw = k_dw(r, P.Bp, P.RP);
+                        const double e0 = q0 / r, e1 = q1 / r, e2 = q2 / r;
+                        const double u0 = tl.vx[s] - vxi, u1 = tl.vy[s] - vyi, u2 = tl.vz[s] - vzi;
+                        div -= u0 * e0 * dw;
+                        div -= u1 * e1 * dw;
+                        div -= u2 * e2 * dw;
+                    }
                 }
-            }
-        });
-    if (!active) return;
-    const double volstrain = (vsp - P.N0p);
-    S.vsp[i] = volstrain;
-    if (st) {
-        S.densA[i] = dA;
-        S.gc[i] = g0;
-        S.gc[N + i] = g1;
-        S.gc[2 * N + i] = g2;
-    }
-    if (init_only) return;  // initialisation evaluates only the densities (:423-425)
-    S.divp[i] = div;
-    double kappa = P.bulk[ti];
-    if (volstrain < 0.0) kappa = 0.0;
-    if (!is_solid(ti)) S.pres[i] = -P.bvisc[ti] * div + kappa * volstrain;
-    if (st) {
-        double pa = P.CofA[ti] * (dA - P.N0a) / P.dx;
-        if (P.N0a <= dA) pa = 0.0;
-        S.pA[i] = pa;
+            });
+        if (!active) continue;
+        const double volstrain = (vsp - P.N0p);
+        S.vsp[i] = volstrain;
+        if (st) {
+            S.densA[i] = dA;
+            S.gc[i] = g0;
+            S.gc[N + i] = g1;
+            S.gc[2 * N + i] = g2;
+        }
+        if (init_only) continue;  // initialisation evaluates only the densities (:423-425)
+        S.divp[i] = div;
+        double kappa = P.bulk[ti];
+        if (volstrain < 0.0) kappa = 0.0;
+        if (!is_solid(ti)) S.pres[i] = -P.bvisc[ti] * div + kappa * volstrain;
+        if (st) {
+            double pa = P.CofA[ti] * (dA - P.N0a) / P.dx;
+            if (P.N0a <= dA) pa = 0.0;
+            S.pA[i] = pa;
+        }
     }
 }
 
@@ -209,157 +209,157 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, 
 // kept in its own accumulator and added to Force in the reference's call
 // order, so the sums are bit-identical.  Wall particles are not visited:
 // their forces are reset at the next step without ever being read.
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, DevState S, int chunk_begin,
-                                                                   int chunk_end)
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, DevState S, const int *dB, int range)
 {
     __shared__ TileB tiles[kWarpsPerBlock];
     TileB &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int N = P.N;
-    const int cidx = chunk_begin + blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-    if (cidx >= chunk_end) return;
-    const Chunk ch = S.chunks[cidx];
-    const int i = ch.i0 + lane;
-    const bool active = lane < ch.cnt;
-    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-    const int ii = active ? i : ch.i0;
-    const int ti = S.type[ii];
-    const bool sol = is_solid(ti);
-    const double xi = S.pos[ii], yi = S.pos[N + ii], zi = S.pos[2 * N + ii];
-    const double vxi = S.vel[ii], vyi = S.vel[N + ii], vzi = S.vel[2 * N + ii];
-    const double Pi = S.pres[ii];
-    const bool st = P.surface_tension;
-    double pai = 0.0, gci0 = 0.0, gci1 = 0.0, gci2 = 0.0;
-    if (st) {
-        pai = S.pA[ii];
-        gci0 = S.gc[ii];
-        gci1 = S.gc[N + ii];
-        gci2 = S.gc[2 * N + ii];
-    }
-    const double mui = P.svisc[ti];
-    const double rhoi = particle_density(S, P, ii, ti);
-    double alpha = 0.0;
-    if (sol) {
-        const int nci = S.nc[ii];
-        alpha = nci > 0 ? (double)(S.snc[ii]) / (nci) : 0.0;
-    }
-    const double ai = P.ai[ti];
-    double fP[3] = {0.0, 0.0, 0.0}, fA[3] = {0.0, 0.0, 0.0}, fI[3] = {0.0, 0.0, 0.0};
-    double fV[3] = {0.0, 0.0, 0.0}, fD[3] = {0.0, 0.0, 0.0}, fB[3] = {0.0, 0.0, 0.0};
-    double dragc = 0.0;
-    bool have_drag = false;
-    traverse_stencil(
-        P, S.cell_start, key_cell, lane, active, 7u,
-        [&](int j, int slot) {
-            tl.x[slot] = S.pos[j];
-            tl.y[slot] = S.pos[N + j];
-            tl.z[slot] = S.pos[2 * N + j];
-            tl.vx[slot] = S.vel[j];
-            tl.vy[slot] = S.vel[N + j];
-            tl.vz[slot] = S.vel[2 * N + j];
-            tl.p[slot] = S.pres[j];
-            tl.t[slot] = S.type[j];
-            if (st) {
-                tl.pa[slot] = S.pA[j];
-                tl.gx[slot] = S.gc[j];
-                tl.gy[slot] = S.gc[N + j];
-                tl.gz[slot] = S.gc[2 * N + j];
-            }
-        },
-        [&](int j, int s) {
-            if (j == i) return;
-            const double q[3] = {rel1(tl.x[s], xi, P.W[0], P.hW[0]), rel1(tl.y[s], yi, P.W[1], P.hW[1]),
-                                 rel1(tl.z[s], zi, P.W[2], P.hW[2])};
-            const double r2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
-            const int tj = tl.t[s];
-            const double u[3] = {tl.vx[s] - vxi, tl.vy[s] - vyi, tl.vz[s] - vzi};
-            // pressure (solid i skipped entirely; fluid i skips no pair)
-            if (!sol && r2 < P.RP2) {
-                const double r = sqrt(r2);
-                const double dw = k_dw(r, P.Bp, P.RP);
-                const double pij = Pi + tl.p[s];
-                for (int d = 0; d < 3; d++) fP[d] += pij * (dw * q[d] / r) * P.V;
-            }
-            const bool sw = (sol && is_wall(tj)) || (is_solid(tj) && is_wall(ti));
-            if (st && !sw) {
-                const double rij_ = P.ratio[ti][tj], rji_ = P.ratio[tj][ti];
-                if (r2 < P.RA2) {
-                    const double r = sqrt(r2);
-                    const double dwij = rij_ * k_dwa(r, P.Ba, P.RA);
-                    const double dwji = rji_ * k_dwa(r, P.Ba, P.RA);
-                    const double paj = tl.pa[s];
-                    for (int d = 0; d < 3; d++) fA[d] += (pai * dwij + paj * dwji) * (q[d] / r) * P.V;
+    FOR_EACH_CHUNK(dB, range, kWarpsPerBlock, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        const int ii = active ? i : ch.i0;
+        const int ti = S.type[ii];
+        const bool sol = is_solid(ti);
+        const double xi = S.pos[ii], yi = S.pos[N + ii], zi = S.pos[2 * N + ii];
+        const double vxi = S.vel[ii], vyi = S.vel[N + ii], vzi = S.vel[2 * N + ii];
+        const double Pi = S.pres[ii];
+        const bool st = P.surface_tension;
+        double pai = 0.0, gci0 = 0.0, gci1 = 0.0, gci2 = 0.0;
+        if (st) {
+            pai = S.pA[ii];
+            gci0 = S.gc[ii];
+            gci1 = S.gc[N + ii];
+            gci2 = S.gc[2 * N + ii];
+        }
+        const double mui = P.svisc[ti];
+        const double rhoi = particle_density(S, P, ii, ti);
+        double alpha = 0.0;
+        if (sol) {
+            const int nci = S.nc[ii];
+            alpha = nci > 0 ? (double)(S.snc[ii]) / (nci) : 0.0;
+        }
+        const double ai = P.ai[ti];
+        double fP[3] = {0.0, 0.0, 0.0}, fA[3] = {0.0, 0.0, 0.0}, fI[3] = {0.0, 0.0, 0.0};
+        double fV[3] = {0.0, 0.0, 0.0}, fD[3] = {0.0, 0.0, 0.0}, fB[3] = {0.0, 0.0, 0.0};
+        double dragc = 0.0;
+        bool have_drag = false;
+        traverse_stencil(
+            P, S.cell_start, key_cell, lane, active, 7u,
+            [&](int j, int slot) {
+                tl.x[slot] = S.pos[j];
+                tl.y[slot] = S.pos[N + j];
+                tl.z[slot] = S.pos[2 * N + j];
+                tl.vx[slot] = S.vel[j];
+                tl.vy[slot] = S.vel[N + j];
+                tl.vz[slot] = S.vel[2 * N + j];
+                tl.p[slot] = S.pres[j];
+                tl.t[slot] = S.type[j];
+                if (st) {
+                    tl.pa[slot] = S.pA[j];
+                    tl.gx[slot] = S.gc[j];
+                    tl.gy[slot] = S.gc[N + j];
+                    tl.gz[slot] = S.gc[2 * N + j];
                 }
-                if (r2 < P.RG2) {
+            },
+            [&](int j, int s) {
+                if (j == i) return;
+                const double q[3] = {rel1(tl.x[s], xi, P.W[0], P.hW[0]), rel1(tl.y[s], yi, P.W[1], P.hW[1]),
+                                     rel1(tl.z[s], zi, P.W[2], P.hW[2])};
+                const double r2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+                const int tj = tl.t[s];
+                const double u[3] = {tl.vx[s] - vxi, tl.vy[s] - vyi, tl.vz[s] - vzi};
+                // pressure (solid i skipped entirely; fluid i skips no pair)
+                if (!sol && r2 < P.RP2) {
                     const double r = sqrt(r2);
-                    const double wij = rij_ * k_w(r, P.Bg, P.RG);
-                    const double wji = rji_ * k_w(r, P.Bg, P.RG);
-                    const double gj[3] = {tl.gx[s], tl.gy[s], tl.gz[s]};
-                    const double gi[3] = {gci0, gci1, gci2};
-                    const double aj = ai;  // the reference uses particle i's CofA here (:2088)
-                    for (int d = 0; d < 3; d++)
-                        fI[d] -= (aj * gj[d] * wji - ai * gi[d] * wij) / P.R2g * P.RG * (P.V / P.dx);
-                    const double dwij = rij_ * k_dw(r, P.Bg, P.RG);
-                    const double dwji = rji_ * k_dw(r, P.Bg, P.RG);
-                    double gr = 0.0;
-                    for (int d = 0; d < 3; d++) gr += (aj * gj[d] * dwji - ai * gi[d] * dwij) * q[d];
-                    for (int d = 0; d < 3; d++) fI[d] -= (gr) * (q[d] / r) / P.R2g * P.RG * (P.V / P.dx);
+                    const double dw = k_dw(r, P.Bp, P.RP);
+                    const double pij = Pi + tl.p[s];
+                    for (int d = 0; d < 3; d++) fP[d] += pij * (dw * q[d] / r) * P.V;
                 }
-            }
-            // viscosity (solid i skips wall j)
-            if (!(sol && is_wall(tj)) && r2 < P.RV2) {
-                const double r = sqrt(r2);
-                const double dwij = -k_dw(r, P.Bv, P.RV);
-                const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
-                const double muj = P.svisc[tj];
-                const double muij = 2.0 * (mui * muj) / (mui + muj);
-                const double dot = (u[0] * e[0] + u[1] * e[1] + u[2] * e[2]);
-                for (int d = 0; d < 3; d++) fV[d] += P.viscC * muij * dot * e[d] * dwij / r * P.V;
-            }
-            // drag and buoyancy on solids from fluid neighbours
-            if (sol && r2 < P.RP2 && is_fluid(tj)) {
-                const double Vs = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-                const double Re = alpha * rhoi * Vs * P.dx / (P.svisc[tj]);
-                double cd;
-                if (alpha < 0.8)
-                    cd = (4.0 / 3.0) * (150.0 * (1.0 - alpha) / (alpha * Re) + 1.75);
-                else if (Re <= 1000.0 && alpha >= 0.8)
-                    cd = 24.0 * (1.0 + 0.15 * pow(Re, 0.687)) / (alpha * Re) * pow(alpha, -2.65);
-                else
-                    cd = 0.44;
-                dragc = cd;
-                have_drag = true;
-                for (int d = 0; d < 3; d++) fD[d] += 0.5 * cd * rhoi * P.dx * P.dx * P.dx * u[d] * Vs;
-                const double w = k_w(sqrt(r2), P.Bp, P.RP);
-                const double rhoj = P.density[tj];
-                for (int d = 0; d < 3; d++) fB[d] += rhoj * P.V * P.g[d] * w;
-            }
-        });
-    if (!active) return;
-    double F[3] = {0.0, 0.0, 0.0};
-    const double m = sol ? rhoi * P.V : P.mass[ti];
-    if (sol) {
-        for (int d = 0; d < 3; d++) F[d] += fD[d];
-        if (st)
-            for (int d = 0; d < 3; d++) F[d] += fA[d];
-        if (st)
-            for (int d = 0; d < 3; d++) F[d] += fI[d];
-        for (int d = 0; d < 3; d++) F[d] += fV[d];
-        for (int d = 0; d < 3; d++) F[d] += fD[d];
-        for (int d = 0; d < 3; d++) F[d] -= fB[d];
-        for (int d = 0; d < 3; d++) F[d] += m * P.g[d];
-        S.alpha[i] = alpha;
-        if (have_drag) S.dragC[i] = dragc;
-    } else {
-        for (int d = 0; d < 3; d++) F[d] += fP[d];
-        if (st)
-            for (int d = 0; d < 3; d++) F[d] += fA[d];
-        if (st)
-            for (int d = 0; d < 3; d++) F[d] += fI[d];
-        for (int d = 0; d < 3; d++) F[d] += fV[d];
-        for (int d = 0; d < 3; d++) F[d] += m * P.g[d];
+                const bool sw = (sol && is_wall(tj)) || (is_solid(tj) && is_wall(ti));
+                if (st && !sw) {
+                    const double rij_ = P.ratio[ti][tj], rji_ = P.ratio[tj][ti];
+                    if (r2 < P.RA2) {
+                        const double r = sqrt(r2);
+                        const double dwij = rij_ * k_dwa(r, P.Ba, P.RA);
+                        const double dwji = rji_ * k_dwa(r, P.Ba, P.RA);
+                        const double paj = tl.pa[s];
+                        for (int d = 0; d < 3; d++) fA[d] += (pai * dwij + paj * dwji) * (q[d] / r) * P.V;
+                    }
+                    if (r2 < P.RG2) {
+                        const double r = sqrt(r2);
+                        const double wij = rij_ * k_w(r, P.Bg, P.RG);
+                        const double wji = rji_ * k_w(r, P.Bg, P.RG);
+                        const double gj[3] = {tl.gx[s], tl.gy[s], tl.gz[s]};
+                        const double gi[3] = {gci0, gci1, gci2};
+                        const double aj = ai;  // the reference uses particle i's CofA here (:2088)
+                        for (int d = 0; d < 3; d++)
+                            fI[d] -= (aj * gj[d] * wji - ai * gi[d] * wij) / P.R2g * P.RG * (P.V / P.dx);
+                        const double dwij = rij_ * k_dw(r, P.Bg, P.RG);
+                        const double dwji = rji_ * k_dw(r, P.Bg, P.RG);
+                        double gr = 0.0;
+                        for (int d = 0; d < 3; d++) gr += (aj * gj[d] * dwji - ai * gi[d] * dwij) * q[d];
+                        for (int d = 0; d < 3; d++) fI[d] -= (gr) * (q[d] / r) / P.R2g * P.RG * (P.V / P.dx);
+                    }
+                }
+                // viscosity (solid i skips wall j)
+                if (!(sol && is_wall(tj)) && r2 < P.RV2) {
+                    const double r = sqrt(r2);
+                    const double dwij = -k_dw(r, P.Bv, P.RV);
+                    const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
+                    const double muj = P.svisc[tj];
+                    const double muij = 2.0 * (mui * muj) / (mui + muj);
+                    const double dot = (u[0] * e[0] + u[1] * e[1] + u[2] * e[2]);
+                    for (int d = 0; d < 3; d++) fV[d] += P.viscC * muij * dot * e[d] * dwij / r * P.V;
+                }
+                // drag and buoyancy on solids from fluid neighbours
+                if (sol && r2 < P.RP2 && is_fluid(tj)) {
+                    const double Vs = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+                    const double Re = alpha * rhoi * Vs * P.dx / (P.svisc[tj]);
+                    double cd;
+                    if (alpha < 0.8)
+                        cd = (4.0 / 3.0) * (150.0 * (1.0 - alpha) / (alpha * Re) + 1.75);
+                    else if (Re <= 1000.0 && alpha >= 0.8)
+                        cd = 24.0 * (1.0 + 0.15 * pow(Re, 0.687)) / (alpha * Re) * pow(alpha, -2.65);
+                    else
+                        cd = 0.44;
+                    dragc = cd;
+                    have_drag = true;
+                    for (int d = 0; d < 3; d++) fD[d] += 0.5 * cd * rhoi * P.dx * P.dx * P.dx * u[d] * Vs;
+                    const double w = k_w(sqrt(r2), P.Bp, P.RP);
+                    const double rhoj = P.density[tj];
+                    for (int d = 0; d < 3; d++) fB[d] += rhoj * P.V * P.g[d] * w;
+                }
+            });
+        if (!active) continue;
+        double F[3] = {0.0, 0.0, 0.0};
+        const double m = sol ? rhoi * P.V : P.mass[ti];
+        if (sol) {
+            for (int d = 0; d < 3; d++) F[d] += fD[d];
+            if (st)
+                for (int d = 0; d < 3; d++) F[d] += fA[d];
+            if (st)
+                for (int d = 0; d < 3; d++) F[d] += fI[d];
+            for (int d = 0; d < 3; d++) F[d] += fV[d];
+            for (int d = 0; d < 3; d++) F[d] += fD[d];
+            for (int d = 0; d < 3; d++) F[d] -= fB[d];
+            for (int d = 0; d < 3; d++) F[d] += m * P.g[d];
+            S.alpha[i] = alpha;
+            if (have_drag) S.dragC[i] = dragc;
+        } else {
+            for (int d = 0; d < 3; d++) F[d] += fP[d];
+            if (st)
+                for (int d = 0; d < 3; d++) F[d] += fA[d];
+            if (st)
+                for (int d = 0; d < 3; d++) F[d] += fI[d];
+            for (int d = 0; d < 3; d++) F[d] += fV[d];
+            for (int d = 0; d < 3; d++) F[d] += m * P.g[d];
+        }
+        for (int d = 0; d < 3; d++) S.frc[d * N + i] = F[d];
     }
-    for (int d = 0; d < 3; d++) S.frc[d * N + i] = F[d];
 }
 
 // ------------------------------------------------------------------ DEM
@@ -375,147 +375,149 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, 
 // MIXED: FP32 split mode, where solids and walls keep FP64 master positions in
 // S.pos/S.vel but fluid particles live in the FP32 arrays p4/v4.
 template <bool MIXED>
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_dem_force(DevParams P, DevState S, int chunk_begin,
-                                                                      int chunk_end, int forces)
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_dem_force(DevParams P, DevState S, const int *dB, int range, int forces)
 {
     __shared__ TileA tiles[kWarpsPerBlock];
     TileA &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int N = P.N;
-    const int cidx = chunk_begin + blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-    if (cidx >= chunk_end) return;
-    const Chunk ch = S.chunks[cidx];
-    const int i = ch.i0 + lane;
-    const bool active = lane < ch.cnt;
-    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-    const int ii = active ? i : ch.i0;
-    const int ti = S.type[ii];
-    const double xi = S.pos[ii], yi = S.pos[N + ii], zi = S.pos[2 * N + ii];
-    const double vxi = S.vel[ii], vyi = S.vel[N + ii], vzi = S.vel[2 * N + ii];
-    auto stage = [&](int j, int slot) {
-        const int t = S.type[j];
-        if (MIXED && is_fluid(t)) {
-            const float4 p = S.p4[j];
-            const float4 v = S.v4[j];
-            const unsigned w = __float_as_uint(p.w);
-            tl.x[slot] = P.dmin[0] + unpack_cx(w) * P.cw[0] + (double)p.x;
-            tl.y[slot] = P.dmin[1] + unpack_cy(w) * P.cw[1] + (double)p.y;
-            tl.z[slot] = P.dmin[2] + unpack_cz(w) * P.cw[2] + (double)p.z;
-            tl.vx[slot] = v.x;
-            tl.vy[slot] = v.y;
-            tl.vz[slot] = v.z;
-        } else {
-            tl.x[slot] = S.pos[j];
-            tl.y[slot] = S.pos[N + j];
-            tl.z[slot] = S.pos[2 * N + j];
-            tl.vx[slot] = S.vel[j];
-            tl.vy[slot] = S.vel[N + j];
-            tl.vz[slot] = S.vel[2 * N + j];
-        }
-        tl.t[slot] = t;
-    };
-    // 1) last neighbour within dx
-    int tlast = -1;
-    double r2last = 0.0;
-    traverse_stencil(P, S.cell_start, key_cell, lane, active, 7u, stage, [&](int j, int s) {
-        if (j == i) return;
-        const double q0 = rel1(tl.x[s], xi, P.W[0], P.hW[0]);
-        const double q1 = rel1(tl.y[s], yi, P.W[1], P.hW[1]);
-        const double q2 = rel1(tl.z[s], zi, P.W[2], P.hW[2]);
-        const double r2 = (q0 * q0 + q1 * q1 + q2 * q2);
-        if (r2 <= P.dx2) {
-            tlast = tl.t[s];
-            r2last = r2;
-        }
-    });
-    double kn, cn, kt, ct;
-    if (active) {
-        if (tlast >= 0) {
-            const double r = sqrt(r2last);
-            const double ov = fmax(0.0, P.dx - r);
-            kn = (4.0 / 3.0) * P.Eeff[ti][tlast] * sqrt(P.Reff * ov);
-            const double mi = P.mass[ti], mj = P.mass[tlast];
-            const double mij = mi * mj / (mi + mj);
-            cn = -2.0 * sqrt(mij * kn) * P.logE[ti] / P.cnDen[ti];
-            kt = P.KtFac[ti][tlast] * sqrt(P.Reff * sqrt(ov));
-            ct = P.ctFac[ti] * sqrt(mij * kt);
-            S.kn[i] = kn;
-            S.cn[i] = cn;
-            S.kt[i] = kt;
-            S.ct[i] = ct;
-        } else {
-            kn = S.kn[i];
-            cn = S.cn[i];
-            kt = S.kt[i];
-            ct = S.ct[i];
-        }
-    }
-    if (!forces) return;  // warp-uniform
-    // 2) normal and tangential forces from non-fluid neighbours within dx
-    double fN[3] = {0.0, 0.0, 0.0}, fT[3] = {0.0, 0.0, 0.0};
-    const double mu_f = P.friction[ti];
-    traverse_stencil(P, S.cell_start, key_cell, lane, active, 6u, stage, [&](int j, int s) {
-        if (j == i) return;
-        const double q[3] = {rel1(tl.x[s], xi, P.W[0], P.hW[0]), rel1(tl.y[s], yi, P.W[1], P.hW[1]),
-                             rel1(tl.z[s], zi, P.W[2], P.hW[2])};
-        const double r2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
-        if (r2 <= P.dx2) {
-            const double r = sqrt(r2);
-            const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
-            const double u[3] = {tl.vx[s] - vxi, tl.vy[s] - vyi, tl.vz[s] - vzi};
-            double vn[3] = {0.0, 0.0, 0.0};
-            for (int d = 0; d < 3; d++) vn[d] += u[d] * e[d];
-            for (int d = 0; d < 3; d++) fN[d] += -kn * (P.dx - r) * e[d] - (cn * vn[d] * e[d] * P.dt);
-            double vn2[3], vt[3], dtv[3] = {0.0, 0.0, 0.0}, sN[3], sT[3];
-            for (int d = 0; d < 3; d++) vn2[d] = u[d] * e[d];
-            for (int d = 0; d < 3; d++) vt[d] = u[d] - vn2[d] * e[d];
-            for (int d = 0; d < 3; d++) dtv[d] += vt[d] * P.ddt;
-            for (int d = 0; d < 3; d++) sN[d] = -kn * (P.dx - r) * e[d] - (cn * vn2[d] * e[d] * P.dt);
-            const double aFn = mu_f * sqrt(sN[0] * sN[0] + sN[1] * sN[1] + sN[2] * sN[2]);
-            for (int d = 0; d < 3; d++) sT[d] = -kt * dtv[d] - (ct * vt[d]);
-            const double aFt = sqrt(sT[0] * sT[0] + sT[1] * sT[1] + sT[2] * sT[2]);
-            if (aFn > aFt) {
-                for (int d = 0; d < 3; d++) fT[d] += -kt * dtv[d] - (ct * vt[d]);
+    FOR_EACH_CHUNK(dB, range, kWarpsPerBlock, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        const int ii = active ? i : ch.i0;
+        const int ti = S.type[ii];
+        const double xi = S.pos[ii], yi = S.pos[N + ii], zi = S.pos[2 * N + ii];
+        const double vxi = S.vel[ii], vyi = S.vel[N + ii], vzi = S.vel[2 * N + ii];
+        auto stage = [&](int j, int slot) {
+            const int t = S.type[j];
+            if (MIXED && is_fluid(t)) {
+                const float4 p = S.p4[j];
+                const float4 v = S.v4[j];
+                const unsigned w = __float_as_uint(p.w);
+                tl.x[slot] = P.dmin[0] + unpack_cx(w) * P.cw[0] + (double)p.x;
+                tl.y[slot] = P.dmin[1] + unpack_cy(w) * P.cw[1] + (double)p.y;
+                tl.z[slot] = P.dmin[2] + unpack_cz(w) * P.cw[2] + (double)p.z;
+                tl.vx[slot] = v.x;
+                tl.vy[slot] = v.y;
+                tl.vz[slot] = v.z;
             } else {
-                const double avt = sqrt(vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]);
-                if (avt != 0)
-                    for (int d = 0; d < 3; d++) fT[d] += aFn * vt[d] / avt;
+                tl.x[slot] = S.pos[j];
+                tl.y[slot] = S.pos[N + j];
+                tl.z[slot] = S.pos[2 * N + j];
+                tl.vx[slot] = S.vel[j];
+                tl.vy[slot] = S.vel[N + j];
+                tl.vz[slot] = S.vel[2 * N + j];
+            }
+            tl.t[slot] = t;
+        };
+        // 1) last neighbour within dx
+        int tlast = -1;
+        double r2last = 0.0;
+        traverse_stencil(P, S.cell_start, key_cell, lane, active, 7u, stage, [&](int j, int s) {
+            if (j == i) return;
+            const double q0 = rel1(tl.x[s], xi, P.W[0], P.hW[0]);
+            const double q1 = rel1(tl.y[s], yi, P.W[1], P.hW[1]);
+            const double q2 = rel1(tl.z[s], zi, P.W[2], P.hW[2]);
+            const double r2 = (q0 * q0 + q1 * q1 + q2 * q2);
+            if (r2 <= P.dx2) {
+                tlast = tl.t[s];
+                r2last = r2;
+            }
+        });
+        double kn, cn, kt, ct;
+        if (active) {
+            if (tlast >= 0) {
+                const double r = sqrt(r2last);
+                const double ov = fmax(0.0, P.dx - r);
+                kn = (4.0 / 3.0) * P.Eeff[ti][tlast] * sqrt(P.Reff * ov);
+                const double mi = P.mass[ti], mj = P.mass[tlast];
+                const double mij = mi * mj / (mi + mj);
+                cn = -2.0 * sqrt(mij * kn) * P.logE[ti] / P.cnDen[ti];
+                kt = P.KtFac[ti][tlast] * sqrt(P.Reff * sqrt(ov));
+                ct = P.ctFac[ti] * sqrt(mij * kt);
+                S.kn[i] = kn;
+                S.cn[i] = cn;
+                S.kt[i] = kt;
+                S.ct[i] = ct;
+            } else {
+                kn = S.kn[i];
+                cn = S.cn[i];
+                kt = S.kt[i];
+                ct = S.ct[i];
             }
         }
-    });
-    if (!active) return;
-    for (int d = 0; d < 3; d++) {
-        double F = S.frc[d * N + i];
-        F += fN[d];
-        F += fT[d];
-        S.frc[d * N + i] = F;
+        if (!forces) continue;  // warp-uniform
+        // 2) normal and tangential forces from non-fluid neighbours within dx
+        double fN[3] = {0.0, 0.0, 0.0}, fT[3] = {0.0, 0.0, 0.0};
+        const double mu_f = P.friction[ti];
+        traverse_stencil(P, S.cell_start, key_cell, lane, active, 6u, stage, [&](int j, int s) {
+            if (j == i) return;
+            const double q[3] = {rel1(tl.x[s], xi, P.W[0], P.hW[0]), rel1(tl.y[s], yi, P.W[1], P.hW[1]),
+                                 rel1(tl.z[s], zi, P.W[2], P.hW[2])};
+            const double r2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+            if (r2 <= P.dx2) {
+                const double r = sqrt(r2);
+                const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
+                const double u[3] = {tl.vx[s] - vxi, tl.vy[s] - vyi, tl.vz[s] - vzi};
+                double vn[3] = {0.0, 0.0, 0.0};
+                for (int d = 0; d < 3; d++) vn[d] += u[d] * e[d];
+                for (int d = 0; d < 3; d++) fN[d] += -kn * (P.dx - r) * e[d] - (cn * vn[d] * e[d] * P.dt);
+                double vn2[3], vt[3], dtv[3] = {0.0, 0.0, 0.0}, sN[3], sT[3];
+                for (int d = 0; d < 3; d++) vn2[d] = u[d] * e[d];
+                for (int d = 0; d < 3; d++) vt[d] = u[d] - vn2[d] * e[d];
+                for (int d = 0; d < 3; d++) dtv[d] += vt[d] * P.ddt;
+                for (int d = 0; d < 3; d++) sN[d] = -kn * (P.dx - r) * e[d] - (cn * vn2[d] * e[d] * P.dt);
+                const double aFn = mu_f * sqrt(sN[0] * sN[0] + sN[1] * sN[1] + sN[2] * sN[2]);
+                for (int d = 0; d < 3; d++) sT[d] = -kt * dtv[d] - (ct * vt[d]);
+                const double aFt = sqrt(sT[0] * sT[0] + sT[1] * sT[1] + sT[2] * sT[2]);
+                if (aFn > aFt) {
+                    for (int d = 0; d < 3; d++) fT[d] += -kt * dtv[d] - (ct * vt[d]);
+                } else {
+                    const double avt = sqrt(vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]);
+                    if (avt != 0)
+                        for (int d = 0; d < 3; d++) fT[d] += aFn * vt[d] / avt;
+                }
+            }
+        });
+        if (!active) continue;
+        for (int d = 0; d < 3; d++) {
+            double F = S.frc[d * N + i];
+            F += fN[d];
+            F += fT[d];
+            S.frc[d * N + i] = F;
+        }
     }
 }
 
 // calculateAcceleration :2832-2843 over the fluid slots [b, e).  A kernel of
 // its own: pass B reads the velocities of neighbouring particles, so they may
 // only change once every force of the step is known.
-__global__ void k_fluid_accel(DevParams P, DevState S, int b, int e)
+__global__ void k_fluid_accel(DevParams P, DevState S, const int *dB)
 {
     const int N = P.N;
-    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= e) return;
-    const double m = P.mass[S.type[i]];
-    for (int d = 0; d < 3; d++) S.vel[d * N + i] += S.frc[d * N + i] / m * P.dt;
+    FOR_EACH_SLOT(dB, -1, B_FE, i)
+    {
+        const double m = P.mass[S.type[i]];
+        for (int d = 0; d < 3; d++) S.vel[d * N + i] += S.frc[d * N + i] / m * P.dt;
+    }
 }
 
 // calculateDEMconvection :1872-1891 over the solid slots [b, e)
-__global__ void k_dem_integrate(DevParams P, DevState S, int b, int e)
+__global__ void k_dem_integrate(DevParams P, DevState S, const int *dB)
 {
     const int N = P.N;
-    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= e) return;
-    const double m = P.mass[S.type[i]];
-    for (int d = 0; d < 3; d++) {
-        double v = S.vel[d * N + i];
-        v += S.frc[d * N + i] / m * P.ddt;
-        S.vel[d * N + i] = v;
-        S.pos[d * N + i] += v * P.ddt;
+    FOR_EACH_SLOT(dB, B_SB, B_SE, i)
+    {
+        const double m = P.mass[S.type[i]];
+        for (int d = 0; d < 3; d++) {
+            double v = S.vel[d * N + i];
+            v += S.frc[d * N + i] / m * P.ddt;
+            S.vel[d * N + i] = v;
+            S.pos[d * N + i] += v * P.ddt;
+        }
     }
 }
 
@@ -523,79 +525,79 @@ __global__ void k_dem_integrate(DevParams P, DevState S, int b, int e)
 // NeighborCount / SolidNeighborCount of calculateNeighbor :1546-1678 (counts
 // of particles within MaxRadius+MARGIN at rebuild time, self included; the
 // rebuild-time positions are kept in xref).
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_counts(DevParams P, DevState S, int chunk_begin,
-                                                                   int chunk_end)
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_counts(DevParams P, DevState S, const int *dB, int range)
 {
     __shared__ TileA tiles[kWarpsPerBlock];
     TileA &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int N = P.N;
-    const int cidx = chunk_begin + blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-    if (cidx >= chunk_end) return;
-    const Chunk ch = S.chunks[cidx];
-    const int i = ch.i0 + lane;
-    const bool active = lane < ch.cnt;
-    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-    const int ii = active ? i : ch.i0;
-    const double xi = S.xref[ii], yi = S.xref[N + ii], zi = S.xref[2 * N + ii];
-    int cnt = 0, scnt = 0;
-    traverse_stencil(
-        P, S.cell_start, key_cell, lane, active, 7u,
-        [&](int j, int slot) {
-            tl.x[slot] = S.xref[j];
-            tl.y[slot] = S.xref[N + j];
-            tl.z[slot] = S.xref[2 * N + j];
-            tl.t[slot] = S.type[j];
-        },
-        [&](int j, int s) {
-            const double q0 = rel1(tl.x[s], xi, P.W[0], P.hW[0]);
-            const double q1 = rel1(tl.y[s], yi, P.W[1], P.hW[1]);
-            const double q2 = rel1(tl.z[s], zi, P.W[2], P.hW[2]);
-            const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
-            if (r2 <= P.rc2) {
-                cnt++;
-                if (is_solid(tl.t[s])) scnt++;
-            }
-        });
-    if (!active) return;
-    S.nc[i] = cnt;
-    S.snc[i] = scnt;
+    FOR_EACH_CHUNK(dB, range, kWarpsPerBlock, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        const int ii = active ? i : ch.i0;
+        const double xi = S.xref[ii], yi = S.xref[N + ii], zi = S.xref[2 * N + ii];
+        int cnt = 0, scnt = 0;
+        traverse_stencil(
+            P, S.cell_start, key_cell, lane, active, 7u,
+            [&](int j, int slot) {
+                tl.x[slot] = S.xref[j];
+                tl.y[slot] = S.xref[N + j];
+                tl.z[slot] = S.xref[2 * N + j];
+                tl.t[slot] = S.type[j];
+            },
+            [&](int j, int s) {
+                const double q0 = rel1(tl.x[s], xi, P.W[0], P.hW[0]);
+                const double q1 = rel1(tl.y[s], yi, P.W[1], P.hW[1]);
+                const double q2 = rel1(tl.z[s], zi, P.W[2], P.hW[2]);
+                const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
+                if (r2 <= P.rc2) {
+                    cnt++;
+                    if (is_solid(tl.t[s])) scnt++;
+                }
+            });
+        if (!active) continue;
+        S.nc[i] = cnt;
+        S.snc[i] = scnt;
+    }
 }
 
 // Fill pass of the CSR neighbour list (calculateNeighbor :1725-1840); ptr
 // holds the exclusive scan of NeighborCount.
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_neighbor_fill(DevParams P, DevState S, int chunk_begin,
-                                                                          int chunk_end, const long long *ptr,
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_neighbor_fill(DevParams P, DevState S, const int *dB, int range, const long long *ptr,
                                                                           int *ind)
 {
     __shared__ TileA tiles[kWarpsPerBlock];
     TileA &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int N = P.N;
-    const int cidx = chunk_begin + blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-    if (cidx >= chunk_end) return;
-    const Chunk ch = S.chunks[cidx];
-    const int i = ch.i0 + lane;
-    const bool active = lane < ch.cnt;
-    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-    const int ii = active ? i : ch.i0;
-    const double xi = S.xref[ii], yi = S.xref[N + ii], zi = S.xref[2 * N + ii];
-    long long w = active ? ptr[i] : 0;
-    const long long wend = active ? ptr[i + 1] : 0;
-    traverse_stencil(
-        P, S.cell_start, key_cell, lane, active, 7u,
-        [&](int j, int slot) {
-            tl.x[slot] = S.xref[j];
-            tl.y[slot] = S.xref[N + j];
-            tl.z[slot] = S.xref[2 * N + j];
-        },
-        [&](int j, int s) {
-            const double q0 = rel1(tl.x[s], xi, P.W[0], P.hW[0]);
-            const double q1 = rel1(tl.y[s], yi, P.W[1], P.hW[1]);
-            const double q2 = rel1(tl.z[s], zi, P.W[2], P.hW[2]);
-            const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
-            if (r2 <= P.rc2 && w < wend) ind[w++] = j;
-        });
+    FOR_EACH_CHUNK(dB, range, kWarpsPerBlock, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        const int ii = active ? i : ch.i0;
+        const double xi = S.xref[ii], yi = S.xref[N + ii], zi = S.xref[2 * N + ii];
+        long long w = active ? ptr[i] : 0;
+        const long long wend = active ? ptr[i + 1] : 0;
+        traverse_stencil(
+            P, S.cell_start, key_cell, lane, active, 7u,
+            [&](int j, int slot) {
+                tl.x[slot] = S.xref[j];
+                tl.y[slot] = S.xref[N + j];
+                tl.z[slot] = S.xref[2 * N + j];
+            },
+            [&](int j, int s) {
+                const double q0 = rel1(tl.x[s], xi, P.W[0], P.hW[0]);
+                const double q1 = rel1(tl.y[s], yi, P.W[1], P.hW[1]);
+                const double q2 = rel1(tl.z[s], zi, P.W[2], P.hW[2]);
+                const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
+                if (r2 <= P.rc2 && w < wend) ind[w++] = j;
+            });
+    }
 }
 
 // launch helpers (host side of this translation unit)
@@ -610,41 +612,48 @@ void launch_drift(const DevParams &P, const DevState &S, const WallMotion &Wm, u
     k_drift<<<blocks, threads, 0, st>>>(P, S, Wm, maxshift);
 }
 
-static inline int chunk_blocks(int b, int e) { return (e - b + kWarpsPerBlock - 1) / kWarpsPerBlock; }
+constexpr int kBlock = kWarpsPerBlock * kWarp;
+constexpr int kElemGrid = 148 * 4;
 
-void launch_pass_a(const DevParams &P, const DevState &S, int cb, int ce, int init_only, cudaStream_t st)
+void launch_pass_a(const DevParams &P, const DevState &S, const int *dB, int range, int init_only, cudaStream_t st)
 {
-    if (ce > cb) k_pass_a<<<chunk_blocks(cb, ce), kWarpsPerBlock * kWarp, 0, st>>>(P, S, cb, ce, init_only);
+    static const int g = persistent_grid((const void *)k_pass_a, kBlock);
+    k_pass_a<<<g, kBlock, 0, st>>>(P, S, dB, range, init_only);
 }
-void launch_pass_b(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st)
+void launch_pass_b(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
 {
-    if (ce > cb) k_pass_b<<<chunk_blocks(cb, ce), kWarpsPerBlock * kWarp, 0, st>>>(P, S, cb, ce);
+    static const int g = persistent_grid((const void *)k_pass_b, kBlock);
+    k_pass_b<<<g, kBlock, 0, st>>>(P, S, dB, CR_FLUID_SOLID);
 }
-void launch_dem_force(const DevParams &P, const DevState &S, int cb, int ce, int forces, cudaStream_t st, bool mixed)
+void launch_dem_force(const DevParams &P, const DevState &S, const int *dB, int range, int forces, cudaStream_t st,
+                      bool mixed)
 {
-    if (ce <= cb) return;
-    if (mixed)
-        k_dem_force<true><<<chunk_blocks(cb, ce), kWarpsPerBlock * kWarp, 0, st>>>(P, S, cb, ce, forces);
-    else
-        k_dem_force<false><<<chunk_blocks(cb, ce), kWarpsPerBlock * kWarp, 0, st>>>(P, S, cb, ce, forces);
+    if (mixed) {
+        static const int g = persistent_grid((const void *)k_dem_force<true>, kBlock);
+        k_dem_force<true><<<g, kBlock, 0, st>>>(P, S, dB, range, forces);
+    } else {
+        static const int g = persistent_grid((const void *)k_dem_force<false>, kBlock);
+        k_dem_force<false><<<g, kBlock, 0, st>>>(P, S, dB, range, forces);
+    }
 }
-void launch_fluid_accel(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st)
+void launch_fluid_accel(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
 {
-    if (e > b) k_fluid_accel<<<(e - b + 255) / 256, 256, 0, st>>>(P, S, b, e);
+    k_fluid_accel<<<kElemGrid, 256, 0, st>>>(P, S, dB);
 }
-void launch_dem_integrate(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st)
+void launch_dem_integrate(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
 {
-    if (e > b) k_dem_integrate<<<(e - b + 127) / 128, 128, 0, st>>>(P, S, b, e);
+    k_dem_integrate<<<kElemGrid / 4, 256, 0, st>>>(P, S, dB);
 }
-void launch_counts(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st)
+void launch_counts(const DevParams &P, const DevState &S, const int *dB, int range, cudaStream_t st)
 {
-    if (ce > cb) k_counts<<<chunk_blocks(cb, ce), kWarpsPerBlock * kWarp, 0, st>>>(P, S, cb, ce);
+    static const int g = persistent_grid((const void *)k_counts, kBlock);
+    k_counts<<<g, kBlock, 0, st>>>(P, S, dB, range);
 }
-void launch_neighbor_fill(const DevParams &P, const DevState &S, int cb, int ce, const long long *ptr, int *ind,
+void launch_neighbor_fill(const DevParams &P, const DevState &S, const int *dB, const long long *ptr, int *ind,
                           cudaStream_t st)
 {
-    if (ce > cb)
-        k_neighbor_fill<<<chunk_blocks(cb, ce), kWarpsPerBlock * kWarp, 0, st>>>(P, S, cb, ce, ptr, ind);
+    static const int g = persistent_grid((const void *)k_neighbor_fill, kBlock);
+    k_neighbor_fill<<<g, kBlock, 0, st>>>(P, S, dB, CR_ALL, ptr, ind);
 }
 
 }  // namespace dmph

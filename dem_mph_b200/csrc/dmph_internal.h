@@ -21,41 +21,51 @@ int launch_exclusive_scan(const T *in, T *out, int n, T *block_sums, T *total, c
 void launch_chunks(const DevParams &P, const unsigned long long *words, const int *start, int *flag, int *offs,
                    int *block_sums, int *total, Chunk *chunks, cudaStream_t st);
 void launch_widen(const int *in, long long *out, int n, cudaStream_t st);
+void launch_bounds(const DevParams &P, const int *start, const int *offs, const int *total, int *dB, cudaStream_t st);
+void launch_wet_partition(const DevParams &P, const unsigned long long *words, const int *start, Chunk *chunks,
+                          Chunk *tmp, int *dB, int *flag, int *offs, int *block_sums, int *total, cudaStream_t st);
+void launch_decide(const DevParams &P, const unsigned long long *maxshift, int *dB, unsigned long long graph_cond,
+                   cudaStream_t st);
 
 // dmph_f64.cu
 void launch_drift(const DevParams &P, const DevState &S, const WallMotion &Wm, unsigned long long *maxshift, int sms,
                   cudaStream_t st);
-void launch_pass_a(const DevParams &P, const DevState &S, int cb, int ce, int init_only, cudaStream_t st);
-void launch_pass_b(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st);
-void launch_fluid_accel(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st);
-void launch_dem_force(const DevParams &P, const DevState &S, int cb, int ce, int forces, cudaStream_t st,
+void launch_pass_a(const DevParams &P, const DevState &S, const int *dB, int range, int init_only, cudaStream_t st);
+void launch_pass_b(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
+void launch_fluid_accel(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
+void launch_dem_force(const DevParams &P, const DevState &S, const int *dB, int range, int forces, cudaStream_t st,
                       bool mixed = false);
-void launch_dem_integrate(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st);
-void launch_counts(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st);
-void launch_neighbor_fill(const DevParams &P, const DevState &S, int cb, int ce, const long long *ptr, int *ind,
+void launch_dem_integrate(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
+void launch_counts(const DevParams &P, const DevState &S, const int *dB, int range, cudaStream_t st);
+void launch_neighbor_fill(const DevParams &P, const DevState &S, const int *dB, const long long *ptr, int *ind,
                           cudaStream_t st);
 
 // dmph_f32.cu
 DevParams32 make_params32(const DevParams &P);
 void launch_drift32(const DevParams &P, const DevParams32 &Q, const DevState &S, const WallMotion &Wm,
                     unsigned long long *maxshift, int sms, cudaStream_t st);
-void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, cudaStream_t st);
-void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, int cb, int ce, cudaStream_t st);
-void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, int b, int e, cudaStream_t st);
+void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int range,
+                     cudaStream_t st);
+void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
+void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
 void launch_export32(const DevParams &P, const DevState &S, double *pos, double *vel, cudaStream_t st);
 void launch_import32(const DevParams &P, const DevState &S, const double *pos, const double *vel, cudaStream_t st);
 void launch_permute32(const DevParams &P, const unsigned long long *words, const double *xabs, const float4 *v_in,
                       const int *type_in, const int *pidx_in, float4 *p_out, float4 *v_out, int *type_out,
                       int *pidx_out, double *xref, float4 *xref4, const int *bid_in, int *bid_out, const double *vabs,
                       double *pos_out, double *vel_out, cudaStream_t st);
-void launch_solid_force_to64(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st);
-void launch_sync_solids32(const DevParams &P, const DevState &S, int b, int e, cudaStream_t st);
+void launch_solid_force_to64(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
+void launch_sync_solids32(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
+double lattice_n0p32(const DevParams &P, const DevParams32 &Q, cudaStream_t st);
 void launch_widen_f(const float *in, double *out, int n, cudaStream_t st);
 void launch_widen_f4(const float4 *in, double *out, int count, int stride, cudaStream_t st);
 
 // dmph_bodies.cu
 void launch_slot_of_row(const DevParams &P, const int *pidx, int *slot_of_row, cudaStream_t st);
-void launch_clump_dem(const DevParams &P, const DevState &S, int cb, int ce, cudaStream_t st);
+void launch_clump_dem(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 void launch_body_step(const DevParams &P, const DevState &S, const DevBodies &Bd, bool f32, cudaStream_t st);
+
+void launch_xyz_to_planes(const double *xyz, double *planes, int n, cudaStream_t st);
+void launch_planes_to_xyz(const double *planes, double *xyz, int n, cudaStream_t st);
 
 }  // namespace dmph

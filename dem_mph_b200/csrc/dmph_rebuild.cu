@@ -293,6 +293,114 @@ void launch_chunks(const DevParams &P, const unsigned long long *words, const in
     k_chunk_write<<<(P.N + 255) / 256, 256, 0, st>>>(P, words, start, flag, offs, chunks);
 }
 
+// Device-side bounds after the chunk build: slot ranges of the classes from
+// cell_start, chunk ranges from the chunk-head scan (offs[i] = chunks before
+// slot i).  One thread.
+__global__ void k_bounds(DevParams P, const int *__restrict__ start, const int *__restrict__ offs,
+                         const int *__restrict__ total, int *__restrict__ dB)
+{
+    const int N = P.N;
+    const int sb = start[P.T], wb = start[2 * P.T], nch = *total;
+    dB[B_FE] = sb;
+    dB[B_SB] = sb;
+    dB[B_SE] = wb;
+    dB[B_CH_S0] = sb < N ? offs[sb] : nch;
+    dB[B_CH_W0] = wb < N ? offs[wb] : nch;
+    dB[B_CH_END] = nch;
+    dB[B_CH_WET] = nch;
+}
+
+// Wall chunks whose 27-cell stencil holds no fluid particle ("dry" walls):
+// their pressure is read only by fluid neighbours, and no fluid particle can
+// come within reach before the next rebuild (the stencil covers every pair
+// within MaxRadius+MARGIN at the rebuild, and the trigger keeps every pair
+// that is within RadiusP now inside that radius), so the FP32 build skips
+// them in pass A.  flag[k] = 1 for wet wall chunk ch_w0 + k, 0 beyond the
+// wall chunks (the scan runs over n slots).
+__global__ void k_wet_flags(DevParams P, const unsigned long long *__restrict__ words,
+                            const int *__restrict__ start, const Chunk *__restrict__ chunks, const int *__restrict__ dB,
+                            int n, int *__restrict__ flag)
+{
+    const int cb = dB[B_CH_W0], ce = dB[B_CH_END];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int wet = 0;
+        if (cb + k < ce) {
+            const int kc = (int)(word_key(words[chunks[cb + k].i0]) % (unsigned)P.T);
+            const int ns = stencil_size(P);
+            for (int s = 0; s < ns && !wet; s++) {
+                const int cell = stencil_cell(P, kc, s);
+                wet = start[cell + 1] > start[cell];  // fluid keys are [0, T)
+            }
+        }
+        flag[k] = wet;
+    }
+}
+
+// stable partition of the wall chunks: wet first, then dry (into tmp)
+__global__ void k_partition_chunks(const Chunk *__restrict__ in, Chunk *__restrict__ tmp, const int *__restrict__ dB,
+                                   const int *__restrict__ flag, const int *__restrict__ offs,
+                                   const int *__restrict__ total)
+{
+    const int cb = dB[B_CH_W0], n = dB[B_CH_END] - cb, nwet = *total;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int dst = flag[k] ? offs[k] : nwet + (k - offs[k]);
+        tmp[cb + dst] = in[cb + k];
+    }
+}
+__global__ void k_copy_chunks(const Chunk *__restrict__ tmp, Chunk *__restrict__ out, int *__restrict__ dB,
+                              const int *__restrict__ total)
+{
+    const int cb = dB[B_CH_W0], n = dB[B_CH_END] - cb;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) out[cb + k] = tmp[cb + k];
+    if (blockIdx.x == 0 && threadIdx.x == 0) dB[B_CH_WET] = cb + *total;
+}
+
+// rebuild decision of neighborCalculation (:1276-1285) from the reduced max
+// displacement: max |dx|^2 > (0.5 MARGIN)^2
+__global__ void k_decide(const unsigned long long *maxshift, double threshold, int *dB)
+{
+    const double m2 = __longlong_as_double((long long)*maxshift);
+    const int need = m2 > threshold ? 1 : 0;
+    dB[B_NEED] = need;
+    dB[B_REBUILDS] += need;
+}
+// same, inside a CUDA graph: also sets the condition of the graph's rebuild node
+__global__ void k_decide_graph(const unsigned long long *maxshift, double threshold, int *dB,
+                               cudaGraphConditionalHandle cond)
+{
+    const double m2 = __longlong_as_double((long long)*maxshift);
+    const int need = m2 > threshold ? 1 : 0;
+    dB[B_NEED] = need;
+    dB[B_REBUILDS] += need;
+    cudaGraphSetConditional(cond, need ? 1u : 0u);
+}
+
+void launch_decide(const DevParams &P, const unsigned long long *maxshift, int *dB, unsigned long long graph_cond,
+                   cudaStream_t st)
+{
+    const double margin = (0.1 * P.dx);
+    const double thr = 0.5 * margin * 0.5 * margin;  // :1278
+    if (graph_cond)
+        k_decide_graph<<<1, 1, 0, st>>>(maxshift, thr, dB, (cudaGraphConditionalHandle)graph_cond);
+    else
+        k_decide<<<1, 1, 0, st>>>(maxshift, thr, dB);
+}
+
+void launch_bounds(const DevParams &P, const int *start, const int *offs, const int *total, int *dB, cudaStream_t st)
+{
+    k_bounds<<<1, 1, 0, st>>>(P, start, offs, total, dB);
+}
+
+void launch_wet_partition(const DevParams &P, const unsigned long long *words, const int *start, Chunk *chunks,
+                          Chunk *tmp, int *dB, int *flag, int *offs, int *block_sums, int *total, cudaStream_t st)
+{
+    const int n = P.N;  // upper bound of the number of wall chunks
+    k_wet_flags<<<148 * 4, 256, 0, st>>>(P, words, start, chunks, dB, n, flag);
+    launch_exclusive_scan<int>(flag, offs, n, block_sums, total, st);
+    k_partition_chunks<<<148 * 4, 256, 0, st>>>(chunks, tmp, dB, flag, offs, total);
+    k_copy_chunks<<<148 * 4, 256, 0, st>>>(tmp, chunks, dB, total);
+}
+
 // int64 neighbour pointers for the CSR diagnostic: small enough to scan on
 // the host side of the caller; provided here as a widening copy.
 __global__ void k_widen(const int *in, long long *out, int n)
@@ -303,6 +411,39 @@ __global__ void k_widen(const int *in, long long *out, int n)
 void launch_widen(const int *in, long long *out, int n, cudaStream_t st)
 {
     if (n > 0) k_widen<<<(n + 255) / 256, 256, 0, st>>>(in, out, n);
+}
+
+// ---------------------------------------------------- host-layout transfers
+// The C ABI takes positions and velocities as x,y,z per particle; the device
+// keeps component planes.  These two kernels transpose on the device so that a
+// host transfer is one contiguous copy straight from or into the caller's
+// buffer.
+__global__ void k_xyz_to_planes(const double *__restrict__ xyz, double *__restrict__ planes, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        planes[i] = xyz[3 * (size_t)i];
+        planes[(size_t)n + i] = xyz[3 * (size_t)i + 1];
+        planes[2 * (size_t)n + i] = xyz[3 * (size_t)i + 2];
+    }
+}
+
+__global__ void k_planes_to_xyz(const double *__restrict__ planes, double *__restrict__ xyz, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        xyz[3 * (size_t)i] = planes[i];
+        xyz[3 * (size_t)i + 1] = planes[(size_t)n + i];
+        xyz[3 * (size_t)i + 2] = planes[2 * (size_t)n + i];
+    }
+}
+
+void launch_xyz_to_planes(const double *xyz, double *planes, int n, cudaStream_t st)
+{
+    if (n > 0) k_xyz_to_planes<<<(n + 255) / 256, 256, 0, st>>>(xyz, planes, n);
+}
+
+void launch_planes_to_xyz(const double *planes, double *xyz, int n, cudaStream_t st)
+{
+    if (n > 0) k_planes_to_xyz<<<(n + 255) / 256, 256, 0, st>>>(planes, xyz, n);
 }
 
 }  // namespace dmph

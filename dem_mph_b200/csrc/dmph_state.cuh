@@ -88,6 +88,9 @@ struct DevParams32 {
     float Eeff[kTypes][kTypes], KtFac[kTypes][kTypes];
     float logE[kTypes], cnDen[kTypes], ctFac[kTypes];
     float drag_pref;                     // 0.5 dx^3
+    float dwpV;                          // -2 Bp / RP * V
+    double N0p32;                        // lattice sum evaluated with the FP32 kernel arithmetic
+    float muij[kTypes][kTypes];          // C * harmonic-mean viscosity * 2 Bv / RV * V
 };
 
 // Moving-wall constants (calculateWall, source/DEM-MPH.cpp:2846-2900)

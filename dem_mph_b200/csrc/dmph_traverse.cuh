@@ -63,3 +63,44 @@ __device__ __forceinline__ void traverse_stencil(const DevParams &P, const int *
 }
 
 }  // namespace dmph
+
+namespace dmph {
+
+// Same walk as traverse_stencil, but hands each staged batch of up to 32
+// candidates to Batch(base, nb), called by every lane of the warp (active or
+// not) between the staging barriers, so the caller can first build a per-lane
+// bitmask of the candidates in range and then loop over the set bits.
+template <class Stage, class Batch>
+__device__ __forceinline__ void traverse_stencil_batched(const DevParams &P, const int *__restrict__ cell_start,
+                                                         int key_cell, int lane, unsigned class_mask, Stage &&stage,
+                                                         Batch &&batch)
+{
+    const int n = stencil_size(P);
+    const int my_id = lane < n ? stencil_cell(P, key_cell, lane) : 0;
+    const int prev = __shfl_up_sync(kFull, my_id, 1);
+    const bool run_start = lane < n && (lane == 0 || my_id != prev + 1);
+    const unsigned starts = __ballot_sync(kFull, run_start);
+    for (int cls = 0; cls < 3; cls++) {
+        if (!((class_mask >> cls) & 1u)) continue;
+        const int off = cls * P.T;
+        unsigned m = starts;
+        while (m) {
+            const int s = __ffs(m) - 1;
+            m &= m - 1;
+            const int e = m ? (__ffs(m) - 1) : n;
+            const int lo = __shfl_sync(kFull, my_id, s);
+            const int hi = __shfl_sync(kFull, my_id, e - 1);
+            const int jb = __ldg(cell_start + off + lo);
+            const int je = __ldg(cell_start + off + hi + 1);
+            for (int base = jb; base < je; base += kWarp) {
+                const int j = base + lane;
+                if (j < je) stage(j, lane);
+                __syncwarp();
+                batch(base, min(kWarp, je - base));
+                __syncwarp();
+            }
+        }
+    }
+}
+
+}  // namespace dmph

@@ -42,6 +42,7 @@ def lib():
         L.dmph_set_bodies.argtypes = [vp, C.c_int, vp, vp]
         L.dmph_get_bodies.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
         L.dmph_set_profiling.argtypes = [vp, C.c_int]
+        L.dmph_set_graph.argtypes = [vp, C.c_int]
         L.dmph_get_phase_times.argtypes = [vp, vp, vp, C.c_int]
         L.dmph_destroy.argtypes = [vp]
         L.dmph_last_error.argtypes = [vp]
@@ -89,12 +90,18 @@ class Solver:
         self._check(lib().dmph_step_timed(self._h, n, C.byref(ms)))
         return ms.value
 
-    def state(self):
-        """(type, x[N,3], v[N,3], orig_id) in the current sorted order"""
-        t = np.empty(self.n, np.int32)
-        x = np.empty((self.n, 3), np.float64)
-        v = np.empty((self.n, 3), np.float64)
-        o = np.empty(self.n, np.int32)
+    def state(self, out=None):
+        """(type, x[N,3], v[N,3], orig_id) in the current sorted order.  `out`
+        may give the four arrays to fill (e.g. page-locked host buffers, which
+        the copies then reach at full link speed)."""
+        if out is None:
+            out = (np.empty(self.n, np.int32), np.empty((self.n, 3), np.float64),
+                   np.empty((self.n, 3), np.float64), np.empty(self.n, np.int32))
+        t, x, v, o = out
+        for a, dt, shape in ((t, np.int32, (self.n,)), (x, np.float64, (self.n, 3)),
+                             (v, np.float64, (self.n, 3)), (o, np.int32, (self.n,))):
+            if a.dtype != dt or a.shape != shape or not a.flags.c_contiguous:
+                raise ValueError("state(out=...) wants C-contiguous %s arrays of shape %s" % (np.dtype(dt), shape))
         self._check(lib().dmph_get_state(self._h, _ptr(t), _ptr(x), _ptr(v), _ptr(o)))
         return t, x, v, o
 
@@ -140,6 +147,10 @@ class Solver:
         return out
 
     PHASES = ("drift", "rebuild", "pass_a", "pass_b", "dem", "bodies")
+
+    def set_graph(self, on=True):
+        """replay each step as one CUDA graph (see dmph_set_graph)"""
+        self._check(lib().dmph_set_graph(self._h, 1 if on else 0))
 
     def set_profiling(self, on=True):
         self._check(lib().dmph_set_profiling(self._h, 1 if on else 0))

@@ -233,6 +233,14 @@ int dmph_set_bodies(dmph_ctx *ctx, int nbodies, const int *body_of_row, const do
  * F,T 3 per body (total force and torque of the last substep). */
 int dmph_get_bodies(dmph_ctx *ctx, double *X, double *V, double *q, double *L, double *mass, double *F, double *T);
 
+/* Record a step as one CUDA graph and replay it (enable != 0): the rebuild
+ * decision is taken on the device and the neighbour rebuild runs as the body
+ * of a conditional graph node, so steps need no host synchronisation.  Steps
+ * that cannot use the recorded graph (Time <= 0, the moving-wall window
+ * 0.2 <= Time <= 0.4 of calculateWall :2857, or profiling on) fall back to
+ * individual launches.  Results are identical either way. */
+int dmph_set_graph(dmph_ctx *ctx, int enable);
+
 /* Per-phase device timing.  With enable != 0, every following step records
  * CUDA events on the context's stream around each phase (this adds event
  * overhead, so time throughput with it off); dmph_get_phase_times returns the

@@ -533,6 +533,8 @@ static void drag_force(dmph_oracle *o)
 
 /* calculatePressureP :2200-2246 (solids neither get a pressure nor a
  * pressure force; their PressureP is never written and stays 0) */
+static void pressure_force(dmph_oracle *o, const double *P, double *F, double *fsc);
+
 static void pressure_p(dmph_oracle *o)
 {
 #pragma omp parallel for
@@ -540,6 +542,13 @@ static void pressure_p(dmph_oracle *o)
         if (is_solid(o->prop[i])) continue;
         o->P[i] = -o->lambda[i] * o->div[i] + o->kappa[i] * o->vsp[i];
     }
+    pressure_force(o, o->P, o->F, o->fsc);
+}
+
+/* the pressure-gradient force of calculatePressureP :2213-2246 for a given
+ * pressure field, added to F (and its term magnitudes to fsc when non-NULL) */
+static void pressure_force(dmph_oracle *o, const double *P, double *F, double *fsc)
+{
 #pragma omp parallel for
     for (int i = 0; i < o->N; i++) {
         const int ti = o->prop[i];
@@ -559,11 +568,11 @@ static void pressure_p(dmph_oracle *o)
                 const double r = sqrt(r2);
                 const double dw = k_dw(r, o->Bp, o->RP);
                 const double g[3] = {dw * q[0] / r, dw * q[1] / r, dw * q[2] / r};
-                for (int d = 0; d < 3; d++) f[d] += (o->P[i] + o->P[j]) * g[d] * o->V;
-                o->fsc[i] += fabs((o->P[i] + o->P[j]) * dw * o->V);
+                for (int d = 0; d < 3; d++) f[d] += (P[i] + P[j]) * g[d] * o->V;
+                if (fsc) fsc[i] += fabs((P[i] + P[j]) * dw * o->V);
             }
         }
-        for (int d = 0; d < 3; d++) o->F[3 * i + d] += f[d];
+        for (int d = 0; d < 3; d++) F[3 * i + d] += f[d];
     }
 }
 
@@ -1310,6 +1319,14 @@ static int inv3(const double *a, double *out)
     out[6] = c02 * id;
     out[7] = (a[1] * a[6] - a[0] * a[7]) * id;
     out[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+    return 0;
+}
+
+int dmph_oracle_pressure_force(dmph_oracle *o, const double *P, double *F)
+{
+    if (!o || !P || !F) return -1;
+    memset(F, 0, sizeof(double) * 3 * (size_t)o->N);
+    pressure_force(o, P, F, NULL);
     return 0;
 }
 

@@ -34,6 +34,9 @@ int dmph_oracle_get(dmph_oracle *o, const char *name, void *out);
 double dmph_oracle_scalar(dmph_oracle *o, const char *name);
 /* rigid debris bodies (the library's DMPH_FLAG_RIGID_CLUMPS mode; no
  * reference counterpart): same model as dmph_set_bodies, restated in FP64 */
+/* Pressure-gradient force (calculatePressureP :2213-2246) of a given pressure
+ * field on the current positions and neighbour lists, written to F[3N]. */
+int dmph_oracle_pressure_force(dmph_oracle *o, const double *P, double *F);
 int dmph_oracle_set_bodies(dmph_oracle *o, int nbodies, const int *body_of_row, const double *body_density);
 /* X,V,L 3 per body, q 4 per body, M 1 per body (any may be NULL) */
 int dmph_oracle_get_bodies(dmph_oracle *o, double *X, double *V, double *q, double *L, double *M);

@@ -38,6 +38,7 @@ def lib():
         L.dmph_oracle_destroy.argtypes = [C.c_void_p]
         L.dmph_oracle_set_bodies.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.dmph_oracle_get_bodies.argtypes = [C.c_void_p] + [C.c_void_p] * 5
+        L.dmph_oracle_pressure_force.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -93,6 +94,16 @@ class Oracle:
         lib().dmph_oracle_get_bodies(self._h, out["X"].ctypes.data, out["V"].ctypes.data, out["q"].ctypes.data,
                                      out["L"].ctypes.data, out["M"].ctypes.data)
         return out
+
+    def pressure_force(self, pressure):
+        """pressure-gradient force [N,3] of the given pressure field on the
+        current positions and neighbour lists"""
+        P = np.ascontiguousarray(pressure, dtype=np.float64)
+        if P.shape != (self.n,):
+            raise ValueError("pressure_force wants %d pressures" % self.n)
+        F = np.zeros((self.n, 3))
+        lib().dmph_oracle_pressure_force(self._h, P.ctypes.data, F.ctypes.data)
+        return F
 
     def scalar(self, name):
         return lib().dmph_oracle_scalar(self._h, name.encode())
