@@ -146,12 +146,13 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config2", "config1"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config1", "config3"])
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--settle", type=int, default=200,
                     help="untimed steps run before warm-up so the flow is moving and rebuilds fire in the timed steps")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels one by one instead of graph replay")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch variants of the pair passes")
     ap.add_argument("--no-bodies", action="store_true",
                     help="move debris particles individually (reference DEM) instead of as rigid bodies")
     args = ap.parse_args()
@@ -174,6 +175,8 @@ def main():
     from dem_mph_b200 import solver
     from dem_mph_b200.abi import PRECISION_FP64, PRECISION_FP32_SPLIT
 
+    if args.workload == "config3":
+        return run_ensemble(args, rank, world)
     scene = make_scene(args.workload, rank)
     p = scene.params.copy()
     p.precision = PRECISION_FP64 if args.precision == "fp64" else PRECISION_FP32_SPLIT
@@ -183,6 +186,10 @@ def main():
         g.set_bodies(scene.body, scene.body_density)
     n = scene.n
     g.step(args.settle)
+    variants = None
+    if args.precision == "fp32" and not args.no_autotune:
+        va, vb, _, _ = g.autotune()
+        variants = [va, vb]
     if not args.no_graph:
         g.set_graph(True)
     g.step(args.warmup)
@@ -284,6 +291,7 @@ def main():
                    "precision": args.precision, "dt": p.dt, "dem_substeps": inf.dem_substeps,
                    "rebuilds_in_timed_steps": rebuilds_timed - rebuilds_before, "parallelism": "replicas x%d" % world,
                    "settle_steps": args.settle, "graph_replay": not args.no_graph,
+                   "pass_variants": variants,
                    "l2": "inputs larger than L2 (particle state alone %.0f MB)" % (n * 60 / 1e6)},
         "sim_s_per_hour": p.dt * args.steps / (ms_max / 1e3) * 3600.0,
         "clocks": clk.summary(),
@@ -292,6 +300,108 @@ def main():
         "e2e": e2e,
         "gpu_launches": launches,
     }
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_ensemble(args, rank, world):
+    """Config 3: 64 independent scenes of uneven size advanced as one ensemble
+    (FP32 split, rigid bodies): pass A and pass B of all scenes are one
+    persistent launch each and a whole ensemble step is one CUDA graph."""
+    import torch
+    import torch.distributed as dist
+    from dem_mph_b200 import scenes, solver
+    from dem_mph_b200.abi import PRECISION_FP32_SPLIT
+
+    sc = scenes.config3(seed=1234 + rank)
+    sv = []
+    for s in sc:
+        p = s.params.copy()
+        p.precision = PRECISION_FP32_SPLIT
+        g = solver.Solver(p, s.type, s.x, s.v)
+        if len(s.body_density):
+            g.set_bodies(s.body, s.body_density)
+        sv.append(g)
+    ens = solver.Ensemble(sv)
+    n = sum(s.n for s in sc)
+    ens.step(args.settle)
+    variants = None
+    if not args.no_autotune:
+        va, vb, _, _ = ens.autotune()
+        variants = [va, vb]
+    ens.set_graph(not args.no_graph)
+    ens.step(args.warmup)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    barrier()
+    torch.cuda.synchronize()
+    l0 = ens.info()["kernel_launches"] + sum(g.info().kernel_launches for g in sv)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms = ens.step_timed(args.steps)
+        torch.cuda.synchronize()
+    barrier()
+    launches = ens.info()["kernel_launches"] + sum(g.info().kernel_launches for g in sv) - l0
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = n * world * args.steps / (ms_max / 1e3)
+    peaks, peak_src = load_peaks()
+    bpp = algorithmic_bytes("fp32")
+    achieved = n * bpp / (ms_max / args.steps / 1e3) / 1e9
+    # end to end: per step, upload every scene's state from pinned host memory,
+    # one ensemble step, read every scene's state back
+    host = []
+    for g in sv:
+        host.append((torch.empty(g.n, dtype=torch.int32, pin_memory=True).numpy(),
+                     torch.empty((g.n, 3), dtype=torch.float64, pin_memory=True).numpy(),
+                     torch.empty((g.n, 3), dtype=torch.float64, pin_memory=True).numpy(),
+                     torch.empty(g.n, dtype=torch.int32, pin_memory=True).numpy()))
+        g.state(out=host[-1])
+    e2e_steps = 3
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for g, h in zip(sv, host):
+            g.set_state(h[1], h[2])
+        ens.step(1)
+        for g, h in zip(sv, host):
+            g.state(out=h)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    dts = [s.params.dt for s in sc]
+    out = {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded ensemble of dam breaks, dem_mph_b200.scenes.config3)",
+        "config": {"workload": "config3_ensemble_64_scenes", "n_scenes": len(sc), "n_particles": n,
+                   "scene_particles_min": min(s.n for s in sc), "scene_particles_max": max(s.n for s in sc),
+                   "n_debris_bodies": int(sum(len(s.body_density) for s in sc)), "precision": "fp32",
+                   "dt_range": [min(dts), max(dts)], "settle_steps": args.settle,
+                   "graph_replay": not args.no_graph, "pass_variants": variants,
+                   "parallelism": "replicas x%d" % world,
+                   "l2": "inputs larger than L2 (particle state alone %.0f MB)" % (n * 60 / 1e6)},
+        "clocks": clk.summary(),
+        "roofline": {"bound": "hbm", "kernel": "whole ensemble step", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     "traffic": None, "peak_source": peak_src},
+        "cpu_baseline": None,
+        "e2e": {"value": n * world * e2e_steps / float(e2e_t.item()), "unit": "particle-steps/s",
+                "h2d_bytes_per_step": int(n * 48), "d2h_bytes_per_step": int(n * 56), "steps": e2e_steps},
+        "gpu_launches": int(launches),
+    }
+    ens.close()
+    for g in sv:
+        g.close()
     if rank == 0:
         print(json.dumps(out))
     if world > 1:

@@ -24,6 +24,7 @@ struct dmph_ctx {
     cudaStream_t st = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int sms = 148;
+    int device = 0;
     DevState S{};
     // second buffers of the permuted arrays
     double *pos2 = nullptr, *vel2 = nullptr;
@@ -42,6 +43,7 @@ struct dmph_ctx {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     long long graph_steps = 0, host_rebuilds = 0;
+    int var_a = 0, var_b = 0;  // launch variants of the FP32 pair passes (dmph_autotune)
     Chunk *chunks2 = nullptr;  // partition scratch
     int demSteps = 0;
     double time = 0.0;
@@ -79,13 +81,12 @@ static int dalloc(dmph_ctx *ctx, T **ptr, size_t count)
     return cudaMemsetAsync(p, 0, count ? count * sizeof(T) : 16, ctx->st) == cudaSuccess ? DMPH_OK : DMPH_ECUDA;
 }
 
+static void drop_graph(dmph_ctx *ctx);
+
 static void release(dmph_ctx *ctx)
 {
     if (ctx->st) cudaStreamSynchronize(ctx->st);
-    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
-    if (ctx->graph) cudaGraphDestroy(ctx->graph);
-    ctx->gexec = nullptr;
-    ctx->graph = nullptr;
+    drop_graph(ctx);
     if (ctx->st2) cudaStreamDestroy(ctx->st2);
     ctx->st2 = nullptr;
     for (void *p : ctx->allocs) cudaFree(p);
@@ -186,8 +187,8 @@ static void enqueue_head(dmph_ctx *ctx, unsigned long long graph_cond, cudaStrea
     launch_decide(P, ctx->maxshift, ctx->dB, graph_cond, st);
 }
 
-// the force passes and the DEM substeps (second part of a step)
-static void enqueue_tail(dmph_ctx *ctx, cudaStream_t st)
+// the pair passes (first part of a step's tail)
+static void enqueue_passes(dmph_ctx *ctx, cudaStream_t st)
 {
     const DevParams &P = ctx->P;
     DevState &S = ctx->S;
@@ -195,14 +196,32 @@ static void enqueue_tail(dmph_ctx *ctx, cudaStream_t st)
     if (ctx->fp32) {
         const DevParams32 &Q = ctx->Q;
         phase_begin(ctx);
-        launch_pass_a32(P, Q, S, dB, CR_WET, st);
+        launch_pass_a32(P, Q, S, dB, CR_WET, ctx->var_a, st);
         phase_end(ctx, 2);
         phase_begin(ctx);
-        launch_pass_b32(P, Q, S, dB, st);
+        launch_pass_b32(P, Q, S, dB, ctx->var_b, st);
         launch_fluid_accel32(Q, S, dB, st);
         phase_end(ctx, 3);
-        // DEM and rigid bodies in FP64 on the solids' and walls' master state
+    } else {
         phase_begin(ctx);
+        launch_pass_a(P, S, dB, CR_ALL, 0, st);
+        phase_end(ctx, 2);
+        phase_begin(ctx);
+        launch_pass_b(P, S, dB, st);
+        launch_fluid_accel(P, S, dB, st);
+        phase_end(ctx, 3);
+    }
+}
+
+// the DEM substeps or rigid bodies (second part of a step's tail)
+static void enqueue_dem(dmph_ctx *ctx, cudaStream_t st)
+{
+    const DevParams &P = ctx->P;
+    DevState &S = ctx->S;
+    const int *dB = ctx->dB;
+    phase_begin(ctx);
+    if (ctx->fp32) {
+        // DEM and rigid bodies in FP64 on the solids' and walls' master state
         launch_solid_force_to64(P, S, dB, st);
         for (int k = 0; k < ctx->demSteps; ++k) {
             if (ctx->Bd.B > 0) {
@@ -215,16 +234,7 @@ static void enqueue_tail(dmph_ctx *ctx, cudaStream_t st)
             launch_dem_integrate(P, S, dB, st);
         }
         launch_sync_solids32(P, S, dB, st);
-        phase_end(ctx, ctx->Bd.B > 0 ? 5 : 4);
     } else {
-        phase_begin(ctx);
-        launch_pass_a(P, S, dB, CR_ALL, 0, st);
-        phase_end(ctx, 2);
-        phase_begin(ctx);
-        launch_pass_b(P, S, dB, st);
-        launch_fluid_accel(P, S, dB, st);
-        phase_end(ctx, 3);
-        phase_begin(ctx);
         for (int k = 0; k < ctx->demSteps; ++k) {
             if (ctx->Bd.B > 0) {
                 launch_clump_dem(P, S, dB, st);
@@ -235,14 +245,26 @@ static void enqueue_tail(dmph_ctx *ctx, cudaStream_t st)
             if (P.wall_dem_coeffs) launch_dem_force(P, S, dB, CR_WALL, 0, st);
             launch_dem_integrate(P, S, dB, st);
         }
-        phase_end(ctx, ctx->Bd.B > 0 ? 5 : 4);
     }
+    phase_end(ctx, ctx->Bd.B > 0 ? 5 : 4);
+}
+
+// the force passes and the DEM substeps (second part of a step)
+static void enqueue_tail(dmph_ctx *ctx, cudaStream_t st)
+{
+    enqueue_passes(ctx, st);
+    enqueue_dem(ctx, st);
+}
+
+static long long dem_launches(const dmph_ctx *ctx)
+{
+    const long long dem = ctx->Bd.B > 0 ? 2 : 2 + (ctx->P.wall_dem_coeffs ? 1 : 0);
+    return ctx->demSteps * dem + (ctx->fp32 ? 2 : 0);
 }
 
 static long long tail_launches(const dmph_ctx *ctx)
 {
-    const long long dem = ctx->Bd.B > 0 ? 2 : 2 + (ctx->P.wall_dem_coeffs ? 1 : 0);
-    return 3 + ctx->demSteps * dem + (ctx->fp32 ? 2 : 0);
+    return 3 + dem_launches(ctx);
 }
 
 static void advance_host_clock(dmph_ctx *ctx)
@@ -259,19 +281,19 @@ static void advance_host_clock(dmph_ctx *ctx)
 // rebuild (its condition set on the device by the decision kernel), tail.
 // Valid while the head's parameters do not change: no moving-wall window and
 // Time > 0 (the wall centres move only while Time <= 0).
-static int build_graph(dmph_ctx *ctx)
+// Record, on a capturing stream, the head of a step followed by an IF node
+// whose body is the rebuild; the decision kernel of the head sets the
+// condition on the device.
+static int capture_head_and_rebuild(dmph_ctx *ctx, cudaGraph_t g, cudaStream_t st)
 {
-    cudaGraph_t g = nullptr;
-    CK(cudaGraphCreate(&g, 0));
     cudaGraphConditionalHandle cond;
     CK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
-    CK(cudaStreamBeginCaptureToGraph(ctx->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    enqueue_head(ctx, (unsigned long long)cond, ctx->st);
+    enqueue_head(ctx, (unsigned long long)cond, st);
     cudaStreamCaptureStatus status;
     const cudaGraphNode_t *deps = nullptr;
     size_t ndeps = 0;
     cudaGraph_t cg = nullptr;
-    CK(cudaStreamGetCaptureInfo(ctx->st, &status, nullptr, &cg, &deps, &ndeps));
+    CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &cg, &deps, &ndeps));
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = cond;
@@ -280,15 +302,41 @@ static int build_graph(dmph_ctx *ctx)
     cudaGraphNode_t cnode;
     CK(cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
-    CK(cudaStreamUpdateCaptureDependencies(ctx->st, &cnode, 1, cudaStreamSetCaptureDependencies));
+    CK(cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies));
     CK(cudaStreamBeginCaptureToGraph(ctx->st2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     enqueue_rebuild(ctx, false, ctx->st2);
     CK(cudaStreamEndCapture(ctx->st2, &body));
+    return DMPH_OK;
+}
+
+// One step recorded as a CUDA graph: head, an IF node whose body is the
+// rebuild (its condition set on the device by the decision kernel), tail.
+// Valid while the head's parameters do not change: no moving-wall window and
+// Time > 0 (the wall centres move only while Time <= 0).
+static int build_graph(dmph_ctx *ctx)
+{
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    CK(cudaStreamBeginCaptureToGraph(ctx->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int rc = capture_head_and_rebuild(ctx, g, ctx->st);
+    if (rc) {
+        cudaStreamEndCapture(ctx->st, &g);
+        cudaGraphDestroy(g);
+        return rc;
+    }
     enqueue_tail(ctx, ctx->st);
     CK(cudaStreamEndCapture(ctx->st, &g));
     CK(cudaGraphInstantiate(&ctx->gexec, g, 0));
     ctx->graph = g;
     return DMPH_OK;
+}
+
+static void drop_graph(dmph_ctx *ctx)
+{
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    if (ctx->graph) cudaGraphDestroy(ctx->graph);
+    ctx->gexec = nullptr;
+    ctx->graph = nullptr;
 }
 
 static bool graph_usable(const dmph_ctx *ctx)
@@ -396,6 +444,7 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     } while (0)
     int dev = 0;
     CKC(cudaGetDevice(&dev));
+    ctx->device = dev;
     CKC(cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, dev));
     CKC(cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking));
     CKC(cudaStreamCreateWithFlags(&ctx->st2, cudaStreamNonBlocking));
@@ -491,7 +540,7 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     if (ctx->fp32) ctx->Q.N0p32 = lattice_n0p32(P, ctx->Q, ctx->st);
     enqueue_rebuild(ctx, true, ctx->st);
     if (ctx->fp32)
-        launch_pass_a32(P, ctx->Q, ctx->S, ctx->dB, CR_ALL, ctx->st);
+        launch_pass_a32(P, ctx->Q, ctx->S, ctx->dB, CR_ALL, ctx->var_a, ctx->st);
     else
         launch_pass_a(P, S, ctx->dB, CR_ALL, 1, ctx->st);
     CKC(cudaGetLastError());
@@ -977,3 +1026,360 @@ extern "C" const char *dmph_version(void)
                                  std::to_string(__CUDACC_VER_MINOR__);
     return v.c_str();
 }
+
+// ------------------------------------------------------------- autotuner
+// Times every launch variant of a pair pass on the live state (the passes are
+// pure functions of the state they read, so repeating them changes nothing)
+// and keeps the fastest.
+template <class Launch>
+static int time_variants(dmph_ctx *ctx, cudaStream_t st, Launch &&launch, float *ms_out, int *best)
+{
+    float best_ms = 1e30f;
+    *best = 0;
+    for (int v = 0; v < kPassVariants; ++v) {
+        launch(v);  // warm-up: first launch of a variant also sizes its grid
+        CK(cudaEventRecord(ctx->ev0, st));
+        for (int r = 0; r < 3; ++r) launch(v);
+        CK(cudaEventRecord(ctx->ev1, st));
+        CK(cudaEventSynchronize(ctx->ev1));
+        CK(cudaGetLastError());
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        ms /= 3.f;
+        if (ms_out) ms_out[v] = ms;
+        if (ms < best_ms) {
+            best_ms = ms;
+            *best = v;
+        }
+    }
+    return DMPH_OK;
+}
+
+extern "C" int dmph_autotune(dmph_ctx *ctx, int *variant_a, int *variant_b, float *ms_a, float *ms_b)
+{
+    if (!ctx) return DMPH_EINVAL;
+    if (!ctx->fp32) {
+        ctx->err = "dmph_autotune: the FP64 parity build has one launch shape";
+        return DMPH_EINVAL;
+    }
+    const DevParams &P = ctx->P;
+    const DevParams32 &Q = ctx->Q;
+    int rc = time_variants(ctx, ctx->st, [&](int v) { launch_pass_a32(P, Q, ctx->S, ctx->dB, CR_WET, v, ctx->st); },
+                           ms_a, &ctx->var_a);
+    if (rc) return rc;
+    // pass A of the chosen variant last, so the pressures pass B reads are its own
+    launch_pass_a32(P, Q, ctx->S, ctx->dB, CR_WET, ctx->var_a, ctx->st);
+    rc = time_variants(ctx, ctx->st, [&](int v) { launch_pass_b32(P, Q, ctx->S, ctx->dB, v, ctx->st); }, ms_b,
+                       &ctx->var_b);
+    if (rc) return rc;
+    launch_pass_b32(P, Q, ctx->S, ctx->dB, ctx->var_b, ctx->st);
+    CK(cudaStreamSynchronize(ctx->st));
+    drop_graph(ctx);
+    if (variant_a) *variant_a = ctx->var_a;
+    if (variant_b) *variant_b = ctx->var_b;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_set_variants(dmph_ctx *ctx, int variant_a, int variant_b)
+{
+    if (!ctx) return DMPH_EINVAL;
+    if (variant_a < 0 || variant_a >= kPassVariants || variant_b < 0 || variant_b >= kPassVariants) {
+        ctx->err = "launch variant out of range";
+        return DMPH_ERANGE;
+    }
+    ctx->var_a = variant_a;
+    ctx->var_b = variant_b;
+    drop_graph(ctx);
+    return DMPH_OK;
+}
+
+// ------------------------------------------------------------- ensemble
+struct dmph_ensemble {
+    std::vector<dmph_ctx *> scenes;
+    EnsScene *tab = nullptr;  // device scene table
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> fork;  // one per scene: scene joined the ensemble stream
+    cudaEvent_t join = nullptr;
+    int var_a = 0, var_b = 0;
+    bool use_graph = true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    long long launches = 0, steps = 0, graph_steps = 0;
+    std::string err;
+    dmph_ctx *ctx0 = nullptr;  // for error strings of the helpers
+};
+
+#define EK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            e->err = std::string(#call) + ": " + cudaGetErrorString(e_);                  \
+            return DMPH_ECUDA;                                                            \
+        }                                                                                 \
+    } while (0)
+
+static void ens_drop_graph(dmph_ensemble *e)
+{
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->gexec = nullptr;
+    e->graph = nullptr;
+}
+
+static void ens_release(dmph_ensemble *e)
+{
+    if (e->st) cudaStreamSynchronize(e->st);
+    ens_drop_graph(e);
+    if (e->tab) cudaFree(e->tab);
+    for (cudaEvent_t v : e->fork) cudaEventDestroy(v);
+    if (e->join) cudaEventDestroy(e->join);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->st) cudaStreamDestroy(e->st);
+    e->tab = nullptr;
+    e->fork.clear();
+    e->join = e->ev0 = e->ev1 = nullptr;
+    e->st = nullptr;
+}
+
+extern "C" int dmph_ensemble_create(dmph_ctx *const *scenes, int nscenes, dmph_ensemble **out)
+{
+    if (!out) return DMPH_EINVAL;
+    *out = nullptr;
+    if (!scenes || nscenes <= 0 || nscenes > kMaxEnsemble) return DMPH_ERANGE;
+    int dev = -1;
+    for (int k = 0; k < nscenes; ++k) {
+        dmph_ctx *c = scenes[k];
+        if (!c || !c->fp32) return DMPH_EINVAL;  // the ensemble kernels are the FP32 split passes
+        for (int j = 0; j < k; ++j)
+            if (scenes[j] == c) return DMPH_EINVAL;
+        if (dev < 0) dev = c->device;
+        if (c->device != dev) return DMPH_EINVAL;
+    }
+    cudaSetDevice(dev);
+    dmph_ensemble *e = new dmph_ensemble();
+    e->scenes.assign(scenes, scenes + nscenes);
+    e->ctx0 = scenes[0];
+    std::vector<EnsScene> h(nscenes);
+    for (int k = 0; k < nscenes; ++k) {
+        dmph_ctx *c = scenes[k];
+        h[k].P = c->P;
+        h[k].Q = c->Q;
+        h[k].S = c->S;
+        h[k].dB = c->dB;
+    }
+    cudaError_t ce = cudaMalloc((void **)&e->tab, sizeof(EnsScene) * nscenes);
+    if (ce == cudaSuccess) ce = cudaMemcpy(e->tab, h.data(), sizeof(EnsScene) * nscenes, cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e->ev0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e->ev1);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->join, cudaEventDisableTiming);
+    e->fork.assign(nscenes, nullptr);
+    for (int k = 0; ce == cudaSuccess && k < nscenes; ++k)
+        ce = cudaEventCreateWithFlags(&e->fork[k], cudaEventDisableTiming);
+    if (ce != cudaSuccess) {
+        ens_release(e);
+        delete e;
+        return DMPH_ECUDA;
+    }
+    for (dmph_ctx *c : e->scenes) drop_graph(c);
+    *out = e;
+    return DMPH_OK;
+}
+
+// Enqueue one ensemble step.  graph_mode: the heads carry conditional rebuild
+// nodes (capture); otherwise the rebuild decisions are read on the host.
+static int ens_enqueue_step(dmph_ensemble *e, cudaGraph_t g)
+{
+    const int ns = (int)e->scenes.size();
+    // heads (and rebuilds) of every scene on its own stream
+    EK(cudaEventRecord(e->join, e->st));
+    for (int k = 0; k < ns; ++k) {
+        dmph_ctx *c = e->scenes[k];
+        c->Wm.moving = (c->time >= 0.2 && 0.4 >= c->time) ? 1 : 0;
+        EK(cudaStreamWaitEvent(c->st, e->join, 0));
+        if (g) {
+            const int rc = capture_head_and_rebuild(c, g, c->st);
+            if (rc) {
+                e->err = c->err;
+                return rc;
+            }
+        } else {
+            enqueue_head(c, 0, c->st);
+            EK(cudaMemcpyAsync(c->h_small, c->dB + B_NEED, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        }
+    }
+    if (!g) {
+        for (int k = 0; k < ns; ++k) {
+            dmph_ctx *c = e->scenes[k];
+            EK(cudaStreamSynchronize(c->st));
+            c->launches += 2;
+            if (c->h_small[0]) {
+                enqueue_rebuild(c, false, c->st);
+                c->launches += rebuild_launches(c, false);
+                c->host_rebuilds++;
+            }
+        }
+    }
+    for (int k = 0; k < ns; ++k) {
+        EK(cudaEventRecord(e->fork[k], e->scenes[k]->st));
+        EK(cudaStreamWaitEvent(e->st, e->fork[k], 0));
+    }
+    // the pair passes of all scenes: one persistent launch each
+    launch_ens_pass_a32(e->tab, ns, e->var_a, e->st);
+    launch_ens_pass_b32(e->tab, ns, e->var_b, e->st);
+    launch_ens_fluid_accel32(e->tab, ns, e->st);
+    EK(cudaGetLastError());
+    EK(cudaEventRecord(e->join, e->st));
+    // DEM / rigid bodies per scene, then join
+    for (int k = 0; k < ns; ++k) {
+        dmph_ctx *c = e->scenes[k];
+        EK(cudaStreamWaitEvent(c->st, e->join, 0));
+        enqueue_dem(c, c->st);
+        EK(cudaEventRecord(e->fork[k], c->st));
+        EK(cudaStreamWaitEvent(e->st, e->fork[k], 0));
+    }
+    EK(cudaGetLastError());
+    return DMPH_OK;
+}
+
+static long long ens_step_launches(const dmph_ensemble *e)
+{
+    long long n = 3;
+    for (const dmph_ctx *c : e->scenes) n += 2 + dem_launches(c);
+    return n;
+}
+
+static bool ens_graph_usable(const dmph_ensemble *e)
+{
+    if (!e->use_graph) return false;
+    for (const dmph_ctx *c : e->scenes)
+        if (c->prof || !(0.0 < c->time) || (c->time >= 0.2 && 0.4 >= c->time)) return false;
+    return true;
+}
+
+static int ens_build_graph(dmph_ensemble *e)
+{
+    cudaGraph_t g = nullptr;
+    EK(cudaGraphCreate(&g, 0));
+    EK(cudaStreamBeginCaptureToGraph(e->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const int rc = ens_enqueue_step(e, g);
+    cudaGraph_t g2 = g;
+    const cudaError_t ce = cudaStreamEndCapture(e->st, &g2);
+    if (rc || ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        if (!rc) e->err = std::string("ensemble capture: ") + cudaGetErrorString(ce);
+        return rc ? rc : DMPH_ECUDA;
+    }
+    EK(cudaGraphInstantiate(&e->gexec, g, 0));
+    e->graph = g;
+    return DMPH_OK;
+}
+
+static int ens_step_once(dmph_ensemble *e)
+{
+    if (ens_graph_usable(e)) {
+        if (!e->gexec) {
+            const int rc = ens_build_graph(e);
+            if (rc) return rc;
+        }
+        EK(cudaGraphLaunch(e->gexec, e->st));
+        e->graph_steps++;
+    } else {
+        const int rc = ens_enqueue_step(e, nullptr);
+        if (rc) return rc;
+        e->launches += 3;
+        for (dmph_ctx *c : e->scenes) c->launches += dem_launches(c);
+    }
+    for (dmph_ctx *c : e->scenes) {
+        advance_host_clock(c);
+    }
+    e->steps++;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_ensemble_step(dmph_ensemble *e, int nsteps)
+{
+    if (!e || nsteps < 0) return DMPH_EINVAL;
+    for (int s = 0; s < nsteps; ++s) {
+        const int rc = ens_step_once(e);
+        if (rc) return rc;
+    }
+    EK(cudaStreamSynchronize(e->st));
+    return DMPH_OK;
+}
+
+extern "C" int dmph_ensemble_step_timed(dmph_ensemble *e, int nsteps, float *device_ms)
+{
+    if (!e || nsteps < 0) return DMPH_EINVAL;
+    EK(cudaEventRecord(e->ev0, e->st));
+    for (int s = 0; s < nsteps; ++s) {
+        const int rc = ens_step_once(e);
+        if (rc) return rc;
+    }
+    EK(cudaEventRecord(e->ev1, e->st));
+    EK(cudaEventSynchronize(e->ev1));
+    float ms = 0.f;
+    EK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+    if (device_ms) *device_ms = ms;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_ensemble_autotune(dmph_ensemble *e, int *variant_a, int *variant_b, float *ms_a, float *ms_b)
+{
+    if (!e) return DMPH_EINVAL;
+    const int ns = (int)e->scenes.size();
+    dmph_ctx *ctx = e->ctx0;
+    for (dmph_ctx *c : e->scenes) cudaStreamSynchronize(c->st);
+    int rc = time_variants(ctx, e->st, [&](int v) { launch_ens_pass_a32(e->tab, ns, v, e->st); }, ms_a, &e->var_a);
+    if (rc) {
+        e->err = ctx->err;
+        return rc;
+    }
+    launch_ens_pass_a32(e->tab, ns, e->var_a, e->st);
+    rc = time_variants(ctx, e->st, [&](int v) { launch_ens_pass_b32(e->tab, ns, v, e->st); }, ms_b, &e->var_b);
+    if (rc) {
+        e->err = ctx->err;
+        return rc;
+    }
+    launch_ens_pass_b32(e->tab, ns, e->var_b, e->st);
+    EK(cudaStreamSynchronize(e->st));
+    ens_drop_graph(e);
+    if (variant_a) *variant_a = e->var_a;
+    if (variant_b) *variant_b = e->var_b;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_ensemble_set_graph(dmph_ensemble *e, int enable)
+{
+    if (!e) return DMPH_EINVAL;
+    e->use_graph = enable != 0;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_ensemble_info(dmph_ensemble *e, int64_t *kernel_launches, int64_t *steps)
+{
+    if (!e) return DMPH_EINVAL;
+    if (kernel_launches) {
+        // graph steps: every scene's head, the ensemble passes and every tail
+        // (rebuilds inside graphs are counted by the scenes' own counters)
+        *kernel_launches = e->launches + e->graph_steps * ens_step_launches(e);
+    }
+    if (steps) *steps = e->steps;
+    return DMPH_OK;
+}
+
+extern "C" const char *dmph_ensemble_last_error(dmph_ensemble *e)
+{
+    return e ? e->err.c_str() : "null ensemble";
+}
+
+extern "C" int dmph_ensemble_destroy(dmph_ensemble *e)
+{
+    if (!e) return DMPH_OK;
+    ens_release(e);
+    delete e;
+    return DMPH_OK;
+}
+

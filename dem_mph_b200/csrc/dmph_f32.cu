@@ -24,7 +24,6 @@ struct TileST {
     float4 g[kWarp];  // gravity centre; .w = attractive pressure
 };
 
-constexpr int kWarpsPerBlock32 = 8;
 
 __device__ __forceinline__ int min_image_cell(int d, int c)
 {
@@ -127,13 +126,9 @@ __global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm,
 // fully unrolled distance test), then each lane walks its own set bits, so
 // the kernel-weight arithmetic runs only for pairs that contribute.
 template <bool ST>
-__global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_a32(DevParams P, DevParams32 Q, DevState S,
-                                                                       const int *dB, int range)
+__device__ __forceinline__ void pass_a32_chunk(const DevParams &P, const DevParams32 &Q, const DevState &S,
+                                               Tile32 &tl, int lane, int cidx)
 {
-    __shared__ Tile32 tiles[kWarpsPerBlock32];
-    Tile32 &tl = tiles[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    FOR_EACH_CHUNK(dB, range, kWarpsPerBlock32, cidx)
     {
         const Chunk ch = S.chunks[cidx];
         const int i = ch.i0 + lane;
@@ -203,7 +198,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_a32(DevParams
                     }
                 }
             });
-        if (!active) continue;
+        if (!active) return;
         const double volstrain = vsp - Q.N0p32;
         S.vsp32[i] = (float)volstrain;
         S.div32[i] = (float)div;
@@ -224,15 +219,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_a32(DevParams
 // scheme.  Chunks hold one particle class, so the fluid/solid split below is
 // uniform across the warp.
 template <bool ST>
-__global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_b32(DevParams P, DevParams32 Q, DevState S,
-                                                                       const int *dB, int range)
+__device__ __forceinline__ void pass_b32_chunk(const DevParams &P, const DevParams32 &Q, const DevState &S,
+                                               Tile32 &tl, TileST &ts, int lane, int cidx)
 {
-    __shared__ Tile32 tiles[kWarpsPerBlock32];
-    __shared__ TileST tst[ST ? kWarpsPerBlock32 : 1];
-    Tile32 &tl = tiles[threadIdx.x >> 5];
-    TileST &ts = tst[ST ? (threadIdx.x >> 5) : 0];
-    const int lane = threadIdx.x & 31;
-    FOR_EACH_CHUNK(dB, range, kWarpsPerBlock32, cidx)
     {
         const Chunk ch = S.chunks[cidx];
         const int i = ch.i0 + lane;
@@ -375,7 +364,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_b32(DevParams
                     }
                 }
             });
-        if (!active) continue;
+        if (!active) return;
         const float m = sol ? rhoi * Q.V : Q.mass[ti];
         float4 F;
         if (sol) {
@@ -391,6 +380,115 @@ __global__ void __launch_bounds__(kWarpsPerBlock32 * kWarp) k_pass_b32(DevParams
         }
         F.w = 0.f;
         S.f4[i] = F;
+    }
+}
+
+// ------------------------------------------------- pass kernels (one scene)
+// Persistent grids; WPB warps per block (one shared tile per warp) and MINB
+// resident blocks per SM requested from the register allocator are the
+// autotuned launch parameters (dmph_autotune).
+template <bool ST, int WPB, int MINB>
+__global__ void __launch_bounds__(WPB * kWarp, MINB) k_pass_a32(DevParams P, DevParams32 Q, DevState S, const int *dB,
+                                                                int range)
+{
+    __shared__ Tile32 tiles[WPB];
+    const int lane = threadIdx.x & 31;
+    FOR_EACH_CHUNK(dB, range, WPB, cidx) pass_a32_chunk<ST>(P, Q, S, tiles[threadIdx.x >> 5], lane, cidx);
+}
+
+template <bool ST, int WPB, int MINB>
+__global__ void __launch_bounds__(WPB * kWarp, MINB) k_pass_b32(DevParams P, DevParams32 Q, DevState S, const int *dB,
+                                                                int range)
+{
+    __shared__ Tile32 tiles[WPB];
+    __shared__ TileST tst[ST ? WPB : 1];
+    const int lane = threadIdx.x & 31;
+    FOR_EACH_CHUNK(dB, range, WPB, cidx)
+    pass_b32_chunk<ST>(P, Q, S, tiles[threadIdx.x >> 5], tst[ST ? (threadIdx.x >> 5) : 0], lane, cidx);
+}
+
+// ------------------------------------------------- pass kernels (ensemble)
+// One persistent launch over the chunks of every scene of an ensemble: the
+// scenes' chunk ranges are concatenated (prefix sums built per block from
+// each scene's device bounds), each warp maps its global chunk index to a
+// scene by binary search and runs the same per-chunk body with that scene's
+// parameters and state, read from the scene table in global memory.
+__device__ __forceinline__ int ens_prefix(const EnsScene *__restrict__ tab, int ns, int range, int *pre, int *beg)
+{
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+        int b, e;
+        chunk_range(tab[k].dB, range, b, e);
+        beg[k] = b;
+        pre[k + 1] = e - b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        pre[0] = 0;
+        for (int k = 0; k < ns; ++k) pre[k + 1] += pre[k];
+    }
+    __syncthreads();
+    return pre[ns];
+}
+
+__device__ __forceinline__ int ens_scene_of(const int *pre, int ns, int g)
+{
+    int lo = 0, hi = ns - 1;  // largest k with pre[k] <= g
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int WPB, int MINB>
+__global__ void __launch_bounds__(WPB * kWarp, MINB) k_ens_pass_a32(const EnsScene *__restrict__ tab, int ns, int range)
+{
+    __shared__ Tile32 tiles[WPB];
+    __shared__ int pre[kMaxEnsemble + 1], beg[kMaxEnsemble];
+    const int total = ens_prefix(tab, ns, range, pre, beg);
+    const int lane = threadIdx.x & 31;
+    for (int g = blockIdx.x * WPB + (int)(threadIdx.x >> 5); g < total; g += gridDim.x * WPB) {
+        const int k = ens_scene_of(pre, ns, g);
+        const EnsScene &e = tab[k];
+        const int cidx = beg[k] + g - pre[k];
+        if (e.P.surface_tension) pass_a32_chunk<true>(e.P, e.Q, e.S, tiles[threadIdx.x >> 5], lane, cidx);
+        else pass_a32_chunk<false>(e.P, e.Q, e.S, tiles[threadIdx.x >> 5], lane, cidx);
+    }
+}
+
+template <int WPB, int MINB>
+__global__ void __launch_bounds__(WPB * kWarp, MINB) k_ens_pass_b32(const EnsScene *__restrict__ tab, int ns)
+{
+    __shared__ Tile32 tiles[WPB];
+    __shared__ TileST tst[WPB];
+    __shared__ int pre[kMaxEnsemble + 1], beg[kMaxEnsemble];
+    const int total = ens_prefix(tab, ns, CR_FLUID_SOLID, pre, beg);
+    const int lane = threadIdx.x & 31;
+    for (int g = blockIdx.x * WPB + (int)(threadIdx.x >> 5); g < total; g += gridDim.x * WPB) {
+        const int k = ens_scene_of(pre, ns, g);
+        const EnsScene &e = tab[k];
+        const int cidx = beg[k] + g - pre[k];
+        const int w = threadIdx.x >> 5;
+        if (e.P.surface_tension) pass_b32_chunk<true>(e.P, e.Q, e.S, tiles[w], tst[w], lane, cidx);
+        else pass_b32_chunk<false>(e.P, e.Q, e.S, tiles[w], tst[w], lane, cidx);
+    }
+}
+
+__global__ void k_ens_fluid_accel32(const EnsScene *__restrict__ tab, int ns)
+{
+    for (int k = 0; k < ns; ++k) {
+        const EnsScene &e = tab[k];
+        const int fe = e.dB[B_FE];
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < fe; i += gridDim.x * blockDim.x) {
+            const float4 f = e.S.f4[i];
+            float4 v = e.S.v4[i];
+            const float c = e.Q.dt / e.Q.mass[unpack_type(__float_as_uint(e.S.p4[i].w))];
+            v.x = fmaf(f.x, c, v.x);
+            v.y = fmaf(f.y, c, v.y);
+            v.z = fmaf(f.z, c, v.z);
+            e.S.v4[i] = v;
+        }
     }
 }
 
@@ -651,29 +749,91 @@ void launch_drift32(const DevParams &P, const DevParams32 &Q, const DevState &S,
     if (blocks > sms * 8) blocks = sms * 8;
     k_drift32<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(P, Q, S, Wm, maxshift);
 }
+// launch-parameter variants the autotuner chooses from: warps per block x
+// requested resident blocks per SM
+#define DMPH_PASS_VARIANTS(X) X(0, 8, 1) X(1, 4, 1) X(2, 16, 1) X(3, 8, 4) X(4, 4, 8)
+
+template <class K>
+static int grid_for(K kernel, int threads)
+{
+    return persistent_grid((const void *)kernel, threads);
+}
+
 void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int range,
+                     int variant, cudaStream_t st)
+{
+#define DMPH_LAUNCH_A(ID, WPB, MINB)                                                              \
+    case ID:                                                                                      \
+        if (P.surface_tension) {                                                                  \
+            static const int g = grid_for(k_pass_a32<true, WPB, MINB>, WPB * kWarp);              \
+            k_pass_a32<true, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, range);           \
+        } else {                                                                                  \
+            static const int g = grid_for(k_pass_a32<false, WPB, MINB>, WPB * kWarp);             \
+            k_pass_a32<false, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, range);          \
+        }                                                                                         \
+        break;
+    switch (variant) {
+        DMPH_PASS_VARIANTS(DMPH_LAUNCH_A)
+    default: break;
+    }
+#undef DMPH_LAUNCH_A
+}
+
+void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
                      cudaStream_t st)
 {
-    constexpr int B = kWarpsPerBlock32 * kWarp;
-    if (P.surface_tension) {
-        static const int g = persistent_grid((const void *)k_pass_a32<true>, B);
-        k_pass_a32<true><<<g, B, 0, st>>>(P, Q, S, dB, range);
-    } else {
-        static const int g = persistent_grid((const void *)k_pass_a32<false>, B);
-        k_pass_a32<false><<<g, B, 0, st>>>(P, Q, S, dB, range);
+#define DMPH_LAUNCH_B(ID, WPB, MINB)                                                              \
+    case ID:                                                                                      \
+        if (P.surface_tension) {                                                                  \
+            static const int g = grid_for(k_pass_b32<true, WPB, MINB>, WPB * kWarp);              \
+            k_pass_b32<true, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, CR_FLUID_SOLID);  \
+        } else {                                                                                  \
+            static const int g = grid_for(k_pass_b32<false, WPB, MINB>, WPB * kWarp);             \
+            k_pass_b32<false, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, CR_FLUID_SOLID); \
+        }                                                                                         \
+        break;
+    switch (variant) {
+        DMPH_PASS_VARIANTS(DMPH_LAUNCH_B)
+    default: break;
     }
+#undef DMPH_LAUNCH_B
 }
-void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st)
+
+void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t st)
 {
-    constexpr int B = kWarpsPerBlock32 * kWarp;
-    if (P.surface_tension) {
-        static const int g = persistent_grid((const void *)k_pass_b32<true>, B);
-        k_pass_b32<true><<<g, B, 0, st>>>(P, Q, S, dB, CR_FLUID_SOLID);
-    } else {
-        static const int g = persistent_grid((const void *)k_pass_b32<false>, B);
-        k_pass_b32<false><<<g, B, 0, st>>>(P, Q, S, dB, CR_FLUID_SOLID);
+#define DMPH_LAUNCH_EA(ID, WPB, MINB)                                                     \
+    case ID: {                                                                            \
+        static const int g = grid_for(k_ens_pass_a32<WPB, MINB>, WPB * kWarp);            \
+        k_ens_pass_a32<WPB, MINB><<<g, WPB * kWarp, 0, st>>>(tab, ns, CR_WET);            \
+        break;                                                                            \
     }
+    switch (variant) {
+        DMPH_PASS_VARIANTS(DMPH_LAUNCH_EA)
+    default: break;
+    }
+#undef DMPH_LAUNCH_EA
 }
+
+void launch_ens_pass_b32(const EnsScene *tab, int ns, int variant, cudaStream_t st)
+{
+#define DMPH_LAUNCH_EB(ID, WPB, MINB)                                                     \
+    case ID: {                                                                            \
+        static const int g = grid_for(k_ens_pass_b32<WPB, MINB>, WPB * kWarp);            \
+        k_ens_pass_b32<WPB, MINB><<<g, WPB * kWarp, 0, st>>>(tab, ns);                    \
+        break;                                                                            \
+    }
+    switch (variant) {
+        DMPH_PASS_VARIANTS(DMPH_LAUNCH_EB)
+    default: break;
+    }
+#undef DMPH_LAUNCH_EB
+}
+
+void launch_ens_fluid_accel32(const EnsScene *tab, int ns, cudaStream_t st)
+{
+    k_ens_fluid_accel32<<<148 * 4, 256, 0, st>>>(tab, ns);
+}
+
 void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st)
 {
     k_fluid_accel32<<<148 * 4, 256, 0, st>>>(Q, S, dB);

@@ -44,9 +44,13 @@ void launch_neighbor_fill(const DevParams &P, const DevState &S, const int *dB, 
 DevParams32 make_params32(const DevParams &P);
 void launch_drift32(const DevParams &P, const DevParams32 &Q, const DevState &S, const WallMotion &Wm,
                     unsigned long long *maxshift, int sms, cudaStream_t st);
-void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int range,
+void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int range, int variant,
                      cudaStream_t st);
-void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
+void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
+                     cudaStream_t st);
+void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t st);
+void launch_ens_pass_b32(const EnsScene *tab, int ns, int variant, cudaStream_t st);
+void launch_ens_fluid_accel32(const EnsScene *tab, int ns, cudaStream_t st);
 void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
 void launch_export32(const DevParams &P, const DevState &S, double *pos, double *vel, cudaStream_t st);
 void launch_import32(const DevParams &P, const DevState &S, const double *pos, const double *vel, cudaStream_t st);

@@ -102,4 +102,15 @@ struct WallMotion {
     int moving;  // 1 when 0.2 <= Time <= 0.4 for this step
 };
 
+// One scene of an ensemble as the ensemble kernels see it (a device array of
+// these is the scene table)
+constexpr int kMaxEnsemble = 256;
+constexpr int kPassVariants = 5;
+struct EnsScene {
+    DevParams P;
+    DevParams32 Q;
+    DevState S;
+    const int *dB;
+};
+
 }  // namespace dmph

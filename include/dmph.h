@@ -241,6 +241,37 @@ int dmph_get_bodies(dmph_ctx *ctx, double *X, double *V, double *q, double *L, d
  * individual launches.  Results are identical either way. */
 int dmph_set_graph(dmph_ctx *ctx, int enable);
 
+/* Autotuner of the FP32 pair passes: times every launch variant (warps per
+ * block x resident blocks per SM requested from the register allocator) of
+ * pass A and pass B on the current state and keeps the fastest for the
+ * following steps.  Reports the chosen variants and, when ms_a/ms_b are
+ * non-NULL, the time of each of DMPH_PASS_VARIANTS variants.  The passes
+ * only read the state, so tuning changes no result.  FP32 split build only. */
+#define DMPH_PASS_VARIANTS 5
+int dmph_autotune(dmph_ctx *ctx, int *variant_a, int *variant_b, float *ms_a, float *ms_b);
+int dmph_set_variants(dmph_ctx *ctx, int variant_a, int variant_b);
+
+/* Ensemble of independent scenes (no counterpart in the reference, which runs
+ * one scene per process).  Every scene keeps its own context, parameters,
+ * cell grid and state; an ensemble step advances all of them by one step:
+ * each scene's drift and rebuild decision (with its own conditional rebuild),
+ * then pass A and pass B of ALL scenes as one persistent launch each over the
+ * concatenated chunk lists, then each scene's DEM substeps or rigid bodies.
+ * With graph replay on (the default) a whole ensemble step is one CUDA graph.
+ * Results are bit-identical to stepping each scene alone.  Scenes must be FP32
+ * split contexts on one device, at most 256, each in at most one ensemble;
+ * set their bodies before creating the ensemble and step them only through it
+ * while it exists. */
+typedef struct dmph_ensemble dmph_ensemble;
+int dmph_ensemble_create(dmph_ctx *const *scenes, int nscenes, dmph_ensemble **out);
+int dmph_ensemble_step(dmph_ensemble *e, int nsteps);
+int dmph_ensemble_step_timed(dmph_ensemble *e, int nsteps, float *device_ms);
+int dmph_ensemble_autotune(dmph_ensemble *e, int *variant_a, int *variant_b, float *ms_a, float *ms_b);
+int dmph_ensemble_set_graph(dmph_ensemble *e, int enable);
+int dmph_ensemble_info(dmph_ensemble *e, int64_t *kernel_launches, int64_t *steps);
+const char *dmph_ensemble_last_error(dmph_ensemble *e);
+int dmph_ensemble_destroy(dmph_ensemble *e);
+
 /* Per-phase device timing.  With enable != 0, every following step records
  * CUDA events on the context's stream around each phase (this adds event
  * overhead, so time throughput with it off); dmph_get_phase_times returns the

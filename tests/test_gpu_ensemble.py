@@ -1,0 +1,114 @@
+"""Ensemble of independent scenes (dmph_ensemble_*) and the pair-pass
+autotuner (dmph_autotune).  Neither has a counterpart in the reference; the
+bar is that they change no result: an ensemble step must give, for every
+scene, the same bits as stepping that scene alone, whatever launch variants
+the tuner picked and with or without graph replay."""
+import numpy as np
+import pytest
+
+from helpers import small3d_st_params
+from dem_mph_b200 import scenes, solver
+from dem_mph_b200.abi import PRECISION_FP32_SPLIT
+
+pytestmark = pytest.mark.gpu
+
+
+def scene_list():
+    """uneven scenes: sizes, debris counts, rigid bodies on/off, surface tension on/off"""
+    out = []
+    for seed, dx, nd, bodies, st in ((7, 0.02, 3, False, False), (8, 0.025, 2, True, False),
+                                     (9, 0.018, 4, True, False), (10, 0.03, 1, False, True)):
+        s = scenes.small(seed=seed, dx=dx, n_debris=nd)
+        p = s.params.copy()
+        if st:
+            p = small3d_st_params(p)
+        p.precision = PRECISION_FP32_SPLIT
+        out.append((s, p, bodies))
+    return out
+
+
+def make(items):
+    sv = []
+    for s, p, bodies in items:
+        g = solver.Solver(p, s.type, s.x, s.v)
+        if bodies:
+            g.set_bodies(s.body, s.body_density)
+        sv.append(g)
+    return sv
+
+
+def same_state(a, b):
+    ta, xa, va, oa = a.state()
+    tb, xb, vb, ob = b.state()
+    return (np.array_equal(oa, ob) and np.array_equal(ta, tb) and np.array_equal(xa, xb)
+            and np.array_equal(va, vb) and np.array_equal(a.field("PressureP"), b.field("PressureP")))
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_ensemble_matches_scenes_stepped_alone(graph):
+    items = scene_list()
+    alone = make(items)
+    members = make(items)
+    ens = solver.Ensemble(members)
+    ens.set_graph(graph)
+    assert len({g.n for g in members}) == len(members)  # uneven sizes
+    for steps in (1, 9, 50):
+        for g in alone:
+            g.step(steps)
+        ens.step(steps)
+        for k, (a, b) in enumerate(zip(alone, members)):
+            assert a.info().rebuilds == b.info().rebuilds, k
+            assert same_state(a, b), k
+            if getattr(a, "nbodies", 0):
+                ba, bb = a.bodies(), b.bodies()
+                assert all(np.array_equal(ba[q], bb[q]) for q in ("X", "V", "q", "L")), k
+    assert sum(g.info().rebuilds for g in members) > len(members)
+    assert ens.info()["steps"] == 60
+    ens.close()
+    for g in alone + members:
+        g.close()
+
+
+def test_autotuned_variants_change_no_result():
+    items = scene_list()[:2]
+    ref = make(items)
+    tuned = make(items)
+    ens = solver.Ensemble(tuned)
+    for g in ref:
+        g.step(5)
+    ens.step(5)
+    va, vb, ma, mb = ens.autotune()
+    assert 0 <= va < solver.PASS_VARIANTS and 0 <= vb < solver.PASS_VARIANTS
+    assert np.all(ma > 0) and np.all(mb > 0)
+    for g in ref:
+        g.step(30)
+    ens.step(30)
+    for a, b in zip(ref, tuned):
+        assert same_state(a, b)
+    ens.close()
+    # single-scene tuner, and every variant forced in turn
+    a, b = ref[0], tuned[0]
+    ta, tb, _, _ = b.autotune()
+    for v in range(solver.PASS_VARIANTS):
+        b.set_variants(v, (v + 2) % solver.PASS_VARIANTS)
+        a.step(3)
+        b.step(3)
+        assert same_state(a, b), v
+    for g in ref + tuned:
+        g.close()
+
+
+def test_ensemble_rejects_fp64_and_duplicates():
+    s = scenes.small()
+    g = solver.Solver(s.params, s.type, s.x, s.v)  # FP64 parity build
+    with pytest.raises(solver.DmphError):
+        solver.Ensemble([g])
+    p = s.params.copy()
+    p.precision = PRECISION_FP32_SPLIT
+    h = solver.Solver(p, s.type, s.x, s.v)
+    with pytest.raises(solver.DmphError):
+        solver.Ensemble([h, h])
+    with pytest.raises(solver.DmphError):
+        g.autotune()
+    g.close()
+    h.close()
