@@ -112,6 +112,44 @@ class Info(C.Structure):
     ]
 
 
+class SurrogateParams(C.Structure):
+    """dmph_surrogate_params"""
+    _fields_ = [
+        ("substeps", C.c_int32),
+        ("check_interval", C.c_int32),
+        ("tolerance", C.c_double),
+        ("fallback_blocks", C.c_int32),
+        ("train_iters_per_block", C.c_int32),
+        ("batch", C.c_int32),
+        ("pool_rows", C.c_int32),
+        ("learning_rate", C.c_float),
+        ("seed", C.c_uint64),
+    ]
+
+
+class SurrogateStats(C.Structure):
+    """dmph_surrogate_stats"""
+    _fields_ = [
+        ("calls", C.c_int64),
+        ("plain_blocks", C.c_int64),
+        ("judged", C.c_int64),
+        ("fallbacks", C.c_int64),
+        ("samples", C.c_int64),
+        ("train_iters", C.c_int64),
+        ("pool_rows", C.c_int64),
+        ("in_fallback", C.c_int32),
+        ("last_error", C.c_double),
+        ("last_error_v", C.c_double),
+        ("last_loss", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+MLP_IN, MLP_OUT, MLP_FEATURES, MLP_TARGETS = 64, 16, 48, 6
+
+
 def default_params():
     """The reference's static initialisers (source/DEM-MPH.cpp:61-75): Dt and
     DEMDt 1e100, everything else zero; dim 3."""

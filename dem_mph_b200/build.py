@@ -43,9 +43,11 @@ CU_SOURCES = [
     ("dmph_f32.cu", []),
     ("dmph_noalloc.cu", ["-fmad=false"]),
     ("dmph_bodies.cu", []),
+    ("dmph_mlp.cu", []),
+    ("dmph_surrogate.cu", []),
 ]
 CPP_SOURCES = ["dmph_params.cpp", "dmph_io.cpp"]
-HEADERS = ["dmph_device.cuh", "dmph_state.cuh", "dmph_traverse.cuh", "dmph_internal.h"]
+HEADERS = ["dmph_device.cuh", "dmph_state.cuh", "dmph_traverse.cuh", "dmph_internal.h", "dmph_ctx.h", "dmph_mlp.h"]
 
 
 def _newer(target, deps):

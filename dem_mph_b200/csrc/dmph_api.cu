@@ -7,7 +7,7 @@
 #include <string>
 #include <vector>
 
-#include "dmph_internal.h"
+#include "dmph_ctx.h"
 
 using namespace dmph;
 
@@ -15,57 +15,6 @@ namespace {
 thread_local std::string g_create_err;
 }
 
-struct dmph_ctx {
-    dmph_params p;
-    DevParams P;
-    DevParams32 Q;
-    bool fp32 = false;
-    WallMotion Wm;
-    cudaStream_t st = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    int sms = 148;
-    int device = 0;
-    DevState S{};
-    // second buffers of the permuted arrays
-    double *pos2 = nullptr, *vel2 = nullptr;
-    int *type2 = nullptr, *pidx2 = nullptr;
-    float4 *p4b = nullptr, *v4b = nullptr;  // second buffers of the FP32 state
-    int *bid2 = nullptr;                     // second buffer of the body ids
-    DevBodies Bd{};                          // rigid clumps (B = 0: off)
-    unsigned long long *words = nullptr;
-    int *flag = nullptr, *offs = nullptr, *bsums = nullptr, *total = nullptr;
-    unsigned long long *maxshift = nullptr;
-    unsigned long long *h_maxshift = nullptr;  // pinned
-    int *h_small = nullptr;                    // pinned scratch for small read-backs
-    int *dB = nullptr;         // device bounds (DevBound)
-    cudaStream_t st2 = nullptr;      // capture stream of the rebuild body
-    bool use_graph = false;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    long long graph_steps = 0, host_rebuilds = 0;
-    int var_a = 0, var_b = 0;  // launch variants of the FP32 pair passes (dmph_autotune)
-    Chunk *chunks2 = nullptr;  // partition scratch
-    int demSteps = 0;
-    double time = 0.0;
-    long long steps = 0, rebuilds = 0;
-    long long launches = 0;  // kernels launched by dmph_step
-    bool all_counts = false;
-    bool prof = false;
-    cudaEvent_t pe0 = nullptr, pe1 = nullptr;
-    double phase_ms[DMPH_PHASE_COUNT] = {0};
-    long long phase_n[DMPH_PHASE_COUNT] = {0};
-    std::string err;
-    std::vector<void *> allocs;
-};
-
-#define CK(call)                                                                                       \
-    do {                                                                                               \
-        cudaError_t e_ = (call);                                                                       \
-        if (e_ != cudaSuccess) {                                                                       \
-            ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                             \
-            return DMPH_ECUDA;                                                                         \
-        }                                                                                              \
-    } while (0)
 
 template <class T>
 static int dalloc(dmph_ctx *ctx, T **ptr, size_t count)
@@ -81,11 +30,11 @@ static int dalloc(dmph_ctx *ctx, T **ptr, size_t count)
     return cudaMemsetAsync(p, 0, count ? count * sizeof(T) : 16, ctx->st) == cudaSuccess ? DMPH_OK : DMPH_ECUDA;
 }
 
-static void drop_graph(dmph_ctx *ctx);
 
 static void release(dmph_ctx *ctx)
 {
     if (ctx->st) cudaStreamSynchronize(ctx->st);
+    surrogate_release(ctx);
     drop_graph(ctx);
     if (ctx->st2) cudaStreamDestroy(ctx->st2);
     ctx->st2 = nullptr;
@@ -117,7 +66,7 @@ static long long bitonic_launches(int n, int nlog)
 // Every launch has a static shape and every range lives in ctx->dB, so the
 // sequence can be recorded into a CUDA graph; permuted arrays are written to
 // the second buffers and copied back, so device pointers never change.
-static void enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
+void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
 {
     const DevParams &P = ctx->P;
     const size_t N = (size_t)P.N;
@@ -152,7 +101,7 @@ static void enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
     launch_counts(P, S, ctx->dB, ctx->all_counts ? CR_ALL : CR_SOLID, st);
 }
 
-static long long rebuild_launches(const dmph_ctx *ctx, bool first)
+long long dmph::rebuild_launches(const dmph_ctx *ctx, bool first)
 {
     const DevParams &P = ctx->P;
     return 1 + bitonic_launches(P.P2, P.P2log) + 1 + 1 + (ctx->fp32 && !first ? 1 : 0) + 5 + 1 +
@@ -176,7 +125,7 @@ static void phase_end(dmph_ctx *ctx, int ph)
 }
 
 // drift + rebuild decision (first part of a step)
-static void enqueue_head(dmph_ctx *ctx, unsigned long long graph_cond, cudaStream_t st)
+void dmph::enqueue_head(dmph_ctx *ctx, unsigned long long graph_cond, cudaStream_t st)
 {
     const DevParams &P = ctx->P;
     cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), st);
@@ -188,7 +137,7 @@ static void enqueue_head(dmph_ctx *ctx, unsigned long long graph_cond, cudaStrea
 }
 
 // the pair passes (first part of a step's tail)
-static void enqueue_passes(dmph_ctx *ctx, cudaStream_t st)
+void dmph::enqueue_passes(dmph_ctx *ctx, cudaStream_t st)
 {
     const DevParams &P = ctx->P;
     DevState &S = ctx->S;
@@ -214,7 +163,7 @@ static void enqueue_passes(dmph_ctx *ctx, cudaStream_t st)
 }
 
 // the DEM substeps or rigid bodies (second part of a step's tail)
-static void enqueue_dem(dmph_ctx *ctx, cudaStream_t st)
+void dmph::enqueue_dem(dmph_ctx *ctx, cudaStream_t st)
 {
     const DevParams &P = ctx->P;
     DevState &S = ctx->S;
@@ -256,18 +205,18 @@ static void enqueue_tail(dmph_ctx *ctx, cudaStream_t st)
     enqueue_dem(ctx, st);
 }
 
-static long long dem_launches(const dmph_ctx *ctx)
+long long dmph::dem_launches(const dmph_ctx *ctx)
 {
     const long long dem = ctx->Bd.B > 0 ? 2 : 2 + (ctx->P.wall_dem_coeffs ? 1 : 0);
     return ctx->demSteps * dem + (ctx->fp32 ? 2 : 0);
 }
 
-static long long tail_launches(const dmph_ctx *ctx)
+long long dmph::tail_launches(const dmph_ctx *ctx)
 {
     return 3 + dem_launches(ctx);
 }
 
-static void advance_host_clock(dmph_ctx *ctx)
+void dmph::advance_host_clock(dmph_ctx *ctx)
 {
     // WallCenter moves only while `0.0 < Time < 0.2` holds, i.e. Time <= 0 (:2892)
     if (!(0.0 < ctx->time))
@@ -331,7 +280,7 @@ static int build_graph(dmph_ctx *ctx)
     return DMPH_OK;
 }
 
-static void drop_graph(dmph_ctx *ctx)
+void dmph::drop_graph(dmph_ctx *ctx)
 {
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     if (ctx->graph) cudaGraphDestroy(ctx->graph);
@@ -344,7 +293,7 @@ static bool graph_usable(const dmph_ctx *ctx)
     return ctx->use_graph && !ctx->prof && 0.0 < ctx->time && !(ctx->time >= 0.2 && 0.4 >= ctx->time);
 }
 
-static int step_once(dmph_ctx *ctx)
+int dmph::step_once(dmph_ctx *ctx)
 {
     ctx->Wm.moving = (ctx->time >= 0.2 && 0.4 >= ctx->time) ? 1 : 0;
     if (graph_usable(ctx)) {
@@ -378,7 +327,7 @@ static int step_once(dmph_ctx *ctx)
 }
 
 // host copy of the device bounds (synchronises the stream)
-static int read_bounds(dmph_ctx *ctx, int *b)
+int dmph::read_bounds(dmph_ctx *ctx, int *b)
 {
     CK(cudaMemcpyAsync(ctx->h_small, ctx->dB, B_COUNT * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));

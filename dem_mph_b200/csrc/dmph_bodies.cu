@@ -147,35 +147,6 @@ __global__ void __launch_bounds__(4 * kWarp) k_clump_dem(DevParams P, DevState S
     }
 }
 
-__device__ __forceinline__ double warp_sum(double v)
-{
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-    return v;
-}
-
-__device__ __forceinline__ void quat_to_R(const double *q, double R[3][3])
-{
-    const double w = q[0], x = q[1], y = q[2], z = q[3];
-    R[0][0] = 1.0 - 2.0 * (y * y + z * z);
-    R[0][1] = 2.0 * (x * y - w * z);
-    R[0][2] = 2.0 * (x * z + w * y);
-    R[1][0] = 2.0 * (x * y + w * z);
-    R[1][1] = 1.0 - 2.0 * (x * x + z * z);
-    R[1][2] = 2.0 * (y * z - w * x);
-    R[2][0] = 2.0 * (x * z - w * y);
-    R[2][1] = 2.0 * (y * z + w * x);
-    R[2][2] = 1.0 - 2.0 * (x * x + y * y);
-}
-
-// w = R I0^-1 R^T L
-__device__ __forceinline__ void omega_of(const double R[3][3], const double *Ii, const double *L, double *w)
-{
-    double a[3], b[3];
-    for (int r = 0; r < 3; r++) a[r] = R[0][r] * L[0] + R[1][r] * L[1] + R[2][r] * L[2];  // R^T L
-    for (int r = 0; r < 3; r++) b[r] = Ii[3 * r] * a[0] + Ii[3 * r + 1] * a[1] + Ii[3 * r + 2] * a[2];
-    for (int r = 0; r < 3; r++) w[r] = R[r][0] * b[0] + R[r][1] * b[1] + R[r][2] * b[2];
-}
-
 template <bool F32>
 __global__ void k_body_step(DevParams P, DevState S, DevBodies Bd)
 {

@@ -1,0 +1,90 @@
+// The solver context behind the C ABI and the step helpers shared by the
+// step driver (dmph_api.cu) and the surrogate driver (dmph_surrogate.cu).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "dmph.h"
+#include "dmph_internal.h"
+
+namespace dmph {
+struct Surrogate;
+}
+
+// private header of the library: the context is written with the library's own types
+using namespace dmph;
+
+struct dmph_ctx {
+    dmph_params p;
+    DevParams P;
+    DevParams32 Q;
+    bool fp32 = false;
+    WallMotion Wm;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int sms = 148;
+    int device = 0;
+    DevState S{};
+    // second buffers of the permuted arrays
+    double *pos2 = nullptr, *vel2 = nullptr;
+    int *type2 = nullptr, *pidx2 = nullptr;
+    float4 *p4b = nullptr, *v4b = nullptr;  // second buffers of the FP32 state
+    int *bid2 = nullptr;                     // second buffer of the body ids
+    DevBodies Bd{};                          // rigid clumps (B = 0: off)
+    unsigned long long *words = nullptr;
+    int *flag = nullptr, *offs = nullptr, *bsums = nullptr, *total = nullptr;
+    unsigned long long *maxshift = nullptr;
+    unsigned long long *h_maxshift = nullptr;  // pinned
+    int *h_small = nullptr;                    // pinned scratch for small read-backs
+    int *dB = nullptr;         // device bounds (DevBound)
+    cudaStream_t st2 = nullptr;      // capture stream of the rebuild body
+    bool use_graph = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    long long graph_steps = 0, host_rebuilds = 0;
+    int var_a = 0, var_b = 0;  // launch variants of the FP32 pair passes (dmph_autotune)
+    Chunk *chunks2 = nullptr;  // partition scratch
+    int demSteps = 0;
+    double time = 0.0;
+    long long steps = 0, rebuilds = 0;
+    long long launches = 0;  // kernels launched by dmph_step
+    bool all_counts = false;
+    bool prof = false;
+    cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+    double phase_ms[DMPH_PHASE_COUNT] = {0};
+    long long phase_n[DMPH_PHASE_COUNT] = {0};
+    std::string err;
+    std::vector<void *> allocs;
+    dmph::Surrogate *sg = nullptr;  // surrogate state (dmph_surrogate_enable)
+};
+
+
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                             \
+            return DMPH_ECUDA;                                                                         \
+        }                                                                                              \
+    } while (0)
+
+namespace dmph {
+
+// step pieces (dmph_api.cu)
+void enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st);
+long long rebuild_launches(const dmph_ctx *ctx, bool first);
+void enqueue_head(dmph_ctx *ctx, unsigned long long graph_cond, cudaStream_t st);
+void enqueue_passes(dmph_ctx *ctx, cudaStream_t st);
+void enqueue_dem(dmph_ctx *ctx, cudaStream_t st);
+long long dem_launches(const dmph_ctx *ctx);
+long long tail_launches(const dmph_ctx *ctx);
+void advance_host_clock(dmph_ctx *ctx);
+int step_once(dmph_ctx *ctx);
+int read_bounds(dmph_ctx *ctx, int *b);
+void drop_graph(dmph_ctx *ctx);
+
+// surrogate (dmph_surrogate.cu)
+void surrogate_release(dmph_ctx *ctx);
+
+}  // namespace dmph

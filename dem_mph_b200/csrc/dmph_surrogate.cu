@@ -1,0 +1,1070 @@
+// Learned surrogate of K solver steps (no counterpart in the reference).
+//
+// A surrogate call advances the FP32 split state by K steps at once:
+//   1. pass A and pass B at the current state (pressures, forces),
+//   2. k_features32: 48 cell-list aggregated features per fluid and debris
+//      particle, in one stencil traversal,
+//   3. the MLP on the tensor cores (dmph_mlp.cu) predicts, per particle, the
+//      K-step velocity increment and the residual of the position increment
+//      beyond what the velocity history implies:
+//          dv = y[0:3] * K dt a_s
+//          dx = K dt v0 + (K - 1)/2 dt dv + y[3:6] * (K dt)^2 a_s
+//      (exact for a constant acceleration with y[3:6] = 0),
+//   4. k_apply32 moves fluid particles; rigid debris bodies are translated by
+//      the mean prediction of their members (orientation and angular
+//      momentum kept); walls stay put,
+//   5. the usual device-side rebuild decision.
+// Training data come from the solver itself: at the start of a K-step block
+// the features and (x, v) of every fluid/debris particle are recorded, the
+// plain solver runs K steps, and the increments (matched by original id
+// across rebuilds) become the targets of a sampled subset, appended to a
+// ring-buffer pool.  Every `check_interval` surrogate calls one block runs on
+// the plain solver instead, as the judge: the network's prediction for that
+// block is compared with what the solver did, and above `tolerance` the
+// driver falls back to the plain solver for `fallback_blocks` blocks, during
+// which it keeps collecting samples and training.
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "dmph_ctx.h"
+#include "dmph_mlp.h"
+#include "dmph_traverse.cuh"
+
+namespace dmph {
+
+struct FeatScales {
+    float inv_vs, inv_as, inv_Ps, inv_W0, inv_dx;
+    float vs, as;
+    float K, dt;  // substeps, FP32 time step
+};
+
+struct Surrogate {
+    dmph_surrogate_params prm{};
+    MlpParamsDev M;
+    int adam_t = 0;
+    int n_rows = 0;  // fluid + debris slots
+    FeatScales fs{};
+    // per-slot buffers (capacity N)
+    __nv_bfloat16 *X = nullptr;  // features [N][64]
+    float *Y = nullptr;          // outputs [N][16]
+    __nv_bfloat16 *H[2] = {nullptr, nullptr};
+    float4 *v0 = nullptr;   // start-of-block velocity
+    double *x0 = nullptr;   // start-of-block absolute position (3 per row)
+    int *orig = nullptr;    // start-of-block original id
+    int *inv = nullptr;     // original id -> current slot
+    // sample pool
+    __nv_bfloat16 *poolX = nullptr;
+    float *poolT = nullptr;
+    long long pool_cap = 0, pool_count = 0;
+    unsigned long long *d_cursor = nullptr;
+    // training batch
+    int B = 0;
+    __nv_bfloat16 *Xb = nullptr, *XTb = nullptr, *Hb[3] = {}, *HTb[3] = {}, *dZ[2] = {}, *dZT[2] = {};
+    __nv_bfloat16 *dY = nullptr, *dYT = nullptr;
+    float *Yb = nullptr, *Tb = nullptr;
+    float *d_loss = nullptr;
+    int *d_err = nullptr;
+    int *d_bad = nullptr;
+    double *d_acc = nullptr;  // judge sums
+    float *feat32 = nullptr;  // optional FP32 copy of the features (tests)
+    std::vector<void *> allocs;
+    dmph_surrogate_stats st{};
+    int fallback_left = 0;
+    int since_check = 0;
+    unsigned long long block_seed = 0;
+};
+
+namespace {
+
+constexpr int kFeatWarps = 8;
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x)
+{
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+struct TileF {
+    float4 p[kWarp];  // position in the frame of the warp's cell; .w = type
+    float4 v[kWarp];  // velocity; .w = pressure
+    float4 a[kWarp];  // acceleration of the last force evaluation
+};
+
+__device__ __forceinline__ float particle_mass32(const DevParams &P, const DevState &S, int j, int t)
+{
+    return (float)(particle_density(S, P, j, t) * P.V);
+}
+
+// ------------------------------------------------------------ features
+__global__ void __launch_bounds__(kFeatWarps * kWarp) k_features32(DevParams P, DevParams32 Q, DevState S,
+                                                                   const int *dB, FeatScales F,
+                                                                   __nv_bfloat16 *__restrict__ X,
+                                                                   float *__restrict__ X32)
+{
+    __shared__ TileF tiles[kFeatWarps];
+    TileF &tl = tiles[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    FOR_EACH_CHUNK(dB, CR_FLUID_SOLID, kFeatWarps, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        const int cix = key_cell / (P.cc[1] * P.cc[2]);
+        const int ciy = (key_cell / P.cc[2]) % P.cc[1];
+        const int ciz = key_cell % P.cc[2];
+        const int ii = active ? i : ch.i0;
+        const float4 pi = S.p4[ii];
+        const float4 vi = S.v4[ii];
+        const int ti = unpack_type(__float_as_uint(pi.w));
+        const float mi = particle_mass32(P, S, ii, ti);
+        const float4 fi = S.f4[ii];
+        const float ai[3] = {fi.x / mi, fi.y / mi, fi.z / mi};
+        const float Pi = S.pres32[ii];
+        float f[kMlpFeatures];
+#pragma unroll
+        for (int k = 0; k < kMlpFeatures; ++k) f[k] = 0.f;
+        traverse_stencil_batched(
+            P, S.cell_start, key_cell, lane, 7u,
+            [&](int j, int slot) {
+                const float4 pj = S.p4[j];
+                const unsigned w = __float_as_uint(pj.w);
+                int dx = unpack_cx(w) - cix, dy = unpack_cy(w) - ciy, dz = unpack_cz(w) - ciz;
+                dx = dx > 1 ? dx - P.cc[0] : (dx < -1 ? dx + P.cc[0] : dx);
+                dy = dy > 1 ? dy - P.cc[1] : (dy < -1 ? dy + P.cc[1] : dy);
+                dz = dz > 1 ? dz - P.cc[2] : (dz < -1 ? dz + P.cc[2] : dz);
+                const int tj = unpack_type(w);
+                tl.p[slot] = make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
+                                         fmaf((float)dz, Q.cw[2], pj.z), __int_as_float(tj));
+                float4 vj = S.v4[j];
+                vj.w = S.pres32[j];
+                tl.v[slot] = vj;
+                const float4 fj = S.f4[j];
+                const float mj = particle_mass32(P, S, j, tj);
+                tl.a[slot] = make_float4(fj.x / mj, fj.y / mj, fj.z / mj, 0.f);
+            },
+            [&](int base, int nb) {
+                if (!active) return;
+                unsigned m = 0;
+#pragma unroll
+                for (int s = 0; s < kWarp; ++s) {
+                    const float4 pj = tl.p[s];
+                    const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+                    const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
+                    m |= (s < nb && r2 < Q.RP2) ? (1u << s) : 0u;
+                }
+                const int self = i - base;
+                if (self >= 0 && self < kWarp) m &= ~(1u << self);
+                while (m) {
+                    const int s = __ffs(m) - 1;
+                    m &= m - 1;
+                    const float4 pj = tl.p[s];
+                    const float4 vj = tl.v[s];
+                    const float4 aj = tl.a[s];
+                    const int tj = __float_as_int(pj.w);
+                    const float q[3] = {pj.x - pi.x, pj.y - pi.y, pj.z - pi.z};
+                    const float r = sqrtf(fmaf(q[0], q[0], fmaf(q[1], q[1], q[2] * q[2])));
+                    const float ir = r > 0.f ? 1.f / r : 0.f;
+                    const float e[3] = {q[0] * ir, q[1] * ir, q[2] * ir};
+                    const float a = fmaf(-r, Q.iRP, 1.f);
+                    const float w = a * a;
+                    const float u[3] = {vj.x - vi.x, vj.y - vi.y, vj.z - vi.z};
+                    const int cls = is_fluid(tj) ? 0 : (is_solid(tj) ? 1 : 2);
+                    f[11 + cls] += w;
+                    for (int d = 0; d < 3; ++d) f[14 + 3 * cls + d] += w * q[d];
+                    for (int d = 0; d < 3; ++d) f[23 + d] += w * u[d];
+                    f[26] += w * (aj.x - ai[0]);
+                    f[27] += w * (aj.y - ai[1]);
+                    f[28] += w * (aj.z - ai[2]);
+                    f[29] += w * e[0] * e[0];
+                    f[30] += w * e[1] * e[1];
+                    f[31] += w * e[2] * e[2];
+                    f[32] += w * e[0] * e[1];
+                    f[33] += w * e[0] * e[2];
+                    f[34] += w * e[1] * e[2];
+                    const float ue = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
+                    f[35] += w * ue;
+                    f[36] += w * (e[1] * u[2] - e[2] * u[1]);
+                    f[37] += w * (e[2] * u[0] - e[0] * u[2]);
+                    f[38] += w * (e[0] * u[1] - e[1] * u[0]);
+                    const float dp = vj.w - Pi;
+                    f[39] += w * dp;
+                    for (int d = 0; d < 3; ++d) f[40 + d] += w * dp * e[d];
+                    f[43] += 1.f;
+                    if (cls == 2)
+                        for (int d = 0; d < 3; ++d) f[44 + d] += w * u[d];
+                    f[47] += w * r * Q.iRP;
+                }
+            });
+        if (!active) continue;
+        // own state and normalisation
+        f[0] = vi.x * F.inv_vs;
+        f[1] = vi.y * F.inv_vs;
+        f[2] = vi.z * F.inv_vs;
+        f[3] = ai[0] * F.inv_as;
+        f[4] = ai[1] * F.inv_as;
+        f[5] = ai[2] * F.inv_as;
+        f[6] = Pi * F.inv_Ps;
+        f[7] = S.vsp32[i] / Q.N0p;
+        f[8] = S.div32[i] * Q.dx * F.inv_vs;
+        f[9] = is_fluid(ti) ? 1.f : 0.f;
+        f[10] = is_solid(ti) ? 1.f : 0.f;
+        for (int k = 11; k < 14; ++k) f[k] *= F.inv_W0;
+        for (int k = 14; k < 23; ++k) f[k] *= F.inv_W0 * F.inv_dx;
+        for (int k = 23; k < 26; ++k) f[k] *= F.inv_W0 * F.inv_vs;
+        for (int k = 26; k < 29; ++k) f[k] *= F.inv_W0 * F.inv_as;
+        for (int k = 29; k < 35; ++k) f[k] *= F.inv_W0;
+        for (int k = 35; k < 39; ++k) f[k] *= F.inv_W0 * F.inv_vs;
+        for (int k = 39; k < 43; ++k) f[k] *= F.inv_W0 * F.inv_Ps;
+        f[43] *= 0.01f;
+        for (int k = 44; k < 47; ++k) f[k] *= F.inv_W0 * F.inv_vs;
+        f[47] *= F.inv_W0;
+        __align__(16) __nv_bfloat16 h[kMlpIn];
+        for (int k = 0; k < kMlpIn; ++k) h[k] = __float2bfloat16_rn(k < kMlpFeatures ? f[k] : 0.f);
+        uint4 *dst = reinterpret_cast<uint4 *>(X + (long long)i * kMlpIn);
+        for (int k = 0; k < kMlpIn / 8; ++k) dst[k] = reinterpret_cast<const uint4 *>(h)[k];
+        if (X32)
+            for (int k = 0; k < kMlpFeatures; ++k) X32[(long long)i * kMlpFeatures + k] = f[k];
+    }
+}
+
+__device__ __forceinline__ void abs_pos(const DevParams &P, const float4 p, double *x)
+{
+    const unsigned w = __float_as_uint(p.w);
+    x[0] = P.dmin[0] + unpack_cx(w) * P.cw[0] + (double)p.x;
+    x[1] = P.dmin[1] + unpack_cy(w) * P.cw[1] + (double)p.y;
+    x[2] = P.dmin[2] + unpack_cz(w) * P.cw[2] + (double)p.z;
+}
+
+// start-of-block record of the fluid/debris slots
+__global__ void k_record_start(DevParams P, DevState S, const int *dB, float4 *v0, double *x0, int *orig)
+{
+    FOR_EACH_SLOT(dB, -1, B_SE, i)
+    {
+        const float4 p = S.p4[i];
+        double x[3];
+        abs_pos(P, p, x);
+        for (int d = 0; d < 3; ++d) x0[3 * (long long)i + d] = x[d];
+        v0[i] = S.v4[i];
+        orig[i] = S.pidx[i];
+    }
+}
+
+__global__ void k_inverse_perm(DevParams P, DevState S, int *inv)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.N; i += gridDim.x * blockDim.x) inv[S.pidx[i]] = i;
+}
+
+__device__ __forceinline__ double min_image(const DevParams &P, double d, int k)
+{
+    return d - P.W[k] * rint(d / P.W[k]);
+}
+
+// normalised targets of one recorded row (start slot s)
+__device__ __forceinline__ void row_targets(const DevParams &P, const DevState &S, const FeatScales &F,
+                                            const float4 *v0, const double *x0, const int *orig, const int *inv,
+                                            int s, float *t, double *dv, double *dx)
+{
+    const int j = inv[orig[s]];
+    double x1[3];
+    abs_pos(P, S.p4[j], x1);
+    const float4 v1 = S.v4[j];
+    const float4 vs = v0[s];
+    dv[0] = (double)v1.x - vs.x;
+    dv[1] = (double)v1.y - vs.y;
+    dv[2] = (double)v1.z - vs.z;
+    const double v0d[3] = {vs.x, vs.y, vs.z};
+    const double Kdt = (double)F.K * F.dt;
+    for (int d = 0; d < 3; ++d) {
+        dx[d] = min_image(P, x1[d] - x0[3 * (long long)s + d], d);
+        t[d] = (float)(dv[d] / (Kdt * F.as));
+        const double res = dx[d] - Kdt * v0d[d] - 0.5 * (F.K - 1.0) * F.dt * dv[d];
+        t[3 + d] = (float)(res / (Kdt * Kdt * F.as));
+    }
+}
+
+// append a sampled subset of the recorded rows to the pool (ring buffer)
+__global__ void k_record_end(DevParams P, DevState S, const int *dB, FeatScales F, const float4 *v0,
+                             const double *x0, const int *orig, const int *inv, const __nv_bfloat16 *X,
+                             __nv_bfloat16 *poolX, float *poolT, unsigned long long *cursor, long long cap,
+                             unsigned keep_threshold, unsigned long long seed)
+{
+    FOR_EACH_SLOT(dB, -1, B_SE, s)
+    {
+        if ((unsigned)(mix64(seed ^ (unsigned long long)s) >> 32) > keep_threshold) continue;
+        float t[6];
+        double dv[3], dx[3];
+        row_targets(P, S, F, v0, x0, orig, inv, s, t, dv, dx);
+        bool finite = true;
+        for (int k = 0; k < 6; ++k) finite = finite && isfinite(t[k]);
+        if (!finite) continue;
+        const long long r = (long long)(atomicAdd(cursor, 1ull) % (unsigned long long)cap);
+        const uint4 *src = reinterpret_cast<const uint4 *>(X + (long long)s * kMlpIn);
+        uint4 *dst = reinterpret_cast<uint4 *>(poolX + r * kMlpIn);
+        for (int k = 0; k < kMlpIn / 8; ++k) dst[k] = src[k];
+        for (int k = 0; k < kMlpOut; ++k) poolT[r * kMlpOut + k] = k < 6 ? t[k] : 0.f;
+    }
+}
+
+// judge: prediction of the block (outputs Y of the start features) against
+// what the solver did; sums of squares over fluid rows
+__global__ void k_judge(DevParams P, DevState S, const int *dB, FeatScales F, const float4 *v0, const double *x0,
+                        const int *orig, const int *inv, const float *Y, double *acc)
+{
+    double e[4] = {0.0, 0.0, 0.0, 0.0};  // |dx err|^2, |dx|^2, |dv err|^2, |dv|^2
+    FOR_EACH_SLOT(dB, -1, B_FE, s)
+    {
+        float t[6];
+        double dv[3], dx[3];
+        row_targets(P, S, F, v0, x0, orig, inv, s, t, dv, dx);
+        const double Kdt = (double)F.K * F.dt;
+        const float4 vs = v0[s];
+        const double v0d[3] = {vs.x, vs.y, vs.z};
+        for (int d = 0; d < 3; ++d) {
+            const double pdv = (double)Y[(long long)s * kMlpOut + d] * Kdt * F.as;
+            const double pdx = Kdt * v0d[d] + 0.5 * (F.K - 1.0) * F.dt * pdv +
+                               (double)Y[(long long)s * kMlpOut + 3 + d] * Kdt * Kdt * F.as;
+            e[0] += (pdx - dx[d]) * (pdx - dx[d]);
+            e[1] += dx[d] * dx[d];
+            e[2] += (pdv - dv[d]) * (pdv - dv[d]);
+            e[3] += dv[d] * dv[d];
+        }
+    }
+    for (int k = 0; k < 4; ++k) {
+        double v = e[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(acc + k, v);
+    }
+}
+
+// every prediction of the rows that will be applied is finite
+__global__ void k_check_finite(const int *dB, const float *Y, int solids_too, int *bad)
+{
+    FOR_EACH_SLOT(dB, -1, solids_too ? B_SE : B_FE, i)
+    {
+        for (int k = 0; k < kMlpTargets; ++k)
+            if (!isfinite(Y[(long long)i * kMlpOut + k])) atomicExch(bad, 1);
+    }
+}
+
+// apply the prediction to the fluid slots (and to individual debris
+// particles when they are not rigid bodies)
+__global__ void k_apply32(DevParams P, DevState S, const int *dB, FeatScales F, const float *Y, int solids_too,
+                          int *bad)
+{
+    const int N = P.N;
+    const int end_key = solids_too ? B_SE : B_FE;
+    FOR_EACH_SLOT(dB, -1, end_key, i)
+    {
+        const float *y = Y + (long long)i * kMlpOut;
+        const float Kdt = F.K * F.dt;
+        float4 p = S.p4[i];
+        float4 v = S.v4[i];
+        const float dvx = y[0] * Kdt * F.as, dvy = y[1] * Kdt * F.as, dvz = y[2] * Kdt * F.as;
+        const float h = 0.5f * (F.K - 1.f) * F.dt, c = Kdt * Kdt * F.as;
+        const float dxx = Kdt * v.x + h * dvx + y[3] * c;
+        const float dxy = Kdt * v.y + h * dvy + y[4] * c;
+        const float dxz = Kdt * v.z + h * dvz + y[5] * c;
+        if (!(isfinite(dxx) && isfinite(dxy) && isfinite(dxz) && isfinite(dvx) && isfinite(dvy) && isfinite(dvz))) {
+            atomicExch(bad, 1);
+            continue;
+        }
+        const int t = unpack_type(__float_as_uint(p.w));
+        if (is_fluid(t)) {
+            p.x += dxx;
+            p.y += dxy;
+            p.z += dxz;
+            v.x += dvx;
+            v.y += dvy;
+            v.z += dvz;
+            S.p4[i] = p;
+            S.v4[i] = v;
+        } else {
+            // debris without rigid bodies: FP64 master state, then the FP32 copy
+            const double dxd[3] = {dxx, dxy, dxz}, dvd[3] = {dvx, dvy, dvz};
+            for (int d = 0; d < 3; ++d) {
+                const double a = S.pos[d * N + i] + dxd[d] - P.dmin[d];
+                S.pos[d * N + i] = (a - P.W[d] * floor(a / P.W[d])) + P.dmin[d];
+                S.vel[d * N + i] += dvd[d];
+            }
+        }
+    }
+}
+
+// rigid debris: translate each body by the mean prediction of its members
+__global__ void k_body_translate(DevParams P, DevState S, DevBodies Bd, FeatScales F, const float *Y)
+{
+    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (b >= Bd.B) return;
+    const int N = P.N;
+    const int m0 = Bd.ptr[b], m1 = Bd.ptr[b + 1];
+    const double Kdt = (double)F.K * F.dt;
+    double dV[3] = {0.0, 0.0, 0.0}, dR[3] = {0.0, 0.0, 0.0};
+    for (int m = m0 + lane; m < m1; m += kWarp) {
+        const int i = Bd.slot_of_row[Bd.member_row[m]];
+        const float *y = Y + (long long)i * kMlpOut;
+        for (int d = 0; d < 3; ++d) {
+            dV[d] += (double)y[d] * Kdt * F.as;
+            dR[d] += (double)y[3 + d] * Kdt * Kdt * F.as;
+        }
+    }
+    const double inv = 1.0 / (double)(m1 - m0);
+    double V[3], X[3], Vn[3];
+    for (int d = 0; d < 3; ++d) {
+        dV[d] = warp_sum(dV[d]) * inv;
+        dR[d] = warp_sum(dR[d]) * inv;
+        V[d] = Bd.V[3 * b + d];
+        Vn[d] = V[d] + dV[d];
+        X[d] = Bd.X[3 * b + d] + Kdt * V[d] + 0.5 * (F.K - 1.0) * F.dt * dV[d] + dR[d];
+    }
+    double R[3][3], w[3];
+    const double q[4] = {Bd.q[4 * b], Bd.q[4 * b + 1], Bd.q[4 * b + 2], Bd.q[4 * b + 3]};
+    quat_to_R(q, R);
+    omega_of(R, Bd.Iinv0 + 9 * b, Bd.L + 3 * b, w);
+    __syncwarp();
+    if (lane == 0)
+        for (int d = 0; d < 3; ++d) {
+            Bd.X[3 * b + d] = X[d];
+            Bd.V[3 * b + d] = Vn[d];
+        }
+    for (int m = m0 + lane; m < m1; m += kWarp) {
+        const int i = Bd.slot_of_row[Bd.member_row[m]];
+        const double *r0 = Bd.r0 + 3 * m;
+        double r[3];
+        for (int k = 0; k < 3; k++) r[k] = R[k][0] * r0[0] + R[k][1] * r0[1] + R[k][2] * r0[2];
+        const double v[3] = {Vn[0] + w[1] * r[2] - w[2] * r[1], Vn[1] + w[2] * r[0] - w[0] * r[2],
+                             Vn[2] + w[0] * r[1] - w[1] * r[0]};
+        for (int k = 0; k < 3; k++) {
+            const double a = X[k] + r[k] - P.dmin[k];
+            S.pos[k * N + i] = (a - P.W[k] * floor(a / P.W[k])) + P.dmin[k];
+            S.vel[k * N + i] = v[k];
+        }
+    }
+}
+
+// largest displacement since the last rebuild (FP32 frame), for the decision
+__global__ void k_maxshift32(DevParams P, DevState S, unsigned long long *maxshift)
+{
+    float m2 = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.N; i += gridDim.x * blockDim.x) {
+        const float4 p = S.p4[i], r = S.xref4[i];
+        const float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
+        m2 = fmaxf(m2, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+    }
+    unsigned long long b = __double_as_longlong((double)m2);
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long ob = __shfl_down_sync(kFull, b, o);
+        b = ob > b ? ob : b;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(maxshift, b);
+}
+
+// minibatch of pool rows: row-major and transposed features, targets
+__global__ void k_gather_batch(const __nv_bfloat16 *poolX, const float *poolT, long long count, int B,
+                               unsigned long long seed, __nv_bfloat16 *Xb, __nv_bfloat16 *XTb, float *Tb)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B; i += gridDim.x * blockDim.x) {
+        const long long r = (long long)(mix64(seed ^ (unsigned long long)i * 0x9E3779B97F4A7C15ull) %
+                                        (unsigned long long)count);
+        const __nv_bfloat16 *src = poolX + r * kMlpIn;
+        for (int k = 0; k < kMlpIn; ++k) {
+            const __nv_bfloat16 h = src[k];
+            Xb[(long long)i * kMlpIn + k] = h;
+            XTb[(long long)k * B + i] = h;
+        }
+        for (int k = 0; k < kMlpOut; ++k) Tb[(long long)i * kMlpOut + k] = poolT[r * kMlpOut + k];
+    }
+}
+
+template <class T>
+int salloc(dmph_ctx *ctx, Surrogate *s, T **p, size_t count)
+{
+    if (cudaMalloc((void **)p, count * sizeof(T) + 16) != cudaSuccess) {
+        ctx->err = "surrogate: device allocation failed";
+        return DMPH_ENOMEM;
+    }
+    cudaMemset(*p, 0, count * sizeof(T) + 16);
+    s->allocs.push_back(*p);
+    return DMPH_OK;
+}
+
+#define SA(ptr, n)                                \
+    do {                                          \
+        const int rc_ = salloc(ctx, s, &(ptr), (n)); \
+        if (rc_) return rc_;                      \
+    } while (0)
+
+// ---------------------------------------------------------- MLP driver
+GemmArgs gemm(const __nv_bfloat16 *A, long long lda, const __nv_bfloat16 *B, long long ldb, long long M, int N,
+              long long K, int epi, int *err)
+{
+    GemmArgs g;
+    g.A = A;
+    g.lda = lda;
+    g.B = B;
+    g.ldb = ldb;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.epi = epi;
+    g.err = err;
+    return g;
+}
+
+// forward over rows [0, n) of X (row-major [n][64]) into Y [n][16]
+void mlp_forward(Surrogate *s, const __nv_bfloat16 *X, long long n, float *Y, cudaStream_t st)
+{
+    const MlpParamsDev &M = s->M;
+    const __nv_bfloat16 *in = X;
+    long long ld = kMlpIn;
+    for (int l = 0; l < 3; ++l) {
+        GemmArgs g = gemm(in, ld, M.wb[l], M.in[l], n, kMlpHidden, M.in[l], EPI_RELU, s->d_err);
+        g.bias = M.w + M.boff[l];
+        g.outB = s->H[l & 1];
+        g.ldo = kMlpHidden;
+        launch_gemm(g, 1, st);
+        in = s->H[l & 1];
+        ld = kMlpHidden;
+    }
+    GemmArgs g = gemm(in, ld, M.wb[3], kMlpHidden, n, kMlpOut, kMlpHidden, EPI_OUT, s->d_err);
+    g.bias = M.w + M.boff[3];
+    g.outF = Y;
+    g.ldo = kMlpOut;
+    launch_gemm(g, 1, st);
+}
+
+// loss and gradient of the batch in Xb/XTb/Tb (B rows) into M.grad
+void mlp_backprop(Surrogate *s, cudaStream_t st)
+{
+    const MlpParamsDev &M = s->M;
+    const long long B = s->B;
+    const int ks = (int)(B / 1024);
+    cudaMemsetAsync(s->d_loss, 0, sizeof(float), st);
+    const __nv_bfloat16 *in = s->Xb;
+    long long ld = kMlpIn;
+    for (int l = 0; l < 3; ++l) {
+        GemmArgs g = gemm(in, ld, M.wb[l], M.in[l], B, kMlpHidden, M.in[l], EPI_RELU, s->d_err);
+        g.bias = M.w + M.boff[l];
+        g.outB = s->Hb[l];
+        g.ldo = kMlpHidden;
+        g.outT = s->HTb[l];
+        g.ldT = B;
+        launch_gemm(g, 1, st);
+        in = s->Hb[l];
+        ld = kMlpHidden;
+    }
+    {
+        GemmArgs g = gemm(s->Hb[2], kMlpHidden, M.wb[3], kMlpHidden, B, kMlpOut, kMlpHidden, EPI_OUT, s->d_err);
+        g.bias = M.w + M.boff[3];
+        g.outF = s->Yb;
+        g.ldo = kMlpOut;
+        g.target = s->Tb;
+        g.ldt = kMlpOut;
+        g.n_valid = kMlpTargets;
+        g.grad_scale = 2.f / (float)(B * kMlpTargets);
+        g.loss = s->d_loss;
+        g.outB = s->dY;
+        g.outT = s->dYT;
+        g.ldT = B;
+        launch_gemm(g, 1, st);
+    }
+    // layer 4: dW4^T = H3^T dY, db4, dZ3 = (dY W4) * [H3 > 0]
+    {
+        GemmArgs g = gemm(s->HTb[2], B, s->dYT, B, kMlpHidden, kMlpOut, B, EPI_WGRAD, s->d_err);
+        g.outF = M.grad + M.woff[3];
+        g.ldo = kMlpHidden;
+        g.transpose_out = 1;
+        launch_gemm(g, ks, st);
+        launch_row_sums(s->dYT, B, kMlpOut, (int)B, M.grad + M.boff[3], st);
+        GemmArgs h = gemm(s->dY, kMlpOut, M.wt[3], kMlpOut, B, kMlpHidden, kMlpOut, EPI_BWD_RELU, s->d_err);
+        h.mask = s->Hb[2];
+        h.ldm = kMlpHidden;
+        h.outB = s->dZ[0];
+        h.ldo = kMlpHidden;
+        h.outT = s->dZT[0];
+        h.ldT = B;
+        launch_gemm(h, 1, st);
+    }
+    // hidden layers 3, 2, 1
+    int cur = 0;
+    for (int l = 2; l >= 0; --l) {
+        const __nv_bfloat16 *act_T = l > 0 ? s->HTb[l - 1] : s->XTb;
+        const int nin = M.in[l];
+        GemmArgs g = gemm(s->dZT[cur], B, act_T, B, kMlpHidden, nin, B, EPI_WGRAD, s->d_err);
+        g.outF = M.grad + M.woff[l];
+        g.ldo = nin;
+        launch_gemm(g, ks, st);
+        launch_row_sums(s->dZT[cur], B, kMlpHidden, (int)B, M.grad + M.boff[l], st);
+        if (l == 0) break;
+        GemmArgs h = gemm(s->dZ[cur], kMlpHidden, M.wt[l], kMlpHidden, B, kMlpHidden, kMlpHidden, EPI_BWD_RELU,
+                          s->d_err);
+        h.mask = s->Hb[l - 1];
+        h.ldm = kMlpHidden;
+        h.outB = s->dZ[cur ^ 1];
+        h.ldo = kMlpHidden;
+        h.outT = s->dZT[cur ^ 1];
+        h.ldT = B;
+        launch_gemm(h, 1, st);
+        cur ^= 1;
+    }
+}
+
+void feat_scales(dmph_ctx *ctx, Surrogate *s)
+{
+    const dmph_params &p = ctx->p;
+    const double rho = p.density[1] > 0 ? p.density[1] : 1000.0;
+    const double c0 = p.bulk_modulus[1] > 0 ? std::sqrt(p.bulk_modulus[1] / rho) : 10.0;
+    const double vs = c0 / 10.0;
+    const double g = std::sqrt(p.gravity[0] * p.gravity[0] + p.gravity[1] * p.gravity[1] + p.gravity[2] * p.gravity[2]);
+    const double as = g > 0 ? g : 1.0;
+    const double W0 = ctx->Q.N0p32 / ctx->Q.Bp;
+    FeatScales &F = s->fs;
+    F.vs = (float)vs;
+    F.as = (float)as;
+    F.inv_vs = (float)(1.0 / vs);
+    F.inv_as = (float)(1.0 / as);
+    F.inv_Ps = (float)(1.0 / (rho * vs * vs));
+    F.inv_W0 = (float)(1.0 / W0);
+    F.inv_dx = (float)(1.0 / ctx->P.dx);
+    F.K = (float)s->prm.substeps;
+    F.dt = (float)ctx->P.dt;
+}
+
+int grid_slots(const dmph_ctx *ctx) { return ctx->sms * 4; }
+
+// pass A, pass B and the features at the current state
+void enqueue_features(dmph_ctx *ctx, Surrogate *s, float *x32, cudaStream_t st)
+{
+    launch_pass_a32(ctx->P, ctx->Q, ctx->S, ctx->dB, CR_WET, ctx->var_a, st);
+    launch_pass_b32(ctx->P, ctx->Q, ctx->S, ctx->dB, ctx->var_b, st);
+    static const int g = persistent_grid((const void *)k_features32, kFeatWarps * kWarp);
+    k_features32<<<g, kFeatWarps * kWarp, 0, st>>>(ctx->P, ctx->Q, ctx->S, ctx->dB, s->fs, s->X, x32);
+}
+
+int check_err(dmph_ctx *ctx, Surrogate *s)
+{
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (e) {
+        ctx->err = "surrogate: a tensor-core wait ran out";
+        return DMPH_ETIMEOUT;
+    }
+    return DMPH_OK;
+}
+
+// one block of K plain steps that records samples (and, with judge, scores
+// the network's prediction of the same block)
+int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev)
+{
+    cudaStream_t st = ctx->st;
+    enqueue_features(ctx, s, nullptr, st);
+    const int gs = grid_slots(ctx);
+    k_record_start<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->v0, s->x0, s->orig);
+    if (judge) mlp_forward(s, s->X, s->n_rows, s->Y, st);
+    CK(cudaGetLastError());
+    for (int k = 0; k < s->prm.substeps; ++k) {
+        const int rc = step_once(ctx);
+        if (rc) return rc;
+    }
+    k_inverse_perm<<<gs, 256, 0, st>>>(ctx->P, ctx->S, s->inv);
+    if (judge) {
+        CK(cudaMemsetAsync(s->d_acc, 0, 4 * sizeof(double), st));
+        k_judge<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->v0, s->x0, s->orig, s->inv, s->Y, s->d_acc);
+    }
+    // keep about pool/16 rows of every block
+    const double keep = std::min(1.0, (double)s->pool_cap / 16.0 / std::max(1, s->n_rows));
+    const unsigned thr = (unsigned)std::min(4294967295.0, keep * 4294967296.0);
+    k_record_end<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->v0, s->x0, s->orig, s->inv, s->X, s->poolX,
+                                     s->poolT, s->d_cursor, s->pool_cap, thr, s->block_seed++ * 0x632BE59BD9B4E019ull);
+    CK(cudaGetLastError());
+    unsigned long long cur = 0;
+    double acc[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(&cur, s->d_cursor, sizeof(cur), cudaMemcpyDeviceToHost, st));
+    if (judge) CK(cudaMemcpyAsync(acc, s->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    s->pool_count = std::min<long long>((long long)cur, s->pool_cap);
+    s->st.samples = (int64_t)cur;
+    s->st.plain_blocks++;
+    if (judge) {
+        *ex = std::sqrt(acc[0] / std::max(acc[1], 1e-300));
+        *ev = std::sqrt(acc[2] / std::max(acc[3], 1e-300));
+    }
+    return check_err(ctx, s);
+}
+
+int train(dmph_ctx *ctx, Surrogate *s, int iters, float *loss_out)
+{
+    if (s->pool_count < s->B / 4) {
+        ctx->err = "surrogate: too few samples to train (collect first)";
+        return DMPH_EINVAL;
+    }
+    cudaStream_t st = ctx->st;
+    float loss = 0.f;
+    for (int it = 0; it < iters; ++it) {
+        k_gather_batch<<<ctx->sms * 4, 256, 0, st>>>(s->poolX, s->poolT, s->pool_count, s->B,
+                                                     0xA5A5ull + (unsigned long long)s->st.train_iters * 0x9E37ull,
+                                                     s->Xb, s->XTb, s->Tb);
+        mlp_backprop(s, st);
+        s->adam_t++;
+        launch_adam(s->M, s->prm.learning_rate, s->adam_t, st);
+        launch_weights_to_bf16(s->M, st);
+        CK(cudaGetLastError());
+        s->st.train_iters++;
+    }
+    CK(cudaMemcpyAsync(&loss, s->d_loss, sizeof(float), cudaMemcpyDeviceToHost, st));
+    const int rc = check_err(ctx, s);
+    if (rc) return rc;
+    loss /= (float)((double)s->B * kMlpTargets);  // mean squared error of the last batch
+    s->st.last_loss = loss;
+    if (loss_out) *loss_out = loss;
+    return DMPH_OK;
+}
+
+// one surrogate call: K steps of simulated time
+int surrogate_block(dmph_ctx *ctx, Surrogate *s)
+{
+    cudaStream_t st = ctx->st;
+    enqueue_features(ctx, s, nullptr, st);
+    mlp_forward(s, s->X, s->n_rows, s->Y, st);
+    CK(cudaMemsetAsync(s->d_bad, 0, sizeof(int), st));
+    const int gs = grid_slots(ctx);
+    const bool bodies = ctx->Bd.B > 0;
+    // a non-finite prediction leaves the state untouched
+    k_check_finite<<<gs, 256, 0, st>>>(ctx->dB, s->Y, 1, s->d_bad);
+    int bad = 0;
+    CK(cudaMemcpyAsync(&bad, s->d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (bad) {
+        ctx->err = "surrogate: non-finite prediction";
+        return DMPH_ENAN;
+    }
+    k_apply32<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->Y, bodies ? 0 : 1, s->d_bad);
+    if (bodies) k_body_translate<<<(ctx->Bd.B * 32 + 255) / 256, 256, 0, st>>>(ctx->P, ctx->S, ctx->Bd, s->fs, s->Y);
+    launch_sync_solids32(ctx->P, ctx->S, ctx->dB, st);
+    // the forces of the next evaluation start from zero like after a drift
+    CK(cudaMemsetAsync(ctx->S.f4, 0, sizeof(float4) * (size_t)ctx->P.N, st));
+    CK(cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), st));
+    k_maxshift32<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->maxshift);
+    launch_decide(ctx->P, ctx->maxshift, ctx->dB, 0, st);
+    CK(cudaGetLastError());
+    int flags[2] = {0, 0};
+    CK(cudaMemcpyAsync(&flags[0], ctx->dB + B_NEED, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&flags[1], s->d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (flags[1]) {
+        ctx->err = "surrogate: non-finite prediction";
+        return DMPH_ENAN;
+    }
+    if (flags[0]) {
+        enqueue_rebuild(ctx, false, st);
+        ctx->launches += rebuild_launches(ctx, false);
+        ctx->host_rebuilds++;
+    }
+    ctx->launches += 16 + (bodies ? 1 : 0);
+    for (int k = 0; k < s->prm.substeps; ++k) advance_host_clock(ctx);
+    s->st.calls++;
+    return check_err(ctx, s);
+}
+
+bool surrogate_allowed(const dmph_ctx *ctx, const Surrogate *s)
+{
+    // moving walls and the first step (wall centres move while Time <= 0) run plain
+    const double t1 = ctx->time + s->prm.substeps * ctx->P.dt;
+    return 0.0 < ctx->time && !(t1 >= 0.2 && 0.4 >= ctx->time);
+}
+
+}  // namespace
+
+void surrogate_release(dmph_ctx *ctx)
+{
+    Surrogate *s = ctx->sg;
+    if (!s) return;
+    for (void *p : s->allocs) cudaFree(p);
+    delete s;
+    ctx->sg = nullptr;
+}
+
+}  // namespace dmph
+
+// ================================================================ C ABI
+extern "C" int dmph_surrogate_params_default(dmph_surrogate_params *p)
+{
+    if (!p) return DMPH_EINVAL;
+    p->substeps = 8;
+    p->check_interval = 50;
+    p->tolerance = 0.02;
+    p->fallback_blocks = 50;
+    p->train_iters_per_block = 4;
+    p->batch = 65536;
+    p->pool_rows = 1 << 22;
+    p->learning_rate = 1e-3f;
+    p->seed = 1234;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_surrogate_enable(dmph_ctx *ctx, const dmph_surrogate_params *prm)
+{
+    using namespace dmph;
+    if (!ctx || !prm) return DMPH_EINVAL;
+    if (!ctx->fp32) {
+        ctx->err = "the surrogate runs on the FP32 split build";
+        return DMPH_EINVAL;
+    }
+    if (prm->substeps < 1 || prm->check_interval < 1 || prm->batch < 8192 || prm->batch % 8192 ||
+        prm->pool_rows < prm->batch || !(prm->tolerance > 0) || prm->fallback_blocks < 1) {
+        ctx->err = "surrogate parameters out of range (batch a multiple of 8192, pool >= batch)";
+        return DMPH_ERANGE;
+    }
+    surrogate_release(ctx);
+    Surrogate *s = new Surrogate();
+    ctx->sg = s;
+    s->prm = *prm;
+    const long long N = ctx->P.N;
+    int b[B_COUNT];
+    int rc = read_bounds(ctx, b);
+    if (rc) return rc;
+    s->n_rows = b[B_SE];
+    // parameters
+    MlpParamsDev &M = s->M;
+    const int ins[4] = {kMlpIn, kMlpHidden, kMlpHidden, kMlpHidden};
+    const int outs[4] = {kMlpHidden, kMlpHidden, kMlpHidden, kMlpOut};
+    int off = 0;
+    for (int l = 0; l < 4; ++l) {
+        M.in[l] = ins[l];
+        M.out[l] = outs[l];
+        M.woff[l] = off;
+        off += ins[l] * outs[l];
+        M.boff[l] = off;
+        off += outs[l];
+    }
+    M.count = off;
+    SA(M.w, off);
+    SA(M.m, off);
+    SA(M.v, off);
+    SA(M.grad, off);
+    for (int l = 0; l < 4; ++l) {
+        SA(M.wb[l], (size_t)ins[l] * outs[l]);
+        SA(M.wt[l], (size_t)ins[l] * outs[l]);
+    }
+    // He-uniform initial weights (mt19937_64 from the seed), output layer x0.1, zero biases
+    std::vector<float> w(off, 0.f);
+    std::mt19937_64 rng(prm->seed);
+    std::uniform_real_distribution<float> U(-1.f, 1.f);
+    for (int l = 0; l < 4; ++l) {
+        const float a = std::sqrt(6.f / (float)(l == 0 ? kMlpFeatures : ins[l])) * (l == 3 ? 0.1f : 1.f);
+        for (int o = 0; o < outs[l]; ++o)
+            for (int k = 0; k < ins[l]; ++k)
+                w[M.woff[l] + o * ins[l] + k] = (l == 0 && k >= kMlpFeatures) ? 0.f : a * U(rng);
+    }
+    CK(cudaMemcpy(M.w, w.data(), sizeof(float) * off, cudaMemcpyHostToDevice));
+    launch_weights_to_bf16(M, ctx->st);
+    // buffers
+    SA(s->X, (size_t)N * kMlpIn);
+    SA(s->Y, (size_t)N * kMlpOut);
+    SA(s->H[0], (size_t)N * kMlpHidden);
+    SA(s->H[1], (size_t)N * kMlpHidden);
+    SA(s->v0, (size_t)N);
+    SA(s->x0, (size_t)N * 3);
+    SA(s->orig, (size_t)N);
+    SA(s->inv, (size_t)N);
+    s->pool_cap = prm->pool_rows;
+    SA(s->poolX, (size_t)s->pool_cap * kMlpIn);
+    SA(s->poolT, (size_t)s->pool_cap * kMlpOut);
+    SA(s->d_cursor, 1);
+    s->B = prm->batch;
+    const size_t B = (size_t)s->B;
+    SA(s->Xb, B * kMlpIn);
+    SA(s->XTb, B * kMlpIn);
+    for (int l = 0; l < 3; ++l) {
+        SA(s->Hb[l], B * kMlpHidden);
+        SA(s->HTb[l], B * kMlpHidden);
+    }
+    for (int l = 0; l < 2; ++l) {
+        SA(s->dZ[l], B * kMlpHidden);
+        SA(s->dZT[l], B * kMlpHidden);
+    }
+    SA(s->dY, B * kMlpOut);
+    SA(s->dYT, B * kMlpOut);
+    SA(s->Yb, B * kMlpOut);
+    SA(s->Tb, B * kMlpOut);
+    SA(s->d_loss, 1);
+    SA(s->d_err, 1);
+    SA(s->d_bad, 1);
+    SA(s->d_acc, 4);
+    feat_scales(ctx, s);
+    CK(cudaStreamSynchronize(ctx->st));
+    drop_graph(ctx);
+    return DMPH_OK;
+}
+
+static dmph::Surrogate *need_sg(dmph_ctx *ctx)
+{
+    if (!ctx) return nullptr;
+    if (!ctx->sg) ctx->err = "surrogate not enabled (dmph_surrogate_enable)";
+    return ctx->sg;
+}
+
+extern "C" int dmph_surrogate_collect(dmph_ctx *ctx, int nblocks)
+{
+    dmph::Surrogate *s = need_sg(ctx);
+    if (!s) return DMPH_EINVAL;
+    for (int k = 0; k < nblocks; ++k) {
+        const int rc = dmph::plain_block(ctx, s, false, nullptr, nullptr);
+        if (rc) return rc;
+    }
+    return DMPH_OK;
+}
+
+extern "C" int dmph_surrogate_train(dmph_ctx *ctx, int iters, float *loss)
+{
+    dmph::Surrogate *s = need_sg(ctx);
+    if (!s) return DMPH_EINVAL;
+    return dmph::train(ctx, s, iters, loss);
+}
+
+extern "C" int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks)
+{
+    using namespace dmph;
+    Surrogate *s = need_sg(ctx);
+    if (!s) return DMPH_EINVAL;
+    for (int k = 0; k < nblocks; ++k) {
+        int rc = DMPH_OK;
+        if (s->fallback_left > 0 || !surrogate_allowed(ctx, s)) {
+            // plain block: keep collecting and training while the surrogate is out
+            rc = plain_block(ctx, s, false, nullptr, nullptr);
+            if (!rc && s->fallback_left > 0) {
+                s->fallback_left--;
+                if (s->prm.train_iters_per_block > 0 && s->pool_count >= s->B / 4)
+                    rc = train(ctx, s, s->prm.train_iters_per_block, nullptr);
+            }
+        } else if (s->since_check >= s->prm.check_interval) {
+            double ex = 0, ev = 0;
+            rc = plain_block(ctx, s, true, &ex, &ev);
+            s->since_check = 0;
+            s->st.judged++;
+            s->st.last_error = ex;
+            s->st.last_error_v = ev;
+            if (!rc && !(ex <= s->prm.tolerance)) {
+                s->st.fallbacks++;
+                s->fallback_left = s->prm.fallback_blocks;
+            }
+        } else {
+            rc = surrogate_block(ctx, s);
+            if (rc == DMPH_ENAN) {
+                // nothing was applied: fall back and continue with the plain solver
+                s->st.fallbacks++;
+                s->fallback_left = s->prm.fallback_blocks;
+                ctx->err.clear();
+                rc = DMPH_OK;
+            }
+            s->since_check++;
+        }
+        if (rc) return rc;
+    }
+    return DMPH_OK;
+}
+
+extern "C" int dmph_surrogate_get_stats(dmph_ctx *ctx, dmph_surrogate_stats *out)
+{
+    dmph::Surrogate *s = need_sg(ctx);
+    if (!s || !out) return DMPH_EINVAL;
+    *out = s->st;
+    out->pool_rows = s->pool_count;
+    out->in_fallback = s->fallback_left > 0 ? 1 : 0;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_surrogate_get_weights(dmph_ctx *ctx, float *w, int count)
+{
+    dmph::Surrogate *s = need_sg(ctx);
+    if (!s) return DMPH_EINVAL;
+    if (!w) return s->M.count;
+    if (count != s->M.count) return DMPH_ERANGE;
+    CK(cudaMemcpy(w, s->M.w, sizeof(float) * count, cudaMemcpyDeviceToHost));
+    return DMPH_OK;
+}
+
+extern "C" int dmph_surrogate_set_weights(dmph_ctx *ctx, const float *w, int count)
+{
+    dmph::Surrogate *s = need_sg(ctx);
+    if (!s || !w) return DMPH_EINVAL;
+    if (count != s->M.count) return DMPH_ERANGE;
+    CK(cudaMemcpy(s->M.w, w, sizeof(float) * count, cudaMemcpyHostToDevice));
+    dmph::launch_weights_to_bf16(s->M, ctx->st);
+    CK(cudaStreamSynchronize(ctx->st));
+    return DMPH_OK;
+}
+
+// MLP on host rows (n x 64 features, FP32) -> n x 16 outputs
+extern "C" int dmph_mlp_forward(dmph_ctx *ctx, const float *X, int n, float *Y)
+{
+    using namespace dmph;
+    Surrogate *s = need_sg(ctx);
+    if (!s || !X || !Y || n <= 0) return DMPH_EINVAL;
+    if (n > ctx->P.N) return DMPH_ERANGE;
+    std::vector<__nv_bfloat16> xb((size_t)n * kMlpIn);
+    for (size_t i = 0; i < xb.size(); ++i) xb[i] = __float2bfloat16_rn(X[i]);
+    CK(cudaMemcpyAsync(s->X, xb.data(), xb.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, ctx->st));
+    mlp_forward(s, s->X, n, s->Y, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(Y, s->Y, sizeof(float) * (size_t)n * kMlpOut, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return check_err(ctx, s);
+}
+
+// loss and parameter gradient of one batch of host rows (n = the batch size)
+extern "C" int dmph_mlp_gradient(dmph_ctx *ctx, const float *X, const float *T, int n, float *grad, float *loss)
+{
+    using namespace dmph;
+    Surrogate *s = need_sg(ctx);
+    if (!s || !X || !T || !grad) return DMPH_EINVAL;
+    if (n != s->B) {
+        ctx->err = "dmph_mlp_gradient: n must equal the training batch";
+        return DMPH_ERANGE;
+    }
+    std::vector<__nv_bfloat16> xb((size_t)n * kMlpIn), xt((size_t)n * kMlpIn);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < kMlpIn; ++k) {
+            const __nv_bfloat16 h = __float2bfloat16_rn(X[(size_t)i * kMlpIn + k]);
+            xb[(size_t)i * kMlpIn + k] = h;
+            xt[(size_t)k * n + i] = h;
+        }
+    CK(cudaMemcpyAsync(s->Xb, xb.data(), xb.size() * 2, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(s->XTb, xt.data(), xt.size() * 2, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(s->Tb, T, sizeof(float) * (size_t)n * kMlpOut, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemsetAsync(s->M.grad, 0, sizeof(float) * s->M.count, ctx->st));
+    mlp_backprop(s, ctx->st);
+    CK(cudaGetLastError());
+    float l = 0.f;
+    CK(cudaMemcpyAsync(grad, s->M.grad, sizeof(float) * s->M.count, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(&l, s->d_loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemsetAsync(s->M.grad, 0, sizeof(float) * s->M.count, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (loss) *loss = l / (float)((double)n * kMlpTargets);
+    return check_err(ctx, s);
+}
+
+// features of the current state (pass A, pass B, features) for the fluid and
+// debris slots [0, rows), FP32, rows x 48; returns rows through *rows
+extern "C" int dmph_surrogate_features(dmph_ctx *ctx, float *F, int *rows)
+{
+    using namespace dmph;
+    Surrogate *s = need_sg(ctx);
+    if (!s || !F) return DMPH_EINVAL;
+    if (!s->feat32) SA(s->feat32, (size_t)ctx->P.N * kMlpFeatures);
+    enqueue_features(ctx, s, s->feat32, ctx->st);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(F, s->feat32, sizeof(float) * (size_t)s->n_rows * kMlpFeatures, cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (rows) *rows = s->n_rows;
+    return DMPH_OK;
+}

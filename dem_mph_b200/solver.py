@@ -55,6 +55,17 @@ def lib():
         L.dmph_ensemble_last_error.argtypes = [vp]
         L.dmph_ensemble_last_error.restype = C.c_char_p
         L.dmph_ensemble_destroy.argtypes = [vp]
+        L.dmph_surrogate_params_default.argtypes = [vp]
+        L.dmph_surrogate_enable.argtypes = [vp, vp]
+        L.dmph_surrogate_collect.argtypes = [vp, C.c_int]
+        L.dmph_surrogate_train.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
+        L.dmph_surrogate_advance.argtypes = [vp, C.c_int]
+        L.dmph_surrogate_get_stats.argtypes = [vp, vp]
+        L.dmph_surrogate_get_weights.argtypes = [vp, vp, C.c_int]
+        L.dmph_surrogate_set_weights.argtypes = [vp, vp, C.c_int]
+        L.dmph_mlp_forward.argtypes = [vp, vp, C.c_int, vp]
+        L.dmph_mlp_gradient.argtypes = [vp, vp, vp, C.c_int, vp, C.POINTER(C.c_float)]
+        L.dmph_surrogate_features.argtypes = [vp, vp, C.POINTER(C.c_int)]
         L.dmph_destroy.argtypes = [vp]
         L.dmph_last_error.argtypes = [vp]
         L.dmph_last_error.restype = C.c_char_p
@@ -177,6 +188,67 @@ class Solver:
 
     def set_variants(self, variant_a, variant_b):
         self._check(lib().dmph_set_variants(self._h, variant_a, variant_b))
+
+    # ---------------------------------------------------------- surrogate
+    def enable_surrogate(self, **kw):
+        """attach the learned K-step surrogate (dmph_surrogate_enable); keyword
+        arguments override fields of dmph_surrogate_params_default"""
+        sp = abi.SurrogateParams()
+        lib().dmph_surrogate_params_default(C.byref(sp))
+        for k, v in kw.items():
+            if not hasattr(sp, k):
+                raise KeyError(k)
+            setattr(sp, k, v)
+        self._check(lib().dmph_surrogate_enable(self._h, C.byref(sp)))
+        self.surrogate_params = sp
+
+    def surrogate_collect(self, nblocks):
+        self._check(lib().dmph_surrogate_collect(self._h, nblocks))
+
+    def surrogate_train(self, iters):
+        loss = C.c_float()
+        self._check(lib().dmph_surrogate_train(self._h, iters, C.byref(loss)))
+        return loss.value
+
+    def surrogate_advance(self, nblocks):
+        self._check(lib().dmph_surrogate_advance(self._h, nblocks))
+
+    def surrogate_stats(self):
+        st = abi.SurrogateStats()
+        self._check(lib().dmph_surrogate_get_stats(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def surrogate_weights(self):
+        n = lib().dmph_surrogate_get_weights(self._h, None, 0)
+        if n < 0:
+            self._check(n)
+        w = np.zeros(n, np.float32)
+        self._check(lib().dmph_surrogate_get_weights(self._h, _ptr(w), n))
+        return w
+
+    def set_surrogate_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._check(lib().dmph_surrogate_set_weights(self._h, _ptr(w), len(w)))
+
+    def mlp_forward(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, abi.MLP_IN)
+        Y = np.zeros((len(X), abi.MLP_OUT), np.float32)
+        self._check(lib().dmph_mlp_forward(self._h, _ptr(X), len(X), _ptr(Y)))
+        return Y
+
+    def mlp_gradient(self, X, T):
+        X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, abi.MLP_IN)
+        T = np.ascontiguousarray(T, dtype=np.float32).reshape(-1, abi.MLP_OUT)
+        g = np.zeros(len(self.surrogate_weights()), np.float32)
+        loss = C.c_float()
+        self._check(lib().dmph_mlp_gradient(self._h, _ptr(X), _ptr(T), len(X), _ptr(g), C.byref(loss)))
+        return g, loss.value
+
+    def surrogate_features(self):
+        F = np.zeros((self.n, abi.MLP_FEATURES), np.float32)
+        rows = C.c_int()
+        self._check(lib().dmph_surrogate_features(self._h, _ptr(F), C.byref(rows)))
+        return F[:rows.value]
 
     def set_profiling(self, on=True):
         self._check(lib().dmph_set_profiling(self._h, 1 if on else 0))

@@ -272,6 +272,68 @@ int dmph_ensemble_info(dmph_ensemble *e, int64_t *kernel_launches, int64_t *step
 const char *dmph_ensemble_last_error(dmph_ensemble *e);
 int dmph_ensemble_destroy(dmph_ensemble *e);
 
+/* Learned surrogate of K solver steps (no counterpart in the reference).
+ * FP32 split build only.  A surrogate call evaluates pass A and pass B at the
+ * current state, computes 48 cell-list aggregated features per fluid and
+ * debris particle, runs a 64-128-128-128-16 MLP (BF16 on the tensor cores,
+ * FP32 accumulation) predicting the K-step velocity increment and the
+ * position-increment residual, and applies them (rigid debris bodies move by
+ * the mean of their members' predictions; walls stay).  The network is
+ * trained (Adam, FP32 master weights) on samples the solver generates:
+ * dmph_surrogate_collect runs plain K-step blocks and records (features,
+ * increments) of a sampled subset of particles into a pool.
+ * dmph_surrogate_advance(ctx, n) advances n blocks of K steps: surrogate
+ * calls, except that every check_interval calls one block runs on the plain
+ * solver as the judge; if the relative L2 error of the predicted
+ * displacements of that block exceeds `tolerance`, the next fallback_blocks
+ * blocks run plain (collecting and training with train_iters_per_block Adam
+ * steps each).  Blocks that would touch the moving-wall window or Time <= 0
+ * run plain too. */
+typedef struct dmph_surrogate_params {
+    int substeps;              /* K (8) */
+    int check_interval;        /* surrogate calls between two judged blocks (50) */
+    double tolerance;          /* judged displacement error that triggers the fallback (0.02) */
+    int fallback_blocks;       /* plain blocks after a fallback (50) */
+    int train_iters_per_block; /* Adam steps per plain block during a fallback (4) */
+    int batch;                 /* training batch, a multiple of 8192 (65536) */
+    int pool_rows;             /* sample pool capacity, >= batch (4,194,304) */
+    float learning_rate;       /* Adam (1e-3) */
+    unsigned long long seed;   /* initial weights */
+} dmph_surrogate_params;
+
+typedef struct dmph_surrogate_stats {
+    int64_t calls;        /* surrogate calls (blocks advanced by the network) */
+    int64_t plain_blocks; /* blocks advanced by the plain solver (collect, judge, fallback) */
+    int64_t judged;       /* judged blocks */
+    int64_t fallbacks;    /* fallbacks triggered */
+    int64_t samples;      /* samples ever appended to the pool */
+    int64_t train_iters;  /* Adam steps */
+    int64_t pool_rows;    /* samples currently in the pool */
+    int in_fallback;      /* 1 while plain blocks of a fallback remain */
+    double last_error;    /* last judged relative L2 error of the displacements */
+    double last_error_v;  /* same for the velocity increments */
+    double last_loss;     /* mean squared error of the last training batch */
+} dmph_surrogate_stats;
+
+int dmph_surrogate_params_default(dmph_surrogate_params *p);
+int dmph_surrogate_enable(dmph_ctx *ctx, const dmph_surrogate_params *p);
+int dmph_surrogate_collect(dmph_ctx *ctx, int nblocks);
+int dmph_surrogate_train(dmph_ctx *ctx, int iters, float *loss);
+int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks);
+int dmph_surrogate_get_stats(dmph_ctx *ctx, dmph_surrogate_stats *out);
+/* parameters: weights [out][in] then biases of each layer, FP32; with w NULL
+ * returns the parameter count */
+int dmph_surrogate_get_weights(dmph_ctx *ctx, float *w, int count);
+int dmph_surrogate_set_weights(dmph_ctx *ctx, const float *w, int count);
+/* the network on host rows: X n x 64 (FP32, rounded to BF16 on upload),
+ * Y n x 16 FP32 (first 6 meaningful); n <= particle count */
+int dmph_mlp_forward(dmph_ctx *ctx, const float *X, int n, float *Y);
+/* mean squared error over the first 6 outputs and the parameter gradient of
+ * one batch of host rows (n = the training batch) */
+int dmph_mlp_gradient(dmph_ctx *ctx, const float *X, const float *T, int n, float *grad, float *loss);
+/* features of the current state for the fluid and debris slots, rows x 48 */
+int dmph_surrogate_features(dmph_ctx *ctx, float *F, int *rows);
+
 /* Per-phase device timing.  With enable != 0, every following step records
  * CUDA events on the context's stream around each phase (this adds event
  * overhead, so time throughput with it off); dmph_get_phase_times returns the

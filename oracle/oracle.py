@@ -39,6 +39,10 @@ def lib():
         L.dmph_oracle_set_bodies.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.dmph_oracle_get_bodies.argtypes = [C.c_void_p] + [C.c_void_p] * 5
         L.dmph_oracle_pressure_force.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.mlp_oracle_param_count.restype = C.c_int
+        L.mlp_oracle_forward.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.mlp_oracle_grad.restype = C.c_double
+        L.mlp_oracle_grad.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         _lib = L
     return _lib
 
@@ -118,6 +122,25 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+
+def mlp_forward(params, X):
+    """CPU restatement of the surrogate MLP (oracle/dmph_mlp_oracle.c): X n x 64 -> n x 16"""
+    P = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    Y = np.zeros((len(X), 16), np.float32)
+    lib().mlp_oracle_forward(P.ctypes.data, len(X), X.ctypes.data, Y.ctypes.data)
+    return Y
+
+
+def mlp_grad(params, X, T, n_valid=6):
+    """(gradient, loss) of the mean squared error over the first n_valid outputs"""
+    P = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    G = np.zeros(lib().mlp_oracle_param_count(), np.float32)
+    loss = lib().mlp_oracle_grad(P.ctypes.data, len(X), X.ctypes.data, T.ctypes.data, n_valid, G.ctypes.data)
+    return G, loss
 
 
 def read_ref_dump(d):
