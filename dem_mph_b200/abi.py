@@ -124,6 +124,7 @@ class SurrogateParams(C.Structure):
         ("pool_rows", C.c_int32),
         ("learning_rate", C.c_float),
         ("seed", C.c_uint64),
+        ("residual", C.c_int32),
     ]
 
 

@@ -7,12 +7,14 @@
 //   3. the MLP on the tensor cores (dmph_mlp.cu) predicts, per particle, the
 //      K-step velocity increment and the residual of the position increment
 //      beyond what the velocity history implies:
-//          dv = y[0:3] * K dt a_s
+//          dv = (y[0:3] a_s + r a0) K dt
 //          dx = K dt v0 + (K - 1)/2 dt dv + y[3:6] * (K dt)^2 a_s
-//      (exact for a constant acceleration with y[3:6] = 0),
-//   4. k_apply32 moves fluid particles; rigid debris bodies are translated by
-//      the mean prediction of their members (orientation and angular
-//      momentum kept); walls stay put,
+//      (exact for a constant acceleration with y[3:6] = 0); a0 is the
+//      acceleration of the block start, r = 1 when the network learns the
+//      residual on it (default) and 0 when it learns the whole increment,
+//   4. k_apply32 moves the fluid particles; debris advance by the solver's
+//      own DEM or rigid-body substeps for the K steps with the fluid force of
+//      the block start held; walls stay put,
 //   5. the usual device-side rebuild decision.
 // Training data come from the solver itself: at the start of a K-step block
 // the features and (x, v) of every fluid/debris particle are recorded, the
@@ -37,7 +39,8 @@ namespace dmph {
 struct FeatScales {
     float inv_vs, inv_as, inv_Ps, inv_W0, inv_dx;
     float vs, as;
-    float K, dt;  // substeps, FP32 time step
+    float K, dt;    // substeps, FP32 time step
+    float residual; // 1: the network predicts dv - K dt a0 (a0 = acceleration at the block start)
 };
 
 struct Surrogate {
@@ -45,12 +48,14 @@ struct Surrogate {
     MlpParamsDev M;
     int adam_t = 0;
     int n_rows = 0;  // fluid + debris slots
+    int n_fluid = 0;
     FeatScales fs{};
     // per-slot buffers (capacity N)
     __nv_bfloat16 *X = nullptr;  // features [N][64]
     float *Y = nullptr;          // outputs [N][16]
     __nv_bfloat16 *H[2] = {nullptr, nullptr};
     float4 *v0 = nullptr;   // start-of-block velocity
+    float4 *a0 = nullptr;   // start-of-block acceleration (pass B force / mass)
     double *x0 = nullptr;   // start-of-block absolute position (3 per row)
     int *orig = nullptr;    // start-of-block original id
     int *inv = nullptr;     // original id -> current slot
@@ -243,7 +248,7 @@ __device__ __forceinline__ void abs_pos(const DevParams &P, const float4 p, doub
 }
 
 // start-of-block record of the fluid/debris slots
-__global__ void k_record_start(DevParams P, DevState S, const int *dB, float4 *v0, double *x0, int *orig)
+__global__ void k_record_start(DevParams P, DevState S, const int *dB, float4 *v0, float4 *a0, double *x0, int *orig)
 {
     FOR_EACH_SLOT(dB, -1, B_SE, i)
     {
@@ -252,6 +257,9 @@ __global__ void k_record_start(DevParams P, DevState S, const int *dB, float4 *v
         abs_pos(P, p, x);
         for (int d = 0; d < 3; ++d) x0[3 * (long long)i + d] = x[d];
         v0[i] = S.v4[i];
+        const float4 f = S.f4[i];
+        const float m = particle_mass32(P, S, i, unpack_type(__float_as_uint(p.w)));
+        a0[i] = make_float4(f.x / m, f.y / m, f.z / m, 0.f);
         orig[i] = S.pidx[i];
     }
 }
@@ -268,9 +276,11 @@ __device__ __forceinline__ double min_image(const DevParams &P, double d, int k)
 
 // normalised targets of one recorded row (start slot s)
 __device__ __forceinline__ void row_targets(const DevParams &P, const DevState &S, const FeatScales &F,
-                                            const float4 *v0, const double *x0, const int *orig, const int *inv,
-                                            int s, float *t, double *dv, double *dx)
+                                            const float4 *v0, const float4 *a0, const double *x0, const int *orig,
+                                            const int *inv, int s, float *t, double *dv, double *dx)
 {
+    const float4 as0 = a0[s];
+    const double base[3] = {F.residual * as0.x / F.as, F.residual * as0.y / F.as, F.residual * as0.z / F.as};
     const int j = inv[orig[s]];
     double x1[3];
     abs_pos(P, S.p4[j], x1);
@@ -283,7 +293,7 @@ __device__ __forceinline__ void row_targets(const DevParams &P, const DevState &
     const double Kdt = (double)F.K * F.dt;
     for (int d = 0; d < 3; ++d) {
         dx[d] = min_image(P, x1[d] - x0[3 * (long long)s + d], d);
-        t[d] = (float)(dv[d] / (Kdt * F.as));
+        t[d] = (float)(dv[d] / (Kdt * F.as) - base[d]);
         const double res = dx[d] - Kdt * v0d[d] - 0.5 * (F.K - 1.0) * F.dt * dv[d];
         t[3 + d] = (float)(res / (Kdt * Kdt * F.as));
     }
@@ -291,16 +301,17 @@ __device__ __forceinline__ void row_targets(const DevParams &P, const DevState &
 
 // append a sampled subset of the recorded rows to the pool (ring buffer)
 __global__ void k_record_end(DevParams P, DevState S, const int *dB, FeatScales F, const float4 *v0,
-                             const double *x0, const int *orig, const int *inv, const __nv_bfloat16 *X,
-                             __nv_bfloat16 *poolX, float *poolT, unsigned long long *cursor, long long cap,
-                             unsigned keep_threshold, unsigned long long seed)
+                             const float4 *a0, const double *x0, const int *orig, const int *inv,
+                             const __nv_bfloat16 *X, __nv_bfloat16 *poolX, float *poolT, unsigned long long *cursor,
+                             long long cap, unsigned keep_threshold, unsigned long long seed)
 {
-    FOR_EACH_SLOT(dB, -1, B_SE, s)
+    // fluid rows: debris move with the DEM and rigid-body substeps in surrogate blocks
+    FOR_EACH_SLOT(dB, -1, B_FE, s)
     {
         if ((unsigned)(mix64(seed ^ (unsigned long long)s) >> 32) > keep_threshold) continue;
         float t[6];
         double dv[3], dx[3];
-        row_targets(P, S, F, v0, x0, orig, inv, s, t, dv, dx);
+        row_targets(P, S, F, v0, a0, x0, orig, inv, s, t, dv, dx);
         bool finite = true;
         for (int k = 0; k < 6; ++k) finite = finite && isfinite(t[k]);
         if (!finite) continue;
@@ -314,20 +325,21 @@ __global__ void k_record_end(DevParams P, DevState S, const int *dB, FeatScales 
 
 // judge: prediction of the block (outputs Y of the start features) against
 // what the solver did; sums of squares over fluid rows
-__global__ void k_judge(DevParams P, DevState S, const int *dB, FeatScales F, const float4 *v0, const double *x0,
-                        const int *orig, const int *inv, const float *Y, double *acc)
+__global__ void k_judge(DevParams P, DevState S, const int *dB, FeatScales F, const float4 *v0, const float4 *a0,
+                        const double *x0, const int *orig, const int *inv, const float *Y, double *acc)
 {
     double e[4] = {0.0, 0.0, 0.0, 0.0};  // |dx err|^2, |dx|^2, |dv err|^2, |dv|^2
     FOR_EACH_SLOT(dB, -1, B_FE, s)
     {
         float t[6];
         double dv[3], dx[3];
-        row_targets(P, S, F, v0, x0, orig, inv, s, t, dv, dx);
+        row_targets(P, S, F, v0, a0, x0, orig, inv, s, t, dv, dx);
         const double Kdt = (double)F.K * F.dt;
-        const float4 vs = v0[s];
+        const float4 vs = v0[s], as0 = a0[s];
         const double v0d[3] = {vs.x, vs.y, vs.z};
+        const double ad[3] = {as0.x, as0.y, as0.z};
         for (int d = 0; d < 3; ++d) {
-            const double pdv = (double)Y[(long long)s * kMlpOut + d] * Kdt * F.as;
+            const double pdv = ((double)Y[(long long)s * kMlpOut + d] * F.as + F.residual * ad[d]) * Kdt;
             const double pdx = Kdt * v0d[d] + 0.5 * (F.K - 1.0) * F.dt * pdv +
                                (double)Y[(long long)s * kMlpOut + 3 + d] * Kdt * Kdt * F.as;
             e[0] += (pdx - dx[d]) * (pdx - dx[d]);
@@ -366,7 +378,16 @@ __global__ void k_apply32(DevParams P, DevState S, const int *dB, FeatScales F, 
         const float Kdt = F.K * F.dt;
         float4 p = S.p4[i];
         float4 v = S.v4[i];
-        const float dvx = y[0] * Kdt * F.as, dvy = y[1] * Kdt * F.as, dvz = y[2] * Kdt * F.as;
+        float ab[3] = {0.f, 0.f, 0.f};
+        if (F.residual != 0.f) {
+            const float4 f = S.f4[i];
+            const float m = particle_mass32(P, S, i, unpack_type(__float_as_uint(p.w)));
+            ab[0] = f.x / m;
+            ab[1] = f.y / m;
+            ab[2] = f.z / m;
+        }
+        const float dvx = (y[0] * F.as + ab[0]) * Kdt, dvy = (y[1] * F.as + ab[1]) * Kdt,
+                    dvz = (y[2] * F.as + ab[2]) * Kdt;
         const float h = 0.5f * (F.K - 1.f) * F.dt, c = Kdt * Kdt * F.as;
         const float dxx = Kdt * v.x + h * dvx + y[3] * c;
         const float dxy = Kdt * v.y + h * dvy + y[4] * c;
@@ -393,58 +414,6 @@ __global__ void k_apply32(DevParams P, DevState S, const int *dB, FeatScales F, 
                 S.pos[d * N + i] = (a - P.W[d] * floor(a / P.W[d])) + P.dmin[d];
                 S.vel[d * N + i] += dvd[d];
             }
-        }
-    }
-}
-
-// rigid debris: translate each body by the mean prediction of its members
-__global__ void k_body_translate(DevParams P, DevState S, DevBodies Bd, FeatScales F, const float *Y)
-{
-    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (b >= Bd.B) return;
-    const int N = P.N;
-    const int m0 = Bd.ptr[b], m1 = Bd.ptr[b + 1];
-    const double Kdt = (double)F.K * F.dt;
-    double dV[3] = {0.0, 0.0, 0.0}, dR[3] = {0.0, 0.0, 0.0};
-    for (int m = m0 + lane; m < m1; m += kWarp) {
-        const int i = Bd.slot_of_row[Bd.member_row[m]];
-        const float *y = Y + (long long)i * kMlpOut;
-        for (int d = 0; d < 3; ++d) {
-            dV[d] += (double)y[d] * Kdt * F.as;
-            dR[d] += (double)y[3 + d] * Kdt * Kdt * F.as;
-        }
-    }
-    const double inv = 1.0 / (double)(m1 - m0);
-    double V[3], X[3], Vn[3];
-    for (int d = 0; d < 3; ++d) {
-        dV[d] = warp_sum(dV[d]) * inv;
-        dR[d] = warp_sum(dR[d]) * inv;
-        V[d] = Bd.V[3 * b + d];
-        Vn[d] = V[d] + dV[d];
-        X[d] = Bd.X[3 * b + d] + Kdt * V[d] + 0.5 * (F.K - 1.0) * F.dt * dV[d] + dR[d];
-    }
-    double R[3][3], w[3];
-    const double q[4] = {Bd.q[4 * b], Bd.q[4 * b + 1], Bd.q[4 * b + 2], Bd.q[4 * b + 3]};
-    quat_to_R(q, R);
-    omega_of(R, Bd.Iinv0 + 9 * b, Bd.L + 3 * b, w);
-    __syncwarp();
-    if (lane == 0)
-        for (int d = 0; d < 3; ++d) {
-            Bd.X[3 * b + d] = X[d];
-            Bd.V[3 * b + d] = Vn[d];
-        }
-    for (int m = m0 + lane; m < m1; m += kWarp) {
-        const int i = Bd.slot_of_row[Bd.member_row[m]];
-        const double *r0 = Bd.r0 + 3 * m;
-        double r[3];
-        for (int k = 0; k < 3; k++) r[k] = R[k][0] * r0[0] + R[k][1] * r0[1] + R[k][2] * r0[2];
-        const double v[3] = {Vn[0] + w[1] * r[2] - w[2] * r[1], Vn[1] + w[2] * r[0] - w[0] * r[2],
-                             Vn[2] + w[0] * r[1] - w[1] * r[0]};
-        for (int k = 0; k < 3; k++) {
-            const double a = X[k] + r[k] - P.dmin[k];
-            S.pos[k * N + i] = (a - P.W[k] * floor(a / P.W[k])) + P.dmin[k];
-            S.vel[k * N + i] = v[k];
         }
     }
 }
@@ -634,6 +603,7 @@ void feat_scales(dmph_ctx *ctx, Surrogate *s)
     F.inv_W0 = (float)(1.0 / W0);
     F.inv_dx = (float)(1.0 / ctx->P.dx);
     F.K = (float)s->prm.substeps;
+    F.residual = s->prm.residual ? 1.f : 0.f;
     F.dt = (float)ctx->P.dt;
 }
 
@@ -667,7 +637,7 @@ int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev)
     cudaStream_t st = ctx->st;
     enqueue_features(ctx, s, nullptr, st);
     const int gs = grid_slots(ctx);
-    k_record_start<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->v0, s->x0, s->orig);
+    k_record_start<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->v0, s->a0, s->x0, s->orig);
     if (judge) mlp_forward(s, s->X, s->n_rows, s->Y, st);
     CK(cudaGetLastError());
     for (int k = 0; k < s->prm.substeps; ++k) {
@@ -677,12 +647,14 @@ int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev)
     k_inverse_perm<<<gs, 256, 0, st>>>(ctx->P, ctx->S, s->inv);
     if (judge) {
         CK(cudaMemsetAsync(s->d_acc, 0, 4 * sizeof(double), st));
-        k_judge<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->v0, s->x0, s->orig, s->inv, s->Y, s->d_acc);
+        k_judge<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->v0, s->a0, s->x0, s->orig, s->inv, s->Y,
+                                    s->d_acc);
     }
     // keep about pool/16 rows of every block
-    const double keep = std::min(1.0, (double)s->pool_cap / 16.0 / std::max(1, s->n_rows));
+    const double keep = std::min(1.0, (double)s->pool_cap / 16.0 / std::max(1, s->n_fluid));
     const unsigned thr = (unsigned)std::min(4294967295.0, keep * 4294967296.0);
-    k_record_end<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->v0, s->x0, s->orig, s->inv, s->X, s->poolX,
+    k_record_end<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->v0, s->a0, s->x0, s->orig, s->inv, s->X,
+                                     s->poolX,
                                      s->poolT, s->d_cursor, s->pool_cap, thr, s->block_seed++ * 0x632BE59BD9B4E019ull);
     CK(cudaGetLastError());
     unsigned long long cur = 0;
@@ -733,12 +705,11 @@ int surrogate_block(dmph_ctx *ctx, Surrogate *s)
 {
     cudaStream_t st = ctx->st;
     enqueue_features(ctx, s, nullptr, st);
-    mlp_forward(s, s->X, s->n_rows, s->Y, st);
+    mlp_forward(s, s->X, s->n_fluid, s->Y, st);
     CK(cudaMemsetAsync(s->d_bad, 0, sizeof(int), st));
     const int gs = grid_slots(ctx);
-    const bool bodies = ctx->Bd.B > 0;
     // a non-finite prediction leaves the state untouched
-    k_check_finite<<<gs, 256, 0, st>>>(ctx->dB, s->Y, 1, s->d_bad);
+    k_check_finite<<<gs, 256, 0, st>>>(ctx->dB, s->Y, 0, s->d_bad);
     int bad = 0;
     CK(cudaMemcpyAsync(&bad, s->d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -746,39 +717,52 @@ int surrogate_block(dmph_ctx *ctx, Surrogate *s)
         ctx->err = "surrogate: non-finite prediction";
         return DMPH_ENAN;
     }
-    k_apply32<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->Y, bodies ? 0 : 1, s->d_bad);
-    if (bodies) k_body_translate<<<(ctx->Bd.B * 32 + 255) / 256, 256, 0, st>>>(ctx->P, ctx->S, ctx->Bd, s->fs, s->Y);
-    launch_sync_solids32(ctx->P, ctx->S, ctx->dB, st);
+    k_apply32<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->Y, 0, s->d_bad);
+    // debris: the solver's own DEM / rigid-body substeps for the K steps, with
+    // the fluid force of the block start held
+    if (s->n_rows > s->n_fluid)
+        for (int k = 0; k < s->prm.substeps; ++k) enqueue_dem(ctx, st);
     // the forces of the next evaluation start from zero like after a drift
     CK(cudaMemsetAsync(ctx->S.f4, 0, sizeof(float4) * (size_t)ctx->P.N, st));
     CK(cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), st));
     k_maxshift32<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->maxshift);
     launch_decide(ctx->P, ctx->maxshift, ctx->dB, 0, st);
     CK(cudaGetLastError());
-    int flags[2] = {0, 0};
-    CK(cudaMemcpyAsync(&flags[0], ctx->dB + B_NEED, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&flags[1], s->d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int need = 0;
+    CK(cudaMemcpyAsync(&need, ctx->dB + B_NEED, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (flags[1]) {
-        ctx->err = "surrogate: non-finite prediction";
-        return DMPH_ENAN;
-    }
-    if (flags[0]) {
+    if (need) {
         enqueue_rebuild(ctx, false, st);
         ctx->launches += rebuild_launches(ctx, false);
         ctx->host_rebuilds++;
     }
-    ctx->launches += 16 + (bodies ? 1 : 0);
+    ctx->launches += 13 + (s->n_rows > s->n_fluid ? s->prm.substeps * dem_launches(ctx) : 0);
     for (int k = 0; k < s->prm.substeps; ++k) advance_host_clock(ctx);
     s->st.calls++;
     return check_err(ctx, s);
 }
 
+// the walls never move when every wall type has zero velocity and spin and
+// an identity rotation (then the moving-wall window changes nothing)
+bool walls_static(const dmph_ctx *ctx)
+{
+    const WallMotion &W = ctx->Wm;
+    for (int t = DMPH_WALL_BEGIN; t < DMPH_WALL_END; ++t)
+        for (int a = 0; a < 3; ++a) {
+            if (W.Vel[t][a] != 0.0 || W.Om[t][a] != 0.0) return false;
+            for (int b = 0; b < 3; ++b)
+                if (W.R[t][a][b] != (a == b ? 1.0 : 0.0)) return false;
+        }
+    return true;
+}
+
 bool surrogate_allowed(const dmph_ctx *ctx, const Surrogate *s)
 {
-    // moving walls and the first step (wall centres move while Time <= 0) run plain
+    // the first step (wall centres move while Time <= 0) and blocks that reach
+    // into the window of moving walls run plain
     const double t1 = ctx->time + s->prm.substeps * ctx->P.dt;
-    return 0.0 < ctx->time && !(t1 >= 0.2 && 0.4 >= ctx->time);
+    if (!(0.0 < ctx->time)) return false;
+    return walls_static(ctx) || !(t1 >= 0.2 && 0.4 >= ctx->time);
 }
 
 }  // namespace
@@ -807,6 +791,7 @@ extern "C" int dmph_surrogate_params_default(dmph_surrogate_params *p)
     p->pool_rows = 1 << 22;
     p->learning_rate = 1e-3f;
     p->seed = 1234;
+    p->residual = 1;
     return DMPH_OK;
 }
 
@@ -832,6 +817,7 @@ extern "C" int dmph_surrogate_enable(dmph_ctx *ctx, const dmph_surrogate_params 
     int rc = read_bounds(ctx, b);
     if (rc) return rc;
     s->n_rows = b[B_SE];
+    s->n_fluid = b[B_FE];
     // parameters
     MlpParamsDev &M = s->M;
     const int ins[4] = {kMlpIn, kMlpHidden, kMlpHidden, kMlpHidden};
@@ -872,6 +858,7 @@ extern "C" int dmph_surrogate_enable(dmph_ctx *ctx, const dmph_surrogate_params 
     SA(s->H[0], (size_t)N * kMlpHidden);
     SA(s->H[1], (size_t)N * kMlpHidden);
     SA(s->v0, (size_t)N);
+    SA(s->a0, (size_t)N);
     SA(s->x0, (size_t)N * 3);
     SA(s->orig, (size_t)N);
     SA(s->inv, (size_t)N);

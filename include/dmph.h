@@ -277,8 +277,9 @@ int dmph_ensemble_destroy(dmph_ensemble *e);
  * current state, computes 48 cell-list aggregated features per fluid and
  * debris particle, runs a 64-128-128-128-16 MLP (BF16 on the tensor cores,
  * FP32 accumulation) predicting the K-step velocity increment and the
- * position-increment residual, and applies them (rigid debris bodies move by
- * the mean of their members' predictions; walls stay).  The network is
+ * position-increment residual, and applies them to the fluid; debris advance
+ * by the solver's own DEM or rigid-body substeps with the fluid force of the
+ * block start held; walls stay.  The network is
  * trained (Adam, FP32 master weights) on samples the solver generates:
  * dmph_surrogate_collect runs plain K-step blocks and records (features,
  * increments) of a sampled subset of particles into a pool.
@@ -287,8 +288,8 @@ int dmph_ensemble_destroy(dmph_ensemble *e);
  * solver as the judge; if the relative L2 error of the predicted
  * displacements of that block exceeds `tolerance`, the next fallback_blocks
  * blocks run plain (collecting and training with train_iters_per_block Adam
- * steps each).  Blocks that would touch the moving-wall window or Time <= 0
- * run plain too. */
+ * steps each).  Blocks at Time <= 0, and blocks that reach into the
+ * moving-wall window while a wall type actually moves, run plain too. */
 typedef struct dmph_surrogate_params {
     int substeps;              /* K (8) */
     int check_interval;        /* surrogate calls between two judged blocks (50) */
@@ -299,6 +300,7 @@ typedef struct dmph_surrogate_params {
     int pool_rows;             /* sample pool capacity, >= batch (4,194,304) */
     float learning_rate;       /* Adam (1e-3) */
     unsigned long long seed;   /* initial weights */
+    int residual;              /* 1: learn dv - K dt a0 (a0 = acceleration at the block start), 0: dv (1) */
 } dmph_surrogate_params;
 
 typedef struct dmph_surrogate_stats {
