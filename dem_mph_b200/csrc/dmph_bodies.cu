@@ -32,118 +32,106 @@ __global__ void k_slot_of_row(int N, const int *__restrict__ pidx, int *__restri
     if (i < N) slot_of_row[pidx[i]] = i;
 }
 
-struct ClumpTile {
-    double x[kWarp], y[kWarp], z[kWarp], vx[kWarp], vy[kWarp], vz[kWarp];
-    int t[kWarp], b[kWarp];
-};
-
-// position of slot j in FP64: absolute (FP64 mode) or in the frame of cell
-// (cix, ciy, ciz) (FP32 split mode)
-template <bool F32>
-__device__ __forceinline__ void load_xv(const DevParams &P, const DevState &S, int j, int cix, int ciy, int ciz,
-                                        double *x, double *v, int *t)
+// One warp per debris particle i (slots [sb, se) walked by a persistent
+// grid); the lanes stride over the candidates of the neighbour cells that
+// can hold a contact partner: contacts need |x_j - x_i| <= dx, so only the
+// neighbour cells within 1.6 dx of i's rebuild-time position (about 8 of the
+// 27) are visited, for the solid and wall classes.  FP64 on the master
+// planes; per-lane partial sums are combined with warp shuffles.
+__global__ void __launch_bounds__(8 * kWarp) k_clump_dem(DevParams P, DevState S, const int *dB)
 {
-    const int N = P.N;
-    if (F32) {
-        const float4 p = S.p4[j];
-        const float4 vv = S.v4[j];
-        const unsigned w = __float_as_uint(p.w);
-        int d[3] = {unpack_cx(w) - cix, unpack_cy(w) - ciy, unpack_cz(w) - ciz};
-        for (int k = 0; k < 3; k++) d[k] = d[k] > 1 ? d[k] - P.cc[k] : (d[k] < -1 ? d[k] + P.cc[k] : d[k]);
-        x[0] = d[0] * P.cw[0] + (double)p.x;
-        x[1] = d[1] * P.cw[1] + (double)p.y;
-        x[2] = d[2] * P.cw[2] + (double)p.z;
-        v[0] = vv.x;
-        v[1] = vv.y;
-        v[2] = vv.z;
-        *t = unpack_type(w);
-    } else {
-        for (int k = 0; k < 3; k++) {
-            x[k] = S.pos[k * N + j];
-            v[k] = S.vel[k * N + j];
-        }
-        *t = S.type[j];
-    }
-}
-
-template <bool F32>
-__global__ void __launch_bounds__(4 * kWarp) k_clump_dem(DevParams P, DevState S, const int *dB, int range)
-{
-    __shared__ ClumpTile tiles[4];
-    ClumpTile &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int N = P.N;
-    FOR_EACH_CHUNK(dB, range, 4, cidx)
-    {
-        const Chunk ch = S.chunks[cidx];
-        const int i = ch.i0 + lane;
-        const bool active = lane < ch.cnt;
-        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-        const int cix = key_cell / (P.cc[1] * P.cc[2]), ciy = (key_cell / P.cc[2]) % P.cc[1], ciz = key_cell % P.cc[2];
-        const int ii = active ? i : ch.i0;
-        double xi[3], vi[3];
-        int ti;
-        load_xv<F32>(P, S, ii, cix, ciy, ciz, xi, vi, &ti);
-        const int bi = S.bid[ii];
-        const double mi = particle_density(S, P, ii, ti) * P.V;
-        double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
-        traverse_stencil(
-            P, S.cell_start, key_cell, lane, active, 6u,
-            [&](int j, int slot) {
-                double x[3], v[3];
-                int t;
-                load_xv<F32>(P, S, j, cix, ciy, ciz, x, v, &t);
-                tl.x[slot] = x[0];
-                tl.y[slot] = x[1];
-                tl.z[slot] = x[2];
-                tl.vx[slot] = v[0];
-                tl.vy[slot] = v[1];
-                tl.vz[slot] = v[2];
-                tl.t[slot] = t;
-                tl.b[slot] = S.bid[j];
-            },
-            [&](int j, int s) {
-                if (j == i || (bi >= 0 && tl.b[s] == bi)) return;
-                double q[3] = {tl.x[s] - xi[0], tl.y[s] - xi[1], tl.z[s] - xi[2]};
-                if (!F32)
-                    for (int k = 0; k < 3; k++) q[k] -= P.W[k] * rint(q[k] / P.W[k]);
-                const double r2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
-                if (r2 > P.dx2 || r2 <= 0.0) return;
-                const int tj = tl.t[s];
-                const double r = sqrt(r2);
-                const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
-                const double ov = P.dx - r;
-                const double u[3] = {tl.vx[s] - vi[0], tl.vy[s] - vi[1], tl.vz[s] - vi[2]};
-                const double un = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
-                const int bj = tl.b[s];
-                const double mj = (bj >= 0 ? S.body_rho[bj] : P.density[tj]) * P.V;
-                const double mij = mi * mj / (mi + mj);
-                const double kn = (4.0 / 3.0) * P.Eeff[ti][tj] * sqrt(P.Reff * ov);
-                const double cn = sqrt(mij * kn) * P.pairDamp[ti][tj];
-                const double kt = P.KtFac[ti][tj] * sqrt(P.Reff * sqrt(ov));
-                const double ct = sqrt(mij * kt) * P.pairDamp[ti][tj];
-                double f[3], ut[3];
-                const double fnm = fmin(-kn * ov + cn * un, 0.0);  // no adhesion
-                for (int k = 0; k < 3; k++) {
-                    f[k] = fnm * e[k];
-                    ut[k] = u[k] - un * e[k];
-                }
-                const double ctot = ct + kt * P.ddt;
-                const double aut = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
-                const double cap = P.pairFric[ti][tj] * fabs(fnm);
-                const double ft = ctot * aut > cap && aut > 0.0 ? cap / aut : ctot;
-                for (int k = 0; k < 3; k++) f[k] += ft * ut[k];
-                for (int k = 0; k < 3; k++) F[k] += f[k];
-                // offset of the contact midpoint from the particle centre: 0.5 q
-                T[0] += 0.5 * (q[1] * f[2] - q[2] * f[1]);
-                T[1] += 0.5 * (q[2] * f[0] - q[0] * f[2]);
-                T[2] += 0.5 * (q[0] * f[1] - q[1] * f[0]);
-            });
-        if (!active) continue;
-        for (int k = 0; k < 3; k++) {
-            S.frc_dem[k * N + i] = F[k];
-            S.frc_dem[(3 + k) * N + i] = T[k];
+    const int sb = dB[B_SB], se = dB[B_SE];
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    for (int i = sb + blockIdx.x * (blockDim.x >> 5) + (int)(threadIdx.x >> 5); i < se; i += nwarps) {
+        const double xi[3] = {S.pos[i], S.pos[N + i], S.pos[2 * N + i]};
+        const double vi[3] = {S.vel[i], S.vel[N + i], S.vel[2 * N + i]};
+        const int ti = S.type[i];
+        const int bi = S.bid[i];
+        const double mi = particle_density(S, P, i, ti) * P.V;
+        // rebuild-time cell and the neighbour cells within reach
+        const int key_cell = (int)(word_key(S.skey[i]) % (unsigned)P.T);
+        int c[3];
+        if (P.dim == 2) {
+            c[0] = key_cell / P.cc[1];
+            c[1] = key_cell % P.cc[1];
+            c[2] = 0;
+        } else {
+            c[0] = key_cell / (P.cc[1] * P.cc[2]);
+            c[1] = (key_cell / P.cc[2]) % P.cc[1];
+            c[2] = key_cell % P.cc[2];
         }
+        // contact partners are within dx now; positions drift at most 0.05 dx
+        // from their rebuild-time values between rebuild checks, and up to
+        // about 0.25 dx inside one surrogate block: 1.6 dx covers both
+        const double reach = 1.6 * P.dx;
+        int lo[3], hi[3];
+        for (int k = 0; k < 3; k++) {
+            const double loc = S.xref[k * N + i] - (P.dmin[k] + c[k] * P.cw[k]);
+            const bool flat = (k == 2 && P.dim == 2);
+            lo[k] = flat ? 0 : (loc < reach ? -1 : 0);
+            hi[k] = flat ? 0 : (P.cw[k] - loc < reach ? 1 : 0);
+        }
+        double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
+        for (int ox = lo[0]; ox <= hi[0]; ++ox)
+            for (int oy = lo[1]; oy <= hi[1]; ++oy)
+                for (int oz = lo[2]; oz <= hi[2]; ++oz) {
+                    const int cell = cell_id(P, c[0] + ox, c[1] + oy, c[2] + oz);
+                    for (int cls = 1; cls < 3; ++cls) {
+                        const int off = cls * P.T + cell;
+                        const int jb = __ldg(S.cell_start + off), je = __ldg(S.cell_start + off + 1);
+                        for (int j = jb + lane; j < je; j += kWarp) {
+                            if (j == i) continue;
+                            const int bj = S.bid[j];
+                            if (bi >= 0 && bj == bi) continue;
+                            double q[3];
+                            for (int k = 0; k < 3; k++) {
+                                q[k] = S.pos[k * N + j] - xi[k];
+                                q[k] -= P.W[k] * rint(q[k] / P.W[k]);
+                            }
+                            const double r2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+                            if (r2 > P.dx2 || r2 <= 0.0) continue;
+                            const int tj = S.type[j];
+                            const double r = sqrt(r2);
+                            const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
+                            const double ov = P.dx - r;
+                            const double u[3] = {S.vel[j] - vi[0], S.vel[N + j] - vi[1], S.vel[2 * N + j] - vi[2]};
+                            const double un = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
+                            const double mj = (bj >= 0 ? S.body_rho[bj] : P.density[tj]) * P.V;
+                            const double mij = mi * mj / (mi + mj);
+                            const double kn = (4.0 / 3.0) * P.Eeff[ti][tj] * sqrt(P.Reff * ov);
+                            const double cn = sqrt(mij * kn) * P.pairDamp[ti][tj];
+                            const double kt = P.KtFac[ti][tj] * sqrt(P.Reff * sqrt(ov));
+                            const double ct = sqrt(mij * kt) * P.pairDamp[ti][tj];
+                            double f[3], ut[3];
+                            const double fnm = fmin(-kn * ov + cn * un, 0.0);  // no adhesion
+                            for (int k = 0; k < 3; k++) {
+                                f[k] = fnm * e[k];
+                                ut[k] = u[k] - un * e[k];
+                            }
+                            const double ctot = ct + kt * P.ddt;
+                            const double aut = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
+                            const double cap = P.pairFric[ti][tj] * fabs(fnm);
+                            const double ft = ctot * aut > cap && aut > 0.0 ? cap / aut : ctot;
+                            for (int k = 0; k < 3; k++) f[k] += ft * ut[k];
+                            for (int k = 0; k < 3; k++) F[k] += f[k];
+                            // offset of the contact midpoint from the particle centre: 0.5 q
+                            T[0] += 0.5 * (q[1] * f[2] - q[2] * f[1]);
+                            T[1] += 0.5 * (q[2] * f[0] - q[0] * f[2]);
+                            T[2] += 0.5 * (q[0] * f[1] - q[1] * f[0]);
+                        }
+                    }
+                }
+        for (int k = 0; k < 3; k++) {
+            F[k] = warp_sum(F[k]);
+            T[k] = warp_sum(T[k]);
+        }
+        if (lane == 0)
+            for (int k = 0; k < 3; k++) {
+                S.frc_dem[k * N + i] = F[k];
+                S.frc_dem[(3 + k) * N + i] = T[k];
+            }
     }
 }
 
@@ -261,8 +249,8 @@ void launch_slot_of_row(const DevParams &P, const int *pidx, int *slot_of_row, c
 // substeps), so the template's FP32 branches are not instantiated.
 void launch_clump_dem(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
 {
-    static const int g = persistent_grid((const void *)k_clump_dem<false>, 4 * kWarp);
-    k_clump_dem<false><<<g, 4 * kWarp, 0, st>>>(P, S, dB, CR_SOLID);
+    static const int g = persistent_grid((const void *)k_clump_dem, 8 * kWarp);
+    k_clump_dem<<<g, 8 * kWarp, 0, st>>>(P, S, dB);
 }
 
 void launch_body_step(const DevParams &P, const DevState &S, const DevBodies &Bd, bool f32, cudaStream_t st)

@@ -299,6 +299,14 @@ __device__ __forceinline__ void row_targets(const DevParams &P, const DevState &
     }
 }
 
+// importance of a row: fast particles (the surge front, splashes) are rare
+// but decide the front position, so they are kept and judged with a weight
+// growing with the squared speed at the block start
+__device__ __forceinline__ float row_weight(const FeatScales &F, float4 v)
+{
+    return 1.f + 20.f * (v.x * v.x + v.y * v.y + v.z * v.z) * F.inv_vs * F.inv_vs;
+}
+
 // append a sampled subset of the recorded rows to the pool (ring buffer)
 __global__ void k_record_end(DevParams P, DevState S, const int *dB, FeatScales F, const float4 *v0,
                              const float4 *a0, const double *x0, const int *orig, const int *inv,
@@ -308,7 +316,8 @@ __global__ void k_record_end(DevParams P, DevState S, const int *dB, FeatScales 
     // fluid rows: debris move with the DEM and rigid-body substeps in surrogate blocks
     FOR_EACH_SLOT(dB, -1, B_FE, s)
     {
-        if ((unsigned)(mix64(seed ^ (unsigned long long)s) >> 32) > keep_threshold) continue;
+        const float u = (float)(mix64(seed ^ (unsigned long long)s) >> 40) * (1.f / 16777216.f);
+        if (u * 4294967296.f > (float)keep_threshold * row_weight(F, v0[s])) continue;
         float t[6];
         double dv[3], dx[3];
         row_targets(P, S, F, v0, a0, x0, orig, inv, s, t, dv, dx);
@@ -324,7 +333,7 @@ __global__ void k_record_end(DevParams P, DevState S, const int *dB, FeatScales 
 }
 
 // judge: prediction of the block (outputs Y of the start features) against
-// what the solver did; sums of squares over fluid rows
+// what the solver did; speed-weighted sums of squares over fluid rows
 __global__ void k_judge(DevParams P, DevState S, const int *dB, FeatScales F, const float4 *v0, const float4 *a0,
                         const double *x0, const int *orig, const int *inv, const float *Y, double *acc)
 {
@@ -338,14 +347,15 @@ __global__ void k_judge(DevParams P, DevState S, const int *dB, FeatScales F, co
         const float4 vs = v0[s], as0 = a0[s];
         const double v0d[3] = {vs.x, vs.y, vs.z};
         const double ad[3] = {as0.x, as0.y, as0.z};
+        const double wgt = row_weight(F, vs);
         for (int d = 0; d < 3; ++d) {
             const double pdv = ((double)Y[(long long)s * kMlpOut + d] * F.as + F.residual * ad[d]) * Kdt;
             const double pdx = Kdt * v0d[d] + 0.5 * (F.K - 1.0) * F.dt * pdv +
                                (double)Y[(long long)s * kMlpOut + 3 + d] * Kdt * Kdt * F.as;
-            e[0] += (pdx - dx[d]) * (pdx - dx[d]);
-            e[1] += dx[d] * dx[d];
-            e[2] += (pdv - dv[d]) * (pdv - dv[d]);
-            e[3] += dv[d] * dv[d];
+            e[0] += wgt * (pdx - dx[d]) * (pdx - dx[d]);
+            e[1] += wgt * dx[d] * dx[d];
+            e[2] += wgt * (pdv - dv[d]) * (pdv - dv[d]);
+            e[3] += wgt * dv[d] * dv[d];
         }
     }
     for (int k = 0; k < 4; ++k) {

@@ -286,7 +286,9 @@ int dmph_ensemble_destroy(dmph_ensemble *e);
  * dmph_surrogate_advance(ctx, n) advances n blocks of K steps: surrogate
  * calls, except that every check_interval calls one block runs on the plain
  * solver as the judge; if the relative L2 error of the predicted
- * displacements of that block exceeds `tolerance`, the next fallback_blocks
+ * displacements of that block (each particle weighted by 1 + 20 |v0|^2 / vs^2,
+ * vs = c0 / 10, so that the fast particles of the surge front count) exceeds
+ * `tolerance`, the next fallback_blocks
  * blocks run plain (collecting and training with train_iters_per_block Adam
  * steps each).  Blocks at Time <= 0, and blocks that reach into the
  * moving-wall window while a wall type actually moves, run plain too. */
