@@ -125,14 +125,18 @@ __global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm,
 // per-lane bitmask of the candidates within the cut-off (a branch-free,
 // fully unrolled distance test), then each lane walks its own set bits, so
 // the kernel-weight arithmetic runs only for pairs that contribute.
-template <bool ST>
-__device__ __forceinline__ void pass_a32_chunk(const DevParams &P, const DevParams32 &Q, const DevState &S,
+template <bool ST, int L>
+__device__ __forceinline__ void pass_a32_body(const DevParams &P, const DevParams32 &Q, const DevState &S,
                                                Tile32 &tl, int lane, int cidx)
 {
     {
         const Chunk ch = S.chunks[cidx];
-        const int i = ch.i0 + lane;
-        const bool active = lane < ch.cnt;
+        // L lanes per particle: lane = part * G + p holds particle p and tests
+        // candidates [part * G, part * G + G) of every staged batch
+        constexpr int G = kWarp / L;
+        const int part = lane / G;
+        const int i = ch.i0 + (lane % G);
+        const bool active = (lane % G) < ch.cnt;
         const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
         int cix, ciy, ciz;
         chunk_cell(P, key_cell, cix, ciy, ciz);
@@ -153,7 +157,8 @@ __device__ __forceinline__ void pass_a32_chunk(const DevParams &P, const DevPara
                 if (!active) return;
                 unsigned m = 0;
     #pragma unroll
-                for (int s = 0; s < kWarp; ++s) {
+                for (int s0 = 0; s0 < G; ++s0) {
+                    const int s = part * G + s0;
                     const float4 pj = tl.p[s];
                     const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
                     const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
@@ -198,7 +203,18 @@ __device__ __forceinline__ void pass_a32_chunk(const DevParams &P, const DevPara
                     }
                 }
             });
-        if (!active) return;
+        // combine the L partial sums of each particle
+        for (int o = G; o < kWarp; o <<= 1) {
+            vsp += __shfl_xor_sync(kFull, vsp, o);
+            div += __shfl_xor_sync(kFull, div, o);
+            if (ST) {
+                dA += __shfl_xor_sync(kFull, dA, o);
+                g0 += __shfl_xor_sync(kFull, g0, o);
+                g1 += __shfl_xor_sync(kFull, g1, o);
+                g2 += __shfl_xor_sync(kFull, g2, o);
+            }
+        }
+        if (!active || part != 0) return;
         const double volstrain = vsp - Q.N0p32;
         S.vsp32[i] = (float)volstrain;
         S.div32[i] = (float)div;
@@ -218,14 +234,16 @@ __device__ __forceinline__ void pass_a32_chunk(const DevParams &P, const DevPara
 // All fluid forces (the FP32 counterpart of k_pass_b), same two-phase batch
 // scheme.  Chunks hold one particle class, so the fluid/solid split below is
 // uniform across the warp.
-template <bool ST>
-__device__ __forceinline__ void pass_b32_chunk(const DevParams &P, const DevParams32 &Q, const DevState &S,
+template <bool ST, int L>
+__device__ __forceinline__ void pass_b32_body(const DevParams &P, const DevParams32 &Q, const DevState &S,
                                                Tile32 &tl, TileST &ts, int lane, int cidx)
 {
     {
         const Chunk ch = S.chunks[cidx];
-        const int i = ch.i0 + lane;
-        const bool active = lane < ch.cnt;
+        constexpr int G = kWarp / L;  // L lanes per particle, as in pass A
+        const int part = lane / G;
+        const int i = ch.i0 + (lane % G);
+        const bool active = (lane % G) < ch.cnt;
         const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
         int cix, ciy, ciz;
         chunk_cell(P, key_cell, cix, ciy, ciz);
@@ -251,7 +269,7 @@ __device__ __forceinline__ void pass_b32_chunk(const DevParams &P, const DevPara
         double3 fP = make_double3(0.0, 0.0, 0.0), fV = fP;
         float3 fD = make_float3(0.f, 0.f, 0.f), fB = fD, fS = fD;
         float dragc = 0.f;
-        bool have_drag = false;
+        int drag_j = -1;  // candidate that wrote dragc: the last one in the reference's order wins
         traverse_stencil_batched(
             P, S.cell_start, key_cell, lane, 7u,
             [&](int j, int slot) {
@@ -266,7 +284,8 @@ __device__ __forceinline__ void pass_b32_chunk(const DevParams &P, const DevPara
                 if (!active) return;
                 unsigned m = 0;
     #pragma unroll
-                for (int s = 0; s < kWarp; ++s) {
+                for (int s0 = 0; s0 < G; ++s0) {
+                    const int s = part * G + s0;
                     const float4 pj = tl.p[s];
                     const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
                     const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
@@ -322,7 +341,7 @@ __device__ __forceinline__ void pass_b32_chunk(const DevParams &P, const DevPara
                             else
                                 cd = 0.44f;
                             dragc = cd;
-                            have_drag = true;
+                            drag_j = base + s;
                             const float c = cd * rhoi * Q.drag_pref * Vs;
                             fD.x = fmaf(c, u0, fD.x);
                             fD.y = fmaf(c, u1, fD.y);
@@ -364,7 +383,32 @@ __device__ __forceinline__ void pass_b32_chunk(const DevParams &P, const DevPara
                     }
                 }
             });
-        if (!active) return;
+        for (int o = G; o < kWarp; o <<= 1) {
+            fP.x += __shfl_xor_sync(kFull, fP.x, o);
+            fP.y += __shfl_xor_sync(kFull, fP.y, o);
+            fP.z += __shfl_xor_sync(kFull, fP.z, o);
+            fV.x += __shfl_xor_sync(kFull, fV.x, o);
+            fV.y += __shfl_xor_sync(kFull, fV.y, o);
+            fV.z += __shfl_xor_sync(kFull, fV.z, o);
+            fD.x += __shfl_xor_sync(kFull, fD.x, o);
+            fD.y += __shfl_xor_sync(kFull, fD.y, o);
+            fD.z += __shfl_xor_sync(kFull, fD.z, o);
+            fB.x += __shfl_xor_sync(kFull, fB.x, o);
+            fB.y += __shfl_xor_sync(kFull, fB.y, o);
+            fB.z += __shfl_xor_sync(kFull, fB.z, o);
+            if (ST) {
+                fS.x += __shfl_xor_sync(kFull, fS.x, o);
+                fS.y += __shfl_xor_sync(kFull, fS.y, o);
+                fS.z += __shfl_xor_sync(kFull, fS.z, o);
+            }
+            const int oj = __shfl_xor_sync(kFull, drag_j, o);
+            const float oc = __shfl_xor_sync(kFull, dragc, o);
+            if (oj > drag_j) {
+                drag_j = oj;
+                dragc = oc;
+            }
+        }
+        if (!active || part != 0) return;
         const float m = sol ? rhoi * Q.V : Q.mass[ti];
         float4 F;
         if (sol) {
@@ -372,7 +416,7 @@ __device__ __forceinline__ void pass_b32_chunk(const DevParams &P, const DevPara
             F.y = (float)(2.0 * fD.y + fS.y + fV.y - fB.y + (double)m * P.g[1]);
             F.z = (float)(2.0 * fD.z + fS.z + fV.z - fB.z + (double)m * P.g[2]);
             S.alpha32[i] = alpha;
-            if (have_drag) S.dragC32[i] = dragc;
+            if (drag_j >= 0) S.dragC32[i] = dragc;
         } else {
             F.x = (float)(fP.x + fS.x + fV.x + (double)m * P.g[0]);
             F.y = (float)(fP.y + fS.y + fV.y + (double)m * P.g[1]);
@@ -381,6 +425,29 @@ __device__ __forceinline__ void pass_b32_chunk(const DevParams &P, const DevPara
         F.w = 0.f;
         S.f4[i] = F;
     }
+}
+
+// chunk bodies dispatched on the chunk's size: 4 lanes per particle for up to
+// 8 particles, 2 for up to 16, 1 otherwise, so that small chunks (cells at
+// free surfaces, walls and debris) keep the warp busy
+template <bool ST>
+__device__ __forceinline__ void pass_a32_chunk(const DevParams &P, const DevParams32 &Q, const DevState &S,
+                                               Tile32 &tl, int lane, int cidx)
+{
+    const int cnt = S.chunks[cidx].cnt;
+    if (cnt <= 8) pass_a32_body<ST, 4>(P, Q, S, tl, lane, cidx);
+    else if (cnt <= 16) pass_a32_body<ST, 2>(P, Q, S, tl, lane, cidx);
+    else pass_a32_body<ST, 1>(P, Q, S, tl, lane, cidx);
+}
+
+template <bool ST>
+__device__ __forceinline__ void pass_b32_chunk(const DevParams &P, const DevParams32 &Q, const DevState &S,
+                                               Tile32 &tl, TileST &ts, int lane, int cidx)
+{
+    const int cnt = S.chunks[cidx].cnt;
+    if (cnt <= 8) pass_b32_body<ST, 4>(P, Q, S, tl, ts, lane, cidx);
+    else if (cnt <= 16) pass_b32_body<ST, 2>(P, Q, S, tl, ts, lane, cidx);
+    else pass_b32_body<ST, 1>(P, Q, S, tl, ts, lane, cidx);
 }
 
 // ------------------------------------------------- pass kernels (one scene)
