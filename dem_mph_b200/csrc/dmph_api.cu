@@ -98,6 +98,7 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
     if (ctx->fp32)
         launch_wet_partition(P, ctx->words, S.cell_start, S.chunks, ctx->chunks2, ctx->dB, ctx->flag, ctx->offs,
                              ctx->bsums, ctx->total, st);
+    if (ctx->fp32 && ctx->use_list) launch_build_list32(P, ctx->Q, S, ctx->dB, st);
     launch_counts(P, S, ctx->dB, ctx->all_counts ? CR_ALL : CR_SOLID, st);
 }
 
@@ -105,7 +106,7 @@ long long dmph::rebuild_launches(const dmph_ctx *ctx, bool first)
 {
     const DevParams &P = ctx->P;
     return 1 + bitonic_launches(P.P2, P.P2log) + 1 + 1 + (ctx->fp32 && !first ? 1 : 0) + 5 + 1 +
-           (ctx->fp32 ? 6 : 0) + 1 + (ctx->S.bid ? 1 : 0);
+           (ctx->fp32 ? 6 : 0) + 1 + (ctx->S.bid ? 1 : 0) + (ctx->fp32 && ctx->use_list ? 1 : 0);
 }
 
 // phase timing (dmph_set_profiling): events around one phase, synchronised
@@ -145,10 +146,12 @@ void dmph::enqueue_passes(dmph_ctx *ctx, cudaStream_t st)
     if (ctx->fp32) {
         const DevParams32 &Q = ctx->Q;
         phase_begin(ctx);
-        launch_pass_a32(P, Q, S, dB, CR_WET, ctx->var_a, st);
+        if (ctx->use_list) launch_pass_a32_list(P, Q, S, dB, st);
+        launch_pass_a32(P, Q, S, dB, CR_WET, ctx->var_a, st, ctx->use_list ? 1 : 0);
         phase_end(ctx, 2);
         phase_begin(ctx);
-        launch_pass_b32(P, Q, S, dB, ctx->var_b, st);
+        if (ctx->use_list) launch_pass_b32_list(P, Q, S, dB, st);
+        launch_pass_b32(P, Q, S, dB, ctx->var_b, st, ctx->use_list ? 1 : 0);
         launch_fluid_accel32(Q, S, dB, st);
         phase_end(ctx, 3);
     } else {
@@ -160,6 +163,19 @@ void dmph::enqueue_passes(dmph_ctx *ctx, cudaStream_t st)
         launch_fluid_accel(P, S, dB, st);
         phase_end(ctx, 3);
     }
+}
+
+// pass A and pass B of the FP32 build without the fluid update (surrogate
+// evaluations): over the Verlet lists in list mode, with the stencil kernels
+// standing in after a list overflow
+void dmph::enqueue_pair_passes32(dmph_ctx *ctx, cudaStream_t st)
+{
+    const DevParams &P = ctx->P;
+    const DevParams32 &Q = ctx->Q;
+    if (ctx->use_list) launch_pass_a32_list(P, Q, ctx->S, ctx->dB, st);
+    launch_pass_a32(P, Q, ctx->S, ctx->dB, CR_WET, ctx->var_a, st, ctx->use_list ? 1 : 0);
+    if (ctx->use_list) launch_pass_b32_list(P, Q, ctx->S, ctx->dB, st);
+    launch_pass_b32(P, Q, ctx->S, ctx->dB, ctx->var_b, st, ctx->use_list ? 1 : 0);
 }
 
 // the DEM substeps or rigid bodies (second part of a step's tail)
@@ -213,7 +229,7 @@ long long dmph::dem_launches(const dmph_ctx *ctx)
 
 long long dmph::tail_launches(const dmph_ctx *ctx)
 {
-    return 3 + dem_launches(ctx);
+    return 3 + dem_launches(ctx) + (ctx->fp32 && ctx->use_list ? 2 : 0);
 }
 
 void dmph::advance_host_clock(dmph_ctx *ctx)
@@ -454,6 +470,12 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         AL(S.pA32, N);
         AL(S.alpha32, N);
         AL(S.dragC32, N);
+        // Verlet lists: the lattice holds 122 (3D) / 28 (2D) particles within
+        // MaxRadius + MARGIN = 3.1 dx; the capacity leaves room for compression
+        S.nbl_cap = P.dim == 2 ? 64 : 192;
+        AL(S.nbl, (size_t)S.nbl_cap * N);
+        AL(S.nbn, N);
+        ctx->use_list = true;
     }
     AL(ctx->flag, N);
     AL(ctx->offs, N);
@@ -926,6 +948,27 @@ extern "C" int dmph_get_bodies(dmph_ctx *ctx, double *X, double *V, double *q, d
     return DMPH_OK;
 }
 
+extern "C" int dmph_set_pair_mode(dmph_ctx *ctx, int mode)
+{
+    if (!ctx) return DMPH_EINVAL;
+    if (mode != DMPH_PAIRS_STENCIL && mode != DMPH_PAIRS_VERLET_LIST) return DMPH_EINVAL;
+    if (!ctx->fp32) {
+        if (mode == DMPH_PAIRS_STENCIL) return DMPH_OK;
+        ctx->err = "Verlet lists belong to the FP32 split build";
+        return DMPH_EINVAL;
+    }
+    const bool want = mode == DMPH_PAIRS_VERLET_LIST;
+    if (want && !ctx->use_list) {
+        // lists of the current cell sort
+        launch_build_list32(ctx->P, ctx->Q, ctx->S, ctx->dB, ctx->st);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    ctx->use_list = want;
+    drop_graph(ctx);
+    return DMPH_OK;
+}
+
 extern "C" int dmph_set_graph(dmph_ctx *ctx, int enable)
 {
     if (!ctx) return DMPH_EINVAL;
@@ -1132,7 +1175,11 @@ extern "C" int dmph_ensemble_create(dmph_ctx *const *scenes, int nscenes, dmph_e
         delete e;
         return DMPH_ECUDA;
     }
-    for (dmph_ctx *c : e->scenes) drop_graph(c);
+    for (dmph_ctx *c : e->scenes) {
+        // the ensemble kernels walk the stencil; its members build no lists
+        c->use_list = false;
+        drop_graph(c);
+    }
     *out = e;
     return DMPH_OK;
 }

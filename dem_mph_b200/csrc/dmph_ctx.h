@@ -44,6 +44,7 @@ struct dmph_ctx {
     cudaGraphExec_t gexec = nullptr;
     long long graph_steps = 0, host_rebuilds = 0;
     int var_a = 0, var_b = 0;  // launch variants of the FP32 pair passes (dmph_autotune)
+    bool use_list = false;     // FP32 pair passes over Verlet lists built at each rebuild
     Chunk *chunks2 = nullptr;  // partition scratch
     int demSteps = 0;
     double time = 0.0;
@@ -76,6 +77,7 @@ void enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st);
 long long rebuild_launches(const dmph_ctx *ctx, bool first);
 void enqueue_head(dmph_ctx *ctx, unsigned long long graph_cond, cudaStream_t st);
 void enqueue_passes(dmph_ctx *ctx, cudaStream_t st);
+void enqueue_pair_passes32(dmph_ctx *ctx, cudaStream_t st);
 void enqueue_dem(dmph_ctx *ctx, cudaStream_t st);
 long long dem_launches(const dmph_ctx *ctx);
 long long tail_launches(const dmph_ctx *ctx);

@@ -88,6 +88,7 @@ enum DevBound {
     B_SE = 6,
     B_NEED = 7,     // rebuild decided for this step
     B_REBUILDS = 8, // rebuilds since creation
+    B_LIST_OVF = 9, // a Verlet list of the last rebuild overflowed (FP32 list mode): stencil passes run
     B_COUNT = 16
 };
 

@@ -119,6 +119,75 @@ __global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm,
     }
 }
 
+// ---------------------------------------------------- pass A pair math
+// Shared by the stencil kernels and the Verlet-list kernels, so both paths
+// evaluate identical arithmetic.
+struct IA {  // particle i of pass A
+    float4 pi, vi;
+    int ti;
+    bool si, wi;
+};
+// VolStrainP = sum(w) - N0p cancels to ~1e-3 of the sum, so the sums are
+// carried in FP64 (one add per pair); the pair terms stay FP32
+struct AccA {
+    double vsp, div;
+    float dA, g0, g1, g2;
+};
+
+// one pair (pj in the frame of i's cell, .w = type bits), within the cut-off
+template <bool ST>
+__device__ __forceinline__ void pair_a32(const DevParams32 &Q, const IA &I, const float4 pj, const float4 vj, AccA &A)
+{
+    const float q0 = pj.x - I.pi.x, q1 = pj.y - I.pi.y, q2 = pj.z - I.pi.z;
+    const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
+    const int tj = __float_as_int(pj.w);
+    // correctly rounded sqrt: the approximate reciprocal square root has a
+    // bias that would add up over ~100 neighbours
+    const float r = sqrtf(r2);
+    const float ir = __frcp_rn(r);
+    if (!ST || r2 <= Q.RP2) {
+        const float a = fmaf(-r, Q.iRP, 1.f);  // 1 - r/h
+        A.vsp += (double)(Q.Bp * a * a);
+        const bool sj = is_solid(tj);
+        if (!((I.si && is_wall(tj)) || (sj && I.wi) || (sj && I.si))) {
+            const float uq = fmaf(vj.x - I.vi.x, q0, fmaf(vj.y - I.vi.y, q1, (vj.z - I.vi.z) * q2));
+            A.div -= (double)(uq * ir * Q.dwp * a);  // -(u.e) dw
+        }
+    }
+    if (ST && !(I.si && is_wall(tj))) {
+        const float ratio = Q.ratio[I.ti][tj];
+        if (r2 <= Q.RA2) {
+            const float x = r * Q.iRA;
+            A.dA = fmaf(ratio * Q.Ba * x * (1.f - x), (1.f - x), A.dA);
+        }
+        if (r2 <= Q.RG2) {
+            const float a = fmaf(-r, Q.iRG, 1.f);
+            const float w = ratio * Q.Bg * a * a * Q.R2g_inv_RG;
+            A.g0 = fmaf(q0, w, A.g0);
+            A.g1 = fmaf(q1, w, A.g1);
+            A.g2 = fmaf(q2, w, A.g2);
+        }
+    }
+}
+
+template <bool ST>
+__device__ __forceinline__ void finish_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, int i,
+                                           const IA &I, const AccA &A)
+{
+    const double volstrain = A.vsp - Q.N0p32;
+    S.vsp32[i] = (float)volstrain;
+    S.div32[i] = (float)A.div;
+    const double kappa = volstrain < 0.0 ? 0.0 : P.bulk[I.ti];
+    if (!I.si) S.pres32[i] = (float)(-P.bvisc[I.ti] * A.div + kappa * volstrain);
+    if (ST) {
+        S.densA32[i] = A.dA;
+        float pa = Q.CofA[I.ti] * (A.dA - Q.N0a) / Q.dx;
+        if (Q.N0a <= A.dA) pa = 0.f;
+        S.pA32[i] = pa;
+        S.gc4[i] = make_float4(A.g0, A.g1, A.g2, 0.f);
+    }
+}
+
 // ---------------------------------------------------------------- pass A
 // Densities, divergence and pressures (the FP32 counterpart of k_pass_a in
 // dmph_f64.cu).  Each staged batch of 32 candidates is first reduced to a
@@ -144,12 +213,9 @@ __device__ __forceinline__ void pass_a32_body(const DevParams &P, const DevParam
         const float4 pi = S.p4[ii];
         const float4 vi = S.v4[ii];
         const int ti = unpack_type(__float_as_uint(pi.w));
-        const bool si = is_solid(ti), wi = is_wall(ti);
+        const IA I{pi, vi, ti, is_solid(ti), is_wall(ti)};
         const float cut2 = ST ? fmaxf(Q.RP2, fmaxf(Q.RA2, Q.RG2)) : Q.RP2;
-        // VolStrainP = sum(w) - N0p cancels to ~1e-3 of the sum, so the sums are
-        // carried in FP64 (one add per pair); the pair terms stay FP32
-        double vsp = 0.0, div = 0.0;
-        float dA = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
+        AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
         traverse_stencil_batched(
             P, S.cell_start, key_cell, lane, 7u,
             [&](int j, int slot) { stage32(P, Q, S, tl, j, slot, cix, ciy, ciz, false); },
@@ -169,65 +235,187 @@ __device__ __forceinline__ void pass_a32_body(const DevParams &P, const DevParam
                 while (m) {
                     const int s = __ffs(m) - 1;
                     m &= m - 1;
-                    const float4 pj = tl.p[s];
-                    const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-                    const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
-                    const int tj = __float_as_int(pj.w);
-                    // correctly rounded sqrt: the approximate reciprocal square
-                    // root has a bias that would add up over ~100 neighbours
-                    const float r = sqrtf(r2);
-                    const float ir = __frcp_rn(r);
-                    if (!ST || r2 <= Q.RP2) {
-                        const float a = fmaf(-r, Q.iRP, 1.f);  // 1 - r/h
-                        vsp += (double)(Q.Bp * a * a);
-                        const bool sj = is_solid(tj);
-                        if (!((si && is_wall(tj)) || (sj && wi) || (sj && si))) {
-                            const float4 vj = tl.v[s];
-                            const float uq = fmaf(vj.x - vi.x, q0, fmaf(vj.y - vi.y, q1, (vj.z - vi.z) * q2));
-                            div -= (double)(uq * ir * Q.dwp * a);  // -(u.e) dw
-                        }
-                    }
-                    if (ST && !(si && is_wall(tj))) {
-                        const float ratio = Q.ratio[ti][tj];
-                        if (r2 <= Q.RA2) {
-                            const float x = r * Q.iRA;
-                            dA = fmaf(ratio * Q.Ba * x * (1.f - x), (1.f - x), dA);
-                        }
-                        if (r2 <= Q.RG2) {
-                            const float a = fmaf(-r, Q.iRG, 1.f);
-                            const float w = ratio * Q.Bg * a * a * Q.R2g_inv_RG;
-                            g0 = fmaf(q0, w, g0);
-                            g1 = fmaf(q1, w, g1);
-                            g2 = fmaf(q2, w, g2);
-                        }
-                    }
+                    pair_a32<ST>(Q, I, tl.p[s], tl.v[s], A);
                 }
             });
         // combine the L partial sums of each particle
         for (int o = G; o < kWarp; o <<= 1) {
-            vsp += __shfl_xor_sync(kFull, vsp, o);
-            div += __shfl_xor_sync(kFull, div, o);
+            A.vsp += __shfl_xor_sync(kFull, A.vsp, o);
+            A.div += __shfl_xor_sync(kFull, A.div, o);
             if (ST) {
-                dA += __shfl_xor_sync(kFull, dA, o);
-                g0 += __shfl_xor_sync(kFull, g0, o);
-                g1 += __shfl_xor_sync(kFull, g1, o);
-                g2 += __shfl_xor_sync(kFull, g2, o);
+                A.dA += __shfl_xor_sync(kFull, A.dA, o);
+                A.g0 += __shfl_xor_sync(kFull, A.g0, o);
+                A.g1 += __shfl_xor_sync(kFull, A.g1, o);
+                A.g2 += __shfl_xor_sync(kFull, A.g2, o);
             }
         }
         if (!active || part != 0) return;
-        const double volstrain = vsp - Q.N0p32;
-        S.vsp32[i] = (float)volstrain;
-        S.div32[i] = (float)div;
-        const double kappa = volstrain < 0.0 ? 0.0 : P.bulk[ti];
-        if (!si) S.pres32[i] = (float)(-P.bvisc[ti] * div + kappa * volstrain);
-        if (ST) {
-            S.densA32[i] = dA;
-            float pa = Q.CofA[ti] * (dA - Q.N0a) / Q.dx;
-            if (Q.N0a <= dA) pa = 0.f;
-            S.pA32[i] = pa;
-            S.gc4[i] = make_float4(g0, g1, g2, 0.f);
+        finish_a32<ST>(P, Q, S, i, I, A);
+    }
+}
+
+// ---------------------------------------------------- pass B pair math
+struct IB {  // particle i of pass B
+    float4 pi, vi, gi;  // gi: gravity centre, .w = attractive pressure (surface tension)
+    int ti;
+    bool sol;
+    float Pi, rhoi, alpha;
+};
+// the pressure and viscous pair terms nearly cancel: their sums are FP64
+struct AccB {
+    double3 fP, fV;
+    float3 fD, fB, fS;
+    float dragc;
+    int drag_j;  // candidate that wrote dragc: the last one in the reference's order wins
+};
+
+__device__ __forceinline__ AccB acc_b_zero()
+{
+    AccB B;
+    B.fP = make_double3(0.0, 0.0, 0.0);
+    B.fV = B.fP;
+    B.fD = make_float3(0.f, 0.f, 0.f);
+    B.fB = B.fD;
+    B.fS = B.fD;
+    B.dragc = 0.f;
+    B.drag_j = -1;
+    return B;
+}
+
+template <bool ST>
+__device__ __forceinline__ IB make_ib(const DevParams &P, const DevState &S, int ii, float4 pi, float4 vi, int ti)
+{
+    IB I;
+    I.pi = pi;
+    I.vi = vi;
+    I.ti = ti;
+    I.sol = is_solid(ti);
+    I.Pi = S.pres32[ii];
+    I.rhoi = (float)particle_density(S, P, ii, ti);
+    I.gi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ST) {
+        I.gi = S.gc4[ii];
+        I.gi.w = S.pA32[ii];
+    }
+    I.alpha = 0.f;
+    if (I.sol) {
+        const int nci = S.nc[ii];
+        I.alpha = nci > 0 ? (float)S.snc[ii] / (float)nci : 0.f;
+    }
+    return I;
+}
+
+// one pair (pj in the frame of i's cell, .w = type bits; vj.w = pressure of
+// j; gj = gravity centre of j, .w its attractive pressure), j its slot
+template <bool ST>
+__device__ __forceinline__ void pair_b32(const DevParams32 &Q, const IB &I, const float4 pj, const float4 vj,
+                                         const float4 gj, int j, AccB &B)
+{
+    const float q0 = pj.x - I.pi.x, q1 = pj.y - I.pi.y, q2 = pj.z - I.pi.z;
+    const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
+    const int tj = __float_as_int(pj.w);
+    const int ti = I.ti;
+    const float u0 = vj.x - I.vi.x, u1 = vj.y - I.vi.y, u2 = vj.z - I.vi.z;
+    const float ir = rsqrtf(r2);
+    const float r = r2 * ir;
+    if (!I.sol) {
+        if (r2 < Q.RP2) {
+            const float a = fmaf(-r, Q.iRP, 1.f);
+            const float c = (I.Pi + vj.w) * Q.dwpV * a * ir;  // (Pi+Pj) dw/r V
+            B.fP.x += (double)(c * q0);
+            B.fP.y += (double)(c * q1);
+            B.fP.z += (double)(c * q2);
+        }
+        if (r2 < Q.RV2) {
+            const float a = fmaf(-r, Q.iRV, 1.f);
+            const float uq = fmaf(u0, q0, fmaf(u1, q1, u2 * q2));
+            // C mu (u.e) e (-dw)/r V with e = q/r
+            const float c = Q.muij[ti][tj] * uq * a * (ir * ir * ir);
+            B.fV.x += (double)(c * q0);
+            B.fV.y += (double)(c * q1);
+            B.fV.z += (double)(c * q2);
+        }
+    } else {
+        if (!is_wall(tj) && r2 < Q.RV2) {
+            const float a = fmaf(-r, Q.iRV, 1.f);
+            const float uq = fmaf(u0, q0, fmaf(u1, q1, u2 * q2));
+            const float c = Q.muij[ti][tj] * uq * a * (ir * ir * ir);
+            B.fV.x += (double)(c * q0);
+            B.fV.y += (double)(c * q1);
+            B.fV.z += (double)(c * q2);
+        }
+        if (r2 < Q.RP2 && is_fluid(tj)) {
+            const float alpha = I.alpha, rhoi = I.rhoi;
+            const float Vs = sqrtf(fmaf(u0, u0, fmaf(u1, u1, u2 * u2)));
+            const float Re = alpha * rhoi * Vs * Q.dx / Q.svisc[tj];
+            float cd;
+            if (alpha < 0.8f)
+                cd = (4.f / 3.f) * (150.f * (1.f - alpha) / (alpha * Re) + 1.75f);
+            else if (Re <= 1000.f)
+                cd = 24.f * (1.f + 0.15f * powf(Re, 0.687f)) / (alpha * Re) * powf(alpha, -2.65f);
+            else
+                cd = 0.44f;
+            B.dragc = cd;
+            B.drag_j = j;
+            const float c = cd * rhoi * Q.drag_pref * Vs;
+            B.fD.x = fmaf(c, u0, B.fD.x);
+            B.fD.y = fmaf(c, u1, B.fD.y);
+            B.fD.z = fmaf(c, u2, B.fD.z);
+            const float a = fmaf(-r, Q.iRP, 1.f);
+            const float wb = Q.density[tj] * Q.V * Q.Bp * a * a;
+            B.fB.x = fmaf(wb, Q.g[0], B.fB.x);
+            B.fB.y = fmaf(wb, Q.g[1], B.fB.y);
+            B.fB.z = fmaf(wb, Q.g[2], B.fB.z);
         }
     }
+    if (ST && !((I.sol && is_wall(tj)) || (is_solid(tj) && is_wall(ti)))) {
+        const float4 gi = I.gi;
+        const float rij_ = Q.ratio[ti][tj], rji_ = Q.ratio[tj][ti];
+        if (r2 < Q.RA2) {
+            const float x = r * Q.iRA;
+            const float dwa = Q.Ba * (1.f - x) * (1.f - 3.f * x) * Q.iRA;
+            const float c = (gi.w * rij_ + gj.w * rji_) * dwa * ir * Q.V;
+            B.fS.x = fmaf(c, q0, B.fS.x);
+            B.fS.y = fmaf(c, q1, B.fS.y);
+            B.fS.z = fmaf(c, q2, B.fS.z);
+        }
+        if (r2 < Q.RG2) {
+            const float a = fmaf(-r, Q.iRG, 1.f);
+            const float w2 = Q.Bg * a * a, dw2 = Q.dwg * a;
+            const float ai = Q.ai[ti];
+            const float k = Q.R2g_inv_RG * Q.Vdx;
+            B.fS.x -= (ai * gj.x * rji_ * w2 - ai * gi.x * rij_ * w2) * k;
+            B.fS.y -= (ai * gj.y * rji_ * w2 - ai * gi.y * rij_ * w2) * k;
+            B.fS.z -= (ai * gj.z * rji_ * w2 - ai * gi.z * rij_ * w2) * k;
+            const float gr = (ai * gj.x * rji_ * dw2 - ai * gi.x * rij_ * dw2) * q0 +
+                             (ai * gj.y * rji_ * dw2 - ai * gi.y * rij_ * dw2) * q1 +
+                             (ai * gj.z * rji_ * dw2 - ai * gi.z * rij_ * dw2) * q2;
+            const float c = gr * ir * k;
+            B.fS.x -= c * q0;
+            B.fS.y -= c * q1;
+            B.fS.z -= c * q2;
+        }
+    }
+}
+
+__device__ __forceinline__ void finish_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, int i,
+                                           const IB &I, const AccB &B)
+{
+    const float m = I.sol ? I.rhoi * Q.V : Q.mass[I.ti];
+    float4 F;
+    if (I.sol) {
+        F.x = (float)(2.0 * B.fD.x + B.fS.x + B.fV.x - B.fB.x + (double)m * P.g[0]);
+        F.y = (float)(2.0 * B.fD.y + B.fS.y + B.fV.y - B.fB.y + (double)m * P.g[1]);
+        F.z = (float)(2.0 * B.fD.z + B.fS.z + B.fV.z - B.fB.z + (double)m * P.g[2]);
+        S.alpha32[i] = I.alpha;
+        if (B.drag_j >= 0) S.dragC32[i] = B.dragc;
+    } else {
+        F.x = (float)(B.fP.x + B.fS.x + B.fV.x + (double)m * P.g[0]);
+        F.y = (float)(B.fP.y + B.fS.y + B.fV.y + (double)m * P.g[1]);
+        F.z = (float)(B.fP.z + B.fS.z + B.fV.z + (double)m * P.g[2]);
+    }
+    F.w = 0.f;
+    S.f4[i] = F;
 }
 
 // ---------------------------------------------------------------- pass B
@@ -251,25 +439,9 @@ __device__ __forceinline__ void pass_b32_body(const DevParams &P, const DevParam
         const float4 pi = S.p4[ii];
         const float4 vi = S.v4[ii];
         const int ti = unpack_type(__float_as_uint(pi.w));
-        const bool sol = is_solid(ti);
-        const float Pi = S.pres32[ii];
-        const float rhoi = (float)particle_density(S, P, ii, ti);
-        float4 gi = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (ST) {
-            gi = S.gc4[ii];
-            gi.w = S.pA32[ii];
-        }
-        float alpha = 0.f;
-        if (sol) {
-            const int nci = S.nc[ii];
-            alpha = nci > 0 ? (float)S.snc[ii] / (float)nci : 0.f;
-        }
+        const IB I = make_ib<ST>(P, S, ii, pi, vi, ti);
         const float cut2 = ST ? fmaxf(fmaxf(Q.RP2, Q.RV2), fmaxf(Q.RA2, Q.RG2)) : fmaxf(Q.RP2, Q.RV2);
-        // the pressure and viscous pair terms nearly cancel: their sums are FP64
-        double3 fP = make_double3(0.0, 0.0, 0.0), fV = fP;
-        float3 fD = make_float3(0.f, 0.f, 0.f), fB = fD, fS = fD;
-        float dragc = 0.f;
-        int drag_j = -1;  // candidate that wrote dragc: the last one in the reference's order wins
+        AccB B = acc_b_zero();
         traverse_stencil_batched(
             P, S.cell_start, key_cell, lane, 7u,
             [&](int j, int slot) {
@@ -296,134 +468,164 @@ __device__ __forceinline__ void pass_b32_body(const DevParams &P, const DevParam
                 while (m) {
                     const int s = __ffs(m) - 1;
                     m &= m - 1;
-                    const float4 pj = tl.p[s];
-                    const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-                    const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
-                    const int tj = __float_as_int(pj.w);
-                    const float4 vj = tl.v[s];
-                    const float u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
-                    const float ir = rsqrtf(r2);
-                    const float r = r2 * ir;
-                    if (!sol) {
-                        if (r2 < Q.RP2) {
-                            const float a = fmaf(-r, Q.iRP, 1.f);
-                            const float c = (Pi + vj.w) * Q.dwpV * a * ir;  // (Pi+Pj) dw/r V
-                            fP.x += (double)(c * q0);
-                            fP.y += (double)(c * q1);
-                            fP.z += (double)(c * q2);
-                        }
-                        if (r2 < Q.RV2) {
-                            const float a = fmaf(-r, Q.iRV, 1.f);
-                            const float uq = fmaf(u0, q0, fmaf(u1, q1, u2 * q2));
-                            // C mu (u.e) e (-dw)/r V with e = q/r
-                            const float c = Q.muij[ti][tj] * uq * a * (ir * ir * ir);
-                            fV.x += (double)(c * q0);
-                            fV.y += (double)(c * q1);
-                            fV.z += (double)(c * q2);
-                        }
-                    } else {
-                        if (!is_wall(tj) && r2 < Q.RV2) {
-                            const float a = fmaf(-r, Q.iRV, 1.f);
-                            const float uq = fmaf(u0, q0, fmaf(u1, q1, u2 * q2));
-                            const float c = Q.muij[ti][tj] * uq * a * (ir * ir * ir);
-                            fV.x += (double)(c * q0);
-                            fV.y += (double)(c * q1);
-                            fV.z += (double)(c * q2);
-                        }
-                        if (r2 < Q.RP2 && is_fluid(tj)) {
-                            const float Vs = sqrtf(fmaf(u0, u0, fmaf(u1, u1, u2 * u2)));
-                            const float Re = alpha * rhoi * Vs * Q.dx / Q.svisc[tj];
-                            float cd;
-                            if (alpha < 0.8f)
-                                cd = (4.f / 3.f) * (150.f * (1.f - alpha) / (alpha * Re) + 1.75f);
-                            else if (Re <= 1000.f)
-                                cd = 24.f * (1.f + 0.15f * powf(Re, 0.687f)) / (alpha * Re) * powf(alpha, -2.65f);
-                            else
-                                cd = 0.44f;
-                            dragc = cd;
-                            drag_j = base + s;
-                            const float c = cd * rhoi * Q.drag_pref * Vs;
-                            fD.x = fmaf(c, u0, fD.x);
-                            fD.y = fmaf(c, u1, fD.y);
-                            fD.z = fmaf(c, u2, fD.z);
-                            const float a = fmaf(-r, Q.iRP, 1.f);
-                            const float wb = Q.density[tj] * Q.V * Q.Bp * a * a;
-                            fB.x = fmaf(wb, Q.g[0], fB.x);
-                            fB.y = fmaf(wb, Q.g[1], fB.y);
-                            fB.z = fmaf(wb, Q.g[2], fB.z);
-                        }
-                    }
-                    if (ST && !((sol && is_wall(tj)) || (is_solid(tj) && is_wall(ti)))) {
-                        const float rij_ = Q.ratio[ti][tj], rji_ = Q.ratio[tj][ti];
-                        const float4 gj = ts.g[s];
-                        if (r2 < Q.RA2) {
-                            const float x = r * Q.iRA;
-                            const float dwa = Q.Ba * (1.f - x) * (1.f - 3.f * x) * Q.iRA;
-                            const float c = (gi.w * rij_ + gj.w * rji_) * dwa * ir * Q.V;
-                            fS.x = fmaf(c, q0, fS.x);
-                            fS.y = fmaf(c, q1, fS.y);
-                            fS.z = fmaf(c, q2, fS.z);
-                        }
-                        if (r2 < Q.RG2) {
-                            const float a = fmaf(-r, Q.iRG, 1.f);
-                            const float w2 = Q.Bg * a * a, dw2 = Q.dwg * a;
-                            const float ai = Q.ai[ti];
-                            const float k = Q.R2g_inv_RG * Q.Vdx;
-                            fS.x -= (ai * gj.x * rji_ * w2 - ai * gi.x * rij_ * w2) * k;
-                            fS.y -= (ai * gj.y * rji_ * w2 - ai * gi.y * rij_ * w2) * k;
-                            fS.z -= (ai * gj.z * rji_ * w2 - ai * gi.z * rij_ * w2) * k;
-                            const float gr = (ai * gj.x * rji_ * dw2 - ai * gi.x * rij_ * dw2) * q0 +
-                                             (ai * gj.y * rji_ * dw2 - ai * gi.y * rij_ * dw2) * q1 +
-                                             (ai * gj.z * rji_ * dw2 - ai * gi.z * rij_ * dw2) * q2;
-                            const float c = gr * ir * k;
-                            fS.x -= c * q0;
-                            fS.y -= c * q1;
-                            fS.z -= c * q2;
-                        }
-                    }
+                    pair_b32<ST>(Q, I, tl.p[s], tl.v[s], ST ? ts.g[s] : make_float4(0.f, 0.f, 0.f, 0.f), base + s, B);
                 }
             });
         for (int o = G; o < kWarp; o <<= 1) {
-            fP.x += __shfl_xor_sync(kFull, fP.x, o);
-            fP.y += __shfl_xor_sync(kFull, fP.y, o);
-            fP.z += __shfl_xor_sync(kFull, fP.z, o);
-            fV.x += __shfl_xor_sync(kFull, fV.x, o);
-            fV.y += __shfl_xor_sync(kFull, fV.y, o);
-            fV.z += __shfl_xor_sync(kFull, fV.z, o);
-            fD.x += __shfl_xor_sync(kFull, fD.x, o);
-            fD.y += __shfl_xor_sync(kFull, fD.y, o);
-            fD.z += __shfl_xor_sync(kFull, fD.z, o);
-            fB.x += __shfl_xor_sync(kFull, fB.x, o);
-            fB.y += __shfl_xor_sync(kFull, fB.y, o);
-            fB.z += __shfl_xor_sync(kFull, fB.z, o);
+            B.fP.x += __shfl_xor_sync(kFull, B.fP.x, o);
+            B.fP.y += __shfl_xor_sync(kFull, B.fP.y, o);
+            B.fP.z += __shfl_xor_sync(kFull, B.fP.z, o);
+            B.fV.x += __shfl_xor_sync(kFull, B.fV.x, o);
+            B.fV.y += __shfl_xor_sync(kFull, B.fV.y, o);
+            B.fV.z += __shfl_xor_sync(kFull, B.fV.z, o);
+            B.fD.x += __shfl_xor_sync(kFull, B.fD.x, o);
+            B.fD.y += __shfl_xor_sync(kFull, B.fD.y, o);
+            B.fD.z += __shfl_xor_sync(kFull, B.fD.z, o);
+            B.fB.x += __shfl_xor_sync(kFull, B.fB.x, o);
+            B.fB.y += __shfl_xor_sync(kFull, B.fB.y, o);
+            B.fB.z += __shfl_xor_sync(kFull, B.fB.z, o);
             if (ST) {
-                fS.x += __shfl_xor_sync(kFull, fS.x, o);
-                fS.y += __shfl_xor_sync(kFull, fS.y, o);
-                fS.z += __shfl_xor_sync(kFull, fS.z, o);
+                B.fS.x += __shfl_xor_sync(kFull, B.fS.x, o);
+                B.fS.y += __shfl_xor_sync(kFull, B.fS.y, o);
+                B.fS.z += __shfl_xor_sync(kFull, B.fS.z, o);
             }
-            const int oj = __shfl_xor_sync(kFull, drag_j, o);
-            const float oc = __shfl_xor_sync(kFull, dragc, o);
-            if (oj > drag_j) {
-                drag_j = oj;
-                dragc = oc;
+            const int oj = __shfl_xor_sync(kFull, B.drag_j, o);
+            const float oc = __shfl_xor_sync(kFull, B.dragc, o);
+            if (oj > B.drag_j) {
+                B.drag_j = oj;
+                B.dragc = oc;
             }
         }
         if (!active || part != 0) return;
-        const float m = sol ? rhoi * Q.V : Q.mass[ti];
-        float4 F;
-        if (sol) {
-            F.x = (float)(2.0 * fD.x + fS.x + fV.x - fB.x + (double)m * P.g[0]);
-            F.y = (float)(2.0 * fD.y + fS.y + fV.y - fB.y + (double)m * P.g[1]);
-            F.z = (float)(2.0 * fD.z + fS.z + fV.z - fB.z + (double)m * P.g[2]);
-            S.alpha32[i] = alpha;
-            if (drag_j >= 0) S.dragC32[i] = dragc;
-        } else {
-            F.x = (float)(fP.x + fS.x + fV.x + (double)m * P.g[0]);
-            F.y = (float)(fP.y + fS.y + fV.y + (double)m * P.g[1]);
-            F.z = (float)(fP.z + fS.z + fV.z + (double)m * P.g[2]);
+        finish_b32(P, Q, S, i, I, B);
+    }
+}
+
+// ------------------------------------------------------- Verlet lists
+// List mode of the FP32 build: at every rebuild each particle of pass A's
+// range (fluid, debris, walls with fluid in reach) records the particles
+// within the reference's list radius MaxRadius + MARGIN at the rebuild-time
+// positions (calculateNeighbor, source/DEM-MPH.cpp:1521-1851, uses the same
+// radius), in ascending slot order; the rebuild trigger bounds every later
+// displacement by MARGIN/2, so every pair a kernel accepts until the next
+// rebuild is in the list.  The passes then run one thread per particle over
+// its list instead of over the ~800 candidates of the 27-cell stencil.
+struct TileL {
+    float4 p[kWarp];     // position in the frame of the warp's cell
+    unsigned e[kWarp];   // j | cell-offset code << 24
+};
+
+__global__ void __launch_bounds__(8 * kWarp) k_build_list32(DevParams P, DevParams32 Q, DevState S, int *dB, float rc2)
+{
+    __shared__ TileL tiles[8];
+    TileL &tl = tiles[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int cap = S.nbl_cap;
+    const long long ld = P.N;
+    FOR_EACH_CHUNK(dB, CR_WET, 8, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        int cix, ciy, ciz;
+        chunk_cell(P, key_cell, cix, ciy, ciz);
+        const float4 pi = S.p4[active ? i : ch.i0];
+        int cnt = 0;
+        traverse_stencil_batched(
+            P, S.cell_start, key_cell, lane, 7u,
+            [&](int j, int slot) {
+                const float4 pj = S.p4[j];
+                const unsigned w = __float_as_uint(pj.w);
+                const int dx = min_image_cell(unpack_cx(w) - cix, P.cc[0]);
+                const int dy = min_image_cell(unpack_cy(w) - ciy, P.cc[1]);
+                const int dz = min_image_cell(unpack_cz(w) - ciz, P.cc[2]);
+                tl.p[slot] = make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
+                                         fmaf((float)dz, Q.cw[2], pj.z), 0.f);
+                tl.e[slot] = (unsigned)j | ((unsigned)((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)) << 24);
+            },
+            [&](int base, int nb) {
+                if (!active) return;
+                for (int s = 0; s < nb; ++s) {
+                    if (base + s == i) continue;
+                    const float4 pj = tl.p[s];
+                    const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+                    if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= rc2) {
+                        if (cnt < cap) S.nbl[(long long)cnt * ld + i] = tl.e[s];
+                        ++cnt;
+                    }
+                }
+            });
+        if (!active) continue;
+        if (cnt > cap) atomicExch(dB + B_LIST_OVF, 1);
+        S.nbn[i] = cnt < cap ? cnt : cap;
+    }
+}
+
+// j's position in the frame of i's cell, type bits in .w
+__device__ __forceinline__ float4 list_pos(const DevParams32 &Q, const DevState &S, unsigned e, int &j)
+{
+    j = (int)(e & 0xFFFFFFu);
+    const int code = (int)(e >> 24);
+    const int dx = code / 9 - 1, dy = (code / 3) % 3 - 1, dz = code % 3 - 1;
+    const float4 pj = S.p4[j];
+    return make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
+                       fmaf((float)dz, Q.cw[2], pj.z), __int_as_float(unpack_type(__float_as_uint(pj.w))));
+}
+
+template <bool ST>
+__global__ void __launch_bounds__(256) k_pass_a32_list(DevParams P, DevParams32 Q, DevState S, const int *dB)
+{
+    if (dB[B_LIST_OVF]) return;
+    const long long ld = P.N;
+    const float cut2 = ST ? fmaxf(Q.RP2, fmaxf(Q.RA2, Q.RG2)) : Q.RP2;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.N; i += gridDim.x * blockDim.x) {
+        const int cnt = S.nbn[i];
+        if (cnt < 0) continue;
+        const float4 pi = S.p4[i];
+        const int ti = unpack_type(__float_as_uint(pi.w));
+        const IA I{pi, S.v4[i], ti, is_solid(ti), is_wall(ti)};
+        AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
+        for (int k = 0; k < cnt; ++k) {
+            int j;
+            const float4 pj = list_pos(Q, S, __ldg(S.nbl + (long long)k * ld + i), j);
+            const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+            if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= cut2) pair_a32<ST>(Q, I, pj, S.v4[j], A);
         }
-        F.w = 0.f;
-        S.f4[i] = F;
+        finish_a32<ST>(P, Q, S, i, I, A);
+    }
+}
+
+template <bool ST>
+__global__ void __launch_bounds__(256) k_pass_b32_list(DevParams P, DevParams32 Q, DevState S, const int *dB)
+{
+    if (dB[B_LIST_OVF]) return;
+    const long long ld = P.N;
+    const float cut2 = ST ? fmaxf(fmaxf(Q.RP2, Q.RV2), fmaxf(Q.RA2, Q.RG2)) : fmaxf(Q.RP2, Q.RV2);
+    const int end = dB[B_SE];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+        const int cnt = S.nbn[i];
+        if (cnt < 0) continue;
+        const float4 pi = S.p4[i];
+        const int ti = unpack_type(__float_as_uint(pi.w));
+        const IB I = make_ib<ST>(P, S, i, pi, S.v4[i], ti);
+        AccB B = acc_b_zero();
+        for (int k = 0; k < cnt; ++k) {
+            int j;
+            const float4 pj = list_pos(Q, S, __ldg(S.nbl + (long long)k * ld + i), j);
+            const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+            if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) < cut2) {
+                float4 vj = S.v4[j];
+                vj.w = S.pres32[j];
+                float4 gj = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (ST) {
+                    gj = S.gc4[j];
+                    gj.w = S.pA32[j];
+                }
+                pair_b32<ST>(Q, I, pj, vj, gj, j, B);
+            }
+        }
+        finish_b32(P, Q, S, i, I, B);
     }
 }
 
@@ -456,8 +658,10 @@ __device__ __forceinline__ void pass_b32_chunk(const DevParams &P, const DevPara
 // autotuned launch parameters (dmph_autotune).
 template <bool ST, int WPB, int MINB>
 __global__ void __launch_bounds__(WPB * kWarp, MINB) k_pass_a32(DevParams P, DevParams32 Q, DevState S, const int *dB,
-                                                                int range)
+                                                                int range, int gate)
 {
+    // gate: list mode, where this stencil pass stands in only after a list overflow
+    if (gate && dB[B_LIST_OVF] == 0) return;
     __shared__ Tile32 tiles[WPB];
     const int lane = threadIdx.x & 31;
     FOR_EACH_CHUNK(dB, range, WPB, cidx) pass_a32_chunk<ST>(P, Q, S, tiles[threadIdx.x >> 5], lane, cidx);
@@ -465,8 +669,9 @@ __global__ void __launch_bounds__(WPB * kWarp, MINB) k_pass_a32(DevParams P, Dev
 
 template <bool ST, int WPB, int MINB>
 __global__ void __launch_bounds__(WPB * kWarp, MINB) k_pass_b32(DevParams P, DevParams32 Q, DevState S, const int *dB,
-                                                                int range)
+                                                                int range, int gate)
 {
+    if (gate && dB[B_LIST_OVF] == 0) return;
     __shared__ Tile32 tiles[WPB];
     __shared__ TileST tst[ST ? WPB : 1];
     const int lane = threadIdx.x & 31;
@@ -827,16 +1032,16 @@ static int grid_for(K kernel, int threads)
 }
 
 void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int range,
-                     int variant, cudaStream_t st)
+                     int variant, cudaStream_t st, int gate)
 {
 #define DMPH_LAUNCH_A(ID, WPB, MINB)                                                              \
     case ID:                                                                                      \
         if (P.surface_tension) {                                                                  \
             static const int g = grid_for(k_pass_a32<true, WPB, MINB>, WPB * kWarp);              \
-            k_pass_a32<true, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, range);           \
+            k_pass_a32<true, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, range, gate);           \
         } else {                                                                                  \
             static const int g = grid_for(k_pass_a32<false, WPB, MINB>, WPB * kWarp);             \
-            k_pass_a32<false, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, range);          \
+            k_pass_a32<false, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, range, gate);          \
         }                                                                                         \
         break;
     switch (variant) {
@@ -847,16 +1052,16 @@ void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S
 }
 
 void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
-                     cudaStream_t st)
+                     cudaStream_t st, int gate)
 {
 #define DMPH_LAUNCH_B(ID, WPB, MINB)                                                              \
     case ID:                                                                                      \
         if (P.surface_tension) {                                                                  \
             static const int g = grid_for(k_pass_b32<true, WPB, MINB>, WPB * kWarp);              \
-            k_pass_b32<true, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, CR_FLUID_SOLID);  \
+            k_pass_b32<true, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, CR_FLUID_SOLID, gate);  \
         } else {                                                                                  \
             static const int g = grid_for(k_pass_b32<false, WPB, MINB>, WPB * kWarp);             \
-            k_pass_b32<false, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, CR_FLUID_SOLID); \
+            k_pass_b32<false, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, CR_FLUID_SOLID, gate); \
         }                                                                                         \
         break;
     switch (variant) {
@@ -864,6 +1069,36 @@ void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S
     default: break;
     }
 #undef DMPH_LAUNCH_B
+}
+
+void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, cudaStream_t st)
+{
+    cudaMemsetAsync(dB + B_LIST_OVF, 0, sizeof(int), st);
+    cudaMemsetAsync(S.nbn, 0xFF, sizeof(int) * (size_t)P.N, st);
+    static const int g = grid_for(k_build_list32, 8 * kWarp);
+    k_build_list32<<<g, 8 * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2);
+}
+
+void launch_pass_a32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st)
+{
+    if (P.surface_tension) {
+        static const int g = grid_for(k_pass_a32_list<true>, 256);
+        k_pass_a32_list<true><<<g, 256, 0, st>>>(P, Q, S, dB);
+    } else {
+        static const int g = grid_for(k_pass_a32_list<false>, 256);
+        k_pass_a32_list<false><<<g, 256, 0, st>>>(P, Q, S, dB);
+    }
+}
+
+void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st)
+{
+    if (P.surface_tension) {
+        static const int g = grid_for(k_pass_b32_list<true>, 256);
+        k_pass_b32_list<true><<<g, 256, 0, st>>>(P, Q, S, dB);
+    } else {
+        static const int g = grid_for(k_pass_b32_list<false>, 256);
+        k_pass_b32_list<false><<<g, 256, 0, st>>>(P, Q, S, dB);
+    }
 }
 
 void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t st)

@@ -45,9 +45,12 @@ DevParams32 make_params32(const DevParams &P);
 void launch_drift32(const DevParams &P, const DevParams32 &Q, const DevState &S, const WallMotion &Wm,
                     unsigned long long *maxshift, int sms, cudaStream_t st);
 void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int range, int variant,
-                     cudaStream_t st);
+                     cudaStream_t st, int gate = 0);
 void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
-                     cudaStream_t st);
+                     cudaStream_t st, int gate = 0);
+void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, cudaStream_t st);
+void launch_pass_a32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
+void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
 void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t st);
 void launch_ens_pass_b32(const EnsScene *tab, int ns, int variant, cudaStream_t st);
 void launch_ens_fluid_accel32(const EnsScene *tab, int ns, cudaStream_t st);

@@ -622,8 +622,7 @@ int grid_slots(const dmph_ctx *ctx) { return ctx->sms * 4; }
 // pass A, pass B and the features at the current state
 void enqueue_features(dmph_ctx *ctx, Surrogate *s, float *x32, cudaStream_t st)
 {
-    launch_pass_a32(ctx->P, ctx->Q, ctx->S, ctx->dB, CR_WET, ctx->var_a, st);
-    launch_pass_b32(ctx->P, ctx->Q, ctx->S, ctx->dB, ctx->var_b, st);
+    enqueue_pair_passes32(ctx, st);
     static const int g = persistent_grid((const void *)k_features32, kFeatWarps * kWarp);
     k_features32<<<g, kFeatWarps * kWarp, 0, st>>>(ctx->P, ctx->Q, ctx->S, ctx->dB, s->fs, s->X, x32);
 }

@@ -43,6 +43,7 @@ def lib():
         L.dmph_get_bodies.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
         L.dmph_set_profiling.argtypes = [vp, C.c_int]
         L.dmph_set_graph.argtypes = [vp, C.c_int]
+        L.dmph_set_pair_mode.argtypes = [vp, C.c_int]
         L.dmph_get_phase_times.argtypes = [vp, vp, vp, C.c_int]
         L.dmph_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp, vp]
         L.dmph_set_variants.argtypes = [vp, C.c_int, C.c_int]
@@ -172,6 +173,10 @@ class Solver:
         return out
 
     PHASES = ("drift", "rebuild", "pass_a", "pass_b", "dem", "bodies")
+
+    def set_pair_mode(self, mode):
+        """"stencil" or "list" (dmph_set_pair_mode; FP32 split build)"""
+        self._check(lib().dmph_set_pair_mode(self._h, {"stencil": 0, "list": 1}[mode]))
 
     def set_graph(self, on=True):
         """replay each step as one CUDA graph (see dmph_set_graph)"""
@@ -311,6 +316,10 @@ class Ensemble:
         mb = np.zeros(PASS_VARIANTS, np.float32)
         self._check(lib().dmph_ensemble_autotune(self._h, C.byref(a), C.byref(b), _ptr(ma), _ptr(mb)))
         return a.value, b.value, ma, mb
+
+    def set_pair_mode(self, mode):
+        """"stencil" or "list" (dmph_set_pair_mode; FP32 split build)"""
+        self._check(lib().dmph_set_pair_mode(self._h, {"stencil": 0, "list": 1}[mode]))
 
     def set_graph(self, on=True):
         self._check(lib().dmph_ensemble_set_graph(self._h, 1 if on else 0))

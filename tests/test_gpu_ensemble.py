@@ -48,6 +48,8 @@ def same_state(a, b):
 def test_ensemble_matches_scenes_stepped_alone(graph):
     items = scene_list()
     alone = make(items)
+    for g in alone:
+        g.set_pair_mode("stencil")  # the ensemble kernels walk the stencil
     members = make(items)
     ens = solver.Ensemble(members)
     ens.set_graph(graph)
@@ -72,6 +74,8 @@ def test_ensemble_matches_scenes_stepped_alone(graph):
 def test_autotuned_variants_change_no_result():
     items = scene_list()[:2]
     ref = make(items)
+    for g in ref:
+        g.set_pair_mode("stencil")
     tuned = make(items)
     ens = solver.Ensemble(tuned)
     for g in ref:
