@@ -1095,6 +1095,7 @@ struct dmph_ensemble {
     cudaEvent_t join = nullptr;
     int var_a = 0, var_b = 0;
     bool use_graph = true;
+    bool use_list = false;  // pair passes over the members' Verlet lists
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     long long launches = 0, steps = 0, graph_steps = 0;
@@ -1175,11 +1176,12 @@ extern "C" int dmph_ensemble_create(dmph_ctx *const *scenes, int nscenes, dmph_e
         delete e;
         return DMPH_ECUDA;
     }
-    for (dmph_ctx *c : e->scenes) {
-        // the ensemble kernels walk the stencil; its members build no lists
-        c->use_list = false;
-        drop_graph(c);
-    }
+    // list mode when every member is in list mode
+    e->use_list = true;
+    for (dmph_ctx *c : e->scenes) e->use_list = e->use_list && c->use_list;
+    if (!e->use_list)
+        for (dmph_ctx *c : e->scenes) c->use_list = false;
+    for (dmph_ctx *c : e->scenes) drop_graph(c);
     *out = e;
     return DMPH_OK;
 }
@@ -1223,8 +1225,15 @@ static int ens_enqueue_step(dmph_ensemble *e, cudaGraph_t g)
         EK(cudaStreamWaitEvent(e->st, e->fork[k], 0));
     }
     // the pair passes of all scenes: one persistent launch each
-    launch_ens_pass_a32(e->tab, ns, e->var_a, e->st);
-    launch_ens_pass_b32(e->tab, ns, e->var_b, e->st);
+    if (e->use_list) {
+        launch_ens_pass_list(e->tab, ns, false, e->st);
+        launch_ens_pass_a32(e->tab, ns, e->var_a, e->st, 1);
+        launch_ens_pass_list(e->tab, ns, true, e->st);
+        launch_ens_pass_b32(e->tab, ns, e->var_b, e->st, 1);
+    } else {
+        launch_ens_pass_a32(e->tab, ns, e->var_a, e->st);
+        launch_ens_pass_b32(e->tab, ns, e->var_b, e->st);
+    }
     launch_ens_fluid_accel32(e->tab, ns, e->st);
     EK(cudaGetLastError());
     EK(cudaEventRecord(e->join, e->st));
@@ -1242,7 +1251,7 @@ static int ens_enqueue_step(dmph_ensemble *e, cudaGraph_t g)
 
 static long long ens_step_launches(const dmph_ensemble *e)
 {
-    long long n = 3;
+    long long n = 3 + (e->use_list ? 2 : 0);
     for (const dmph_ctx *c : e->scenes) n += 2 + dem_launches(c);
     return n;
 }
@@ -1285,7 +1294,7 @@ static int ens_step_once(dmph_ensemble *e)
     } else {
         const int rc = ens_enqueue_step(e, nullptr);
         if (rc) return rc;
-        e->launches += 3;
+        e->launches += 3 + (e->use_list ? 2 : 0);
         for (dmph_ctx *c : e->scenes) c->launches += dem_launches(c);
     }
     for (dmph_ctx *c : e->scenes) {

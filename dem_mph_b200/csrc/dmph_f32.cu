@@ -574,59 +574,69 @@ __device__ __forceinline__ float4 list_pos(const DevParams32 &Q, const DevState 
 }
 
 template <bool ST>
+__device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const DevParams32 &Q, const DevState &S, int i)
+{
+    const int cnt = S.nbn[i];
+    if (cnt < 0) return;
+    const long long ld = P.N;
+    const float cut2 = ST ? fmaxf(Q.RP2, fmaxf(Q.RA2, Q.RG2)) : Q.RP2;
+    const float4 pi = S.p4[i];
+    const int ti = unpack_type(__float_as_uint(pi.w));
+    const IA I{pi, S.v4[i], ti, is_solid(ti), is_wall(ti)};
+    AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
+    for (int k = 0; k < cnt; ++k) {
+        int j;
+        const float4 pj = list_pos(Q, S, __ldg(S.nbl + (long long)k * ld + i), j);
+        const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+        if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= cut2) pair_a32<ST>(Q, I, pj, S.v4[j], A);
+    }
+    finish_a32<ST>(P, Q, S, i, I, A);
+}
+
+template <bool ST>
 __global__ void __launch_bounds__(256) k_pass_a32_list(DevParams P, DevParams32 Q, DevState S, const int *dB)
 {
     if (dB[B_LIST_OVF]) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.N; i += gridDim.x * blockDim.x)
+        pass_a32_list_slot<ST>(P, Q, S, i);
+}
+
+template <bool ST>
+__device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const DevParams32 &Q, const DevState &S, int i)
+{
+    const int cnt = S.nbn[i];
+    if (cnt < 0) return;
     const long long ld = P.N;
-    const float cut2 = ST ? fmaxf(Q.RP2, fmaxf(Q.RA2, Q.RG2)) : Q.RP2;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.N; i += gridDim.x * blockDim.x) {
-        const int cnt = S.nbn[i];
-        if (cnt < 0) continue;
-        const float4 pi = S.p4[i];
-        const int ti = unpack_type(__float_as_uint(pi.w));
-        const IA I{pi, S.v4[i], ti, is_solid(ti), is_wall(ti)};
-        AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
-        for (int k = 0; k < cnt; ++k) {
-            int j;
-            const float4 pj = list_pos(Q, S, __ldg(S.nbl + (long long)k * ld + i), j);
-            const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-            if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= cut2) pair_a32<ST>(Q, I, pj, S.v4[j], A);
+    const float cut2 = ST ? fmaxf(fmaxf(Q.RP2, Q.RV2), fmaxf(Q.RA2, Q.RG2)) : fmaxf(Q.RP2, Q.RV2);
+    const float4 pi = S.p4[i];
+    const int ti = unpack_type(__float_as_uint(pi.w));
+    const IB I = make_ib<ST>(P, S, i, pi, S.v4[i], ti);
+    AccB B = acc_b_zero();
+    for (int k = 0; k < cnt; ++k) {
+        int j;
+        const float4 pj = list_pos(Q, S, __ldg(S.nbl + (long long)k * ld + i), j);
+        const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+        if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) < cut2) {
+            float4 vj = S.v4[j];
+            vj.w = S.pres32[j];
+            float4 gj = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (ST) {
+                gj = S.gc4[j];
+                gj.w = S.pA32[j];
+            }
+            pair_b32<ST>(Q, I, pj, vj, gj, j, B);
         }
-        finish_a32<ST>(P, Q, S, i, I, A);
     }
+    finish_b32(P, Q, S, i, I, B);
 }
 
 template <bool ST>
 __global__ void __launch_bounds__(256) k_pass_b32_list(DevParams P, DevParams32 Q, DevState S, const int *dB)
 {
     if (dB[B_LIST_OVF]) return;
-    const long long ld = P.N;
-    const float cut2 = ST ? fmaxf(fmaxf(Q.RP2, Q.RV2), fmaxf(Q.RA2, Q.RG2)) : fmaxf(Q.RP2, Q.RV2);
     const int end = dB[B_SE];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
-        const int cnt = S.nbn[i];
-        if (cnt < 0) continue;
-        const float4 pi = S.p4[i];
-        const int ti = unpack_type(__float_as_uint(pi.w));
-        const IB I = make_ib<ST>(P, S, i, pi, S.v4[i], ti);
-        AccB B = acc_b_zero();
-        for (int k = 0; k < cnt; ++k) {
-            int j;
-            const float4 pj = list_pos(Q, S, __ldg(S.nbl + (long long)k * ld + i), j);
-            const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-            if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) < cut2) {
-                float4 vj = S.v4[j];
-                vj.w = S.pres32[j];
-                float4 gj = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (ST) {
-                    gj = S.gc4[j];
-                    gj.w = S.pA32[j];
-                }
-                pair_b32<ST>(Q, I, pj, vj, gj, j, B);
-            }
-        }
-        finish_b32(P, Q, S, i, I, B);
-    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x)
+        pass_b32_list_slot<ST>(P, Q, S, i);
 }
 
 // chunk bodies dispatched on the chunk's size: 4 lanes per particle for up to
@@ -685,13 +695,16 @@ __global__ void __launch_bounds__(WPB * kWarp, MINB) k_pass_b32(DevParams P, Dev
 // each scene's device bounds), each warp maps its global chunk index to a
 // scene by binary search and runs the same per-chunk body with that scene's
 // parameters and state, read from the scene table in global memory.
-__device__ __forceinline__ int ens_prefix(const EnsScene *__restrict__ tab, int ns, int range, int *pre, int *beg)
+__device__ __forceinline__ int ens_prefix(const EnsScene *__restrict__ tab, int ns, int range, int *pre, int *beg,
+                                          int gate)
 {
     for (int k = threadIdx.x; k < ns; k += blockDim.x) {
         int b, e;
         chunk_range(tab[k].dB, range, b, e);
+        // gate: list mode, where the stencil walks only scenes whose lists overflowed
+        const bool skip = gate && tab[k].S.nbn != nullptr && tab[k].dB[B_LIST_OVF] == 0;
         beg[k] = b;
-        pre[k + 1] = e - b;
+        pre[k + 1] = skip ? 0 : e - b;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -714,11 +727,12 @@ __device__ __forceinline__ int ens_scene_of(const int *pre, int ns, int g)
 }
 
 template <int WPB, int MINB>
-__global__ void __launch_bounds__(WPB * kWarp, MINB) k_ens_pass_a32(const EnsScene *__restrict__ tab, int ns, int range)
+__global__ void __launch_bounds__(WPB * kWarp, MINB) k_ens_pass_a32(const EnsScene *__restrict__ tab, int ns, int range,
+                                                                    int gate)
 {
     __shared__ Tile32 tiles[WPB];
     __shared__ int pre[kMaxEnsemble + 1], beg[kMaxEnsemble];
-    const int total = ens_prefix(tab, ns, range, pre, beg);
+    const int total = ens_prefix(tab, ns, range, pre, beg, gate);
     const int lane = threadIdx.x & 31;
     for (int g = blockIdx.x * WPB + (int)(threadIdx.x >> 5); g < total; g += gridDim.x * WPB) {
         const int k = ens_scene_of(pre, ns, g);
@@ -730,12 +744,12 @@ __global__ void __launch_bounds__(WPB * kWarp, MINB) k_ens_pass_a32(const EnsSce
 }
 
 template <int WPB, int MINB>
-__global__ void __launch_bounds__(WPB * kWarp, MINB) k_ens_pass_b32(const EnsScene *__restrict__ tab, int ns)
+__global__ void __launch_bounds__(WPB * kWarp, MINB) k_ens_pass_b32(const EnsScene *__restrict__ tab, int ns, int gate)
 {
     __shared__ Tile32 tiles[WPB];
     __shared__ TileST tst[WPB];
     __shared__ int pre[kMaxEnsemble + 1], beg[kMaxEnsemble];
-    const int total = ens_prefix(tab, ns, CR_FLUID_SOLID, pre, beg);
+    const int total = ens_prefix(tab, ns, CR_FLUID_SOLID, pre, beg, gate);
     const int lane = threadIdx.x & 31;
     for (int g = blockIdx.x * WPB + (int)(threadIdx.x >> 5); g < total; g += gridDim.x * WPB) {
         const int k = ens_scene_of(pre, ns, g);
@@ -744,6 +758,45 @@ __global__ void __launch_bounds__(WPB * kWarp, MINB) k_ens_pass_b32(const EnsSce
         const int w = threadIdx.x >> 5;
         if (e.P.surface_tension) pass_b32_chunk<true>(e.P, e.Q, e.S, tiles[w], tst[w], lane, cidx);
         else pass_b32_chunk<false>(e.P, e.Q, e.S, tiles[w], tst[w], lane, cidx);
+    }
+}
+
+// List-mode ensemble passes: one thread per slot over the concatenated slot
+// ranges of the scenes (all slots for pass A, fluid and debris for pass B);
+// a scene whose lists overflowed at its last rebuild is left to the stencil
+// ensemble kernels, which then run for that scene only.
+__device__ __forceinline__ int ens_slot_prefix(const EnsScene *__restrict__ tab, int ns, bool pass_b, int *pre)
+{
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+        const EnsScene &e = tab[k];
+        const bool ok = e.S.nbn != nullptr && e.dB[B_LIST_OVF] == 0;
+        pre[k + 1] = ok ? (pass_b ? e.dB[B_SE] : e.P.N) : 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        pre[0] = 0;
+        for (int k = 0; k < ns; ++k) pre[k + 1] += pre[k];
+    }
+    __syncthreads();
+    return pre[ns];
+}
+
+template <bool PASS_B>
+__global__ void __launch_bounds__(256) k_ens_pass_list(const EnsScene *__restrict__ tab, int ns)
+{
+    __shared__ int pre[kMaxEnsemble + 1];
+    const int total = ens_slot_prefix(tab, ns, PASS_B, pre);
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        const int k = ens_scene_of(pre, ns, g);
+        const EnsScene &e = tab[k];
+        const int i = g - pre[k];
+        if (PASS_B) {
+            if (e.P.surface_tension) pass_b32_list_slot<true>(e.P, e.Q, e.S, i);
+            else pass_b32_list_slot<false>(e.P, e.Q, e.S, i);
+        } else {
+            if (e.P.surface_tension) pass_a32_list_slot<true>(e.P, e.Q, e.S, i);
+            else pass_a32_list_slot<false>(e.P, e.Q, e.S, i);
+        }
     }
 }
 
@@ -1101,12 +1154,12 @@ void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevSta
     }
 }
 
-void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t st)
+void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t st, int gate)
 {
 #define DMPH_LAUNCH_EA(ID, WPB, MINB)                                                     \
     case ID: {                                                                            \
         static const int g = grid_for(k_ens_pass_a32<WPB, MINB>, WPB * kWarp);            \
-        k_ens_pass_a32<WPB, MINB><<<g, WPB * kWarp, 0, st>>>(tab, ns, CR_WET);            \
+        k_ens_pass_a32<WPB, MINB><<<g, WPB * kWarp, 0, st>>>(tab, ns, CR_WET, gate);            \
         break;                                                                            \
     }
     switch (variant) {
@@ -1116,12 +1169,12 @@ void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t 
 #undef DMPH_LAUNCH_EA
 }
 
-void launch_ens_pass_b32(const EnsScene *tab, int ns, int variant, cudaStream_t st)
+void launch_ens_pass_b32(const EnsScene *tab, int ns, int variant, cudaStream_t st, int gate)
 {
 #define DMPH_LAUNCH_EB(ID, WPB, MINB)                                                     \
     case ID: {                                                                            \
         static const int g = grid_for(k_ens_pass_b32<WPB, MINB>, WPB * kWarp);            \
-        k_ens_pass_b32<WPB, MINB><<<g, WPB * kWarp, 0, st>>>(tab, ns);                    \
+        k_ens_pass_b32<WPB, MINB><<<g, WPB * kWarp, 0, st>>>(tab, ns, gate);                    \
         break;                                                                            \
     }
     switch (variant) {
@@ -1129,6 +1182,17 @@ void launch_ens_pass_b32(const EnsScene *tab, int ns, int variant, cudaStream_t 
     default: break;
     }
 #undef DMPH_LAUNCH_EB
+}
+
+void launch_ens_pass_list(const EnsScene *tab, int ns, bool pass_b, cudaStream_t st)
+{
+    if (pass_b) {
+        static const int g = grid_for(k_ens_pass_list<true>, 256);
+        k_ens_pass_list<true><<<g, 256, 0, st>>>(tab, ns);
+    } else {
+        static const int g = grid_for(k_ens_pass_list<false>, 256);
+        k_ens_pass_list<false><<<g, 256, 0, st>>>(tab, ns);
+    }
 }
 
 void launch_ens_fluid_accel32(const EnsScene *tab, int ns, cudaStream_t st)

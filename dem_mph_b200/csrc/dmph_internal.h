@@ -51,8 +51,9 @@ void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S
 void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, cudaStream_t st);
 void launch_pass_a32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
 void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
-void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t st);
-void launch_ens_pass_b32(const EnsScene *tab, int ns, int variant, cudaStream_t st);
+void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t st, int gate = 0);
+void launch_ens_pass_b32(const EnsScene *tab, int ns, int variant, cudaStream_t st, int gate = 0);
+void launch_ens_pass_list(const EnsScene *tab, int ns, bool pass_b, cudaStream_t st);
 void launch_ens_fluid_accel32(const EnsScene *tab, int ns, cudaStream_t st);
 void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
 void launch_export32(const DevParams &P, const DevState &S, double *pos, double *vel, cudaStream_t st);

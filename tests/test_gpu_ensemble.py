@@ -44,13 +44,13 @@ def same_state(a, b):
             and np.array_equal(va, vb) and np.array_equal(a.field("PressureP"), b.field("PressureP")))
 
 
-@pytest.mark.parametrize("graph", [True, False])
-def test_ensemble_matches_scenes_stepped_alone(graph):
+@pytest.mark.parametrize("graph,mode", [(True, "list"), (False, "list"), (True, "stencil")])
+def test_ensemble_matches_scenes_stepped_alone(graph, mode):
     items = scene_list()
     alone = make(items)
-    for g in alone:
-        g.set_pair_mode("stencil")  # the ensemble kernels walk the stencil
     members = make(items)
+    for g in alone + members:
+        g.set_pair_mode(mode)
     ens = solver.Ensemble(members)
     ens.set_graph(graph)
     assert len({g.n for g in members}) == len(members)  # uneven sizes
@@ -74,8 +74,6 @@ def test_ensemble_matches_scenes_stepped_alone(graph):
 def test_autotuned_variants_change_no_result():
     items = scene_list()[:2]
     ref = make(items)
-    for g in ref:
-        g.set_pair_mode("stencil")
     tuned = make(items)
     ens = solver.Ensemble(tuned)
     for g in ref:
