@@ -146,11 +146,11 @@ void dmph::enqueue_passes(dmph_ctx *ctx, cudaStream_t st)
     if (ctx->fp32) {
         const DevParams32 &Q = ctx->Q;
         phase_begin(ctx);
-        if (ctx->use_list) launch_pass_a32_list(P, Q, S, dB, st);
+        if (ctx->use_list) launch_pass_a32_list(P, Q, S, dB, ctx->var_la, st);
         launch_pass_a32(P, Q, S, dB, CR_WET, ctx->var_a, st, ctx->use_list ? 1 : 0);
         phase_end(ctx, 2);
         phase_begin(ctx);
-        if (ctx->use_list) launch_pass_b32_list(P, Q, S, dB, st);
+        if (ctx->use_list) launch_pass_b32_list(P, Q, S, dB, ctx->var_lb, st);
         launch_pass_b32(P, Q, S, dB, ctx->var_b, st, ctx->use_list ? 1 : 0);
         launch_fluid_accel32(Q, S, dB, st);
         phase_end(ctx, 3);
@@ -172,9 +172,9 @@ void dmph::enqueue_pair_passes32(dmph_ctx *ctx, cudaStream_t st)
 {
     const DevParams &P = ctx->P;
     const DevParams32 &Q = ctx->Q;
-    if (ctx->use_list) launch_pass_a32_list(P, Q, ctx->S, ctx->dB, st);
+    if (ctx->use_list) launch_pass_a32_list(P, Q, ctx->S, ctx->dB, ctx->var_la, st);
     launch_pass_a32(P, Q, ctx->S, ctx->dB, CR_WET, ctx->var_a, st, ctx->use_list ? 1 : 0);
-    if (ctx->use_list) launch_pass_b32_list(P, Q, ctx->S, ctx->dB, st);
+    if (ctx->use_list) launch_pass_b32_list(P, Q, ctx->S, ctx->dB, ctx->var_lb, st);
     launch_pass_b32(P, Q, ctx->S, ctx->dB, ctx->var_b, st, ctx->use_list ? 1 : 0);
 }
 
@@ -1024,11 +1024,12 @@ extern "C" const char *dmph_version(void)
 // pure functions of the state they read, so repeating them changes nothing)
 // and keeps the fastest.
 template <class Launch>
-static int time_variants(dmph_ctx *ctx, cudaStream_t st, Launch &&launch, float *ms_out, int *best)
+static int time_variants(dmph_ctx *ctx, cudaStream_t st, Launch &&launch, float *ms_out, int *best,
+                         int nvar = kPassVariants)
 {
     float best_ms = 1e30f;
     *best = 0;
-    for (int v = 0; v < kPassVariants; ++v) {
+    for (int v = 0; v < nvar; ++v) {
         launch(v);  // warm-up: first launch of a variant also sizes its grid
         CK(cudaEventRecord(ctx->ev0, st));
         for (int r = 0; r < 3; ++r) launch(v);
@@ -1056,6 +1057,23 @@ extern "C" int dmph_autotune(dmph_ctx *ctx, int *variant_a, int *variant_b, floa
     }
     const DevParams &P = ctx->P;
     const DevParams32 &Q = ctx->Q;
+    if (ctx->use_list) {
+        // list mode: the variants of the list passes (the lists of the last
+        // rebuild are valid for the current state)
+        int rc = time_variants(ctx, ctx->st, [&](int v) { launch_pass_a32_list(P, Q, ctx->S, ctx->dB, v, ctx->st); },
+                               ms_a, &ctx->var_la, kListVariants);
+        if (rc) return rc;
+        launch_pass_a32_list(P, Q, ctx->S, ctx->dB, ctx->var_la, ctx->st);
+        rc = time_variants(ctx, ctx->st, [&](int v) { launch_pass_b32_list(P, Q, ctx->S, ctx->dB, v, ctx->st); },
+                           ms_b, &ctx->var_lb, kListVariants);
+        if (rc) return rc;
+        launch_pass_b32_list(P, Q, ctx->S, ctx->dB, ctx->var_lb, ctx->st);
+        CK(cudaStreamSynchronize(ctx->st));
+        drop_graph(ctx);
+        if (variant_a) *variant_a = ctx->var_la;
+        if (variant_b) *variant_b = ctx->var_lb;
+        return DMPH_OK;
+    }
     int rc = time_variants(ctx, ctx->st, [&](int v) { launch_pass_a32(P, Q, ctx->S, ctx->dB, CR_WET, v, ctx->st); },
                            ms_a, &ctx->var_a);
     if (rc) return rc;
@@ -1075,12 +1093,18 @@ extern "C" int dmph_autotune(dmph_ctx *ctx, int *variant_a, int *variant_b, floa
 extern "C" int dmph_set_variants(dmph_ctx *ctx, int variant_a, int variant_b)
 {
     if (!ctx) return DMPH_EINVAL;
-    if (variant_a < 0 || variant_a >= kPassVariants || variant_b < 0 || variant_b >= kPassVariants) {
+    const int nv = ctx->use_list ? kListVariants : kPassVariants;
+    if (variant_a < 0 || variant_a >= nv || variant_b < 0 || variant_b >= nv) {
         ctx->err = "launch variant out of range";
         return DMPH_ERANGE;
     }
-    ctx->var_a = variant_a;
-    ctx->var_b = variant_b;
+    if (ctx->use_list) {
+        ctx->var_la = variant_a;
+        ctx->var_lb = variant_b;
+    } else {
+        ctx->var_a = variant_a;
+        ctx->var_b = variant_b;
+    }
     drop_graph(ctx);
     return DMPH_OK;
 }

@@ -45,6 +45,7 @@ struct dmph_ctx {
     long long graph_steps = 0, host_rebuilds = 0;
     int var_a = 0, var_b = 0;  // launch variants of the FP32 pair passes (dmph_autotune)
     bool use_list = false;     // FP32 pair passes over Verlet lists built at each rebuild
+    int var_la = 1, var_lb = 1;  // launch variants of the list passes
     Chunk *chunks2 = nullptr;  // partition scratch
     int demSteps = 0;
     double time = 0.0;

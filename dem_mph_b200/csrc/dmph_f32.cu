@@ -573,7 +573,9 @@ __device__ __forceinline__ float4 list_pos(const DevParams32 &Q, const DevState 
                        fmaf((float)dz, Q.cw[2], pj.z), __int_as_float(unpack_type(__float_as_uint(pj.w))));
 }
 
-template <bool ST>
+// BATCH list entries at a time: their index loads, then their gathers, are
+// independent, so the latencies overlap; pairs are still taken in list order
+template <bool ST, int BATCH>
 __device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const DevParams32 &Q, const DevState &S, int i)
 {
     const int cnt = S.nbn[i];
@@ -584,24 +586,35 @@ __device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const Dev
     const int ti = unpack_type(__float_as_uint(pi.w));
     const IA I{pi, S.v4[i], ti, is_solid(ti), is_wall(ti)};
     AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
-    for (int k = 0; k < cnt; ++k) {
-        int j;
-        const float4 pj = list_pos(Q, S, __ldg(S.nbl + (long long)k * ld + i), j);
-        const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-        if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= cut2) pair_a32<ST>(Q, I, pj, S.v4[j], A);
+    for (int k0 = 0; k0 < cnt; k0 += BATCH) {
+        unsigned e[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) e[u] = k0 + u < cnt ? __ldg(S.nbl + (long long)(k0 + u) * ld + i) : 0u;
+        float4 pj[BATCH], vj[BATCH];
+        int j[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+            pj[u] = list_pos(Q, S, e[u], j[u]);
+            vj[u] = S.v4[j[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+            const float q0 = pj[u].x - pi.x, q1 = pj[u].y - pi.y, q2 = pj[u].z - pi.z;
+            if (k0 + u < cnt && fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= cut2) pair_a32<ST>(Q, I, pj[u], vj[u], A);
+        }
     }
     finish_a32<ST>(P, Q, S, i, I, A);
 }
 
-template <bool ST>
-__global__ void __launch_bounds__(256) k_pass_a32_list(DevParams P, DevParams32 Q, DevState S, const int *dB)
+template <bool ST, int BATCH, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_pass_a32_list(DevParams P, DevParams32 Q, DevState S, const int *dB)
 {
     if (dB[B_LIST_OVF]) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.N; i += gridDim.x * blockDim.x)
-        pass_a32_list_slot<ST>(P, Q, S, i);
+        pass_a32_list_slot<ST, BATCH>(P, Q, S, i);
 }
 
-template <bool ST>
+template <bool ST, int BATCH>
 __device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const DevParams32 &Q, const DevState &S, int i)
 {
     const int cnt = S.nbn[i];
@@ -612,31 +625,41 @@ __device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const Dev
     const int ti = unpack_type(__float_as_uint(pi.w));
     const IB I = make_ib<ST>(P, S, i, pi, S.v4[i], ti);
     AccB B = acc_b_zero();
-    for (int k = 0; k < cnt; ++k) {
-        int j;
-        const float4 pj = list_pos(Q, S, __ldg(S.nbl + (long long)k * ld + i), j);
-        const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-        if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) < cut2) {
-            float4 vj = S.v4[j];
-            vj.w = S.pres32[j];
-            float4 gj = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (ST) {
-                gj = S.gc4[j];
-                gj.w = S.pA32[j];
+    for (int k0 = 0; k0 < cnt; k0 += BATCH) {
+        unsigned e[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) e[u] = k0 + u < cnt ? __ldg(S.nbl + (long long)(k0 + u) * ld + i) : 0u;
+        float4 pj[BATCH], vj[BATCH];
+        int j[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+            pj[u] = list_pos(Q, S, e[u], j[u]);
+            vj[u] = S.v4[j[u]];
+            vj[u].w = S.pres32[j[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < BATCH; ++u) {
+            const float q0 = pj[u].x - pi.x, q1 = pj[u].y - pi.y, q2 = pj[u].z - pi.z;
+            if (k0 + u < cnt && fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) < cut2) {
+                float4 gj = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (ST) {
+                    gj = S.gc4[j[u]];
+                    gj.w = S.pA32[j[u]];
+                }
+                pair_b32<ST>(Q, I, pj[u], vj[u], gj, j[u], B);
             }
-            pair_b32<ST>(Q, I, pj, vj, gj, j, B);
         }
     }
     finish_b32(P, Q, S, i, I, B);
 }
 
-template <bool ST>
-__global__ void __launch_bounds__(256) k_pass_b32_list(DevParams P, DevParams32 Q, DevState S, const int *dB)
+template <bool ST, int BATCH, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_pass_b32_list(DevParams P, DevParams32 Q, DevState S, const int *dB)
 {
     if (dB[B_LIST_OVF]) return;
     const int end = dB[B_SE];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x)
-        pass_b32_list_slot<ST>(P, Q, S, i);
+        pass_b32_list_slot<ST, BATCH>(P, Q, S, i);
 }
 
 // chunk bodies dispatched on the chunk's size: 4 lanes per particle for up to
@@ -791,11 +814,11 @@ __global__ void __launch_bounds__(256) k_ens_pass_list(const EnsScene *__restric
         const EnsScene &e = tab[k];
         const int i = g - pre[k];
         if (PASS_B) {
-            if (e.P.surface_tension) pass_b32_list_slot<true>(e.P, e.Q, e.S, i);
-            else pass_b32_list_slot<false>(e.P, e.Q, e.S, i);
+            if (e.P.surface_tension) pass_b32_list_slot<true, 2>(e.P, e.Q, e.S, i);
+            else pass_b32_list_slot<false, 2>(e.P, e.Q, e.S, i);
         } else {
-            if (e.P.surface_tension) pass_a32_list_slot<true>(e.P, e.Q, e.S, i);
-            else pass_a32_list_slot<false>(e.P, e.Q, e.S, i);
+            if (e.P.surface_tension) pass_a32_list_slot<true, 2>(e.P, e.Q, e.S, i);
+            else pass_a32_list_slot<false, 2>(e.P, e.Q, e.S, i);
         }
     }
 }
@@ -1132,26 +1155,48 @@ void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevStat
     k_build_list32<<<g, 8 * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2);
 }
 
-void launch_pass_a32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st)
+// list-pass variants the autotuner chooses from: entries per batch x
+// resident blocks of 256 threads requested per SM
+#define DMPH_LIST_VARIANTS(X) X(0, 1, 4) X(1, 2, 3) X(2, 4, 2) X(3, 2, 4)
+
+void launch_pass_a32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
+                          cudaStream_t st)
 {
-    if (P.surface_tension) {
-        static const int g = grid_for(k_pass_a32_list<true>, 256);
-        k_pass_a32_list<true><<<g, 256, 0, st>>>(P, Q, S, dB);
-    } else {
-        static const int g = grid_for(k_pass_a32_list<false>, 256);
-        k_pass_a32_list<false><<<g, 256, 0, st>>>(P, Q, S, dB);
+#define DMPH_LAUNCH_LA(ID, BATCH, MINB)                                                   \
+    case ID:                                                                              \
+        if (P.surface_tension) {                                                          \
+            static const int g = grid_for(k_pass_a32_list<true, BATCH, MINB>, 256);       \
+            k_pass_a32_list<true, BATCH, MINB><<<g, 256, 0, st>>>(P, Q, S, dB);           \
+        } else {                                                                          \
+            static const int g = grid_for(k_pass_a32_list<false, BATCH, MINB>, 256);      \
+            k_pass_a32_list<false, BATCH, MINB><<<g, 256, 0, st>>>(P, Q, S, dB);          \
+        }                                                                                 \
+        break;
+    switch (variant) {
+        DMPH_LIST_VARIANTS(DMPH_LAUNCH_LA)
+    default: break;
     }
+#undef DMPH_LAUNCH_LA
 }
 
-void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st)
+void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
+                          cudaStream_t st)
 {
-    if (P.surface_tension) {
-        static const int g = grid_for(k_pass_b32_list<true>, 256);
-        k_pass_b32_list<true><<<g, 256, 0, st>>>(P, Q, S, dB);
-    } else {
-        static const int g = grid_for(k_pass_b32_list<false>, 256);
-        k_pass_b32_list<false><<<g, 256, 0, st>>>(P, Q, S, dB);
+#define DMPH_LAUNCH_LB(ID, BATCH, MINB)                                                   \
+    case ID:                                                                              \
+        if (P.surface_tension) {                                                          \
+            static const int g = grid_for(k_pass_b32_list<true, BATCH, MINB>, 256);       \
+            k_pass_b32_list<true, BATCH, MINB><<<g, 256, 0, st>>>(P, Q, S, dB);           \
+        } else {                                                                          \
+            static const int g = grid_for(k_pass_b32_list<false, BATCH, MINB>, 256);      \
+            k_pass_b32_list<false, BATCH, MINB><<<g, 256, 0, st>>>(P, Q, S, dB);          \
+        }                                                                                 \
+        break;
+    switch (variant) {
+        DMPH_LIST_VARIANTS(DMPH_LAUNCH_LB)
+    default: break;
     }
+#undef DMPH_LAUNCH_LB
 }
 
 void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t st, int gate)

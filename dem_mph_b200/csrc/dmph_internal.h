@@ -49,8 +49,10 @@ void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S
 void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
                      cudaStream_t st, int gate = 0);
 void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, cudaStream_t st);
-void launch_pass_a32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
-void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
+void launch_pass_a32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
+                          cudaStream_t st);
+void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
+                          cudaStream_t st);
 void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t st, int gate = 0);
 void launch_ens_pass_b32(const EnsScene *tab, int ns, int variant, cudaStream_t st, int gate = 0);
 void launch_ens_pass_list(const EnsScene *tab, int ns, bool pass_b, cudaStream_t st);

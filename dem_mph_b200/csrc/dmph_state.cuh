@@ -146,6 +146,7 @@ struct WallMotion {
 // these is the scene table)
 constexpr int kMaxEnsemble = 256;
 constexpr int kPassVariants = 5;
+constexpr int kListVariants = 4;
 struct EnsScene {
     DevParams P;
     DevParams32 Q;

@@ -75,7 +75,8 @@ def lib():
     return _lib
 
 
-PASS_VARIANTS = 5  # DMPH_PASS_VARIANTS
+PASS_VARIANTS = 5  # DMPH_PASS_VARIANTS (stencil passes)
+LIST_VARIANTS = 4  # DMPH_LIST_VARIANTS (Verlet-list passes, the FP32 default)
 
 
 class DmphError(RuntimeError):

@@ -258,8 +258,12 @@ int dmph_set_graph(dmph_ctx *ctx, int enable);
  * block x resident blocks per SM requested from the register allocator) of
  * pass A and pass B on the current state and keeps the fastest for the
  * following steps.  Reports the chosen variants and, when ms_a/ms_b are
- * non-NULL, the time of each of DMPH_PASS_VARIANTS variants.  The passes
- * only read the state, so tuning changes no result.  FP32 split build only. */
+ * non-NULL, the time of each of DMPH_PASS_VARIANTS variants.  In Verlet-list
+ * mode (dmph_set_pair_mode) the variants are those of the list passes
+ * (entries loaded per batch x resident blocks, DMPH_LIST_VARIANTS of them)
+ * and dmph_set_variants sets those.  The passes only read the state, so
+ * tuning changes no result.  FP32 split build only. */
+#define DMPH_LIST_VARIANTS 4
 #define DMPH_PASS_VARIANTS 5
 int dmph_autotune(dmph_ctx *ctx, int *variant_a, int *variant_b, float *ms_a, float *ms_b);
 int dmph_set_variants(dmph_ctx *ctx, int variant_a, int variant_b);

@@ -88,9 +88,18 @@ def test_autotuned_variants_change_no_result():
     for a, b in zip(ref, tuned):
         assert same_state(a, b)
     ens.close()
-    # single-scene tuner, and every variant forced in turn
+    # single-scene tuner, and every variant forced in turn, in both pair modes
     a, b = ref[0], tuned[0]
-    ta, tb, _, _ = b.autotune()
+    ta, tb, ma, mb = b.autotune()  # list mode: the list-pass variants
+    assert 0 <= ta < solver.LIST_VARIANTS and np.all(ma[:solver.LIST_VARIANTS] > 0)
+    for v in range(solver.LIST_VARIANTS):
+        b.set_variants(v, (v + 2) % solver.LIST_VARIANTS)
+        a.step(3)
+        b.step(3)
+        assert same_state(a, b), v
+    a.set_pair_mode("stencil")
+    b.set_pair_mode("stencil")
+    b.autotune()
     for v in range(solver.PASS_VARIANTS):
         b.set_variants(v, (v + 2) % solver.PASS_VARIANTS)
         a.step(3)
