@@ -241,8 +241,14 @@ def main():
         bytes_launch = n * (bpp - 24)
         dur = pa_ms / max(pa_n, 1)
     achieved = bytes_launch / (dur / 1e3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_" + top, "achieved": achieved, "peak": peaks["hbm_gbs"],
-                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+    # DRAM bytes of one pass-B list launch on config 2 from an ncu capture
+    # (dram__bytes_read.sum + dram__bytes_write.sum); the list is most of it
+    traffic = 679.4e6 if (args.workload == "config2" and args.precision == "fp32" and top == "pass_b") else None
+    roofline = {"bound": "hbm", "kernel": ("k_pass_b32_list" if args.precision == "fp32" and top == "pass_b"
+                                           else "k_" + top),
+                "achieved": achieved, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                "traffic_source": "ncu capture of one launch of the same kernel and workload" if traffic else None,
                 "peak_source": peak_src, "launch_ms": dur,
                 "phase_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in ph.items()}}
 

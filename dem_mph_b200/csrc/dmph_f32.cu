@@ -546,14 +546,20 @@ __global__ void __launch_bounds__(8 * kWarp) k_build_list32(DevParams P, DevPara
             },
             [&](int base, int nb) {
                 if (!active) return;
-                for (int s = 0; s < nb; ++s) {
-                    if (base + s == i) continue;
+                unsigned m = 0;
+#pragma unroll
+                for (int s = 0; s < kWarp; ++s) {
                     const float4 pj = tl.p[s];
                     const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-                    if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= rc2) {
-                        if (cnt < cap) S.nbl[(long long)cnt * ld + i] = tl.e[s];
-                        ++cnt;
-                    }
+                    m |= (s < nb && fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= rc2) ? (1u << s) : 0u;
+                }
+                const int self = i - base;
+                if (self >= 0 && self < kWarp) m &= ~(1u << self);
+                while (m) {  // ascending candidate order
+                    const int s = __ffs(m) - 1;
+                    m &= m - 1;
+                    if (cnt < cap) S.nbl[(long long)cnt * ld + i] = tl.e[s];
+                    ++cnt;
                 }
             });
         if (!active) continue;
