@@ -42,6 +42,7 @@ FIELDS = {
     "SolidNeighborCount": (14, "i4", 1),
     "CellIndex": (15, "i4", 1),
     "Mass": (16, "f8", 1),
+    "VirialPressure": (17, "f8", 1),
 }
 
 _D6 = C.c_double * TYPE_COUNT

@@ -638,6 +638,25 @@ extern "C" int dmph_get_field(dmph_ctx *ctx, int field_id, void *out)
         }
         CK(cudaGetLastError());
     }
+    if (field_id == DMPH_FIELD_VIRIAL_PRESSURE) {
+        if (!ctx->vir) {
+            const int rc = dalloc(ctx, &ctx->vir, N);
+            if (rc) return rc;
+        }
+        if (ctx->fp32) {
+            // the FP64 planes of the state the virial reads
+            const int n = (int)N;
+            launch_export32(ctx->P, S, S.pos, S.vel, ctx->st);
+            launch_widen_f(S.pres32, S.pres, n, ctx->st);
+            launch_widen_f(S.pA32, S.pA, n, ctx->st);
+            launch_widen_f4(S.gc4, S.gc, n, n, ctx->st);
+        }
+        launch_virial(ctx->P, S, ctx->dB, ctx->vir, ctx->st);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, ctx->vir, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        return DMPH_OK;
+    }
     switch (field_id) {
     case DMPH_FIELD_FORCE: return d2h_planes(ctx, S.frc, (double *)out);
     case DMPH_FIELD_GRAVITY_CENTER: return d2h_planes(ctx, S.gc, (double *)out);

@@ -46,6 +46,7 @@ struct dmph_ctx {
     int var_a = 0, var_b = 0;  // launch variants of the FP32 pair passes (dmph_autotune)
     bool use_list = false;     // FP32 pair passes over Verlet lists built at each rebuild
     int var_la = 1, var_lb = 1;  // launch variants of the list passes
+    double *vir = nullptr;        // virial pressure (allocated on the first request)
     Chunk *chunks2 = nullptr;  // partition scratch
     int demSteps = 0;
     double time = 0.0;

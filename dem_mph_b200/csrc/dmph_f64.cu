@@ -620,6 +620,116 @@ void launch_pass_a(const DevParams &P, const DevState &S, const int *dB, int ran
     static const int g = persistent_grid((const void *)k_pass_a, kBlock);
     k_pass_a<<<g, kBlock, 0, st>>>(P, S, dB, range, init_only);
 }
+// Virial stress and pressure of the output cadence
+// (calculateVirialStressAtParticle, source/DEM-MPH.cpp:2904-3149): the
+// reference runs four passes over the neighbour list (pressure P, attractive
+// pressure A, viscosity V, diffuse interface G) and adds each pass's
+// per-particle stress matrix in turn.  The four matrices are accumulated here
+// in one traversal, pair by pair in list order, and added in the same order,
+// so the result is the reference's to the last bit.  Reads the FP64 planes:
+// pos, vel, pres, pA, gc (FP32 builds widen into them first).
+__global__ void __launch_bounds__(kBlock) k_virial(DevParams P, DevState S, const int *dB, double *vir)
+{
+    __shared__ TileA tiles[kWarpsPerBlock];
+    TileA &tl = tiles[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int N = P.N;
+    const double C = P.dim == 2 ? 8.0 : 10.0;
+    FOR_EACH_CHUNK(dB, CR_ALL, kWarpsPerBlock, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        const int ii = active ? i : ch.i0;
+        const int ti = S.type[ii];
+        const double xi = S.pos[ii], yi = S.pos[N + ii], zi = S.pos[2 * N + ii];
+        const double vxi = S.vel[ii], vyi = S.vel[N + ii], vzi = S.vel[2 * N + ii];
+        const double Pi = S.pres[ii], PAi = S.pA[ii];
+        const double gci[3] = {S.gc[ii], S.gc[N + ii], S.gc[2 * N + ii]};
+        const double mui = P.svisc[ti];
+        const double a = P.CofA[ti] * (P.CofK) * (P.CofK);
+        double sP[3][3] = {{0.0}}, sA[3][3] = {{0.0}}, sV[3][3] = {{0.0}}, sG[3][3] = {{0.0}};
+        traverse_stencil(
+            P, S.cell_start, key_cell, lane, active, 7u,
+            [&](int j, int slot) {
+                tl.x[slot] = S.pos[j];
+                tl.y[slot] = S.pos[N + j];
+                tl.z[slot] = S.pos[2 * N + j];
+                tl.vx[slot] = S.vel[j];
+                tl.vy[slot] = S.vel[N + j];
+                tl.vz[slot] = S.vel[2 * N + j];
+                tl.t[slot] = S.type[j];
+            },
+            [&](int j, int s) {
+                if (j == i) return;
+                const double q[3] = {rel1(tl.x[s], xi, P.W[0], P.hW[0]), rel1(tl.y[s], yi, P.W[1], P.hW[1]),
+                                     rel1(tl.z[s], zi, P.W[2], P.hW[2])};
+                const double r2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+                const int tj = tl.t[s];
+                if (P.RP * P.RP - r2 > 0) {
+                    const double r = sqrt(r2);
+                    const double dw = k_dw(r, P.Bp, P.RP);
+                    const double g[3] = {dw * q[0] / r, dw * q[1] / r, dw * q[2] / r};
+                    double f[3];
+                    for (int d = 0; d < 3; d++) f[d] = (Pi)*g[d] * P.V;
+                    for (int d = 0; d < 3; d++)
+                        for (int e = 0; e < 3; e++) sP[d][e] += 1.0 * f[d] * q[e] / P.V;
+                }
+                if (P.RA * P.RA - r2 > 0) {
+                    const double ratio = P.ratio[ti][tj];
+                    const double r = sqrt(r2);
+                    const double dw = ratio * k_dwa(r, P.Ba, P.RA);
+                    const double g[3] = {dw * q[0] / r, dw * q[1] / r, dw * q[2] / r};
+                    double f[3];
+                    for (int d = 0; d < 3; d++) f[d] = (PAi)*g[d] * P.V;
+                    for (int d = 0; d < 3; d++)
+                        for (int e = 0; e < 3; e++) sA[d][e] += 1.0 * f[d] * q[e] / P.V;
+                }
+                if (P.RV * P.RV - r2 > 0) {
+                    const double r = sqrt(r2);
+                    const double dw = -k_dw(r, P.Bv, P.RV);
+                    const double e_[3] = {q[0] / r, q[1] / r, q[2] / r};
+                    const double u[3] = {tl.vx[s] - vxi, tl.vy[s] - vyi, tl.vz[s] - vzi};
+                    const double muj = P.svisc[tj];
+                    const double muij = 2.0 * (mui * muj) / (mui + muj);
+                    double f[3];
+                    for (int d = 0; d < 3; d++)
+                        f[d] = C * muij * (u[0] * e_[0] + u[1] * e_[1] + u[2] * e_[2]) * e_[d] * dw / r * P.V;
+                    for (int d = 0; d < 3; d++)
+                        for (int e = 0; e < 3; e++) sV[d][e] += 0.5 * f[d] * q[e] / P.V;
+                }
+                if (P.RG * P.RG - r2 > 0) {
+                    const double ratio = P.ratio[ti][tj];
+                    const double r = sqrt(r2);
+                    const double w = ratio * k_w(r, P.Bg, P.RG);
+                    double f[3];
+                    for (int d = 0; d < 3; d++) f[d] = -a * (-gci[d]) * w / P.R2g * P.RG * (P.V / P.dx);
+                    for (int d = 0; d < 3; d++)
+                        for (int e = 0; e < 3; e++) sG[d][e] += 1.0 * f[d] * q[e] / P.V;
+                    const double dw = ratio * k_dw(r, P.Bg, P.RG);
+                    const double g[3] = {dw * q[0] / r, dw * q[1] / r, dw * q[2] / r};
+                    double gr = 0.0;
+                    for (int d = 0; d < 3; d++) gr += (-gci[d]) * q[d];
+                    for (int d = 0; d < 3; d++) f[d] = -a * (gr)*g[d] / P.R2g * P.RG * (P.V / P.dx);
+                    for (int d = 0; d < 3; d++)
+                        for (int e = 0; e < 3; e++) sG[d][e] += 1.0 * f[d] * q[e] / P.V;
+                }
+            });
+        if (!active) continue;
+        double vs[3][3];
+        for (int d = 0; d < 3; d++)
+            for (int e = 0; e < 3; e++) vs[d][e] = (((0.0 + sP[d][e]) + sA[d][e]) + sV[d][e]) + sG[d][e];
+        vir[i] = P.dim == 2 ? -1.0 / 2.0 * (vs[0][0] + vs[1][1]) : -1.0 / 3.0 * (vs[0][0] + vs[1][1] + vs[2][2]);
+    }
+}
+
+void launch_virial(const DevParams &P, const DevState &S, const int *dB, double *vir, cudaStream_t st)
+{
+    static const int g = persistent_grid((const void *)k_virial, kBlock);
+    k_virial<<<g, kBlock, 0, st>>>(P, S, dB, vir);
+}
+
 void launch_pass_b(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
 {
     static const int g = persistent_grid((const void *)k_pass_b, kBlock);

@@ -31,6 +31,7 @@ void launch_decide(const DevParams &P, const unsigned long long *maxshift, int *
 void launch_drift(const DevParams &P, const DevState &S, const WallMotion &Wm, unsigned long long *maxshift, int sms,
                   cudaStream_t st);
 void launch_pass_a(const DevParams &P, const DevState &S, const int *dB, int range, int init_only, cudaStream_t st);
+void launch_virial(const DevParams &P, const DevState &S, const int *dB, double *vir, cudaStream_t st);
 void launch_pass_b(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 void launch_fluid_accel(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 void launch_dem_force(const DevParams &P, const DevState &S, const int *dB, int range, int forces, cudaStream_t st,

@@ -170,3 +170,79 @@ extern "C" int dmph_write_prof_file(const char *path, const dmph_params *p, int 
     std::fclose(fp);
     return bad ? DMPH_EIO : DMPH_OK;
 }
+
+// The VTK output of writeVtkFile (source/DEM-MPH.cpp:879-1005): legacy ASCII
+// unstructured grid of vertices with the reference's point data, in its order
+// and with its number formats (positions and velocities rounded to float).
+extern "C" int dmph_write_vtk_file(const char *path, int n, const int *type, const double *x3, const double *v3,
+                                   const double *kn, const double *cn, const double *kt, const double *ct,
+                                   const int *neighbor_count, const double *alpha, const double *drag,
+                                   const double *vol_strain, const double *virial_pressure)
+{
+    if (!path || n < 0) return DMPH_EINVAL;
+    if (n > 0 && (!type || !x3 || !v3 || !kn || !cn || !kt || !ct || !neighbor_count || !alpha || !drag ||
+                  !vol_strain || !virial_pressure))
+        return DMPH_EINVAL;
+    FILE *fp = std::fopen(path, "w");
+    if (!fp) {
+        g_io_msg = std::string("cannot write ") + path;
+        return DMPH_EIO;
+    }
+    std::fprintf(fp, "# vtk DataFile Version 2.0\n");
+    std::fprintf(fp, "Unstructured Grid Example\n");
+    std::fprintf(fp, "ASCII\n");
+    std::fprintf(fp, "DATASET UNSTRUCTURED_GRID\n");
+    std::fprintf(fp, "POINTS %d float\n", n);
+    for (int i = 0; i < n; ++i)
+        std::fprintf(fp, "%e %e %e\n", (float)x3[3 * i], (float)x3[3 * i + 1], (float)x3[3 * i + 2]);
+    std::fprintf(fp, "CELLS %d %d\n", n, 2 * n);
+    for (int i = 0; i < n; ++i) std::fprintf(fp, "1 %d ", i);
+    std::fprintf(fp, "\n");
+    std::fprintf(fp, "CELL_TYPES %d\n", n);
+    for (int i = 0; i < n; ++i) std::fprintf(fp, "1 ");
+    std::fprintf(fp, "\n");
+    std::fprintf(fp, "\n");
+    std::fprintf(fp, "POINT_DATA %d\n", n);
+    std::fprintf(fp, "SCALARS label float 1\n");
+    std::fprintf(fp, "LOOKUP_TABLE default\n");
+    for (int i = 0; i < n; ++i) std::fprintf(fp, "%d\n", type[i]);
+    std::fprintf(fp, "\n");
+    const struct {
+        const char *name;
+        const double *a;
+    } dem[4] = {{"NormalSpringConstant", kn},
+                {"NormalViscousDampingConstant", cn},
+                {"TangentialSpringConstant", kt},
+                {"TangentialViscousDampingConstant", ct}};
+    for (const auto &f : dem) {
+        std::fprintf(fp, "SCALARS %s float 1\n", f.name);
+        std::fprintf(fp, "LOOKUP_TABLE default\n");
+        for (int i = 0; i < n; ++i) std::fprintf(fp, "%e\n", f.a[i]);
+    }
+    std::fprintf(fp, "SCALARS neighbor float 1\n");
+    std::fprintf(fp, "LOOKUP_TABLE default\n");
+    for (int i = 0; i < n; ++i) std::fprintf(fp, "%d\n", neighbor_count[i]);
+    std::fprintf(fp, "SCALARS volumef float 1\n");
+    std::fprintf(fp, "LOOKUP_TABLE default\n");
+    for (int i = 0; i < n; ++i) std::fprintf(fp, "%e\n", alpha[i]);
+    std::fprintf(fp, "SCALARS drag float 1\n");
+    std::fprintf(fp, "LOOKUP_TABLE default\n");
+    for (int i = 0; i < n; ++i) std::fprintf(fp, "%e\n", drag[i]);
+    std::fprintf(fp, "\n");
+    std::fprintf(fp, "VECTORS velocity float\n");
+    for (int i = 0; i < n; ++i)
+        std::fprintf(fp, "%e %e %e\n", (float)v3[3 * i], (float)v3[3 * i + 1], (float)v3[3 * i + 2]);
+    std::fprintf(fp, "\n");
+    std::fprintf(fp, "SCALARS VolStrainP float 1\n");
+    std::fprintf(fp, "LOOKUP_TABLE default\n");
+    for (int i = 0; i < n; ++i) std::fprintf(fp, "%e\n", (float)vol_strain[i]);
+    std::fprintf(fp, "\n");
+    std::fprintf(fp, "SCALARS VirialPressureAtParticle float 1\n");
+    std::fprintf(fp, "LOOKUP_TABLE default\n");
+    for (int i = 0; i < n; ++i) std::fprintf(fp, "%e\n", (float)virial_pressure[i]);
+    std::fprintf(fp, "\n");
+    std::fflush(fp);
+    const int bad = std::ferror(fp);
+    std::fclose(fp);
+    return bad ? DMPH_EIO : DMPH_OK;
+}

@@ -6,11 +6,13 @@
 // main (source/DEM-MPH.cpp:350-617): it reads dem.data and the .grid file,
 // writes a .prof (positions and velocities in the solver's sorted order) at
 // the top of every step whose time reaches the next OutputInterval boundary
-// and advances until EndTime.  All computation happens in libdmph.so through
-// the C ABI of include/dmph.h.  The reference is compiled 2D by default
-// (source/DEM-MPH.cpp:39); --dim 3 selects its 3D branches.  The reference
-// also writes a sixth argument-free VTK output; this build's VTK writer is not
-// implemented, and a non-default VTK pattern is reported and ignored.
+// and advances until EndTime; after initialisation it writes output.vtk, and
+// at the end of every step whose time reaches the next VtkOutputInterval
+// boundary it computes the virial pressure and writes a VTK file named by the
+// VTK pattern, as the reference does (:426, :566-575).  All computation
+// happens in libdmph.so through the C ABI of include/dmph.h.  The reference is
+// compiled 2D by default (source/DEM-MPH.cpp:39); --dim 3 selects its 3D
+// branches.
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -84,7 +86,9 @@ int main(int argc, char **argv)
     if (rc) return log_printf("cannot read %s: %s\n", gridf.c_str(), dmph_io_last_message()), 1;
     p.dim = dim;
     p.precision = fp32 ? DMPH_PRECISION_FP32_SPLIT : DMPH_PRECISION_FP64;
-    p.flags |= DMPH_FLAG_ALL_NEIGHBOR_COUNTS;
+    // the VTK output carries every particle's NeighborCount and the DEM
+    // constants the reference also evaluates for wall particles
+    p.flags |= DMPH_FLAG_ALL_NEIGHBOR_COUNTS | DMPH_FLAG_WALL_DEM_COEFFS;
     if (cudaSetDevice(gpu) != cudaSuccess) return log_printf("cannot select GPU %d\n", gpu), 1;
     {
         time_t t = time(NULL);
@@ -100,9 +104,33 @@ int main(int argc, char **argv)
                info.cell_count[2], info.total_cell_count);
     log_printf("CellWidth[DIM]: %e %e %e\n", info.cell_width[0], info.cell_width[1], info.cell_width[2]);
     log_printf("Using GPU %d (%s)\n", gpu, dmph_version());
-    if (vtkf != "sample%03d.vtk") log_printf("VTK output (%s) is not produced by this build\n", vtkf.c_str());
 
-    double Time = p.time, OutputNext = 0.0;
+    // VTK output: the fields of writeVtkFile from the current state
+    std::vector<double> kn(n), cn(n), kt(n), ct(n), alpha(n), drag(n), vsp(n), vir(n, 0.0);
+    std::vector<int> ncount(n);
+    auto write_vtk = [&](const char *fn, bool with_virial) -> int {
+        int r = dmph_get_state(ctx, type.data(), x.data(), v.data(), nullptr);
+        const struct {
+            int id;
+            void *out;
+        } fields[] = {{DMPH_FIELD_NORMAL_SPRING, kn.data()},       {DMPH_FIELD_NORMAL_DAMPING, cn.data()},
+                      {DMPH_FIELD_TANGENTIAL_SPRING, kt.data()},   {DMPH_FIELD_TANGENTIAL_DAMPING, ct.data()},
+                      {DMPH_FIELD_NEIGHBOR_COUNT, ncount.data()}, {DMPH_FIELD_ALPHA, alpha.data()},
+                      {DMPH_FIELD_DRAG_C, drag.data()},           {DMPH_FIELD_VOL_STRAIN_P, vsp.data()}};
+        for (const auto &f : fields)
+            if (!r) r = dmph_get_field(ctx, f.id, f.out);
+        if (!r && with_virial) r = dmph_get_field(ctx, DMPH_FIELD_VIRIAL_PRESSURE, vir.data());
+        if (r) return fail("reading the VTK fields", r, ctx);
+        r = dmph_write_vtk_file(fn, n, type.data(), x.data(), v.data(), kn.data(), cn.data(), kt.data(), ct.data(),
+                                ncount.data(), alpha.data(), drag.data(), vsp.data(), vir.data());
+        if (r) return log_printf("cannot write %s\n", fn), 1;
+        return 0;
+    };
+    // the reference writes this file after initialisation (:426); its virial
+    // pressure has not been computed yet and is zero
+    if (write_vtk("output.vtk", false)) return 1;
+
+    double Time = p.time, OutputNext = 0.0, VtkOutputNext = 0.0;
     const double Dt = p.dt;
     int iStep = (int)(Time / Dt);
     {
@@ -125,6 +153,13 @@ int main(int argc, char **argv)
         }
         rc = dmph_step(ctx, 1);
         if (rc) return fail("dmph_step", rc, ctx);
+        if (Time + 1.0e-5 * Dt >= VtkOutputNext) {
+            char fn[1024];
+            std::snprintf(fn, sizeof(fn), vtkf.c_str(), iStep);
+            if (write_vtk(fn, true)) return 1;
+            log_printf("@ Vtk Output Time : %e\n", Time);
+            VtkOutputNext += p.vtk_output_interval;
+        }
         Time += Dt;
         iStep++;
     }

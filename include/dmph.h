@@ -129,6 +129,15 @@ int dmph_read_grid_file(const char *path, dmph_params *p, int *n, int *type, dou
 int dmph_write_prof_file(const char *path, const dmph_params *p, int n, const int *type, const double *x3,
                          const double *v3);
 
+/* Write a VTK file (writeVtkFile, source/DEM-MPH.cpp:879-1005): legacy ASCII
+ * unstructured grid, point data label, the four DEM constants, neighbor,
+ * volumef, drag, velocity, VolStrainP, VirialPressureAtParticle in the
+ * reference's order and formats; arrays in the solver's current order. */
+int dmph_write_vtk_file(const char *path, int n, const int *type, const double *x3, const double *v3,
+                        const double *kn, const double *cn, const double *kt, const double *ct,
+                        const int *neighbor_count, const double *alpha, const double *drag,
+                        const double *vol_strain, const double *virial_pressure);
+
 /* Last informational message of the I/O layer (invalid data-file lines). */
 const char *dmph_io_last_message(void);
 
@@ -180,7 +189,9 @@ enum dmph_field {
     DMPH_FIELD_SOLID_NEIGHBOR_COUNT = 14, /* int32[n]  SolidNeighborCount :94 (rebuild time) */
     DMPH_FIELD_CELL_INDEX = 15,         /* int32[n]    sorted cell key CellIndex :121 */
     DMPH_FIELD_MASS = 16,               /* double[n]   Mass :84 */
-    DMPH_FIELD_COUNT_ = 17
+    DMPH_FIELD_VIRIAL_PRESSURE = 17,    /* double[n]   VirialPressureAtParticle :147, computed on request
+                                           from the current state (calculateVirialStressAtParticle :2904) */
+    DMPH_FIELD_COUNT_ = 18
 };
 int dmph_get_field(dmph_ctx *ctx, int field_id, void *out);
 

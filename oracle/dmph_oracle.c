@@ -43,6 +43,7 @@ struct dmph_oracle {
     double *densA, *gc, *pA, *vsp, *div, *P;
     double *kn, *cn, *kt, *ct, *alpha, *dragC;
     double *fsc; /* per particle: sum of |pair force| terms of the step (test scale, not a reference array) */
+    double *vir; /* VirialPressureAtParticle, computed when requested */
     int *nc, *fnc, *snc;
     long *nptr;
     int *nind;
@@ -1140,6 +1141,7 @@ dmph_oracle *dmph_oracle_create(const dmph_params *p, int n, const int *type, co
     o->alpha = xcalloc(N, sizeof(double));
     o->dragC = xcalloc(N, sizeof(double));
     o->fsc = xcalloc(N, sizeof(double));
+    o->vir = xcalloc(N, sizeof(double));
     o->nc = xcalloc(N, sizeof(int));
     o->fnc = xcalloc(N, sizeof(int));
     o->snc = xcalloc(N, sizeof(int));
@@ -1213,6 +1215,7 @@ static const field_t FIELDS[] = {
     {"alpha", FO(alpha), 1},
     {"DragC", FO(dragC), 1},
     {"ForceScale", FO(fsc), 1},
+    {"VirialPressure", FO(vir), 1},
     {"NeighborCount", FO(nc), 0},
     {"FluidNeighborCount", FO(fnc), 0},
     {"SolidNeighborCount", FO(snc), 0},
@@ -1244,6 +1247,108 @@ long dmph_oracle_size(dmph_oracle *o, const char *name)
     return -1;
 }
 
+/* calculateVirialStressAtParticle :2904-3149 and the virial pressure: four
+ * passes over the neighbour lists (pressure P, attractive pressure A,
+ * viscosity V, diffuse interface G), each adding its per-particle stress
+ * matrix in turn; pressure = -trace / dim (2D: the x and y entries) */
+static void virial(dmph_oracle *o)
+{
+    const double C = o->dim == 2 ? 8.0 : 10.0;
+#pragma omp parallel for
+    for (int i = 0; i < o->N; i++) {
+        double vs[3][3], sP[3][3] = {{0.0}}, sA[3][3] = {{0.0}}, sV[3][3] = {{0.0}}, sG[3][3] = {{0.0}};
+        const int ti = o->prop[i];
+        const double *xi = o->x + 3 * i, *vi = o->v + 3 * i;
+        FOR_NEIGHBORS(o, i, j)
+        {
+            if (i == j) continue;
+            double q[3];
+            rel(o, xi, o->x + 3 * j, q);
+            const double r2 = sq3(q);
+            if (o->RP * o->RP - r2 > 0) {
+                const double r = sqrt(r2);
+                const double dw = k_dw(r, o->Bp, o->RP);
+                const double g[3] = {dw * q[0] / r, dw * q[1] / r, dw * q[2] / r};
+                double f[3];
+                for (int d = 0; d < 3; d++) f[d] = (o->P[i]) * g[d] * o->V;
+                for (int d = 0; d < 3; d++)
+                    for (int e = 0; e < 3; e++) sP[d][e] += 1.0 * f[d] * q[e] / o->V;
+            }
+        }
+        FOR_NEIGHBORS(o, i, j)
+        {
+            if (i == j) continue;
+            double q[3];
+            rel(o, xi, o->x + 3 * j, q);
+            const double r2 = sq3(q);
+            if (o->RA * o->RA - r2 > 0) {
+                const double ratio = o->p.interaction_ratio[ti][o->prop[j]];
+                const double r = sqrt(r2);
+                const double dw = ratio * k_dwa(r, o->Ba, o->RA);
+                const double g[3] = {dw * q[0] / r, dw * q[1] / r, dw * q[2] / r};
+                double f[3];
+                for (int d = 0; d < 3; d++) f[d] = (o->pA[i]) * g[d] * o->V;
+                for (int d = 0; d < 3; d++)
+                    for (int e = 0; e < 3; e++) sA[d][e] += 1.0 * f[d] * q[e] / o->V;
+            }
+        }
+        FOR_NEIGHBORS(o, i, j)
+        {
+            if (i == j) continue;
+            double q[3];
+            rel(o, xi, o->x + 3 * j, q);
+            const double r2 = sq3(q);
+            if (o->RV * o->RV - r2 > 0) {
+                const double r = sqrt(r2);
+                const double dw = -k_dw(r, o->Bv, o->RV);
+                const double e_[3] = {q[0] / r, q[1] / r, q[2] / r};
+                const double *vj = o->v + 3 * j;
+                const double u[3] = {vj[0] - vi[0], vj[1] - vi[1], vj[2] - vi[2]};
+                const double muij = 2.0 * (o->mu[i] * o->mu[j]) / (o->mu[i] + o->mu[j]);
+                double f[3];
+                for (int d = 0; d < 3; d++)
+                    f[d] = C * muij * (u[0] * e_[0] + u[1] * e_[1] + u[2] * e_[2]) * e_[d] * dw / r * o->V;
+                for (int d = 0; d < 3; d++)
+                    for (int e = 0; e < 3; e++) sV[d][e] += 0.5 * f[d] * q[e] / o->V;
+            }
+        }
+        FOR_NEIGHBORS(o, i, j)
+        {
+            if (i == j) continue;
+            double q[3];
+            rel(o, xi, o->x + 3 * j, q);
+            const double r2 = sq3(q);
+            const double *gc = o->gc + 3 * i;
+            if (o->RG * o->RG - r2 > 0) {
+                const double a = o->CofA[ti] * (o->CofK) * (o->CofK);
+                const double ratio = o->p.interaction_ratio[ti][o->prop[j]];
+                const double r = sqrt(r2);
+                const double w = ratio * k_w(r, o->Bg, o->RG);
+                double f[3];
+                for (int d = 0; d < 3; d++) f[d] = -a * (-gc[d]) * w / o->R2g * o->RG * (o->V / o->dx);
+                for (int d = 0; d < 3; d++)
+                    for (int e = 0; e < 3; e++) sG[d][e] += 1.0 * f[d] * q[e] / o->V;
+            }
+            if (o->RG * o->RG - r2 > 0.0) {
+                const double a = o->CofA[ti] * (o->CofK) * (o->CofK);
+                const double ratio = o->p.interaction_ratio[ti][o->prop[j]];
+                const double r = sqrt(r2);
+                const double dw = ratio * k_dw(r, o->Bg, o->RG);
+                const double g[3] = {dw * q[0] / r, dw * q[1] / r, dw * q[2] / r};
+                double gr = 0.0;
+                for (int d = 0; d < 3; d++) gr += (-gc[d]) * q[d];
+                double f[3];
+                for (int d = 0; d < 3; d++) f[d] = -a * (gr)*g[d] / o->R2g * o->RG * (o->V / o->dx);
+                for (int d = 0; d < 3; d++)
+                    for (int e = 0; e < 3; e++) sG[d][e] += 1.0 * f[d] * q[e] / o->V;
+            }
+        }
+        for (int d = 0; d < 3; d++)
+            for (int e = 0; e < 3; e++) vs[d][e] = (((0.0 + sP[d][e]) + sA[d][e]) + sV[d][e]) + sG[d][e];
+        o->vir[i] = o->dim == 2 ? -1.0 / 2.0 * (vs[0][0] + vs[1][1]) : -1.0 / 3.0 * (vs[0][0] + vs[1][1] + vs[2][2]);
+    }
+}
+
 int dmph_oracle_get(dmph_oracle *o, const char *name, void *out)
 {
     if (!o || !name || !out) return DMPH_EINVAL;
@@ -1255,6 +1360,7 @@ int dmph_oracle_get(dmph_oracle *o, const char *name, void *out)
         memcpy(out, o->nind, sizeof(int) * o->nindCount);
         return 0;
     }
+    if (!strcmp(name, "VirialPressure")) virial(o);
     for (size_t k = 0; k < sizeof(FIELDS) / sizeof(FIELDS[0]); k++)
         if (!strcmp(FIELDS[k].name, name)) {
             const void *src = *(void *const *)((const char *)o + FIELDS[k].off);
@@ -1458,7 +1564,7 @@ void dmph_oracle_destroy(dmph_oracle *o)
                      (void **)&o->lambda, (void **)&o->mu,   (void **)&o->densA,  (void **)&o->gc,
                      (void **)&o->pA,    (void **)&o->vsp,   (void **)&o->div,    (void **)&o->P,
                      (void **)&o->kn,    (void **)&o->cn,    (void **)&o->kt,     (void **)&o->ct,
-                     (void **)&o->alpha, (void **)&o->dragC, (void **)&o->fsc,    (void **)&o->nc,
+                     (void **)&o->alpha, (void **)&o->dragC, (void **)&o->fsc, (void **)&o->vir,    (void **)&o->nc,
                      (void **)&o->fnc,
                      (void **)&o->snc,   (void **)&o->nptr,  (void **)&o->nind,   (void **)&o->key,
                      (void **)&o->payload, (void **)&o->cfb, (void **)&o->cfe,    (void **)&o->csb,

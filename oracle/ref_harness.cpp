@@ -110,6 +110,10 @@ static void harness_dump(const std::string &dir)
     dump_raw(dir, "TangentialViscousDampingConstant.f64", TangentialViscousDampingConstant, N * 8);
     dump_raw(dir, "alpha.f64", alpha, N * 8);
     dump_raw(dir, "DragC.f64", DragC, N * 8);
+    // the output-cadence virial stress of the state being dumped
+    // (calculateVirialStressAtParticle writes only the two virial arrays)
+    calculateVirialStressAtParticle();
+    dump_raw(dir, "VirialPressure.f64", VirialPressureAtParticle, N * 8);
     dump_raw(dir, "NeighborCount.i32", NeighborCount, N * 4);
     dump_raw(dir, "FluidNeighborCount.i32", FluidNeighborCount, N * 4);
     dump_raw(dir, "SolidNeighborCount.i32", SolidNeighborCount, N * 4);

@@ -1,0 +1,72 @@
+"""The drop-in executable against the reference executable built from its own
+sources (oracle/_ref/DEM-MPH-2d, the unmodified 2D solver): same command
+line, same input files, a short SYSU-2mm run with .prof and VTK output every
+few steps; every output file must be byte-identical (FP64 build).  Also the
+virial pressure of the VTK output against the oracle."""
+import filecmp
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN, load_scene
+from oracle.oracle import Oracle, REF_DIR
+from dem_mph_b200 import files, generator, solver
+from dem_mph_b200.abi import PRECISION_FP32_SPLIT
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "dem_mph_b200", "dem_mph")
+REF2D = os.path.join(REF_DIR, "DEM-MPH-2d")
+
+
+@pytest.mark.parametrize("name", ["sysu2mm", "small3d_st"])
+def test_virial_pressure_matches_oracle(name):
+    p, typ, x, v = load_scene(name)
+    g = solver.Solver(p, typ, x, v)
+    o = Oracle(p, typ, x, v)
+    for steps in (1, 30):
+        g.step(steps)
+        o.step(steps)
+        a, b = g.field("VirialPressure"), o.get("VirialPressure")
+        assert np.array_equal(a, b) or np.abs(a - b).max() <= 1e-12 * np.abs(b).max(), name
+    q = p.copy()
+    q.precision = PRECISION_FP32_SPLIT
+    h = solver.Solver(q, typ, x, v)
+    h.step(1)
+    o2 = Oracle(p, typ, x, v)
+    o2.step(1)
+    a, b = h.field("VirialPressure"), o2.get("VirialPressure")
+    # FP32 pressures carry the strain floor of the split precision (K * 1e-7)
+    assert np.abs(a - b).max() <= 1e-3 * np.abs(b).max() + 1e-6 * p.bulk_modulus[1]
+    g.close()
+    h.close()
+
+
+@pytest.mark.skipif(not os.path.exists(REF2D), reason="reference executable not built")
+def test_drop_in_outputs_identical_to_reference():
+    with tempfile.TemporaryDirectory() as tmp:
+        data = os.path.join(tmp, "dem.data")
+        grid = os.path.join(tmp, "DEM.grid")
+        p = files.read_data_file(os.path.join(GOLDEN, "sysu2mm", "dem.data"))
+        p.end_time = 24 * p.dt
+        p.output_interval = 8 * p.dt
+        p.vtk_output_interval = 12 * p.dt
+        files.write_data_file(data, p)
+        generator.boid_to_grid(os.path.join(GOLDEN, "sysu2mm", "DEM.boid"), grid)
+        outs = {}
+        for tag, cmd in (("ref", [REF2D]), ("ours", [EXE, "--dim", "2"])):
+            d = os.path.join(tmp, tag)
+            os.makedirs(d)
+            r = subprocess.run(cmd + [data, grid, "p%03d.prof", "v%03d.vtk", "run.log"], cwd=d,
+                               capture_output=True, text=True, timeout=600)
+            assert r.returncode == 0, (tag, r.stderr[-2000:])
+            outs[tag] = sorted(f for f in os.listdir(d) if f.endswith((".prof", ".vtk")))
+        assert outs["ref"] == outs["ours"] and len(outs["ref"]) >= 6, outs
+        assert "output.vtk" in outs["ref"]
+        for f in outs["ref"]:
+            a, b = os.path.join(tmp, "ref", f), os.path.join(tmp, "ours", f)
+            assert filecmp.cmp(a, b, shallow=False), f

@@ -8,19 +8,23 @@ import numpy as np
 import pytest
 
 from dem_mph_b200 import files, scenes
+from helpers import small3d_st_params
 from oracle.oracle import Oracle, read_ref_dump, REF_DIR
 
 EXE3 = os.path.join(REF_DIR, "ref_dump3d")
 
 
 @pytest.mark.skipif(not os.path.exists(EXE3), reason="oracle/_ref not built (reference tree absent)")
-@pytest.mark.parametrize("seed,yaw", [(11, False), (12, True)])
-def test_oracle_bit_exact_vs_reference(seed, yaw):
+@pytest.mark.parametrize("seed,yaw,st", [(11, False, False), (12, True, False), (13, False, True)])
+def test_oracle_bit_exact_vs_reference(seed, yaw, st):
+    """every array the harness dumps, the virial pressure of the output
+    cadence included; st: surface tension with non-zero interaction ratios"""
     s = scenes.small(seed=seed, yaw=yaw)
+    params = small3d_st_params(s.params) if st else s.params
     with tempfile.TemporaryDirectory() as tmp:
         data, grid = os.path.join(tmp, "d.data"), os.path.join(tmp, "s.grid")
-        files.write_data_file(data, s.params)
-        files.write_grid(grid, s.params, s.type, s.x, s.v)
+        files.write_data_file(data, params)
+        files.write_grid(grid, params, s.type, s.x, s.v)
         subprocess.run([EXE3, data, grid, os.path.join(tmp, "out"), "60", "60"], check=True, capture_output=True)
         ref = read_ref_dump(os.path.join(tmp, "out", "step60"))
         p = files.read_data_file(data)
