@@ -13,7 +13,7 @@ import pytest
 
 from helpers import GOLDEN, load_scene
 from oracle.oracle import Oracle, REF_DIR
-from dem_mph_b200 import files, generator, solver
+from dem_mph_b200 import files, generator, scenes, solver
 from dem_mph_b200.abi import PRECISION_FP32_SPLIT
 
 pytestmark = pytest.mark.gpu
@@ -46,19 +46,34 @@ def test_virial_pressure_matches_oracle(name):
     h.close()
 
 
-@pytest.mark.skipif(not os.path.exists(REF2D), reason="reference executable not built")
-def test_drop_in_outputs_identical_to_reference():
-    with tempfile.TemporaryDirectory() as tmp:
-        data = os.path.join(tmp, "dem.data")
-        grid = os.path.join(tmp, "DEM.grid")
+REF3D = os.path.join(REF_DIR, "DEM-MPH-3d")
+
+
+def write_inputs(tmp, case):
+    data = os.path.join(tmp, "dem.data")
+    grid = os.path.join(tmp, "DEM.grid")
+    if case == "sysu2mm_2d":
         p = files.read_data_file(os.path.join(GOLDEN, "sysu2mm", "dem.data"))
-        p.end_time = 24 * p.dt
-        p.output_interval = 8 * p.dt
-        p.vtk_output_interval = 12 * p.dt
-        files.write_data_file(data, p)
         generator.boid_to_grid(os.path.join(GOLDEN, "sysu2mm", "DEM.boid"), grid)
+    else:
+        s = scenes.small()
+        p = s.params.copy()
+        files.write_grid(grid, p, s.type, s.x, s.v)
+    p.end_time = 24 * p.dt
+    p.output_interval = 8 * p.dt
+    p.vtk_output_interval = 12 * p.dt
+    files.write_data_file(data, p)
+    return data, grid
+
+
+@pytest.mark.parametrize("case,ref,dim", [("sysu2mm_2d", REF2D, "2"), ("dambreak_3d", REF3D, "3")])
+def test_drop_in_outputs_identical_to_reference(case, ref, dim):
+    if not os.path.exists(ref):
+        pytest.skip("reference executable not built")
+    with tempfile.TemporaryDirectory() as tmp:
+        data, grid = write_inputs(tmp, case)
         outs = {}
-        for tag, cmd in (("ref", [REF2D]), ("ours", [EXE, "--dim", "2"])):
+        for tag, cmd in (("ref", [ref]), ("ours", [EXE, "--dim", dim])):
             d = os.path.join(tmp, tag)
             os.makedirs(d)
             r = subprocess.run(cmd + [data, grid, "p%03d.prof", "v%03d.vtk", "run.log"], cwd=d,
