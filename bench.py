@@ -46,6 +46,18 @@ def load_peaks():
         return PEAKS_FALLBACK, "fallback"
 
 
+def max_over_ranks(x, world, device):
+    """the largest value over the ranks (timings are taken as the slowest
+    rank's); a plain float with one rank"""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_scene(workload, rank):
     from dem_mph_b200 import scenes
     seed = 1234 + rank
@@ -215,10 +227,7 @@ def main():
     inf_t = g.info()
     launches = int(inf_t.kernel_launches - l0)
     rebuilds_timed = int(inf_t.rebuilds)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(ms, world, "cuda")
     inf = g.info()
     value = n * world * args.steps / (ms_max / 1e3)
 
@@ -269,10 +278,7 @@ def main():
         g.state(out=host)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e = {"value": n * world * e2e_steps / float(e2e_t.item()), "unit": "particle-steps/s",
+    e2e = {"value": n * world * e2e_steps / max_over_ranks(e2e_s, world, "cuda"), "unit": "particle-steps/s",
            "h2d_bytes_per_step": int(n * 48), "d2h_bytes_per_step": int(n * 48 + n * 8),
            "steps": e2e_steps}
     g.close()
@@ -451,10 +457,7 @@ def run_ensemble(args, rank, world):
         torch.cuda.synchronize()
     barrier()
     launches = ens.info()["kernel_launches"] + sum(g.info().kernel_launches for g in sv) - l0
-    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(ms, world, "cuda")
     value = n * world * args.steps / (ms_max / 1e3)
     peaks, peak_src = load_peaks()
     bpp = algorithmic_bytes("fp32")
@@ -479,9 +482,7 @@ def run_ensemble(args, rank, world):
             g.state(out=h)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_max = max_over_ranks(e2e_s, world, "cuda")
     dts = [s.params.dt for s in sc]
     out = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
@@ -500,7 +501,7 @@ def run_ensemble(args, rank, world):
                      "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                      "traffic": None, "peak_source": peak_src},
         "cpu_baseline": None,
-        "e2e": {"value": n * world * e2e_steps / float(e2e_t.item()), "unit": "particle-steps/s",
+        "e2e": {"value": n * world * e2e_steps / e2e_max, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": int(n * 48), "d2h_bytes_per_step": int(n * 56), "steps": e2e_steps},
         "gpu_launches": int(launches),
     }
