@@ -168,6 +168,8 @@ def main():
     ap.add_argument("--surrogate", action="store_true",
                     help="plain vs surrogate sim-s/hour and surge-front / debris-centroid error (config1 by default)")
     ap.add_argument("--substeps", type=int, default=8, help="surrogate K")
+    ap.add_argument("--sg-tolerance", type=float, default=0.02,
+                    help="surrogate judge tolerance on the velocity-increment error")
     ap.add_argument("--no-bodies", action="store_true",
                     help="move debris particles individually (reference DEM) instead of as rigid bodies")
     args = ap.parse_args()
@@ -370,7 +372,8 @@ def run_surrogate(args, rank, world):
     dt = scene.params.dt
 
     b = make()
-    b.enable_surrogate(substeps=K, check_interval=50, tolerance=0.02, fallback_blocks=20, train_iters_per_block=20)
+    b.enable_surrogate(substeps=K, check_interval=50, tolerance=args.sg_tolerance, fallback_blocks=20,
+                       train_iters_per_block=20)
     settle = max(args.settle, 200)
     b.step(settle)
     nb_collect = 480 // K
@@ -402,7 +405,7 @@ def run_surrogate(args, rank, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 MLP + f32/f64 solver",
         "data": "synthetic (seeded dam break with debris, dem_mph_b200.scenes)",
         "config": {"workload": scene.name, "n_particles": scene.n, "substeps_K": K, "check_interval": 50,
-                   "tolerance": 0.02, "settle_steps": settle, "collect_steps": nb_collect * K,
+                   "tolerance": args.sg_tolerance, "settle_steps": settle, "collect_steps": nb_collect * K,
                    "surrogate_blocks": nblocks, "dt": dt},
         "plain_sim_s_per_hour": plain_rate, "speedup_vs_plain": sg_rate / plain_rate,
         "front_error_rel_travel": front_err, "front_plain_m": fa, "front_surrogate_m": fb, "front_start_m": f0,

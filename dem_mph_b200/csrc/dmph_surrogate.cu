@@ -21,10 +21,11 @@
 // plain solver runs K steps, and the increments (matched by original id
 // across rebuilds) become the targets of a sampled subset, appended to a
 // ring-buffer pool.  Every `check_interval` surrogate calls one block runs on
-// the plain solver instead, as the judge: the network's prediction for that
-// block is compared with what the solver did, and above `tolerance` the
-// driver falls back to the plain solver for `fallback_blocks` blocks, during
-// which it keeps collecting samples and training.
+// the plain solver instead, as the judge: the network's prediction of that
+// block's velocity increments is compared with what the solver did (relative
+// L2, fast particles weighted up), and above `tolerance` the driver falls back
+// to the plain solver for `fallback_blocks` blocks, during which it keeps
+// collecting samples and training.
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -948,7 +949,9 @@ extern "C" int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks)
             s->st.judged++;
             s->st.last_error = ex;
             s->st.last_error_v = ev;
-            if (!rc && !(ex <= s->prm.tolerance)) {
+            // the velocity increments carry the dynamics; the displacements are
+            // mostly the known drift K dt v0 and would hide their error
+            if (!rc && !(ev <= s->prm.tolerance)) {
                 s->st.fallbacks++;
                 s->fallback_left = s->prm.fallback_blocks;
             }

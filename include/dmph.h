@@ -313,8 +313,8 @@ int dmph_ensemble_destroy(dmph_ensemble *e);
  * increments) of a sampled subset of particles into a pool.
  * dmph_surrogate_advance(ctx, n) advances n blocks of K steps: surrogate
  * calls, except that every check_interval calls one block runs on the plain
- * solver as the judge; if the relative L2 error of the predicted
- * displacements of that block (each particle weighted by 1 + 20 |v0|^2 / vs^2,
+ * solver as the judge; if the relative L2 error of the predicted velocity
+ * increments of that block (each particle weighted by 1 + 20 |v0|^2 / vs^2,
  * vs = c0 / 10, so that the fast particles of the surge front count) exceeds
  * `tolerance`, the next fallback_blocks
  * blocks run plain (collecting and training with train_iters_per_block Adam
@@ -323,7 +323,7 @@ int dmph_ensemble_destroy(dmph_ensemble *e);
 typedef struct dmph_surrogate_params {
     int substeps;              /* K (8) */
     int check_interval;        /* surrogate calls between two judged blocks (50) */
-    double tolerance;          /* judged displacement error that triggers the fallback (0.02) */
+    double tolerance;          /* judged velocity-increment error that triggers the fallback (0.02) */
     int fallback_blocks;       /* plain blocks after a fallback (50) */
     int train_iters_per_block; /* Adam steps per plain block during a fallback (4) */
     int batch;                 /* training batch, a multiple of 8192 (65536) */
@@ -343,7 +343,7 @@ typedef struct dmph_surrogate_stats {
     int64_t pool_rows;    /* samples currently in the pool */
     int in_fallback;      /* 1 while plain blocks of a fallback remain */
     double last_error;    /* last judged relative L2 error of the displacements */
-    double last_error_v;  /* same for the velocity increments */
+    double last_error_v;  /* same for the velocity increments (the fallback criterion) */
     double last_loss;     /* mean squared error of the last training batch */
 } dmph_surrogate_stats;
 
