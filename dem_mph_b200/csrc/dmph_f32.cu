@@ -178,7 +178,13 @@ __device__ __forceinline__ void finish_a32(const DevParams &P, const DevParams32
     S.vsp32[i] = (float)volstrain;
     S.div32[i] = (float)A.div;
     const double kappa = volstrain < 0.0 ? 0.0 : P.bulk[I.ti];
-    if (!I.si) S.pres32[i] = (float)(-P.bvisc[I.ti] * A.div + kappa * volstrain);
+    if (!I.si) {
+        // the pressure also goes to v4.w, where pass B gathers it together with
+        // the velocity (solids keep 0 there, as their PressureP stays 0)
+        const float pres = (float)(-P.bvisc[I.ti] * A.div + kappa * volstrain);
+        S.pres32[i] = pres;
+        reinterpret_cast<float *>(S.v4 + i)[3] = pres;
+    }
     if (ST) {
         S.densA32[i] = A.dA;
         float pa = Q.CofA[I.ti] * (A.dA - Q.N0a) / Q.dx;
@@ -640,8 +646,7 @@ __device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const Dev
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {
             pj[u] = list_pos(Q, S, e[u], j[u]);
-            vj[u] = S.v4[j[u]];
-            vj[u].w = S.pres32[j[u]];
+            vj[u] = S.v4[j[u]];  // .w = pressure, written by pass A
         }
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {

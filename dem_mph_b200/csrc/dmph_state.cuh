@@ -30,7 +30,9 @@ struct DevState {
     // FP32 split-precision state (DMPH_PRECISION_FP32_SPLIT): positions relative
     // to the origin of the particle's rebuild-time cell, the cell coordinates
     // and type packed in .w (pack_cell), so every pair is formed in the frame
-    // of one cell with FP32 magnitudes of a few particle spacings
+    // of one cell with FP32 magnitudes of a few particle spacings; v4.w holds
+    // the pressure of the last pass A (0 for solids and for walls without
+    // fluid in reach), read by pass B together with the velocity
     float4 *p4, *v4, *f4, *xref4, *gc4;
     float *pres32, *vsp32, *div32, *densA32, *pA32;
     float *alpha32, *dragC32;
