@@ -363,10 +363,16 @@ __device__ __forceinline__ void pair_b32(const DevParams32 &Q, const IB &I, cons
                 cd = 0.44f;
             B.dragc = cd;
             B.drag_j = j;
-            const float c = cd * rhoi * Q.drag_pref * Vs;
-            B.fD.x = fmaf(c, u0, B.fD.x);
-            B.fD.y = fmaf(c, u1, B.fD.y);
-            B.fD.z = fmaf(c, u2, B.fD.z);
+            // at zero relative velocity the reference's expression is inf * 0
+            // (Re = 0 makes cd infinite, :2785-2791); cd * Vs stays finite as
+            // Vs -> 0, so the drag force's limit there is 0, which this build
+            // uses (the FP64 parity build keeps the reference's NaN)
+            if (Vs > 0.f) {
+                const float c = cd * rhoi * Q.drag_pref * Vs;
+                B.fD.x = fmaf(c, u0, B.fD.x);
+                B.fD.y = fmaf(c, u1, B.fD.y);
+                B.fD.z = fmaf(c, u2, B.fD.z);
+            }
             const float a = fmaf(-r, Q.iRP, 1.f);
             const float wb = Q.density[tj] * Q.V * Q.Bp * a * a;
             B.fB.x = fmaf(wb, Q.g[0], B.fB.x);

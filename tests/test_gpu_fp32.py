@@ -130,3 +130,27 @@ def test_verlet_list_mode_matches_stencil_mode(name):
         assert np.abs(xa - xb).max() <= 1e-6 * L
     a.close()
     b.close()
+
+
+def test_fp32_drag_at_rest_on_the_cutoff_stays_finite():
+    """A scene whose debris and fluid lattices put pairs exactly at RadiusP:
+    FP32 rounding takes some of them in (FP64 leaves them out), and at rest the
+    reference's drag expression is inf * 0 there.  The FP32 build uses the
+    limit, 0, so the state stays finite."""
+    import os
+    import tempfile
+    from dem_mph_b200 import files, scenes
+    s = scenes.small(seed=3, dx=0.025)
+    with tempfile.TemporaryDirectory() as tmp:
+        d, g = os.path.join(tmp, "d.data"), os.path.join(tmp, "s.grid")
+        files.write_data_file(d, s.params)
+        files.write_grid(g, s.params, s.type, s.x, s.v)
+        p = files.read_data_file(d)
+        p, typ, x, v = files.read_grid(g, p)
+    p.dim = 3
+    p.precision = PRECISION_FP32_SPLIT
+    g = solver.Solver(p, typ, x, v)
+    g.step(5)
+    _, xs, vs, _ = g.state()
+    assert np.all(np.isfinite(xs)) and np.all(np.isfinite(vs)) and np.all(np.isfinite(g.field("Force")))
+    g.close()
