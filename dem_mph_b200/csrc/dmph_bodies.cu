@@ -74,55 +74,62 @@ __global__ void __launch_bounds__(8 * kWarp) k_clump_dem(DevParams P, DevState S
             hi[k] = flat ? 0 : (P.cw[k] - loc < reach ? 1 : 0);
         }
         double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
-        for (int ox = lo[0]; ox <= hi[0]; ++ox)
-            for (int oy = lo[1]; oy <= hi[1]; ++oy)
-                for (int oz = lo[2]; oz <= hi[2]; ++oz) {
-                    const int cell = cell_id(P, c[0] + ox, c[1] + oy, c[2] + oz);
-                    for (int cls = 1; cls < 3; ++cls) {
-                        const int off = cls * P.T + cell;
-                        const int jb = __ldg(S.cell_start + off), je = __ldg(S.cell_start + off + 1);
-                        for (int j = jb + lane; j < je; j += kWarp) {
-                            if (j == i) continue;
-                            const int bj = S.bid[j];
-                            if (bi >= 0 && bj == bi) continue;
-                            double q[3];
-                            for (int k = 0; k < 3; k++) {
-                                q[k] = S.pos[k * N + j] - xi[k];
-                                q[k] -= P.W[k] * rint(q[k] / P.W[k]);
-                            }
-                            const double r2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
-                            if (r2 > P.dx2 || r2 <= 0.0) continue;
-                            const int tj = S.type[j];
-                            const double r = sqrt(r2);
-                            const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
-                            const double ov = P.dx - r;
-                            const double u[3] = {S.vel[j] - vi[0], S.vel[N + j] - vi[1], S.vel[2 * N + j] - vi[2]};
-                            const double un = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
-                            const double mj = (bj >= 0 ? S.body_rho[bj] : P.density[tj]) * P.V;
-                            const double mij = mi * mj / (mi + mj);
-                            const double kn = (4.0 / 3.0) * P.Eeff[ti][tj] * sqrt(P.Reff * ov);
-                            const double cn = sqrt(mij * kn) * P.pairDamp[ti][tj];
-                            const double kt = P.KtFac[ti][tj] * sqrt(P.Reff * sqrt(ov));
-                            const double ct = sqrt(mij * kt) * P.pairDamp[ti][tj];
-                            double f[3], ut[3];
-                            const double fnm = fmin(-kn * ov + cn * un, 0.0);  // no adhesion
-                            for (int k = 0; k < 3; k++) {
-                                f[k] = fnm * e[k];
-                                ut[k] = u[k] - un * e[k];
-                            }
-                            const double ctot = ct + kt * P.ddt;
-                            const double aut = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
-                            const double cap = P.pairFric[ti][tj] * fabs(fnm);
-                            const double ft = ctot * aut > cap && aut > 0.0 ? cap / aut : ctot;
-                            for (int k = 0; k < 3; k++) f[k] += ft * ut[k];
-                            for (int k = 0; k < 3; k++) F[k] += f[k];
-                            // offset of the contact midpoint from the particle centre: 0.5 q
-                            T[0] += 0.5 * (q[1] * f[2] - q[2] * f[1]);
-                            T[1] += 0.5 * (q[2] * f[0] - q[0] * f[2]);
-                            T[2] += 0.5 * (q[0] * f[1] - q[1] * f[0]);
-                        }
-                    }
+        // the (cell, class) ranges to visit, fetched by 16 lanes at once:
+        // lane r < 16 holds range r = (cell index r / 2 of the <= 8 cells,
+        // class 1 + r % 2)
+        const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+        const int nranges = 2 * nx * ny * nz;
+        int rb = 0, re = 0;
+        if (lane < nranges) {
+            const int c_ = lane >> 1, cls = 1 + (lane & 1);
+            const int oz = lo[2] + c_ % nz, oy = lo[1] + (c_ / nz) % ny, ox = lo[0] + c_ / (nz * ny);
+            const int off = cls * P.T + cell_id(P, c[0] + ox, c[1] + oy, c[2] + oz);
+            rb = __ldg(S.cell_start + off);
+            re = __ldg(S.cell_start + off + 1);
+        }
+        for (int r = 0; r < nranges; ++r) {
+            const int jb = __shfl_sync(kFull, rb, r), je = __shfl_sync(kFull, re, r);
+            for (int j = jb + lane; j < je; j += kWarp) {
+                if (j == i) continue;
+                const int bj = S.bid[j];
+                if (bi >= 0 && bj == bi) continue;
+                double q[3];
+                for (int k = 0; k < 3; k++) {
+                    q[k] = S.pos[k * N + j] - xi[k];
+                    q[k] -= P.W[k] * rint(q[k] / P.W[k]);
                 }
+                const double r2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+                if (r2 > P.dx2 || r2 <= 0.0) continue;
+                const int tj = S.type[j];
+                const double r = sqrt(r2);
+                const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
+                const double ov = P.dx - r;
+                const double u[3] = {S.vel[j] - vi[0], S.vel[N + j] - vi[1], S.vel[2 * N + j] - vi[2]};
+                const double un = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
+                const double mj = (bj >= 0 ? S.body_rho[bj] : P.density[tj]) * P.V;
+                const double mij = mi * mj / (mi + mj);
+                const double kn = (4.0 / 3.0) * P.Eeff[ti][tj] * sqrt(P.Reff * ov);
+                const double cn = sqrt(mij * kn) * P.pairDamp[ti][tj];
+                const double kt = P.KtFac[ti][tj] * sqrt(P.Reff * sqrt(ov));
+                const double ct = sqrt(mij * kt) * P.pairDamp[ti][tj];
+                double f[3], ut[3];
+                const double fnm = fmin(-kn * ov + cn * un, 0.0);  // no adhesion
+                for (int k = 0; k < 3; k++) {
+                    f[k] = fnm * e[k];
+                    ut[k] = u[k] - un * e[k];
+                }
+                const double ctot = ct + kt * P.ddt;
+                const double aut = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
+                const double cap = P.pairFric[ti][tj] * fabs(fnm);
+                const double ft = ctot * aut > cap && aut > 0.0 ? cap / aut : ctot;
+                for (int k = 0; k < 3; k++) f[k] += ft * ut[k];
+                for (int k = 0; k < 3; k++) F[k] += f[k];
+                // offset of the contact midpoint from the particle centre: 0.5 q
+                T[0] += 0.5 * (q[1] * f[2] - q[2] * f[1]);
+                T[1] += 0.5 * (q[2] * f[0] - q[0] * f[2]);
+                T[2] += 0.5 * (q[0] * f[1] - q[1] * f[0]);
+            }
+        }
         for (int k = 0; k < 3; k++) {
             F[k] = warp_sum(F[k]);
             T[k] = warp_sum(T[k]);

@@ -586,7 +586,7 @@ __device__ __forceinline__ float4 list_pos(const DevParams32 &Q, const DevState 
     j = (int)(e & 0xFFFFFFu);
     const int code = (int)(e >> 24);
     const int dx = code / 9 - 1, dy = (code / 3) % 3 - 1, dz = code % 3 - 1;
-    const float4 pj = S.p4[j];
+    const float4 pj = __ldg(S.p4 + j);  // positions are read-only in the passes
     return make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
                        fmaf((float)dz, Q.cw[2], pj.z), __int_as_float(unpack_type(__float_as_uint(pj.w))));
 }
@@ -613,7 +613,8 @@ __device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const Dev
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {
             pj[u] = list_pos(Q, S, e[u], j[u]);
-            vj[u] = S.v4[j[u]];
+            // pass A writes only the .w (pressure) of v4, which it does not read
+            vj[u] = __ldg(S.v4 + j[u]);
         }
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {
@@ -652,7 +653,7 @@ __device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const Dev
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {
             pj[u] = list_pos(Q, S, e[u], j[u]);
-            vj[u] = S.v4[j[u]];  // .w = pressure, written by pass A
+            vj[u] = __ldg(S.v4 + j[u]);  // .w = pressure, written by pass A (read-only here)
         }
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {
