@@ -522,6 +522,16 @@ __device__ __forceinline__ void pass_b32_body(const DevParams &P, const DevParam
 // displacement by MARGIN/2, so every pair a kernel accepts until the next
 // rebuild is in the list.  The passes then run one thread per particle over
 // its list instead of over the ~800 candidates of the 27-cell stencil.
+// Blocked list layout: the entries of a particle come in blocks of 8 (one
+// 32-byte sector); block b of slot i is at ((b * N) + i) * 8.  The build fills
+// each particle's sectors one entry after the other, and a warp of consecutive
+// slots reads entry k of its 32 particles from 32 sectors that also hold the
+// particles' next entries.
+__host__ __device__ __forceinline__ long long list_index(int k, int i, long long ld)
+{
+    return (((long long)(k >> 3)) * ld + i) * 8 + (k & 7);
+}
+
 struct TileL {
     float4 p[kWarp];     // position in the frame of the warp's cell
     unsigned e[kWarp];   // j | cell-offset code << 24
@@ -570,7 +580,7 @@ __global__ void __launch_bounds__(8 * kWarp) k_build_list32(DevParams P, DevPara
                 while (m) {  // ascending candidate order
                     const int s = __ffs(m) - 1;
                     m &= m - 1;
-                    if (cnt < cap) S.nbl[(long long)cnt * ld + i] = tl.e[s];
+                    if (cnt < cap) S.nbl[list_index(cnt, i, ld)] = tl.e[s];
                     ++cnt;
                 }
             });
@@ -578,6 +588,30 @@ __global__ void __launch_bounds__(8 * kWarp) k_build_list32(DevParams P, DevPara
         if (cnt > cap) atomicExch(dB + B_LIST_OVF, 1);
         S.nbn[i] = cnt < cap ? cnt : cap;
     }
+}
+
+// entries k0 .. k0 + BATCH - 1 of slot i (BATCH divides 8, so they sit in one
+// block and load as one vector); entries past the count read as slot 0
+template <int BATCH>
+__device__ __forceinline__ void load_entries(const DevState &S, int k0, int cnt, int i, long long ld, unsigned *e)
+{
+    const unsigned *src = S.nbl + list_index(k0, i, ld);
+    if (BATCH == 4) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(src));
+        e[0] = v.x;
+        e[1] = v.y;
+        e[2] = v.z;
+        e[3] = v.w;
+    } else if (BATCH == 2) {
+        const uint2 v = __ldg(reinterpret_cast<const uint2 *>(src));
+        e[0] = v.x;
+        e[1] = v.y;
+    } else {
+        e[0] = __ldg(src);
+    }
+#pragma unroll
+    for (int u = 0; u < BATCH; ++u)
+        if (k0 + u >= cnt) e[u] = 0u;
 }
 
 // j's position in the frame of i's cell, type bits in .w
@@ -606,8 +640,7 @@ __device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const Dev
     AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
     for (int k0 = 0; k0 < cnt; k0 += BATCH) {
         unsigned e[BATCH];
-#pragma unroll
-        for (int u = 0; u < BATCH; ++u) e[u] = k0 + u < cnt ? __ldg(S.nbl + (long long)(k0 + u) * ld + i) : 0u;
+        load_entries<BATCH>(S, k0, cnt, i, ld, e);
         float4 pj[BATCH], vj[BATCH];
         int j[BATCH];
 #pragma unroll
@@ -646,8 +679,7 @@ __device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const Dev
     AccB B = acc_b_zero();
     for (int k0 = 0; k0 < cnt; k0 += BATCH) {
         unsigned e[BATCH];
-#pragma unroll
-        for (int u = 0; u < BATCH; ++u) e[u] = k0 + u < cnt ? __ldg(S.nbl + (long long)(k0 + u) * ld + i) : 0u;
+        load_entries<BATCH>(S, k0, cnt, i, ld, e);
         float4 pj[BATCH], vj[BATCH];
         int j[BATCH];
 #pragma unroll

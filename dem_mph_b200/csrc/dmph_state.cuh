@@ -6,10 +6,10 @@
 namespace dmph {
 
 struct DevState {
-    // FP32 Verlet lists (list mode): entry k of slot i at nbl[k * N + i] =
-    // j | cell-offset code << 24 (code = (dx+1)*9 + (dy+1)*3 + (dz+1) of j's
-    // rebuild-time cell relative to i's), ascending j; nbn[i] = count, -1 for
-    // slots without a list (dry walls)
+    // FP32 Verlet lists (list mode): entry k of slot i at
+    // nbl[((k / 8) * N + i) * 8 + k % 8] = j | cell-offset code << 24 (code =
+    // (dx+1)*9 + (dy+1)*3 + (dz+1) of j's rebuild-time cell relative to i's),
+    // ascending j; nbn[i] = count, -1 for slots without a list (dry walls)
     unsigned *nbl;
     int *nbn;
     int nbl_cap;
