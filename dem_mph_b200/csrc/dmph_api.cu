@@ -98,7 +98,10 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
     if (ctx->fp32)
         launch_wet_partition(P, ctx->words, S.cell_start, S.chunks, ctx->chunks2, ctx->dB, ctx->flag, ctx->offs,
                              ctx->bsums, ctx->total, st);
-    if (ctx->fp32 && ctx->use_list) launch_build_list32(P, ctx->Q, S, ctx->dB, st);
+    if (ctx->use_list) {
+        if (ctx->fp32) launch_build_list32(P, ctx->Q, S, ctx->dB, st);
+        else launch_build_list64(P, S, ctx->dB, st);
+    }
     launch_counts(P, S, ctx->dB, ctx->all_counts ? CR_ALL : CR_SOLID, st);
 }
 
@@ -106,7 +109,7 @@ long long dmph::rebuild_launches(const dmph_ctx *ctx, bool first)
 {
     const DevParams &P = ctx->P;
     return 1 + bitonic_launches(P.P2, P.P2log) + 1 + 1 + (ctx->fp32 && !first ? 1 : 0) + 5 + 1 +
-           (ctx->fp32 ? 6 : 0) + 1 + (ctx->S.bid ? 1 : 0) + (ctx->fp32 && ctx->use_list ? 1 : 0);
+           (ctx->fp32 ? 6 : 0) + 1 + (ctx->S.bid ? 1 : 0) + (ctx->use_list ? 1 : 0);
 }
 
 // phase timing (dmph_set_profiling): events around one phase, synchronised
@@ -155,11 +158,14 @@ void dmph::enqueue_passes(dmph_ctx *ctx, cudaStream_t st)
         launch_fluid_accel32(Q, S, dB, st);
         phase_end(ctx, 3);
     } else {
+        const int lst = ctx->use_list ? 1 : 0;
         phase_begin(ctx);
-        launch_pass_a(P, S, dB, CR_ALL, 0, st);
+        if (lst) launch_pass_a(P, S, dB, CR_ALL, 0, st, 1, 0);
+        launch_pass_a(P, S, dB, CR_ALL, 0, st, 0, lst);
         phase_end(ctx, 2);
         phase_begin(ctx);
-        launch_pass_b(P, S, dB, st);
+        if (lst) launch_pass_b(P, S, dB, st, 1, 0);
+        launch_pass_b(P, S, dB, st, 0, lst);
         launch_fluid_accel(P, S, dB, st);
         phase_end(ctx, 3);
     }
@@ -229,7 +235,7 @@ long long dmph::dem_launches(const dmph_ctx *ctx)
 
 long long dmph::tail_launches(const dmph_ctx *ctx)
 {
-    return 3 + dem_launches(ctx) + (ctx->fp32 && ctx->use_list ? 2 : 0);
+    return 3 + dem_launches(ctx) + (ctx->use_list ? 2 : 0);
 }
 
 void dmph::advance_host_clock(dmph_ctx *ctx)
@@ -470,6 +476,8 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         AL(S.pA32, N);
         AL(S.alpha32, N);
         AL(S.dragC32, N);
+    }
+    {
         // Verlet lists: the lattice holds 122 (3D) / 28 (2D) particles within
         // MaxRadius + MARGIN = 3.1 dx; the capacity leaves room for compression
         S.nbl_cap = P.dim == 2 ? 64 : 192;
@@ -971,15 +979,11 @@ extern "C" int dmph_set_pair_mode(dmph_ctx *ctx, int mode)
 {
     if (!ctx) return DMPH_EINVAL;
     if (mode != DMPH_PAIRS_STENCIL && mode != DMPH_PAIRS_VERLET_LIST) return DMPH_EINVAL;
-    if (!ctx->fp32) {
-        if (mode == DMPH_PAIRS_STENCIL) return DMPH_OK;
-        ctx->err = "Verlet lists belong to the FP32 split build";
-        return DMPH_EINVAL;
-    }
     const bool want = mode == DMPH_PAIRS_VERLET_LIST;
     if (want && !ctx->use_list) {
         // lists of the current cell sort
-        launch_build_list32(ctx->P, ctx->Q, ctx->S, ctx->dB, ctx->st);
+        if (ctx->fp32) launch_build_list32(ctx->P, ctx->Q, ctx->S, ctx->dB, ctx->st);
+        else launch_build_list64(ctx->P, ctx->S, ctx->dB, ctx->st);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(ctx->st));
     }

@@ -522,16 +522,6 @@ __device__ __forceinline__ void pass_b32_body(const DevParams &P, const DevParam
 // displacement by MARGIN/2, so every pair a kernel accepts until the next
 // rebuild is in the list.  The passes then run one thread per particle over
 // its list instead of over the ~800 candidates of the 27-cell stencil.
-// Blocked list layout: the entries of a particle come in blocks of 8 (one
-// 32-byte sector); block b of slot i is at ((b * N) + i) * 8.  The build fills
-// each particle's sectors one entry after the other, and a warp of consecutive
-// slots reads entry k of its 32 particles from 32 sectors that also hold the
-// particles' next entries.
-__host__ __device__ __forceinline__ long long list_index(int k, int i, long long ld)
-{
-    return (((long long)(k >> 3)) * ld + i) * 8 + (k & 7);
-}
-
 struct TileL {
     float4 p[kWarp];     // position in the frame of the warp's cell
     unsigned e[kWarp];   // j | cell-offset code << 24

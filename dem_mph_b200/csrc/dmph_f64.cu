@@ -117,8 +117,14 @@ __global__ void k_drift(DevParams P, DevState S, WallMotion Wm, unsigned long lo
 // :2129, calculateDivergenceP :2158, calculatePhysicalCoefficients :1918 and
 // the pressures of calculatePressureP :2203-2208 and calculatePressureA
 // :2026-2031, for every particle.
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, DevState S, const int *dB, int range, int init_only)
+// LIST: walk each particle's Verlet list (the reference's own neighbour list,
+// same order) instead of the stencil; gate: this stencil launch stands in
+// only after a list overflow
+template <bool LIST>
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, DevState S, const int *dB, int range,
+                                                                   int init_only, int gate)
 {
+    if (LIST ? dB[B_LIST_OVF] != 0 : (gate && dB[B_LIST_OVF] == 0)) return;
     __shared__ TileA tiles[kWarpsPerBlock];
     TileA &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -135,8 +141,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, 
         const double vxi = S.vel[ii], vyi = S.vel[N + ii], vzi = S.vel[2 * N + ii];
         double vsp = 0.0, div = 0.0, dA = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0;
         const bool st = P.surface_tension;
-        traverse_stencil(
-            P, S.cell_start, key_cell, lane, active, 7u,
+        traverse_pairs<LIST>(
+            P, S, key_cell, lane, active, i, 7u,
             [&](int j, int slot) {
                 tl.x[slot] = S.pos[j];
                 tl.y[slot] = S.pos[N + j];
@@ -209,8 +215,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, 
 // kept in its own accumulator and added to Force in the reference's call
 // order, so the sums are bit-identical.  Wall particles are not visited:
 // their forces are reset at the next step without ever being read.
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, DevState S, const int *dB, int range)
+template <bool LIST>
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, DevState S, const int *dB, int range,
+                                                                   int gate)
 {
+    if (LIST ? dB[B_LIST_OVF] != 0 : (gate && dB[B_LIST_OVF] == 0)) return;
     __shared__ TileB tiles[kWarpsPerBlock];
     TileB &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -247,8 +256,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, 
         double fV[3] = {0.0, 0.0, 0.0}, fD[3] = {0.0, 0.0, 0.0}, fB[3] = {0.0, 0.0, 0.0};
         double dragc = 0.0;
         bool have_drag = false;
-        traverse_stencil(
-            P, S.cell_start, key_cell, lane, active, 7u,
+        traverse_pairs<LIST>(
+            P, S, key_cell, lane, active, i, 7u,
             [&](int j, int slot) {
                 tl.x[slot] = S.pos[j];
                 tl.y[slot] = S.pos[N + j];
@@ -615,10 +624,66 @@ void launch_drift(const DevParams &P, const DevState &S, const WallMotion &Wm, u
 constexpr int kBlock = kWarpsPerBlock * kWarp;
 constexpr int kElemGrid = 148 * 4;
 
-void launch_pass_a(const DevParams &P, const DevState &S, const int *dB, int range, int init_only, cudaStream_t st)
+// Verlet lists of the FP64 build: exactly the reference's NeighborInd
+// (calculateNeighbor :1521-1851): every j, i itself included, with
+// |x_j - x_i|^2 <= (MaxRadius + MARGIN)^2 at the rebuild-time positions, in
+// ascending slot order; blocked layout as in the FP32 build, entry = j
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_build_list64(DevParams P, DevState S, int *dB)
 {
-    static const int g = persistent_grid((const void *)k_pass_a, kBlock);
-    k_pass_a<<<g, kBlock, 0, st>>>(P, S, dB, range, init_only);
+    __shared__ TileA tiles[kWarpsPerBlock];
+    TileA &tl = tiles[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int N = P.N;
+    const int cap = S.nbl_cap;
+    FOR_EACH_CHUNK(dB, CR_ALL, kWarpsPerBlock, cidx)
+    {
+        const Chunk ch = S.chunks[cidx];
+        const int i = ch.i0 + lane;
+        const bool active = lane < ch.cnt;
+        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+        const int ii = active ? i : ch.i0;
+        const double xi = S.xref[ii], yi = S.xref[N + ii], zi = S.xref[2 * N + ii];
+        int cnt = 0;
+        traverse_stencil(
+            P, S.cell_start, key_cell, lane, active, 7u,
+            [&](int j, int slot) {
+                tl.x[slot] = S.xref[j];
+                tl.y[slot] = S.xref[N + j];
+                tl.z[slot] = S.xref[2 * N + j];
+            },
+            [&](int j, int s) {
+                const double q0 = rel1(tl.x[s], xi, P.W[0], P.hW[0]);
+                const double q1 = rel1(tl.y[s], yi, P.W[1], P.hW[1]);
+                const double q2 = rel1(tl.z[s], zi, P.W[2], P.hW[2]);
+                const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
+                if (r2 <= P.rc2) {
+                    if (cnt < cap) S.nbl[list_index(cnt, i, N)] = (unsigned)j;
+                    ++cnt;
+                }
+            });
+        if (!active) continue;
+        if (cnt > cap) atomicExch(dB + B_LIST_OVF, 1);
+        S.nbn[i] = cnt < cap ? cnt : cap;
+    }
+}
+
+void launch_build_list64(const DevParams &P, const DevState &S, int *dB, cudaStream_t st)
+{
+    cudaMemsetAsync(dB + B_LIST_OVF, 0, sizeof(int), st);
+    static const int g = persistent_grid((const void *)k_build_list64, kBlock);
+    k_build_list64<<<g, kBlock, 0, st>>>(P, S, dB);
+}
+
+void launch_pass_a(const DevParams &P, const DevState &S, const int *dB, int range, int init_only, cudaStream_t st,
+                   int list, int gate)
+{
+    if (list) {
+        static const int g = persistent_grid((const void *)k_pass_a<true>, kBlock);
+        k_pass_a<true><<<g, kBlock, 0, st>>>(P, S, dB, range, init_only, 0);
+    } else {
+        static const int g = persistent_grid((const void *)k_pass_a<false>, kBlock);
+        k_pass_a<false><<<g, kBlock, 0, st>>>(P, S, dB, range, init_only, gate);
+    }
 }
 // Virial stress and pressure of the output cadence
 // (calculateVirialStressAtParticle, source/DEM-MPH.cpp:2904-3149): the
@@ -730,10 +795,15 @@ void launch_virial(const DevParams &P, const DevState &S, const int *dB, double 
     k_virial<<<g, kBlock, 0, st>>>(P, S, dB, vir);
 }
 
-void launch_pass_b(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
+void launch_pass_b(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st, int list, int gate)
 {
-    static const int g = persistent_grid((const void *)k_pass_b, kBlock);
-    k_pass_b<<<g, kBlock, 0, st>>>(P, S, dB, CR_FLUID_SOLID);
+    if (list) {
+        static const int g = persistent_grid((const void *)k_pass_b<true>, kBlock);
+        k_pass_b<true><<<g, kBlock, 0, st>>>(P, S, dB, CR_FLUID_SOLID, 0);
+    } else {
+        static const int g = persistent_grid((const void *)k_pass_b<false>, kBlock);
+        k_pass_b<false><<<g, kBlock, 0, st>>>(P, S, dB, CR_FLUID_SOLID, gate);
+    }
 }
 void launch_dem_force(const DevParams &P, const DevState &S, const int *dB, int range, int forces, cudaStream_t st,
                       bool mixed)

@@ -30,9 +30,11 @@ void launch_decide(const DevParams &P, const unsigned long long *maxshift, int *
 // dmph_f64.cu
 void launch_drift(const DevParams &P, const DevState &S, const WallMotion &Wm, unsigned long long *maxshift, int sms,
                   cudaStream_t st);
-void launch_pass_a(const DevParams &P, const DevState &S, const int *dB, int range, int init_only, cudaStream_t st);
+void launch_pass_a(const DevParams &P, const DevState &S, const int *dB, int range, int init_only, cudaStream_t st,
+                   int list = 0, int gate = 0);
+void launch_build_list64(const DevParams &P, const DevState &S, int *dB, cudaStream_t st);
 void launch_virial(const DevParams &P, const DevState &S, const int *dB, double *vir, cudaStream_t st);
-void launch_pass_b(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
+void launch_pass_b(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st, int list = 0, int gate = 0);
 void launch_fluid_accel(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 void launch_dem_force(const DevParams &P, const DevState &S, const int *dB, int range, int forces, cudaStream_t st,
                       bool mixed = false);

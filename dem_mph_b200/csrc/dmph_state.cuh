@@ -70,6 +70,17 @@ struct DevBodies {
     double *Fsum, *Tsum;    // 3 per body: last substep's total force and torque (diagnostics)
 };
 
+// Blocked list layout: the entries of a particle come in blocks of 8 (one
+// 32-byte sector); block b of slot i is at ((b * N) + i) * 8.  The build fills
+// each particle's sectors one entry after the other, and a warp of consecutive
+// slots reads entry k of its 32 particles from 32 sectors that also hold the
+// particles' next entries.
+__host__ __device__ __forceinline__ long long list_index(int k, int i, long long ld)
+{
+    return (((long long)(k >> 3)) * ld + i) * 8 + (k & 7);
+}
+
+
 #ifdef __CUDACC__
 // rigid-body helpers shared by the body kernels and the surrogate
 __device__ __forceinline__ double warp_sum(double v)

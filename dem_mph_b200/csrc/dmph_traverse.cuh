@@ -19,7 +19,7 @@
 // the same pairs in the same order without materialising the list.
 #pragma once
 
-#include "dmph_device.cuh"
+#include "dmph_state.cuh"
 
 namespace dmph {
 
@@ -100,6 +100,32 @@ __device__ __forceinline__ void traverse_stencil_batched(const DevParams &P, con
                 __syncwarp();
             }
         }
+    }
+}
+
+}  // namespace dmph
+
+namespace dmph {
+
+// Per-lane walk of a particle's Verlet list (list mode): entry k of slot i is
+// visited in list order (ascending j, the order of the reference's neighbour
+// list), each lane staging its own candidate into its own tile slot, so the
+// same Stage/Visit callbacks serve both walks.  LIST = false walks the stencil.
+template <bool LIST, class Stage, class Visit>
+__device__ __forceinline__ void traverse_pairs(const DevParams &P, const DevState &S, int key_cell, int lane,
+                                               bool active, int i, unsigned class_mask, Stage &&stage, Visit &&visit)
+{
+    if (!LIST) {
+        traverse_stencil(P, S.cell_start, key_cell, lane, active, class_mask, stage, visit);
+        return;
+    }
+    if (!active) return;
+    const int cnt = S.nbn[i];
+    const long long ld = P.N;
+    for (int k = 0; k < cnt; ++k) {
+        const int j = (int)(__ldg(S.nbl + list_index(k, i, ld)) & 0xFFFFFFu);
+        stage(j, lane);
+        visit(j, lane);
     }
 }
 

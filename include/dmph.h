@@ -244,14 +244,15 @@ int dmph_set_bodies(dmph_ctx *ctx, int nbodies, const int *body_of_row, const do
  * F,T 3 per body (total force and torque of the last substep). */
 int dmph_get_bodies(dmph_ctx *ctx, double *X, double *V, double *q, double *L, double *mass, double *F, double *T);
 
-/* How the FP32 split build finds the pairs of pass A and pass B (the FP64
- * parity build always walks the stencil):
+/* How pass A and pass B find their pairs:
  *  DMPH_PAIRS_VERLET_LIST (default): at every rebuild each particle records
  *    the particles within the reference's list radius MaxRadius + MARGIN
  *    (calculateNeighbor, source/DEM-MPH.cpp:1521-1851) in ascending order, at
- *    most 192 (3D) or 64 (2D); the passes then run one thread per particle
- *    over its list.  A list that would overflow makes the step fall back to
- *    the stencil kernels until the next rebuild.
+ *    most 192 (3D) or 64 (2D) (in the FP64 build exactly the reference's
+ *    NeighborInd); the passes then walk the lists (FP32: one thread per
+ *    particle).  A list that would overflow makes the step fall back to the
+ *    stencil kernels until the next rebuild.  Results are bit-identical to
+ *    the stencil walk in the FP64 build.
  *  DMPH_PAIRS_STENCIL: every pass walks the 27 (9) cells of the stencil. */
 #define DMPH_PAIRS_STENCIL 0
 #define DMPH_PAIRS_VERLET_LIST 1
