@@ -129,13 +129,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, 
     TileA &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int N = P.N;
-    FOR_EACH_CHUNK(dB, range, kWarpsPerBlock, cidx)
-    {
-        const Chunk ch = S.chunks[cidx];
-        const int i = ch.i0 + lane;
-        const bool active = lane < ch.cnt;
-        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-        const int ii = active ? i : ch.i0;
+    auto body = [&](const int i, const bool active, const int key_cell, const int ii) {
         const int ti = S.type[ii];
         const double xi = S.pos[ii], yi = S.pos[N + ii], zi = S.pos[2 * N + ii];
         const double vxi = S.vel[ii], vyi = S.vel[N + ii], vzi = S.vel[2 * N + ii];
@@ -184,7 +178,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, 
                     }
                 }
             });
-        if (!active) continue;
+        if (!active) return;
         const double volstrain = (vsp - P.N0p);
         S.vsp[i] = volstrain;
         if (st) {
@@ -193,7 +187,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, 
             S.gc[N + i] = g1;
             S.gc[2 * N + i] = g2;
         }
-        if (init_only) continue;  // initialisation evaluates only the densities (:423-425)
+        if (init_only) return;  // initialisation evaluates only the densities (:423-425)
         S.divp[i] = div;
         double kappa = P.bulk[ti];
         if (volstrain < 0.0) kappa = 0.0;
@@ -202,6 +196,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_a(DevParams P, 
             double pa = P.CofA[ti] * (dA - P.N0a) / P.dx;
             if (P.N0a <= dA) pa = 0.0;
             S.pA[i] = pa;
+        }
+    };
+    if (LIST) {
+        // one thread per slot: nothing in the list walk is warp-synchronous
+        const int end = range == CR_ALL ? N : dB[B_SE];
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) body(i, true, 0, i);
+    } else {
+        FOR_EACH_CHUNK(dB, range, kWarpsPerBlock, cidx)
+        {
+            const Chunk ch = S.chunks[cidx];
+            const int i = ch.i0 + lane;
+            const bool active = lane < ch.cnt;
+            body(i, active, (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T), active ? i : ch.i0);
         }
     }
 }
@@ -224,13 +231,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, 
     TileB &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int N = P.N;
-    FOR_EACH_CHUNK(dB, range, kWarpsPerBlock, cidx)
-    {
-        const Chunk ch = S.chunks[cidx];
-        const int i = ch.i0 + lane;
-        const bool active = lane < ch.cnt;
-        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-        const int ii = active ? i : ch.i0;
+    auto body = [&](const int i, const bool active, const int key_cell, const int ii) {
         const int ti = S.type[ii];
         const bool sol = is_solid(ti);
         const double xi = S.pos[ii], yi = S.pos[N + ii], zi = S.pos[2 * N + ii];
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, 
                     for (int d = 0; d < 3; d++) fB[d] += rhoj * P.V * P.g[d] * w;
                 }
             });
-        if (!active) continue;
+        if (!active) return;
         double F[3] = {0.0, 0.0, 0.0};
         const double m = sol ? rhoi * P.V : P.mass[ti];
         if (sol) {
@@ -368,6 +369,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, 
             for (int d = 0; d < 3; d++) F[d] += m * P.g[d];
         }
         for (int d = 0; d < 3; d++) S.frc[d * N + i] = F[d];
+    };
+    if (LIST) {
+        // one thread per slot: nothing in the list walk is warp-synchronous
+        const int end = dB[B_SE];
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) body(i, true, 0, i);
+    } else {
+        FOR_EACH_CHUNK(dB, range, kWarpsPerBlock, cidx)
+        {
+            const Chunk ch = S.chunks[cidx];
+            const int i = ch.i0 + lane;
+            const bool active = lane < ch.cnt;
+            body(i, active, (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T), active ? i : ch.i0);
+        }
     }
 }
 
