@@ -384,6 +384,12 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         delete ctx;
         return rc;
     }
+    for (long long k = 0; k < 3ll * n; k++)
+        if (!std::isfinite(x3[k]) || !std::isfinite(v3[k])) {
+            g_create_err = "non-finite position or velocity at row " + std::to_string(k / 3);
+            delete ctx;
+            return DMPH_ENAN;
+        }
     ctx->all_counts = (p->flags & DMPH_FLAG_ALL_NEIGHBOR_COUNTS) != 0;
     ctx->fp32 = p->precision == DMPH_PRECISION_FP32_SPLIT;
     if (ctx->fp32) {
@@ -1022,7 +1028,7 @@ extern "C" int dmph_get_phase_times(dmph_ctx *ctx, double *ms, int64_t *launches
 
 extern "C" int dmph_destroy(dmph_ctx *ctx)
 {
-    if (!ctx) return DMPH_EINVAL;
+    if (!ctx) return DMPH_OK;  // like free(NULL)
     release(ctx);
     delete ctx;
     return DMPH_OK;

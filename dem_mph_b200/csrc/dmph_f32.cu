@@ -3,12 +3,19 @@
 // Same step structure, pair sets and per-particle semantics as the FP64
 // kernels in dmph_f64.cu (which restate the reference, source/DEM-MPH.cpp),
 // but the pair arithmetic runs in FP32 on positions stored relative to the
-// origin of each particle's rebuild-time cell:  when a warp stages a
-// neighbour j it shifts j into the frame of the warp's cell by the
-// minimum-image cell offset times the cell width, so every difference is
-// formed between numbers of a few particle spacings.  Reciprocal square roots
-// and fused multiply-adds are used freely; accuracy is checked against the
-// FP64 oracle with a 1e-5 bound on forces relative to their field maximum.
+// origin of each particle's rebuild-time cell: a neighbour j is shifted into
+// the frame of i's cell by the minimum-image cell offset times the cell width,
+// so every difference is formed between numbers of a few particle spacings.
+// The per-pair arithmetic (pair_a32, pair_b32) is shared by two walks:
+//   * Verlet lists (default): built at each rebuild by k_build_list32, walked
+//     by one thread per particle (k_pass_a32_list, k_pass_b32_list);
+//   * the warp-cooperative stencil (k_pass_a32, k_pass_b32, 1/2/4 lanes per
+//     particle), used after a list overflow, in DMPH_PAIRS_STENCIL mode and by
+//     the stencil ensemble kernels.
+// Pass A uses correctly rounded square roots (its strain sum cancels against
+// N0p); pass B uses the approximate reciprocal square root.  Sums that cancel
+// are carried in FP64.  Accuracy is checked against the FP64 oracle: forces
+// within 1e-5 of each particle's force scale at equal pressures.
 #include "dmph_state.cuh"
 #include "dmph_traverse.cuh"
 

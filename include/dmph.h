@@ -299,7 +299,7 @@ int dmph_ensemble_autotune(dmph_ensemble *e, int *variant_a, int *variant_b, flo
 int dmph_ensemble_set_graph(dmph_ensemble *e, int enable);
 int dmph_ensemble_info(dmph_ensemble *e, int64_t *kernel_launches, int64_t *steps);
 const char *dmph_ensemble_last_error(dmph_ensemble *e);
-int dmph_ensemble_destroy(dmph_ensemble *e);
+int dmph_ensemble_destroy(dmph_ensemble *e); /* NULL: nothing to do, returns 0 */
 
 /* Learned surrogate of K solver steps (no counterpart in the reference).
  * FP32 split build only.  A surrogate call evaluates pass A and pass B at the
@@ -404,7 +404,7 @@ int dmph_get_phase_times(dmph_ctx *ctx, double *ms, int64_t *launches, int n);
 int dmph_cell_sort_noalloc(const dmph_params *p, int n, const double *pos_planes, const int *type,
                            int32_t *sorted_key, int32_t *perm, void *stream);
 
-/* Release the context and its device memory. */
+/* Release the context and its device memory (NULL: nothing to do, returns 0). */
 int dmph_destroy(dmph_ctx *ctx);
 
 /* Message of the last failing call on ctx (or of the last failing
