@@ -235,7 +235,8 @@ long long dmph::dem_launches(const dmph_ctx *ctx)
 
 long long dmph::tail_launches(const dmph_ctx *ctx)
 {
-    return 3 + dem_launches(ctx) + (ctx->use_list ? 2 : 0);
+    // list mode: pass A list, pass B list (FP32: fluid and debris kernels)
+    return 3 + dem_launches(ctx) + (ctx->use_list ? (ctx->fp32 ? 3 : 2) : 0);
 }
 
 void dmph::advance_host_clock(dmph_ctx *ctx)

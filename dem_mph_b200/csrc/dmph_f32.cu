@@ -274,9 +274,14 @@ struct IB {  // particle i of pass B
     bool sol;
     float Pi, rhoi, alpha;
 };
-// the pressure and viscous pair terms nearly cancel: their sums are FP64
+// The pressure and viscous pair terms both point along the pair direction
+// and nearly cancel over the neighbourhood: they are summed as one FP32
+// coefficient per pair into a short FP32 partial (fq: the pairs of one block
+// of 8 list entries, or one pair in the stencil walk), which is added to the
+// FP64 sum f at the end of the block (flush_b).
 struct AccB {
-    double3 fP, fV;
+    double3 f;  // pressure + viscous terms (fluid), viscous terms (debris)
+    float3 fq;  // pending FP32 partial of f
     float3 fD, fB, fS;
     float dragc;
     int drag_j;  // candidate that wrote dragc: the last one in the reference's order wins
@@ -285,14 +290,22 @@ struct AccB {
 __device__ __forceinline__ AccB acc_b_zero()
 {
     AccB B;
-    B.fP = make_double3(0.0, 0.0, 0.0);
-    B.fV = B.fP;
-    B.fD = make_float3(0.f, 0.f, 0.f);
-    B.fB = B.fD;
-    B.fS = B.fD;
+    B.f = make_double3(0.0, 0.0, 0.0);
+    B.fq = make_float3(0.f, 0.f, 0.f);
+    B.fD = B.fq;
+    B.fB = B.fq;
+    B.fS = B.fq;
     B.dragc = 0.f;
     B.drag_j = -1;
     return B;
+}
+
+__device__ __forceinline__ void flush_b(AccB &B)
+{
+    B.f.x += (double)B.fq.x;
+    B.f.y += (double)B.fq.y;
+    B.f.z += (double)B.fq.z;
+    B.fq = make_float3(0.f, 0.f, 0.f);
 }
 
 template <bool ST>
@@ -319,8 +332,9 @@ __device__ __forceinline__ IB make_ib(const DevParams &P, const DevState &S, int
 }
 
 // one pair (pj in the frame of i's cell, .w = type bits; vj.w = pressure of
-// j; gj = gravity centre of j, .w its attractive pressure), j its slot
-template <bool ST>
+// j; gj = gravity centre of j, .w its attractive pressure), j its slot.
+// CLS: 0 = i is fluid, 1 = i is debris, 2 = either (read from I.sol).
+template <bool ST, int CLS = 2>
 __device__ __forceinline__ void pair_b32(const DevParams32 &Q, const IB &I, const float4 pj, const float4 vj,
                                          const float4 gj, int j, AccB &B)
 {
@@ -328,34 +342,33 @@ __device__ __forceinline__ void pair_b32(const DevParams32 &Q, const IB &I, cons
     const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
     const int tj = __float_as_int(pj.w);
     const int ti = I.ti;
+    const bool sol = CLS == 2 ? I.sol : CLS == 1;
     const float u0 = vj.x - I.vi.x, u1 = vj.y - I.vi.y, u2 = vj.z - I.vi.z;
     const float ir = rsqrtf(r2);
     const float r = r2 * ir;
-    if (!I.sol) {
+    if (!sol) {
+        float c = 0.f;
         if (r2 < Q.RP2) {
             const float a = fmaf(-r, Q.iRP, 1.f);
-            const float c = (I.Pi + vj.w) * Q.dwpV * a * ir;  // (Pi+Pj) dw/r V
-            B.fP.x += (double)(c * q0);
-            B.fP.y += (double)(c * q1);
-            B.fP.z += (double)(c * q2);
+            c = (I.Pi + vj.w) * Q.dwpV * a * ir;  // (Pi+Pj) dw/r V
         }
         if (r2 < Q.RV2) {
             const float a = fmaf(-r, Q.iRV, 1.f);
             const float uq = fmaf(u0, q0, fmaf(u1, q1, u2 * q2));
             // C mu (u.e) e (-dw)/r V with e = q/r
-            const float c = Q.muij[ti][tj] * uq * a * (ir * ir * ir);
-            B.fV.x += (double)(c * q0);
-            B.fV.y += (double)(c * q1);
-            B.fV.z += (double)(c * q2);
+            c += Q.muij[ti][tj] * uq * a * (ir * ir * ir);
         }
+        B.fq.x = fmaf(c, q0, B.fq.x);
+        B.fq.y = fmaf(c, q1, B.fq.y);
+        B.fq.z = fmaf(c, q2, B.fq.z);
     } else {
         if (!is_wall(tj) && r2 < Q.RV2) {
             const float a = fmaf(-r, Q.iRV, 1.f);
             const float uq = fmaf(u0, q0, fmaf(u1, q1, u2 * q2));
             const float c = Q.muij[ti][tj] * uq * a * (ir * ir * ir);
-            B.fV.x += (double)(c * q0);
-            B.fV.y += (double)(c * q1);
-            B.fV.z += (double)(c * q2);
+            B.fq.x = fmaf(c, q0, B.fq.x);
+            B.fq.y = fmaf(c, q1, B.fq.y);
+            B.fq.z = fmaf(c, q2, B.fq.z);
         }
         if (r2 < Q.RP2 && is_fluid(tj)) {
             const float alpha = I.alpha, rhoi = I.rhoi;
@@ -387,7 +400,7 @@ __device__ __forceinline__ void pair_b32(const DevParams32 &Q, const IB &I, cons
             B.fB.z = fmaf(wb, Q.g[2], B.fB.z);
         }
     }
-    if (ST && !((I.sol && is_wall(tj)) || (is_solid(tj) && is_wall(ti)))) {
+    if (ST && !((sol && is_wall(tj)) || (is_solid(tj) && is_wall(ti)))) {
         const float4 gi = I.gi;
         const float rij_ = Q.ratio[ti][tj], rji_ = Q.ratio[tj][ti];
         if (r2 < Q.RA2) {
@@ -417,21 +430,23 @@ __device__ __forceinline__ void pair_b32(const DevParams32 &Q, const IB &I, cons
     }
 }
 
+template <int CLS = 2>
 __device__ __forceinline__ void finish_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, int i,
                                            const IB &I, const AccB &B)
 {
-    const float m = I.sol ? I.rhoi * Q.V : Q.mass[I.ti];
+    const bool sol = CLS == 2 ? I.sol : CLS == 1;
+    const float m = sol ? I.rhoi * Q.V : Q.mass[I.ti];
     float4 F;
-    if (I.sol) {
-        F.x = (float)(2.0 * B.fD.x + B.fS.x + B.fV.x - B.fB.x + (double)m * P.g[0]);
-        F.y = (float)(2.0 * B.fD.y + B.fS.y + B.fV.y - B.fB.y + (double)m * P.g[1]);
-        F.z = (float)(2.0 * B.fD.z + B.fS.z + B.fV.z - B.fB.z + (double)m * P.g[2]);
+    if (sol) {
+        F.x = (float)(2.0 * B.fD.x + B.fS.x + B.f.x - B.fB.x + (double)m * P.g[0]);
+        F.y = (float)(2.0 * B.fD.y + B.fS.y + B.f.y - B.fB.y + (double)m * P.g[1]);
+        F.z = (float)(2.0 * B.fD.z + B.fS.z + B.f.z - B.fB.z + (double)m * P.g[2]);
         S.alpha32[i] = I.alpha;
         if (B.drag_j >= 0) S.dragC32[i] = B.dragc;
     } else {
-        F.x = (float)(B.fP.x + B.fS.x + B.fV.x + (double)m * P.g[0]);
-        F.y = (float)(B.fP.y + B.fS.y + B.fV.y + (double)m * P.g[1]);
-        F.z = (float)(B.fP.z + B.fS.z + B.fV.z + (double)m * P.g[2]);
+        F.x = (float)(B.f.x + B.fS.x + (double)m * P.g[0]);
+        F.y = (float)(B.f.y + B.fS.y + (double)m * P.g[1]);
+        F.z = (float)(B.f.z + B.fS.z + (double)m * P.g[2]);
     }
     F.w = 0.f;
     S.f4[i] = F;
@@ -488,15 +503,13 @@ __device__ __forceinline__ void pass_b32_body(const DevParams &P, const DevParam
                     const int s = __ffs(m) - 1;
                     m &= m - 1;
                     pair_b32<ST>(Q, I, tl.p[s], tl.v[s], ST ? ts.g[s] : make_float4(0.f, 0.f, 0.f, 0.f), base + s, B);
+                    flush_b(B);
                 }
             });
         for (int o = G; o < kWarp; o <<= 1) {
-            B.fP.x += __shfl_xor_sync(kFull, B.fP.x, o);
-            B.fP.y += __shfl_xor_sync(kFull, B.fP.y, o);
-            B.fP.z += __shfl_xor_sync(kFull, B.fP.z, o);
-            B.fV.x += __shfl_xor_sync(kFull, B.fV.x, o);
-            B.fV.y += __shfl_xor_sync(kFull, B.fV.y, o);
-            B.fV.z += __shfl_xor_sync(kFull, B.fV.z, o);
+            B.f.x += __shfl_xor_sync(kFull, B.f.x, o);
+            B.f.y += __shfl_xor_sync(kFull, B.f.y, o);
+            B.f.z += __shfl_xor_sync(kFull, B.f.z, o);
             B.fD.x += __shfl_xor_sync(kFull, B.fD.x, o);
             B.fD.y += __shfl_xor_sync(kFull, B.fD.y, o);
             B.fD.z += __shfl_xor_sync(kFull, B.fD.z, o);
@@ -663,7 +676,10 @@ __global__ void __launch_bounds__(256, MINB) k_pass_a32_list(DevParams P, DevPar
         pass_a32_list_slot<ST, BATCH>(P, Q, S, i);
 }
 
-template <bool ST, int BATCH>
+// CLS: 0 = slot i holds fluid, 1 = debris, 2 = either.  The single-scene
+// step runs the fluid slots [0, fe) and the debris slots [sb, se) as two
+// kernels, so the fluid kernel carries none of the drag and buoyancy state.
+template <bool ST, int BATCH, int CLS = 2>
 __device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const DevParams32 &Q, const DevState &S, int i)
 {
     const int cnt = S.nbn[i];
@@ -693,20 +709,23 @@ __device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const Dev
                     gj = S.gc4[j[u]];
                     gj.w = S.pA32[j[u]];
                 }
-                pair_b32<ST>(Q, I, pj[u], vj[u], gj, j[u], B);
+                pair_b32<ST, CLS>(Q, I, pj[u], vj[u], gj, j[u], B);
             }
         }
+        // one FP64 add per block of 8 entries, whatever BATCH is, so every
+        // launch variant gives the same bits
+        if (((k0 + BATCH) & 7) == 0) flush_b(B);
     }
-    finish_b32(P, Q, S, i, I, B);
+    flush_b(B);
+    finish_b32<CLS>(P, Q, S, i, I, B);
 }
 
-template <bool ST, int BATCH, int MINB>
+template <bool ST, int BATCH, int MINB, int CLS>
 __global__ void __launch_bounds__(256, MINB) k_pass_b32_list(DevParams P, DevParams32 Q, DevState S, const int *dB)
 {
     if (dB[B_LIST_OVF]) return;
-    const int end = dB[B_SE];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x)
-        pass_b32_list_slot<ST, BATCH>(P, Q, S, i);
+    FOR_EACH_SLOT(dB, CLS == 1 ? B_SB : -1, CLS == 0 ? B_FE : B_SE, i)
+    pass_b32_list_slot<ST, BATCH, CLS>(P, Q, S, i);
 }
 
 // chunk bodies dispatched on the chunk's size: 4 lanes per particle for up to
@@ -1229,14 +1248,15 @@ void launch_pass_a32_list(const DevParams &P, const DevParams32 &Q, const DevSta
 void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
                           cudaStream_t st)
 {
+    // fluid slots with the tuned variant
 #define DMPH_LAUNCH_LB(ID, BATCH, MINB)                                                   \
     case ID:                                                                              \
         if (P.surface_tension) {                                                          \
-            static const int g = grid_for(k_pass_b32_list<true, BATCH, MINB>, 256);       \
-            k_pass_b32_list<true, BATCH, MINB><<<g, 256, 0, st>>>(P, Q, S, dB);           \
+            static const int g = grid_for(k_pass_b32_list<true, BATCH, MINB, 0>, 256);    \
+            k_pass_b32_list<true, BATCH, MINB, 0><<<g, 256, 0, st>>>(P, Q, S, dB);        \
         } else {                                                                          \
-            static const int g = grid_for(k_pass_b32_list<false, BATCH, MINB>, 256);      \
-            k_pass_b32_list<false, BATCH, MINB><<<g, 256, 0, st>>>(P, Q, S, dB);          \
+            static const int g = grid_for(k_pass_b32_list<false, BATCH, MINB, 0>, 256);   \
+            k_pass_b32_list<false, BATCH, MINB, 0><<<g, 256, 0, st>>>(P, Q, S, dB);       \
         }                                                                                 \
         break;
     switch (variant) {
@@ -1244,6 +1264,16 @@ void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevSta
     default: break;
     }
 #undef DMPH_LAUNCH_LB
+    // debris slots
+    {
+        if (P.surface_tension) {
+            static const int g = grid_for(k_pass_b32_list<true, 2, 2, 1>, 256);
+            k_pass_b32_list<true, 2, 2, 1><<<g, 256, 0, st>>>(P, Q, S, dB);
+        } else {
+            static const int g = grid_for(k_pass_b32_list<false, 2, 2, 1>, 256);
+            k_pass_b32_list<false, 2, 2, 1><<<g, 256, 0, st>>>(P, Q, S, dB);
+        }
+    }
 }
 
 void launch_ens_pass_a32(const EnsScene *tab, int ns, int variant, cudaStream_t st, int gate)

@@ -746,7 +746,9 @@ int surrogate_block(dmph_ctx *ctx, Surrogate *s)
         ctx->launches += rebuild_launches(ctx, false);
         ctx->host_rebuilds++;
     }
-    ctx->launches += 13 + (s->n_rows > s->n_fluid ? s->prm.substeps * dem_launches(ctx) : 0);
+    // pair passes (list mode: 5, stencil: 2), features, 4 GEMMs, check, apply,
+    // maxshift, decide
+    ctx->launches += (ctx->use_list ? 14 : 11) + (s->n_rows > s->n_fluid ? s->prm.substeps * dem_launches(ctx) : 0);
     for (int k = 0; k < s->prm.substeps; ++k) advance_host_clock(ctx);
     s->st.calls++;
     return check_err(ctx, s);
