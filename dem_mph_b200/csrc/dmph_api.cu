@@ -99,7 +99,7 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
         launch_wet_partition(P, ctx->words, S.cell_start, S.chunks, ctx->chunks2, ctx->dB, ctx->flag, ctx->offs,
                              ctx->bsums, ctx->total, st);
     if (ctx->use_list) {
-        if (ctx->fp32) launch_build_list32(P, ctx->Q, S, ctx->dB, st);
+        if (ctx->fp32) launch_build_list32(P, ctx->Q, S, ctx->dB, ctx->Wm.moving ? 0 : 1, st);
         else launch_build_list64(P, S, ctx->dB, st);
     }
     launch_counts(P, S, ctx->dB, ctx->all_counts ? CR_ALL : CR_SOLID, st);
@@ -149,6 +149,7 @@ void dmph::enqueue_passes(dmph_ctx *ctx, cudaStream_t st)
     if (ctx->fp32) {
         const DevParams32 &Q = ctx->Q;
         phase_begin(ctx);
+        if (ctx->use_list && ctx->Wm.moving) launch_list_wall_guard(ctx->dB, st);
         if (ctx->use_list) launch_pass_a32_list(P, Q, S, dB, ctx->var_la, st);
         launch_pass_a32(P, Q, S, dB, CR_WET, ctx->var_a, st, ctx->use_list ? 1 : 0);
         phase_end(ctx, 2);
@@ -178,6 +179,7 @@ void dmph::enqueue_pair_passes32(dmph_ctx *ctx, cudaStream_t st)
 {
     const DevParams &P = ctx->P;
     const DevParams32 &Q = ctx->Q;
+    if (ctx->use_list && ctx->Wm.moving) launch_list_wall_guard(ctx->dB, st);
     if (ctx->use_list) launch_pass_a32_list(P, Q, ctx->S, ctx->dB, ctx->var_la, st);
     launch_pass_a32(P, Q, ctx->S, ctx->dB, CR_WET, ctx->var_a, st, ctx->use_list ? 1 : 0);
     if (ctx->use_list) launch_pass_b32_list(P, Q, ctx->S, ctx->dB, ctx->var_lb, st);
@@ -233,10 +235,12 @@ long long dmph::dem_launches(const dmph_ctx *ctx)
     return ctx->demSteps * dem + (ctx->fp32 ? 2 : 0);
 }
 
-long long dmph::tail_launches(const dmph_ctx *ctx)
+long long dmph::tail_launches(const dmph_ctx *ctx, bool graph)
 {
-    // list mode: pass A list, pass B list (FP32: fluid and debris kernels)
-    return 3 + dem_launches(ctx) + (ctx->use_list ? (ctx->fp32 ? 3 : 2) : 0);
+    // list mode: pass A list, pass B list (FP32: fluid and debris kernels,
+    // and the list guard in a moving-wall window, which graphs never cover)
+    return 3 + dem_launches(ctx) +
+           (ctx->use_list ? (ctx->fp32 ? 3 + (!graph && ctx->Wm.moving ? 1 : 0) : 2) : 0);
 }
 
 void dmph::advance_host_clock(dmph_ctx *ctx)
@@ -490,6 +494,10 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         S.nbl_cap = P.dim == 2 ? 64 : 192;
         AL(S.nbl, (size_t)S.nbl_cap * N);
         AL(S.nbn, N);
+        if (ctx->fp32) {
+            AL(S.vsp_st, N);
+            AL(S.st4, N);
+        }
         ctx->use_list = true;
     }
     AL(ctx->flag, N);
@@ -747,7 +755,7 @@ extern "C" int dmph_get_info(dmph_ctx *ctx, dmph_info *info)
     info->surface_tension = P.surface_tension;
     {
         const long long graph_rebuilds = b[B_REBUILDS] - ctx->host_rebuilds;
-        info->kernel_launches = ctx->launches + ctx->graph_steps * (2 + tail_launches(ctx)) +
+        info->kernel_launches = ctx->launches + ctx->graph_steps * (2 + tail_launches(ctx, true)) +
                                 graph_rebuilds * rebuild_launches(ctx, false);
     }
     return DMPH_OK;
@@ -989,7 +997,7 @@ extern "C" int dmph_set_pair_mode(dmph_ctx *ctx, int mode)
     const bool want = mode == DMPH_PAIRS_VERLET_LIST;
     if (want && !ctx->use_list) {
         // lists of the current cell sort
-        if (ctx->fp32) launch_build_list32(ctx->P, ctx->Q, ctx->S, ctx->dB, ctx->st);
+        if (ctx->fp32) launch_build_list32(ctx->P, ctx->Q, ctx->S, ctx->dB, ctx->Wm.moving ? 0 : 1, ctx->st);
         else launch_build_list64(ctx->P, ctx->S, ctx->dB, ctx->st);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(ctx->st));
@@ -1271,6 +1279,10 @@ static int ens_enqueue_step(dmph_ensemble *e, cudaGraph_t g)
                 enqueue_rebuild(c, false, c->st);
                 c->launches += rebuild_launches(c, false);
                 c->host_rebuilds++;
+            }
+            if (e->use_list && c->Wm.moving) {
+                launch_list_wall_guard(c->dB, c->st);
+                c->launches++;
             }
         }
     }

@@ -82,7 +82,7 @@ void enqueue_passes(dmph_ctx *ctx, cudaStream_t st);
 void enqueue_pair_passes32(dmph_ctx *ctx, cudaStream_t st);
 void enqueue_dem(dmph_ctx *ctx, cudaStream_t st);
 long long dem_launches(const dmph_ctx *ctx);
-long long tail_launches(const dmph_ctx *ctx);
+long long tail_launches(const dmph_ctx *ctx, bool graph = false);
 void advance_host_clock(dmph_ctx *ctx);
 int step_once(dmph_ctx *ctx);
 int read_bounds(dmph_ctx *ctx, int *b);

@@ -89,6 +89,7 @@ enum DevBound {
     B_NEED = 7,     // rebuild decided for this step
     B_REBUILDS = 8, // rebuilds since creation
     B_LIST_OVF = 9, // a Verlet list of the last rebuild overflowed (FP32 list mode): stencil passes run
+    B_LIST_SPLIT = 10, // the FP32 lists hold no wall-wall pairs (built with the walls at rest)
     B_COUNT = 16
 };
 

@@ -543,17 +543,27 @@ __device__ __forceinline__ void pass_b32_body(const DevParams &P, const DevParam
 // rebuild is in the list.  The passes then run one thread per particle over
 // its list instead of over the ~800 candidates of the 27-cell stencil.
 struct TileL {
-    float4 p[kWarp];     // position in the frame of the warp's cell
-    unsigned e[kWarp];   // j | cell-offset code << 24
+    float4 p[kWarp];     // position in the frame of the warp's cell, .w = type bits
+    unsigned e[kWarp];   // list entry of the candidate
 };
 
-__global__ void __launch_bounds__(8 * kWarp) k_build_list32(DevParams P, DevParams32 Q, DevState S, int *dB, float rc2)
+// split: the walls are at rest until the next rebuild (set by the host when no
+// wall motion is active).  Wall-wall pairs are then summed here, once, with
+// pass A's arithmetic (pair_a32 on the same FP32 positions), and only the
+// pairs of a wall with fluid or debris go to its list; every entry whose j is
+// a wall carries kEntryStaticWall, so pass A skips gathering its (zero)
+// velocity.
+template <bool ST>
+__global__ void __launch_bounds__(8 * kWarp) k_build_list32(DevParams P, DevParams32 Q, DevState S, int *dB, float rc2,
+                                                            int split)
 {
     __shared__ TileL tiles[8];
     TileL &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int cap = S.nbl_cap;
     const long long ld = P.N;
+    const float cut2 = ST ? fmaxf(Q.RP2, fmaxf(Q.RA2, Q.RG2)) : Q.RP2;  // pass A's
+    if (blockIdx.x == 0 && threadIdx.x == 0) dB[B_LIST_SPLIT] = split;
     FOR_EACH_CHUNK(dB, CR_WET, 8, cidx)
     {
         const Chunk ch = S.chunks[cidx];
@@ -563,18 +573,24 @@ __global__ void __launch_bounds__(8 * kWarp) k_build_list32(DevParams P, DevPara
         int cix, ciy, ciz;
         chunk_cell(P, key_cell, cix, ciy, ciz);
         const float4 pi = S.p4[active ? i : ch.i0];
+        const int ti = unpack_type(__float_as_uint(pi.w));
+        const bool wall_i = split && is_wall(ti);
+        const IA I{pi, make_float4(0.f, 0.f, 0.f, 0.f), ti, is_solid(ti), is_wall(ti)};
+        AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
         int cnt = 0;
         traverse_stencil_batched(
             P, S.cell_start, key_cell, lane, 7u,
             [&](int j, int slot) {
                 const float4 pj = S.p4[j];
                 const unsigned w = __float_as_uint(pj.w);
+                const int tj = unpack_type(w);
                 const int dx = min_image_cell(unpack_cx(w) - cix, P.cc[0]);
                 const int dy = min_image_cell(unpack_cy(w) - ciy, P.cc[1]);
                 const int dz = min_image_cell(unpack_cz(w) - ciz, P.cc[2]);
                 tl.p[slot] = make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
-                                         fmaf((float)dz, Q.cw[2], pj.z), 0.f);
-                tl.e[slot] = (unsigned)j | ((unsigned)((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)) << 24);
+                                         fmaf((float)dz, Q.cw[2], pj.z), __int_as_float(tj));
+                tl.e[slot] = (unsigned)j | ((unsigned)((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)) << 24) |
+                             (split && is_wall(tj) ? kEntryStaticWall : 0u);
             },
             [&](int base, int nb) {
                 if (!active) return;
@@ -590,14 +606,34 @@ __global__ void __launch_bounds__(8 * kWarp) k_build_list32(DevParams P, DevPara
                 while (m) {  // ascending candidate order
                     const int s = __ffs(m) - 1;
                     m &= m - 1;
-                    if (cnt < cap) S.nbl[list_index(cnt, i, ld)] = tl.e[s];
+                    const unsigned e = tl.e[s];
+                    if (wall_i && (e & kEntryStaticWall)) {
+                        const float4 pj = tl.p[s];
+                        const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+                        if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= cut2)
+                            pair_a32<ST>(Q, I, pj, make_float4(0.f, 0.f, 0.f, 0.f), A);
+                        continue;
+                    }
+                    if (cnt < cap) S.nbl[list_index(cnt, i, ld)] = e;
                     ++cnt;
                 }
             });
         if (!active) continue;
         if (cnt > cap) atomicExch(dB + B_LIST_OVF, 1);
         S.nbn[i] = cnt < cap ? cnt : cap;
+        if (wall_i) {
+            S.vsp_st[i] = A.vsp;
+            S.st4[i] = make_float4(A.dA, A.g0, A.g1, A.g2);
+        }
     }
+}
+
+// Lists built with the walls at rest become invalid once a wall moves: the
+// step enqueues this guard in a moving-wall window, and the stencil passes
+// stand in until a rebuild makes complete lists.
+__global__ void k_list_wall_guard(int *dB)
+{
+    if (dB[B_LIST_SPLIT]) dB[B_LIST_OVF] = 1;
 }
 
 // entries k0 .. k0 + BATCH - 1 of slot i (BATCH divides 8, so they sit in one
@@ -627,8 +663,8 @@ __device__ __forceinline__ void load_entries(const DevState &S, int k0, int cnt,
 // j's position in the frame of i's cell, type bits in .w
 __device__ __forceinline__ float4 list_pos(const DevParams32 &Q, const DevState &S, unsigned e, int &j)
 {
-    j = (int)(e & 0xFFFFFFu);
-    const int code = (int)(e >> 24);
+    j = (int)(e & kEntrySlot);
+    const int code = entry_code(e);
     const int dx = code / 9 - 1, dy = (code / 3) % 3 - 1, dz = code % 3 - 1;
     const float4 pj = __ldg(S.p4 + j);  // positions are read-only in the passes
     return make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
@@ -637,8 +673,11 @@ __device__ __forceinline__ float4 list_pos(const DevParams32 &Q, const DevState 
 
 // BATCH list entries at a time: their index loads, then their gathers, are
 // independent, so the latencies overlap; pairs are still taken in list order
+// split: the lists of the last rebuild hold no wall-wall pairs; a wall's sums
+// start from the ones the build made of them
 template <bool ST, int BATCH>
-__device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const DevParams32 &Q, const DevState &S, int i)
+__device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const DevParams32 &Q, const DevState &S, int i,
+                                                   int split)
 {
     const int cnt = S.nbn[i];
     if (cnt < 0) return;
@@ -648,6 +687,16 @@ __device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const Dev
     const int ti = unpack_type(__float_as_uint(pi.w));
     const IA I{pi, S.v4[i], ti, is_solid(ti), is_wall(ti)};
     AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
+    if (split && I.wi) {
+        A.vsp = S.vsp_st[i];
+        if (ST) {
+            const float4 t = S.st4[i];
+            A.dA = t.x;
+            A.g0 = t.y;
+            A.g1 = t.z;
+            A.g2 = t.w;
+        }
+    }
     for (int k0 = 0; k0 < cnt; k0 += BATCH) {
         unsigned e[BATCH];
         load_entries<BATCH>(S, k0, cnt, i, ld, e);
@@ -656,8 +705,9 @@ __device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const Dev
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {
             pj[u] = list_pos(Q, S, e[u], j[u]);
-            // pass A writes only the .w (pressure) of v4, which it does not read
-            vj[u] = __ldg(S.v4 + j[u]);
+            // pass A writes only the .w (pressure) of v4, which it does not
+            // read; a wall at rest has zero velocity, which is not gathered
+            vj[u] = (e[u] & kEntryStaticWall) ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(S.v4 + j[u]);
         }
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {
@@ -672,8 +722,9 @@ template <bool ST, int BATCH, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_pass_a32_list(DevParams P, DevParams32 Q, DevState S, const int *dB)
 {
     if (dB[B_LIST_OVF]) return;
+    const int split = dB[B_LIST_SPLIT];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.N; i += gridDim.x * blockDim.x)
-        pass_a32_list_slot<ST, BATCH>(P, Q, S, i);
+        pass_a32_list_slot<ST, BATCH>(P, Q, S, i, split);
 }
 
 // CLS: 0 = slot i holds fluid, 1 = debris, 2 = either.  The single-scene
@@ -883,8 +934,9 @@ __global__ void __launch_bounds__(256) k_ens_pass_list(const EnsScene *__restric
             if (e.P.surface_tension) pass_b32_list_slot<true, 2>(e.P, e.Q, e.S, i);
             else pass_b32_list_slot<false, 2>(e.P, e.Q, e.S, i);
         } else {
-            if (e.P.surface_tension) pass_a32_list_slot<true, 2>(e.P, e.Q, e.S, i);
-            else pass_a32_list_slot<false, 2>(e.P, e.Q, e.S, i);
+            const int split = e.dB[B_LIST_SPLIT];
+            if (e.P.surface_tension) pass_a32_list_slot<true, 2>(e.P, e.Q, e.S, i, split);
+            else pass_a32_list_slot<false, 2>(e.P, e.Q, e.S, i, split);
         }
     }
 }
@@ -1213,12 +1265,23 @@ void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S
 #undef DMPH_LAUNCH_B
 }
 
-void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, cudaStream_t st)
+void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, int split,
+                         cudaStream_t st)
 {
     cudaMemsetAsync(dB + B_LIST_OVF, 0, sizeof(int), st);
     cudaMemsetAsync(S.nbn, 0xFF, sizeof(int) * (size_t)P.N, st);
-    static const int g = grid_for(k_build_list32, 8 * kWarp);
-    k_build_list32<<<g, 8 * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2);
+    if (P.surface_tension) {
+        static const int g = grid_for(k_build_list32<true>, 8 * kWarp);
+        k_build_list32<true><<<g, 8 * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2, split);
+    } else {
+        static const int g = grid_for(k_build_list32<false>, 8 * kWarp);
+        k_build_list32<false><<<g, 8 * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2, split);
+    }
+}
+
+void launch_list_wall_guard(int *dB, cudaStream_t st)
+{
+    k_list_wall_guard<<<1, 1, 0, st>>>(dB);
 }
 
 // list-pass variants the autotuner chooses from: entries per batch x

@@ -51,7 +51,9 @@ void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S
                      cudaStream_t st, int gate = 0);
 void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
                      cudaStream_t st, int gate = 0);
-void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, cudaStream_t st);
+void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, int split,
+                         cudaStream_t st);
+void launch_list_wall_guard(int *dB, cudaStream_t st);
 void launch_pass_a32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
                           cudaStream_t st);
 void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,

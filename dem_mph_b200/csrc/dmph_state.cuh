@@ -8,11 +8,18 @@ namespace dmph {
 struct DevState {
     // FP32 Verlet lists (list mode): entry k of slot i at
     // nbl[((k / 8) * N + i) * 8 + k % 8] = j | cell-offset code << 24 (code =
-    // (dx+1)*9 + (dy+1)*3 + (dz+1) of j's rebuild-time cell relative to i's),
-    // ascending j; nbn[i] = count, -1 for slots without a list (dry walls)
+    // (dx+1)*9 + (dy+1)*3 + (dz+1) of j's rebuild-time cell relative to i's)
+    // | kEntryStaticWall when j is a wall that stays put until the next
+    // rebuild; ascending j; nbn[i] = count, -1 for slots without a list (dry
+    // walls).  Lists built with the walls at rest (dB[B_LIST_SPLIT] = 1) leave
+    // the wall-wall pairs out of the walls' lists: their pass-A sums cannot
+    // change before the next rebuild and are kept in vsp_st (FP64 strain sum)
+    // and st4 (surface-tension density sum, gravity-centre sum)
     unsigned *nbl;
     int *nbn;
     int nbl_cap;
+    double *vsp_st;
+    float4 *st4;
     // FP64 particle state, component planes v[d*N + i], current sorted order
     double *pos, *vel, *frc, *xref;
     int *type, *pidx;
@@ -75,6 +82,10 @@ struct DevBodies {
 // each particle's sectors one entry after the other, and a warp of consecutive
 // slots reads entry k of its 32 particles from 32 sectors that also hold the
 // particles' next entries.
+constexpr unsigned kEntrySlot = 0xFFFFFFu;        // j
+constexpr unsigned kEntryStaticWall = 1u << 29;    // j is a wall at rest
+__host__ __device__ __forceinline__ int entry_code(unsigned e) { return (int)((e >> 24) & 31u); }
+
 __host__ __device__ __forceinline__ long long list_index(int k, int i, long long ld)
 {
     return (((long long)(k >> 3)) * ld + i) * 8 + (k & 7);
