@@ -198,7 +198,7 @@ void dmph::enqueue_dem(dmph_ctx *ctx, cudaStream_t st)
         launch_solid_force_to64(P, S, dB, st);
         for (int k = 0; k < ctx->demSteps; ++k) {
             if (ctx->Bd.B > 0) {
-                launch_clump_dem(P, S, dB, st);
+                launch_clump_dem(P, S, dB, ctx->use_list, st);
                 launch_body_step(P, S, ctx->Bd, true, st);
                 continue;
             }
@@ -210,7 +210,7 @@ void dmph::enqueue_dem(dmph_ctx *ctx, cudaStream_t st)
     } else {
         for (int k = 0; k < ctx->demSteps; ++k) {
             if (ctx->Bd.B > 0) {
-                launch_clump_dem(P, S, dB, st);
+                launch_clump_dem(P, S, dB, false, st);
                 launch_body_step(P, S, ctx->Bd, false, st);
                 continue;
             }
@@ -231,7 +231,10 @@ static void enqueue_tail(dmph_ctx *ctx, cudaStream_t st)
 
 long long dmph::dem_launches(const dmph_ctx *ctx)
 {
-    const long long dem = ctx->Bd.B > 0 ? 2 : 2 + (ctx->P.wall_dem_coeffs ? 1 : 0);
+    // clump contacts (FP32 list mode: list walk and gated cell walk) and the
+    // body update, or the reference's DEM force(s) and integration
+    const long long dem =
+        ctx->Bd.B > 0 ? (ctx->fp32 && ctx->use_list ? 3 : 2) : 2 + (ctx->P.wall_dem_coeffs ? 1 : 0);
     return ctx->demSteps * dem + (ctx->fp32 ? 2 : 0);
 }
 

@@ -13,8 +13,9 @@
 //      the contact midpoint, so the offset torque 0.5 q x F is kept too; pair
 //      forces are antisymmetric and total linear and angular momentum of
 //      colliding bodies are conserved.
-//   2. k_body_step: one warp per body reduces, in FP64 with warp shuffles,
-//      the total force F = sum(fluid + contact) and torque
+//   2. k_body_step: one block per body reduces, in FP64 (warp shuffles, then
+//      across the block's warps in a fixed order), the total force
+//      F = sum(fluid + contact) and torque
 //      T = sum(R r0 x f + contact offset torques) over its members (gathered
 //      through slot_of_row, so the reduction order is the body's fixed member
 //      order, independent of the cell sort), then advances the body in FP64:
@@ -32,14 +33,79 @@ __global__ void k_slot_of_row(int N, const int *__restrict__ pidx, int *__restri
     if (i < N) slot_of_row[pidx[i]] = i;
 }
 
+// Contact of debris particle i (position xi, velocity vi, type ti, body bi,
+// mass mi) with candidate j: skipped when j is i, of the same body, or not
+// within dx; otherwise the pair force and the offset torque are added to F, T.
+__device__ __forceinline__ void clump_pair(const DevParams &P, const DevState &S, int i, const double *xi,
+                                           const double *vi, int ti, int bi, double mi, int j, double *F, double *T)
+{
+    const int N = P.N;
+    if (j == i) return;
+    const int bj = S.bid[j];
+    if (bi >= 0 && bj == bi) return;
+    double q[3];
+    for (int k = 0; k < 3; k++) {
+        q[k] = S.pos[k * N + j] - xi[k];
+        q[k] -= P.W[k] * rint(q[k] / P.W[k]);
+    }
+    const double r2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+    if (r2 > P.dx2 || r2 <= 0.0) return;
+    const int tj = S.type[j];
+    const double r = sqrt(r2);
+    const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
+    const double ov = P.dx - r;
+    const double u[3] = {S.vel[j] - vi[0], S.vel[N + j] - vi[1], S.vel[2 * N + j] - vi[2]};
+    const double un = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
+    const double mj = (bj >= 0 ? S.body_rho[bj] : P.density[tj]) * P.V;
+    const double mij = mi * mj / (mi + mj);
+    const double kn = (4.0 / 3.0) * P.Eeff[ti][tj] * sqrt(P.Reff * ov);
+    const double cn = sqrt(mij * kn) * P.pairDamp[ti][tj];
+    const double kt = P.KtFac[ti][tj] * sqrt(P.Reff * sqrt(ov));
+    const double ct = sqrt(mij * kt) * P.pairDamp[ti][tj];
+    double f[3], ut[3];
+    const double fnm = fmin(-kn * ov + cn * un, 0.0);  // no adhesion
+    for (int k = 0; k < 3; k++) {
+        f[k] = fnm * e[k];
+        ut[k] = u[k] - un * e[k];
+    }
+    const double ctot = ct + kt * P.ddt;
+    const double aut = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
+    const double cap = P.pairFric[ti][tj] * fabs(fnm);
+    const double ft = ctot * aut > cap && aut > 0.0 ? cap / aut : ctot;
+    for (int k = 0; k < 3; k++) f[k] += ft * ut[k];
+    for (int k = 0; k < 3; k++) F[k] += f[k];
+    // offset of the contact midpoint from the particle centre: 0.5 q
+    T[0] += 0.5 * (q[1] * f[2] - q[2] * f[1]);
+    T[1] += 0.5 * (q[2] * f[0] - q[0] * f[2]);
+    T[2] += 0.5 * (q[0] * f[1] - q[1] * f[0]);
+}
+
+__device__ __forceinline__ void clump_store(const DevParams &P, const DevState &S, int i, int lane, double *F,
+                                            double *T)
+{
+    const int N = P.N;
+    for (int k = 0; k < 3; k++) {
+        F[k] = warp_sum(F[k]);
+        T[k] = warp_sum(T[k]);
+    }
+    if (lane == 0)
+        for (int k = 0; k < 3; k++) {
+            S.frc_dem[k * N + i] = F[k];
+            S.frc_dem[(3 + k) * N + i] = T[k];
+        }
+}
+
 // One warp per debris particle i (slots [sb, se) walked by a persistent
 // grid); the lanes stride over the candidates of the neighbour cells that
 // can hold a contact partner: contacts need |x_j - x_i| <= dx, so only the
 // neighbour cells within 1.6 dx of i's rebuild-time position (about 8 of the
 // 27) are visited, for the solid and wall classes.  FP64 on the master
-// planes; per-lane partial sums are combined with warp shuffles.
-__global__ void __launch_bounds__(8 * kWarp) k_clump_dem(DevParams P, DevState S, const int *dB)
+// planes; per-lane partial sums are combined with warp shuffles.  gate: the
+// FP32 Verlet lists are in use, and this walk stands in only after a list
+// overflow.
+__global__ void __launch_bounds__(8 * kWarp) k_clump_dem(DevParams P, DevState S, const int *dB, int gate)
 {
+    if (gate && dB[B_LIST_OVF] == 0) return;
     const int lane = threadIdx.x & 31;
     const int N = P.N;
     const int sb = dB[B_SB], se = dB[B_SE];
@@ -89,72 +155,59 @@ __global__ void __launch_bounds__(8 * kWarp) k_clump_dem(DevParams P, DevState S
         }
         for (int r = 0; r < nranges; ++r) {
             const int jb = __shfl_sync(kFull, rb, r), je = __shfl_sync(kFull, re, r);
-            for (int j = jb + lane; j < je; j += kWarp) {
-                if (j == i) continue;
-                const int bj = S.bid[j];
-                if (bi >= 0 && bj == bi) continue;
-                double q[3];
-                for (int k = 0; k < 3; k++) {
-                    q[k] = S.pos[k * N + j] - xi[k];
-                    q[k] -= P.W[k] * rint(q[k] / P.W[k]);
-                }
-                const double r2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
-                if (r2 > P.dx2 || r2 <= 0.0) continue;
-                const int tj = S.type[j];
-                const double r = sqrt(r2);
-                const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
-                const double ov = P.dx - r;
-                const double u[3] = {S.vel[j] - vi[0], S.vel[N + j] - vi[1], S.vel[2 * N + j] - vi[2]};
-                const double un = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
-                const double mj = (bj >= 0 ? S.body_rho[bj] : P.density[tj]) * P.V;
-                const double mij = mi * mj / (mi + mj);
-                const double kn = (4.0 / 3.0) * P.Eeff[ti][tj] * sqrt(P.Reff * ov);
-                const double cn = sqrt(mij * kn) * P.pairDamp[ti][tj];
-                const double kt = P.KtFac[ti][tj] * sqrt(P.Reff * sqrt(ov));
-                const double ct = sqrt(mij * kt) * P.pairDamp[ti][tj];
-                double f[3], ut[3];
-                const double fnm = fmin(-kn * ov + cn * un, 0.0);  // no adhesion
-                for (int k = 0; k < 3; k++) {
-                    f[k] = fnm * e[k];
-                    ut[k] = u[k] - un * e[k];
-                }
-                const double ctot = ct + kt * P.ddt;
-                const double aut = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
-                const double cap = P.pairFric[ti][tj] * fabs(fnm);
-                const double ft = ctot * aut > cap && aut > 0.0 ? cap / aut : ctot;
-                for (int k = 0; k < 3; k++) f[k] += ft * ut[k];
-                for (int k = 0; k < 3; k++) F[k] += f[k];
-                // offset of the contact midpoint from the particle centre: 0.5 q
-                T[0] += 0.5 * (q[1] * f[2] - q[2] * f[1]);
-                T[1] += 0.5 * (q[2] * f[0] - q[0] * f[2]);
-                T[2] += 0.5 * (q[0] * f[1] - q[1] * f[0]);
-            }
+            for (int j = jb + lane; j < je; j += kWarp) clump_pair(P, S, i, xi, vi, ti, bi, mi, j, F, T);
         }
-        for (int k = 0; k < 3; k++) {
-            F[k] = warp_sum(F[k]);
-            T[k] = warp_sum(T[k]);
-        }
-        if (lane == 0)
-            for (int k = 0; k < 3; k++) {
-                S.frc_dem[k * N + i] = F[k];
-                S.frc_dem[(3 + k) * N + i] = T[k];
-            }
+        clump_store(P, S, i, lane, F, T);
     }
 }
 
-template <bool F32>
-__global__ void k_body_step(DevParams P, DevState S, DevBodies Bd)
+// FP32 list mode: one warp per debris particle over its Verlet list (radius
+// MaxRadius + MARGIN, far beyond the contact distance dx plus any drift
+// before the next rebuild), whose entries carry the class of j, so the fluid
+// entries are passed over without a gather.
+__global__ void __launch_bounds__(8 * kWarp) k_clump_dem_list(DevParams P, DevState S, const int *dB)
 {
-    const int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (dB[B_LIST_OVF]) return;
     const int lane = threadIdx.x & 31;
-    if (b >= Bd.B) return;
+    const int N = P.N;
+    const long long ld = N;
+    const int sb = dB[B_SB], se = dB[B_SE];
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    for (int i = sb + blockIdx.x * (blockDim.x >> 5) + (int)(threadIdx.x >> 5); i < se; i += nwarps) {
+        const int cnt = S.nbn[i];
+        const double xi[3] = {S.pos[i], S.pos[N + i], S.pos[2 * N + i]};
+        const double vi[3] = {S.vel[i], S.vel[N + i], S.vel[2 * N + i]};
+        const int ti = S.type[i];
+        const int bi = S.bid[i];
+        const double mi = particle_density(S, P, i, ti) * P.V;
+        double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
+        for (int k = lane; k < cnt; k += kWarp) {
+            const unsigned e = __ldg(S.nbl + list_index(k, i, ld));
+            if (e & (kEntrySolid | kEntryWall)) clump_pair(P, S, i, xi, vi, ti, bi, mi, (int)(e & kEntrySlot), F, T);
+        }
+        clump_store(P, S, i, lane, F, T);
+    }
+}
+
+// One block per body: its threads take the members, the per-thread sums are
+// reduced by warp shuffles and then across the block's warps in warp order
+constexpr int kBodyThreads = 256;
+
+template <bool F32>
+__global__ void __launch_bounds__(kBodyThreads) k_body_step(DevParams P, DevState S, DevBodies Bd)
+{
+    constexpr int NW = kBodyThreads / kWarp;
+    __shared__ double red[NW][6];
+    __shared__ double tot[6];
+    const int b = blockIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int N = P.N;
     const int m0 = Bd.ptr[b], m1 = Bd.ptr[b + 1];
     double q[4] = {Bd.q[4 * b], Bd.q[4 * b + 1], Bd.q[4 * b + 2], Bd.q[4 * b + 3]};
     double R[3][3];
     quat_to_R(q, R);
     double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
-    for (int m = m0 + lane; m < m1; m += kWarp) {
+    for (int m = m0 + (int)threadIdx.x; m < m1; m += kBodyThreads) {
         const int i = Bd.slot_of_row[Bd.member_row[m]];
         double f[3];
         if (F32) {
@@ -178,7 +231,23 @@ __global__ void k_body_step(DevParams P, DevState S, DevBodies Bd)
         F[k] = warp_sum(F[k]);
         T[k] = warp_sum(T[k]);
     }
-    // integrate (every lane holds the same values)
+    if (lane == 0)
+        for (int k = 0; k < 3; k++) {
+            red[wid][k] = F[k];
+            red[wid][3 + k] = T[k];
+        }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double a = 0.0;
+        for (int w = 0; w < NW; ++w) a += red[w][threadIdx.x];
+        tot[threadIdx.x] = a;
+    }
+    __syncthreads();
+    for (int k = 0; k < 3; k++) {
+        F[k] = tot[k];
+        T[k] = tot[3 + k];
+    }
+    // integrate (every thread holds the same values)
     const double dt = P.ddt, M = Bd.M[b];
     double X[3], V[3], L[3];
     for (int k = 0; k < 3; k++) {
@@ -203,7 +272,7 @@ __global__ void k_body_step(DevParams P, DevState S, DevBodies Bd)
     }
     quat_to_R(q, R);
     omega_of(R, Ii, L, w);
-    if (lane == 0) {
+    if (threadIdx.x == 0) {
         for (int k = 0; k < 3; k++) {
             Bd.X[3 * b + k] = X[k];
             Bd.V[3 * b + k] = V[k];
@@ -214,7 +283,7 @@ __global__ void k_body_step(DevParams P, DevState S, DevBodies Bd)
         for (int k = 0; k < 4; k++) Bd.q[4 * b + k] = q[k];
     }
     // place the members
-    for (int m = m0 + lane; m < m1; m += kWarp) {
+    for (int m = m0 + (int)threadIdx.x; m < m1; m += kBodyThreads) {
         const int i = Bd.slot_of_row[Bd.member_row[m]];
         const double *r0 = Bd.r0 + 3 * m;
         double r[3], x[3], v[3];
@@ -254,19 +323,21 @@ void launch_slot_of_row(const DevParams &P, const int *pidx, int *slot_of_row, c
 // FP64 state of solids and walls (in the FP32 split mode these planes are the
 // solids' and walls' master copies, refreshed into the FP32 arrays after the
 // substeps), so the template's FP32 branches are not instantiated.
-void launch_clump_dem(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
+void launch_clump_dem(const DevParams &P, const DevState &S, const int *dB, bool lists, cudaStream_t st)
 {
+    if (lists) {
+        static const int gl = persistent_grid((const void *)k_clump_dem_list, 8 * kWarp);
+        k_clump_dem_list<<<gl, 8 * kWarp, 0, st>>>(P, S, dB);
+    }
     static const int g = persistent_grid((const void *)k_clump_dem, 8 * kWarp);
-    k_clump_dem<<<g, 8 * kWarp, 0, st>>>(P, S, dB);
+    k_clump_dem<<<g, 8 * kWarp, 0, st>>>(P, S, dB, lists ? 1 : 0);
 }
 
 void launch_body_step(const DevParams &P, const DevState &S, const DevBodies &Bd, bool f32, cudaStream_t st)
 {
     (void)f32;
     if (Bd.B <= 0) return;
-    const int threads = 128;
-    const int blocks = (Bd.B * kWarp + threads - 1) / threads;
-    k_body_step<false><<<blocks, threads, 0, st>>>(P, S, Bd);
+    k_body_step<false><<<Bd.B, kBodyThreads, 0, st>>>(P, S, Bd);
 }
 
 }  // namespace dmph

@@ -590,7 +590,8 @@ __global__ void __launch_bounds__(8 * kWarp) k_build_list32(DevParams P, DevPara
                 tl.p[slot] = make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
                                          fmaf((float)dz, Q.cw[2], pj.z), __int_as_float(tj));
                 tl.e[slot] = (unsigned)j | ((unsigned)((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)) << 24) |
-                             (split && is_wall(tj) ? kEntryStaticWall : 0u);
+                             (is_solid(tj) ? kEntrySolid : 0u) |
+                             (is_wall(tj) ? (split ? kEntryWall | kEntryStaticWall : kEntryWall) : 0u);
             },
             [&](int base, int nb) {
                 if (!active) return;

@@ -77,7 +77,7 @@ void launch_widen_f4(const float4 *in, double *out, int count, int stride, cudaS
 
 // dmph_bodies.cu
 void launch_slot_of_row(const DevParams &P, const int *pidx, int *slot_of_row, cudaStream_t st);
-void launch_clump_dem(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
+void launch_clump_dem(const DevParams &P, const DevState &S, const int *dB, bool lists, cudaStream_t st);
 void launch_body_step(const DevParams &P, const DevState &S, const DevBodies &Bd, bool f32, cudaStream_t st);
 
 void launch_xyz_to_planes(const double *xyz, double *planes, int n, cudaStream_t st);

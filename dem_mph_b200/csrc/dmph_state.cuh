@@ -9,8 +9,8 @@ struct DevState {
     // FP32 Verlet lists (list mode): entry k of slot i at
     // nbl[((k / 8) * N + i) * 8 + k % 8] = j | cell-offset code << 24 (code =
     // (dx+1)*9 + (dy+1)*3 + (dz+1) of j's rebuild-time cell relative to i's)
-    // | kEntryStaticWall when j is a wall that stays put until the next
-    // rebuild; ascending j; nbn[i] = count, -1 for slots without a list (dry
+    // | j's class (kEntrySolid, kEntryWall) | kEntryStaticWall when j is a
+    // wall that stays put until the next rebuild; ascending j; nbn[i] = count, -1 for slots without a list (dry
     // walls).  Lists built with the walls at rest (dB[B_LIST_SPLIT] = 1) leave
     // the wall-wall pairs out of the walls' lists: their pass-A sums cannot
     // change before the next rebuild and are kept in vsp_st (FP64 strain sum)
@@ -84,6 +84,8 @@ struct DevBodies {
 // particles' next entries.
 constexpr unsigned kEntrySlot = 0xFFFFFFu;        // j
 constexpr unsigned kEntryStaticWall = 1u << 29;    // j is a wall at rest
+constexpr unsigned kEntrySolid = 1u << 30;         // j is debris
+constexpr unsigned kEntryWall = 1u << 31;          // j is a wall
 __host__ __device__ __forceinline__ int entry_code(unsigned e) { return (int)((e >> 24) & 31u); }
 
 __host__ __device__ __forceinline__ long long list_index(int k, int i, long long ld)
