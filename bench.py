@@ -165,6 +165,8 @@ def main():
                     help="untimed steps run before warm-up so the flow is moving and rebuilds fire in the timed steps")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels one by one instead of graph replay")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch variants of the pair passes")
+    ap.add_argument("--variants", type=int, nargs=2, default=None, metavar=("A", "B"),
+                    help="set the pair-pass launch variants (pass A, pass B) instead of autotuning")
     ap.add_argument("--surrogate", action="store_true",
                     help="plain vs surrogate sim-s/hour and surge-front / debris-centroid error (config1 by default)")
     ap.add_argument("--substeps", type=int, default=8, help="surrogate K")
@@ -206,7 +208,10 @@ def main():
     n = scene.n
     g.step(args.settle)
     variants = None
-    if args.precision == "fp32" and not args.no_autotune:
+    if args.variants is not None:
+        g.set_variants(*args.variants)
+        variants = list(args.variants)
+    elif args.precision == "fp32" and not args.no_autotune:
         va, vb, _, _ = g.autotune()
         variants = [va, vb]
     if not args.no_graph:
