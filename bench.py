@@ -257,16 +257,27 @@ def main():
         bytes_launch = n * (bpp - 24)
         dur = pa_ms / max(pa_n, 1)
     achieved = bytes_launch / (dur / 1e3) / 1e9
-    # DRAM bytes of one pass-B list launch on config 2 from an ncu capture
+    # DRAM bytes of one list-pass launch on config 2 from an ncu capture
     # (dram__bytes_read.sum + dram__bytes_write.sum); the list is most of it
-    traffic = 679.4e6 if (args.workload == "config2" and args.precision == "fp32" and top == "pass_b") else None
-    roofline = {"bound": "hbm", "kernel": ("k_pass_b32_list" if args.precision == "fp32" and top == "pass_b"
-                                           else "k_" + top),
+    traffic = None
+    if args.workload == "config2" and args.precision == "fp32":
+        traffic = 685.2e6 if top == "pass_b" else 745.9e6
+    # pair work: Verlet-list entries each pass walks per launch (each entry is
+    # one candidate pair: two 16-byte neighbour gathers and the pair arithmetic)
+    ea, eb = g.list_stats()
+    pa_dur, pb_dur = pa_ms / max(pa_n, 1), pb_ms / max(pb_n, 1)
+    pairs = {"pass_a": {"entries_per_launch": ea, "launch_ms": pa_dur, "entries_per_s": ea / (pa_dur / 1e3)},
+             "pass_b": {"entries_per_launch": eb, "launch_ms": pb_dur, "entries_per_s": eb / (pb_dur / 1e3)},
+             "bound": "L1 data pipe serving the neighbour gathers (about 75% of peak in the ncu capture) "
+                      "and instruction issue (about 76%)"}
+    roofline = {"bound": "hbm", "kernel": (("k_pass_b32_list" if top == "pass_b" else "k_pass_a32_list")
+                                           if args.precision == "fp32" else "k_" + top),
                 "achieved": achieved, "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                 "traffic_source": "ncu capture of one launch of the same kernel and workload" if traffic else None,
                 "peak_source": peak_src, "launch_ms": dur,
-                "phase_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in ph.items()}}
+                "phase_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in ph.items()},
+                "pairs": pairs}
 
     # ---- end to end through the C ABI with host buffers: every step uploads
     # the particle state from pinned host memory, steps, reads it back

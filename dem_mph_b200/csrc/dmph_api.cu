@@ -764,6 +764,49 @@ extern "C" int dmph_get_info(dmph_ctx *ctx, dmph_info *info)
     return DMPH_OK;
 }
 
+// sums of the list lengths over all slots and over the fluid and debris slots
+__global__ void k_list_stats(const int *__restrict__ nbn, int n, const int *__restrict__ dB,
+                             unsigned long long *__restrict__ out)
+{
+    const int se = dB[B_SE];
+    unsigned long long a = 0, b = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int c = nbn[i];
+        if (c > 0) {
+            a += (unsigned long long)c;
+            if (i < se) b += (unsigned long long)c;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, a);
+        atomicAdd(out + 1, b);
+    }
+}
+
+extern "C" int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64_t *entries_pass_b)
+{
+    if (!ctx) return DMPH_EINVAL;
+    unsigned long long h[2] = {0, 0};
+    if (ctx->use_list) {
+        if (!ctx->stats) {  // two counters, allocated on first use
+            const int rc = dalloc(ctx, &ctx->stats, 2);
+            if (rc) return rc;
+        }
+        CK(cudaMemsetAsync(ctx->stats, 0, 2 * sizeof(unsigned long long), ctx->st));
+        k_list_stats<<<ctx->sms * 4, 256, 0, ctx->st>>>(ctx->S.nbn, ctx->P.N, ctx->dB, ctx->stats);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(h, ctx->stats, sizeof(h), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    if (entries_pass_a) *entries_pass_a = (int64_t)h[0];
+    if (entries_pass_b) *entries_pass_b = (int64_t)h[1];
+    return DMPH_OK;
+}
+
 extern "C" int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind, int64_t capacity)
 {
     if (!ctx || !ptr) return DMPH_EINVAL;

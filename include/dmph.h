@@ -220,11 +220,20 @@ int dmph_get_info(dmph_ctx *ctx, dmph_info *info);
  * source/DEM-MPH.cpp:1521-1851): for every particle, all particles within
  * MaxRadius+MARGIN at the last rebuild, fluid then solid then wall cells of
  * the periodic 3x3(x3) stencil; ptr has n+1 entries.  Call first with
- * ind == NULL to get the total count in *ptr[n].  The timestep path never
- * materialises this list (it traverses the same cells directly); this entry
- * point exists so the neighbour sets can be checked against the reference.
+ * ind == NULL to get the total count in *ptr[n].  This CSR copy is made on
+ * demand, so the neighbour sets can be checked against the reference; the
+ * timestep keeps its own per-particle lists (dmph_set_pair_mode).
  */
 int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind, int64_t capacity);
+
+/*
+ * Size of the pair work of the current Verlet lists (no counterpart in the
+ * reference): the entries pass A walks (all particles with a list) and those
+ * pass B walks (fluid and debris).  In the FP32 build, lists made with the
+ * walls at rest hold no wall-wall pairs.  Either pointer may be NULL; both
+ * read 0 in stencil mode.
+ */
+int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64_t *entries_pass_b);
 
 /*
  * Rigid debris bodies (no counterpart in the reference, whose debris particles

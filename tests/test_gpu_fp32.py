@@ -171,3 +171,21 @@ def test_fp32_drag_at_rest_on_the_cutoff_stays_finite():
     _, xs, vs, _ = g.state()
     assert np.all(np.isfinite(xs)) and np.all(np.isfinite(vs)) and np.all(np.isfinite(g.field("Force")))
     g.close()
+
+
+def test_list_stats_count_the_list_entries():
+    """dmph_get_list_stats: pass B walks the fluid and debris lists, pass A
+    those and the lists of walls with fluid in reach (without wall-wall
+    pairs); stencil mode has no lists."""
+    p, typ, x, v = load_scene("small3d")
+    p.precision = PRECISION_FP32_SPLIT
+    g = solver.Solver(p, typ, x, v)
+    g.step(2)
+    ea, eb = g.list_stats()
+    t = g.state()[0]
+    n_fs = int(np.sum(t < 4))
+    assert 0 < eb <= ea
+    assert eb >= 20 * n_fs  # a 3D lattice holds ~120 particles within the list radius
+    g.set_pair_mode("stencil")
+    assert g.list_stats() == (0, 0)
+    g.close()
