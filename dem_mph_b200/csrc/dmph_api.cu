@@ -1363,7 +1363,7 @@ static int ens_enqueue_step(dmph_ensemble *e, cudaGraph_t g)
 
 static long long ens_step_launches(const dmph_ensemble *e)
 {
-    long long n = 3 + (e->use_list ? 2 : 0);
+    long long n = 3 + (e->use_list ? 3 : 0);  // list passes: A, B fluid, B debris
     for (const dmph_ctx *c : e->scenes) n += 2 + dem_launches(c);
     return n;
 }

@@ -181,9 +181,19 @@ __global__ void __launch_bounds__(8 * kWarp) k_clump_dem_list(DevParams P, DevSt
         const int bi = S.bid[i];
         const double mi = particle_density(S, P, i, ti) * P.V;
         double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
-        for (int k = lane; k < cnt; k += kWarp) {
-            const unsigned e = __ldg(S.nbl + list_index(k, i, ld));
-            if (e & (kEntrySolid | kEntryWall)) clump_pair(P, S, i, xi, vi, ti, bi, mi, (int)(e & kEntrySlot), F, T);
+        // four entries per lane loaded before any is used (lists hold at
+        // most 192 entries in 3D: at most two rounds)
+        for (int k0 = 0; k0 < cnt; k0 += 4 * kWarp) {
+            unsigned e[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + lane + u * kWarp;
+                e[u] = k < cnt ? __ldg(S.nbl + list_index(k, i, ld)) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (e[u] & (kEntrySolid | kEntryWall))
+                    clump_pair(P, S, i, xi, vi, ti, bi, mi, (int)(e[u] & kEntrySlot), F, T);
         }
         clump_store(P, S, i, lane, F, T);
     }

@@ -729,8 +729,9 @@ __global__ void __launch_bounds__(256, MINB) k_pass_a32_list(DevParams P, DevPar
 }
 
 // CLS: 0 = slot i holds fluid, 1 = debris, 2 = either.  The single-scene
-// step runs the fluid slots [0, fe) and the debris slots [sb, se) as two
-// kernels, so the fluid kernel carries none of the drag and buoyancy state.
+// step runs the fluid slots [0, fe) here and the debris slots [sb, se) in
+// k_pass_b32_list_debris, so the fluid kernel carries none of the drag and
+// buoyancy state.
 template <bool ST, int BATCH, int CLS = 2>
 __device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const DevParams32 &Q, const DevState &S, int i)
 {
@@ -778,6 +779,75 @@ __global__ void __launch_bounds__(256, MINB) k_pass_b32_list(DevParams P, DevPar
     if (dB[B_LIST_OVF]) return;
     FOR_EACH_SLOT(dB, CLS == 1 ? B_SB : -1, CLS == 0 ? B_FE : B_SE, i)
     pass_b32_list_slot<ST, BATCH, CLS>(P, Q, S, i);
+}
+
+// Debris slots [sb, se): few particles, each with a long list, so one warp
+// per particle with the lanes over its entries (lane l takes entries l,
+// l + 32, ...); every pair goes to the FP64 sums on its own and the lanes'
+// sums are combined by shuffles; the drag coefficient of the last candidate
+// in list order (the largest j) wins, as in the reference.
+template <bool ST>
+__device__ __forceinline__ void pass_b32_debris_warp(const DevParams &P, const DevParams32 &Q, const DevState &S,
+                                                     int i, int lane)
+{
+    const int cnt = S.nbn[i];
+    if (cnt < 0) return;
+    const long long ld = P.N;
+    const float cut2 = ST ? fmaxf(fmaxf(Q.RP2, Q.RV2), fmaxf(Q.RA2, Q.RG2)) : fmaxf(Q.RP2, Q.RV2);
+    const float4 pi = S.p4[i];
+    const int ti = unpack_type(__float_as_uint(pi.w));
+    const IB I = make_ib<ST>(P, S, i, pi, S.v4[i], ti);
+    AccB B = acc_b_zero();
+    for (int k = lane; k < cnt; k += kWarp) {
+        const unsigned e = __ldg(S.nbl + list_index(k, i, ld));
+        int j;
+        const float4 pj = list_pos(Q, S, e, j);
+        const float4 vj = __ldg(S.v4 + j);
+        const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+        if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) < cut2) {
+            float4 gj = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (ST) {
+                gj = S.gc4[j];
+                gj.w = S.pA32[j];
+            }
+            pair_b32<ST, 1>(Q, I, pj, vj, gj, j, B);
+            flush_b(B);
+        }
+    }
+    for (int o = 1; o < kWarp; o <<= 1) {
+        B.f.x += __shfl_xor_sync(kFull, B.f.x, o);
+        B.f.y += __shfl_xor_sync(kFull, B.f.y, o);
+        B.f.z += __shfl_xor_sync(kFull, B.f.z, o);
+        B.fD.x += __shfl_xor_sync(kFull, B.fD.x, o);
+        B.fD.y += __shfl_xor_sync(kFull, B.fD.y, o);
+        B.fD.z += __shfl_xor_sync(kFull, B.fD.z, o);
+        B.fB.x += __shfl_xor_sync(kFull, B.fB.x, o);
+        B.fB.y += __shfl_xor_sync(kFull, B.fB.y, o);
+        B.fB.z += __shfl_xor_sync(kFull, B.fB.z, o);
+        if (ST) {
+            B.fS.x += __shfl_xor_sync(kFull, B.fS.x, o);
+            B.fS.y += __shfl_xor_sync(kFull, B.fS.y, o);
+            B.fS.z += __shfl_xor_sync(kFull, B.fS.z, o);
+        }
+        const int oj = __shfl_xor_sync(kFull, B.drag_j, o);
+        const float oc = __shfl_xor_sync(kFull, B.dragc, o);
+        if (oj > B.drag_j) {
+            B.drag_j = oj;
+            B.dragc = oc;
+        }
+    }
+    if (lane == 0) finish_b32<1>(P, Q, S, i, I, B);
+}
+
+template <bool ST>
+__global__ void __launch_bounds__(256) k_pass_b32_list_debris(DevParams P, DevParams32 Q, DevState S, const int *dB)
+{
+    if (dB[B_LIST_OVF]) return;
+    const int lane = threadIdx.x & 31;
+    const int sb = dB[B_SB], se = dB[B_SE];
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    for (int i = sb + blockIdx.x * (blockDim.x >> 5) + (int)(threadIdx.x >> 5); i < se; i += nwarps)
+        pass_b32_debris_warp<ST>(P, Q, S, i, lane);
 }
 
 // chunk bodies dispatched on the chunk's size: 4 lanes per particle for up to
@@ -903,15 +973,17 @@ __global__ void __launch_bounds__(WPB * kWarp, MINB) k_ens_pass_b32(const EnsSce
 }
 
 // List-mode ensemble passes: one thread per slot over the concatenated slot
-// ranges of the scenes (all slots for pass A, fluid and debris for pass B);
-// a scene whose lists overflowed at its last rebuild is left to the stencil
-// ensemble kernels, which then run for that scene only.
-__device__ __forceinline__ int ens_slot_prefix(const EnsScene *__restrict__ tab, int ns, bool pass_b, int *pre)
+// ranges of the scenes (kind 0: all slots, pass A; 1: fluid slots, pass B;
+// 2: debris slots, pass B); a scene whose lists overflowed at its last
+// rebuild is left to the stencil ensemble kernels, which then run for that
+// scene only.
+__device__ __forceinline__ int ens_slot_prefix(const EnsScene *__restrict__ tab, int ns, int kind, int *pre)
 {
     for (int k = threadIdx.x; k < ns; k += blockDim.x) {
         const EnsScene &e = tab[k];
         const bool ok = e.S.nbn != nullptr && e.dB[B_LIST_OVF] == 0;
-        pre[k + 1] = ok ? (pass_b ? e.dB[B_SE] : e.P.N) : 0;
+        const int n = kind == 0 ? e.P.N : (kind == 1 ? e.dB[B_FE] : e.dB[B_SE] - e.dB[B_SB]);
+        pre[k + 1] = ok ? n : 0;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -926,19 +998,36 @@ template <bool PASS_B>
 __global__ void __launch_bounds__(256) k_ens_pass_list(const EnsScene *__restrict__ tab, int ns)
 {
     __shared__ int pre[kMaxEnsemble + 1];
-    const int total = ens_slot_prefix(tab, ns, PASS_B, pre);
+    const int total = ens_slot_prefix(tab, ns, PASS_B ? 1 : 0, pre);
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
         const int k = ens_scene_of(pre, ns, g);
         const EnsScene &e = tab[k];
         const int i = g - pre[k];
-        if (PASS_B) {
-            if (e.P.surface_tension) pass_b32_list_slot<true, 2>(e.P, e.Q, e.S, i);
-            else pass_b32_list_slot<false, 2>(e.P, e.Q, e.S, i);
+        if (PASS_B) {  // fluid slots; the debris slots go to k_ens_pass_b_debris
+            if (e.P.surface_tension) pass_b32_list_slot<true, 2, 0>(e.P, e.Q, e.S, i);
+            else pass_b32_list_slot<false, 2, 0>(e.P, e.Q, e.S, i);
         } else {
             const int split = e.dB[B_LIST_SPLIT];
             if (e.P.surface_tension) pass_a32_list_slot<true, 2>(e.P, e.Q, e.S, i, split);
             else pass_a32_list_slot<false, 2>(e.P, e.Q, e.S, i, split);
         }
+    }
+}
+
+// pass B of the debris slots of all scenes: one warp per particle, as in the
+// single-scene step
+__global__ void __launch_bounds__(256) k_ens_pass_b_debris(const EnsScene *__restrict__ tab, int ns)
+{
+    __shared__ int pre[kMaxEnsemble + 1];
+    const int total = ens_slot_prefix(tab, ns, 2, pre);
+    const int lane = threadIdx.x & 31;
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    for (int g = blockIdx.x * (blockDim.x >> 5) + (int)(threadIdx.x >> 5); g < total; g += nwarps) {
+        const int k = ens_scene_of(pre, ns, g);
+        const EnsScene &e = tab[k];
+        const int i = e.dB[B_SB] + g - pre[k];
+        if (e.P.surface_tension) pass_b32_debris_warp<true>(e.P, e.Q, e.S, i, lane);
+        else pass_b32_debris_warp<false>(e.P, e.Q, e.S, i, lane);
     }
 }
 
@@ -1328,15 +1417,13 @@ void launch_pass_b32_list(const DevParams &P, const DevParams32 &Q, const DevSta
     default: break;
     }
 #undef DMPH_LAUNCH_LB
-    // debris slots
-    {
-        if (P.surface_tension) {
-            static const int g = grid_for(k_pass_b32_list<true, 2, 2, 1>, 256);
-            k_pass_b32_list<true, 2, 2, 1><<<g, 256, 0, st>>>(P, Q, S, dB);
-        } else {
-            static const int g = grid_for(k_pass_b32_list<false, 2, 2, 1>, 256);
-            k_pass_b32_list<false, 2, 2, 1><<<g, 256, 0, st>>>(P, Q, S, dB);
-        }
+    // debris slots: one warp per particle
+    if (P.surface_tension) {
+        static const int g = grid_for(k_pass_b32_list_debris<true>, 256);
+        k_pass_b32_list_debris<true><<<g, 256, 0, st>>>(P, Q, S, dB);
+    } else {
+        static const int g = grid_for(k_pass_b32_list_debris<false>, 256);
+        k_pass_b32_list_debris<false><<<g, 256, 0, st>>>(P, Q, S, dB);
     }
 }
 
@@ -1375,6 +1462,8 @@ void launch_ens_pass_list(const EnsScene *tab, int ns, bool pass_b, cudaStream_t
     if (pass_b) {
         static const int g = grid_for(k_ens_pass_list<true>, 256);
         k_ens_pass_list<true><<<g, 256, 0, st>>>(tab, ns);
+        static const int gd = grid_for(k_ens_pass_b_debris, 256);
+        k_ens_pass_b_debris<<<gd, 256, 0, st>>>(tab, ns);
     } else {
         static const int g = grid_for(k_ens_pass_list<false>, 256);
         k_ens_pass_list<false><<<g, 256, 0, st>>>(tab, ns);
