@@ -787,10 +787,12 @@ __global__ void k_list_stats(const int *__restrict__ nbn, int n, const int *__re
     }
 }
 
-extern "C" int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64_t *entries_pass_b)
+extern "C" int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64_t *entries_pass_b,
+                                   int32_t *overflowed)
 {
     if (!ctx) return DMPH_EINVAL;
     unsigned long long h[2] = {0, 0};
+    int ovf = 0;
     if (ctx->use_list) {
         if (!ctx->stats) {  // two counters, allocated on first use
             const int rc = dalloc(ctx, &ctx->stats, 2);
@@ -800,10 +802,12 @@ extern "C" int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64
         k_list_stats<<<ctx->sms * 4, 256, 0, ctx->st>>>(ctx->S.nbn, ctx->P.N, ctx->dB, ctx->stats);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(h, ctx->stats, sizeof(h), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(&ovf, ctx->dB + B_LIST_OVF, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
     }
     if (entries_pass_a) *entries_pass_a = (int64_t)h[0];
     if (entries_pass_b) *entries_pass_b = (int64_t)h[1];
+    if (overflowed) *overflowed = ovf ? 1 : 0;
     return DMPH_OK;
 }
 

@@ -39,7 +39,7 @@ def lib():
         L.dmph_get_field.argtypes = [vp, C.c_int, vp]
         L.dmph_get_info.argtypes = [vp, vp]
         L.dmph_get_neighbor_list.argtypes = [vp, vp, vp, C.c_int64]
-        L.dmph_get_list_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.dmph_get_list_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
         L.dmph_set_bodies.argtypes = [vp, C.c_int, vp, vp]
         L.dmph_get_bodies.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
         L.dmph_set_profiling.argtypes = [vp, C.c_int]
@@ -156,12 +156,13 @@ class Solver:
         self._check(lib().dmph_get_neighbor_list(self._h, _ptr(ptr), _ptr(ind), int(ptr[-1])))
         return ptr, ind[:int(ptr[-1])]
 
-    def list_stats(self):
+    def list_stats(self, with_overflow=False):
         """(entries walked by pass A, entries walked by pass B) of the current
-        Verlet lists (dmph_get_list_stats); (0, 0) in stencil mode"""
-        a, b = C.c_int64(0), C.c_int64(0)
-        self._check(lib().dmph_get_list_stats(self._h, C.byref(a), C.byref(b)))
-        return a.value, b.value
+        Verlet lists (dmph_get_list_stats), plus the overflow flag when asked;
+        zeros in stencil mode"""
+        a, b, o = C.c_int64(0), C.c_int64(0), C.c_int32(0)
+        self._check(lib().dmph_get_list_stats(self._h, C.byref(a), C.byref(b), C.byref(o)))
+        return (a.value, b.value, bool(o.value)) if with_overflow else (a.value, b.value)
 
     def set_bodies(self, body_of_row, body_density):
         """Make debris bodies rigid (see dmph_set_bodies): body_of_row[r] is the

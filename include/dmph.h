@@ -230,10 +230,12 @@ int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind, int64_t ca
  * Size of the pair work of the current Verlet lists (no counterpart in the
  * reference): the entries pass A walks (all particles with a list) and those
  * pass B walks (fluid and debris).  In the FP32 build, lists made with the
- * walls at rest hold no wall-wall pairs.  Either pointer may be NULL; both
- * read 0 in stencil mode.
+ * walls at rest hold no wall-wall pairs.  *overflowed = 1 when a list of the
+ * last rebuild outgrew its capacity (the steps then walk the stencil until
+ * the next rebuild, and the counts are those of the truncated lists).  Any
+ * pointer may be NULL; all read 0 in stencil mode.
  */
-int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64_t *entries_pass_b);
+int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64_t *entries_pass_b, int32_t *overflowed);
 
 /*
  * Rigid debris bodies (no counterpart in the reference, whose debris particles

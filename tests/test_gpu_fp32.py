@@ -189,3 +189,28 @@ def test_list_stats_count_the_list_entries():
     g.set_pair_mode("stencil")
     assert g.list_stats() == (0, 0)
     g.close()
+
+
+@pytest.mark.parametrize("precision", [0, PRECISION_FP32_SPLIT])
+def test_list_overflow_falls_back_to_the_stencil(precision):
+    """A fluid block at three times the lattice density gives lists longer
+    than their capacity: the rebuild flags the overflow and the step walks the
+    stencil instead, with the same bits as stencil mode (FP64 and FP32)."""
+    p, typ, x, v = load_scene("small3d")
+    fl = typ < 2
+    h = 0.5 * p.particle_spacing
+    typ3 = np.concatenate([typ, typ[fl], typ[fl]])
+    x3 = np.concatenate([x, x[fl] + [h, 0.0, 0.0], x[fl] + [0.0, h, 0.0]])
+    v3 = np.concatenate([v, v[fl], v[fl]])
+    p.precision = precision
+    a = solver.Solver(p, typ3, x3, v3)
+    b = solver.Solver(p, typ3, x3, v3)
+    b.set_pair_mode("stencil")
+    assert a.list_stats(with_overflow=True)[2]
+    a.step(1)
+    b.step(1)
+    for f in ("Force", "PressureP", "VolStrainP"):
+        assert np.array_equal(a.field(f), b.field(f)), f
+    assert np.array_equal(a.state()[1], b.state()[1])
+    a.close()
+    b.close()
