@@ -54,13 +54,7 @@ static void release(dmph_ctx *ctx)
 }
 
 // number of kernels launch_bitonic issues for n = 2^nlog words
-static long long bitonic_launches(int n, int nlog)
-{
-    const int tlog = n < 2048 ? nlog : 11;
-    long long c = tlog > 0 ? 1 : 0;
-    for (int stage = tlog; stage < nlog; ++stage) c += (stage - tlog + 1) + 1;
-    return c;
-}
+static long long bitonic_launches(int n, int nlog) { return bitonic_launch_count(n, nlog); }
 
 // calculateCellParticle :1288 + the parts of calculateNeighbor the step needs.
 // Every launch has a static shape and every range lives in ctx->dB, so the

@@ -12,6 +12,7 @@ int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, std
 // dmph_rebuild.cu
 void launch_keys(const DevParams &P, const double *pos, const int *type, unsigned long long *words, cudaStream_t st);
 void launch_bitonic(unsigned long long *words, int n, int nlog, cudaStream_t st);
+int bitonic_launch_count(int n, int nlog);  // kernels launch_bitonic issues
 void launch_cell_start(const DevParams &P, const unsigned long long *words, int *start, cudaStream_t st);
 void launch_permute(const DevParams &P, const unsigned long long *words, const double *pos_in, const double *vel_in,
                     const int *type_in, const int *pidx_in, double *pos_out, double *vel_out, int *type_out,

@@ -14,8 +14,10 @@
 
 namespace dmph {
 
-constexpr int kSortTileLog = 11;  // 2048 words = 16 KiB of shared memory per block
+constexpr int kSortTileLog = 12;  // 4096 words = 32 KiB of shared memory per block
 constexpr int kSortTile = 1 << kSortTileLog;
+constexpr int kSortThreads = 1024;
+constexpr int kSortFuse = 4;  // global sub-passes done per launch
 
 // cell key + class offset (:1295-1313) and identity payload; pad with 3T
 __global__ void k_keys(DevParams P, const double *__restrict__ pos, const int *__restrict__ type,
@@ -54,7 +56,7 @@ __device__ __forceinline__ void cmp_exchange(unsigned long long &a, unsigned lon
 
 // Stages (stage, dist) with dist < tile, from `stage_lo` (starting at
 // dist_start) to `stage_hi`, inside one tile in shared memory.
-__global__ void __launch_bounds__(kSortTile / 2) k_bitonic_local(unsigned long long *words, int tile, int stage_lo,
+__global__ void __launch_bounds__(kSortThreads) k_bitonic_local(unsigned long long *words, int tile, int stage_lo,
                                                                  int stage_hi, int dist_start)
 {
     __shared__ unsigned long long sm[kSortTile];
@@ -77,17 +79,33 @@ __global__ void __launch_bounds__(kSortTile / 2) k_bitonic_local(unsigned long l
     for (int k = threadIdx.x; k < tile; k += blockDim.x) words[base + k] = sm[k];
 }
 
+// R consecutive sub-passes of one stage, distances dist, dist/2, ...,
+// dist >> (R-1), all at least the tile: those sub-passes compare the words
+// base + m * h (h = dist >> (R-1), m < 2^R) only among themselves, so each
+// thread loads such a group, applies the R sub-passes in order in registers
+// and stores it back.  Consecutive threads own consecutive bases, so every
+// load and store is coalesced.  All words of a group lie in one aligned
+// block of 2 * dist <= 2^(stage+1) words and share the direction bit.
+template <int R>
 __global__ void k_bitonic_global(unsigned long long *words, int n, int stage, int dist)
 {
+    const int h = dist >> (R - 1);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n / 2) return;
-    const int lo = (t / dist) * 2 * dist + (t % dist);
-    const bool up = ((lo >> stage) & 2) == 0;
-    unsigned long long a = words[lo], b = words[lo + dist];
-    if ((word_key(a) > word_key(b)) == up) {
-        words[lo] = b;
-        words[lo + dist] = a;
+    if (t >= (n >> R)) return;
+    const int base = (t / h) * 2 * dist + (t % h);
+    const bool up = ((base >> stage) & 2) == 0;
+    unsigned long long v[1 << R];
+#pragma unroll
+    for (int m = 0; m < (1 << R); ++m) v[m] = words[base + m * h];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int d = 1 << (R - 1 - r);
+#pragma unroll
+        for (int m = 0; m < (1 << R); ++m)
+            if ((m & d) == 0) cmp_exchange(v[m], v[m + d], up);
     }
+#pragma unroll
+    for (int m = 0; m < (1 << R); ++m) words[base + m * h] = v[m];
 }
 
 // cell_start[c] = number of sorted keys below c, c in [0, 3T]  (the begin/end
@@ -244,17 +262,39 @@ void launch_keys(const DevParams &P, const double *pos, const int *type, unsigne
     k_keys<<<(P.P2 + 255) / 256, 256, 0, st>>>(P, pos, type, words);
 }
 
+int bitonic_launch_count(int n, int nlog)
+{
+    const int tlog = n < kSortTile ? nlog : kSortTileLog;
+    int c = tlog > 0 ? 1 : 0;
+    for (int stage = tlog; stage < nlog; ++stage) c += (stage - tlog + kSortFuse) / kSortFuse + 1;
+    return c;
+}
+
 void launch_bitonic(unsigned long long *words, int n, int nlog, cudaStream_t st)
 {
     const int tile = n < kSortTile ? n : kSortTile;
     const int tlog = n < kSortTile ? nlog : kSortTileLog;
-    const int threads = tile / 2 > 0 ? tile / 2 : 1;
+    const int threads = tile / 2 > kSortThreads ? kSortThreads : (tile / 2 > 0 ? tile / 2 : 1);
     const int blocks = n / tile;
     // all stages whose distance fits the tile: stages 0 .. tlog-1
     if (tlog > 0) k_bitonic_local<<<blocks, threads, 0, st>>>(words, tile, 0, tlog - 1, 1);
     for (int stage = tlog; stage < nlog; ++stage) {
-        for (int dist = 1 << stage; dist >= tile; dist >>= 1)
-            k_bitonic_global<<<(n / 2 + 255) / 256, 256, 0, st>>>(words, n, stage, dist);
+        // the distances 2^stage .. tile, up to kSortFuse of them per launch
+        int dist = 1 << stage;
+        int left = stage - tlog + 1;
+        while (left > 0) {
+            const int r = left < kSortFuse ? left : kSortFuse;
+            const int groups = n >> r;
+            const int g = (groups + 255) / 256;
+            switch (r) {
+            case 1: k_bitonic_global<1><<<g, 256, 0, st>>>(words, n, stage, dist); break;
+            case 2: k_bitonic_global<2><<<g, 256, 0, st>>>(words, n, stage, dist); break;
+            case 3: k_bitonic_global<3><<<g, 256, 0, st>>>(words, n, stage, dist); break;
+            default: k_bitonic_global<4><<<g, 256, 0, st>>>(words, n, stage, dist); break;
+            }
+            dist >>= r;
+            left -= r;
+        }
         k_bitonic_local<<<blocks, threads, 0, st>>>(words, tile, stage, stage, tile / 2);
     }
 }
