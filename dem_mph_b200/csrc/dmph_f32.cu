@@ -553,79 +553,130 @@ struct TileL {
 // pairs of a wall with fluid or debris go to its list; every entry whose j is
 // a wall carries kEntryStaticWall, so pass A skips gathering its (zero)
 // velocity.
+// One chunk with L lanes per particle: lane = part * G + p holds particle p
+// (G = 32 / L) and tests candidates [part * G, part * G + G) of every staged
+// batch, so chunks of at most 16 (8) particles take half (a quarter) of the
+// distance tests per lane.  A particle's entries stay in ascending order:
+// each part writes after the entries of the lower parts of the same batch.
+template <bool ST, int L>
+__device__ __forceinline__ void build_list32_chunk(const DevParams &P, const DevParams32 &Q, const DevState &S,
+                                                   int *dB, float rc2, int split, TileL &tl, int lane, int cidx)
+{
+    constexpr int G = kWarp / L;
+    const int part = lane / G, pl = lane % G;
+    const int cap = S.nbl_cap;
+    const long long ld = P.N;
+    const float cut2 = ST ? fmaxf(Q.RP2, fmaxf(Q.RA2, Q.RG2)) : Q.RP2;  // pass A's
+    const Chunk ch = S.chunks[cidx];
+    const int i = ch.i0 + pl;
+    const bool active = pl < ch.cnt;
+    const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
+    int cix, ciy, ciz;
+    chunk_cell(P, key_cell, cix, ciy, ciz);
+    const float4 pi = S.p4[active ? i : ch.i0];
+    const int ti = unpack_type(__float_as_uint(pi.w));
+    const bool wall_i = split && is_wall(ti);
+    const IA I{pi, make_float4(0.f, 0.f, 0.f, 0.f), ti, is_solid(ti), is_wall(ti)};
+    AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
+    int cnt = 0;
+    traverse_stencil_batched(
+        P, S.cell_start, key_cell, lane, 7u,
+        [&](int j, int slot) {
+            const float4 pj = S.p4[j];
+            const unsigned w = __float_as_uint(pj.w);
+            const int tj = unpack_type(w);
+            const int dx = min_image_cell(unpack_cx(w) - cix, P.cc[0]);
+            const int dy = min_image_cell(unpack_cy(w) - ciy, P.cc[1]);
+            const int dz = min_image_cell(unpack_cz(w) - ciz, P.cc[2]);
+            tl.p[slot] = make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
+                                     fmaf((float)dz, Q.cw[2], pj.z), __int_as_float(tj));
+            tl.e[slot] = (unsigned)j | ((unsigned)((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)) << 24) |
+                         (is_solid(tj) ? kEntrySolid : 0u) |
+                         (is_wall(tj) ? (split ? kEntryWall | kEntryStaticWall : kEntryWall) : 0u);
+        },
+        [&](int base, int nb) {
+            // called by every lane: the count exchange below needs them all
+            unsigned m = 0;  // bit s0: candidate part * G + s0
+            if (active) {
+#pragma unroll
+                for (int s0 = 0; s0 < G; ++s0) {
+                    const int s = part * G + s0;
+                    const float4 pj = tl.p[s];
+                    const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+                    m |= (s < nb && fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= rc2) ? (1u << s0) : 0u;
+                }
+                const int self = i - base - part * G;
+                if (self >= 0 && self < G) m &= ~(1u << self);
+                // a batch holds candidates of one class: static walls are
+                // summed here (each part its own) and not listed
+                if (wall_i && (tl.e[0] & kEntryStaticWall)) {
+                    unsigned w = m;
+                    while (w) {
+                        const int s0 = __ffs(w) - 1;
+                        w &= w - 1;
+                        const float4 pj = tl.p[part * G + s0];
+                        const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
+                        if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= cut2)
+                            pair_a32<ST>(Q, I, pj, make_float4(0.f, 0.f, 0.f, 0.f), A);
+                    }
+                    m = 0;
+                }
+            }
+            const int c = __popc(m);
+            int before = 0, total = c;
+            if (L > 1) {
+                total = 0;
+#pragma unroll
+                for (int q = 0; q < L; ++q) {
+                    const int cq = __shfl_sync(kFull, c, q * G + pl);
+                    before += q < part ? cq : 0;
+                    total += cq;
+                }
+            }
+            int k = cnt + before;
+            while (m) {  // ascending candidate order
+                const int s0 = __ffs(m) - 1;
+                m &= m - 1;
+                if (k < cap) S.nbl[list_index(k, i, ld)] = tl.e[part * G + s0];
+                ++k;
+            }
+            cnt += total;
+        });
+    if (L > 1 && wall_i) {
+        // the parts' static sums, combined
+        for (int o = G; o < kWarp; o <<= 1) {
+            A.vsp += __shfl_xor_sync(kFull, A.vsp, o);
+            if (ST) {
+                A.dA += __shfl_xor_sync(kFull, A.dA, o);
+                A.g0 += __shfl_xor_sync(kFull, A.g0, o);
+                A.g1 += __shfl_xor_sync(kFull, A.g1, o);
+                A.g2 += __shfl_xor_sync(kFull, A.g2, o);
+            }
+        }
+    }
+    if (!active || part != 0) return;
+    if (cnt > cap) atomicExch(dB + B_LIST_OVF, 1);
+    S.nbn[i] = cnt < cap ? cnt : cap;
+    if (wall_i) {
+        S.vsp_st[i] = A.vsp;
+        S.st4[i] = make_float4(A.dA, A.g0, A.g1, A.g2);
+    }
+}
+
 template <bool ST>
-__global__ void __launch_bounds__(8 * kWarp) k_build_list32(DevParams P, DevParams32 Q, DevState S, int *dB, float rc2,
+__global__ void __launch_bounds__(8 * kWarp, 4) k_build_list32(DevParams P, DevParams32 Q, DevState S, int *dB, float rc2,
                                                             int split)
 {
     __shared__ TileL tiles[8];
     TileL &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
-    const int cap = S.nbl_cap;
-    const long long ld = P.N;
-    const float cut2 = ST ? fmaxf(Q.RP2, fmaxf(Q.RA2, Q.RG2)) : Q.RP2;  // pass A's
     if (blockIdx.x == 0 && threadIdx.x == 0) dB[B_LIST_SPLIT] = split;
     FOR_EACH_CHUNK(dB, CR_WET, 8, cidx)
     {
-        const Chunk ch = S.chunks[cidx];
-        const int i = ch.i0 + lane;
-        const bool active = lane < ch.cnt;
-        const int key_cell = (int)(word_key(S.skey[ch.i0]) % (unsigned)P.T);
-        int cix, ciy, ciz;
-        chunk_cell(P, key_cell, cix, ciy, ciz);
-        const float4 pi = S.p4[active ? i : ch.i0];
-        const int ti = unpack_type(__float_as_uint(pi.w));
-        const bool wall_i = split && is_wall(ti);
-        const IA I{pi, make_float4(0.f, 0.f, 0.f, 0.f), ti, is_solid(ti), is_wall(ti)};
-        AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
-        int cnt = 0;
-        traverse_stencil_batched(
-            P, S.cell_start, key_cell, lane, 7u,
-            [&](int j, int slot) {
-                const float4 pj = S.p4[j];
-                const unsigned w = __float_as_uint(pj.w);
-                const int tj = unpack_type(w);
-                const int dx = min_image_cell(unpack_cx(w) - cix, P.cc[0]);
-                const int dy = min_image_cell(unpack_cy(w) - ciy, P.cc[1]);
-                const int dz = min_image_cell(unpack_cz(w) - ciz, P.cc[2]);
-                tl.p[slot] = make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
-                                         fmaf((float)dz, Q.cw[2], pj.z), __int_as_float(tj));
-                tl.e[slot] = (unsigned)j | ((unsigned)((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)) << 24) |
-                             (is_solid(tj) ? kEntrySolid : 0u) |
-                             (is_wall(tj) ? (split ? kEntryWall | kEntryStaticWall : kEntryWall) : 0u);
-            },
-            [&](int base, int nb) {
-                if (!active) return;
-                unsigned m = 0;
-#pragma unroll
-                for (int s = 0; s < kWarp; ++s) {
-                    const float4 pj = tl.p[s];
-                    const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-                    m |= (s < nb && fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= rc2) ? (1u << s) : 0u;
-                }
-                const int self = i - base;
-                if (self >= 0 && self < kWarp) m &= ~(1u << self);
-                while (m) {  // ascending candidate order
-                    const int s = __ffs(m) - 1;
-                    m &= m - 1;
-                    const unsigned e = tl.e[s];
-                    if (wall_i && (e & kEntryStaticWall)) {
-                        const float4 pj = tl.p[s];
-                        const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-                        if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= cut2)
-                            pair_a32<ST>(Q, I, pj, make_float4(0.f, 0.f, 0.f, 0.f), A);
-                        continue;
-                    }
-                    if (cnt < cap) S.nbl[list_index(cnt, i, ld)] = e;
-                    ++cnt;
-                }
-            });
-        if (!active) continue;
-        if (cnt > cap) atomicExch(dB + B_LIST_OVF, 1);
-        S.nbn[i] = cnt < cap ? cnt : cap;
-        if (wall_i) {
-            S.vsp_st[i] = A.vsp;
-            S.st4[i] = make_float4(A.dA, A.g0, A.g1, A.g2);
-        }
+        const int n = S.chunks[cidx].cnt;
+        if (n <= 8) build_list32_chunk<ST, 4>(P, Q, S, dB, rc2, split, tl, lane, cidx);
+        else if (n <= 16) build_list32_chunk<ST, 2>(P, Q, S, dB, rc2, split, tl, lane, cidx);
+        else build_list32_chunk<ST, 1>(P, Q, S, dB, rc2, split, tl, lane, cidx);
     }
 }
 
