@@ -1,19 +1,33 @@
 """Scene generator for the reference's .boid scene descriptions.
 
 Reads a .boid file (ParticleDistance, LowerDomain, UpperDomain, then
-StartCuboid ... EndCuboid and StartCuboid2 ... EndCuboid2 blocks) and emits
-the particles in the order and with the floating-point arithmetic of the
-reference generator (generator/generator.cpp: readfile :127-184, genparticle
-:658-739 for Cuboid and Cuboid2, writefile :948-971), so that the written
-.grid is byte-identical to the reference generator's output.  All Cuboid
-blocks are emitted first, then all Cuboid2 blocks, as in genparticle.
+StartCuboid/Cuboid2/Cyboid/Cyboid2/Recboid/Recboid2 ... End<shape> blocks)
+and emits the particles in the order and with the floating-point arithmetic
+of the reference generator (generator/generator.cpp: readfile :129-184, the
+block readers :187-656, genparticle :660-897, writefile :908-931), so that the
+written .grid is byte-identical to the reference generator's output.  All
+blocks of one shape are emitted before the next shape, in the order Cuboid,
+Cuboid2, Cyboid, Cyboid2, Recboid, Recboid2, as in genparticle.
 
-Quirks kept: Cuboid lattices run from lower + 0.5 h to upper - 0.49 h with
-the spacing accumulated by repeated addition; Cuboid2 starts at
-lower + 0.01 h, runs to upper (exclusive), and rotates about the block
-centre by `Angle` interpreted in RADIANS (generator/generator.cpp:712-713).
+Quirks kept:
+* Cuboid lattices run from lower + 0.5 h to upper - 0.49 h with the spacing
+  accumulated by repeated addition.
+* Cuboid2 starts at lower + 0.01 h, runs to upper (exclusive), and rotates
+  about the block centre by `Angle` interpreted in RADIANS (:712-713).
+* Cyboid ignores Spacing and Ratio: it places the centres of a
+  floor(w * sqrt(3) / min(w)) grid per axis (:719-750).
+* Cyboid2 is a conical shell: rings of max(6, (int)(2 pi r / Spacing))
+  particles at every level from lower + 0.5 s to upper - 0.49 s with the
+  radius interpolated from R1 * Ratio (bottom) to R1 (top), R1 = mean of the
+  x and y half-widths, then one ring at the top face and one at the bottom
+  face (:786-850).
+* Recboid keeps the Cuboid2 lattice points with tan(Angle * 3.1415 / 180) >
+  y / x (IEEE division: x = 0 gives +-inf or NaN) (:854-876); Recboid2
+  rotates the Cuboid2 lattice about the ORIGIN by Angle * 3.1415 / 180
+  (:878-895).
 """
 import math
+import warnings
 
 import numpy as np
 
@@ -25,6 +39,47 @@ def _c_round(x):
     if a - r >= 0.5:
         r += 1
     return int(math.copysign(r, x)) if x < 0 else int(r)
+
+
+_SHAPES = ("StartCuboid", "StartCuboid2", "StartCyboid", "StartCyboid2", "StartRecboid", "StartRecboid2")
+_BASE = {"Spacing", "Type", "Lower", "Upper", "Velocity"}
+# the fields each block reader accepts and those it requires (:187-656):
+# Cuboid2 takes no Enthalpy and needs an Angle
+_ACCEPTED = {"Cuboid": _BASE | {"Enthalpy"}, "Cuboid2": _BASE | {"Angle"},
+             "Cyboid": _BASE | {"Enthalpy", "Ratio"}, "Cyboid2": _BASE | {"Enthalpy", "Ratio"},
+             "Recboid": _BASE | {"Enthalpy", "Angle"}, "Recboid2": _BASE | {"Enthalpy", "Angle"}}
+_REQUIRED = {"Cuboid": _BASE, "Cuboid2": _BASE | {"Angle"},
+             "Cyboid": _BASE | {"Enthalpy", "Ratio"}, "Cyboid2": _BASE | {"Enthalpy", "Ratio"},
+             "Recboid": _BASE | {"Enthalpy", "Angle"}, "Recboid2": _BASE | {"Enthalpy", "Angle"}}
+
+
+def _c_div(a, b):
+    """IEEE double division as C does it (b = 0 gives +-inf or NaN)"""
+    if b != 0.0:
+        return a / b
+    if a == 0.0 or math.isnan(a):
+        return math.nan
+    return math.copysign(math.inf, a) * math.copysign(1.0, b)
+
+
+def _lattice2(blk):
+    """the Cuboid2 / Recboid lattice (:697-709, :861-863): x and y from
+    lower + 0.01 h up to upper (exclusive), z from lower + 0.5 h to
+    upper - 0.49 h, spacing accumulated by repeated addition"""
+    lo, up = blk["lower"], blk["upper"]
+    width = [up[d] - lo[d] for d in range(3)]
+    cnt = [_c_round(width[d] / blk["space"]) for d in range(3)]
+    h = [width[d] / cnt[d] for d in range(3)]
+    px = lo[0] + 0.01 * h[0]
+    while px < up[0] - 0.0 * h[0]:
+        py = lo[1] + 0.01 * h[1]
+        while py < up[1] - 0.0 * h[1]:
+            pz = lo[2] + 0.5 * h[2]
+            while pz < up[2] - 0.49 * h[2]:
+                yield px, py, pz
+                pz += h[2]
+            py += h[1]
+        px += h[0]
 
 
 def parse_boid(text):
@@ -51,9 +106,11 @@ def parse_boid(text):
             dom["ParticleDistance"] = float(w[1])
         elif w[0] in ("LowerDomain", "UpperDomain"):
             dom[w[0]] = [float(s) for s in w[1:4]]
-        elif w[0] in ("StartCuboid", "StartCuboid2"):
-            end = "EndCuboid" if w[0] == "StartCuboid" else "EndCuboid2"
-            blk = {"shape": w[0][5:], "angle": 0.0, "velocity": [0.0, 0.0, 0.0]}
+        elif w[0] in _SHAPES:
+            shape = w[0][5:]
+            end = "End" + shape
+            blk = {"shape": shape, "angle": 0.0, "ratio": 0.0, "enthalpy": 0.0, "velocity": [0.0, 0.0, 0.0],
+                   "lower": [0.0, 0.0, 0.0], "upper": [0.0, 0.0, 0.0], "type": 0}
             # the block body is read token by token with fscanf (whitespace
             # separated, comment lines included as tokens)
             words = []
@@ -63,24 +120,34 @@ def parse_boid(text):
                 words += l2.split()
                 if end in words:
                     break
+            seen = set()
             k = 0
+            bad = None
             while k < len(words) and words[k] != end:
                 t = words[k]
+                if t not in _ACCEPTED[shape]:
+                    bad = "no such indication: %s" % t
+                    break
                 if t == "Spacing":
                     blk["space"] = float(words[k + 1]); k += 2
                 elif t == "Type":
                     blk["type"] = int(words[k + 1]); k += 2
                 elif t in ("Lower", "Upper", "Velocity"):
                     blk[t.lower()] = [float(s) for s in words[k + 1:k + 4]]; k += 4
-                elif t == "Angle":
-                    blk["angle"] = float(words[k + 1]); k += 2
-                elif t == "Enthalpy":
-                    k += 2
-                else:
-                    raise ValueError("no such indication: %s" % t)
+                else:  # Angle, Ratio, Enthalpy
+                    blk[t.lower()] = float(words[k + 1]); k += 2
+                seen.add(t)
+            missing = _REQUIRED[shape] - seen
+            if bad is None and missing:
+                bad = "%s block without %s" % (shape, ", ".join(sorted(missing)))
+            if bad is not None:
+                # the reference's block reader fails, the block is dropped and
+                # readfile stops there; the blocks read so far are generated
+                # (:152-175, :180-183)
+                warnings.warn("boid: %s; the rest of the file is ignored" % bad)
+                break
             blocks.append(blk)
-        elif w[0].startswith("Start"):
-            raise NotImplementedError("shape %s is not supported by this generator" % w[0])
+        # any other line (unknown keywords and shapes included) is ignored
     return dom, blocks
 
 
@@ -120,6 +187,52 @@ def generate(dom, blocks):
                     pz += h[2]
                 py += h[1]
             px += h[0]
+    for blk in [b for b in blocks if b["shape"] == "Cyboid"]:
+        lo, up = blk["lower"], blk["upper"]
+        width = [up[d] - lo[d] for d in range(3)]
+        side = min(width[0], min(width[1], width[2])) / math.sqrt(3.0)
+        nt = [int(math.floor(width[d] / side)) for d in range(3)]
+        h = [width[d] / nt[d] for d in range(3)]
+        for i in range(nt[0]):
+            for j in range(nt[1]):
+                for k in range(nt[2]):
+                    p = (lo[0] + (i + 0.5) * h[0], lo[1] + (j + 0.5) * h[1], lo[2] + (k + 0.5) * h[2])
+                    typ.append(blk["type"]); pos.append(p); vel.append(tuple(blk["velocity"]))
+    for blk in [b for b in blocks if b["shape"] == "Cyboid2"]:
+        lo, up = blk["lower"], blk["upper"]
+        width = [up[d] - lo[d] for d in range(3)]
+        c = [0.5 * (up[d] + lo[d]) for d in range(3)]
+        s = blk["space"]
+        height = width[2]
+        R1 = 0.5 * (width[0] + width[1]) * 0.5
+        R2 = R1 * blk["ratio"]
+
+        def ring(pz, radius):
+            n = max(6, int(2.0 * math.pi * radius / s))
+            for ith in range(n):
+                th = (2.0 * math.pi * ith) / n
+                typ.append(blk["type"])
+                pos.append((c[0] + radius * math.cos(th), c[1] + radius * math.sin(th), pz))
+                vel.append(tuple(blk["velocity"]))
+
+        pz = lo[2] + 0.5 * s
+        while pz < up[2] - 0.49 * s:
+            ratio_z = (pz - lo[2]) / height
+            ring(pz, R2 + (R1 - R2) * ratio_z)
+            pz += s
+        ring(up[2], R1)
+        ring(lo[2], R2)
+    for blk in [b for b in blocks if b["shape"] == "Recboid"]:
+        t = math.tan(blk["angle"] * 3.1415 / 180)
+        for px, py, pz in _lattice2(blk):
+            if t > _c_div(py, px):
+                typ.append(blk["type"]); pos.append((px, py, pz)); vel.append(tuple(blk["velocity"]))
+    for blk in [b for b in blocks if b["shape"] == "Recboid2"]:
+        a = blk["angle"] * 3.1415 / 180
+        ca, sa = math.cos(a), math.sin(a)
+        for px, py, pz in _lattice2(blk):
+            typ.append(blk["type"]); pos.append((px * ca - py * sa, px * sa + py * ca, pz))
+            vel.append(tuple(blk["velocity"]))
     return (np.array(typ, np.int32), np.array(pos, np.float64).reshape(-1, 3),
             np.array(vel, np.float64).reshape(-1, 3))
 
