@@ -254,3 +254,20 @@ def boid_to_grid(boid_path, grid_path):
     with open(grid_path, "w") as f:
         f.write(grid_text(dom, typ, x, v))
     return len(typ)
+
+
+def main(argv=None):
+    """The reference generator's command line (generator.cpp:117-127):
+    `python -m dem_mph_b200.generator [NAME]` reads NAME.boid and writes
+    NAME.grid in the current directory (sample.boid / sample.grid without an
+    argument)."""
+    import sys
+    args = sys.argv[1:] if argv is None else argv
+    name = args[0] if args else "sample"
+    n = boid_to_grid(name + ".boid", name + ".grid")
+    sys.stderr.write("%d particles were generated\n" % n)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
