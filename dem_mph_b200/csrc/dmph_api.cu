@@ -312,14 +312,20 @@ void dmph::drop_graph(dmph_ctx *ctx)
     ctx->graph = nullptr;
 }
 
+// calculateWall moves the walls while 0.2 <= Time <= 0.4 (:2857)
+static bool in_wall_window(const dmph_ctx *ctx)
+{
+    return ctx->time >= 0.2 && 0.4 >= ctx->time && !(ctx->fp32 && ctx->walls_rest);
+}
+
 static bool graph_usable(const dmph_ctx *ctx)
 {
-    return ctx->use_graph && !ctx->prof && 0.0 < ctx->time && !(ctx->time >= 0.2 && 0.4 >= ctx->time);
+    return ctx->use_graph && !ctx->prof && 0.0 < ctx->time && !in_wall_window(ctx);
 }
 
 int dmph::step_once(dmph_ctx *ctx)
 {
-    ctx->Wm.moving = (ctx->time >= 0.2 && 0.4 >= ctx->time) ? 1 : 0;
+    ctx->Wm.moving = in_wall_window(ctx) ? 1 : 0;
     if (graph_usable(ctx)) {
         if (!ctx->gexec) {
             const int rc = build_graph(ctx);
@@ -386,6 +392,10 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         delete ctx;
         return rc;
     }
+    ctx->walls_rest = true;
+    for (int t = DMPH_WALL_BEGIN; t < DMPH_WALL_END; ++t)
+        for (int d = 0; d < 3; ++d)
+            if (p->wall_velocity[t][d] != 0.0 || p->wall_omega[t][d] != 0.0) ctx->walls_rest = false;
     for (long long k = 0; k < 3ll * n; k++)
         if (!std::isfinite(x3[k]) || !std::isfinite(v3[k])) {
             g_create_err = "non-finite position or velocity at row " + std::to_string(k / 3);
@@ -1301,7 +1311,7 @@ static int ens_enqueue_step(dmph_ensemble *e, cudaGraph_t g)
     EK(cudaEventRecord(e->join, e->st));
     for (int k = 0; k < ns; ++k) {
         dmph_ctx *c = e->scenes[k];
-        c->Wm.moving = (c->time >= 0.2 && 0.4 >= c->time) ? 1 : 0;
+        c->Wm.moving = in_wall_window(c) ? 1 : 0;
         EK(cudaStreamWaitEvent(c->st, e->join, 0));
         if (g) {
             const int rc = capture_head_and_rebuild(c, g, c->st);
@@ -1370,7 +1380,7 @@ static bool ens_graph_usable(const dmph_ensemble *e)
 {
     if (!e->use_graph) return false;
     for (const dmph_ctx *c : e->scenes)
-        if (c->prof || !(0.0 < c->time) || (c->time >= 0.2 && 0.4 >= c->time)) return false;
+        if (c->prof || !(0.0 < c->time) || in_wall_window(c)) return false;
     return true;
 }
 

@@ -20,6 +20,10 @@ struct dmph_ctx {
     DevParams P;
     DevParams32 Q;
     bool fp32 = false;
+    // every wall type has zero velocity and zero angular velocity: in the FP32
+    // build the 0.2-0.4 s wall window then moves nothing (the FP32 positions
+    // keep their bits), so it is stepped like any other time
+    bool walls_rest = false;
     WallMotion Wm;
     cudaStream_t st = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
