@@ -66,9 +66,18 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
     const size_t N = (size_t)P.N;
     DevState &S = ctx->S;
     if (ctx->fp32 && !first) launch_export32(P, S, S.pos, nullptr, st);
-    launch_keys(P, S.pos, S.type, ctx->words, st);
-    launch_bitonic(ctx->words, P.P2, P.P2log, st);
-    launch_cell_start(P, ctx->words, S.cell_start, st);
+    // the counting sort orders a cell's particles its own way; the reference's
+    // per-particle DEM constants take the last neighbour in the network's
+    // order (:2305-2341), so scenes with debris outside rigid bodies keep
+    // the network
+    if (ctx->csort && (ctx->n_solid == 0 || ctx->Bd.B > 0)) {
+        launch_counting_sort(P, S.pos, S.type, ctx->ckeys, ctx->ccounts, ctx->words2, ctx->words, S.cell_start,
+                             ctx->bsums, ctx->total, st);
+    } else {
+        launch_keys(P, S.pos, S.type, ctx->words, st);
+        launch_bitonic(ctx->words, P.P2, P.P2log, st);
+        launch_cell_start(P, ctx->words, S.cell_start, st);
+    }
     if (ctx->fp32) {
         launch_permute32(P, ctx->words, S.pos, S.v4, S.type, S.pidx, ctx->p4b, ctx->v4b, ctx->type2, ctx->pidx2,
                          S.xref, S.xref4, S.bid, ctx->bid2, S.vel, ctx->pos2, ctx->vel2, st);
@@ -102,7 +111,9 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
 long long dmph::rebuild_launches(const dmph_ctx *ctx, bool first)
 {
     const DevParams &P = ctx->P;
-    return 1 + bitonic_launches(P.P2, P.P2log) + 1 + 1 + (ctx->fp32 && !first ? 1 : 0) + 5 + 1 +
+    const long long sort =
+        ctx->csort && (ctx->n_solid == 0 || ctx->Bd.B > 0) ? 6 : 1 + bitonic_launches(P.P2, P.P2log) + 1;
+    return sort + 1 + (ctx->fp32 && !first ? 1 : 0) + 5 + 1 +
            (ctx->fp32 ? 6 : 0) + 1 + (ctx->S.bid ? 1 : 0) + (ctx->use_list ? 1 : 0);
 }
 
@@ -392,6 +403,7 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         delete ctx;
         return rc;
     }
+    for (int i = 0; i < n; i++) ctx->n_solid += (type[i] >= DMPH_SOLID_BEGIN && type[i] < DMPH_SOLID_END) ? 1 : 0;
     ctx->walls_rest = true;
     for (int t = DMPH_WALL_BEGIN; t < DMPH_WALL_END; ++t)
         for (int d = 0; d < 3; ++d)
@@ -479,6 +491,12 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     AL(ctx->type2, N);
     AL(ctx->pidx2, N);
     AL(ctx->words, (size_t)P.P2);
+    if (ctx->fp32 && 3LL * P.T + 1 <= kCountingSortMaxKeys) {
+        ctx->csort = true;
+        AL(ctx->ckeys, N);
+        AL(ctx->ccounts, 3 * (size_t)P.T + 1);
+        AL(ctx->words2, N);
+    }
     if (ctx->fp32) {
         AL(S.p4, N);
         AL(S.v4, N);

@@ -37,6 +37,12 @@ struct dmph_ctx {
     int *bid2 = nullptr;                     // second buffer of the body ids
     DevBodies Bd{};                          // rigid clumps (B = 0: off)
     unsigned long long *words = nullptr;
+    // FP32 counting sort (csort): per-particle keys, per-key counts and the
+    // scattered words before each key's range is ordered
+    bool csort = false;
+    int n_solid = 0;  // debris particles (types 2-3) of the scene
+    int *ckeys = nullptr, *ccounts = nullptr;
+    unsigned long long *words2 = nullptr;
     int *flag = nullptr, *offs = nullptr, *bsums = nullptr, *total = nullptr;
     unsigned long long *maxshift = nullptr;
     unsigned long long *stats = nullptr;      // dmph_get_list_stats counters

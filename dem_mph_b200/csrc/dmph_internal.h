@@ -14,6 +14,12 @@ void launch_keys(const DevParams &P, const double *pos, const int *type, unsigne
 void launch_bitonic(unsigned long long *words, int n, int nlog, cudaStream_t st);
 int bitonic_launch_count(int n, int nlog);  // kernels launch_bitonic issues
 void launch_cell_start(const DevParams &P, const unsigned long long *words, int *start, cudaStream_t st);
+// FP32 build: stable counting sort of the cell keys into words[0, N) and
+// cell_start (6 kernels); nonzero when 3T + 1 keys exceed the scan's range
+int launch_counting_sort(const DevParams &P, const double *pos, const int *type, int *keys, int *counts,
+                         unsigned long long *tmp, unsigned long long *words, int *cell_start, int *block_sums,
+                         int *total, cudaStream_t st);
+constexpr long long kCountingSortMaxKeys = 4096LL * 4096LL;
 void launch_permute(const DevParams &P, const unsigned long long *words, const double *pos_in, const double *vel_in,
                     const int *type_in, const int *pidx_in, double *pos_out, double *vel_out, int *type_out,
                     int *pidx_out, double *xref, const int *bid_in, int *bid_out, cudaStream_t st);

@@ -19,7 +19,24 @@ constexpr int kSortTile = 1 << kSortTileLog;
 constexpr int kSortThreads = 1024;
 constexpr int kSortFuse = 4;  // global sub-passes done per launch
 
-// cell key + class offset (:1295-1313) and identity payload; pad with 3T
+// cell key + class offset of particle i (:1295-1313)
+__device__ __forceinline__ int particle_key(const DevParams &P, const double *__restrict__ pos,
+                                            const int *__restrict__ type, int i)
+{
+    const int N = P.N;
+    const int ix = ((int)floor((pos[i] - P.dmin[0]) / P.cw[0])) % P.cc[0];
+    const int iy = ((int)floor((pos[N + i] - P.dmin[1]) / P.cw[1])) % P.cc[1];
+    const int iz = ((int)floor((pos[2 * N + i] - P.dmin[2]) / P.cw[2])) % P.cc[2];
+    int k = cell_id(P, ix, iy, iz);
+    const int t = type[i];
+    if (is_solid(t))
+        k += P.T;
+    else if (is_wall(t))
+        k += 2 * P.T;
+    return k;
+}
+
+// cell key and identity payload; pad with 3T
 __global__ void k_keys(DevParams P, const double *__restrict__ pos, const int *__restrict__ type,
                        unsigned long long *__restrict__ words)
 {
@@ -27,21 +44,92 @@ __global__ void k_keys(DevParams P, const double *__restrict__ pos, const int *_
     if (i >= P.P2) return;
     const int N = P.N;
     unsigned long long w;
-    if (i < N) {
-        const int ix = ((int)floor((pos[i] - P.dmin[0]) / P.cw[0])) % P.cc[0];
-        const int iy = ((int)floor((pos[N + i] - P.dmin[1]) / P.cw[1])) % P.cc[1];
-        const int iz = ((int)floor((pos[2 * N + i] - P.dmin[2]) / P.cw[2])) % P.cc[2];
-        int k = cell_id(P, ix, iy, iz);
-        const int t = type[i];
-        if (is_solid(t))
-            k += P.T;
-        else if (is_wall(t))
-            k += 2 * P.T;
-        w = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)i;
-    } else {
+    if (i < N)
+        w = ((unsigned long long)(uint32_t)particle_key(P, pos, type, i) << 32) | (uint32_t)i;
+    else
         w = ((unsigned long long)(uint32_t)(3 * P.T) << 32) | (uint32_t)N;
-    }
     words[i] = w;
+}
+
+template <class T>
+int launch_exclusive_scan(const T *in, T *out, int n, T *block_sums, T *total, cudaStream_t st);
+
+// ------------------------------------------------ FP32: counting sort
+// The FP32 build sorts the cell keys with a counting sort instead of the
+// reference's bitonic network: the particles of a (class, cell) key keep
+// their previous relative order (a stable sort), so every particle's cell
+// and neighbour set are the reference's while the order inside a cell is
+// this build's own.  Keys are counted, the counts scanned into cell_start,
+// the particles scattered with an atomic cursor per key, and each key's
+// range finally ordered by previous slot, so the result does not depend on
+// the order of the atomics.
+__global__ void k_count_keys(DevParams P, const double *__restrict__ pos, const int *__restrict__ type,
+                             int *__restrict__ keys, int *__restrict__ counts)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.N) return;
+    const int k = particle_key(P, pos, type, i);
+    keys[i] = k;
+    atomicAdd(counts + k, 1);
+}
+
+__global__ void k_scatter_keys(DevParams P, const int *__restrict__ keys, const int *__restrict__ start,
+                               int *__restrict__ cursor, unsigned long long *__restrict__ tmp)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.N) return;
+    const int k = keys[i];
+    tmp[start[k] + atomicAdd(cursor + k, 1)] = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)i;
+}
+
+// one warp per 32 keys; each key's range is ordered by rank (the number of
+// smaller words in the range), for any range length
+__global__ void k_sort_cells(DevParams P, const unsigned long long *__restrict__ tmp, const int *__restrict__ start,
+                             unsigned long long *__restrict__ words)
+{
+    const int lane = threadIdx.x & 31;
+    const int nseg = 3 * P.T;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int k0 = gw * 32; k0 < nseg; k0 += nw * 32) {
+        const int kl = k0 + lane;
+        const int b_l = kl < nseg ? start[kl] : 0;
+        const int n_l = kl < nseg ? start[kl + 1] - b_l : 0;
+        if (n_l == 1) words[b_l] = tmp[b_l];
+        unsigned todo = __ballot_sync(kFull, n_l >= 2);
+        while (todo) {
+            const int t = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int b = __shfl_sync(kFull, b_l, t), n = __shfl_sync(kFull, n_l, t);
+            for (int e0 = 0; e0 < n; e0 += kWarp) {
+                const int e = e0 + lane;
+                const unsigned long long w = e < n ? tmp[b + e] : 0ull;
+                int rank = 0;
+                for (int f0 = 0; f0 < n; f0 += kWarp) {
+                    const unsigned long long wf = f0 + lane < n ? tmp[b + f0 + lane] : 0ull;
+                    const int lim = n - f0 < kWarp ? n - f0 : kWarp;
+                    for (int u = 0; u < lim; ++u) rank += __shfl_sync(kFull, wf, u) < w ? 1 : 0;
+                }
+                if (e < n) words[b + rank] = w;
+            }
+        }
+    }
+}
+
+int launch_counting_sort(const DevParams &P, const double *pos, const int *type, int *keys, int *counts,
+                         unsigned long long *tmp, unsigned long long *words, int *cell_start, int *block_sums,
+                         int *total, cudaStream_t st)
+{
+    const int nk = 3 * P.T + 1;
+    const int g = (P.N + 255) / 256;
+    cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nk, st);
+    k_count_keys<<<g, 256, 0, st>>>(P, pos, type, keys, counts);
+    const int rc = launch_exclusive_scan<int>(counts, cell_start, nk, block_sums, total, st);
+    if (rc) return rc;
+    cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nk, st);
+    k_scatter_keys<<<g, 256, 0, st>>>(P, keys, cell_start, counts, tmp);
+    k_sort_cells<<<148 * 8, 256, 0, st>>>(P, tmp, cell_start, words);
+    return 0;
 }
 
 __device__ __forceinline__ void cmp_exchange(unsigned long long &a, unsigned long long &b, bool up)

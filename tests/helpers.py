@@ -38,8 +38,9 @@ def load_scene(name):
             generator.boid_to_grid(os.path.join(d, "DEM.boid"), grid)
             dim = 2
         else:
-            s = scenes.small()
-            p = s.params if name == "small3d" else small3d_st_params(s.params)
+            # small3d_fluid: the same tank and column without debris
+            s = scenes.small(n_debris=0) if name == "small3d_fluid" else scenes.small()
+            p = small3d_st_params(s.params) if name == "small3d_st" else s.params
             files.write_data_file(data, p)
             files.write_grid(grid, p, s.type, s.x, s.v)
             dim = 3

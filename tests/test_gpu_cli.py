@@ -39,7 +39,9 @@ def test_virial_pressure_matches_oracle(name):
     h.step(1)
     o2 = Oracle(p, typ, x, v)
     o2.step(1)
-    a, b = h.field("VirialPressure"), o2.get("VirialPressure")
+    # by particle id (the FP32 build may order a cell's particles its own way)
+    a = h.field("VirialPressure")[np.argsort(h.state()[3])]
+    b = o2.get("VirialPressure")[np.argsort(o2.get("ParticleIndex"))]
     # FP32 pressures carry the strain floor of the split precision (K * 1e-7)
     assert np.abs(a - b).max() <= 1e-3 * np.abs(b).max() + 1e-6 * p.bulk_modulus[1]
     g.close()
