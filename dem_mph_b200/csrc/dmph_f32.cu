@@ -595,15 +595,18 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
                          (is_wall(tj) ? (split ? kEntryWall | kEntryStaticWall : kEntryWall) : 0u);
         },
         [&](int base, int nb) {
-            // called by every lane: the count exchange below needs them all
+            // called by every lane: the count exchange below needs them all.
+            // Slots past the batch get a position whose squared distance
+            // overflows to infinity, so the tests need no bounds check.
+            if (lane >= nb) tl.p[lane].x = 1.0e30f;
+            __syncwarp();
             unsigned m = 0;  // bit s0: candidate part * G + s0
             if (active) {
 #pragma unroll
                 for (int s0 = 0; s0 < G; ++s0) {
-                    const int s = part * G + s0;
-                    const float4 pj = tl.p[s];
+                    const float4 pj = tl.p[part * G + s0];
                     const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-                    m |= (s < nb && fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= rc2) ? (1u << s0) : 0u;
+                    m |= (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= rc2) ? (1u << s0) : 0u;
                 }
                 const int self = i - base - part * G;
                 if (self >= 0 && self < G) m &= ~(1u << self);
@@ -633,12 +636,17 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
                     total += cq;
                 }
             }
-            int k = cnt + before;
-            while (m) {  // ascending candidate order
-                const int s0 = __ffs(m) - 1;
-                m &= m - 1;
-                if (k < cap) S.nbl[list_index(k, i, ld)] = tl.e[part * G + s0];
-                ++k;
+            if (m) {
+                // entry k of slot i sits at block k / 8 (stride 8 N words), word k % 8
+                int k = cnt + before;
+                unsigned *blk = S.nbl + list_index(k & ~7, i, ld);
+                while (m) {  // ascending candidate order
+                    const int s0 = __ffs(m) - 1;
+                    m &= m - 1;
+                    if (k < cap) blk[k & 7] = tl.e[part * G + s0];
+                    ++k;
+                    if ((k & 7) == 0) blk += 8 * ld;
+                }
             }
             cnt += total;
         });
