@@ -543,8 +543,9 @@ __device__ __forceinline__ void pass_b32_body(const DevParams &P, const DevParam
 // rebuild is in the list.  The passes then run one thread per particle over
 // its list instead of over the ~800 candidates of the 27-cell stencil.
 struct TileL {
-    float4 p[kWarp];     // position in the frame of the warp's cell, .w = type bits
+    float4 p[kWarp];     // position in the frame of the warp's cell, .w = its squared norm
     unsigned e[kWarp];   // list entry of the candidate
+    int t[kWarp];        // type of the candidate
 };
 
 // split: the walls are at rest until the next rebuild (set by the host when no
@@ -578,6 +579,8 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
     const bool wall_i = split && is_wall(ti);
     const IA I{pi, make_float4(0.f, 0.f, 0.f, 0.f), ti, is_solid(ti), is_wall(ti)};
     AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
+    const float a0 = -2.f * pi.x, a1 = -2.f * pi.y, a2 = -2.f * pi.z;
+    const float thr = rc2 * (1.f + 1e-4f) - fmaf(pi.x, pi.x, fmaf(pi.y, pi.y, pi.z * pi.z));
     int cnt = 0;
     traverse_stencil_batched(
         P, S.cell_start, key_cell, lane, 7u,
@@ -588,25 +591,30 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
             const int dx = min_image_cell(unpack_cx(w) - cix, P.cc[0]);
             const int dy = min_image_cell(unpack_cy(w) - ciy, P.cc[1]);
             const int dz = min_image_cell(unpack_cz(w) - ciz, P.cc[2]);
-            tl.p[slot] = make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
-                                     fmaf((float)dz, Q.cw[2], pj.z), __int_as_float(tj));
+            const float x = fmaf((float)dx, Q.cw[0], pj.x), y = fmaf((float)dy, Q.cw[1], pj.y),
+                        z = fmaf((float)dz, Q.cw[2], pj.z);
+            tl.p[slot] = make_float4(x, y, z, fmaf(x, x, fmaf(y, y, z * z)));
+            tl.t[slot] = tj;
             tl.e[slot] = (unsigned)j | ((unsigned)((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)) << 24) |
                          (is_solid(tj) ? kEntrySolid : 0u) |
                          (is_wall(tj) ? (split ? kEntryWall | kEntryStaticWall : kEntryWall) : 0u);
         },
         [&](int base, int nb) {
             // called by every lane: the count exchange below needs them all.
-            // Slots past the batch get a position whose squared distance
-            // overflows to infinity, so the tests need no bounds check.
-            if (lane >= nb) tl.p[lane].x = 1.0e30f;
+            // Slots past the batch get a huge norm, so the tests need no
+            // bounds check.
+            if (lane >= nb) tl.p[lane] = make_float4(0.f, 0.f, 0.f, 1.0e30f);
             __syncwarp();
             unsigned m = 0;  // bit s0: candidate part * G + s0
             if (active) {
+                // |pj - pi|^2 = |pj|^2 - 2 pi.pj + |pi|^2, three FMAs per
+                // candidate; its rounding (a few 1e-6 of rc^2 at these
+                // magnitudes) is covered by testing against rc^2 (1 + 1e-4),
+                // so the list holds every pair within rc and a 5e-5 rc shell
 #pragma unroll
                 for (int s0 = 0; s0 < G; ++s0) {
                     const float4 pj = tl.p[part * G + s0];
-                    const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
-                    m |= (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= rc2) ? (1u << s0) : 0u;
+                    m |= (fmaf(a0, pj.x, fmaf(a1, pj.y, fmaf(a2, pj.z, pj.w))) <= thr) ? (1u << s0) : 0u;
                 }
                 const int self = i - base - part * G;
                 if (self >= 0 && self < G) m &= ~(1u << self);
@@ -617,7 +625,8 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
                     while (w) {
                         const int s0 = __ffs(w) - 1;
                         w &= w - 1;
-                        const float4 pj = tl.p[part * G + s0];
+                        const float4 pp = tl.p[part * G + s0];
+                        const float4 pj = make_float4(pp.x, pp.y, pp.z, __int_as_float(tl.t[part * G + s0]));
                         const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
                         if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= cut2)
                             pair_a32<ST>(Q, I, pj, make_float4(0.f, 0.f, 0.f, 0.f), A);
