@@ -105,7 +105,8 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
         if (ctx->fp32) launch_build_list32(P, ctx->Q, S, ctx->dB, ctx->Wm.moving ? 0 : 1, st);
         else launch_build_list64(P, S, ctx->dB, st);
     }
-    launch_counts(P, S, ctx->dB, ctx->all_counts ? CR_ALL : CR_SOLID, st);
+    if (ctx->fp32 && ctx->use_list && !ctx->all_counts) launch_counts_list(P, S, ctx->dB, st);
+    else launch_counts(P, S, ctx->dB, ctx->all_counts ? CR_ALL : CR_SOLID, st);
 }
 
 long long dmph::rebuild_launches(const dmph_ctx *ctx, bool first)
@@ -114,7 +115,8 @@ long long dmph::rebuild_launches(const dmph_ctx *ctx, bool first)
     const long long sort =
         ctx->csort && (ctx->n_solid == 0 || ctx->Bd.B > 0) ? 6 : 1 + bitonic_launches(P.P2, P.P2log) + 1;
     return sort + 1 + (ctx->fp32 && !first ? 1 : 0) + 5 + 1 +
-           (ctx->fp32 ? 6 : 0) + 1 + (ctx->S.bid ? 1 : 0) + (ctx->use_list ? 1 : 0);
+           (ctx->fp32 ? 6 : 0) + (ctx->fp32 && ctx->use_list && !ctx->all_counts ? 2 : 1) + (ctx->S.bid ? 1 : 0) +
+           (ctx->use_list ? 1 : 0);
 }
 
 // phase timing (dmph_set_profiling): events around one phase, synchronised

@@ -548,8 +548,12 @@ __global__ void k_dem_integrate(DevParams P, DevState S, const int *dB)
 // NeighborCount / SolidNeighborCount of calculateNeighbor :1546-1678 (counts
 // of particles within MaxRadius+MARGIN at rebuild time, self included; the
 // rebuild-time positions are kept in xref).
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_counts(DevParams P, DevState S, const int *dB, int range)
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_counts(DevParams P, DevState S, const int *dB, int range,
+                                                                   int gate)
 {
+    // gate: the FP32 lists count the debris (k_counts_list), this walk stands
+    // in after a list overflow
+    if (gate && dB[B_LIST_OVF] == 0) return;
     __shared__ TileA tiles[kWarpsPerBlock];
     TileA &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -584,6 +588,45 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_counts(DevParams P, 
         if (!active) continue;
         S.nc[i] = cnt;
         S.snc[i] = scnt;
+    }
+}
+
+// FP32 list mode: NeighborCount and SolidNeighborCount of the debris slots
+// from their Verlet lists, which hold every particle within rc of them (and
+// a thin shell past it); the reference's FP64 distance test on the
+// rebuild-time positions decides, as in k_counts, and i itself counts as
+// in the reference's list.  One warp per debris particle.
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_counts_list(DevParams P, DevState S, const int *dB)
+{
+    if (dB[B_LIST_OVF]) return;
+    const int lane = threadIdx.x & 31;
+    const int N = P.N;
+    const long long ld = N;
+    const int sb = dB[B_SB], se = dB[B_SE];
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    for (int i = sb + blockIdx.x * (blockDim.x >> 5) + (int)(threadIdx.x >> 5); i < se; i += nwarps) {
+        const int n = S.nbn[i];
+        const double xi = S.xref[i], yi = S.xref[N + i], zi = S.xref[2 * N + i];
+        int cnt = 0, scnt = 0;
+        for (int k = lane; k < n; k += kWarp) {
+            const int j = (int)(__ldg(S.nbl + list_index(k, i, ld)) & kEntrySlot);
+            const double q0 = rel1(S.xref[j], xi, P.W[0], P.hW[0]);
+            const double q1 = rel1(S.xref[N + j], yi, P.W[1], P.hW[1]);
+            const double q2 = rel1(S.xref[2 * N + j], zi, P.W[2], P.hW[2]);
+            const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
+            if (r2 <= P.rc2) {
+                cnt++;
+                if (is_solid(S.type[j])) scnt++;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            cnt += __shfl_xor_sync(kFull, cnt, o);
+            scnt += __shfl_xor_sync(kFull, scnt, o);
+        }
+        if (lane == 0) {
+            S.nc[i] = cnt + 1;  // i itself
+            S.snc[i] = scnt + 1;
+        }
     }
 }
 
@@ -841,7 +884,15 @@ void launch_dem_integrate(const DevParams &P, const DevState &S, const int *dB, 
 void launch_counts(const DevParams &P, const DevState &S, const int *dB, int range, cudaStream_t st)
 {
     static const int g = persistent_grid((const void *)k_counts, kBlock);
-    k_counts<<<g, kBlock, 0, st>>>(P, S, dB, range);
+    k_counts<<<g, kBlock, 0, st>>>(P, S, dB, range, 0);
+}
+
+void launch_counts_list(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
+{
+    static const int gl = persistent_grid((const void *)k_counts_list, kBlock);
+    k_counts_list<<<gl, kBlock, 0, st>>>(P, S, dB);
+    static const int g = persistent_grid((const void *)k_counts, kBlock);
+    k_counts<<<g, kBlock, 0, st>>>(P, S, dB, CR_SOLID, 1);
 }
 void launch_neighbor_fill(const DevParams &P, const DevState &S, const int *dB, const long long *ptr, int *ind,
                           cudaStream_t st)

@@ -47,6 +47,9 @@ void launch_dem_force(const DevParams &P, const DevState &S, const int *dB, int 
                       bool mixed = false);
 void launch_dem_integrate(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 void launch_counts(const DevParams &P, const DevState &S, const int *dB, int range, cudaStream_t st);
+// FP32 list mode, debris counts from the lists (with the stencil walk gated
+// on a list overflow): 2 kernels
+void launch_counts_list(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 void launch_neighbor_fill(const DevParams &P, const DevState &S, const int *dB, const long long *ptr, int *ind,
                           cudaStream_t st);
 

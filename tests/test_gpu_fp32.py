@@ -241,3 +241,37 @@ def test_list_overflow_falls_back_to_the_stencil(precision):
     assert np.array_equal(a.state()[1], b.state()[1])
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("bodies", [False, True])
+def test_debris_neighbour_counts_from_lists(bodies):
+    """NeighborCount and SolidNeighborCount of the debris (the drag's solid
+    fraction) come from the FP32 Verlet lists with the reference's FP64
+    distance test: equal to the oracle's at the creation rebuild, and, after
+    200 steps, to the FP64 stencil count of the same rebuild (the CSR list
+    of dmph_get_neighbor_list, which recounts every particle that way)."""
+    p, typ, x, v = load_scene("small3d")
+    q = p.copy()
+    q.precision = PRECISION_FP32_SPLIT
+    g = solver.Solver(q, typ, x, v)
+    o = Oracle(p, typ, x, v)
+    if bodies:
+        from dem_mph_b200 import scenes
+        s = scenes.small()
+        g.set_bodies(s.body, s.body_density)
+    ig, io = np.argsort(g.state()[3]), np.argsort(o.get("ParticleIndex"))
+    t = g.state()[0]
+    deb = (t[ig] >= 2) & (t[ig] < 4)
+    for f in ("NeighborCount", "SolidNeighborCount"):
+        assert np.array_equal(g.field(f)[ig][deb], o.get(f)[io][deb]), f
+    g.step(200)
+    assert g.info().rebuilds > 0
+    nc, snc = g.field("NeighborCount"), g.field("SolidNeighborCount")
+    t = g.state()[0]
+    ptr, ind = g.neighbor_list()
+    deb = (t >= 2) & (t < 4)
+    assert np.array_equal(nc[deb], np.diff(ptr)[deb])
+    solid_nb = ((t[ind] >= 2) & (t[ind] < 4)).astype(np.int64)
+    snc_ref = np.add.reduceat(solid_nb, ptr[:-1]) * (np.diff(ptr) > 0)
+    assert np.array_equal(snc[deb], snc_ref[deb])
+    g.close()
