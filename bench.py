@@ -167,6 +167,8 @@ def main():
                     help="untimed steps run before warm-up so the flow is moving and rebuilds fire in the timed steps")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels one by one instead of graph replay")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch variants of the pair passes")
+    ap.add_argument("--profiler-range", action="store_true",
+                    help="open the CUDA profiler range around the timed steps only (ncu --profile-from-start off)")
     ap.add_argument("--variants", type=int, nargs=2, default=None, metavar=("A", "B"),
                     help="set the pair-pass launch variants (pass A, pass B) instead of autotuning")
     ap.add_argument("--surrogate", action="store_true",
@@ -231,9 +233,13 @@ def main():
     torch.cuda.synchronize()
     l0 = g.info().kernel_launches
     rebuilds_before = int(g.info().rebuilds)
+    if args.profiler_range:
+        torch.cuda.profiler.start()
     with ClockSampler(torch.cuda.current_device()) as clk:
         ms = g.step_timed(args.steps)
         torch.cuda.synchronize()
+    if args.profiler_range:
+        torch.cuda.profiler.stop()
     barrier()
     inf_t = g.info()
     launches = int(inf_t.kernel_launches - l0)
