@@ -788,6 +788,67 @@ extern "C" int dmph_get_info(dmph_ctx *ctx, dmph_info *info)
     return DMPH_OK;
 }
 
+// global sums over the fluid and debris slots [0, se): each thread adds its
+// grid-stride slots, each block reduces in a fixed order and the blocks'
+// partial sums are added in block order, so a state always gives the same bits
+constexpr int kSumBlocks = 296, kSumThreads = 256;
+__global__ void __launch_bounds__(kSumThreads) k_global_sums(DevParams P, DevState S, const int *__restrict__ dB,
+                                                            double *__restrict__ part)
+{
+    const int N = P.N;
+    const int se = dB[B_SE];
+    double a[DMPH_SUM_COUNT] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < se; i += gridDim.x * blockDim.x) {
+        const int t = S.type[i];
+        const double m = is_solid(t) ? particle_density(S, P, i, t) * P.V : P.mass[t];
+        const double v0 = S.vel[i], v1 = S.vel[N + i], v2 = S.vel[2 * N + i];
+        a[DMPH_SUM_MASS] += m;
+        a[DMPH_SUM_MOMENTUM_X] += m * v0;
+        a[DMPH_SUM_MOMENTUM_Y] += m * v1;
+        a[DMPH_SUM_MOMENTUM_Z] += m * v2;
+        a[DMPH_SUM_KINETIC] += 0.5 * m * (v0 * v0 + v1 * v1 + v2 * v2);
+        a[DMPH_SUM_POTENTIAL] -= m * (P.g[0] * S.pos[i] + P.g[1] * S.pos[N + i] + P.g[2] * S.pos[2 * N + i]);
+    }
+    __shared__ double red[kSumThreads / 32][DMPH_SUM_COUNT];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int k = 0; k < DMPH_SUM_COUNT; ++k) {
+        a[k] = warp_sum(a[k]);
+        if (lane == 0) red[w][k] = a[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < DMPH_SUM_COUNT) {
+        double x = 0.0;
+        for (int q = 0; q < kSumThreads / 32; ++q) x += red[q][threadIdx.x];
+        part[blockIdx.x * DMPH_SUM_COUNT + threadIdx.x] = x;
+    }
+}
+
+__global__ void k_global_sums_final(const double *__restrict__ part, double *__restrict__ out)
+{
+    const int k = threadIdx.x;
+    if (k >= DMPH_SUM_COUNT) return;
+    double x = 0.0;
+    for (int b = 0; b < kSumBlocks; ++b) x += part[b * DMPH_SUM_COUNT + k];
+    out[k] = x;
+}
+
+extern "C" int dmph_get_global_sums(dmph_ctx *ctx, double sums[DMPH_SUM_COUNT])
+{
+    if (!ctx || !sums) return DMPH_EINVAL;
+    if (!ctx->sums) {  // partial sums and the result, allocated on first use
+        const int rc = dalloc(ctx, &ctx->sums, (size_t)(kSumBlocks + 1) * DMPH_SUM_COUNT);
+        if (rc) return rc;
+    }
+    if (ctx->fp32) launch_export32(ctx->P, ctx->S, ctx->S.pos, ctx->S.vel, ctx->st);
+    k_global_sums<<<kSumBlocks, kSumThreads, 0, ctx->st>>>(ctx->P, ctx->S, ctx->dB, ctx->sums);
+    double *out = ctx->sums + (size_t)kSumBlocks * DMPH_SUM_COUNT;
+    k_global_sums_final<<<1, 32, 0, ctx->st>>>(ctx->sums, out);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(sums, out, DMPH_SUM_COUNT * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return DMPH_OK;
+}
+
 // sums of the list lengths over all slots and over the fluid and debris slots
 __global__ void k_list_stats(const int *__restrict__ nbn, int n, const int *__restrict__ dB,
                              unsigned long long *__restrict__ out)

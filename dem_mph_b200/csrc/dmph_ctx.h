@@ -46,6 +46,7 @@ struct dmph_ctx {
     int *flag = nullptr, *offs = nullptr, *bsums = nullptr, *total = nullptr;
     unsigned long long *maxshift = nullptr;
     unsigned long long *stats = nullptr;      // dmph_get_list_stats counters
+    double *sums = nullptr;                   // dmph_get_global_sums partials and result
     unsigned long long *h_maxshift = nullptr;  // pinned
     int *h_small = nullptr;                    // pinned scratch for small read-backs
     int *dB = nullptr;         // device bounds (DevBound)

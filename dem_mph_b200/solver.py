@@ -39,6 +39,7 @@ def lib():
         L.dmph_get_field.argtypes = [vp, C.c_int, vp]
         L.dmph_get_info.argtypes = [vp, vp]
         L.dmph_get_neighbor_list.argtypes = [vp, vp, vp, C.c_int64]
+        L.dmph_get_global_sums.argtypes = [vp, vp]
         L.dmph_get_list_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
         L.dmph_set_bodies.argtypes = [vp, C.c_int, vp, vp]
         L.dmph_get_bodies.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
@@ -155,6 +156,13 @@ class Solver:
         ind = np.empty(max(int(ptr[-1]), 1), np.int32)
         self._check(lib().dmph_get_neighbor_list(self._h, _ptr(ptr), _ptr(ind), int(ptr[-1])))
         return ptr, ind[:int(ptr[-1])]
+
+    def global_sums(self):
+        """FP64 sums over fluid and debris (dmph_get_global_sums): dict with
+        mass, momentum (3), kinetic and potential energy"""
+        out = np.zeros(6)
+        self._check(lib().dmph_get_global_sums(self._h, _ptr(out)))
+        return {"mass": out[0], "momentum": out[1:4].copy(), "kinetic": out[4], "potential": out[5]}
 
     def list_stats(self, with_overflow=False):
         """(entries walked by pass A, entries walked by pass B) of the current

@@ -227,6 +227,26 @@ int dmph_get_info(dmph_ctx *ctx, dmph_info *info);
 int dmph_get_neighbor_list(dmph_ctx *ctx, int64_t *ptr, int32_t *ind, int64_t capacity);
 
 /*
+ * Global sums over the fluid and debris particles (no counterpart in the
+ * reference): total mass, momentum, kinetic energy 0.5 m |v|^2 and the
+ * potential energy of gravity -m g.x, in FP64 on the GPU with a fixed-order
+ * reduction (the same bits on every call for the same state).  In the FP32
+ * build the fluid's positions and velocities are widened from the FP32
+ * state, the debris use their FP64 master state.  Debris masses are their
+ * body's density times the particle volume in rigid-body mode.
+ */
+enum {
+    DMPH_SUM_MASS = 0,
+    DMPH_SUM_MOMENTUM_X = 1,
+    DMPH_SUM_MOMENTUM_Y = 2,
+    DMPH_SUM_MOMENTUM_Z = 3,
+    DMPH_SUM_KINETIC = 4,
+    DMPH_SUM_POTENTIAL = 5,
+    DMPH_SUM_COUNT = 6
+};
+int dmph_get_global_sums(dmph_ctx *ctx, double sums[DMPH_SUM_COUNT]);
+
+/*
  * Size of the pair work of the current Verlet lists (no counterpart in the
  * reference): the entries pass A walks (all particles with a list) and those
  * pass B walks (fluid and debris).  In the FP32 build, lists made with the

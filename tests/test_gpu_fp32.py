@@ -275,3 +275,40 @@ def test_debris_neighbour_counts_from_lists(bodies):
     snc_ref = np.add.reduceat(solid_nb, ptr[:-1]) * (np.diff(ptr) > 0)
     assert np.array_equal(snc[deb], snc_ref[deb])
     g.close()
+
+
+def test_global_sums_fp64_on_the_gpu_and_fp32_error():
+    """dmph_get_global_sums: the FP64 build's sums equal numpy's over its own
+    state; the FP32 build's, after 100 steps, are within their error against
+    the FP64 run (reported), and two calls give the same bits."""
+    p, typ, x, v = load_scene("small3d_fluid")
+    a = solver.Solver(p, typ, x, v)  # FP64
+    q = p.copy()
+    q.precision = PRECISION_FP32_SPLIT
+    b = solver.Solver(q, typ, x, v)
+    a.step(100)
+    b.step(100)
+    sa, sb = a.global_sums(), b.global_sums()
+    sb2 = b.global_sums()
+    assert all(np.array_equal(np.asarray(sb2[k]), np.asarray(sb[k])) for k in sb)
+    t, xs, vs, _ = a.state()
+    m = a.field("Mass")
+    keep = t < 4
+    mv = m[keep, None] * vs[keep]
+    g = np.array(list(p.gravity))
+    ref = {"mass": m[keep].sum(), "momentum": mv.sum(axis=0),
+           "kinetic": 0.5 * (m[keep] * (vs[keep] ** 2).sum(axis=1)).sum(),
+           "potential": -(m[keep] * (xs[keep] @ g)).sum()}
+    pscale = m[keep].sum() * np.abs(vs[keep]).max()
+    assert abs(sa["mass"] - ref["mass"]) <= 1e-12 * ref["mass"]
+    assert np.abs(sa["momentum"] - ref["momentum"]).max() <= 1e-12 * pscale
+    assert abs(sa["kinetic"] - ref["kinetic"]) <= 1e-12 * ref["kinetic"]
+    assert abs(sa["potential"] - ref["potential"]) <= 1e-12 * abs(ref["potential"])
+    err = {"mass": abs(sb["mass"] - sa["mass"]) / sa["mass"],
+           "momentum": np.abs(sb["momentum"] - sa["momentum"]).max() / pscale,
+           "kinetic": abs(sb["kinetic"] - sa["kinetic"]) / sa["kinetic"],
+           "potential": abs(sb["potential"] - sa["potential"]) / abs(sa["potential"])}
+    print("FP32 global sums against FP64 after 100 steps:", err)
+    assert err["mass"] <= 1e-14 and err["momentum"] <= 1e-4 and err["kinetic"] <= 1e-4 and err["potential"] <= 1e-6
+    a.close()
+    b.close()
