@@ -70,7 +70,13 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
     // per-particle DEM constants take the last neighbour in the network's
     // order (:2305-2341), so scenes with debris outside rigid bodies keep
     // the network
-    if (ctx->csort && (ctx->n_solid == 0 || ctx->Bd.B > 0)) {
+    const bool csort = ctx->csort && (ctx->n_solid == 0 || ctx->Bd.B > 0);
+    // walls at rest stay in their cells, and the stable counting sort keeps
+    // their relative order, so after the first sort every wall keeps its slot
+    // (walls sort after fluid and debris, whose counts never change): the
+    // permutation and the copies then cover only the fluid and debris slots
+    const size_t np = (ctx->fp32 && csort && ctx->walls_rest && !first) ? (size_t)(ctx->n_fluid + ctx->n_solid) : N;
+    if (csort) {
         launch_counting_sort(P, S.pos, S.type, ctx->ckeys, ctx->ccounts, ctx->words2, ctx->words, S.cell_start,
                              ctx->bsums, ctx->total, st);
     } else {
@@ -79,20 +85,22 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
         launch_cell_start(P, ctx->words, S.cell_start, st);
     }
     if (ctx->fp32) {
-        launch_permute32(P, ctx->words, S.pos, S.v4, S.type, S.pidx, ctx->p4b, ctx->v4b, ctx->type2, ctx->pidx2,
-                         S.xref, S.xref4, S.bid, ctx->bid2, S.vel, ctx->pos2, ctx->vel2, st);
-        cudaMemcpyAsync(S.p4, ctx->p4b, N * sizeof(float4), cudaMemcpyDeviceToDevice, st);
-        cudaMemcpyAsync(S.v4, ctx->v4b, N * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+        launch_permute32(P, (int)np, ctx->words, S.pos, S.v4, S.type, S.pidx, ctx->p4b, ctx->v4b, ctx->type2,
+                         ctx->pidx2, S.xref, S.xref4, S.bid, ctx->bid2, S.vel, ctx->pos2, ctx->vel2, st);
+        cudaMemcpyAsync(S.p4, ctx->p4b, np * sizeof(float4), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(S.v4, ctx->v4b, np * sizeof(float4), cudaMemcpyDeviceToDevice, st);
     } else {
         launch_permute(P, ctx->words, S.pos, S.vel, S.type, S.pidx, ctx->pos2, ctx->vel2, ctx->type2, ctx->pidx2,
                        S.xref, S.bid, ctx->bid2, st);
     }
-    cudaMemcpyAsync(S.pos, ctx->pos2, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(S.vel, ctx->vel2, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(S.type, ctx->type2, N * sizeof(int), cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(S.pidx, ctx->pidx2, N * sizeof(int), cudaMemcpyDeviceToDevice, st);
+    for (int d = 0; d < 3; d++) {
+        cudaMemcpyAsync(S.pos + d * N, ctx->pos2 + d * N, np * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(S.vel + d * N, ctx->vel2 + d * N, np * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    }
+    cudaMemcpyAsync(S.type, ctx->type2, np * sizeof(int), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(S.pidx, ctx->pidx2, np * sizeof(int), cudaMemcpyDeviceToDevice, st);
     if (S.bid) {
-        cudaMemcpyAsync(S.bid, ctx->bid2, N * sizeof(int), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(S.bid, ctx->bid2, np * sizeof(int), cudaMemcpyDeviceToDevice, st);
         launch_slot_of_row(P, S.pidx, ctx->Bd.slot_of_row, st);
     }
     S.skey = ctx->words;
@@ -405,7 +413,10 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         delete ctx;
         return rc;
     }
-    for (int i = 0; i < n; i++) ctx->n_solid += (type[i] >= DMPH_SOLID_BEGIN && type[i] < DMPH_SOLID_END) ? 1 : 0;
+    for (int i = 0; i < n; i++) {
+        ctx->n_solid += (type[i] >= DMPH_SOLID_BEGIN && type[i] < DMPH_SOLID_END) ? 1 : 0;
+        ctx->n_fluid += type[i] < DMPH_SOLID_BEGIN ? 1 : 0;
+    }
     ctx->walls_rest = true;
     for (int t = DMPH_WALL_BEGIN; t < DMPH_WALL_END; ++t)
         for (int d = 0; d < 3; ++d)

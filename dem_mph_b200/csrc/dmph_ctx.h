@@ -41,6 +41,7 @@ struct dmph_ctx {
     // scattered words before each key's range is ordered
     bool csort = false;
     int n_solid = 0;  // debris particles (types 2-3) of the scene
+    int n_fluid = 0;  // fluid particles (types 0-1)
     int *ckeys = nullptr, *ccounts = nullptr;
     unsigned long long *words2 = nullptr;
     int *flag = nullptr, *offs = nullptr, *bsums = nullptr, *total = nullptr;

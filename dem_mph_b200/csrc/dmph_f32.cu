@@ -1157,7 +1157,9 @@ __global__ void k_export32(DevParams P, DevState S, double *pos, double *vel, in
 
 // permutation of the FP32 state at a rebuild: the new slot's cell comes from
 // its sorted key, its position is re-expressed relative to that cell
-__global__ void k_permute32(DevParams P, const unsigned long long *__restrict__ words, const double *__restrict__ xabs,
+// slots [0, n) (n < N: the walls keep their slots, see enqueue_rebuild)
+__global__ void k_permute32(DevParams P, int n, const unsigned long long *__restrict__ words,
+                            const double *__restrict__ xabs,
                             const float4 *__restrict__ v_in, const int *__restrict__ type_in,
                             const int *__restrict__ pidx_in, float4 *__restrict__ p_out, float4 *__restrict__ v_out,
                             int *__restrict__ type_out, int *__restrict__ pidx_out, double *__restrict__ xref,
@@ -1166,7 +1168,7 @@ __global__ void k_permute32(DevParams P, const unsigned long long *__restrict__ 
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int N = P.N;
-    if (i >= N) return;
+    if (i >= n) return;
     const unsigned long long wd = words[i];
     const int src = (int)word_slot(wd);
     const int kc = (int)(word_key(wd) % (unsigned)P.T);
@@ -1555,13 +1557,13 @@ void launch_import32(const DevParams &P, const DevState &S, const double *pos, c
 {
     k_import32<<<(P.N + 255) / 256, 256, 0, st>>>(P, S, pos, vel);
 }
-void launch_permute32(const DevParams &P, const unsigned long long *words, const double *xabs, const float4 *v_in,
-                      const int *type_in, const int *pidx_in, float4 *p_out, float4 *v_out, int *type_out,
-                      int *pidx_out, double *xref, float4 *xref4, const int *bid_in, int *bid_out, const double *vabs,
-                      double *pos_out, double *vel_out, cudaStream_t st)
+void launch_permute32(const DevParams &P, int n, const unsigned long long *words, const double *xabs,
+                      const float4 *v_in, const int *type_in, const int *pidx_in, float4 *p_out, float4 *v_out,
+                      int *type_out, int *pidx_out, double *xref, float4 *xref4, const int *bid_in, int *bid_out,
+                      const double *vabs, double *pos_out, double *vel_out, cudaStream_t st)
 {
-    k_permute32<<<(P.N + 255) / 256, 256, 0, st>>>(P, words, xabs, v_in, type_in, pidx_in, p_out, v_out, type_out,
-                                                   pidx_out, xref, xref4, bid_in, bid_out, vabs, pos_out, vel_out);
+    k_permute32<<<(n + 255) / 256, 256, 0, st>>>(P, n, words, xabs, v_in, type_in, pidx_in, p_out, v_out, type_out,
+                                                 pidx_out, xref, xref4, bid_in, bid_out, vabs, pos_out, vel_out);
 }
 void launch_widen_f(const float *in, double *out, int n, cudaStream_t st)
 {

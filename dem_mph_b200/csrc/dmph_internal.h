@@ -75,10 +75,10 @@ void launch_ens_fluid_accel32(const EnsScene *tab, int ns, cudaStream_t st);
 void launch_fluid_accel32(const DevParams32 &Q, const DevState &S, const int *dB, cudaStream_t st);
 void launch_export32(const DevParams &P, const DevState &S, double *pos, double *vel, cudaStream_t st);
 void launch_import32(const DevParams &P, const DevState &S, const double *pos, const double *vel, cudaStream_t st);
-void launch_permute32(const DevParams &P, const unsigned long long *words, const double *xabs, const float4 *v_in,
-                      const int *type_in, const int *pidx_in, float4 *p_out, float4 *v_out, int *type_out,
-                      int *pidx_out, double *xref, float4 *xref4, const int *bid_in, int *bid_out, const double *vabs,
-                      double *pos_out, double *vel_out, cudaStream_t st);
+void launch_permute32(const DevParams &P, int n, const unsigned long long *words, const double *xabs,
+                      const float4 *v_in, const int *type_in, const int *pidx_in, float4 *p_out, float4 *v_out,
+                      int *type_out, int *pidx_out, double *xref, float4 *xref4, const int *bid_in, int *bid_out,
+                      const double *vabs, double *pos_out, double *vel_out, cudaStream_t st);
 void launch_solid_force_to64(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 void launch_sync_solids32(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 double lattice_n0p32(const DevParams &P, const DevParams32 &Q, cudaStream_t st);
