@@ -77,8 +77,8 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
     // permutation and the copies then cover only the fluid and debris slots
     const size_t np = (ctx->fp32 && csort && ctx->walls_rest && !first) ? (size_t)(ctx->n_fluid + ctx->n_solid) : N;
     if (csort) {
-        launch_counting_sort(P, S.pos, S.type, ctx->ckeys, ctx->ccounts, ctx->words2, ctx->words, S.cell_start,
-                             ctx->bsums, ctx->total, st);
+        launch_counting_sort(P, (int)np, S.pos, S.type, ctx->ckeys, ctx->ccounts, ctx->words2, ctx->words,
+                             S.cell_start, ctx->bsums, ctx->total, st);
     } else {
         launch_keys(P, S.pos, S.type, ctx->words, st);
         launch_bitonic(ctx->words, P.P2, P.P2log, st);

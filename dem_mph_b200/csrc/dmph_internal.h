@@ -15,8 +15,9 @@ void launch_bitonic(unsigned long long *words, int n, int nlog, cudaStream_t st)
 int bitonic_launch_count(int n, int nlog);  // kernels launch_bitonic issues
 void launch_cell_start(const DevParams &P, const unsigned long long *words, int *start, cudaStream_t st);
 // FP32 build: stable counting sort of the cell keys into words[0, N) and
-// cell_start (6 kernels); nonzero when 3T + 1 keys exceed the scan's range
-int launch_counting_sort(const DevParams &P, const double *pos, const int *type, int *keys, int *counts,
+// cell_start (6 kernels); slots from n_move on (walls that keep their slots)
+// are left as they are; nonzero when 3T + 1 keys exceed the scan's range
+int launch_counting_sort(const DevParams &P, int n_move, const double *pos, const int *type, int *keys, int *counts,
                          unsigned long long *tmp, unsigned long long *words, int *cell_start, int *block_sums,
                          int *total, cudaStream_t st);
 constexpr long long kCountingSortMaxKeys = 4096LL * 4096LL;

@@ -73,22 +73,23 @@ __global__ void k_count_keys(DevParams P, const double *__restrict__ pos, const 
     atomicAdd(counts + k, 1);
 }
 
-__global__ void k_scatter_keys(DevParams P, const int *__restrict__ keys, const int *__restrict__ start,
+// slots [0, n) (n < N: the walls keep their slots and their words)
+__global__ void k_scatter_keys(DevParams P, int n, const int *__restrict__ keys, const int *__restrict__ start,
                                int *__restrict__ cursor, unsigned long long *__restrict__ tmp)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.N) return;
+    if (i >= n) return;
     const int k = keys[i];
     tmp[start[k] + atomicAdd(cursor + k, 1)] = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)i;
 }
 
 // one warp per 32 keys; each key's range is ordered by rank (the number of
 // smaller words in the range), for any range length
-__global__ void k_sort_cells(DevParams P, const unsigned long long *__restrict__ tmp, const int *__restrict__ start,
-                             unsigned long long *__restrict__ words)
+// keys [0, nseg)
+__global__ void k_sort_cells(DevParams P, int nseg, const unsigned long long *__restrict__ tmp,
+                             const int *__restrict__ start, unsigned long long *__restrict__ words)
 {
     const int lane = threadIdx.x & 31;
-    const int nseg = 3 * P.T;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int k0 = gw * 32; k0 < nseg; k0 += nw * 32) {
@@ -116,10 +117,13 @@ __global__ void k_sort_cells(DevParams P, const unsigned long long *__restrict__
     }
 }
 
-int launch_counting_sort(const DevParams &P, const double *pos, const int *type, int *keys, int *counts,
+int launch_counting_sort(const DevParams &P, int n_move, const double *pos, const int *type, int *keys, int *counts,
                          unsigned long long *tmp, unsigned long long *words, int *cell_start, int *block_sums,
                          int *total, cudaStream_t st)
 {
+    // n_move < N: the walls, which sort last, keep their slots (see
+    // enqueue_rebuild), so only the slots [0, n_move) are scattered and only
+    // the fluid and debris keys ordered; the walls still count for cell_start
     const int nk = 3 * P.T + 1;
     const int g = (P.N + 255) / 256;
     cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nk, st);
@@ -127,8 +131,8 @@ int launch_counting_sort(const DevParams &P, const double *pos, const int *type,
     const int rc = launch_exclusive_scan<int>(counts, cell_start, nk, block_sums, total, st);
     if (rc) return rc;
     cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nk, st);
-    k_scatter_keys<<<g, 256, 0, st>>>(P, keys, cell_start, counts, tmp);
-    k_sort_cells<<<148 * 8, 256, 0, st>>>(P, tmp, cell_start, words);
+    k_scatter_keys<<<(n_move + 255) / 256, 256, 0, st>>>(P, n_move, keys, cell_start, counts, tmp);
+    k_sort_cells<<<148 * 8, 256, 0, st>>>(P, n_move < P.N ? 2 * P.T : 3 * P.T, tmp, cell_start, words);
     return 0;
 }
 
