@@ -85,6 +85,8 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
         launch_cell_start(P, ctx->words, S.cell_start, st);
     }
     if (ctx->fp32) {
+        // the walls' wall-wall sums are kept only while every wall keeps its slot
+        if (np == N && S.st_valid) cudaMemsetAsync(S.st_valid, 0, N * sizeof(int), st);
         launch_permute32(P, (int)np, ctx->words, S.pos, S.v4, S.type, S.pidx, ctx->p4b, ctx->v4b, ctx->type2,
                          ctx->pidx2, S.xref, S.xref4, S.bid, ctx->bid2, S.vel, ctx->pos2, ctx->vel2, st);
         cudaMemcpyAsync(S.p4, ctx->p4b, np * sizeof(float4), cudaMemcpyDeviceToDevice, st);
@@ -535,6 +537,7 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
         if (ctx->fp32) {
             AL(S.vsp_st, N);
             AL(S.st4, N);
+            AL(S.st_valid, N);
         }
         ctx->use_list = true;
     }

@@ -576,14 +576,18 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
     chunk_cell(P, key_cell, cix, ciy, ciz);
     const float4 pi = S.p4[active ? i : ch.i0];
     const int ti = unpack_type(__float_as_uint(pi.w));
-    const bool wall_i = split && is_wall(ti);
+    // walls at rest: their wall-wall sums were made at an earlier rebuild and
+    // still hold (same slots, same positions) when st_valid says so for the
+    // whole chunk; the walk then skips the wall candidates altogether
+    const bool keep_sums = split && is_wall(ti) && __all_sync(kFull, !active || S.st_valid[i] != 0);
+    const bool wall_i = split && is_wall(ti) && !keep_sums;
     const IA I{pi, make_float4(0.f, 0.f, 0.f, 0.f), ti, is_solid(ti), is_wall(ti)};
     AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
     const float a0 = -2.f * pi.x, a1 = -2.f * pi.y, a2 = -2.f * pi.z;
     const float thr = rc2 * (1.f + 1e-4f) - fmaf(pi.x, pi.x, fmaf(pi.y, pi.y, pi.z * pi.z));
     int cnt = 0;
     traverse_stencil_batched(
-        P, S.cell_start, key_cell, lane, 7u,
+        P, S.cell_start, key_cell, lane, keep_sums ? 3u : 7u,
         [&](int j, int slot) {
             const float4 pj = S.p4[j];
             const unsigned w = __float_as_uint(pj.w);
@@ -677,6 +681,7 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
     if (wall_i) {
         S.vsp_st[i] = A.vsp;
         S.st4[i] = make_float4(A.dA, A.g0, A.g1, A.g2);
+        S.st_valid[i] = 1;
     }
 }
 

@@ -20,6 +20,7 @@ struct DevState {
     int nbl_cap;
     double *vsp_st;
     float4 *st4;
+    int *st_valid;  // 1: the slot's vsp_st and st4 hold (cleared whenever walls change slots)
     // FP64 particle state, component planes v[d*N + i], current sorted order
     double *pos, *vel, *frc, *xref;
     int *type, *pidx;
