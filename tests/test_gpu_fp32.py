@@ -312,3 +312,25 @@ def test_global_sums_fp64_on_the_gpu_and_fp32_error():
     assert err["mass"] <= 1e-14 and err["momentum"] <= 1e-4 and err["kinetic"] <= 1e-4 and err["potential"] <= 1e-6
     a.close()
     b.close()
+
+
+def test_walls_at_rest_keep_their_slots():
+    """The rebuild leaves the wall slots alone when the walls are at rest and
+    the counting sort is in use (rigid-body debris); this checks the
+    invariant that shortcut relies on: every wall particle keeps its slot
+    across rebuilds.  (The results of such runs are compared with the FP64
+    oracle in test_gpu_bodies.py and by smoke.)"""
+    from dem_mph_b200 import scenes
+    s = scenes.small()
+    p = s.params.copy()
+    p.precision = PRECISION_FP32_SPLIT
+    g = solver.Solver(p, s.type, s.x, s.v)
+    g.set_bodies(s.body, s.body_density)
+    g.step(1)
+    t0, _, _, id0 = g.state()
+    walls = t0 >= 4
+    g.step(200)
+    assert g.info().rebuilds > 1
+    t1, x1, _, id1 = g.state()
+    assert np.array_equal(id1[walls], id0[walls]) and np.array_equal(t1[walls], t0[walls])
+    g.close()
