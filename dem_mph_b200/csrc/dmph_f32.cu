@@ -134,12 +134,22 @@ struct IA {  // particle i of pass A
     int ti;
     bool si, wi;
 };
-// VolStrainP = sum(w) - N0p cancels to ~1e-3 of the sum, so the sums are
-// carried in FP64 (one add per pair); the pair terms stay FP32
+// VolStrainP = sum(w) - N0p cancels to ~1e-3 of the sum, so that sum is
+// carried in FP64 (one add per pair); the divergence terms go into a short
+// FP32 partial (dq: the pairs of one block of 8 list entries, or one pair in
+// the stencil walk) that is added to the FP64 sum at the end of the block
+// (flush_a); the pair terms stay FP32
 struct AccA {
     double vsp, div;
     float dA, g0, g1, g2;
+    float dq;
 };
+
+__device__ __forceinline__ void flush_a(AccA &A)
+{
+    A.div += (double)A.dq;
+    A.dq = 0.f;
+}
 
 // one pair (pj in the frame of i's cell, .w = type bits), within the cut-off
 template <bool ST>
@@ -148,17 +158,18 @@ __device__ __forceinline__ void pair_a32(const DevParams32 &Q, const IA &I, cons
     const float q0 = pj.x - I.pi.x, q1 = pj.y - I.pi.y, q2 = pj.z - I.pi.z;
     const float r2 = fmaf(q0, q0, fmaf(q1, q1, q2 * q2));
     const int tj = __float_as_int(pj.w);
-    // correctly rounded sqrt: the approximate reciprocal square root has a
-    // bias that would add up over ~100 neighbours
+    // correctly rounded sqrt for the weights: the approximate reciprocal
+    // square root has a bias that would add up over ~100 neighbours in the
+    // strain sum; the divergence (zero at rest) takes the approximate 1/r
     const float r = sqrtf(r2);
-    const float ir = __frcp_rn(r);
+    const float ir = rsqrtf(r2);
     if (!ST || r2 <= Q.RP2) {
         const float a = fmaf(-r, Q.iRP, 1.f);  // 1 - r/h
         A.vsp += (double)(Q.Bp * a * a);
         const bool sj = is_solid(tj);
         if (!((I.si && is_wall(tj)) || (sj && I.wi) || (sj && I.si))) {
             const float uq = fmaf(vj.x - I.vi.x, q0, fmaf(vj.y - I.vi.y, q1, (vj.z - I.vi.z) * q2));
-            A.div -= (double)(uq * ir * Q.dwp * a);  // -(u.e) dw
+            A.dq -= uq * ir * Q.dwp * a;  // -(u.e) dw
         }
     }
     if (ST && !(I.si && is_wall(tj))) {
@@ -228,7 +239,7 @@ __device__ __forceinline__ void pass_a32_body(const DevParams &P, const DevParam
         const int ti = unpack_type(__float_as_uint(pi.w));
         const IA I{pi, vi, ti, is_solid(ti), is_wall(ti)};
         const float cut2 = ST ? fmaxf(Q.RP2, fmaxf(Q.RA2, Q.RG2)) : Q.RP2;
-        AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
+        AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f, 0.f};
         traverse_stencil_batched(
             P, S.cell_start, key_cell, lane, 7u,
             [&](int j, int slot) { stage32(P, Q, S, tl, j, slot, cix, ciy, ciz, false); },
@@ -249,6 +260,7 @@ __device__ __forceinline__ void pass_a32_body(const DevParams &P, const DevParam
                     const int s = __ffs(m) - 1;
                     m &= m - 1;
                     pair_a32<ST>(Q, I, tl.p[s], tl.v[s], A);
+                    flush_a(A);
                 }
             });
         // combine the L partial sums of each particle
@@ -582,7 +594,7 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
     const bool keep_sums = split && is_wall(ti) && __all_sync(kFull, !active || S.st_valid[i] != 0);
     const bool wall_i = split && is_wall(ti) && !keep_sums;
     const IA I{pi, make_float4(0.f, 0.f, 0.f, 0.f), ti, is_solid(ti), is_wall(ti)};
-    AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
+    AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f, 0.f};
     const float a0 = -2.f * pi.x, a1 = -2.f * pi.y, a2 = -2.f * pi.z;
     const float thr = rc2 * (1.f + 1e-4f) - fmaf(pi.x, pi.x, fmaf(pi.y, pi.y, pi.z * pi.z));
     int cnt = 0;
@@ -760,7 +772,7 @@ __device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const Dev
     const float4 pi = S.p4[i];
     const int ti = unpack_type(__float_as_uint(pi.w));
     const IA I{pi, S.v4[i], ti, is_solid(ti), is_wall(ti)};
-    AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f};
+    AccA A{0.0, 0.0, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (split && I.wi) {
         A.vsp = S.vsp_st[i];
         if (ST) {
@@ -788,7 +800,10 @@ __device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const Dev
             const float q0 = pj[u].x - pi.x, q1 = pj[u].y - pi.y, q2 = pj[u].z - pi.z;
             if (k0 + u < cnt && fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= cut2) pair_a32<ST>(Q, I, pj[u], vj[u], A);
         }
+        // one FP64 add per block of 8 entries, whatever BATCH is
+        if (((k0 + BATCH) & 7) == 0) flush_a(A);
     }
+    flush_a(A);
     finish_a32<ST>(P, Q, S, i, I, A);
 }
 
