@@ -665,12 +665,23 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
                 // entry k of slot i sits at block k / 8 (stride 8 N words), word k % 8
                 int k = cnt + before;
                 unsigned *blk = S.nbl + list_index(k & ~7, i, ld);
-                while (m) {  // ascending candidate order
-                    const int s0 = __ffs(m) - 1;
-                    m &= m - 1;
-                    if (k < cap) blk[k & 7] = tl.e[part * G + s0];
-                    ++k;
-                    if ((k & 7) == 0) blk += 8 * ld;
+                const unsigned *te = tl.e + part * G;
+                if (k + c <= cap) {  // the usual case: no capacity test per entry
+                    while (m) {      // ascending candidate order
+                        const int s0 = __ffs(m) - 1;
+                        m &= m - 1;
+                        blk[k & 7] = te[s0];
+                        ++k;
+                        if ((k & 7) == 0) blk += 8 * ld;
+                    }
+                } else {
+                    while (m) {
+                        const int s0 = __ffs(m) - 1;
+                        m &= m - 1;
+                        if (k < cap) blk[k & 7] = te[s0];
+                        ++k;
+                        if ((k & 7) == 0) blk += 8 * ld;
+                    }
                 }
             }
             cnt += total;
@@ -698,7 +709,7 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
 }
 
 template <bool ST>
-__global__ void __launch_bounds__(8 * kWarp, 4) k_build_list32(DevParams P, DevParams32 Q, DevState S, int *dB, float rc2,
+__global__ void __launch_bounds__(8 * kWarp, 3) k_build_list32(DevParams P, DevParams32 Q, DevState S, int *dB, float rc2,
                                                             int split)
 {
     __shared__ TileL tiles[8];
