@@ -143,6 +143,12 @@ def reference_time(scene, steps, warmup, threads=None):
         return json.loads(line), None
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# list-mode kernels on config 2, FP32 split, late in the flow (after 6,000
+# steps), from ncu captures of the bench's own command
+TRAFFIC_CONFIG2_FP32 = {"pass_a": 765.5e6, "pass_b": 690.9e6, "list_build": 824.2e6}
+
+
 def algorithmic_bytes(prec):
     """Compulsory HBM bytes per particle of the dominant kernel (pass B) with
     neighbour re-reads served on chip: read position, velocity, pressure and
@@ -243,7 +249,7 @@ def main():
     barrier()
     inf_t = g.info()
     launches = int(inf_t.kernel_launches - l0)
-    rebuilds_timed = int(inf_t.rebuilds)
+    rebuilds_timed = int(inf_t.rebuilds) - rebuilds_before
     ms_max = max_over_ranks(ms, world, "cuda")
     inf = g.info()
     value = n * world * args.steps / (ms_max / 1e3)
@@ -255,39 +261,56 @@ def main():
     g.step(prof_steps)
     ph = g.phase_times()
     g.set_profiling(False)
-    pb_ms, pb_n = ph["pass_b"]
-    pa_ms, pa_n = ph["pass_a"]
-    top = "pass_b" if pb_ms >= pa_ms else "pass_a"
     inf = g.info()
     n_fs = inf.n_fluid + inf.n_solid
     peaks, peak_src = load_peaks()
     bpp = algorithmic_bytes(args.precision)
-    if top == "pass_b":
-        bytes_launch = n_fs * bpp
-        dur = pb_ms / max(pb_n, 1)
-    else:
-        bytes_launch = n * (bpp - 24)
-        dur = pa_ms / max(pa_n, 1)
-    achieved = bytes_launch / (dur / 1e3) / 1e9
-    # DRAM bytes of one list-pass launch on config 2 from an ncu capture
-    # (dram__bytes_read.sum + dram__bytes_write.sum); the list is most of it
+    ea, eb = g.list_stats()
+    # per kernel: mean launch time over the profiled steps, launches over the
+    # timed run, and compulsory HBM bytes per launch.  Pass B: read p4, v4 and
+    # pressure, write force and velocity of the fluid and debris; pass A: read
+    # p4 and v4, write pressure and the divergence terms of every particle;
+    # list build: write every list entry (4 B) and count (4 B), read each
+    # particle's position once (16 B)
+    kern = {}
+    for ph_name, kname, nbytes, launches in (
+            ("pass_a", "k_pass_a32_list", n * (bpp - 24), args.steps),
+            ("pass_b", "k_pass_b32_list", n_fs * bpp, args.steps),
+            ("list_build", "k_build_list32", 4 * ea + 20 * n, rebuilds_timed)):
+        tot, cnt = ph.get(ph_name, (0.0, 0))
+        if cnt == 0 or (ph_name == "list_build" and args.precision != "fp32"):
+            continue
+        if args.precision != "fp32":
+            kname = "k_" + ph_name
+        kern[ph_name] = {"kernel": kname, "launch_ms": tot / cnt, "bytes": nbytes,
+                         "run_ms": tot / cnt * launches}
+    top = max(kern, key=lambda k: kern[k]["run_ms"])
+    dur = kern[top]["launch_ms"]
+    achieved = kern[top]["bytes"] / (dur / 1e3) / 1e9
+    # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+    # an ncu capture of the same kernels on config 2 late in the flow
     traffic = None
     if args.workload == "config2" and args.precision == "fp32":
-        traffic = 685.2e6 if top == "pass_b" else 745.9e6
+        traffic = TRAFFIC_CONFIG2_FP32.get(top)
     # pair work: Verlet-list entries each pass walks per launch (each entry is
     # one candidate pair: two 16-byte neighbour gathers and the pair arithmetic)
-    ea, eb = g.list_stats()
-    pa_dur, pb_dur = pa_ms / max(pa_n, 1), pb_ms / max(pb_n, 1)
+    pa_dur = kern["pass_a"]["launch_ms"] if "pass_a" in kern else float("nan")
+    pb_dur = kern["pass_b"]["launch_ms"] if "pass_b" in kern else float("nan")
     pairs = {"pass_a": {"entries_per_launch": ea, "launch_ms": pa_dur, "entries_per_s": ea / (pa_dur / 1e3)},
              "pass_b": {"entries_per_launch": eb, "launch_ms": pb_dur, "entries_per_s": eb / (pb_dur / 1e3)},
              "bound": "L1 data pipe serving the neighbour gathers (about 75% of peak in the ncu capture) "
                       "and instruction issue (about 76%)"}
-    roofline = {"bound": "hbm", "kernel": (("k_pass_b32_list" if top == "pass_b" else "k_pass_a32_list")
-                                           if args.precision == "fp32" else "k_" + top),
+    roofline = {"bound": "hbm", "kernel": kern[top]["kernel"],
                 "achieved": achieved, "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                 "traffic_source": "ncu capture of one launch of the same kernel and workload" if traffic else None,
                 "peak_source": peak_src, "launch_ms": dur,
+                "algorithmic_bytes_per_launch": kern[top]["bytes"],
+                "kernels": {k: {"kernel": v["kernel"], "launch_ms": v["launch_ms"],
+                                "ms_over_timed_run": v["run_ms"],
+                                "achieved_gbs": v["bytes"] / (v["launch_ms"] / 1e3) / 1e9,
+                                "traffic": (TRAFFIC_CONFIG2_FP32.get(k) if traffic is not None else None)}
+                            for k, v in kern.items()},
                 "phase_ms_per_step": {k: v[0] / max(prof_steps, 1) for k, v in ph.items()},
                 "phase_steps": prof_steps,
                 "pairs": pairs}
@@ -337,7 +360,7 @@ def main():
                    "n_solid": counts["solid"], "n_wall": counts["wall"], "n_debris_bodies": len(scene.body_density),
                    "debris": "rigid bodies (FP64)" if bodies else "individual DEM particles",
                    "precision": args.precision, "dt": p.dt, "dem_substeps": inf.dem_substeps,
-                   "rebuilds_in_timed_steps": rebuilds_timed - rebuilds_before, "parallelism": "replicas x%d" % world,
+                   "rebuilds_in_timed_steps": rebuilds_timed, "parallelism": "replicas x%d" % world,
                    "settle_steps": args.settle, "graph_replay": not args.no_graph,
                    "pass_variants": variants,
                    "l2": "inputs larger than L2 (particle state alone %.0f MB)" % (n * 60 / 1e6)},

@@ -46,6 +46,8 @@ static void release(dmph_ctx *ctx)
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->pe0) cudaEventDestroy(ctx->pe0);
     if (ctx->pe1) cudaEventDestroy(ctx->pe1);
+    if (ctx->pl0) cudaEventDestroy(ctx->pl0);
+    if (ctx->pl1) cudaEventDestroy(ctx->pl1);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     ctx->h_maxshift = nullptr;
     ctx->h_small = nullptr;
@@ -112,8 +114,18 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
         launch_wet_partition(P, ctx->words, S.cell_start, S.chunks, ctx->chunks2, ctx->dB, ctx->flag, ctx->offs,
                              ctx->bsums, ctx->total, st);
     if (ctx->use_list) {
+        // the list build alone is also timed as phase 6 (inside phase 1)
+        if (ctx->prof) cudaEventRecord(ctx->pl0, st);
         if (ctx->fp32) launch_build_list32(P, ctx->Q, S, ctx->dB, ctx->Wm.moving ? 0 : 1, st);
         else launch_build_list64(P, S, ctx->dB, st);
+        if (ctx->prof) {
+            cudaEventRecord(ctx->pl1, st);
+            cudaEventSynchronize(ctx->pl1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ctx->pl0, ctx->pl1);
+            ctx->phase_ms[6] += ms;
+            ctx->phase_n[6] += 1;
+        }
     }
     if (ctx->fp32 && ctx->use_list && !ctx->all_counts) launch_counts_list(P, S, ctx->dB, st);
     else launch_counts(P, S, ctx->dB, ctx->all_counts ? CR_ALL : CR_SOLID, st);
@@ -468,6 +480,8 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     CKC(cudaEventCreate(&ctx->ev1));
     CKC(cudaEventCreate(&ctx->pe0));
     CKC(cudaEventCreate(&ctx->pe1));
+    CKC(cudaEventCreate(&ctx->pl0));
+    CKC(cudaEventCreate(&ctx->pl1));
     CKC(cudaMallocHost(&ctx->h_maxshift, sizeof(unsigned long long)));
     CKC(cudaMallocHost(&ctx->h_small, 2 * B_COUNT * sizeof(int)));
     const DevParams &P = ctx->P;

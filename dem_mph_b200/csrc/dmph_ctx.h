@@ -67,7 +67,7 @@ struct dmph_ctx {
     long long launches = 0;  // kernels launched by dmph_step
     bool all_counts = false;
     bool prof = false;
-    cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+    cudaEvent_t pe0 = nullptr, pe1 = nullptr, pl0 = nullptr, pl1 = nullptr;
     double phase_ms[DMPH_PHASE_COUNT] = {0};
     long long phase_n[DMPH_PHASE_COUNT] = {0};
     std::string err;

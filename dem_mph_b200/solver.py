@@ -190,7 +190,7 @@ class Solver:
                                           _ptr(out["M"]), _ptr(out["F"]), _ptr(out["T"])))
         return out
 
-    PHASES = ("drift", "rebuild", "pass_a", "pass_b", "dem", "bodies")
+    PHASES = ("drift", "rebuild", "pass_a", "pass_b", "dem", "bodies", "list_build")
 
     def set_pair_mode(self, mode):
         """"stencil" or "list" (dmph_set_pair_mode; FP32 split build)"""

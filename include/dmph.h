@@ -403,8 +403,8 @@ int dmph_surrogate_features(dmph_ctx *ctx, float *F, int *rows);
  * overhead, so time throughput with it off); dmph_get_phase_times returns the
  * accumulated milliseconds and launch counts per phase since it was enabled:
  * index 0 drift, 1 rebuild, 2 pass A, 3 pass B, 4 DEM substeps, 5 rigid
- * bodies. */
-#define DMPH_PHASE_COUNT 6
+ * bodies, 6 the neighbour-list build alone (list mode; part of 1). */
+#define DMPH_PHASE_COUNT 7
 int dmph_set_profiling(dmph_ctx *ctx, int enable);
 int dmph_get_phase_times(dmph_ctx *ctx, double *ms, int64_t *launches, int n);
 
