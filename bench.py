@@ -273,7 +273,7 @@ def main():
     # list build: write every list entry (4 B) and count (4 B), read each
     # particle's position once (16 B)
     kern = {}
-    for ph_name, kname, nbytes, launches in (
+    for ph_name, kname, nbytes, n_launch in (
             ("pass_a", "k_pass_a32_list", n * (bpp - 24), args.steps),
             ("pass_b", "k_pass_b32_list", n_fs * bpp, args.steps),
             ("list_build", "k_build_list32", 4 * ea + 20 * n, rebuilds_timed)):
@@ -283,7 +283,7 @@ def main():
         if args.precision != "fp32":
             kname = "k_" + ph_name
         kern[ph_name] = {"kernel": kname, "launch_ms": tot / cnt, "bytes": nbytes,
-                         "run_ms": tot / cnt * launches}
+                         "run_ms": tot / cnt * n_launch}
     top = max(kern, key=lambda k: kern[k]["run_ms"])
     dur = kern[top]["launch_ms"]
     achieved = kern[top]["bytes"] / (dur / 1e3) / 1e9

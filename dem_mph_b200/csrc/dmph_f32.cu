@@ -563,9 +563,8 @@ struct TileL {
 // split: the walls are at rest until the next rebuild (set by the host when no
 // wall motion is active).  Wall-wall pairs are then summed here, once, with
 // pass A's arithmetic (pair_a32 on the same FP32 positions), and only the
-// pairs of a wall with fluid or debris go to its list; every entry whose j is
-// a wall carries kEntryStaticWall, so pass A skips gathering its (zero)
-// velocity.
+// pairs of a wall with fluid or debris go to its list; pass A reads the
+// velocity of every wall entry of such lists as zero instead of gathering it.
 // One chunk with L lanes per particle: lane = part * G + p holds particle p
 // (G = 32 / L) and tests candidates [part * G, part * G + G) of every staged
 // batch, so chunks of at most 16 (8) particles take half (a quarter) of the
@@ -611,9 +610,8 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
                         z = fmaf((float)dz, Q.cw[2], pj.z);
             tl.p[slot] = make_float4(x, y, z, fmaf(x, x, fmaf(y, y, z * z)));
             tl.t[slot] = tj;
-            tl.e[slot] = (unsigned)j | ((unsigned)((dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)) << 24) |
-                         (is_solid(tj) ? kEntrySolid : 0u) |
-                         (is_wall(tj) ? (split ? kEntryWall | kEntryStaticWall : kEntryWall) : 0u);
+            tl.e[slot] = (unsigned)j | entry_offsets(dx, dy, dz) | (is_solid(tj) ? kEntrySolid : 0u) |
+                         (is_wall(tj) ? kEntryWall : 0u);
         },
         [&](int base, int nb) {
             // called by every lane: the count exchange below needs them all.
@@ -636,7 +634,7 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
                 if (self >= 0 && self < G) m &= ~(1u << self);
                 // a batch holds candidates of one class: static walls are
                 // summed here (each part its own) and not listed
-                if (wall_i && (tl.e[0] & kEntryStaticWall)) {
+                if (wall_i && (tl.e[0] & kEntryWall)) {
                     unsigned w = m;
                     while (w) {
                         const int s0 = __ffs(w) - 1;
@@ -761,11 +759,9 @@ __device__ __forceinline__ void load_entries(const DevState &S, int k0, int cnt,
 __device__ __forceinline__ float4 list_pos(const DevParams32 &Q, const DevState &S, unsigned e, int &j)
 {
     j = (int)(e & kEntrySlot);
-    const int code = entry_code(e);
-    const int dx = code / 9 - 1, dy = (code / 3) % 3 - 1, dz = code % 3 - 1;
     const float4 pj = __ldg(S.p4 + j);  // positions are read-only in the passes
-    return make_float4(fmaf((float)dx, Q.cw[0], pj.x), fmaf((float)dy, Q.cw[1], pj.y),
-                       fmaf((float)dz, Q.cw[2], pj.z), __int_as_float(unpack_type(__float_as_uint(pj.w))));
+    return make_float4(fmaf(entry_offset(e, 0), Q.cw[0], pj.x), fmaf(entry_offset(e, 1), Q.cw[1], pj.y),
+                       fmaf(entry_offset(e, 2), Q.cw[2], pj.z), __int_as_float(unpack_type(__float_as_uint(pj.w))));
 }
 
 // BATCH list entries at a time: their index loads, then their gathers, are
@@ -804,7 +800,7 @@ __device__ __forceinline__ void pass_a32_list_slot(const DevParams &P, const Dev
             pj[u] = list_pos(Q, S, e[u], j[u]);
             // pass A writes only the .w (pressure) of v4, which it does not
             // read; a wall at rest has zero velocity, which is not gathered
-            vj[u] = (e[u] & kEntryStaticWall) ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(S.v4 + j[u]);
+            vj[u] = (split && (e[u] & kEntryWall)) ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(S.v4 + j[u]);
         }
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {

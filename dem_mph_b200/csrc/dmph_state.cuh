@@ -7,11 +7,11 @@ namespace dmph {
 
 struct DevState {
     // FP32 Verlet lists (list mode): entry k of slot i at
-    // nbl[((k / 8) * N + i) * 8 + k % 8] = j | cell-offset code << 24 (code =
-    // (dx+1)*9 + (dy+1)*3 + (dz+1) of j's rebuild-time cell relative to i's)
-    // | j's class (kEntrySolid, kEntryWall) | kEntryStaticWall when j is a
-    // wall that stays put until the next rebuild; ascending j; nbn[i] = count, -1 for slots without a list (dry
-    // walls).  Lists built with the walls at rest (dB[B_LIST_SPLIT] = 1) leave
+    // nbl[((k / 8) * N + i) * 8 + k % 8] = j | the offset (dx, dy, dz) of j's
+    // rebuild-time cell from i's, each + 1 in two bits at bits 24, 26, 28 |
+    // j's class (kEntrySolid, kEntryWall); ascending j; nbn[i] = count, -1
+    // for slots without a list (dry walls).  A wall entry of lists built with
+    // the walls at rest is a wall that stays put until the next rebuild.  Lists built with the walls at rest (dB[B_LIST_SPLIT] = 1) leave
     // the wall-wall pairs out of the walls' lists: their pass-A sums cannot
     // change before the next rebuild and are kept in vsp_st (FP64 strain sum)
     // and st4 (surface-tension density sum, gravity-centre sum)
@@ -84,10 +84,24 @@ struct DevBodies {
 // slots reads entry k of its 32 particles from 32 sectors that also hold the
 // particles' next entries.
 constexpr unsigned kEntrySlot = 0xFFFFFFu;        // j
-constexpr unsigned kEntryStaticWall = 1u << 29;    // j is a wall at rest
 constexpr unsigned kEntrySolid = 1u << 30;         // j is debris
 constexpr unsigned kEntryWall = 1u << 31;          // j is a wall
-__host__ __device__ __forceinline__ int entry_code(unsigned e) { return (int)((e >> 24) & 31u); }
+// cell offsets in -1..1 -> entry bits 24-29
+__host__ __device__ __forceinline__ unsigned entry_offsets(int dx, int dy, int dz)
+{
+    return ((unsigned)(dx + 1) << 24) | ((unsigned)(dy + 1) << 26) | ((unsigned)(dz + 1) << 28);
+}
+// offset along axis a as a float: the two bits v = offset + 1 are placed in
+// the mantissa of 2^23 (2^23 + v exactly), and 2^23 + 1 is subtracted
+__host__ __device__ __forceinline__ float entry_offset(unsigned e, int a)
+{
+    union {
+        unsigned u;
+        float f;
+    } c;
+    c.u = 0x4B000000u | ((e >> (24 + 2 * a)) & 3u);
+    return c.f - 8388609.0f;
+}
 
 __host__ __device__ __forceinline__ long long list_index(int k, int i, long long ld)
 {

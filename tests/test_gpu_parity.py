@@ -105,6 +105,18 @@ def test_step_timed_and_info():
     assert ms > 0
     inf = g.info()
     assert inf.steps == 3 and inf.dem_substeps == 2 and inf.n_solid > 0
+    # phase timing: every phase of a profiled step is recorded; the list
+    # build is timed inside the rebuild, once per rebuild
+    g.set_profiling(True)
+    r0 = g.info().rebuilds
+    g.step(20)
+    ph = g.phase_times()
+    g.set_profiling(False)
+    nreb = g.info().rebuilds - r0
+    assert set(ph) == set(solver.Solver.PHASES) and len(ph) == 7
+    assert ph["pass_a"][1] == 20 and ph["pass_b"][1] == 20 and ph["drift"][1] == 20
+    assert ph["rebuild"][1] == nreb and ph["list_build"][1] == nreb
+    assert 0.0 <= ph["list_build"][0] <= ph["rebuild"][0]
     g.close()
 
 
