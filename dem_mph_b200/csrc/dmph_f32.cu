@@ -19,6 +19,8 @@
 #include "dmph_state.cuh"
 #include "dmph_traverse.cuh"
 
+#include <type_traits>
+
 namespace dmph {
 
 
@@ -733,7 +735,7 @@ __global__ void k_list_wall_guard(int *dB)
 
 // entries k0 .. k0 + BATCH - 1 of slot i (BATCH divides 8, so they sit in one
 // block and load as one vector); entries past the count read as slot 0
-template <int BATCH>
+template <int BATCH, bool TAIL = true>
 __device__ __forceinline__ void load_entries(const DevState &S, int k0, int cnt, int i, long long ld, unsigned *e)
 {
     const unsigned *src = S.nbl + list_index(k0, i, ld);
@@ -750,9 +752,11 @@ __device__ __forceinline__ void load_entries(const DevState &S, int k0, int cnt,
     } else {
         e[0] = __ldg(src);
     }
+    if (TAIL) {
 #pragma unroll
-    for (int u = 0; u < BATCH; ++u)
-        if (k0 + u >= cnt) e[u] = 0u;
+        for (int u = 0; u < BATCH; ++u)
+            if (k0 + u >= cnt) e[u] = 0u;
+    }
 }
 
 // j's position in the frame of i's cell, type bits in .w
@@ -838,9 +842,11 @@ __device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const Dev
     const int ti = unpack_type(__float_as_uint(pi.w));
     const IB I = make_ib<ST>(P, S, i, pi, S.v4[i], ti);
     AccB B = acc_b_zero();
-    for (int k0 = 0; k0 < cnt; k0 += BATCH) {
+    // full batches without per-entry count tests, then the partial one
+    auto batch = [&](int k0, auto tail) {
+        constexpr bool TAIL = decltype(tail)::value;
         unsigned e[BATCH];
-        load_entries<BATCH>(S, k0, cnt, i, ld, e);
+        load_entries<BATCH, TAIL>(S, k0, cnt, i, ld, e);
         float4 pj[BATCH], vj[BATCH];
         int j[BATCH];
 #pragma unroll
@@ -851,7 +857,7 @@ __device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const Dev
 #pragma unroll
         for (int u = 0; u < BATCH; ++u) {
             const float q0 = pj[u].x - pi.x, q1 = pj[u].y - pi.y, q2 = pj[u].z - pi.z;
-            if (k0 + u < cnt && fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) < cut2) {
+            if ((!TAIL || k0 + u < cnt) && fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) < cut2) {
                 float4 gj = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (ST) {
                     gj = S.gc4[j[u]];
@@ -860,10 +866,16 @@ __device__ __forceinline__ void pass_b32_list_slot(const DevParams &P, const Dev
                 pair_b32<ST, CLS>(Q, I, pj[u], vj[u], gj, j[u], B);
             }
         }
+    };
+    const int full = cnt & ~(BATCH - 1);
+    int k0 = 0;
+    for (; k0 < full; k0 += BATCH) {
+        batch(k0, std::false_type{});
         // one FP64 add per block of 8 entries, whatever BATCH is, so every
         // launch variant gives the same bits
         if (((k0 + BATCH) & 7) == 0) flush_b(B);
     }
+    if (k0 < cnt) batch(k0, std::true_type{});
     flush_b(B);
     finish_b32<CLS>(P, Q, S, i, I, B);
 }
