@@ -158,6 +158,36 @@ def algorithmic_bytes(prec):
     return 16 + 16 + 4 + 16 + 16
 
 
+def kernel_table(ph, precision, n, n_fs, entries, steps, rebuilds):
+    """Per-kernel figures for the roofline block and the kernel with the most
+    device time over the timed run.
+
+    ph: {phase: (total_ms, launches)} of the profiled steps; n particles, n_fs
+    fluid and debris; entries: list entries of all particles; steps and
+    rebuilds of the timed run.  Each kernel gets its mean launch time, its
+    time over the timed run (launch time x launches in the run), and its
+    compulsory HBM bytes per launch: pass B reads p4, v4 and pressure and
+    writes force and velocity of the fluid and debris; pass A reads p4 and v4
+    and writes pressure and the divergence terms of every particle; the list
+    build writes every list entry (4 B) and count (4 B) and reads each
+    particle's position once (16 B).  Returns (table, name of the top kernel).
+    """
+    bpp = algorithmic_bytes(precision)
+    kern = {}
+    for ph_name, kname, nbytes, n_launch in (
+            ("pass_a", "k_pass_a32_list", n * (bpp - 24), steps),
+            ("pass_b", "k_pass_b32_list", n_fs * bpp, steps),
+            ("list_build", "k_build_list32", 4 * entries + 20 * n, rebuilds)):
+        tot, cnt = ph.get(ph_name, (0.0, 0))
+        if cnt == 0 or (ph_name == "list_build" and precision != "fp32"):
+            continue
+        if precision != "fp32":
+            kname = "k_" + ph_name
+        kern[ph_name] = {"kernel": kname, "launch_ms": tot / cnt, "bytes": nbytes,
+                         "run_ms": tot / cnt * n_launch}
+    return kern, max(kern, key=lambda k: kern[k]["run_ms"])
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -264,27 +294,8 @@ def main():
     inf = g.info()
     n_fs = inf.n_fluid + inf.n_solid
     peaks, peak_src = load_peaks()
-    bpp = algorithmic_bytes(args.precision)
     ea, eb = g.list_stats()
-    # per kernel: mean launch time over the profiled steps, launches over the
-    # timed run, and compulsory HBM bytes per launch.  Pass B: read p4, v4 and
-    # pressure, write force and velocity of the fluid and debris; pass A: read
-    # p4 and v4, write pressure and the divergence terms of every particle;
-    # list build: write every list entry (4 B) and count (4 B), read each
-    # particle's position once (16 B)
-    kern = {}
-    for ph_name, kname, nbytes, n_launch in (
-            ("pass_a", "k_pass_a32_list", n * (bpp - 24), args.steps),
-            ("pass_b", "k_pass_b32_list", n_fs * bpp, args.steps),
-            ("list_build", "k_build_list32", 4 * ea + 20 * n, rebuilds_timed)):
-        tot, cnt = ph.get(ph_name, (0.0, 0))
-        if cnt == 0 or (ph_name == "list_build" and args.precision != "fp32"):
-            continue
-        if args.precision != "fp32":
-            kname = "k_" + ph_name
-        kern[ph_name] = {"kernel": kname, "launch_ms": tot / cnt, "bytes": nbytes,
-                         "run_ms": tot / cnt * n_launch}
-    top = max(kern, key=lambda k: kern[k]["run_ms"])
+    kern, top = kernel_table(ph, args.precision, n, n_fs, ea, args.steps, rebuilds_timed)
     dur = kern[top]["launch_ms"]
     achieved = kern[top]["bytes"] / (dur / 1e3) / 1e9
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
