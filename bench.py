@@ -170,7 +170,8 @@ def kernel_table(ph, precision, n, n_fs, entries, steps, rebuilds):
     writes force and velocity of the fluid and debris; pass A reads p4 and v4
     and writes pressure and the divergence terms of every particle; the list
     build writes every list entry (4 B) and count (4 B) and reads each
-    particle's position once (16 B).  Returns (table, name of the top kernel).
+    particle's position once (16 B).  Returns (table, name of the top kernel),
+    the name None when no phase was timed.
     """
     bpp = algorithmic_bytes(precision)
     kern = {}
@@ -185,6 +186,8 @@ def kernel_table(ph, precision, n, n_fs, entries, steps, rebuilds):
             kname = "k_" + ph_name
         kern[ph_name] = {"kernel": kname, "launch_ms": tot / cnt, "bytes": nbytes,
                          "run_ms": tot / cnt * n_launch}
+    if not kern:
+        return kern, None
     return kern, max(kern, key=lambda k: kern[k]["run_ms"])
 
 

@@ -13,6 +13,9 @@ using namespace dmph;
 
 namespace {
 thread_local std::string g_create_err;
+// set by failing calls that take no context and must not allocate
+// (dmph_cell_sort_noalloc); cleared by dmph_create
+thread_local const char *g_noctx_literal = nullptr;
 }
 
 
@@ -404,6 +407,7 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
                            dmph_ctx **out)
 {
     g_create_err.clear();
+    g_noctx_literal = nullptr;
     if (!out) return DMPH_EINVAL;
     *out = nullptr;
     if (!p || !type || !x3 || !v3) {
@@ -1206,9 +1210,13 @@ extern "C" int dmph_destroy(dmph_ctx *ctx)
     return DMPH_OK;
 }
 
+namespace dmph {
+void set_noctx_message(const char *literal) { g_noctx_literal = literal; }
+}  // namespace dmph
+
 extern "C" const char *dmph_last_error(dmph_ctx *ctx)
 {
-    if (!ctx) return g_create_err.c_str();
+    if (!ctx) return g_noctx_literal ? g_noctx_literal : g_create_err.c_str();
     return ctx->err.c_str();
 }
 

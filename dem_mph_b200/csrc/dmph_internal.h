@@ -8,6 +8,11 @@
 namespace dmph {
 
 int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, std::string &err);
+// same checks; on failure *msg points at a string literal (allocates nothing)
+int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, const char **msg);
+// dmph_api.cu: message that dmph_last_error(NULL) returns on the calling
+// thread until the next failing call without a context (a string literal)
+void set_noctx_message(const char *literal);
 
 // dmph_rebuild.cu
 void launch_keys(const DevParams &P, const double *pos, const int *type, unsigned long long *words, cudaStream_t st);

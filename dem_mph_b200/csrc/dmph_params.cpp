@@ -19,20 +19,20 @@ static double kernel_norm(double S, double h, int dim) { return dim == 2 ? 1.0 /
 static double w_a(double r, double B, double h) { return B * (r / h) * (1.0 - (r / h)) * (1.0 - (r / h)); }
 static double w_2(double r, double B, double h) { return B * ((1.0 - r / h) * (1.0 - r / h)); }
 
-int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, std::string &err)
+int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, const char **msg)
 {
     std::memset(&P, 0, sizeof(P));
     std::memset(&Wm, 0, sizeof(Wm));
-    if (p.dim != 2 && p.dim != 3) return err = "dim must be 2 or 3", DMPH_EINVAL;
-    if (n <= 0) return err = "particle count must be positive", DMPH_EINVAL;
+    if (p.dim != 2 && p.dim != 3) return *msg = "dim must be 2 or 3", DMPH_EINVAL;
+    if (n <= 0) return *msg = "particle count must be positive", DMPH_EINVAL;
     // the chunk scan handles up to 4096 blocks of 4096 slots
-    if (n > (1 << 24)) return err = "particle count above 2^24", DMPH_ERANGE;
-    if (!(p.particle_spacing > 0.0)) return err = "ParticleSpacing must be positive", DMPH_EINVAL;
-    if (!(p.dt > 0.0) || !(p.dem_dt > 0.0)) return err = "Dt and DEMDt must be positive", DMPH_EINVAL;
+    if (n > (1 << 24)) return *msg = "particle count above 2^24", DMPH_ERANGE;
+    if (!(p.particle_spacing > 0.0)) return *msg = "ParticleSpacing must be positive", DMPH_EINVAL;
+    if (!(p.dt > 0.0) || !(p.dem_dt > 0.0)) return *msg = "Dt and DEMDt must be positive", DMPH_EINVAL;
     if (!(p.radius_ratio_a > 0.0) || !(p.radius_ratio_p > 0.0) || !(p.radius_ratio_v > 0.0))
-        return err = "RadiusRatioA/P/V must be positive", DMPH_EINVAL;
+        return *msg = "RadiusRatioA/P/V must be positive", DMPH_EINVAL;
     for (int d = 0; d < 3; d++)
-        if (!(p.domain_max[d] > p.domain_min[d])) return err = "empty domain extent", DMPH_EINVAL;
+        if (!(p.domain_max[d] > p.domain_min[d])) return *msg = "empty domain extent", DMPH_EINVAL;
 
     const double dx = p.particle_spacing;
     P.dim = p.dim;
@@ -155,15 +155,15 @@ int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, std
     cc[1] = std::floor((p.domain_max[1] - p.domain_min[1]) / (maxR + margin));
     cc[2] = p.dim == 2 ? 1 : std::floor((p.domain_max[2] - p.domain_min[2]) / (maxR + margin));
     for (int d = 0; d < 3; d++)
-        if (!(cc[d] >= 1.0) || cc[d] > 1.0e7) return err = "domain narrower than one neighbour cell", DMPH_EINVAL;
+        if (!(cc[d] >= 1.0) || cc[d] > 1.0e7) return *msg = "domain narrower than one neighbour cell", DMPH_EINVAL;
     const double tot = cc[0] * cc[1] * cc[2];
-    if (3.0 * tot + 1.0 > 2.0e9) return err = "too many cells", DMPH_ERANGE;
+    if (3.0 * tot + 1.0 > 2.0e9) return *msg = "too many cells", DMPH_ERANGE;
     for (int d = 0; d < 3; d++) P.cc[d] = (int)cc[d];
     P.T = (int)tot;
     for (int d = 0; d < 3; d++) P.cw[d] = P.W[d] / P.cc[d];
     // the reference asserts a 3-cell stencil per axis (:1540-1543)
     for (int d = 0; d < (p.dim == 2 ? 2 : 3); d++)
-        if ((int)std::ceil((maxR + margin) / P.cw[d]) > 1) return err = "cell width below the neighbour radius", DMPH_EINVAL;
+        if ((int)std::ceil((maxR + margin) / P.cw[d]) > 1) return *msg = "cell width below the neighbour radius", DMPH_EINVAL;
     P.rc2 = (maxR + margin) * (maxR + margin);
     P.RA2 = P.RA * P.RA;
     P.RG2 = P.RG * P.RG;
@@ -203,6 +203,14 @@ int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, std
         }
     }
     return DMPH_OK;
+}
+
+int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, std::string &err)
+{
+    const char *msg = "";
+    const int rc = derive_params(p, n, P, Wm, &msg);
+    if (rc) err = msg;
+    return rc;
 }
 
 }  // namespace dmph

@@ -424,12 +424,17 @@ int dmph_get_phase_times(dmph_ctx *ctx, double *ms, int64_t *launches, int n);
  *   sorted_key  device, n ints out: the sorted keys (CellIndex)
  *   perm        device, n ints out: input row of each sorted slot
  *   stream      cudaStream_t (NULL = legacy default stream)
- * The first call on a device looks up the scratch array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  All calls share the one array and it keeps the
- * last call's contents, so calls whose work overlaps on the GPU (other
- * streams, other host threads) race; serialise them.  Returns DMPH_ERANGE
- * when n is too large.
+ * Set-up: the first call on a device, and the first call after that
+ * device's CUDA context was replaced (cudaDeviceReset, a primary context
+ * released and made again), looks up the scratch array's device address
+ * (cudaGetSymbolAddress) with that device current and caches it with the
+ * context's id; make that first call before any stream capture.  All calls
+ * share the one array and it keeps the last call's contents, so calls whose
+ * work overlaps on the GPU (other streams, other host threads) race;
+ * serialise them.  Returns DMPH_ERANGE when n is too large, and DMPH_ECUDA
+ * without running anything when a CUDA error of earlier work is pending on
+ * the calling thread (that error is left for its owner to read).  On any
+ * failure dmph_last_error(NULL), on the calling thread, gives the reason.
  */
 #define DMPH_NOALLOC_MAX_WORDS (1 << 19)
 int dmph_cell_sort_noalloc(const dmph_params *p, int n, const double *pos_planes, const int *type,

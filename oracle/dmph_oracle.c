@@ -1180,6 +1180,53 @@ dmph_oracle *dmph_oracle_create(const dmph_params *p, int n, const int *type, co
     return o;
 }
 
+/* The cell sort of calculateCellParticle (:1288-1338) alone, for checking
+ * the library's allocation-free sort: keys and permutation of n particles
+ * given as interleaved x3 and type, without the neighbour build. */
+int dmph_oracle_cell_sort(const dmph_params *p, int n, const int *type, const double *x3, int *key, int *perm)
+{
+    if (!p || n <= 0 || !type || !x3 || !key || !perm) return DMPH_EINVAL;
+    if (p->dim != 2 && p->dim != 3) return DMPH_EINVAL;
+    dmph_oracle *o = xcalloc(1, sizeof(*o));
+    o->p = *p;
+    o->dim = p->dim;
+    o->N = n;
+    o->dx = p->particle_spacing;
+    o->margin = (0.1 * o->dx);
+    while ((n >> o->P2log) != 0) ++o->P2log;
+    o->P2 = 1 << o->P2log;
+    const size_t N = (size_t)n;
+    o->pidx = xcalloc(N, sizeof(int));
+    o->prop = xcalloc(N, sizeof(int));
+    o->x = xcalloc(3 * N, sizeof(double));
+    o->v = xcalloc(3 * N, sizeof(double));
+    o->key = xcalloc((size_t)o->P2, sizeof(int));
+    o->payload = xcalloc((size_t)o->P2, sizeof(int));
+    for (int i = 0; i < n; i++) {
+        o->pidx[i] = i;
+        o->prop[i] = type[i];
+        for (int d = 0; d < 3; d++) o->x[3 * i + d] = x3[3 * i + d];
+    }
+    init_weight(o);
+    init_domain(o);
+    if (o->T <= 0) {
+        dmph_oracle_destroy(o);
+        return DMPH_EINVAL;
+    }
+    const size_t T = (size_t)o->T;
+    o->cfb = xcalloc(T, sizeof(int));
+    o->cfe = xcalloc(T, sizeof(int));
+    o->csb = xcalloc(T, sizeof(int));
+    o->cse = xcalloc(T, sizeof(int));
+    o->cwb = xcalloc(T, sizeof(int));
+    o->cwe = xcalloc(T, sizeof(int));
+    cell_sort(o);
+    memcpy(key, o->key, sizeof(int) * N);
+    memcpy(perm, o->pidx, sizeof(int) * N);
+    dmph_oracle_destroy(o);
+    return 0;
+}
+
 int dmph_oracle_step(dmph_oracle *o, int nsteps)
 {
     if (!o || nsteps < 0) return DMPH_EINVAL;

@@ -40,6 +40,8 @@ int dmph_oracle_pressure_force(dmph_oracle *o, const double *P, double *F);
 int dmph_oracle_set_bodies(dmph_oracle *o, int nbodies, const int *body_of_row, const double *body_density);
 /* X,V,L 3 per body, q 4 per body, M 1 per body (any may be NULL) */
 int dmph_oracle_get_bodies(dmph_oracle *o, double *X, double *V, double *q, double *L, double *M);
+/* the cell sort alone (keys and permutation, n of each), no neighbour build */
+int dmph_oracle_cell_sort(const dmph_params *p, int n, const int *type, const double *x3, int *key, int *perm);
 void dmph_oracle_destroy(dmph_oracle *o);
 
 #ifdef __cplusplus

@@ -39,6 +39,7 @@ def lib():
         L.dmph_oracle_set_bodies.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.dmph_oracle_get_bodies.argtypes = [C.c_void_p] + [C.c_void_p] * 5
         L.dmph_oracle_pressure_force.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dmph_oracle_cell_sort.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.mlp_oracle_param_count.restype = C.c_int
         L.mlp_oracle_forward.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.mlp_oracle_grad.restype = C.c_double
@@ -122,6 +123,20 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+
+def cell_sort(params, typ, x):
+    """(sorted keys, permutation) of the reference's cell sort of the given
+    particles alone (dmph_oracle_cell_sort)"""
+    t = np.ascontiguousarray(typ, dtype=np.int32)
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    key = np.empty(len(t), np.int32)
+    perm = np.empty(len(t), np.int32)
+    rc = lib().dmph_oracle_cell_sort(C.byref(params), len(t), t.ctypes.data, xx.ctypes.data, key.ctypes.data,
+                                     perm.ctypes.data)
+    if rc != 0:
+        raise ValueError("dmph_oracle_cell_sort rejected the input (%d)" % rc)
+    return key, perm
 
 
 def mlp_forward(params, X):

@@ -1,9 +1,10 @@
 """Generate the golden fixtures under tests/golden/ from the REFERENCE itself.
 
-Run in a container that has the reference tree (default /root/reference) and
-oracle/_ref built (make -C oracle ref):
+Run where the reference tree is present ($DMPH_REFERENCE_DIR, default a
+`reference` checkout beside this repository) and oracle/_ref is built
+(make -C oracle ref):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference tree>]
 
 It copies the two shipped SYSU case descriptions (dem.data and DEM.boid,
 results/SYSU/{2mm,0.8mm}) as small input fixtures, records the SHA-256 of the
@@ -80,7 +81,9 @@ def scene_inputs(name, workdir, ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    default_ref = os.environ.get("DMPH_REFERENCE_DIR") or os.path.join(
+        os.path.dirname(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))), "reference")
+    ap.add_argument("--ref", default=default_ref)
     args = ap.parse_args()
     out = {"generator_kat": {}, "scenes": {}}
     # input fixtures

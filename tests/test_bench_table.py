@@ -36,3 +36,10 @@ def test_fp64_has_no_fp32_list_build_row():
     kern, top = bench.kernel_table(ph, "fp64", N, NFS, ENTRIES, 300, 300)
     assert set(kern) == {"pass_a", "pass_b"} and top == "pass_b"
     assert kern["pass_b"]["kernel"] == "k_pass_b"
+
+
+def test_no_timed_phase_gives_no_top_kernel():
+    kern, top = bench.kernel_table({}, "fp32", N, NFS, ENTRIES, 20, 0)
+    assert kern == {} and top is None
+    kern, top = bench.kernel_table({"pass_a": (0.0, 0)}, "fp64", N, NFS, ENTRIES, 20, 0)
+    assert kern == {} and top is None

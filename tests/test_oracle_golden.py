@@ -61,3 +61,16 @@ def test_oracle_matches_reference(name):
         assert o.scalar("Rebuilds") == meta["Rebuilds"]
         assert o.scalar("Time") == meta["Time"]
         assert [o.scalar("CellCount%d" % d) for d in range(3)] == meta["CellCount"]
+
+
+@pytest.mark.parametrize("name", ["small3d", "sysu2mm"])
+def test_oracle_cell_sort_alone_matches_full_oracle(name):
+    """dmph_oracle_cell_sort (the checker of the library's allocation-free
+    sort) gives the CellIndex and ParticleIndex of the full oracle's first
+    sort, which the golden fixtures pin to the reference."""
+    from oracle import oracle as orc
+    p, typ, x, v = load_scene(name)
+    o = Oracle(p, typ, x, v)
+    key, perm = orc.cell_sort(p, typ, x)
+    assert np.array_equal(key, o.get("CellIndex")[:len(typ)])
+    assert np.array_equal(perm, o.get("ParticleIndex"))
