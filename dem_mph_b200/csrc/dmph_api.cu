@@ -246,8 +246,8 @@ void dmph::enqueue_dem(dmph_ctx *ctx, cudaStream_t st)
                 launch_body_step(P, S, ctx->Bd, false, st);
                 continue;
             }
-            launch_dem_force(P, S, dB, CR_SOLID, 1, st);
-            if (P.wall_dem_coeffs) launch_dem_force(P, S, dB, CR_WALL, 0, st);
+            launch_dem_force(P, S, dB, CR_SOLID, 1, st, false, ctx->use_list);
+            if (P.wall_dem_coeffs) launch_dem_force(P, S, dB, CR_WALL, 0, st, false, ctx->use_list);
             launch_dem_integrate(P, S, dB, st);
         }
     }
@@ -265,8 +265,10 @@ long long dmph::dem_launches(const dmph_ctx *ctx)
 {
     // clump contacts (FP32 list mode: list walk and gated cell walk) and the
     // body update, or the reference's DEM force(s) and integration
-    const long long dem =
-        ctx->Bd.B > 0 ? (ctx->fp32 && ctx->use_list ? 3 : 2) : 2 + (ctx->P.wall_dem_coeffs ? 1 : 0);
+    // (FP64 list mode: each DEM force launch is a list walk and a gated cell walk)
+    const long long nforce = (!ctx->fp32 && ctx->use_list) ? 2 : 1;
+    const long long dem = ctx->Bd.B > 0 ? (ctx->fp32 && ctx->use_list ? 3 : 2)
+                                        : nforce * (1 + (ctx->P.wall_dem_coeffs ? 1 : 0)) + 1;
     return ctx->demSteps * dem + (ctx->fp32 ? 2 : 0);
 }
 
@@ -605,31 +607,56 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     return DMPH_OK;
 }
 
-extern "C" int dmph_step(dmph_ctx *ctx, int nsteps)
+int dmph::check_finite(dmph_ctx *ctx)
 {
-    if (!ctx || nsteps < 0) return DMPH_EINVAL;
+    if (!ctx->nonfinite) {
+        CK(cudaMemcpyAsync(ctx->h_small, ctx->dB + B_NONFINITE, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        ctx->nonfinite = ctx->h_small[0] != 0;
+    }
+    if (!ctx->nonfinite) return DMPH_OK;
+    ctx->err = "non-finite position or velocity met by a step (no neighbour rebuild runs until dmph_set_state "
+               "replaces the state)";
+    return DMPH_ENAN;
+}
+
+// the steps of dmph_step / dmph_step_timed, with the non-finite check every
+// kFiniteCheckEvery steps and at the end
+static int run_steps(dmph_ctx *ctx, int nsteps)
+{
+    if (ctx->nonfinite) return check_finite(ctx);
     for (int s = 0; s < nsteps; s++) {
         const int rc = step_once(ctx);
         if (rc) return rc;
+        if ((s + 1) % kFiniteCheckEvery == 0 && s + 1 < nsteps) {
+            const int rf = check_finite(ctx);
+            if (rf) return rf;
+        }
     }
-    CK(cudaStreamSynchronize(ctx->st));
     return DMPH_OK;
+}
+
+extern "C" int dmph_step(dmph_ctx *ctx, int nsteps)
+{
+    if (!ctx || nsteps < 0) return DMPH_EINVAL;
+    const int rc = run_steps(ctx, nsteps);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->st));
+    return check_finite(ctx);
 }
 
 extern "C" int dmph_step_timed(dmph_ctx *ctx, int nsteps, float *device_ms)
 {
     if (!ctx || nsteps < 0) return DMPH_EINVAL;
     CK(cudaEventRecord(ctx->ev0, ctx->st));
-    for (int s = 0; s < nsteps; s++) {
-        const int rc = step_once(ctx);
-        if (rc) return rc;
-    }
+    const int rc = run_steps(ctx, nsteps);
+    if (rc) return rc;
     CK(cudaEventRecord(ctx->ev1, ctx->st));
     CK(cudaEventSynchronize(ctx->ev1));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     if (device_ms) *device_ms = ms;
-    return DMPH_OK;
+    return check_finite(ctx);
 }
 
 // device planes -> caller's x,y,z buffer through a staging buffer (pos2 or
@@ -686,6 +713,9 @@ extern "C" int dmph_set_state(dmph_ctx *ctx, const double *x3, const double *v3)
         if (!x3) launch_export32(ctx->P, ctx->S, ctx->S.pos, nullptr, ctx->st);
         launch_import32(ctx->P, ctx->S, ctx->S.pos, v3 ? ctx->S.vel : nullptr, ctx->st);
     }
+    // a new state: the next drift checks it afresh
+    CK(cudaMemsetAsync(ctx->dB + B_NONFINITE, 0, sizeof(int), ctx->st));
+    ctx->nonfinite = false;
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->st));
     return DMPH_OK;
@@ -1541,6 +1571,19 @@ static int ens_step_once(dmph_ensemble *e)
     return DMPH_OK;
 }
 
+// DMPH_ENAN when a scene's drift met a non-finite position or velocity
+static int ens_check_finite(dmph_ensemble *e)
+{
+    for (size_t k = 0; k < e->scenes.size(); ++k) {
+        dmph_ctx *c = e->scenes[k];
+        if (check_finite(c) == DMPH_ENAN) {
+            e->err = "scene " + std::to_string(k) + ": " + c->err;
+            return DMPH_ENAN;
+        }
+    }
+    return DMPH_OK;
+}
+
 extern "C" int dmph_ensemble_step(dmph_ensemble *e, int nsteps)
 {
     if (!e || nsteps < 0) return DMPH_EINVAL;
@@ -1549,7 +1592,7 @@ extern "C" int dmph_ensemble_step(dmph_ensemble *e, int nsteps)
         if (rc) return rc;
     }
     EK(cudaStreamSynchronize(e->st));
-    return DMPH_OK;
+    return ens_check_finite(e);
 }
 
 extern "C" int dmph_ensemble_step_timed(dmph_ensemble *e, int nsteps, float *device_ms)
@@ -1565,7 +1608,7 @@ extern "C" int dmph_ensemble_step_timed(dmph_ensemble *e, int nsteps, float *dev
     float ms = 0.f;
     EK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
     if (device_ms) *device_ms = ms;
-    return DMPH_OK;
+    return ens_check_finite(e);
 }
 
 extern "C" int dmph_ensemble_autotune(dmph_ensemble *e, int *variant_a, int *variant_b, float *ms_a, float *ms_b)

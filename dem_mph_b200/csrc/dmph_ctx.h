@@ -67,6 +67,7 @@ struct dmph_ctx {
     long long launches = 0;  // kernels launched by dmph_step
     bool all_counts = false;
     bool prof = false;
+    bool nonfinite = false;  // a step met a non-finite position or velocity (until dmph_set_state)
     cudaEvent_t pe0 = nullptr, pe1 = nullptr, pl0 = nullptr, pl1 = nullptr;
     double phase_ms[DMPH_PHASE_COUNT] = {0};
     long long phase_n[DMPH_PHASE_COUNT] = {0};
@@ -99,6 +100,10 @@ long long tail_launches(const dmph_ctx *ctx, bool graph = false);
 void advance_host_clock(dmph_ctx *ctx);
 int step_once(dmph_ctx *ctx);
 int read_bounds(dmph_ctx *ctx, int *b);
+// DMPH_ENAN once a drift has met a non-finite position or velocity
+// (B_NONFINITE; synchronises the stream), else DMPH_OK
+int check_finite(dmph_ctx *ctx);
+constexpr int kFiniteCheckEvery = 256;  // steps between two checks inside one dmph_step call
 void drop_graph(dmph_ctx *ctx);
 
 // surrogate (dmph_surrogate.cu)

@@ -90,6 +90,7 @@ enum DevBound {
     B_REBUILDS = 8, // rebuilds since creation
     B_LIST_OVF = 9, // a Verlet list of the last rebuild overflowed (FP32 list mode): stencil passes run
     B_LIST_SPLIT = 10, // the FP32 lists hold no wall-wall pairs (built with the walls at rest)
+    B_NONFINITE = 11,  // a drift met a non-finite position or velocity (sticky; no rebuild runs while set)
     B_COUNT = 16
 };
 

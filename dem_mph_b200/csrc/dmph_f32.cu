@@ -16,6 +16,8 @@
 // N0p); pass B uses the approximate reciprocal square root.  Sums that cancel
 // are carried in FP64.  Accuracy is checked against the FP64 oracle: forces
 // within 1e-5 of each particle's force scale at equal pressures.
+#include <math_constants.h>
+
 #include "dmph_state.cuh"
 #include "dmph_traverse.cuh"
 
@@ -111,6 +113,9 @@ __global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm,
         const float4 r = S.xref4[i];
         const float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
         m2 = fmaxf(m2, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        // a non-finite position or velocity makes the maximum +inf, which the
+        // rebuild decision reports instead of rebuilding
+        if (!isfinite(p.x + p.y + p.z + v.x + v.y + v.z)) m2 = CUDART_INF_F;
     }
     // reduce as double bits so the host compares like the FP64 path
     unsigned long long b = __double_as_longlong((double)m2);

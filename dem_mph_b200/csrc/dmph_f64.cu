@@ -9,6 +9,8 @@
 // rebuild trigger fused), then after an optional rebuild k_pass_a (densities,
 // divergence, pressure), k_pass_b (all fluid forces, drag, buoyancy, gravity,
 // fluid velocity update), and per DEM substep k_dem_force + k_dem_integrate.
+#include <math_constants.h>
+
 #include "dmph_state.cuh"
 #include "dmph_traverse.cuh"
 
@@ -95,6 +97,9 @@ __global__ void k_drift(DevParams P, DevState S, WallMotion Wm, unsigned long lo
         }
         const double s = d3[0] * d3[0] + d3[1] * d3[1] + d3[2] * d3[2];
         m2 = s > m2 ? s : m2;
+        // a non-finite position or velocity makes the maximum +inf, which the
+        // rebuild decision reports instead of rebuilding
+        if (!isfinite(x[0] + x[1] + x[2] + v[0] + v[1] + v[2])) m2 = CUDART_INF;
     }
     // warp then block max; one atomic per block
     unsigned long long b = __double_as_longlong(m2);
@@ -397,9 +402,48 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_pass_b(DevParams P, 
 // calculateTorque only feed arrays nothing reads and are not run.
 // MIXED: FP32 split mode, where solids and walls keep FP64 master positions in
 // S.pos/S.vel but fluid particles live in the FP32 arrays p4/v4.
-template <bool MIXED>
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_dem_force(DevParams P, DevState S, const int *dB, int range, int forces)
+// LIST (FP64 build): each lane walks its particle's Verlet list, which is the
+// reference's own NeighborInd (the neighbours within MaxRadius+MARGIN at the
+// last rebuild, fluid then solid then wall cells in its visiting order), as
+// the reference's DEM functions do; the stencil walk visits the same
+// candidates in the same order, so both give the same bits.  gate: this
+// stencil launch stands in only after a list overflow.
+
+// the contact of one pair within dx (calculateNormalDirectionForce
+// :2560-2612 and calculateTangentialDirectionForce :2614-2696, with the
+// reference's stray Dt on the normal damping and its component-wise v_n)
+__device__ __forceinline__ void dem_pair(const DevParams &P, double kn, double cn, double kt, double ct, double mu_f,
+                                         const double q[3], double r2, double vxj, double vyj, double vzj,
+                                         double vxi, double vyi, double vzi, double fN[3], double fT[3])
 {
+    const double r = sqrt(r2);
+    const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
+    const double u[3] = {vxj - vxi, vyj - vyi, vzj - vzi};
+    double vn[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < 3; d++) vn[d] += u[d] * e[d];
+    for (int d = 0; d < 3; d++) fN[d] += -kn * (P.dx - r) * e[d] - (cn * vn[d] * e[d] * P.dt);
+    double vn2[3], vt[3], dtv[3] = {0.0, 0.0, 0.0}, sN[3], sT[3];
+    for (int d = 0; d < 3; d++) vn2[d] = u[d] * e[d];
+    for (int d = 0; d < 3; d++) vt[d] = u[d] - vn2[d] * e[d];
+    for (int d = 0; d < 3; d++) dtv[d] += vt[d] * P.ddt;
+    for (int d = 0; d < 3; d++) sN[d] = -kn * (P.dx - r) * e[d] - (cn * vn2[d] * e[d] * P.dt);
+    const double aFn = mu_f * sqrt(sN[0] * sN[0] + sN[1] * sN[1] + sN[2] * sN[2]);
+    for (int d = 0; d < 3; d++) sT[d] = -kt * dtv[d] - (ct * vt[d]);
+    const double aFt = sqrt(sT[0] * sT[0] + sT[1] * sT[1] + sT[2] * sT[2]);
+    if (aFn > aFt) {
+        for (int d = 0; d < 3; d++) fT[d] += -kt * dtv[d] - (ct * vt[d]);
+    } else {
+        const double avt = sqrt(vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]);
+        if (avt != 0)
+            for (int d = 0; d < 3; d++) fT[d] += aFn * vt[d] / avt;
+    }
+}
+
+template <bool MIXED, bool LIST>
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_dem_force(DevParams P, DevState S, const int *dB, int range,
+                                                                      int forces, int gate)
+{
+    if (LIST ? dB[B_LIST_OVF] != 0 : (gate && dB[B_LIST_OVF] == 0)) return;
     __shared__ TileA tiles[kWarpsPerBlock];
     TileA &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -414,6 +458,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_dem_force(DevParams 
         const int ti = S.type[ii];
         const double xi = S.pos[ii], yi = S.pos[N + ii], zi = S.pos[2 * N + ii];
         const double vxi = S.vel[ii], vyi = S.vel[N + ii], vzi = S.vel[2 * N + ii];
+        const int nlist = (LIST && active) ? S.nbn[i] : 0;
         auto stage = [&](int j, int slot) {
             const int t = S.type[j];
             if (MIXED && is_fluid(t)) {
@@ -439,17 +484,32 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_dem_force(DevParams 
         // 1) last neighbour within dx
         int tlast = -1;
         double r2last = 0.0;
-        traverse_stencil(P, S.cell_start, key_cell, lane, active, 7u, stage, [&](int j, int s) {
-            if (j == i) return;
-            const double q0 = rel1(tl.x[s], xi, P.W[0], P.hW[0]);
-            const double q1 = rel1(tl.y[s], yi, P.W[1], P.hW[1]);
-            const double q2 = rel1(tl.z[s], zi, P.W[2], P.hW[2]);
-            const double r2 = (q0 * q0 + q1 * q1 + q2 * q2);
-            if (r2 <= P.dx2) {
-                tlast = tl.t[s];
-                r2last = r2;
+        if (LIST) {
+            for (int k = 0; k < nlist; ++k) {
+                const int j = (int)(__ldg(S.nbl + list_index(k, i, N)) & kEntrySlot);
+                if (j == i) continue;
+                const double q0 = rel1(S.pos[j], xi, P.W[0], P.hW[0]);
+                const double q1 = rel1(S.pos[N + j], yi, P.W[1], P.hW[1]);
+                const double q2 = rel1(S.pos[2 * N + j], zi, P.W[2], P.hW[2]);
+                const double r2 = (q0 * q0 + q1 * q1 + q2 * q2);
+                if (r2 <= P.dx2) {
+                    tlast = S.type[j];
+                    r2last = r2;
+                }
             }
-        });
+        } else {
+            traverse_stencil(P, S.cell_start, key_cell, lane, active, 7u, stage, [&](int j, int s) {
+                if (j == i) return;
+                const double q0 = rel1(tl.x[s], xi, P.W[0], P.hW[0]);
+                const double q1 = rel1(tl.y[s], yi, P.W[1], P.hW[1]);
+                const double q2 = rel1(tl.z[s], zi, P.W[2], P.hW[2]);
+                const double r2 = (q0 * q0 + q1 * q1 + q2 * q2);
+                if (r2 <= P.dx2) {
+                    tlast = tl.t[s];
+                    r2last = r2;
+                }
+            });
+        }
         double kn, cn, kt, ct;
         if (active) {
             if (tlast >= 0) {
@@ -476,35 +536,27 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_dem_force(DevParams 
         // 2) normal and tangential forces from non-fluid neighbours within dx
         double fN[3] = {0.0, 0.0, 0.0}, fT[3] = {0.0, 0.0, 0.0};
         const double mu_f = P.friction[ti];
-        traverse_stencil(P, S.cell_start, key_cell, lane, active, 6u, stage, [&](int j, int s) {
-            if (j == i) return;
-            const double q[3] = {rel1(tl.x[s], xi, P.W[0], P.hW[0]), rel1(tl.y[s], yi, P.W[1], P.hW[1]),
-                                 rel1(tl.z[s], zi, P.W[2], P.hW[2])};
-            const double r2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
-            if (r2 <= P.dx2) {
-                const double r = sqrt(r2);
-                const double e[3] = {q[0] / r, q[1] / r, q[2] / r};
-                const double u[3] = {tl.vx[s] - vxi, tl.vy[s] - vyi, tl.vz[s] - vzi};
-                double vn[3] = {0.0, 0.0, 0.0};
-                for (int d = 0; d < 3; d++) vn[d] += u[d] * e[d];
-                for (int d = 0; d < 3; d++) fN[d] += -kn * (P.dx - r) * e[d] - (cn * vn[d] * e[d] * P.dt);
-                double vn2[3], vt[3], dtv[3] = {0.0, 0.0, 0.0}, sN[3], sT[3];
-                for (int d = 0; d < 3; d++) vn2[d] = u[d] * e[d];
-                for (int d = 0; d < 3; d++) vt[d] = u[d] - vn2[d] * e[d];
-                for (int d = 0; d < 3; d++) dtv[d] += vt[d] * P.ddt;
-                for (int d = 0; d < 3; d++) sN[d] = -kn * (P.dx - r) * e[d] - (cn * vn2[d] * e[d] * P.dt);
-                const double aFn = mu_f * sqrt(sN[0] * sN[0] + sN[1] * sN[1] + sN[2] * sN[2]);
-                for (int d = 0; d < 3; d++) sT[d] = -kt * dtv[d] - (ct * vt[d]);
-                const double aFt = sqrt(sT[0] * sT[0] + sT[1] * sT[1] + sT[2] * sT[2]);
-                if (aFn > aFt) {
-                    for (int d = 0; d < 3; d++) fT[d] += -kt * dtv[d] - (ct * vt[d]);
-                } else {
-                    const double avt = sqrt(vt[0] * vt[0] + vt[1] * vt[1] + vt[2] * vt[2]);
-                    if (avt != 0)
-                        for (int d = 0; d < 3; d++) fT[d] += aFn * vt[d] / avt;
-                }
+        if (LIST) {
+            for (int k = 0; k < nlist; ++k) {
+                const int j = (int)(__ldg(S.nbl + list_index(k, i, N)) & kEntrySlot);
+                if (j == i || is_fluid(S.type[j])) continue;
+                const double q[3] = {rel1(S.pos[j], xi, P.W[0], P.hW[0]), rel1(S.pos[N + j], yi, P.W[1], P.hW[1]),
+                                     rel1(S.pos[2 * N + j], zi, P.W[2], P.hW[2])};
+                const double r2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+                if (r2 <= P.dx2)
+                    dem_pair(P, kn, cn, kt, ct, mu_f, q, r2, S.vel[j], S.vel[N + j], S.vel[2 * N + j], vxi, vyi, vzi,
+                             fN, fT);
             }
-        });
+        } else {
+            traverse_stencil(P, S.cell_start, key_cell, lane, active, 6u, stage, [&](int j, int s) {
+                if (j == i) return;
+                const double q[3] = {rel1(tl.x[s], xi, P.W[0], P.hW[0]), rel1(tl.y[s], yi, P.W[1], P.hW[1]),
+                                     rel1(tl.z[s], zi, P.W[2], P.hW[2])};
+                const double r2 = (q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+                if (r2 <= P.dx2)
+                    dem_pair(P, kn, cn, kt, ct, mu_f, q, r2, tl.vx[s], tl.vy[s], tl.vz[s], vxi, vyi, vzi, fN, fT);
+            });
+        }
         if (!active) continue;
         for (int d = 0; d < 3; d++) {
             double F = S.frc[d * N + i];
@@ -863,15 +915,19 @@ void launch_pass_b(const DevParams &P, const DevState &S, const int *dB, cudaStr
     }
 }
 void launch_dem_force(const DevParams &P, const DevState &S, const int *dB, int range, int forces, cudaStream_t st,
-                      bool mixed)
+                      bool mixed, bool list)
 {
     if (mixed) {
-        static const int g = persistent_grid((const void *)k_dem_force<true>, kBlock);
-        k_dem_force<true><<<g, kBlock, 0, st>>>(P, S, dB, range, forces);
-    } else {
-        static const int g = persistent_grid((const void *)k_dem_force<false>, kBlock);
-        k_dem_force<false><<<g, kBlock, 0, st>>>(P, S, dB, range, forces);
+        static const int g = persistent_grid((const void *)k_dem_force<true, false>, kBlock);
+        k_dem_force<true, false><<<g, kBlock, 0, st>>>(P, S, dB, range, forces, 0);
+        return;
     }
+    if (list) {
+        static const int gl = persistent_grid((const void *)k_dem_force<false, true>, kBlock);
+        k_dem_force<false, true><<<gl, kBlock, 0, st>>>(P, S, dB, range, forces, 0);
+    }
+    static const int g = persistent_grid((const void *)k_dem_force<false, false>, kBlock);
+    k_dem_force<false, false><<<g, kBlock, 0, st>>>(P, S, dB, range, forces, list ? 1 : 0);
 }
 void launch_fluid_accel(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
 {

@@ -49,8 +49,10 @@ void launch_build_list64(const DevParams &P, const DevState &S, int *dB, cudaStr
 void launch_virial(const DevParams &P, const DevState &S, const int *dB, double *vir, cudaStream_t st);
 void launch_pass_b(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st, int list = 0, int gate = 0);
 void launch_fluid_accel(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
+// list (FP64 build): walk the Verlet lists, with the stencil walk gated on a
+// list overflow (2 kernels)
 void launch_dem_force(const DevParams &P, const DevState &S, const int *dB, int range, int forces, cudaStream_t st,
-                      bool mixed = false);
+                      bool mixed = false, bool list = false);
 void launch_dem_integrate(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 void launch_counts(const DevParams &P, const DevState &S, const int *dB, int range, cudaStream_t st);
 // FP32 list mode, debris counts from the lists (with the stencil walk gated

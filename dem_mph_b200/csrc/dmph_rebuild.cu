@@ -489,21 +489,34 @@ __global__ void k_copy_chunks(const Chunk *__restrict__ tmp, Chunk *__restrict__
 
 // rebuild decision of neighborCalculation (:1276-1285) from the reduced max
 // displacement: max |dx|^2 > (0.5 MARGIN)^2
-__global__ void k_decide(const unsigned long long *maxshift, double threshold, int *dB)
+// rebuild decision of :1264-1286 (max shift since the last rebuild above half
+// the margin).  A maximum of +inf (the drift met a non-finite position or
+// velocity) sets the sticky B_NONFINITE flag, and no rebuild runs while it is
+// set: positions become cell indices only in the rebuild, so every index the
+// other kernels use stays the last finite rebuild's.
+__device__ __forceinline__ int decide(const unsigned long long *maxshift, double threshold, int *dB)
 {
-    const double m2 = __longlong_as_double((long long)*maxshift);
+    const unsigned long long bits = *maxshift;
+    if (bits >= 0x7FF0000000000000ull || dB[B_NONFINITE]) {
+        dB[B_NONFINITE] = 1;
+        dB[B_NEED] = 0;
+        return 0;
+    }
+    const double m2 = __longlong_as_double((long long)bits);
     const int need = m2 > threshold ? 1 : 0;
     dB[B_NEED] = need;
     dB[B_REBUILDS] += need;
+    return need;
+}
+__global__ void k_decide(const unsigned long long *maxshift, double threshold, int *dB)
+{
+    decide(maxshift, threshold, dB);
 }
 // same, inside a CUDA graph: also sets the condition of the graph's rebuild node
 __global__ void k_decide_graph(const unsigned long long *maxshift, double threshold, int *dB,
                                cudaGraphConditionalHandle cond)
 {
-    const double m2 = __longlong_as_double((long long)*maxshift);
-    const int need = m2 > threshold ? 1 : 0;
-    dB[B_NEED] = need;
-    dB[B_REBUILDS] += need;
+    const int need = decide(maxshift, threshold, dB);
     cudaGraphSetConditional(cond, need ? 1u : 0u);
 }
 

@@ -26,6 +26,7 @@
 // L2, fast particles weighted up), and above `tolerance` the driver falls back
 // to the plain solver for `fallback_blocks` blocks, during which it keeps
 // collecting samples and training.
+#include <math_constants.h>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -437,6 +438,7 @@ __global__ void k_maxshift32(DevParams P, DevState S, unsigned long long *maxshi
         const float4 p = S.p4[i], r = S.xref4[i];
         const float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
         m2 = fmaxf(m2, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        if (!isfinite(p.x + p.y + p.z)) m2 = CUDART_INF_F;  // reported by the decision, no rebuild
     }
     unsigned long long b = __double_as_longlong((double)m2);
     for (int o = 16; o > 0; o >>= 1) {

@@ -153,7 +153,13 @@ const char *dmph_io_last_message(void);
 int dmph_create(const dmph_params *p, int n, const int *type, const double *x3, const double *v3, dmph_ctx **out);
 
 /* Advance nsteps explicit steps: one iteration of the reference main loop
- * (source/DEM-MPH.cpp:450-579) each, without file output. */
+ * (source/DEM-MPH.cpp:450-579) each, without file output.
+ * Failure detection (no counterpart in the reference, which runs on with NaN):
+ * every step's drift also checks every position and velocity; a non-finite
+ * one sets a device flag, from then on no neighbour rebuild runs (so no
+ * non-finite position ever becomes a cell index), and the call returns
+ * DMPH_ENAN (checked every 256 steps and at the end of the call).  Later
+ * calls return DMPH_ENAN at once until dmph_set_state replaces the state. */
 int dmph_step(dmph_ctx *ctx, int nsteps);
 
 /* Same as dmph_step, and report the device time of the nsteps as measured by
@@ -166,7 +172,8 @@ int dmph_step_timed(dmph_ctx *ctx, int nsteps, float *device_ms);
 int dmph_get_state(dmph_ctx *ctx, int *type, double *x3, double *v3, int *orig_id);
 
 /* Overwrite positions and velocities (current order, 3n each).  Used by
- * host-driven coupling loops; takes effect at the next step. */
+ * host-driven coupling loops; takes effect at the next step, and clears the
+ * non-finite flag of dmph_step (the next step checks the new state). */
 int dmph_set_state(dmph_ctx *ctx, const double *x3, const double *v3);
 
 /* Per-particle fields, current order; `out` holds n (scalars) or 3n (vectors)

@@ -28,9 +28,20 @@ def test_reference_arm_prints_one_contract_line():
     assert d["impl"] == "reference"
     assert d["metric"] == "particle-steps/s" and d["unit"] == "particle-steps/s"
     assert d["value"] > 0 and d["higher_is_better"] is True
-    assert d["n_gpus"] == 1 and d["steps"] == 1 and d["warmup"] >= 1
+    assert d["n_gpus"] == 1 and d["steps"] == 1 and d["warmup"] == 3  # the bench's warm-up floor
     assert d["ms_per_step"] > 0
     assert d["config"]["workload"] == "config1_dambreak_3d_dx10mm"
+    # the same config object the GPU arm prints for the same arguments
+    import argparse
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    from dem_mph_b200 import scenes
+    args = argparse.Namespace(workload="config1", precision="fp32", no_bodies=False,
+                              settle=bench.SETTLE_DEFAULT["config1"])
+    assert d["config"] == json.loads(json.dumps(bench.workload_config(scenes.config1(seed=1234), args, 1)))
+    assert "reference" in d["config"]["arms"] and "ours" in d["config"]["arms"]
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"]
     assert "sample" in cb

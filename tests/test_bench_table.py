@@ -43,3 +43,18 @@ def test_no_timed_phase_gives_no_top_kernel():
     assert kern == {} and top is None
     kern, top = bench.kernel_table({"pass_a": (0.0, 0)}, "fp64", N, NFS, ENTRIES, 20, 0)
     assert kern == {} and top is None
+
+
+def test_reference_rate_adds_rebuilds_at_the_window_cadence():
+    # 4 timed steps of 10 s of which one rebuild of 30 s: 7.5 s per step
+    # without rebuilds; half the steps of the GPU window rebuild
+    res = {"seconds": 40.0, "steps": 4, "rebuilds": 1, "rebuild_seconds": 10.0, "init_rebuild_seconds": 99.0}
+    v, secs, R = bench.reference_rate(res, 1000, 4, 0.5)
+    assert R == 2 and abs(secs - (4 * 7.5 + 2 * 10.0)) < 1e-12 and abs(v - 4000 / secs) < 1e-9
+    # no rebuild in the timed steps: the initialisation's rebuild time is used
+    res = {"seconds": 20.0, "steps": 2, "rebuilds": 0, "rebuild_seconds": 0.0, "init_rebuild_seconds": 30.0}
+    v, secs, R = bench.reference_rate(res, 1000, 2, 1.0)
+    assert R == 2 and abs(secs - 80.0) < 1e-12
+    # no cadence known: the timed steps alone, their own rebuilds removed
+    v, secs, R = bench.reference_rate(res, 1000, 2, None)
+    assert R == 0 and abs(secs - 20.0) < 1e-12

@@ -60,6 +60,15 @@ def test_fp32_one_step_forces(name):
     ids_g, ids_o = g.state()[3], o.get("ParticleIndex")
     assert np.array_equal(neighbour_pairs(ptr, ind, ids_g),
                           neighbour_pairs(o.get("NeighborPtr"), o.get("NeighborInd"), ids_o))
+    check_one_step(g, o, name)
+    g.close()
+
+
+def check_one_step(g, o, name):
+    """One step of the FP32 GPU context g and the FP64 oracle o from the same
+    state: cells by particle id, forces within FORCE_RTOL of their scale at
+    equal pressures, pressures bounded by the strain and divergence
+    differences, VolStrainP within FORCE_RTOL of N0p."""
     g.step(1)
     o.step(1)
     ig = np.argsort(g.state()[3])
@@ -102,7 +111,6 @@ def test_fp32_one_step_forces(name):
     vs_scale = np.abs(O("VolStrainP")).max() + 1e-300
     nw = prop < 4
     assert rel_err(G("VolStrainP")[nw], O("VolStrainP")[nw], scale=vs_scale + o.scalar("N0p")) <= FORCE_RTOL
-    g.close()
 
 
 @pytest.mark.parametrize("name", ["small3d", "sysu2mm"])
