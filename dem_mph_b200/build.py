@@ -46,7 +46,7 @@ CU_SOURCES = [
     ("dmph_mlp.cu", []),
     ("dmph_surrogate.cu", []),
 ]
-CPP_SOURCES = ["dmph_params.cpp", "dmph_io.cpp"]
+CPP_SOURCES = ["dmph_params.cpp", "dmph_io.cpp", "dmph_bodies_io.cpp"]
 HEADERS = ["dmph_device.cuh", "dmph_state.cuh", "dmph_traverse.cuh", "dmph_internal.h", "dmph_ctx.h", "dmph_mlp.h"]
 
 

@@ -1,6 +1,13 @@
 // dem_mph — drop-in replacement of the reference solver executable.
 //
-//   dem_mph [--dim 2|3] [--fp32] [--gpu N] data grid prof_pattern vtk_pattern log
+//   dem_mph [--dim 2|3] [--fp32] [--gpu N] [--bodies FILE | --rigid]
+//           data grid prof_pattern vtk_pattern log
+//
+// --bodies FILE moves the debris as rigid bodies with the membership and
+// densities of a body sidecar file (dmph_read_bodies_file); --rigid does the
+// same with the bodies taken as the solid particles connected by contact at
+// 1.01 dx, each with its type's density (dmph_bodies_from_contacts).  Without
+// either, debris particles move individually, as in the reference.
 //
 // Same positional arguments, defaults and output cadence as the reference's
 // main (source/DEM-MPH.cpp:350-617): it reads dem.data and the .grid file,
@@ -49,7 +56,8 @@ int main(int argc, char **argv)
     // defaults of the reference (:54-58)
     std::string logf = "sample.log", dataf = "sample.data", gridf = "sample.grid", proff = "sample%03d.prof",
                 vtkf = "sample%03d.vtk";
-    int dim = 2, fp32 = 0, gpu = 0;
+    int dim = 2, fp32 = 0, gpu = 0, rigid = 0;
+    std::string bodiesf;
     std::vector<std::string> pos;
     for (int a = 1; a < argc; a++) {
         if (!std::strcmp(argv[a], "--dim") && a + 1 < argc)
@@ -58,6 +66,10 @@ int main(int argc, char **argv)
             fp32 = 1;
         else if (!std::strcmp(argv[a], "--gpu") && a + 1 < argc)
             gpu = std::atoi(argv[++a]);
+        else if (!std::strcmp(argv[a], "--bodies") && a + 1 < argc)
+            bodiesf = argv[++a];
+        else if (!std::strcmp(argv[a], "--rigid"))
+            rigid = 1;
         else
             pos.push_back(argv[a]);
     }
@@ -94,9 +106,33 @@ int main(int argc, char **argv)
         time_t t = time(NULL);
         log_printf("start initialization at %s\n", ctime(&t));
     }
+    // rigid debris bodies: membership and densities by grid row
+    std::vector<int> body_of_row;
+    std::vector<double> body_density;
+    int nbodies = 0;
+    if (!bodiesf.empty()) {
+        int nrows = 0;
+        rc = dmph_read_bodies_file(bodiesf.c_str(), &nbodies, &nrows, nullptr, nullptr);
+        if (!rc && nrows != n) return log_printf("%s has %d rows, the grid %d\n", bodiesf.c_str(), nrows, n), 1;
+        body_of_row.resize(n);
+        body_density.resize(nbodies > 0 ? nbodies : 1);
+        if (!rc) rc = dmph_read_bodies_file(bodiesf.c_str(), &nbodies, &nrows, body_of_row.data(), body_density.data());
+        if (rc) return log_printf("cannot read %s: %s\n", bodiesf.c_str(), dmph_bodies_last_message()), 1;
+    } else if (rigid) {
+        body_of_row.resize(n);
+        body_density.resize(n);
+        rc = dmph_bodies_from_contacts(&p, n, type.data(), x.data(), body_of_row.data(), &nbodies,
+                                       body_density.data(), n);
+        if (rc) return log_printf("rigid bodies: %s\n", dmph_bodies_last_message()), 1;
+    }
     dmph_ctx *ctx = nullptr;
     rc = dmph_create(&p, n, type.data(), x.data(), v.data(), &ctx);
     if (rc) return fail("dmph_create", rc, nullptr);
+    if (nbodies > 0) {
+        rc = dmph_set_bodies(ctx, nbodies, body_of_row.data(), body_density.data());
+        if (rc) return fail("dmph_set_bodies", rc, ctx);
+        log_printf("rigid bodies: %d\n", nbodies);
+    }
     dmph_info info;
     dmph_get_info(ctx, &info);
     log_printf("N0a = %e\nN0p = %e\n", info.n0a, info.n0p);

@@ -69,12 +69,55 @@ def lib():
         L.dmph_mlp_forward.argtypes = [vp, vp, C.c_int, vp]
         L.dmph_mlp_gradient.argtypes = [vp, vp, vp, C.c_int, vp, C.POINTER(C.c_float)]
         L.dmph_surrogate_features.argtypes = [vp, vp, C.POINTER(C.c_int)]
+        L.dmph_write_bodies_file.argtypes = [C.c_char_p, C.c_int, C.c_int, vp, vp]
+        L.dmph_read_bodies_file.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), vp, vp]
+        L.dmph_bodies_from_contacts.argtypes = [vp, C.c_int, vp, vp, vp, C.POINTER(C.c_int), vp, C.c_int]
+        L.dmph_bodies_last_message.restype = C.c_char_p
         L.dmph_destroy.argtypes = [vp]
         L.dmph_last_error.argtypes = [vp]
         L.dmph_last_error.restype = C.c_char_p
         L.dmph_version.restype = C.c_char_p
         _lib = L
     return _lib
+
+
+def write_bodies(path, body_of_row, body_density):
+    """Write a body sidecar file (dmph_write_bodies_file)."""
+    b = np.ascontiguousarray(body_of_row, dtype=np.int32)
+    rho = np.ascontiguousarray(body_density, dtype=np.float64)
+    rc = lib().dmph_write_bodies_file(path.encode(), len(rho), len(b), _ptr(b), _ptr(rho))
+    if rc != 0:
+        raise DmphError(rc, lib().dmph_bodies_last_message().decode())
+
+
+def read_bodies(path):
+    """(body_of_row, body_density) of a body sidecar file (dmph_read_bodies_file)."""
+    L = lib()
+    nb, nr = C.c_int(), C.c_int()
+    rc = L.dmph_read_bodies_file(path.encode(), C.byref(nb), C.byref(nr), None, None)
+    if rc != 0:
+        raise DmphError(rc, L.dmph_bodies_last_message().decode())
+    b = np.empty(nr.value, np.int32)
+    rho = np.empty(nb.value, np.float64)
+    rc = L.dmph_read_bodies_file(path.encode(), C.byref(nb), C.byref(nr), _ptr(b), _ptr(rho))
+    if rc != 0:
+        raise DmphError(rc, L.dmph_bodies_last_message().decode())
+    return b, rho
+
+
+def bodies_from_contacts(params, typ, x):
+    """(body_of_row, body_density): the solid particles connected by contact
+    at 1.01 dx, numbered by first row (dmph_bodies_from_contacts)."""
+    t = np.ascontiguousarray(typ, dtype=np.int32)
+    xx = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+    b = np.empty(len(t), np.int32)
+    rho = np.empty(len(t), np.float64)
+    nb = C.c_int()
+    rc = lib().dmph_bodies_from_contacts(C.byref(params), len(t), _ptr(t), _ptr(xx), _ptr(b), C.byref(nb),
+                                         _ptr(rho), len(t))
+    if rc != 0:
+        raise DmphError(rc, lib().dmph_bodies_last_message().decode())
+    return b, rho[:nb.value].copy()
 
 
 PASS_VARIANTS = 5  # DMPH_PASS_VARIANTS (stencil passes)

@@ -277,6 +277,31 @@ int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64_t *entries
  */
 int dmph_set_bodies(dmph_ctx *ctx, int nbodies, const int *body_of_row, const double *body_density);
 
+/*
+ * Rigid bodies at the drop-in boundary (no counterpart in the reference,
+ * whose .grid rows carry no body and whose two solid types are its only
+ * densities, generator/generator.cpp:97, 211-214).  A body sidecar file beside
+ * the .grid gives each body's density and each grid row's body:
+ *     DMPH_BODIES 1
+ *     <nbodies> <nrows>
+ *     <density of body b>        nbodies lines
+ *     <body of grid row r>       nrows lines, -1 for no body
+ * dmph_read_bodies_file: call with body_of_row == NULL to get the counts;
+ * then with arrays of *nrows and *nbodies entries (their sizes passed in
+ * *nrows and *nbodies).  dmph_bodies_from_contacts: without a sidecar, the
+ * bodies are the connected components of the solid rows under contact at
+ * 1.01 dx (periodic minimum image), numbered by their first row, each with
+ * the density of its first row's type; body_of_row has n entries,
+ * body_density (optional) density_capacity.  Messages of the three calls:
+ * dmph_bodies_last_message().
+ */
+int dmph_write_bodies_file(const char *path, int nbodies, int nrows, const int *body_of_row,
+                           const double *body_density);
+int dmph_read_bodies_file(const char *path, int *nbodies, int *nrows, int *body_of_row, double *body_density);
+int dmph_bodies_from_contacts(const dmph_params *p, int n, const int *type, const double *x3, int *body_of_row,
+                              int *nbodies, double *body_density, int density_capacity);
+const char *dmph_bodies_last_message(void);
+
 /* Body state, each pointer optional: X,V,L 3 per body (centre of mass,
  * velocity, angular momentum), q 4 per body (w,x,y,z), mass 1 per body,
  * F,T 3 per body (total force and torque of the last substep). */
