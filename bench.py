@@ -310,7 +310,14 @@ def main():
     if bodies:
         g.set_bodies(scene.body, scene.body_density)
     n = scene.n
-    g.step(args.settle)
+    # the list-build autotuner times real rebuilds while stepping: its steps
+    # are the last of the settle steps
+    tune_build = args.precision == "fp32" and not args.no_autotune and args.settle >= 60
+    g.step(args.settle - (30 if tune_build else 0))
+    build_variant = None
+    if tune_build:
+        build_variant, build_ms = g.autotune_list_build(10)
+        build_variant = {"variant": build_variant, "list_build_ms": [round(float(x), 4) for x in build_ms]}
     variants = None
     if args.variants is not None:
         g.set_variants(*args.variants)
@@ -403,7 +410,7 @@ def main():
         "config": workload_config(scene, args, world),
         "run": {"rebuilds_in_timed_steps": rebuilds_timed, "rebuild_fraction_timed": frac_timed,
                 "timed_from_step": args.settle + args.warmup, "graph_replay": not args.no_graph,
-                "pass_variants": variants, "precision": args.precision,
+                "pass_variants": variants, "list_build_variant": build_variant, "precision": args.precision,
                 "debris": "rigid bodies (FP64)" if bodies else "individual DEM particles"},
         "sim_s_per_hour": p.dt * args.steps / (ms_max / 1e3) * 3600.0,
         "clocks": clk.summary(),

@@ -119,7 +119,7 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
     if (ctx->use_list) {
         // the list build alone is also timed as phase 6 (inside phase 1)
         if (ctx->prof) cudaEventRecord(ctx->pl0, st);
-        if (ctx->fp32) launch_build_list32(P, ctx->Q, S, ctx->dB, ctx->Wm.moving ? 0 : 1, st);
+        if (ctx->fp32) launch_build_list32(P, ctx->Q, S, ctx->dB, ctx->Wm.moving ? 0 : 1, st, ctx->var_build);
         else launch_build_list64(P, S, ctx->dB, st);
         if (ctx->prof) {
             cudaEventRecord(ctx->pl1, st);
@@ -297,11 +297,20 @@ void dmph::advance_host_clock(dmph_ctx *ctx)
 // Record, on a capturing stream, the head of a step followed by an IF node
 // whose body is the rebuild; the decision kernel of the head sets the
 // condition on the device.
+static int capture_rebuild_if(dmph_ctx *ctx, cudaGraphConditionalHandle cond, cudaStream_t st);
+
 static int capture_head_and_rebuild(dmph_ctx *ctx, cudaGraph_t g, cudaStream_t st)
 {
     cudaGraphConditionalHandle cond;
     CK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
     enqueue_head(ctx, (unsigned long long)cond, st);
+    return capture_rebuild_if(ctx, cond, st);
+}
+
+// On a capturing stream: an IF node after the stream's current work whose
+// body is the scene's rebuild, run when a decision kernel sets `cond`
+static int capture_rebuild_if(dmph_ctx *ctx, cudaGraphConditionalHandle cond, cudaStream_t st)
+{
     cudaStreamCaptureStatus status;
     const cudaGraphNode_t *deps = nullptr;
     size_t ndeps = 0;
@@ -1194,7 +1203,8 @@ extern "C" int dmph_set_pair_mode(dmph_ctx *ctx, int mode)
     const bool want = mode == DMPH_PAIRS_VERLET_LIST;
     if (want && !ctx->use_list) {
         // lists of the current cell sort
-        if (ctx->fp32) launch_build_list32(ctx->P, ctx->Q, ctx->S, ctx->dB, ctx->Wm.moving ? 0 : 1, ctx->st);
+        if (ctx->fp32)
+            launch_build_list32(ctx->P, ctx->Q, ctx->S, ctx->dB, ctx->Wm.moving ? 0 : 1, ctx->st, ctx->var_build);
         else launch_build_list64(ctx->P, ctx->S, ctx->dB, ctx->st);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(ctx->st));
@@ -1329,6 +1339,41 @@ extern "C" int dmph_autotune(dmph_ctx *ctx, int *variant_a, int *variant_b, floa
     return DMPH_OK;
 }
 
+extern "C" int dmph_autotune_list_build(dmph_ctx *ctx, int steps_per_variant, int *variant, float *ms)
+{
+    if (!ctx || steps_per_variant <= 0) return DMPH_EINVAL;
+    if (!ctx->fp32 || !ctx->use_list) {
+        ctx->err = "dmph_autotune_list_build: FP32 split build in Verlet-list mode only";
+        return DMPH_EINVAL;
+    }
+    // every variant builds the same lists, so the steps it times are the
+    // steps the caller would have run anyway
+    const bool graph = ctx->use_graph;
+    drop_graph(ctx);
+    ctx->use_graph = false;
+    const bool prof = ctx->prof;
+    int best = ctx->var_build;
+    float best_ms = 1e30f;
+    int rc = DMPH_OK;
+    for (int v = 0; v < kBuildVariants && !rc; ++v) {
+        ctx->var_build = v;
+        dmph_set_profiling(ctx, 1);
+        rc = dmph_step(ctx, steps_per_variant);
+        const long long n = ctx->phase_n[6];
+        const float t = n > 0 ? (float)(ctx->phase_ms[6] / (double)n) : -1.f;
+        if (ms) ms[v] = t;
+        if (!rc && n > 0 && t < best_ms) {
+            best_ms = t;
+            best = v;
+        }
+    }
+    dmph_set_profiling(ctx, prof ? 1 : 0);
+    ctx->var_build = best;
+    ctx->use_graph = graph;
+    if (variant) *variant = best;
+    return rc;
+}
+
 extern "C" int dmph_set_variants(dmph_ctx *ctx, int variant_a, int variant_b)
 {
     if (!ctx) return DMPH_EINVAL;
@@ -1364,6 +1409,14 @@ struct dmph_ensemble {
     long long launches = 0, steps = 0, graph_steps = 0;
     std::string err;
     dmph_ctx *ctx0 = nullptr;  // for error strings of the helpers
+    // fused: every scene's drift and rebuild decision run as one launch each,
+    // and the DEM / rigid-body tails of all scenes as one launch per kernel
+    // (list mode, walls at rest, debris as rigid bodies or none)
+    bool fused = false;
+    int max_dem = 0;                        // most DEM substeps of any scene
+    int total_bodies = 0;
+    int *bpre = nullptr;                    // device: prefix of the scenes' body counts
+    unsigned long long *handles = nullptr;  // device: the IF-node conditions of the recorded step
 };
 
 #define EK(call)                                                                          \
@@ -1388,6 +1441,10 @@ static void ens_release(dmph_ensemble *e)
     if (e->st) cudaStreamSynchronize(e->st);
     ens_drop_graph(e);
     if (e->tab) cudaFree(e->tab);
+    if (e->bpre) cudaFree(e->bpre);
+    if (e->handles) cudaFree(e->handles);
+    e->bpre = nullptr;
+    e->handles = nullptr;
     for (cudaEvent_t v : e->fork) cudaEventDestroy(v);
     if (e->join) cudaEventDestroy(e->join);
     if (e->ev0) cudaEventDestroy(e->ev0);
@@ -1424,6 +1481,9 @@ extern "C" int dmph_ensemble_create(dmph_ctx *const *scenes, int nscenes, dmph_e
         h[k].Q = c->Q;
         h[k].S = c->S;
         h[k].dB = c->dB;
+        h[k].maxshift = c->maxshift;
+        h[k].Bd = c->Bd;
+        h[k].demSteps = c->demSteps;
     }
     cudaError_t ce = cudaMalloc((void **)&e->tab, sizeof(EnsScene) * nscenes);
     if (ce == cudaSuccess) ce = cudaMemcpy(e->tab, h.data(), sizeof(EnsScene) * nscenes, cudaMemcpyHostToDevice);
@@ -1445,7 +1505,103 @@ extern "C" int dmph_ensemble_create(dmph_ctx *const *scenes, int nscenes, dmph_e
     if (!e->use_list)
         for (dmph_ctx *c : e->scenes) c->use_list = false;
     for (dmph_ctx *c : e->scenes) drop_graph(c);
+    // fused heads and tails
+    e->fused = e->use_list;
+    std::vector<int> bpre(nscenes + 1, 0);
+    for (int k = 0; k < nscenes; ++k) {
+        dmph_ctx *c = e->scenes[k];
+        e->fused = e->fused && c->walls_rest && (c->Bd.B > 0 || c->n_solid == 0);
+        e->max_dem = std::max(e->max_dem, c->demSteps);
+        bpre[k + 1] = bpre[k] + c->Bd.B;
+    }
+    e->total_bodies = bpre[nscenes];
+    if (e->fused) {
+        ce = cudaMalloc((void **)&e->bpre, sizeof(int) * (nscenes + 1));
+        if (ce == cudaSuccess)
+            ce = cudaMemcpy(e->bpre, bpre.data(), sizeof(int) * (nscenes + 1), cudaMemcpyHostToDevice);
+        if (ce == cudaSuccess) ce = cudaMalloc((void **)&e->handles, sizeof(unsigned long long) * nscenes);
+        // the drift accumulates into cleared accumulators; the decision clears them after
+        for (int k = 0; ce == cudaSuccess && k < nscenes; ++k)
+            ce = cudaMemset(e->scenes[k]->maxshift, 0, sizeof(unsigned long long));
+        if (ce != cudaSuccess) {
+            ens_release(e);
+            delete e;
+            return DMPH_ECUDA;
+        }
+    }
     *out = e;
+    return DMPH_OK;
+}
+
+// the pair passes of all scenes: one persistent launch each
+static void ens_enqueue_passes(dmph_ensemble *e)
+{
+    const int ns = (int)e->scenes.size();
+    if (e->use_list) {
+        launch_ens_pass_list(e->tab, ns, false, e->st);
+        launch_ens_pass_a32(e->tab, ns, e->var_a, e->st, 1);
+        launch_ens_pass_list(e->tab, ns, true, e->st);
+        launch_ens_pass_b32(e->tab, ns, e->var_b, e->st, 1);
+    } else {
+        launch_ens_pass_a32(e->tab, ns, e->var_a, e->st);
+        launch_ens_pass_b32(e->tab, ns, e->var_b, e->st);
+    }
+    launch_ens_fluid_accel32(e->tab, ns, e->st);
+}
+
+// kernels of one fused ensemble step outside the scenes' rebuilds
+static long long ens_fused_launches(const dmph_ensemble *e)
+{
+    return 2 + (e->use_list ? 6 : 3) + 2 + 3LL * e->max_dem;
+}
+
+// One fused ensemble step: one drift launch and one decision launch for all
+// scenes, each scene's rebuild when its decision asks for one (an IF node per
+// scene when conds is given, set by the decision kernel; else read on the
+// host), the ensemble passes, then the DEM tails of all scenes as one launch
+// per kernel and substep.
+static int ens_enqueue_fused(dmph_ensemble *e, const std::vector<cudaGraphConditionalHandle> *conds)
+{
+    const int ns = (int)e->scenes.size();
+    for (dmph_ctx *c : e->scenes) c->Wm.moving = 0;  // walls at rest in every scene
+    launch_ens_drift32(e->tab, ns, e->ctx0->sms, e->st);
+    launch_ens_decide(e->tab, ns, conds ? e->handles : nullptr, e->st);
+    EK(cudaEventRecord(e->join, e->st));
+    for (int k = 0; k < ns; ++k) {
+        dmph_ctx *c = e->scenes[k];
+        EK(cudaStreamWaitEvent(c->st, e->join, 0));
+        if (conds) {
+            const int rc = capture_rebuild_if(c, (*conds)[k], c->st);
+            if (rc) {
+                e->err = c->err;
+                return rc;
+            }
+        } else {
+            EK(cudaMemcpyAsync(c->h_small, c->dB + B_NEED, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        }
+    }
+    if (!conds) {
+        for (dmph_ctx *c : e->scenes) {
+            EK(cudaStreamSynchronize(c->st));
+            if (c->h_small[0]) {
+                enqueue_rebuild(c, false, c->st);
+                c->launches += rebuild_launches(c, false);
+                c->host_rebuilds++;
+            }
+        }
+    }
+    for (int k = 0; k < ns; ++k) {
+        EK(cudaEventRecord(e->fork[k], e->scenes[k]->st));
+        EK(cudaStreamWaitEvent(e->st, e->fork[k], 0));
+    }
+    ens_enqueue_passes(e);
+    launch_ens_solid_force_to64(e->tab, ns, e->st);
+    for (int sub = 0; sub < e->max_dem; ++sub) {
+        launch_ens_clump_dem(e->tab, ns, sub, e->st);
+        launch_ens_body_step(e->tab, ns, e->bpre, e->total_bodies, sub, e->st);
+    }
+    launch_ens_sync_solids32(e->tab, ns, e->st);
+    EK(cudaGetLastError());
     return DMPH_OK;
 }
 
@@ -1491,17 +1647,7 @@ static int ens_enqueue_step(dmph_ensemble *e, cudaGraph_t g)
         EK(cudaEventRecord(e->fork[k], e->scenes[k]->st));
         EK(cudaStreamWaitEvent(e->st, e->fork[k], 0));
     }
-    // the pair passes of all scenes: one persistent launch each
-    if (e->use_list) {
-        launch_ens_pass_list(e->tab, ns, false, e->st);
-        launch_ens_pass_a32(e->tab, ns, e->var_a, e->st, 1);
-        launch_ens_pass_list(e->tab, ns, true, e->st);
-        launch_ens_pass_b32(e->tab, ns, e->var_b, e->st, 1);
-    } else {
-        launch_ens_pass_a32(e->tab, ns, e->var_a, e->st);
-        launch_ens_pass_b32(e->tab, ns, e->var_b, e->st);
-    }
-    launch_ens_fluid_accel32(e->tab, ns, e->st);
+    ens_enqueue_passes(e);
     EK(cudaGetLastError());
     EK(cudaEventRecord(e->join, e->st));
     // DEM / rigid bodies per scene, then join
@@ -1518,6 +1664,7 @@ static int ens_enqueue_step(dmph_ensemble *e, cudaGraph_t g)
 
 static long long ens_step_launches(const dmph_ensemble *e)
 {
+    if (e->fused) return ens_fused_launches(e);
     long long n = 3 + (e->use_list ? 3 : 0);  // list passes: A, B fluid, B debris
     for (const dmph_ctx *c : e->scenes) n += 2 + dem_launches(c);
     return n;
@@ -1535,8 +1682,20 @@ static int ens_build_graph(dmph_ensemble *e)
 {
     cudaGraph_t g = nullptr;
     EK(cudaGraphCreate(&g, 0));
+    std::vector<cudaGraphConditionalHandle> conds;
+    if (e->fused) {
+        // one condition per scene, set by the ensemble decision kernel
+        const int ns = (int)e->scenes.size();
+        conds.resize(ns);
+        std::vector<unsigned long long> h(ns);
+        for (int k = 0; k < ns; ++k) {
+            EK(cudaGraphConditionalHandleCreate(&conds[k], g, 0, cudaGraphCondAssignDefault));
+            h[k] = (unsigned long long)conds[k];
+        }
+        EK(cudaMemcpy(e->handles, h.data(), sizeof(unsigned long long) * ns, cudaMemcpyHostToDevice));
+    }
     EK(cudaStreamBeginCaptureToGraph(e->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    const int rc = ens_enqueue_step(e, g);
+    const int rc = e->fused ? ens_enqueue_fused(e, &conds) : ens_enqueue_step(e, g);
     cudaGraph_t g2 = g;
     const cudaError_t ce = cudaStreamEndCapture(e->st, &g2);
     if (rc || ce != cudaSuccess) {
@@ -1558,6 +1717,10 @@ static int ens_step_once(dmph_ensemble *e)
         }
         EK(cudaGraphLaunch(e->gexec, e->st));
         e->graph_steps++;
+    } else if (e->fused) {
+        const int rc = ens_enqueue_fused(e, nullptr);
+        if (rc) return rc;
+        e->launches += ens_fused_launches(e);
     } else {
         const int rc = ens_enqueue_step(e, nullptr);
         if (rc) return rc;

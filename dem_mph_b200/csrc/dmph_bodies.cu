@@ -100,103 +100,112 @@ __device__ __forceinline__ void clump_store(const DevParams &P, const DevState &
 // can hold a contact partner: contacts need |x_j - x_i| <= dx, so only the
 // neighbour cells within 1.6 dx of i's rebuild-time position (about 8 of the
 // 27) are visited, for the solid and wall classes.  FP64 on the master
-// planes; per-lane partial sums are combined with warp shuffles.  gate: the
-// FP32 Verlet lists are in use, and this walk stands in only after a list
-// overflow.
+// planes; per-lane partial sums are combined with warp shuffles.  One warp
+// per debris particle i (lane = its lane).
+__device__ __forceinline__ void clump_dem_stencil_particle(const DevParams &P, const DevState &S, int i, int lane)
+{
+    const int N = P.N;
+    const double xi[3] = {S.pos[i], S.pos[N + i], S.pos[2 * N + i]};
+    const double vi[3] = {S.vel[i], S.vel[N + i], S.vel[2 * N + i]};
+    const int ti = S.type[i];
+    const int bi = S.bid[i];
+    const double mi = particle_density(S, P, i, ti) * P.V;
+    // rebuild-time cell and the neighbour cells within reach
+    const int key_cell = (int)(word_key(S.skey[i]) % (unsigned)P.T);
+    int c[3];
+    if (P.dim == 2) {
+        c[0] = key_cell / P.cc[1];
+        c[1] = key_cell % P.cc[1];
+        c[2] = 0;
+    } else {
+        c[0] = key_cell / (P.cc[1] * P.cc[2]);
+        c[1] = (key_cell / P.cc[2]) % P.cc[1];
+        c[2] = key_cell % P.cc[2];
+    }
+    // contact partners are within dx now; positions drift at most 0.05 dx
+    // from their rebuild-time values between rebuild checks, and up to
+    // about 0.25 dx inside one surrogate block: 1.6 dx covers both
+    const double reach = 1.6 * P.dx;
+    int lo[3], hi[3];
+    for (int k = 0; k < 3; k++) {
+        const double loc = S.xref[k * N + i] - (P.dmin[k] + c[k] * P.cw[k]);
+        const bool flat = (k == 2 && P.dim == 2);
+        lo[k] = flat ? 0 : (loc < reach ? -1 : 0);
+        hi[k] = flat ? 0 : (P.cw[k] - loc < reach ? 1 : 0);
+    }
+    double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
+    // the (cell, class) ranges to visit, fetched by 16 lanes at once:
+    // lane r < 16 holds range r = (cell index r / 2 of the <= 8 cells,
+    // class 1 + r % 2)
+    const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+    const int nranges = 2 * nx * ny * nz;
+    int rb = 0, re = 0;
+    if (lane < nranges) {
+        const int c_ = lane >> 1, cls = 1 + (lane & 1);
+        const int oz = lo[2] + c_ % nz, oy = lo[1] + (c_ / nz) % ny, ox = lo[0] + c_ / (nz * ny);
+        const int off = cls * P.T + cell_id(P, c[0] + ox, c[1] + oy, c[2] + oz);
+        rb = __ldg(S.cell_start + off);
+        re = __ldg(S.cell_start + off + 1);
+    }
+    for (int r = 0; r < nranges; ++r) {
+        const int jb = __shfl_sync(kFull, rb, r), je = __shfl_sync(kFull, re, r);
+        for (int j = jb + lane; j < je; j += kWarp) clump_pair(P, S, i, xi, vi, ti, bi, mi, j, F, T);
+    }
+    clump_store(P, S, i, lane, F, T);
+}
+
+// gate: the FP32 Verlet lists are in use, and this walk stands in only after
+// a list overflow
 __global__ void __launch_bounds__(8 * kWarp) k_clump_dem(DevParams P, DevState S, const int *dB, int gate)
 {
     if (gate && dB[B_LIST_OVF] == 0) return;
     const int lane = threadIdx.x & 31;
-    const int N = P.N;
     const int sb = dB[B_SB], se = dB[B_SE];
     const int nwarps = gridDim.x * (blockDim.x >> 5);
-    for (int i = sb + blockIdx.x * (blockDim.x >> 5) + (int)(threadIdx.x >> 5); i < se; i += nwarps) {
-        const double xi[3] = {S.pos[i], S.pos[N + i], S.pos[2 * N + i]};
-        const double vi[3] = {S.vel[i], S.vel[N + i], S.vel[2 * N + i]};
-        const int ti = S.type[i];
-        const int bi = S.bid[i];
-        const double mi = particle_density(S, P, i, ti) * P.V;
-        // rebuild-time cell and the neighbour cells within reach
-        const int key_cell = (int)(word_key(S.skey[i]) % (unsigned)P.T);
-        int c[3];
-        if (P.dim == 2) {
-            c[0] = key_cell / P.cc[1];
-            c[1] = key_cell % P.cc[1];
-            c[2] = 0;
-        } else {
-            c[0] = key_cell / (P.cc[1] * P.cc[2]);
-            c[1] = (key_cell / P.cc[2]) % P.cc[1];
-            c[2] = key_cell % P.cc[2];
-        }
-        // contact partners are within dx now; positions drift at most 0.05 dx
-        // from their rebuild-time values between rebuild checks, and up to
-        // about 0.25 dx inside one surrogate block: 1.6 dx covers both
-        const double reach = 1.6 * P.dx;
-        int lo[3], hi[3];
-        for (int k = 0; k < 3; k++) {
-            const double loc = S.xref[k * N + i] - (P.dmin[k] + c[k] * P.cw[k]);
-            const bool flat = (k == 2 && P.dim == 2);
-            lo[k] = flat ? 0 : (loc < reach ? -1 : 0);
-            hi[k] = flat ? 0 : (P.cw[k] - loc < reach ? 1 : 0);
-        }
-        double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
-        // the (cell, class) ranges to visit, fetched by 16 lanes at once:
-        // lane r < 16 holds range r = (cell index r / 2 of the <= 8 cells,
-        // class 1 + r % 2)
-        const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
-        const int nranges = 2 * nx * ny * nz;
-        int rb = 0, re = 0;
-        if (lane < nranges) {
-            const int c_ = lane >> 1, cls = 1 + (lane & 1);
-            const int oz = lo[2] + c_ % nz, oy = lo[1] + (c_ / nz) % ny, ox = lo[0] + c_ / (nz * ny);
-            const int off = cls * P.T + cell_id(P, c[0] + ox, c[1] + oy, c[2] + oz);
-            rb = __ldg(S.cell_start + off);
-            re = __ldg(S.cell_start + off + 1);
-        }
-        for (int r = 0; r < nranges; ++r) {
-            const int jb = __shfl_sync(kFull, rb, r), je = __shfl_sync(kFull, re, r);
-            for (int j = jb + lane; j < je; j += kWarp) clump_pair(P, S, i, xi, vi, ti, bi, mi, j, F, T);
-        }
-        clump_store(P, S, i, lane, F, T);
-    }
+    for (int i = sb + blockIdx.x * (blockDim.x >> 5) + (int)(threadIdx.x >> 5); i < se; i += nwarps)
+        clump_dem_stencil_particle(P, S, i, lane);
 }
 
 // FP32 list mode: one warp per debris particle over its Verlet list (radius
 // MaxRadius + MARGIN, far beyond the contact distance dx plus any drift
 // before the next rebuild), whose entries carry the class of j, so the fluid
 // entries are passed over without a gather.
+__device__ __forceinline__ void clump_dem_list_particle(const DevParams &P, const DevState &S, int i, int lane)
+{
+    const int N = P.N;
+    const long long ld = N;
+    const int cnt = S.nbn[i];
+    const double xi[3] = {S.pos[i], S.pos[N + i], S.pos[2 * N + i]};
+    const double vi[3] = {S.vel[i], S.vel[N + i], S.vel[2 * N + i]};
+    const int ti = S.type[i];
+    const int bi = S.bid[i];
+    const double mi = particle_density(S, P, i, ti) * P.V;
+    double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
+    // four entries per lane loaded before any is used (lists hold at
+    // most 192 entries in 3D: at most two rounds)
+    for (int k0 = 0; k0 < cnt; k0 += 4 * kWarp) {
+        unsigned e[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k = k0 + lane + u * kWarp;
+            e[u] = k < cnt ? __ldg(S.nbl + list_index(k, i, ld)) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (e[u] & (kEntrySolid | kEntryWall))
+                clump_pair(P, S, i, xi, vi, ti, bi, mi, (int)(e[u] & kEntrySlot), F, T);
+    }
+    clump_store(P, S, i, lane, F, T);
+}
+
 __global__ void __launch_bounds__(8 * kWarp) k_clump_dem_list(DevParams P, DevState S, const int *dB)
 {
     if (dB[B_LIST_OVF]) return;
     const int lane = threadIdx.x & 31;
-    const int N = P.N;
-    const long long ld = N;
     const int sb = dB[B_SB], se = dB[B_SE];
     const int nwarps = gridDim.x * (blockDim.x >> 5);
-    for (int i = sb + blockIdx.x * (blockDim.x >> 5) + (int)(threadIdx.x >> 5); i < se; i += nwarps) {
-        const int cnt = S.nbn[i];
-        const double xi[3] = {S.pos[i], S.pos[N + i], S.pos[2 * N + i]};
-        const double vi[3] = {S.vel[i], S.vel[N + i], S.vel[2 * N + i]};
-        const int ti = S.type[i];
-        const int bi = S.bid[i];
-        const double mi = particle_density(S, P, i, ti) * P.V;
-        double F[3] = {0.0, 0.0, 0.0}, T[3] = {0.0, 0.0, 0.0};
-        // four entries per lane loaded before any is used (lists hold at
-        // most 192 entries in 3D: at most two rounds)
-        for (int k0 = 0; k0 < cnt; k0 += 4 * kWarp) {
-            unsigned e[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int k = k0 + lane + u * kWarp;
-                e[u] = k < cnt ? __ldg(S.nbl + list_index(k, i, ld)) : 0u;
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (e[u] & (kEntrySolid | kEntryWall))
-                    clump_pair(P, S, i, xi, vi, ti, bi, mi, (int)(e[u] & kEntrySlot), F, T);
-        }
-        clump_store(P, S, i, lane, F, T);
-    }
+    for (int i = sb + blockIdx.x * (blockDim.x >> 5) + (int)(threadIdx.x >> 5); i < se; i += nwarps)
+        clump_dem_list_particle(P, S, i, lane);
 }
 
 // One block per body: its threads take the members, the per-thread sums are
@@ -204,12 +213,11 @@ __global__ void __launch_bounds__(8 * kWarp) k_clump_dem_list(DevParams P, DevSt
 constexpr int kBodyThreads = 256;
 
 template <bool F32>
-__global__ void __launch_bounds__(kBodyThreads) k_body_step(DevParams P, DevState S, DevBodies Bd)
+__device__ __forceinline__ void body_step_block(const DevParams &P, const DevState &S, const DevBodies &Bd, int b)
 {
     constexpr int NW = kBodyThreads / kWarp;
     __shared__ double red[NW][6];
     __shared__ double tot[6];
-    const int b = blockIdx.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int N = P.N;
     const int m0 = Bd.ptr[b], m1 = Bd.ptr[b + 1];
@@ -322,6 +330,67 @@ __global__ void __launch_bounds__(kBodyThreads) k_body_step(DevParams P, DevStat
             }
         }
     }
+}
+
+template <bool F32>
+__global__ void __launch_bounds__(kBodyThreads) k_body_step(DevParams P, DevState S, DevBodies Bd)
+{
+    body_step_block<F32>(P, S, Bd, blockIdx.x);
+}
+
+// ---- ensemble: the contacts and body updates of every scene in one launch
+// each (substep `sub`; scenes with fewer DEM substeps take no part in the
+// later ones)
+
+// one warp per debris particle of every scene whose lists are usable
+// (LIST) or overflowed (stencil walk)
+template <bool LIST>
+__global__ void __launch_bounds__(8 * kWarp) k_ens_clump_dem(const EnsScene *__restrict__ tab, int ns, int sub)
+{
+    __shared__ int pre[kMaxEnsemble + 1];
+    const int total = ens_count_prefix(ns, pre, [&](int k) {
+        const EnsScene &e = tab[k];
+        const bool ovf = e.dB[B_LIST_OVF] != 0;
+        return (sub < e.demSteps && e.Bd.B > 0 && ovf != LIST) ? e.dB[B_SE] - e.dB[B_SB] : 0;
+    });
+    const int lane = threadIdx.x & 31;
+    const int nwarps = gridDim.x * (blockDim.x >> 5);
+    for (int g = blockIdx.x * (blockDim.x >> 5) + (int)(threadIdx.x >> 5); g < total; g += nwarps) {
+        const int k = ens_scene_at(pre, ns, g);
+        const EnsScene &e = tab[k];
+        const int i = e.dB[B_SB] + g - pre[k];
+        if (LIST) clump_dem_list_particle(e.P, e.S, i, lane);
+        else clump_dem_stencil_particle(e.P, e.S, i, lane);
+    }
+}
+
+// one block per body of every scene; bpre[k] = bodies of the scenes before k
+__global__ void __launch_bounds__(kBodyThreads) k_ens_body_step(const EnsScene *__restrict__ tab, int ns,
+                                                                 const int *__restrict__ bpre, int sub)
+{
+    const int g = blockIdx.x;
+    int lo = 0, hi = ns - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (bpre[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    const EnsScene &e = tab[lo];
+    if (sub >= e.demSteps) return;  // block-uniform
+    body_step_block<false>(e.P, e.S, e.Bd, g - bpre[lo]);
+}
+
+void launch_ens_clump_dem(const EnsScene *tab, int ns, int sub, cudaStream_t st)
+{
+    static const int gl = persistent_grid((const void *)k_ens_clump_dem<true>, 8 * kWarp);
+    k_ens_clump_dem<true><<<gl, 8 * kWarp, 0, st>>>(tab, ns, sub);
+    static const int g = persistent_grid((const void *)k_ens_clump_dem<false>, 8 * kWarp);
+    k_ens_clump_dem<false><<<g, 8 * kWarp, 0, st>>>(tab, ns, sub);
+}
+
+void launch_ens_body_step(const EnsScene *tab, int ns, const int *bpre, int total_bodies, int sub, cudaStream_t st)
+{
+    if (total_bodies > 0) k_ens_body_step<<<total_bodies, kBodyThreads, 0, st>>>(tab, ns, bpre, sub);
 }
 
 void launch_slot_of_row(const DevParams &P, const int *pidx, int *slot_of_row, cudaStream_t st)

@@ -59,6 +59,7 @@ struct dmph_ctx {
     int var_a = 0, var_b = 0;  // launch variants of the FP32 pair passes (dmph_autotune)
     bool use_list = false;     // FP32 pair passes over Verlet lists built at each rebuild
     int var_la = 1, var_lb = 1;  // launch variants of the list passes
+    int var_build = 0;           // launch variant of the FP32 list build (dmph_autotune_list_build)
     double *vir = nullptr;        // virial pressure (allocated on the first request)
     Chunk *chunks2 = nullptr;  // partition scratch
     int demSteps = 0;

@@ -65,59 +65,65 @@ __device__ __forceinline__ void chunk_cell(const DevParams &P, int key_cell, int
 }
 
 // ---------------------------------------------------------------- drift
-__global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm, unsigned long long *maxshift)
+// drift of slot i (fluid moves, walls move or stop, everything's force is
+// reset); returns |x - x_ref|^2 in the FP32 frame, +inf for a non-finite
+// position or velocity
+__device__ __forceinline__ float drift32_slot(const DevParams &P, const DevParams32 &Q, const DevState &S,
+                                              const WallMotion &Wm, int i)
 {
     const int N = P.N;
-    float m2 = 0.f;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        float4 p = S.p4[i];
-        float4 v = S.v4[i];
-        const unsigned w = __float_as_uint(p.w);
-        const int t = unpack_type(w);
-        if (is_fluid(t)) {
-            p.x = fmaf(v.x, Q.dt, p.x);
-            p.y = fmaf(v.y, Q.dt, p.y);
-            p.z = fmaf(v.z, Q.dt, p.z);
-        } else if (is_wall(t)) {
-            if (Wm.moving) {
-                const double o[3] = {P.dmin[0] + unpack_cx(w) * P.cw[0], P.dmin[1] + unpack_cy(w) * P.cw[1],
-                                     P.dmin[2] + unpack_cz(w) * P.cw[2]};
-                double x[3] = {o[0] + p.x, o[1] + p.y, o[2] + p.z}, vv[3];
-                double r[3] = {x[0] - Wm.C[t][0], x[1] - Wm.C[t][1], x[2] - Wm.C[t][2]};
-                const double(*R)[3] = Wm.R[t];
-                const double *om = Wm.Om[t];
-                r[0] = R[0][0] * r[0] + R[0][1] * r[1] + R[0][2] * r[2];
-                r[1] = R[1][0] * r[0] + R[1][1] * r[1] + R[1][2] * r[2];
-                r[2] = R[2][0] * r[0] + R[2][1] * r[1] + R[2][2] * r[2];
-                vv[0] = om[1] * r[2] - om[2] * r[1] + Wm.Vel[t][0];
-                vv[1] = om[2] * r[0] - om[0] * r[2] + Wm.Vel[t][1];
-                vv[2] = om[0] * r[1] - om[1] * r[0] + Wm.Vel[t][2];
-                for (int d = 0; d < 3; d++) x[d] = r[d] + Wm.C[t][d] + Wm.Vel[t][d] * P.dt;
-                p.x = (float)(x[0] - o[0]);
-                p.y = (float)(x[1] - o[1]);
-                p.z = (float)(x[2] - o[2]);
-                v = make_float4((float)vv[0], (float)vv[1], (float)vv[2], 0.f);
-                for (int d = 0; d < 3; d++) {
-                    const double t0 = x[d] - P.dmin[d];
-                    S.pos[d * N + i] = (t0 - P.W[d] * floor(t0 / P.W[d])) + P.dmin[d];
-                    S.vel[d * N + i] = vv[d];
-                }
-            } else {
-                v = make_float4(0.f, 0.f, 0.f, 0.f);
-                for (int d = 0; d < 3; d++) S.vel[d * N + i] = 0.0;
+    float4 p = S.p4[i];
+    float4 v = S.v4[i];
+    const unsigned w = __float_as_uint(p.w);
+    const int t = unpack_type(w);
+    if (is_fluid(t)) {
+        p.x = fmaf(v.x, Q.dt, p.x);
+        p.y = fmaf(v.y, Q.dt, p.y);
+        p.z = fmaf(v.z, Q.dt, p.z);
+    } else if (is_wall(t)) {
+        if (Wm.moving) {
+            const double o[3] = {P.dmin[0] + unpack_cx(w) * P.cw[0], P.dmin[1] + unpack_cy(w) * P.cw[1],
+                                 P.dmin[2] + unpack_cz(w) * P.cw[2]};
+            double x[3] = {o[0] + p.x, o[1] + p.y, o[2] + p.z}, vv[3];
+            double r[3] = {x[0] - Wm.C[t][0], x[1] - Wm.C[t][1], x[2] - Wm.C[t][2]};
+            const double(*R)[3] = Wm.R[t];
+            const double *om = Wm.Om[t];
+            r[0] = R[0][0] * r[0] + R[0][1] * r[1] + R[0][2] * r[2];
+            r[1] = R[1][0] * r[0] + R[1][1] * r[1] + R[1][2] * r[2];
+            r[2] = R[2][0] * r[0] + R[2][1] * r[1] + R[2][2] * r[2];
+            vv[0] = om[1] * r[2] - om[2] * r[1] + Wm.Vel[t][0];
+            vv[1] = om[2] * r[0] - om[0] * r[2] + Wm.Vel[t][1];
+            vv[2] = om[0] * r[1] - om[1] * r[0] + Wm.Vel[t][2];
+            for (int d = 0; d < 3; d++) x[d] = r[d] + Wm.C[t][d] + Wm.Vel[t][d] * P.dt;
+            p.x = (float)(x[0] - o[0]);
+            p.y = (float)(x[1] - o[1]);
+            p.z = (float)(x[2] - o[2]);
+            v = make_float4((float)vv[0], (float)vv[1], (float)vv[2], 0.f);
+            for (int d = 0; d < 3; d++) {
+                const double t0 = x[d] - P.dmin[d];
+                S.pos[d * N + i] = (t0 - P.W[d] * floor(t0 / P.W[d])) + P.dmin[d];
+                S.vel[d * N + i] = vv[d];
             }
+        } else {
+            v = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int d = 0; d < 3; d++) S.vel[d * N + i] = 0.0;
         }
-        S.p4[i] = p;
-        S.v4[i] = v;
-        S.f4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 r = S.xref4[i];
-        const float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
-        m2 = fmaxf(m2, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-        // a non-finite position or velocity makes the maximum +inf, which the
-        // rebuild decision reports instead of rebuilding
-        if (!isfinite(p.x + p.y + p.z + v.x + v.y + v.z)) m2 = CUDART_INF_F;
     }
-    // reduce as double bits so the host compares like the FP64 path
+    S.p4[i] = p;
+    S.v4[i] = v;
+    S.f4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 r = S.xref4[i];
+    const float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
+    // a non-finite position or velocity makes the maximum +inf, which the
+    // rebuild decision reports instead of rebuilding
+    if (!isfinite(p.x + p.y + p.z + v.x + v.y + v.z)) return CUDART_INF_F;
+    return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+// block maximum of m2, as double bits so the decision compares like the FP64
+// path, into *maxshift (one atomic per block); all threads of the block call it
+__device__ __forceinline__ void block_max_shift(float m2, unsigned long long *maxshift)
+{
     unsigned long long b = __double_as_longlong((double)m2);
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long ob = __shfl_down_sync(kFull, b, o);
@@ -130,6 +136,31 @@ __global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm,
         unsigned long long mx = 0;
         for (int k = 0; k < (int)(blockDim.x >> 5); k++) mx = red[k] > mx ? red[k] : mx;
         atomicMax(maxshift, mx);
+    }
+    __syncthreads();
+}
+
+__global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm, unsigned long long *maxshift)
+{
+    float m2 = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.N; i += gridDim.x * blockDim.x)
+        m2 = fmaxf(m2, drift32_slot(P, Q, S, Wm, i));
+    block_max_shift(m2, maxshift);
+}
+
+// The drift of every scene of an ensemble in one launch (scenes whose walls
+// are at rest: no wall motion), each scene's maximum into its own
+// accumulator.
+__global__ void k_ens_drift32(const EnsScene *__restrict__ tab, int ns)
+{
+    WallMotion rest;
+    rest.moving = 0;
+    for (int k = 0; k < ns; ++k) {
+        const EnsScene &e = tab[k];
+        float m2 = 0.f;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < e.P.N; i += gridDim.x * blockDim.x)
+            m2 = fmaxf(m2, drift32_slot(e.P, e.Q, e.S, rest, i));
+        block_max_shift(m2, e.maxshift);
     }
 }
 
@@ -561,11 +592,30 @@ __device__ __forceinline__ void pass_b32_body(const DevParams &P, const DevParam
 // displacement by MARGIN/2, so every pair a kernel accepts until the next
 // rebuild is in the list.  The passes then run one thread per particle over
 // its list instead of over the ~800 candidates of the 27-cell stencil.
+// Candidates are staged in pairs (2k, 2k+1) so that one packed FP32x2 FMA
+// (__ffma2_rn, sm_100) advances the distance tests of both: the same
+// round-to-nearest FMAs as scalar fmaf, half the issued instructions.
 struct TileL {
-    float4 p[kWarp];     // position in the frame of the warp's cell, .w = its squared norm
-    unsigned e[kWarp];   // list entry of the candidate
-    int t[kWarp];        // type of the candidate
+    float4 xy[kWarp / 2];  // (x_2k, x_2k+1, y_2k, y_2k+1) in the frame of the warp's cell
+    float4 zw[kWarp / 2];  // (z_2k, z_2k+1, |p_2k|^2, |p_2k+1|^2)
+    unsigned e[kWarp];     // list entry of the candidate
+    int t[kWarp];          // type of the candidate
 };
+__device__ __forceinline__ void tile_put(TileL &tl, int s, float x, float y, float z, float w)
+{
+    float *a = reinterpret_cast<float *>(&tl.xy[s >> 1]);
+    float *b = reinterpret_cast<float *>(&tl.zw[s >> 1]);
+    a[s & 1] = x;
+    a[2 + (s & 1)] = y;
+    b[s & 1] = z;
+    b[2 + (s & 1)] = w;
+}
+__device__ __forceinline__ float4 tile_get(const TileL &tl, int s)
+{
+    const float *a = reinterpret_cast<const float *>(&tl.xy[s >> 1]);
+    const float *b = reinterpret_cast<const float *>(&tl.zw[s >> 1]);
+    return make_float4(a[s & 1], a[2 + (s & 1)], b[s & 1], b[2 + (s & 1)]);
+}
 
 // split: the walls are at rest until the next rebuild (set by the host when no
 // wall motion is active).  Wall-wall pairs are then summed here, once, with
@@ -615,7 +665,7 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
             const int dz = min_image_cell(unpack_cz(w) - ciz, P.cc[2]);
             const float x = fmaf((float)dx, Q.cw[0], pj.x), y = fmaf((float)dy, Q.cw[1], pj.y),
                         z = fmaf((float)dz, Q.cw[2], pj.z);
-            tl.p[slot] = make_float4(x, y, z, fmaf(x, x, fmaf(y, y, z * z)));
+            tile_put(tl, slot, x, y, z, fmaf(x, x, fmaf(y, y, z * z)));
             tl.t[slot] = tj;
             tl.e[slot] = (unsigned)j | entry_offsets(dx, dy, dz) | (is_solid(tj) ? kEntrySolid : 0u) |
                          (is_wall(tj) ? kEntryWall : 0u);
@@ -624,7 +674,7 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
             // called by every lane: the count exchange below needs them all.
             // Slots past the batch get a huge norm, so the tests need no
             // bounds check.
-            if (lane >= nb) tl.p[lane] = make_float4(0.f, 0.f, 0.f, 1.0e30f);
+            if (lane >= nb) tile_put(tl, lane, 0.f, 0.f, 0.f, 1.0e30f);
             __syncwarp();
             unsigned m = 0;  // bit s0: candidate part * G + s0
             if (active) {
@@ -632,10 +682,17 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
                 // candidate; its rounding (a few 1e-6 of rc^2 at these
                 // magnitudes) is covered by testing against rc^2 (1 + 1e-4),
                 // so the list holds every pair within rc and a 5e-5 rc shell
+                const float2 A0 = make_float2(a0, a0), A1 = make_float2(a1, a1), A2 = make_float2(a2, a2);
 #pragma unroll
-                for (int s0 = 0; s0 < G; ++s0) {
-                    const float4 pj = tl.p[part * G + s0];
-                    m |= (fmaf(a0, pj.x, fmaf(a1, pj.y, fmaf(a2, pj.z, pj.w))) <= thr) ? (1u << s0) : 0u;
+                for (int s0 = 0; s0 < G; s0 += 2) {
+                    const int k = (part * G + s0) >> 1;
+                    const float4 xy = tl.xy[k], zw = tl.zw[k];
+                    // fmaf(a0, x, fmaf(a1, y, fmaf(a2, z, w))) of both candidates
+                    float2 d = __ffma2_rn(A2, make_float2(zw.x, zw.y), make_float2(zw.z, zw.w));
+                    d = __ffma2_rn(A1, make_float2(xy.z, xy.w), d);
+                    d = __ffma2_rn(A0, make_float2(xy.x, xy.y), d);
+                    m |= (d.x <= thr) ? (1u << s0) : 0u;
+                    m |= (d.y <= thr) ? (2u << s0) : 0u;
                 }
                 const int self = i - base - part * G;
                 if (self >= 0 && self < G) m &= ~(1u << self);
@@ -646,7 +703,7 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
                     while (w) {
                         const int s0 = __ffs(w) - 1;
                         w &= w - 1;
-                        const float4 pp = tl.p[part * G + s0];
+                        const float4 pp = tile_get(tl, part * G + s0);
                         const float4 pj = make_float4(pp.x, pp.y, pp.z, __int_as_float(tl.t[part * G + s0]));
                         const float q0 = pj.x - pi.x, q1 = pj.y - pi.y, q2 = pj.z - pi.z;
                         if (fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) <= cut2)
@@ -713,15 +770,17 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
     }
 }
 
-template <bool ST>
-__global__ void __launch_bounds__(8 * kWarp, 3) k_build_list32(DevParams P, DevParams32 Q, DevState S, int *dB, float rc2,
-                                                            int split)
+// WPB warps per block, MINB resident blocks per SM requested from the
+// register allocator (the launch variants of dmph_autotune_list_build)
+template <bool ST, int WPB, int MINB>
+__global__ void __launch_bounds__(WPB * kWarp, MINB) k_build_list32(DevParams P, DevParams32 Q, DevState S, int *dB,
+                                                                   float rc2, int split)
 {
-    __shared__ TileL tiles[8];
+    __shared__ TileL tiles[WPB];
     TileL &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     if (blockIdx.x == 0 && threadIdx.x == 0) dB[B_LIST_SPLIT] = split;
-    FOR_EACH_CHUNK(dB, CR_WET, 8, cidx)
+    FOR_EACH_CHUNK(dB, CR_WET, WPB, cidx)
     {
         const int n = S.chunks[cidx].cnt;
         if (n <= 8) build_list32_chunk<ST, 4>(P, Q, S, dB, rc2, split, tl, lane, cidx);
@@ -1263,32 +1322,49 @@ __global__ void k_import32(DevParams P, DevState S, const double *pos, const dou
 // spacings.  Before the substeps, the solids' FP32 fluid forces seed the FP64
 // force planes; after them, the FP32 positions and velocities of the solids
 // are refreshed from the masters.
+__device__ __forceinline__ void solid_force_to64_slot(const DevParams &P, const DevState &S, int i)
+{
+    const float4 f = S.f4[i];
+    S.frc[i] = f.x;
+    S.frc[P.N + i] = f.y;
+    S.frc[2 * P.N + i] = f.z;
+}
+__device__ __forceinline__ void sync_solid32_slot(const DevParams &P, const DevState &S, int i)
+{
+    const int N = P.N;
+    const float4 p = S.p4[i];
+    const unsigned w = __float_as_uint(p.w);
+    const int c[3] = {unpack_cx(w), unpack_cy(w), unpack_cz(w)};
+    float r[3];
+    for (int d = 0; d < 3; d++) {
+        double a = S.pos[d * N + i] - (P.dmin[d] + c[d] * P.cw[d]);
+        a -= P.W[d] * rint(a / P.W[d]);
+        r[d] = (float)a;
+    }
+    S.p4[i] = make_float4(r[0], r[1], r[2], p.w);
+    S.v4[i] = make_float4((float)S.vel[i], (float)S.vel[N + i], (float)S.vel[2 * N + i], 0.f);
+}
 __global__ void k_solid_force_to64(DevParams P, DevState S, const int *dB)
 {
-    FOR_EACH_SLOT(dB, B_SB, B_SE, i)
-    {
-        const float4 f = S.f4[i];
-        S.frc[i] = f.x;
-        S.frc[P.N + i] = f.y;
-        S.frc[2 * P.N + i] = f.z;
-    }
+    FOR_EACH_SLOT(dB, B_SB, B_SE, i) solid_force_to64_slot(P, S, i);
 }
 __global__ void k_sync_solids32(DevParams P, DevState S, const int *dB)
 {
-    const int N = P.N;
-    FOR_EACH_SLOT(dB, B_SB, B_SE, i)
-    {
-        const float4 p = S.p4[i];
-        const unsigned w = __float_as_uint(p.w);
-        const int c[3] = {unpack_cx(w), unpack_cy(w), unpack_cz(w)};
-        float r[3];
-        for (int d = 0; d < 3; d++) {
-            double a = S.pos[d * N + i] - (P.dmin[d] + c[d] * P.cw[d]);
-            a -= P.W[d] * rint(a / P.W[d]);
-            r[d] = (float)a;
-        }
-        S.p4[i] = make_float4(r[0], r[1], r[2], p.w);
-        S.v4[i] = make_float4((float)S.vel[i], (float)S.vel[N + i], (float)S.vel[2 * N + i], 0.f);
+    FOR_EACH_SLOT(dB, B_SB, B_SE, i) sync_solid32_slot(P, S, i);
+}
+// the same over every scene of an ensemble, one launch each
+__global__ void k_ens_solid_force_to64(const EnsScene *__restrict__ tab, int ns)
+{
+    for (int k = 0; k < ns; ++k) {
+        const EnsScene &e = tab[k];
+        FOR_EACH_SLOT(e.dB, B_SB, B_SE, i) solid_force_to64_slot(e.P, e.S, i);
+    }
+}
+__global__ void k_ens_sync_solids32(const EnsScene *__restrict__ tab, int ns)
+{
+    for (int k = 0; k < ns; ++k) {
+        const EnsScene &e = tab[k];
+        FOR_EACH_SLOT(e.dB, B_SB, B_SE, i) sync_solid32_slot(e.P, e.S, i);
     }
 }
 void launch_solid_force_to64(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
@@ -1298,6 +1374,18 @@ void launch_solid_force_to64(const DevParams &P, const DevState &S, const int *d
 void launch_sync_solids32(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
 {
     k_sync_solids32<<<148, 256, 0, st>>>(P, S, dB);
+}
+void launch_ens_drift32(const EnsScene *tab, int ns, int sms, cudaStream_t st)
+{
+    k_ens_drift32<<<sms * 8, 256, 0, st>>>(tab, ns);
+}
+void launch_ens_solid_force_to64(const EnsScene *tab, int ns, cudaStream_t st)
+{
+    k_ens_solid_force_to64<<<148, 256, 0, st>>>(tab, ns);
+}
+void launch_ens_sync_solids32(const EnsScene *tab, int ns, cudaStream_t st)
+{
+    k_ens_sync_solids32<<<148, 256, 0, st>>>(tab, ns);
 }
 
 // The lattice sum N0p (initializeWeight :1078-1119) evaluated with exactly
@@ -1469,18 +1557,30 @@ void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S
 #undef DMPH_LAUNCH_B
 }
 
+// launch variants of the list build: warps per block x requested resident
+// blocks per SM (8 x 3 at 80 registers; 8 x 4 and 4 x 8 at 64)
+#define DMPH_BUILD_VARIANTS(X) X(0, 8, 3) X(1, 8, 4) X(2, 4, 8)
+
 void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, int split,
-                         cudaStream_t st)
+                         cudaStream_t st, int variant)
 {
     cudaMemsetAsync(dB + B_LIST_OVF, 0, sizeof(int), st);
     cudaMemsetAsync(S.nbn, 0xFF, sizeof(int) * (size_t)P.N, st);
-    if (P.surface_tension) {
-        static const int g = grid_for(k_build_list32<true>, 8 * kWarp);
-        k_build_list32<true><<<g, 8 * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2, split);
-    } else {
-        static const int g = grid_for(k_build_list32<false>, 8 * kWarp);
-        k_build_list32<false><<<g, 8 * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2, split);
+#define DMPH_LAUNCH_BUILD(ID, WPB, MINB)                                                              \
+    case ID:                                                                                          \
+        if (P.surface_tension) {                                                                      \
+            static const int g = grid_for(k_build_list32<true, WPB, MINB>, WPB * kWarp);              \
+            k_build_list32<true, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2, split);   \
+        } else {                                                                                      \
+            static const int g = grid_for(k_build_list32<false, WPB, MINB>, WPB * kWarp);             \
+            k_build_list32<false, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2, split);  \
+        }                                                                                             \
+        break;
+    switch (variant) {
+        DMPH_BUILD_VARIANTS(DMPH_LAUNCH_BUILD)
+    default: break;
     }
+#undef DMPH_LAUNCH_BUILD
 }
 
 void launch_list_wall_guard(int *dB, cudaStream_t st)

@@ -70,7 +70,8 @@ void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S
 void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
                      cudaStream_t st, int gate = 0);
 void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, int split,
-                         cudaStream_t st);
+                         cudaStream_t st, int variant = 0);
+constexpr int kBuildVariants = 3;  // launch variants of the FP32 list build
 void launch_list_wall_guard(int *dB, cudaStream_t st);
 void launch_pass_a32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
                           cudaStream_t st);
@@ -97,6 +98,13 @@ void launch_widen_f4(const float4 *in, double *out, int count, int stride, cudaS
 void launch_slot_of_row(const DevParams &P, const int *pidx, int *slot_of_row, cudaStream_t st);
 void launch_clump_dem(const DevParams &P, const DevState &S, const int *dB, bool lists, cudaStream_t st);
 void launch_body_step(const DevParams &P, const DevState &S, const DevBodies &Bd, bool f32, cudaStream_t st);
+// ensemble-wide launches (one per step part over every scene of the table)
+void launch_ens_clump_dem(const EnsScene *tab, int ns, int sub, cudaStream_t st);  // 2 kernels
+void launch_ens_body_step(const EnsScene *tab, int ns, const int *bpre, int total_bodies, int sub, cudaStream_t st);
+void launch_ens_drift32(const EnsScene *tab, int ns, int sms, cudaStream_t st);
+void launch_ens_decide(const EnsScene *tab, int ns, const unsigned long long *handles, cudaStream_t st);
+void launch_ens_solid_force_to64(const EnsScene *tab, int ns, cudaStream_t st);
+void launch_ens_sync_solids32(const EnsScene *tab, int ns, cudaStream_t st);
 
 void launch_xyz_to_planes(const double *xyz, double *planes, int n, cudaStream_t st);
 void launch_planes_to_xyz(const double *planes, double *xyz, int n, cudaStream_t st);

@@ -520,6 +520,25 @@ __global__ void k_decide_graph(const unsigned long long *maxshift, double thresh
     cudaGraphSetConditional(cond, need ? 1u : 0u);
 }
 
+// The decisions of every scene of an ensemble (thread k: scene k), with the
+// threshold of launch_decide; in a graph each scene's IF node gets its
+// condition (handles[k]).  The accumulator is cleared for the next drift.
+__global__ void k_ens_decide(const EnsScene *__restrict__ tab, int ns, const unsigned long long *handles)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ns) return;
+    const EnsScene &e = tab[k];
+    const double margin = (0.1 * e.P.dx);
+    const double thr = 0.5 * margin * 0.5 * margin;  // :1278
+    const int need = decide(e.maxshift, thr, e.dB);
+    if (handles) cudaGraphSetConditional((cudaGraphConditionalHandle)handles[k], need ? 1u : 0u);
+    *e.maxshift = 0ull;
+}
+void launch_ens_decide(const EnsScene *tab, int ns, const unsigned long long *handles, cudaStream_t st)
+{
+    k_ens_decide<<<(ns + 63) / 64, 64, 0, st>>>(tab, ns, handles);
+}
+
 void launch_decide(const DevParams &P, const unsigned long long *maxshift, int *dB, unsigned long long graph_cond,
                    cudaStream_t st)
 {

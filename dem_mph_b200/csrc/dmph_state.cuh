@@ -192,7 +192,39 @@ struct EnsScene {
     DevParams P;
     DevParams32 Q;
     DevState S;
-    const int *dB;
+    int *dB;
+    unsigned long long *maxshift;  // the scene's max-shift accumulator (drift -> decision)
+    DevBodies Bd;                  // its rigid bodies (B = 0: none)
+    int demSteps;                  // DEM substeps per step of the scene
 };
+
+#ifdef __CUDACC__
+// Block-wide exclusive prefix of a per-scene count over the scene table:
+// pre[k] = sum of count(j) for j < k, pre[ns] the total (in shared memory,
+// kMaxEnsemble + 1 entries); every thread of the block must call it.
+template <class Count>
+__device__ __forceinline__ int ens_count_prefix(int ns, int *pre, Count count)
+{
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) pre[k + 1] = count(k);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        pre[0] = 0;
+        for (int k = 0; k < ns; ++k) pre[k + 1] += pre[k];
+    }
+    __syncthreads();
+    return pre[ns];
+}
+// the scene k with pre[k] <= g < pre[k + 1] (pre ascending)
+__device__ __forceinline__ int ens_scene_at(const int *pre, int ns, int g)
+{
+    int lo = 0, hi = ns - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+#endif
 
 }  // namespace dmph

@@ -211,32 +211,59 @@ def small(seed=7, dx=0.02, n_debris=3, yaw=False):
                      debris_x=(0.35, 0.95), yaw=yaw, seed=seed, name="small_dambreak_3d")
 
 
-def config3(seed=1234, n_scenes=64):
+def _dam_break_particles(nh, nw, nl=3):
+    """particle count of a config-3 scene before debris: column nh x nh x nw,
+    tank 3 nh x 1.2 nh x nw (in particles), nl wall layers (floor with
+    corners, x walls over the full z extent, z walls)"""
+    nx, ny = int(round(3.0 * nh)), int(round(1.2 * nh))
+    walls = (nx + 2 * nl) * nl * (nw + 2 * nl) + 2 * nl * ny * (nw + 2 * nl) + 2 * nx * ny * nl
+    return nh * nh * nw + walls
+
+
+def config3(seed=1234, n_scenes=64, n_range=(20000, 300000), debris_range=(5, 50)):
     """Config 3: an ensemble of independent dam breaks with seeded column
-    height H in [0.2, 0.6] m, spacing dx in [5, 10] mm (0.25 mm steps) and
-    up to 50 debris bodies each (as many as a quarter of the downstream floor
-    holds).  The column is H x H x W with W drawn for 6k-80k fluid particles;
-    tank 3H x 1.2H x W.  At the default seed the 64 scenes hold 33k-405k
-    particles each with walls and debris, 9.0 M in total, and 309 bodies."""
+    height H in [0.2, 0.6] m and spacing dx in [5, 10] mm (0.25 mm steps);
+    a particle count (walls and debris included) drawn log-uniformly between
+    20k (or the smallest tank of that column) and 300k; 5 to 50 debris bodies
+    (cuboids of 3 to 4 particles a side, densities 400-900 kg/m^3, seeded
+    yaw), drawn uniformly in [5, 50] and clipped to what 40% of the
+    downstream half of the floor holds.  The column is H x H x W with W chosen for the drawn
+    particle count (widened when fewer than 5 debris would fit); tank
+    3H x 1.2H x W.  A draw that leaves the particle range is drawn again."""
     rng = np.random.default_rng(seed)
     out = []
-    for k in range(n_scenes):
+    side_hi = 4
+    foot = (1.5 * side_hi + 2) ** 2  # yawed footprint with clearance, in dx^2
+    while len(out) < n_scenes:
+        k = len(out)
         H = float(rng.uniform(0.2, 0.6))
         dx = float(rng.uniform(0.005, 0.010))
         dx = round(dx * 4000.0) / 4000.0  # 0.25 mm steps
-        n_f = float(np.exp(rng.uniform(np.log(6e3), np.log(80e3))))
+        u_n, u_deb = float(rng.uniform(0.0, 1.0)), float(rng.uniform(0.0, 1.0))
+        sub_seed = int(rng.integers(1 << 30))
         nh = max(8, int(round(H / dx)))
-        nw = int(np.clip(round(n_f / (nh * nh)), 10, 400))
-        H = nh * dx
-        W = nw * dx
-        n_deb = int(rng.integers(5, 51))
-        # debris no wider than the tank allows, and no more than a third of
-        # the downstream floor can hold
-        side_hi = max(3, min(6, nw // 4))
-        fit = int(0.5 * 3.0 * H * W / ((1.5 * side_hi + 2) * dx) ** 2 / 4.0)
-        n_deb = max(1, min(n_deb, fit))
-        out.append(dam_break(dx=dx, tank=(3.0 * H, 1.2 * H, W), column=(H, H, W), n_debris=n_deb,
-                             debris_sides=((3, side_hi), (3, side_hi), (3, side_hi)),
-                             debris_density=(400.0, 900.0), debris_x=(0.45, 0.95), yaw=True,
-                             seed=int(rng.integers(1 << 30)), name="config3_scene%02d" % k))
+        n_min = max(n_range[0], _dam_break_particles(nh, 10))
+        if n_min >= n_range[1]:
+            continue
+        target = float(np.exp(np.log(n_min) + u_n * (np.log(n_range[1]) - np.log(n_min))))
+        nw = 10
+        while nw < 2000 and _dam_break_particles(nh, nw + 1) <= target:
+            nw += 1
+
+        def fit(w):
+            return int(0.4 * 0.5 * 3.0 * nh * w / foot)
+        while fit(nw) < debris_range[0] and nw < 2000:
+            nw += 1
+        # uniform in the range, clipped to what the floor holds
+        n_deb = debris_range[0] + int(u_deb * (debris_range[1] - debris_range[0] + 1))
+        n_deb = min(n_deb, debris_range[1], fit(nw))
+        try:
+            sc = dam_break(dx=dx, tank=(3.0 * nh * dx, 1.2 * nh * dx, nw * dx), column=(nh * dx, nh * dx, nw * dx),
+                           n_debris=n_deb, debris_sides=((3, side_hi), (3, side_hi), (3, side_hi)),
+                           debris_density=(400.0, 900.0), debris_x=(0.45, 0.95), yaw=True, seed=sub_seed,
+                           name="config3_scene%02d" % k)
+        except ValueError:
+            continue
+        if n_range[0] <= sc.n <= n_range[1]:
+            out.append(sc)
     return out

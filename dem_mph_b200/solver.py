@@ -49,6 +49,7 @@ def lib():
         L.dmph_get_phase_times.argtypes = [vp, vp, vp, C.c_int]
         L.dmph_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp, vp]
         L.dmph_set_variants.argtypes = [vp, C.c_int, C.c_int]
+        L.dmph_autotune_list_build.argtypes = [vp, C.c_int, C.POINTER(C.c_int), vp]
         L.dmph_ensemble_create.argtypes = [vp, C.c_int, C.POINTER(vp)]
         L.dmph_ensemble_step.argtypes = [vp, C.c_int]
         L.dmph_ensemble_step_timed.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
@@ -122,6 +123,7 @@ def bodies_from_contacts(params, typ, x):
 
 PASS_VARIANTS = 5  # DMPH_PASS_VARIANTS (stencil passes)
 LIST_VARIANTS = 4  # DMPH_LIST_VARIANTS (Verlet-list passes, the FP32 default)
+BUILD_VARIANTS = 3  # DMPH_BUILD_VARIANTS (FP32 list build)
 
 
 class DmphError(RuntimeError):
@@ -251,6 +253,15 @@ class Solver:
         mb = np.zeros(PASS_VARIANTS, np.float32)
         self._check(lib().dmph_autotune(self._h, C.byref(a), C.byref(b), _ptr(ma), _ptr(mb)))
         return a.value, b.value, ma, mb
+
+    def autotune_list_build(self, steps_per_variant=10):
+        """(chosen variant, mean list-build ms per variant) of the FP32 list
+        build's launch variants, timed over real rebuilds while stepping
+        (dmph_autotune_list_build; advances 3 x steps_per_variant steps)."""
+        v = C.c_int()
+        ms = np.zeros(BUILD_VARIANTS, np.float32)
+        self._check(lib().dmph_autotune_list_build(self._h, steps_per_variant, C.byref(v), _ptr(ms)))
+        return v.value, ms
 
     def set_variants(self, variant_a, variant_b):
         self._check(lib().dmph_set_variants(self._h, variant_a, variant_b))

@@ -343,6 +343,17 @@ int dmph_set_graph(dmph_ctx *ctx, int enable);
 int dmph_autotune(dmph_ctx *ctx, int *variant_a, int *variant_b, float *ms_a, float *ms_b);
 int dmph_set_variants(dmph_ctx *ctx, int variant_a, int variant_b);
 
+/* Autotuner of the FP32 list build (Verlet-list mode): advances
+ * steps_per_variant steps with each of DMPH_BUILD_VARIANTS launch variants of
+ * the list build (warps per block x resident blocks per SM) and the phase
+ * timer on, and keeps the variant whose rebuilds' list build was fastest.
+ * All variants build the same lists, so the steps are ordinary steps; ms[v]
+ * (optional) gets variant v's mean list-build time, -1 when its steps had no
+ * rebuild.  Runs without graph replay; the setting of dmph_set_graph holds
+ * again afterwards. */
+#define DMPH_BUILD_VARIANTS 3
+int dmph_autotune_list_build(dmph_ctx *ctx, int steps_per_variant, int *variant, float *ms);
+
 /* Ensemble of independent scenes (no counterpart in the reference, which runs
  * one scene per process).  Every scene keeps its own context, parameters,
  * cell grid and state; an ensemble step advances all of them by one step:

@@ -13,11 +13,18 @@ from dem_mph_b200.abi import PRECISION_FP32_SPLIT
 pytestmark = pytest.mark.gpu
 
 
-def scene_list():
+MIXED = ((7, 0.02, 3, False, False), (8, 0.025, 2, True, False), (9, 0.018, 4, True, False),
+         (10, 0.03, 1, False, True))
+# every scene with rigid bodies or without debris: the ensemble runs its
+# drifts, decisions and DEM tails as ensemble-wide launches
+RIGID = ((7, 0.02, 3, True, False), (8, 0.025, 2, True, False), (9, 0.018, 4, True, False),
+         (10, 0.03, 0, False, True))
+
+
+def scene_list(kinds=MIXED):
     """uneven scenes: sizes, debris counts, rigid bodies on/off, surface tension on/off"""
     out = []
-    for seed, dx, nd, bodies, st in ((7, 0.02, 3, False, False), (8, 0.025, 2, True, False),
-                                     (9, 0.018, 4, True, False), (10, 0.03, 1, False, True)):
+    for seed, dx, nd, bodies, st in kinds:
         s = scenes.small(seed=seed, dx=dx, n_debris=nd)
         p = s.params.copy()
         if st:
@@ -44,9 +51,11 @@ def same_state(a, b):
             and np.array_equal(va, vb) and np.array_equal(a.field("PressureP"), b.field("PressureP")))
 
 
-@pytest.mark.parametrize("graph,mode", [(True, "list"), (False, "list"), (True, "stencil")])
-def test_ensemble_matches_scenes_stepped_alone(graph, mode):
-    items = scene_list()
+@pytest.mark.parametrize("graph,mode,kinds", [(True, "list", "mixed"), (False, "list", "mixed"),
+                                              (True, "stencil", "mixed"), (True, "list", "rigid"),
+                                              (False, "list", "rigid")])
+def test_ensemble_matches_scenes_stepped_alone(graph, mode, kinds):
+    items = scene_list(RIGID if kinds == "rigid" else MIXED)
     alone = make(items)
     members = make(items)
     for g in alone + members:
@@ -54,7 +63,8 @@ def test_ensemble_matches_scenes_stepped_alone(graph, mode):
     ens = solver.Ensemble(members)
     ens.set_graph(graph)
     assert len({g.n for g in members}) == len(members)  # uneven sizes
-    for steps in (1, 9, 50):
+    chunks = (1, 9, 50, 140) if kinds == "rigid" else (1, 9, 50)  # rigid bodies rebuild less often
+    for steps in chunks:
         for g in alone:
             g.step(steps)
         ens.step(steps)
@@ -65,7 +75,12 @@ def test_ensemble_matches_scenes_stepped_alone(graph, mode):
                 ba, bb = a.bodies(), b.bodies()
                 assert all(np.array_equal(ba[q], bb[q]) for q in ("X", "V", "q", "L")), k
     assert sum(g.info().rebuilds for g in members) > len(members)
-    assert ens.info()["steps"] == 60
+    assert ens.info()["steps"] == sum(chunks)
+    if kinds == "rigid" and graph:
+        # fused: per recorded step, 2 head + 6 list-pass + 2 + 3 per DEM substep launches
+        l0 = ens.info()["kernel_launches"]
+        ens.step(4)
+        assert ens.info()["kernel_launches"] - l0 == 4 * (2 + 6 + 2 + 3 * 2)
     ens.close()
     for g in alone + members:
         g.close()

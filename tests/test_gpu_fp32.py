@@ -342,3 +342,29 @@ def test_walls_at_rest_keep_their_slots():
     t1, x1, _, id1 = g.state()
     assert np.array_equal(id1[walls], id0[walls]) and np.array_equal(t1[walls], t0[walls])
     g.close()
+
+
+def test_list_build_variants_change_no_result():
+    """the list-build autotuner steps the scene with each launch variant of
+    the list build; the states and fields must equal, bit for bit, those of
+    the same steps with the default variant"""
+    p, typ, x, v = load_scene("small3d")
+    p.precision = PRECISION_FP32_SPLIT
+    a, b = solver.Solver(p, typ, x, v), solver.Solver(p, typ, x, v)
+    a.step(150)
+    b.step(150)
+    r0 = a.info().rebuilds
+    va, ms = a.autotune_list_build(15)
+    b.step(45)
+    assert a.info().rebuilds - r0 >= 2 and np.sum(ms >= 0) >= 2, (a.info().rebuilds - r0, ms)
+    a.set_graph(True)
+    b.set_graph(True)
+    a.step(30)
+    b.step(30)
+    sa, sb = a.state(), b.state()
+    for u, w in zip(sa, sb):
+        assert np.array_equal(u, w)
+    for f in ("Force", "PressureP", "VolStrainP"):
+        assert np.array_equal(a.field(f), b.field(f)), f
+    a.close()
+    b.close()
