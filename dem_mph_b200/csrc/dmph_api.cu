@@ -730,6 +730,145 @@ extern "C" int dmph_set_state(dmph_ctx *ctx, const double *x3, const double *v3)
     return DMPH_OK;
 }
 
+// ---- split steps and row-level state (domain decomposition over ranks)
+
+// B_NEED of a step whose rebuild the caller decided (dmph_step_finish)
+__global__ void k_set_need(int *dB, int need)
+{
+    dB[B_NEED] = need;
+    dB[B_REBUILDS] += need;
+}
+
+extern "C" int dmph_step_begin(dmph_ctx *ctx, double *max_shift2)
+{
+    if (!ctx) return DMPH_EINVAL;
+    if (ctx->in_split_step) {
+        ctx->err = "dmph_step_begin: the previous step was not finished";
+        return DMPH_EINVAL;
+    }
+    drop_graph(ctx);  // split steps run as individual launches
+    ctx->Wm.moving = in_wall_window(ctx) ? 1 : 0;
+    const DevParams &P = ctx->P;
+    CK(cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), ctx->st));
+    if (ctx->fp32)
+        launch_drift32(P, ctx->Q, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, ctx->st);
+    else
+        launch_drift(P, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, ctx->st);
+    CK(cudaMemcpyAsync(ctx->h_maxshift, ctx->maxshift, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->launches += 1;
+    double m2;
+    std::memcpy(&m2, ctx->h_maxshift, sizeof(double));
+    ctx->split_m2 = m2;
+    ctx->in_split_step = true;
+    if (max_shift2) *max_shift2 = m2;
+    return DMPH_OK;
+}
+
+extern "C" int dmph_step_finish(dmph_ctx *ctx, int rebuild)
+{
+    if (!ctx) return DMPH_EINVAL;
+    // a context that has not stepped yet may finish the step whose drift ran
+    // before it was created (its creation made the rebuild of that step)
+    const bool fresh = ctx->steps == 0 && !ctx->in_split_step;
+    if (!ctx->in_split_step && !fresh) {
+        ctx->err = "dmph_step_finish: no step begun";
+        return DMPH_EINVAL;
+    }
+    if (fresh) {
+        if (rebuild) {
+            ctx->err = "dmph_step_finish: a new context's first step has had its rebuild";
+            return DMPH_EINVAL;
+        }
+        drop_graph(ctx);
+        ctx->Wm.moving = in_wall_window(ctx) ? 1 : 0;
+        ctx->split_m2 = 0.0;
+    }
+    ctx->in_split_step = false;
+    if (!std::isfinite(ctx->split_m2)) {
+        // positions become cell indices in the rebuild: never from non-finite ones
+        ctx->nonfinite = true;
+        CK(cudaMemsetAsync(ctx->dB + B_NONFINITE, 0xFF, sizeof(int), ctx->st));
+        return check_finite(ctx);
+    }
+    k_set_need<<<1, 1, 0, ctx->st>>>(ctx->dB, rebuild ? 1 : 0);
+    ctx->launches += 1;
+    if (rebuild) {
+        enqueue_rebuild(ctx, false, ctx->st);
+        ctx->launches += rebuild_launches(ctx, false);
+        ctx->host_rebuilds++;
+    }
+    enqueue_tail(ctx, ctx->st);
+    ctx->launches += tail_launches(ctx);
+    CK(cudaGetLastError());
+    advance_host_clock(ctx);
+    CK(cudaStreamSynchronize(ctx->st));
+    return check_finite(ctx);
+}
+
+__global__ void k_rows_io(DevParams P, double *pos, double *vel, const int *__restrict__ slot_of_row,
+                          const int *__restrict__ rows, int count, double *x3, double *v3, int set)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int r = rows[k];
+    if (r < 0 || r >= P.N) return;  // rejected on the host
+    const int i = slot_of_row[r];
+    for (int d = 0; d < 3; d++) {
+        if (set) {
+            if (x3) pos[d * P.N + i] = x3[3 * k + d];
+            if (v3) vel[d * P.N + i] = v3[3 * k + d];
+        } else {
+            if (x3) x3[3 * k + d] = pos[d * P.N + i];
+            if (v3) v3[3 * k + d] = vel[d * P.N + i];
+        }
+    }
+}
+
+// positions / velocities of input rows through the FP64 planes (exported
+// from and imported into the FP32 state in the split build)
+static int rows_io(dmph_ctx *ctx, int count, const int *rows, double *x3, double *v3, bool set)
+{
+    if (!ctx || count < 0 || (count > 0 && !rows)) return DMPH_EINVAL;
+    const int N = ctx->P.N;
+    if (count > N) return ctx->err = "more rows than particles", DMPH_ERANGE;
+    for (int k = 0; k < count; k++)
+        if (rows[k] < 0 || rows[k] >= N) return ctx->err = "row outside the grid", DMPH_ERANGE;
+    if (count == 0) return DMPH_OK;
+    const DevState &S = ctx->S;
+    // scratch free between steps: flag (rows), offs (slot of each row),
+    // pos2 / vel2 (the values)
+    CK(cudaMemcpyAsync(ctx->flag, rows, sizeof(int) * count, cudaMemcpyHostToDevice, ctx->st));
+    launch_slot_of_row(ctx->P, S.pidx, ctx->offs, ctx->st);
+    if (ctx->fp32) launch_export32(ctx->P, S, S.pos, S.vel, ctx->st);
+    if (set) {
+        if (x3) CK(cudaMemcpyAsync(ctx->pos2, x3, sizeof(double) * 3 * count, cudaMemcpyHostToDevice, ctx->st));
+        if (v3) CK(cudaMemcpyAsync(ctx->vel2, v3, sizeof(double) * 3 * count, cudaMemcpyHostToDevice, ctx->st));
+    }
+    k_rows_io<<<(count + 255) / 256, 256, 0, ctx->st>>>(ctx->P, S.pos, S.vel, ctx->offs, ctx->flag, count,
+                                                         x3 ? ctx->pos2 : nullptr, v3 ? ctx->vel2 : nullptr,
+                                                         set ? 1 : 0);
+    if (set && ctx->fp32) launch_import32(ctx->P, S, S.pos, S.vel, ctx->st);
+    if (!set) {
+        if (x3) CK(cudaMemcpyAsync(x3, ctx->pos2, sizeof(double) * 3 * count, cudaMemcpyDeviceToHost, ctx->st));
+        if (v3) CK(cudaMemcpyAsync(v3, ctx->vel2, sizeof(double) * 3 * count, cudaMemcpyDeviceToHost, ctx->st));
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->st));
+    return DMPH_OK;
+}
+
+extern "C" int dmph_get_rows(dmph_ctx *ctx, int count, const int *rows, double *x3, double *v3)
+{
+    return rows_io(ctx, count, rows, x3, v3, false);
+}
+
+extern "C" int dmph_set_rows(dmph_ctx *ctx, int count, const int *rows, const double *x3, const double *v3)
+{
+    return rows_io(ctx, count, rows, const_cast<double *>(x3), const_cast<double *>(v3), true);
+}
+
 extern "C" int dmph_get_field(dmph_ctx *ctx, int field_id, void *out)
 {
     if (!ctx || !out) return DMPH_EINVAL;

@@ -69,6 +69,8 @@ struct dmph_ctx {
     bool all_counts = false;
     bool prof = false;
     bool nonfinite = false;  // a step met a non-finite position or velocity (until dmph_set_state)
+    bool in_split_step = false;  // dmph_step_begin ran, dmph_step_finish not yet
+    double split_m2 = 0.0;       // the max shift dmph_step_begin reported
     cudaEvent_t pe0 = nullptr, pe1 = nullptr, pl0 = nullptr, pl1 = nullptr;
     double phase_ms[DMPH_PHASE_COUNT] = {0};
     long long phase_n[DMPH_PHASE_COUNT] = {0};

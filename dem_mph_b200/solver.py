@@ -35,6 +35,10 @@ def lib():
         L.dmph_step.argtypes = [vp, C.c_int]
         L.dmph_step_timed.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
         L.dmph_get_state.argtypes = [vp, vp, vp, vp, vp]
+        L.dmph_step_begin.argtypes = [vp, C.POINTER(C.c_double)]
+        L.dmph_step_finish.argtypes = [vp, C.c_int]
+        L.dmph_get_rows.argtypes = [vp, C.c_int, vp, vp, vp]
+        L.dmph_set_rows.argtypes = [vp, C.c_int, vp, vp, vp]
         L.dmph_set_state.argtypes = [vp, vp, vp]
         L.dmph_get_field.argtypes = [vp, C.c_int, vp]
         L.dmph_get_info.argtypes = [vp, vp]
@@ -163,6 +167,30 @@ class Solver:
         ms = C.c_float()
         self._check(lib().dmph_step_timed(self._h, n, C.byref(ms)))
         return ms.value
+
+    def step_begin(self):
+        """drift part of one step; the largest squared displacement since the
+        last rebuild (dmph_step_begin)"""
+        m2 = C.c_double()
+        self._check(lib().dmph_step_begin(self._h, C.byref(m2)))
+        return m2.value
+
+    def step_finish(self, rebuild):
+        self._check(lib().dmph_step_finish(self._h, 1 if rebuild else 0))
+
+    def get_rows(self, rows):
+        """(x[k,3], v[k,3]) of input rows"""
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        x = np.empty((len(r), 3))
+        v = np.empty((len(r), 3))
+        self._check(lib().dmph_get_rows(self._h, len(r), _ptr(r), _ptr(x), _ptr(v)))
+        return x, v
+
+    def set_rows(self, rows, x, v):
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        xx = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+        vv = np.ascontiguousarray(v, dtype=np.float64).reshape(-1, 3)
+        self._check(lib().dmph_set_rows(self._h, len(r), _ptr(r), _ptr(xx), _ptr(vv)))
 
     def state(self, out=None):
         """(type, x[N,3], v[N,3], orig_id) in the current sorted order.  `out`

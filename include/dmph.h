@@ -166,6 +166,29 @@ int dmph_step(dmph_ctx *ctx, int nsteps);
  * CUDA events recorded on the context's stream. */
 int dmph_step_timed(dmph_ctx *ctx, int nsteps, float *device_ms);
 
+/* One step split at the rebuild decision, for drivers that decide it over
+ * several contexts (a domain split into slabs, one context per rank: the
+ * reference's trigger, source/DEM-MPH.cpp:1264-1286, is a maximum over all
+ * particles, so the ranks combine their maxima and rebuild together).
+ * dmph_step_begin runs the drift, wall motion, periodic wrap and force reset
+ * of one step (:1860, :2846, :3153, :1894) and reports the largest squared
+ * displacement since the last rebuild (+inf when a position or velocity is
+ * not finite); dmph_step_finish(rebuild) completes the step: the neighbour
+ * rebuild when rebuild != 0 (never on a non-finite state: DMPH_ENAN), the
+ * passes, the fluid update and the DEM substeps.  No graph replay.  On a
+ * context that has not stepped yet, dmph_step_finish(ctx, 0) alone completes
+ * the step whose drift was applied to the state it was created from (its
+ * creation sorted the particles and built the lists: that step's rebuild). */
+int dmph_step_begin(dmph_ctx *ctx, double *max_shift2);
+int dmph_step_finish(dmph_ctx *ctx, int rebuild);
+
+/* Positions and velocities (3 per row, either pointer may be NULL) of the
+ * given input-grid rows (orig_id), read or overwritten; a write takes effect
+ * at the next step (the ghost particles of a slab decomposition are refreshed
+ * this way from the ranks that own them). */
+int dmph_get_rows(dmph_ctx *ctx, int count, const int *rows, double *x3, double *v3);
+int dmph_set_rows(dmph_ctx *ctx, int count, const int *rows, const double *x3, const double *v3);
+
 /* Copy the particle state to host arrays in the solver's current (sorted)
  * order.  Any pointer may be NULL.  orig_id is the reference's ParticleIndex
  * (source/DEM-MPH.cpp:82): the row of the particle in the input grid. */

@@ -898,8 +898,9 @@ static void wall_motion(dmph_oracle *o)
             for (int d = 0; d < 3; d++) o->wallC[k][d] += o->p.wall_velocity[k][d] * dt;
 }
 
-/* neighborCalculation :1264-1286 */
-static int need_rebuild(dmph_oracle *o)
+/* neighborCalculation :1264-1286: the largest squared displacement since the
+ * last rebuild, and the trigger on it */
+static double max_shift2(dmph_oracle *o)
 {
     double m = 0.0;
     for (int i = 0; i < o->N; i++) {
@@ -909,8 +910,9 @@ static int need_rebuild(dmph_oracle *o)
         const double s = d3[0] * d3[0] + d3[1] * d3[1] + d3[2] * d3[2];
         if (s > m) m = s;
     }
-    return m > 0.5 * o->margin * 0.5 * o->margin;
+    return m;
 }
+static int need_rebuild(dmph_oracle *o) { return max_shift2(o) > 0.5 * o->margin * 0.5 * o->margin; }
 
 /* ---- rigid debris bodies (no reference counterpart; the library's
  * DMPH_FLAG_RIGID_CLUMPS mode restated in FP64).  Contact force per pair of
@@ -1059,7 +1061,8 @@ static void body_step(dmph_oracle *o)
 }
 
 /* one iteration of the main loop, :450-579 */
-static void step_once(dmph_oracle *o)
+/* the step before the rebuild decision: drift, walls, wrap, force reset */
+static void step_head(dmph_oracle *o)
 {
     const int N = o->N;
     for (int i = o->fb; i < o->fe; ++i)
@@ -1070,7 +1073,13 @@ static void step_once(dmph_oracle *o)
             o->x[3 * i + d] = pmod(o->x[3 * i + d] - o->p.domain_min[d], o->W[d]) + o->p.domain_min[d];
     memset(o->F, 0, sizeof(double) * 3 * N); /* resetForce :1894 */
     memset(o->fsc, 0, sizeof(double) * N);
-    if (need_rebuild(o)) {
+}
+
+/* the step after the decision: the rebuild when asked for, then the passes,
+ * the fluid update and the DEM substeps */
+static void step_tail(dmph_oracle *o, int rebuild)
+{
+    if (rebuild) {
         cell_sort(o);
         build_neighbors(o);
         o->rebuilds++;
@@ -1100,6 +1109,54 @@ static void step_once(dmph_oracle *o)
     }
     o->time += o->p.dt;
     o->steps++;
+}
+
+static void step_once(dmph_oracle *o)
+{
+    step_head(o);
+    step_tail(o, need_rebuild(o));
+}
+
+int dmph_oracle_step_begin(dmph_oracle *o, double *m2)
+{
+    if (!o) return DMPH_EINVAL;
+    step_head(o);
+    if (m2) *m2 = max_shift2(o);
+    return 0;
+}
+
+int dmph_oracle_step_finish(dmph_oracle *o, int rebuild)
+{
+    if (!o) return DMPH_EINVAL;
+    step_tail(o, rebuild);
+    return 0;
+}
+
+/* positions and velocities of the given input rows (ParticleIndex), read or
+ * written (set != 0) */
+int dmph_oracle_rows(dmph_oracle *o, int count, const int *rows, double *x3, double *v3, int set)
+{
+    if (!o || count < 0 || (count && !rows)) return DMPH_EINVAL;
+    int *slot = xcalloc((size_t)o->N, sizeof(int));
+    for (int i = 0; i < o->N; i++) slot[o->pidx[i]] = i;
+    for (int k = 0; k < count; k++) {
+        if (rows[k] < 0 || rows[k] >= o->N) {
+            free(slot);
+            return DMPH_ERANGE;
+        }
+        const int i = slot[rows[k]];
+        for (int d = 0; d < 3; d++) {
+            if (set) {
+                if (x3) o->x[3 * (size_t)i + d] = x3[3 * k + d];
+                if (v3) o->v[3 * (size_t)i + d] = v3[3 * k + d];
+            } else {
+                if (x3) x3[3 * k + d] = o->x[3 * (size_t)i + d];
+                if (v3) v3[3 * k + d] = o->v[3 * (size_t)i + d];
+            }
+        }
+    }
+    free(slot);
+    return 0;
 }
 
 dmph_oracle *dmph_oracle_create(const dmph_params *p, int n, const int *type, const double *x3, const double *v3)

@@ -40,6 +40,14 @@ int dmph_oracle_pressure_force(dmph_oracle *o, const double *P, double *F);
 int dmph_oracle_set_bodies(dmph_oracle *o, int nbodies, const int *body_of_row, const double *body_density);
 /* X,V,L 3 per body, q 4 per body, M 1 per body (any may be NULL) */
 int dmph_oracle_get_bodies(dmph_oracle *o, double *X, double *V, double *q, double *L, double *M);
+/* one step split at the rebuild decision: begin runs the drift, walls, wrap
+ * and force reset and reports the largest squared displacement since the last
+ * rebuild; finish runs the rebuild when asked for, then the rest of the step */
+int dmph_oracle_step_begin(dmph_oracle *o, double *max_shift2);
+int dmph_oracle_step_finish(dmph_oracle *o, int rebuild);
+/* positions / velocities (either may be NULL) of input rows: set = 0 reads
+ * them into x3, v3 (3 per row), set = 1 writes them */
+int dmph_oracle_rows(dmph_oracle *o, int count, const int *rows, double *x3, double *v3, int set);
 /* the cell sort alone (keys and permutation, n of each), no neighbour build */
 int dmph_oracle_cell_sort(const dmph_params *p, int n, const int *type, const double *x3, int *key, int *perm);
 void dmph_oracle_destroy(dmph_oracle *o);

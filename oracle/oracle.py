@@ -39,6 +39,9 @@ def lib():
         L.dmph_oracle_set_bodies.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.dmph_oracle_get_bodies.argtypes = [C.c_void_p] + [C.c_void_p] * 5
         L.dmph_oracle_pressure_force.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dmph_oracle_step_begin.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.dmph_oracle_step_finish.argtypes = [C.c_void_p, C.c_int]
+        L.dmph_oracle_rows.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.dmph_oracle_cell_sort.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.mlp_oracle_param_count.restype = C.c_int
         L.mlp_oracle_forward.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
@@ -66,6 +69,31 @@ class Oracle:
         rc = lib().dmph_oracle_step(self._h, n)
         if rc != 0:
             raise RuntimeError("dmph_oracle_step failed (%d)" % rc)
+
+    def step_begin(self):
+        """drift, walls, wrap, force reset; returns the largest squared
+        displacement since the last rebuild"""
+        m2 = C.c_double()
+        lib().dmph_oracle_step_begin(self._h, C.byref(m2))
+        return m2.value
+
+    def step_finish(self, rebuild):
+        lib().dmph_oracle_step_finish(self._h, 1 if rebuild else 0)
+
+    def get_rows(self, rows):
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        x = np.empty((len(r), 3))
+        v = np.empty((len(r), 3))
+        if lib().dmph_oracle_rows(self._h, len(r), r.ctypes.data, x.ctypes.data, v.ctypes.data, 0) != 0:
+            raise ValueError("row out of range")
+        return x, v
+
+    def set_rows(self, rows, x, v):
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        xx = np.ascontiguousarray(x, dtype=np.float64)
+        vv = np.ascontiguousarray(v, dtype=np.float64)
+        if lib().dmph_oracle_rows(self._h, len(r), r.ctypes.data, xx.ctypes.data, vv.ctypes.data, 1) != 0:
+            raise ValueError("row out of range")
 
     def get(self, name):
         L = lib()
