@@ -509,7 +509,7 @@ def run_surrogate(args, rank, world):
     b = make()
     b.enable_surrogate(substeps=K, check_interval=50, tolerance=args.sg_tolerance, fallback_blocks=20,
                        train_iters_per_block=20)
-    settle = max(args.settle, 200)
+    settle = args.settle if "--settle" in sys.argv else SETTLE_DEFAULT.get(wl, 200)
     b.step(settle)
     nb_collect = 480 // K
     b.surrogate_collect(nb_collect)

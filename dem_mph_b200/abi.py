@@ -149,7 +149,7 @@ class SurrogateStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-MLP_IN, MLP_OUT, MLP_FEATURES, MLP_TARGETS = 64, 16, 48, 6
+MLP_IN, MLP_OUT, MLP_FEATURES, MLP_TARGETS = 64, 16, 52, 6
 
 
 def default_params():

@@ -297,8 +297,6 @@ void dmph::advance_host_clock(dmph_ctx *ctx)
 // Record, on a capturing stream, the head of a step followed by an IF node
 // whose body is the rebuild; the decision kernel of the head sets the
 // condition on the device.
-static int capture_rebuild_if(dmph_ctx *ctx, cudaGraphConditionalHandle cond, cudaStream_t st);
-
 static int capture_head_and_rebuild(dmph_ctx *ctx, cudaGraph_t g, cudaStream_t st)
 {
     cudaGraphConditionalHandle cond;
@@ -309,7 +307,7 @@ static int capture_head_and_rebuild(dmph_ctx *ctx, cudaGraph_t g, cudaStream_t s
 
 // On a capturing stream: an IF node after the stream's current work whose
 // body is the scene's rebuild, run when a decision kernel sets `cond`
-static int capture_rebuild_if(dmph_ctx *ctx, cudaGraphConditionalHandle cond, cudaStream_t st)
+int dmph::capture_rebuild_if(dmph_ctx *ctx, cudaGraphConditionalHandle cond, cudaStream_t st)
 {
     cudaStreamCaptureStatus status;
     const cudaGraphNode_t *deps = nullptr;

@@ -103,6 +103,9 @@ long long tail_launches(const dmph_ctx *ctx, bool graph = false);
 void advance_host_clock(dmph_ctx *ctx);
 int step_once(dmph_ctx *ctx);
 int read_bounds(dmph_ctx *ctx, int *b);
+// on a capturing stream: an IF node whose body is the rebuild, run when a
+// decision kernel sets cond
+int capture_rebuild_if(dmph_ctx *ctx, cudaGraphConditionalHandle cond, cudaStream_t st);
 // DMPH_ENAN once a drift has met a non-finite position or velocity
 // (B_NONFINITE; synchronises the stream), else DMPH_OK
 int check_finite(dmph_ctx *ctx);

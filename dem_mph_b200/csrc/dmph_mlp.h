@@ -8,7 +8,7 @@
 namespace dmph {
 
 constexpr int kMlpLayers = 4;
-constexpr int kMlpFeatures = 48;  // features computed per particle
+constexpr int kMlpFeatures = 52;  // features computed per particle
 constexpr int kMlpIn = 64;        // features padded to the K granularity of the weight-gradient GEMM
 constexpr int kMlpHidden = 128;
 constexpr int kMlpTargets = 6;    // velocity increment (3) and position residual (3)

@@ -43,6 +43,7 @@ struct FeatScales {
     float vs, as;
     float K, dt;    // substeps, FP32 time step
     float residual; // 1: the network predicts dv - K dt a0 (a0 = acceleration at the block start)
+    float ts;       // unit of the velocity-increment outputs (an acceleration): |g| / 16
 };
 
 struct Surrogate {
@@ -81,6 +82,12 @@ struct Surrogate {
     int fallback_left = 0;
     int since_check = 0;
     unsigned long long block_seed = 0;
+    // the tail of a surrogate call as one graph: apply the prediction, the
+    // debris substeps, the rebuild decision with the rebuild as an IF node
+    // (recorded at the first call of each dmph_surrogate_advance)
+    cudaGraph_t tail_graph = nullptr;
+    cudaGraphExec_t tail_exec = nullptr;
+    int *h_bad = nullptr;  // pinned
 };
 
 namespace {
@@ -109,11 +116,95 @@ __device__ __forceinline__ float particle_mass32(const DevParams &P, const DevSt
 }
 
 // ------------------------------------------------------------ features
+// one neighbour j of i (pj in the frame of i's cell, .w = type; vj.w =
+// pressure; aj its acceleration) into the feature sums f
+__device__ __forceinline__ void feature_pair(const DevParams32 &Q, const float4 pi, const float4 vi, const float *ai,
+                                             float Pi, const float4 pj, const float4 vj, const float4 aj, float divi,
+                                             float divj, float *f)
+{
+    const int tj = __float_as_int(pj.w);
+    const float q[3] = {pj.x - pi.x, pj.y - pi.y, pj.z - pi.z};
+    const float r = sqrtf(fmaf(q[0], q[0], fmaf(q[1], q[1], q[2] * q[2])));
+    const float ir = r > 0.f ? 1.f / r : 0.f;
+    const float e[3] = {q[0] * ir, q[1] * ir, q[2] * ir};
+    const float a = fmaf(-r, Q.iRP, 1.f);
+    const float w = a * a;
+    const float u[3] = {vj.x - vi.x, vj.y - vi.y, vj.z - vi.z};
+    const int cls = is_fluid(tj) ? 0 : (is_solid(tj) ? 1 : 2);
+    f[11 + cls] += w;
+    for (int d = 0; d < 3; ++d) f[14 + 3 * cls + d] += w * q[d];
+    for (int d = 0; d < 3; ++d) f[23 + d] += w * u[d];
+    f[26] += w * (aj.x - ai[0]);
+    f[27] += w * (aj.y - ai[1]);
+    f[28] += w * (aj.z - ai[2]);
+    f[29] += w * e[0] * e[0];
+    f[30] += w * e[1] * e[1];
+    f[31] += w * e[2] * e[2];
+    f[32] += w * e[0] * e[1];
+    f[33] += w * e[0] * e[2];
+    f[34] += w * e[1] * e[2];
+    const float ue = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
+    f[35] += w * ue;
+    f[36] += w * (e[1] * u[2] - e[2] * u[1]);
+    f[37] += w * (e[2] * u[0] - e[0] * u[2]);
+    f[38] += w * (e[0] * u[1] - e[1] * u[0]);
+    const float dp = vj.w - Pi;
+    f[39] += w * dp;
+    for (int d = 0; d < 3; ++d) f[40 + d] += w * dp * e[d];
+    f[43] += 1.f;
+    if (cls == 2)
+        for (int d = 0; d < 3; ++d) f[44 + d] += w * u[d];
+    f[47] += w * r * Q.iRP;
+    // the spread of the velocity divergence around i: the pressure changes at
+    // the rate K div, so its gradient is what changes i's pressure force over
+    // the coming steps (information two neighbours away)
+    const float dd = divj - divi;
+    f[48] += w * dd;
+    for (int d = 0; d < 3; ++d) f[49 + d] += w * dd * e[d];
+}
+
+// own state, normalisation and the BF16 row of slot i
+__device__ __forceinline__ void feature_finish(const DevParams32 &Q, const DevState &S, const FeatScales &F, int i,
+                                               int ti, const float4 vi, const float *ai, float Pi, float *f,
+                                               __nv_bfloat16 *__restrict__ X, float *__restrict__ X32)
+{
+    f[0] = vi.x * F.inv_vs;
+    f[1] = vi.y * F.inv_vs;
+    f[2] = vi.z * F.inv_vs;
+    f[3] = ai[0] * F.inv_as;
+    f[4] = ai[1] * F.inv_as;
+    f[5] = ai[2] * F.inv_as;
+    f[6] = Pi * F.inv_Ps;
+    f[7] = S.vsp32[i] / Q.N0p;
+    f[8] = S.div32[i] * Q.dx * F.inv_vs;
+    f[9] = is_fluid(ti) ? 1.f : 0.f;
+    f[10] = is_solid(ti) ? 1.f : 0.f;
+    for (int k = 11; k < 14; ++k) f[k] *= F.inv_W0;
+    for (int k = 14; k < 23; ++k) f[k] *= F.inv_W0 * F.inv_dx;
+    for (int k = 23; k < 26; ++k) f[k] *= F.inv_W0 * F.inv_vs;
+    for (int k = 26; k < 29; ++k) f[k] *= F.inv_W0 * F.inv_as;
+    for (int k = 29; k < 35; ++k) f[k] *= F.inv_W0;
+    for (int k = 35; k < 39; ++k) f[k] *= F.inv_W0 * F.inv_vs;
+    for (int k = 39; k < 43; ++k) f[k] *= F.inv_W0 * F.inv_Ps;
+    f[43] *= 0.01f;
+    for (int k = 44; k < 47; ++k) f[k] *= F.inv_W0 * F.inv_vs;
+    f[47] *= F.inv_W0;
+    for (int k = 48; k < 52; ++k) f[k] *= F.inv_W0 * Q.dx * F.inv_vs;
+    __align__(16) __nv_bfloat16 h[kMlpIn];
+    for (int k = 0; k < kMlpIn; ++k) h[k] = __float2bfloat16_rn(k < kMlpFeatures ? f[k] : 0.f);
+    uint4 *dst = reinterpret_cast<uint4 *>(X + (long long)i * kMlpIn);
+    for (int k = 0; k < kMlpIn / 8; ++k) dst[k] = reinterpret_cast<const uint4 *>(h)[k];
+    if (X32)
+        for (int k = 0; k < kMlpFeatures; ++k) X32[(long long)i * kMlpFeatures + k] = f[k];
+}
+
+// the 27-cell walk (stencil mode, and after a list overflow: gate)
 __global__ void __launch_bounds__(kFeatWarps * kWarp) k_features32(DevParams P, DevParams32 Q, DevState S,
                                                                    const int *dB, FeatScales F,
                                                                    __nv_bfloat16 *__restrict__ X,
-                                                                   float *__restrict__ X32)
+                                                                   float *__restrict__ X32, int gate)
 {
+    if (gate && dB[B_LIST_OVF] == 0) return;
     __shared__ TileF tiles[kFeatWarps];
     TileF &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -134,6 +225,7 @@ __global__ void __launch_bounds__(kFeatWarps * kWarp) k_features32(DevParams P, 
         const float4 fi = S.f4[ii];
         const float ai[3] = {fi.x / mi, fi.y / mi, fi.z / mi};
         const float Pi = S.pres32[ii];
+        const float divi = S.div32[ii];
         float f[kMlpFeatures];
 #pragma unroll
         for (int k = 0; k < kMlpFeatures; ++k) f[k] = 0.f;
@@ -154,7 +246,7 @@ __global__ void __launch_bounds__(kFeatWarps * kWarp) k_features32(DevParams P, 
                 tl.v[slot] = vj;
                 const float4 fj = S.f4[j];
                 const float mj = particle_mass32(P, S, j, tj);
-                tl.a[slot] = make_float4(fj.x / mj, fj.y / mj, fj.z / mj, 0.f);
+                tl.a[slot] = make_float4(fj.x / mj, fj.y / mj, fj.z / mj, S.div32[j]);
             },
             [&](int base, int nb) {
                 if (!active) return;
@@ -171,73 +263,56 @@ __global__ void __launch_bounds__(kFeatWarps * kWarp) k_features32(DevParams P, 
                 while (m) {
                     const int s = __ffs(m) - 1;
                     m &= m - 1;
-                    const float4 pj = tl.p[s];
-                    const float4 vj = tl.v[s];
-                    const float4 aj = tl.a[s];
-                    const int tj = __float_as_int(pj.w);
-                    const float q[3] = {pj.x - pi.x, pj.y - pi.y, pj.z - pi.z};
-                    const float r = sqrtf(fmaf(q[0], q[0], fmaf(q[1], q[1], q[2] * q[2])));
-                    const float ir = r > 0.f ? 1.f / r : 0.f;
-                    const float e[3] = {q[0] * ir, q[1] * ir, q[2] * ir};
-                    const float a = fmaf(-r, Q.iRP, 1.f);
-                    const float w = a * a;
-                    const float u[3] = {vj.x - vi.x, vj.y - vi.y, vj.z - vi.z};
-                    const int cls = is_fluid(tj) ? 0 : (is_solid(tj) ? 1 : 2);
-                    f[11 + cls] += w;
-                    for (int d = 0; d < 3; ++d) f[14 + 3 * cls + d] += w * q[d];
-                    for (int d = 0; d < 3; ++d) f[23 + d] += w * u[d];
-                    f[26] += w * (aj.x - ai[0]);
-                    f[27] += w * (aj.y - ai[1]);
-                    f[28] += w * (aj.z - ai[2]);
-                    f[29] += w * e[0] * e[0];
-                    f[30] += w * e[1] * e[1];
-                    f[31] += w * e[2] * e[2];
-                    f[32] += w * e[0] * e[1];
-                    f[33] += w * e[0] * e[2];
-                    f[34] += w * e[1] * e[2];
-                    const float ue = u[0] * e[0] + u[1] * e[1] + u[2] * e[2];
-                    f[35] += w * ue;
-                    f[36] += w * (e[1] * u[2] - e[2] * u[1]);
-                    f[37] += w * (e[2] * u[0] - e[0] * u[2]);
-                    f[38] += w * (e[0] * u[1] - e[1] * u[0]);
-                    const float dp = vj.w - Pi;
-                    f[39] += w * dp;
-                    for (int d = 0; d < 3; ++d) f[40 + d] += w * dp * e[d];
-                    f[43] += 1.f;
-                    if (cls == 2)
-                        for (int d = 0; d < 3; ++d) f[44 + d] += w * u[d];
-                    f[47] += w * r * Q.iRP;
+                    feature_pair(Q, pi, vi, ai, Pi, tl.p[s], tl.v[s], tl.a[s], divi, tl.a[s].w, f);
                 }
             });
         if (!active) continue;
-        // own state and normalisation
-        f[0] = vi.x * F.inv_vs;
-        f[1] = vi.y * F.inv_vs;
-        f[2] = vi.z * F.inv_vs;
-        f[3] = ai[0] * F.inv_as;
-        f[4] = ai[1] * F.inv_as;
-        f[5] = ai[2] * F.inv_as;
-        f[6] = Pi * F.inv_Ps;
-        f[7] = S.vsp32[i] / Q.N0p;
-        f[8] = S.div32[i] * Q.dx * F.inv_vs;
-        f[9] = is_fluid(ti) ? 1.f : 0.f;
-        f[10] = is_solid(ti) ? 1.f : 0.f;
-        for (int k = 11; k < 14; ++k) f[k] *= F.inv_W0;
-        for (int k = 14; k < 23; ++k) f[k] *= F.inv_W0 * F.inv_dx;
-        for (int k = 23; k < 26; ++k) f[k] *= F.inv_W0 * F.inv_vs;
-        for (int k = 26; k < 29; ++k) f[k] *= F.inv_W0 * F.inv_as;
-        for (int k = 29; k < 35; ++k) f[k] *= F.inv_W0;
-        for (int k = 35; k < 39; ++k) f[k] *= F.inv_W0 * F.inv_vs;
-        for (int k = 39; k < 43; ++k) f[k] *= F.inv_W0 * F.inv_Ps;
-        f[43] *= 0.01f;
-        for (int k = 44; k < 47; ++k) f[k] *= F.inv_W0 * F.inv_vs;
-        f[47] *= F.inv_W0;
-        __align__(16) __nv_bfloat16 h[kMlpIn];
-        for (int k = 0; k < kMlpIn; ++k) h[k] = __float2bfloat16_rn(k < kMlpFeatures ? f[k] : 0.f);
-        uint4 *dst = reinterpret_cast<uint4 *>(X + (long long)i * kMlpIn);
-        for (int k = 0; k < kMlpIn / 8; ++k) dst[k] = reinterpret_cast<const uint4 *>(h)[k];
-        if (X32)
-            for (int k = 0; k < kMlpFeatures; ++k) X32[(long long)i * kMlpFeatures + k] = f[k];
+        feature_finish(Q, S, F, i, ti, vi, ai, Pi, f, X, X32);
+    }
+}
+
+// Verlet-list mode: one thread per fluid or debris slot over its list (the
+// particles within the list radius at the last rebuild, ascending slot; their
+// cell offsets in the entries), the pairs within RadiusP taken in list order
+__global__ void __launch_bounds__(256) k_features32_list(DevParams P, DevParams32 Q, DevState S, const int *dB,
+                                                          FeatScales F, __nv_bfloat16 *__restrict__ X,
+                                                          float *__restrict__ X32)
+{
+    if (dB[B_LIST_OVF]) return;
+    const int se = dB[B_SE];
+    const long long ld = P.N;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < se; i += gridDim.x * blockDim.x) {
+        const float4 pi = S.p4[i];
+        const int ti = unpack_type(__float_as_uint(pi.w));
+        if (is_wall(ti)) continue;  // the slots [0, se) are fluid then debris
+        const float4 vi = S.v4[i];
+        const float mi = particle_mass32(P, S, i, ti);
+        const float4 fi = S.f4[i];
+        const float ai[3] = {fi.x / mi, fi.y / mi, fi.z / mi};
+        const float Pi = S.pres32[i];
+        const float divi = S.div32[i];
+        float f[kMlpFeatures];
+#pragma unroll
+        for (int k = 0; k < kMlpFeatures; ++k) f[k] = 0.f;
+        const int cnt = S.nbn[i];
+        for (int k = 0; k < cnt; ++k) {
+            const unsigned e = __ldg(S.nbl + list_index(k, i, ld));
+            const int j = (int)(e & kEntrySlot);
+            const float4 pj = __ldg(S.p4 + j);
+            const int tj = unpack_type(__float_as_uint(pj.w));
+            const float4 pjr = make_float4(fmaf(entry_offset(e, 0), Q.cw[0], pj.x),
+                                           fmaf(entry_offset(e, 1), Q.cw[1], pj.y),
+                                           fmaf(entry_offset(e, 2), Q.cw[2], pj.z), __int_as_float(tj));
+            const float q0 = pjr.x - pi.x, q1 = pjr.y - pi.y, q2 = pjr.z - pi.z;
+            if (!(fmaf(q0, q0, fmaf(q1, q1, q2 * q2)) < Q.RP2)) continue;
+            float4 vj = __ldg(S.v4 + j);
+            vj.w = __ldg(S.pres32 + j);
+            const float4 fj = __ldg(S.f4 + j);
+            const float mj = particle_mass32(P, S, j, tj);
+            feature_pair(Q, pi, vi, ai, Pi, pjr, vj, make_float4(fj.x / mj, fj.y / mj, fj.z / mj, 0.f), divi,
+                         __ldg(S.div32 + j), f);
+        }
+        feature_finish(Q, S, F, i, ti, vi, ai, Pi, f, X, X32);
     }
 }
 
@@ -282,7 +357,7 @@ __device__ __forceinline__ void row_targets(const DevParams &P, const DevState &
                                             const int *inv, int s, float *t, double *dv, double *dx)
 {
     const float4 as0 = a0[s];
-    const double base[3] = {F.residual * as0.x / F.as, F.residual * as0.y / F.as, F.residual * as0.z / F.as};
+    const double base[3] = {F.residual * as0.x / F.ts, F.residual * as0.y / F.ts, F.residual * as0.z / F.ts};
     const int j = inv[orig[s]];
     double x1[3];
     abs_pos(P, S.p4[j], x1);
@@ -295,9 +370,13 @@ __device__ __forceinline__ void row_targets(const DevParams &P, const DevState &
     const double Kdt = (double)F.K * F.dt;
     for (int d = 0; d < 3; ++d) {
         dx[d] = min_image(P, x1[d] - x0[3 * (long long)s + d], d);
-        t[d] = (float)(dv[d] / (Kdt * F.as) - base[d]);
-        const double res = dx[d] - Kdt * v0d[d] - 0.5 * (F.K - 1.0) * F.dt * dv[d];
-        t[3 + d] = (float)(res / (Kdt * Kdt * F.as));
+        // clipped at +-2 g: the few particles that strike a wall within the
+        // block would otherwise dominate the squared loss
+        t[d] = (float)fmin(32.0, fmax(-32.0, dv[d] / (Kdt * F.ts) - base[d]));
+        // the displacement follows from the velocity increment (below); its
+        // remainder is not learned, so that the loss is the increment's alone
+        (void)v0d;
+        t[3 + d] = 0.f;
     }
 }
 
@@ -319,7 +398,7 @@ __global__ void k_record_end(DevParams P, DevState S, const int *dB, FeatScales 
     FOR_EACH_SLOT(dB, -1, B_FE, s)
     {
         const float u = (float)(mix64(seed ^ (unsigned long long)s) >> 40) * (1.f / 16777216.f);
-        if (u * 4294967296.f > (float)keep_threshold * row_weight(F, v0[s])) continue;
+        if (u * 4294967296.f > (float)keep_threshold) continue;  // every fluid row alike
         float t[6];
         double dv[3], dx[3];
         row_targets(P, S, F, v0, a0, x0, orig, inv, s, t, dv, dx);
@@ -351,9 +430,8 @@ __global__ void k_judge(DevParams P, DevState S, const int *dB, FeatScales F, co
         const double ad[3] = {as0.x, as0.y, as0.z};
         const double wgt = row_weight(F, vs);
         for (int d = 0; d < 3; ++d) {
-            const double pdv = ((double)Y[(long long)s * kMlpOut + d] * F.as + F.residual * ad[d]) * Kdt;
-            const double pdx = Kdt * v0d[d] + 0.5 * (F.K - 1.0) * F.dt * pdv +
-                               (double)Y[(long long)s * kMlpOut + 3 + d] * Kdt * Kdt * F.as;
+            const double pdv = ((double)Y[(long long)s * kMlpOut + d] * F.ts + F.residual * ad[d]) * Kdt;
+            const double pdx = Kdt * v0d[d] + 0.5 * (F.K - 1.0) * F.dt * pdv;
             e[0] += wgt * (pdx - dx[d]) * (pdx - dx[d]);
             e[1] += wgt * dx[d] * dx[d];
             e[2] += wgt * (pdv - dv[d]) * (pdv - dv[d]);
@@ -398,12 +476,13 @@ __global__ void k_apply32(DevParams P, DevState S, const int *dB, FeatScales F, 
             ab[1] = f.y / m;
             ab[2] = f.z / m;
         }
-        const float dvx = (y[0] * F.as + ab[0]) * Kdt, dvy = (y[1] * F.as + ab[1]) * Kdt,
-                    dvz = (y[2] * F.as + ab[2]) * Kdt;
-        const float h = 0.5f * (F.K - 1.f) * F.dt, c = Kdt * Kdt * F.as;
-        const float dxx = Kdt * v.x + h * dvx + y[3] * c;
-        const float dxy = Kdt * v.y + h * dvy + y[4] * c;
-        const float dxz = Kdt * v.z + h * dvz + y[5] * c;
+        const float dvx = (y[0] * F.ts + ab[0]) * Kdt, dvy = (y[1] * F.ts + ab[1]) * Kdt,
+                    dvz = (y[2] * F.ts + ab[2]) * Kdt;
+        // K steps of x += v dt with v growing by dv / K a step
+        const float h = 0.5f * (F.K - 1.f) * F.dt;
+        const float dxx = Kdt * v.x + h * dvx;
+        const float dxy = Kdt * v.y + h * dvy;
+        const float dxz = Kdt * v.z + h * dvz;
         if (!(isfinite(dxx) && isfinite(dxy) && isfinite(dxz) && isfinite(dvx) && isfinite(dvy) && isfinite(dvz))) {
             atomicExch(bad, 1);
             continue;
@@ -610,6 +689,7 @@ void feat_scales(dmph_ctx *ctx, Surrogate *s)
     FeatScales &F = s->fs;
     F.vs = (float)vs;
     F.as = (float)as;
+    F.ts = (float)(as / 16.0);
     F.inv_vs = (float)(1.0 / vs);
     F.inv_as = (float)(1.0 / as);
     F.inv_Ps = (float)(1.0 / (rho * vs * vs));
@@ -626,8 +706,13 @@ int grid_slots(const dmph_ctx *ctx) { return ctx->sms * 4; }
 void enqueue_features(dmph_ctx *ctx, Surrogate *s, float *x32, cudaStream_t st)
 {
     enqueue_pair_passes32(ctx, st);
+    if (ctx->use_list) {
+        static const int gl = persistent_grid((const void *)k_features32_list, 256);
+        k_features32_list<<<gl, 256, 0, st>>>(ctx->P, ctx->Q, ctx->S, ctx->dB, s->fs, s->X, x32);
+    }
     static const int g = persistent_grid((const void *)k_features32, kFeatWarps * kWarp);
-    k_features32<<<g, kFeatWarps * kWarp, 0, st>>>(ctx->P, ctx->Q, ctx->S, ctx->dB, s->fs, s->X, x32);
+    k_features32<<<g, kFeatWarps * kWarp, 0, st>>>(ctx->P, ctx->Q, ctx->S, ctx->dB, s->fs, s->X, x32,
+                                                   ctx->use_list ? 1 : 0);
 }
 
 int check_err(dmph_ctx *ctx, Surrogate *s)
@@ -712,7 +797,55 @@ int train(dmph_ctx *ctx, Surrogate *s, int iters, float *loss_out)
     return DMPH_OK;
 }
 
-// one surrogate call: K steps of simulated time
+void drop_tail(Surrogate *s)
+{
+    if (s->tail_exec) cudaGraphExecDestroy(s->tail_exec);
+    if (s->tail_graph) cudaGraphDestroy(s->tail_graph);
+    s->tail_exec = nullptr;
+    s->tail_graph = nullptr;
+}
+
+// the part of a surrogate call after the prediction was found finite: apply
+// it to the fluid, advance the debris by the solver's own DEM or rigid-body
+// substeps with the fluid force of the block start held, clear the forces as
+// a drift would, and take the reference's rebuild decision on the device
+void enqueue_tail_ops(dmph_ctx *ctx, Surrogate *s, unsigned long long cond, cudaStream_t st)
+{
+    const int gs = grid_slots(ctx);
+    k_apply32<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->Y, 0, s->d_bad);
+    if (s->n_rows > s->n_fluid)
+        for (int k = 0; k < s->prm.substeps; ++k) enqueue_dem(ctx, st);
+    cudaMemsetAsync(ctx->S.f4, 0, sizeof(float4) * (size_t)ctx->P.N, st);
+    cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), st);
+    k_maxshift32<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->maxshift);
+    launch_decide(ctx->P, ctx->maxshift, ctx->dB, cond, st);
+}
+
+int capture_tail(dmph_ctx *ctx, Surrogate *s)
+{
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle cond;
+    CK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+    CK(cudaStreamBeginCaptureToGraph(ctx->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_tail_ops(ctx, s, (unsigned long long)cond, ctx->st);
+    int rc = capture_rebuild_if(ctx, cond, ctx->st);
+    cudaGraph_t g2 = g;
+    const cudaError_t ce = cudaStreamEndCapture(ctx->st, &g2);
+    if (rc || ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        if (!rc) ctx->err = std::string("surrogate tail capture: ") + cudaGetErrorString(ce);
+        return rc ? rc : DMPH_ECUDA;
+    }
+    CK(cudaGraphInstantiate(&s->tail_exec, g, 0));
+    s->tail_graph = g;
+    return DMPH_OK;
+}
+
+// one surrogate call: K steps of simulated time.  One host synchronisation:
+// whether every prediction is finite (a non-finite one leaves the state
+// untouched and sends the driver back to the plain solver); the rest runs as
+// the recorded tail graph, whose rebuild decision is taken on the device.
 int surrogate_block(dmph_ctx *ctx, Surrogate *s)
 {
     cudaStream_t st = ctx->st;
@@ -720,40 +853,37 @@ int surrogate_block(dmph_ctx *ctx, Surrogate *s)
     mlp_forward(s, s->X, s->n_fluid, s->Y, st);
     CK(cudaMemsetAsync(s->d_bad, 0, sizeof(int), st));
     const int gs = grid_slots(ctx);
-    // a non-finite prediction leaves the state untouched
     k_check_finite<<<gs, 256, 0, st>>>(ctx->dB, s->Y, 0, s->d_bad);
-    int bad = 0;
-    CK(cudaMemcpyAsync(&bad, s->d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(s->h_bad, s->d_bad, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (bad) {
+    if (*s->h_bad) {
         ctx->err = "surrogate: non-finite prediction";
         return DMPH_ENAN;
     }
-    k_apply32<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->Y, 0, s->d_bad);
-    // debris: the solver's own DEM / rigid-body substeps for the K steps, with
-    // the fluid force of the block start held
-    if (s->n_rows > s->n_fluid)
-        for (int k = 0; k < s->prm.substeps; ++k) enqueue_dem(ctx, st);
-    // the forces of the next evaluation start from zero like after a drift
-    CK(cudaMemsetAsync(ctx->S.f4, 0, sizeof(float4) * (size_t)ctx->P.N, st));
-    CK(cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), st));
-    k_maxshift32<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->maxshift);
-    launch_decide(ctx->P, ctx->maxshift, ctx->dB, 0, st);
-    CK(cudaGetLastError());
-    int need = 0;
-    CK(cudaMemcpyAsync(&need, ctx->dB + B_NEED, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (need) {
-        enqueue_rebuild(ctx, false, st);
-        ctx->launches += rebuild_launches(ctx, false);
-        ctx->host_rebuilds++;
+    if (ctx->prof) {
+        // phase timing synchronises inside the DEM phase: no recorded graph
+        enqueue_tail_ops(ctx, s, 0, st);
+        CK(cudaMemcpyAsync(s->h_bad, ctx->dB + B_NEED, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (*s->h_bad) {
+            enqueue_rebuild(ctx, false, st);
+            ctx->launches += rebuild_launches(ctx, false);
+            ctx->host_rebuilds++;
+        }
+    } else {
+        if (!s->tail_exec) {
+            const int rc = capture_tail(ctx, s);
+            if (rc) return rc;
+        }
+        CK(cudaGraphLaunch(s->tail_exec, st));
     }
-    // pair passes (list mode: 5, stencil: 2), features, 4 GEMMs, check, apply,
-    // maxshift, decide
-    ctx->launches += (ctx->use_list ? 14 : 11) + (s->n_rows > s->n_fluid ? s->prm.substeps * dem_launches(ctx) : 0);
+    // pair passes (list mode: 5, stencil: 2), features (list mode: 2), 4
+    // GEMMs, check, apply, maxshift, decide; the rebuilds the graph runs are
+    // counted by the device's rebuild counter
+    ctx->launches += (ctx->use_list ? 15 : 11) + (s->n_rows > s->n_fluid ? s->prm.substeps * dem_launches(ctx) : 0);
     for (int k = 0; k < s->prm.substeps; ++k) advance_host_clock(ctx);
     s->st.calls++;
-    return check_err(ctx, s);
+    return DMPH_OK;
 }
 
 // the walls never move when every wall type has zero velocity and spin and
@@ -785,6 +915,8 @@ void surrogate_release(dmph_ctx *ctx)
 {
     Surrogate *s = ctx->sg;
     if (!s) return;
+    drop_tail(s);
+    if (s->h_bad) cudaFreeHost(s->h_bad);
     for (void *p : s->allocs) cudaFree(p);
     delete s;
     ctx->sg = nullptr;
@@ -900,6 +1032,7 @@ extern "C" int dmph_surrogate_enable(dmph_ctx *ctx, const dmph_surrogate_params 
     SA(s->d_err, 1);
     SA(s->d_bad, 1);
     SA(s->d_acc, 4);
+    CK(cudaMallocHost(&s->h_bad, sizeof(int)));
     feat_scales(ctx, s);
     CK(cudaStreamSynchronize(ctx->st));
     drop_graph(ctx);
@@ -936,6 +1069,8 @@ extern "C" int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks)
     using namespace dmph;
     Surrogate *s = need_sg(ctx);
     if (!s) return DMPH_EINVAL;
+    drop_tail(s);  // recorded again with the context's current settings
+    drop_graph(ctx);
     for (int k = 0; k < nblocks; ++k) {
         int rc = DMPH_OK;
         if (s->fallback_left > 0 || !surrogate_allowed(ctx, s)) {
@@ -972,7 +1107,7 @@ extern "C" int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks)
         }
         if (rc) return rc;
     }
-    return DMPH_OK;
+    return check_err(ctx, s);  // a tensor-core wait that ran out, in any call
 }
 
 extern "C" int dmph_surrogate_get_stats(dmph_ctx *ctx, dmph_surrogate_stats *out)

@@ -400,10 +400,12 @@ int dmph_ensemble_destroy(dmph_ensemble *e); /* NULL: nothing to do, returns 0 *
 
 /* Learned surrogate of K solver steps (no counterpart in the reference).
  * FP32 split build only.  A surrogate call evaluates pass A and pass B at the
- * current state, computes 48 cell-list aggregated features per fluid and
+ * current state, computes 52 cell-list aggregated features per fluid and
  * debris particle, runs a 64-128-128-128-16 MLP (BF16 on the tensor cores,
- * FP32 accumulation) predicting the K-step velocity increment and the
- * position-increment residual, and applies them to the fluid; debris advance
+ * FP32 accumulation) predicting the K-step velocity increment dv of each
+ * fluid particle (outputs 0-2: (dv / (K dt) - a0) / (|g| / 16), a0 its
+ * acceleration at the block start; outputs 3-15 unused), and applies it to
+ * the fluid with the displacement K dt v0 + (K - 1) dt dv / 2; debris advance
  * by the solver's own DEM or rigid-body substeps with the fluid force of the
  * block start held; walls stay.  The network is
  * trained (Adam, FP32 master weights) on samples the solver generates:
@@ -461,7 +463,7 @@ int dmph_mlp_forward(dmph_ctx *ctx, const float *X, int n, float *Y);
 /* mean squared error over the first 6 outputs and the parameter gradient of
  * one batch of host rows (n = the training batch) */
 int dmph_mlp_gradient(dmph_ctx *ctx, const float *X, const float *T, int n, float *grad, float *loss);
-/* features of the current state for the fluid and debris slots, rows x 48 */
+/* features of the current state for the fluid and debris slots, rows x 52 */
 int dmph_surrogate_features(dmph_ctx *ctx, float *F, int *rows);
 
 /* Per-phase device timing.  With enable != 0, every following step records
