@@ -42,6 +42,7 @@ CU_SOURCES = [
     ("dmph_api.cu", ["-fmad=false"]),
     ("dmph_f32.cu", []),
     ("dmph_noalloc.cu", ["-fmad=false"]),
+    ("dmph_checkpoint.cu", ["-fmad=false"]),
     ("dmph_bodies.cu", []),
     ("dmph_mlp.cu", []),
     ("dmph_surrogate.cu", []),

@@ -19,16 +19,19 @@ thread_local const char *g_noctx_literal = nullptr;
 }
 
 
+// state: the allocation is part of the context's state (a checkpoint holds
+// it); false for output buffers allocated on first request
 template <class T>
-static int dalloc(dmph_ctx *ctx, T **ptr, size_t count)
+static int dalloc(dmph_ctx *ctx, T **ptr, size_t count, bool state = true)
 {
     void *p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, count ? count * sizeof(T) : 16);
+    const size_t bytes = count ? count * sizeof(T) : 16;
+    const cudaError_t e = cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {
         ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
         return DMPH_ENOMEM;
     }
-    ctx->allocs.push_back(p);
+    ctx->allocs.push_back({p, bytes, state});
     *ptr = (T *)p;
     return cudaMemsetAsync(p, 0, count ? count * sizeof(T) : 16, ctx->st) == cudaSuccess ? DMPH_OK : DMPH_ECUDA;
 }
@@ -41,7 +44,7 @@ static void release(dmph_ctx *ctx)
     drop_graph(ctx);
     if (ctx->st2) cudaStreamDestroy(ctx->st2);
     ctx->st2 = nullptr;
-    for (void *p : ctx->allocs) cudaFree(p);
+    for (const auto &a : ctx->allocs) cudaFree(a.p);
     ctx->allocs.clear();
     if (ctx->h_maxshift) cudaFreeHost(ctx->h_maxshift);
     if (ctx->h_small) cudaFreeHost(ctx->h_small);
@@ -898,7 +901,7 @@ extern "C" int dmph_get_field(dmph_ctx *ctx, int field_id, void *out)
     }
     if (field_id == DMPH_FIELD_VIRIAL_PRESSURE) {
         if (!ctx->vir) {
-            const int rc = dalloc(ctx, &ctx->vir, N);
+            const int rc = dalloc(ctx, &ctx->vir, N, false);
             if (rc) return rc;
         }
         if (ctx->fp32) {
@@ -957,6 +960,14 @@ extern "C" int dmph_get_field(dmph_ctx *ctx, int field_id, void *out)
     }
     CK(cudaMemcpyAsync(out, src, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    return DMPH_OK;
+}
+
+extern "C" int dmph_get_params(dmph_ctx *ctx, dmph_params *out)
+{
+    if (!ctx || !out) return DMPH_EINVAL;
+    *out = ctx->p;
+    out->time = ctx->time;
     return DMPH_OK;
 }
 
@@ -1044,7 +1055,7 @@ extern "C" int dmph_get_global_sums(dmph_ctx *ctx, double sums[DMPH_SUM_COUNT])
 {
     if (!ctx || !sums) return DMPH_EINVAL;
     if (!ctx->sums) {  // partial sums and the result, allocated on first use
-        const int rc = dalloc(ctx, &ctx->sums, (size_t)(kSumBlocks + 1) * DMPH_SUM_COUNT);
+        const int rc = dalloc(ctx, &ctx->sums, (size_t)(kSumBlocks + 1) * DMPH_SUM_COUNT, false);
         if (rc) return rc;
     }
     if (ctx->fp32) launch_export32(ctx->P, ctx->S, ctx->S.pos, ctx->S.vel, ctx->st);
@@ -1088,7 +1099,7 @@ extern "C" int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64
     int ovf = 0;
     if (ctx->use_list) {
         if (!ctx->stats) {  // two counters, allocated on first use
-            const int rc = dalloc(ctx, &ctx->stats, 2);
+            const int rc = dalloc(ctx, &ctx->stats, 2, false);
             if (rc) return rc;
         }
         CK(cudaMemsetAsync(ctx->stats, 0, 2 * sizeof(unsigned long long), ctx->st));
@@ -1312,6 +1323,8 @@ extern "C" int dmph_set_bodies(dmph_ctx *ctx, int nbodies, const int *body_of_ro
     ctx->bid2 = dbid2;
     ctx->S.body_rho = drho;
     ctx->S.frc_dem = dfd;
+    ctx->body_of_row.assign(body_of_row, body_of_row + N);
+    ctx->body_density.assign(body_density, body_density + nbodies);
     return DMPH_OK;
 }
 
@@ -1389,6 +1402,11 @@ extern "C" int dmph_destroy(dmph_ctx *ctx)
 
 namespace dmph {
 void set_noctx_message(const char *literal) { g_noctx_literal = literal; }
+void set_noctx_error(const std::string &msg)
+{
+    g_noctx_literal = nullptr;
+    g_create_err = msg;
+}
 }  // namespace dmph
 
 extern "C" const char *dmph_last_error(dmph_ctx *ctx)

@@ -75,7 +75,17 @@ struct dmph_ctx {
     double phase_ms[DMPH_PHASE_COUNT] = {0};
     long long phase_n[DMPH_PHASE_COUNT] = {0};
     std::string err;
-    std::vector<void *> allocs;
+    // every device allocation of the context, in allocation order; `state`
+    // ones (all but the lazily allocated output buffers) make a checkpoint
+    struct DevAlloc {
+        void *p;
+        size_t bytes;
+        bool state;
+    };
+    std::vector<DevAlloc> allocs;
+    // dmph_set_bodies' arguments (a checkpoint re-creates the same bodies)
+    std::vector<int> body_of_row;
+    std::vector<double> body_density;
     dmph::Surrogate *sg = nullptr;  // surrogate state (dmph_surrogate_enable)
 };
 

@@ -13,6 +13,8 @@ int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, con
 // dmph_api.cu: message that dmph_last_error(NULL) returns on the calling
 // thread until the next failing call without a context (a string literal)
 void set_noctx_message(const char *literal);
+// the same for calls that may allocate (dmph_checkpoint_open)
+void set_noctx_error(const std::string &msg);
 
 // dmph_rebuild.cu
 void launch_keys(const DevParams &P, const double *pos, const int *type, unsigned long long *words, cudaStream_t st);

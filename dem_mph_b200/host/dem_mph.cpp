@@ -1,7 +1,18 @@
 // dem_mph — drop-in replacement of the reference solver executable.
 //
 //   dem_mph [--dim 2|3] [--fp32] [--gpu N] [--bodies FILE | --rigid]
+//           [--checkpoint] [--resume FILE]
 //           data grid prof_pattern vtk_pattern log
+//
+// --checkpoint writes, beside every .prof file, NAME.prof.ckpt: a checkpoint
+// of the solver (dmph_checkpoint_write) with this driver's output schedule.
+// --resume FILE continues the run such a file was taken from: the solver
+// state, its parameters and the output schedule come from FILE, the data
+// file gives EndTime (so a run can be extended) and the grid file is not
+// read; no output.vtk is written.  The files written after a resume are
+// byte-identical to those of the uninterrupted run.  The reference's own
+// restart (a .prof file given as the grid) remains: it starts afresh from the
+// positions and velocities of the file.
 //
 // --bodies FILE moves the debris as rigid bodies with the membership and
 // densities of a body sidecar file (dmph_read_bodies_file); --rigid does the
@@ -56,8 +67,8 @@ int main(int argc, char **argv)
     // defaults of the reference (:54-58)
     std::string logf = "sample.log", dataf = "sample.data", gridf = "sample.grid", proff = "sample%03d.prof",
                 vtkf = "sample%03d.vtk";
-    int dim = 2, fp32 = 0, gpu = 0, rigid = 0;
-    std::string bodiesf;
+    int dim = 2, fp32 = 0, gpu = 0, rigid = 0, checkpoint = 0;
+    std::string bodiesf, resumef;
     std::vector<std::string> pos;
     for (int a = 1; a < argc; a++) {
         if (!std::strcmp(argv[a], "--dim") && a + 1 < argc)
@@ -70,6 +81,10 @@ int main(int argc, char **argv)
             bodiesf = argv[++a];
         else if (!std::strcmp(argv[a], "--rigid"))
             rigid = 1;
+        else if (!std::strcmp(argv[a], "--checkpoint"))
+            checkpoint = 1;
+        else if (!std::strcmp(argv[a], "--resume") && a + 1 < argc)
+            resumef = argv[++a];
         else
             pos.push_back(argv[a]);
     }
@@ -89,19 +104,41 @@ int main(int argc, char **argv)
     int rc = dmph_read_data_file(dataf.c_str(), &p);
     if (rc) return log_printf("cannot read %s: %s\n", dataf.c_str(), dmph_io_last_message()), 1;
     if (*dmph_io_last_message()) log_printf("%s", dmph_io_last_message());
+    if (cudaSetDevice(gpu) != cudaSuccess) return log_printf("cannot select GPU %d\n", gpu), 1;
+    // this driver's part of a checkpoint: its clock and output schedule
+    struct Schedule {
+        double time, output_next, vtk_output_next;
+        int step;
+    } sched = {p.time, 0.0, 0.0, 0};
+    dmph_ctx *ctx = nullptr;
     int n = 0;
-    rc = dmph_read_grid_file(gridf.c_str(), &p, &n, nullptr, nullptr, nullptr);
+    if (!resumef.empty()) {
+        int nu = 0;
+        rc = dmph_checkpoint_open(resumef.c_str(), &ctx, &sched, (int)sizeof(sched), &nu);
+        if (rc) return fail("dmph_checkpoint_open", rc, nullptr);
+        if (nu != (int)sizeof(sched)) return log_printf("%s was not written by dem_mph\n", resumef.c_str()), 1;
+        const double end_time = p.end_time;
+        dmph_get_params(ctx, &p);
+        p.end_time = end_time;
+        dmph_info inf;
+        dmph_get_info(ctx, &inf);
+        n = inf.n;
+        log_printf("resumed from %s at Time %e (step %d)\n", resumef.c_str(), sched.time, sched.step);
+    }
+    if (!ctx) rc = dmph_read_grid_file(gridf.c_str(), &p, &n, nullptr, nullptr, nullptr);
     if (rc) return log_printf("cannot read %s: %s\n", gridf.c_str(), dmph_io_last_message()), 1;
     std::vector<int> type(n);
     std::vector<double> x(3 * (size_t)n), v(3 * (size_t)n);
-    rc = dmph_read_grid_file(gridf.c_str(), &p, &n, type.data(), x.data(), v.data());
-    if (rc) return log_printf("cannot read %s: %s\n", gridf.c_str(), dmph_io_last_message()), 1;
-    p.dim = dim;
-    p.precision = fp32 ? DMPH_PRECISION_FP32_SPLIT : DMPH_PRECISION_FP64;
-    // the VTK output carries every particle's NeighborCount and the DEM
-    // constants the reference also evaluates for wall particles
-    p.flags |= DMPH_FLAG_ALL_NEIGHBOR_COUNTS | DMPH_FLAG_WALL_DEM_COEFFS;
-    if (cudaSetDevice(gpu) != cudaSuccess) return log_printf("cannot select GPU %d\n", gpu), 1;
+    if (!ctx) {
+        rc = dmph_read_grid_file(gridf.c_str(), &p, &n, type.data(), x.data(), v.data());
+        if (rc) return log_printf("cannot read %s: %s\n", gridf.c_str(), dmph_io_last_message()), 1;
+        p.dim = dim;
+        p.precision = fp32 ? DMPH_PRECISION_FP32_SPLIT : DMPH_PRECISION_FP64;
+        // the VTK output carries every particle's NeighborCount and the DEM
+        // constants the reference also evaluates for wall particles
+        p.flags |= DMPH_FLAG_ALL_NEIGHBOR_COUNTS | DMPH_FLAG_WALL_DEM_COEFFS;
+        sched.time = p.time;
+    }
     {
         time_t t = time(NULL);
         log_printf("start initialization at %s\n", ctime(&t));
@@ -110,7 +147,9 @@ int main(int argc, char **argv)
     std::vector<int> body_of_row;
     std::vector<double> body_density;
     int nbodies = 0;
-    if (!bodiesf.empty()) {
+    if (ctx) {
+        // resumed: the bodies come with the checkpoint
+    } else if (!bodiesf.empty()) {
         int nrows = 0;
         rc = dmph_read_bodies_file(bodiesf.c_str(), &nbodies, &nrows, nullptr, nullptr);
         if (!rc && nrows != n) return log_printf("%s has %d rows, the grid %d\n", bodiesf.c_str(), nrows, n), 1;
@@ -125,9 +164,10 @@ int main(int argc, char **argv)
                                        body_density.data(), n);
         if (rc) return log_printf("rigid bodies: %s\n", dmph_bodies_last_message()), 1;
     }
-    dmph_ctx *ctx = nullptr;
-    rc = dmph_create(&p, n, type.data(), x.data(), v.data(), &ctx);
-    if (rc) return fail("dmph_create", rc, nullptr);
+    if (!ctx) {
+        rc = dmph_create(&p, n, type.data(), x.data(), v.data(), &ctx);
+        if (rc) return fail("dmph_create", rc, nullptr);
+    }
     if (nbodies > 0) {
         rc = dmph_set_bodies(ctx, nbodies, body_of_row.data(), body_density.data());
         if (rc) return fail("dmph_set_bodies", rc, ctx);
@@ -164,11 +204,11 @@ int main(int argc, char **argv)
     };
     // the reference writes this file after initialisation (:426); its virial
     // pressure has not been computed yet and is zero
-    if (write_vtk("output.vtk", false)) return 1;
+    if (resumef.empty() && write_vtk("output.vtk", false)) return 1;
 
-    double Time = p.time, OutputNext = 0.0, VtkOutputNext = 0.0;
+    double Time = sched.time, OutputNext = sched.output_next, VtkOutputNext = sched.vtk_output_next;
     const double Dt = p.dt;
-    int iStep = (int)(Time / Dt);
+    int iStep = resumef.empty() ? (int)(Time / Dt) : sched.step;
     {
         time_t t = time(NULL);
         log_printf("start main roop at %s\n", ctime(&t));
@@ -186,6 +226,12 @@ int main(int argc, char **argv)
             if (rc) return log_printf("cannot write %s\n", fn), 1;
             log_printf("@ Prof Output Time : %e\n", Time);
             OutputNext += p.output_interval;
+            if (checkpoint) {
+                const Schedule now = {Time, OutputNext, VtkOutputNext, iStep};
+                const std::string ck = std::string(fn) + ".ckpt";
+                rc = dmph_checkpoint_write(ctx, ck.c_str(), &now, (int)sizeof(now));
+                if (rc) return fail("dmph_checkpoint_write", rc, ctx);
+            }
         }
         rc = dmph_step(ctx, 1);
         if (rc) return fail("dmph_step", rc, ctx);

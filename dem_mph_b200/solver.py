@@ -6,11 +6,14 @@ is present the calls fail loudly.
 """
 import ctypes as C
 import os
+import struct
 
 import numpy as np
 
 from . import abi
 from .abi import Params, Info, FIELDS
+
+CHECKPOINT_USER_MAX = 4096  # DMPH_CHECKPOINT_USER_MAX
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdmph.so")
@@ -46,6 +49,8 @@ def lib():
         L.dmph_get_global_sums.argtypes = [vp, vp]
         L.dmph_get_list_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
         L.dmph_set_bodies.argtypes = [vp, C.c_int, vp, vp]
+        L.dmph_checkpoint_write.argtypes = [vp, C.c_char_p, vp, C.c_int]
+        L.dmph_checkpoint_open.argtypes = [C.c_char_p, C.POINTER(vp), vp, C.c_int, C.POINTER(C.c_int)]
         L.dmph_get_bodies.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
         L.dmph_set_profiling.argtypes = [vp, C.c_int]
         L.dmph_set_graph.argtypes = [vp, C.c_int]
@@ -159,6 +164,38 @@ class Solver:
     def _check(self, rc):
         if rc != 0:
             raise DmphError(rc, lib().dmph_last_error(self._h).decode())
+
+    def checkpoint(self, path, user=b""):
+        """write a checkpoint for an exact resume (dmph_checkpoint_write);
+        `user`: up to CHECKPOINT_USER_MAX bytes of the caller's own"""
+        u = bytes(user)
+        self._check(lib().dmph_checkpoint_write(self._h, os.fsencode(path), u if u else None, len(u)))
+
+    @classmethod
+    def open_checkpoint(cls, path):
+        """(Solver, user bytes) from a checkpoint file (dmph_checkpoint_open):
+        stepping it gives the bits the writing context would have given"""
+        L = lib()
+        h = C.c_void_p()
+        ubuf = C.create_string_buffer(CHECKPOINT_USER_MAX)
+        nu = C.c_int()
+        rc = L.dmph_checkpoint_open(os.fsencode(path), C.byref(h), ubuf, CHECKPOINT_USER_MAX, C.byref(nu))
+        if rc != 0:
+            raise DmphError(rc, L.dmph_last_error(None).decode())
+        self = cls.__new__(cls)
+        self._h = h
+        # the creation parameters and the types by row, from the file's head
+        with open(path, "rb") as f:
+            head = f.read(40)
+            pbytes, hbytes = struct.unpack_from("<II", head, 12)
+            nrows, nbodies, _, ubytes = struct.unpack_from("<iiii", head, 24)
+            self.params = Params.from_buffer_copy(f.read(pbytes))
+            f.seek(hbytes + ubytes, 1)
+            self._typ = np.frombuffer(f.read(4 * nrows), np.int32).copy()
+        self.n = nrows
+        if nbodies > 0:
+            self.nbodies = nbodies
+        return self, ubuf.raw[:nu.value]
 
     def step(self, n=1):
         self._check(lib().dmph_step(self._h, n))

@@ -199,6 +199,29 @@ int dmph_get_state(dmph_ctx *ctx, int *type, double *x3, double *v3, int *orig_i
  * non-finite flag of dmph_step (the next step checks the new state). */
 int dmph_set_state(dmph_ctx *ctx, const double *x3, const double *v3);
 
+/* Checkpoint for an exact resume.  The reference restarts from a .prof file
+ * (source/DEM-MPH.cpp:433, :690, :853-877) and so loses what the file does not
+ * hold: the positions of the last neighbour rebuild (the trigger's
+ * NeighborCalculatedPosition), the sorted order and the neighbour lists of
+ * that rebuild, the DEM constants, the wall centres and the body states; a
+ * run resumed from it follows another trajectory.  dmph_checkpoint_write
+ * saves all of the context's device state and its clock (time, step and
+ * rebuild counts, wall centres, launch settings) to one binary file, with
+ * the parameters, the particle types and rows and the rigid-body membership,
+ * plus up to DMPH_CHECKPOINT_USER_MAX bytes of the caller's own (e.g. its
+ * output schedule).  dmph_checkpoint_open creates a context on the current
+ * device from such a file; stepping it gives the same bits as stepping the
+ * context that wrote the file.  The file is native (little-endian, this
+ * library's structure layouts) and about as large as the context's device
+ * memory.  Not saved: a surrogate (dmph_surrogate_enable), profiling and
+ * graph settings.  Write fails with DMPH_ENAN on a state dmph_step has
+ * flagged non-finite and with DMPH_EINVAL between dmph_step_begin and
+ * dmph_step_finish; open fails with DMPH_EIO on a truncated or foreign file
+ * and with DMPH_EINVAL when user_capacity is smaller than the saved bytes. */
+#define DMPH_CHECKPOINT_USER_MAX 4096
+int dmph_checkpoint_write(dmph_ctx *ctx, const char *path, const void *user, int user_bytes);
+int dmph_checkpoint_open(const char *path, dmph_ctx **out, void *user, int user_capacity, int *user_bytes);
+
 /* Per-particle fields, current order; `out` holds n (scalars) or 3n (vectors)
  * values of the type given beside each id. */
 enum dmph_field {
@@ -244,6 +267,11 @@ typedef struct dmph_info {
     int64_t kernel_launches;   /* kernels this library launched in dmph_step calls since create */
 } dmph_info;
 int dmph_get_info(dmph_ctx *ctx, dmph_info *info);
+
+/* The parameters the context was created with, `time` set to its current
+ * Time (a context opened from a checkpoint gives those of the context that
+ * wrote it). */
+int dmph_get_params(dmph_ctx *ctx, dmph_params *out);
 
 /*
  * Neighbour list in the reference's CSR form (calculateNeighbor,

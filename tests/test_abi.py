@@ -38,3 +38,21 @@ def test_create_rejects_bad_input_without_gpu_work():
     p = default_params()
     with __import__("pytest").raises(solver.DmphError):
         solver.Solver(p, np.array([9], np.int32), np.zeros((1, 3)), np.zeros((1, 3)))
+
+
+def test_checkpoint_open_rejects_foreign_files_without_gpu_work(tmp_path):
+    """the header is read and checked before any device call: a missing file,
+    a file of another kind and a truncated checkpoint head fail with DMPH_EIO
+    (-4); the user-buffer limit mirrors DMPH_CHECKPOINT_USER_MAX"""
+    import pytest
+    with open(os.path.join(ROOT, "include", "dmph.h")) as f:
+        m = re.search(r"#define DMPH_CHECKPOINT_USER_MAX (\d+)", f.read())
+    assert int(m.group(1)) == solver.CHECKPOINT_USER_MAX
+    foreign = tmp_path / "foreign.ckpt"
+    foreign.write_bytes(b"not a checkpoint at all" * 4)
+    head = tmp_path / "head.ckpt"
+    head.write_bytes(b"DMPHCKPT" + bytes(8))
+    for path in (tmp_path / "missing.ckpt", foreign, head):
+        with pytest.raises(solver.DmphError) as e:
+            solver.Solver.open_checkpoint(str(path))
+        assert e.value.code == -4, str(e.value)
