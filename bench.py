@@ -1,7 +1,7 @@
 """Benchmark of the DEM-MPH explicit timestep on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload config2|config1] [--precision fp64|fp32]
+                    [--workload config2|config1|config3|config5] [--precision fp64|fp32]
 
 One "step" is one explicit timestep of the whole scene (the reference main
 loop body, source/DEM-MPH.cpp:450-579): drift, walls, periodic wrap, the
@@ -42,7 +42,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # step ~6,450 on (3.3 ms/step), 6,219 rebuilds and 2.49 ms/step on average.
 # A short timed window therefore settles into the late flow, the costliest
 # regime of the run, so that it does not overstate the run.
-SETTLE_DEFAULT = {"config2": 7000, "config1": 200, "config3": 200}
+SETTLE_DEFAULT = {"config2": 7000, "config1": 200, "config3": 200, "config5": 2000}
 WINDOW = {"config2": "late flow after 7,000 settle steps: a neighbour rebuild every step, the costliest regime of "
                      "the 10,000-step configured run (which rebuilds in 62% of its steps)"}
 # Rebuild fraction of the timed window that SETTLE_DEFAULT leads to, as the
@@ -83,6 +83,8 @@ def make_scene(workload, rank):
         return scenes.config1(seed=seed)
     if workload == "config2":
         return scenes.config2(seed=seed)
+    if workload == "config5":
+        return scenes.config5(seed=seed)
     raise ValueError(workload)
 
 
@@ -252,15 +254,15 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None,
                     help="timed steps (default: the configured run, 10000 for config 2, 2000 for config 1, "
-                         "300 for config 3)")
+                         "300 for config 3, 1000 for config 5)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config2", "config1", "config3"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config1", "config3", "config5"])
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--settle", type=int, default=None,
                     help="untimed steps run before warm-up (default per workload: 7000 for config2, the late flow; "
-                         "200 otherwise)")
+                         "2000 for config5; 200 otherwise)")
     ap.add_argument("--no-graph", action="store_true", help="launch kernels one by one instead of graph replay")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch variants of the pair passes")
     ap.add_argument("--profiler-range", action="store_true",
@@ -279,7 +281,8 @@ def main():
     if args.settle is None:
         args.settle = SETTLE_DEFAULT.get(args.workload, 200)
     if args.steps is None:
-        args.steps = 2000 if args.surrogate else {"config2": 10000, "config1": 2000, "config3": 300}[args.workload]
+        args.steps = 2000 if args.surrogate else {"config2": 10000, "config1": 2000, "config3": 300,
+                                                  "config5": 1000}[args.workload]
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -204,6 +204,16 @@ def config2(seed=1234, dx=0.005):
                      debris_x=(0.3, 0.95), yaw=True, seed=seed, name="config2_dambreak_3d_dx5mm")
 
 
+def config5(seed=1234, dx=0.0035):
+    """Config 5 (the surrogate's production case): 3.2 x 1.0 x 1.0 m tank at
+    3.5 mm, a 0.5 x 0.35 (H) x 1.0 m column (4.09 M fluid), 1000 debris
+    cuboids with sides of 3-6 particles, densities 400-900 kg/m^3 and seeded
+    yaw, drawn over 20-97% of the tank length."""
+    return dam_break(dx=dx, tank=(3.2, 1.0, 1.0), column=(0.5, 0.35, 1.0), n_debris=1000,
+                     debris_sides=((3, 6), (3, 6), (3, 6)), debris_density=(400.0, 900.0),
+                     debris_x=(0.2, 0.97), yaw=True, seed=seed, name="config5_dambreak_3d_dx3p5mm")
+
+
 def small(seed=7, dx=0.02, n_debris=3, yaw=False):
     """A small 3D dam break (about 5k particles) for parity tests."""
     return dam_break(dx=dx, tank=(0.6, 0.3, 0.3), column=(0.16, 0.12, 0.3), n_debris=n_debris,
