@@ -173,16 +173,28 @@ def workload_config(scene, args, world):
     ours = ("FP32 split pair forces on cell-relative positions, FP64 rigid-body debris (DEM contacts and "
             "body update)" if args.precision == "fp32" else "FP64 throughout (the parity build)")
     ours += "; debris as rigid bodies" if bodies else "; debris as individual DEM particles"
+    if list_reuse_on(args, scene):
+        ours += ("; the reference's rebuild trigger refreshes the trigger positions and neighbour counts every "
+                 "time, the cell sort and Verlet lists (skin up to 0.4 dx) are remade only when they could "
+                 "miss a pair (list reuse)")
     return {"workload": scene.name, "n_particles": c["total"], "n_fluid": c["fluid"], "n_solid": c["solid"],
             "n_wall": c["wall"], "n_debris_bodies": len(scene.body_density), "dt": p.dt,
             "dem_substeps": int(p.dt / p.dem_dt), "settle_steps": args.settle,
             "window": WINDOW.get(args.workload, "after %d settle steps" % args.settle),
-            "arms": {"ours": ours + "; neighbour rebuild by the reference's trigger",
+            "arms": {"ours": ours + "; neighbour rebuild triggers by the reference's test",
                      "reference": "the reference's own CPU step (FP64, debris as individual DEM particles: it "
                                   "has no rigid bodies) on all host cores, its neighbour rebuild timed and "
                                   "added at the GPU window's cadence"},
             "parallelism": "replicas x%d" % world,
             "l2": "inputs larger than L2 (particle state alone %.0f MB)" % (c["total"] * 60 / 1e6)}
+
+
+def list_reuse_on(args, scene):
+    """list reuse (DMPH_FLAG_LIST_REUSE) in the GPU arm: FP32 split build,
+    debris as rigid bodies or none, unless --no-list-reuse"""
+    bodies = not args.no_bodies and len(scene.body_density) > 0
+    return (args.precision == "fp32" and not getattr(args, "no_list_reuse", False)
+            and (bodies or len(scene.body_density) == 0))
 
 
 def reference_rate(res, n, steps, rebuild_fraction):
@@ -204,6 +216,8 @@ def reference_rate(res, n, steps, rebuild_fraction):
 # list-mode kernels on config 2, FP32 split, late in the flow (after 6,000
 # steps), from ncu captures of the bench's own command
 TRAFFIC_CONFIG2_FP32 = {"pass_a": 765.5e6, "pass_b": 690.9e6, "list_build": 824.2e6}
+# the same with list reuse (lists with a skin of up to 0.4 dx); empty until captured
+TRAFFIC_CONFIG2_FP32_REUSE = {}
 TRAFFIC_SOURCE = "ncu capture of one launch of the same kernel and workload in the late flow"
 
 
@@ -276,6 +290,8 @@ def main():
                     help="surrogate judge tolerance on the velocity-increment error")
     ap.add_argument("--no-bodies", action="store_true",
                     help="move debris particles individually (reference DEM) instead of as rigid bodies")
+    ap.add_argument("--no-list-reuse", action="store_true",
+                    help="remake the cell sort and Verlet lists at every rebuild trigger (FP32 build)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.settle is None:
@@ -299,7 +315,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     from dem_mph_b200 import solver
-    from dem_mph_b200.abi import PRECISION_FP64, PRECISION_FP32_SPLIT
+    from dem_mph_b200.abi import FLAG_LIST_REUSE, PRECISION_FP64, PRECISION_FP32_SPLIT
 
     if args.workload == "config3":
         return run_ensemble(args, rank, world)
@@ -308,6 +324,8 @@ def main():
     scene = make_scene(args.workload, rank)
     p = scene.params.copy()
     p.precision = PRECISION_FP64 if args.precision == "fp64" else PRECISION_FP32_SPLIT
+    if list_reuse_on(args, scene):
+        p.flags |= FLAG_LIST_REUSE
     g = solver.Solver(p, scene.type, scene.x, scene.v)
     bodies = not args.no_bodies and len(scene.body_density) > 0
     if bodies:
@@ -341,6 +359,7 @@ def main():
     torch.cuda.synchronize()
     l0 = g.info().kernel_launches
     rebuilds_before = int(g.info().rebuilds)
+    builds_before = g.rebuild_stats()[1]
     if args.profiler_range:
         torch.cuda.profiler.start()
     with ClockSampler(torch.cuda.current_device()) as clk:
@@ -352,6 +371,7 @@ def main():
     inf_t = g.info()
     launches = int(inf_t.kernel_launches - l0)
     rebuilds_timed = int(inf_t.rebuilds) - rebuilds_before
+    builds_timed = g.rebuild_stats()[1] - builds_before
     ms_max = max_over_ranks(ms, world, "cuda")
     value = n * world * args.steps / (ms_max / 1e3)
 
@@ -365,7 +385,8 @@ def main():
     inf = g.info()
     n_fs = inf.n_fluid + inf.n_solid
     ea, eb = g.list_stats()
-    roofline = roofline_block(ph, args, n, n_fs, ea, eb, rebuilds_timed, prof_steps)
+    # the list build runs at the full rebuilds only (all of them without list reuse)
+    roofline = roofline_block(ph, args, n, n_fs, ea, eb, builds_timed, prof_steps, list_reuse_on(args, scene))
 
     # ---- end to end through the C ABI with host buffers: every step uploads
     # the particle state from pinned host memory, steps, reads it back
@@ -412,6 +433,7 @@ def main():
         "data": "synthetic (seeded dam break with debris, dem_mph_b200.scenes)",
         "config": workload_config(scene, args, world),
         "run": {"rebuilds_in_timed_steps": rebuilds_timed, "rebuild_fraction_timed": frac_timed,
+                "list_reuse": list_reuse_on(args, scene), "list_builds_in_timed_steps": builds_timed,
                 "timed_from_step": args.settle + args.warmup, "graph_replay": not args.no_graph,
                 "pass_variants": variants, "list_build_variant": build_variant, "precision": args.precision,
                 "debris": "rigid bodies (FP64)" if bodies else "individual DEM particles"},
@@ -428,19 +450,22 @@ def main():
         dist.destroy_process_group()
 
 
-def roofline_block(ph, args, n, n_fs, ea, eb, rebuilds_timed, prof_steps):
+def roofline_block(ph, args, n, n_fs, ea, eb, builds_timed, prof_steps, reuse=False):
     """The roofline object for the kernel with the most device time over the
     timed run, with the other timed kernels beside it; None when no phase was
-    timed."""
+    timed.  builds_timed: list builds in the timed steps; reuse: list reuse
+    on (longer lists: the traffic table's captures were made without it)."""
     peaks, peak_src = load_peaks()
-    kern, top = kernel_table(ph, args.precision, n, n_fs, ea, args.steps, rebuilds_timed)
+    kern, top = kernel_table(ph, args.precision, n, n_fs, ea, args.steps, builds_timed)
     if top is None:
         return None
     dur = kern[top]["launch_ms"]
     achieved = kern[top]["bytes"] / (dur / 1e3) / 1e9
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
     # an ncu capture of the same kernels on config 2 in the late flow
-    traffic_tab = TRAFFIC_CONFIG2_FP32 if (args.workload == "config2" and args.precision == "fp32") else {}
+    traffic_tab = {}
+    if args.workload == "config2" and args.precision == "fp32":
+        traffic_tab = TRAFFIC_CONFIG2_FP32_REUSE if reuse else TRAFFIC_CONFIG2_FP32
     # pair work: Verlet-list entries each pass walks per launch (each entry is
     # one candidate pair: two 16-byte neighbour gathers and the pair arithmetic)
     pa_dur = kern["pass_a"]["launch_ms"] if "pass_a" in kern else float("nan")

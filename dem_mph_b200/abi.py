@@ -22,6 +22,7 @@ FLAG_SURFACE_TENSION_OFF = 1 << 1
 FLAG_WALL_DEM_COEFFS = 1 << 2
 FLAG_RIGID_CLUMPS = 1 << 3
 FLAG_ALL_NEIGHBOR_COUNTS = 1 << 4
+FLAG_LIST_REUSE = 1 << 5
 
 # dmph_field ids and (dtype, components)
 FIELDS = {

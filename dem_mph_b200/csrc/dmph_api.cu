@@ -96,7 +96,8 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
         // the walls' wall-wall sums are kept only while every wall keeps its slot
         if (np == N && S.st_valid) cudaMemsetAsync(S.st_valid, 0, N * sizeof(int), st);
         launch_permute32(P, (int)np, ctx->words, S.pos, S.v4, S.type, S.pidx, ctx->p4b, ctx->v4b, ctx->type2,
-                         ctx->pidx2, S.xref, S.xref4, S.bid, ctx->bid2, S.vel, ctx->pos2, ctx->vel2, st);
+                         ctx->pidx2, S.xref, S.xref4, S.bid, ctx->bid2, S.vel, ctx->pos2, ctx->vel2, st,
+                         ctx->list_reuse ? S.xrefL4 : nullptr);
         cudaMemcpyAsync(S.p4, ctx->p4b, np * sizeof(float4), cudaMemcpyDeviceToDevice, st);
         cudaMemcpyAsync(S.v4, ctx->v4b, np * sizeof(float4), cudaMemcpyDeviceToDevice, st);
     } else {
@@ -122,7 +123,9 @@ void dmph::enqueue_rebuild(dmph_ctx *ctx, bool first, cudaStream_t st)
     if (ctx->use_list) {
         // the list build alone is also timed as phase 6 (inside phase 1)
         if (ctx->prof) cudaEventRecord(ctx->pl0, st);
-        if (ctx->fp32) launch_build_list32(P, ctx->Q, S, ctx->dB, ctx->Wm.moving ? 0 : 1, st, ctx->var_build);
+        if (ctx->fp32)
+            launch_build_list32(P, ctx->Q, S, ctx->dB, ctx->Wm.moving ? 0 : 1, st, ctx->var_build,
+                                ctx->list_reuse ? 1 : 0);
         else launch_build_list64(P, S, ctx->dB, st);
         if (ctx->prof) {
             cudaEventRecord(ctx->pl1, st);
@@ -164,16 +167,37 @@ static void phase_end(dmph_ctx *ctx, int ph)
 }
 
 // drift + rebuild decision (first part of a step)
+bool dmph::reuse_active(const dmph_ctx *ctx)
+{
+    // (the neighbour counts of every particle, DMPH_FLAG_ALL_NEIGHBOR_COUNTS,
+    // are made by the full rebuild only)
+    return ctx->list_reuse && ctx->fp32 && ctx->use_list && ctx->walls_rest && ctx->csort && !ctx->Wm.moving &&
+           !ctx->all_counts && (ctx->n_solid == 0 || ctx->Bd.B > 0);
+}
+
+// Head of a step: drift and the rebuild decision (B_NEED: 0 none, 1 full
+// rebuild, 2 with list reuse a trigger that keeps the lists, whose trigger
+// positions and debris counts the two gated kernels after the decision
+// refresh)
 void dmph::enqueue_head(dmph_ctx *ctx, unsigned long long graph_cond, cudaStream_t st)
 {
     const DevParams &P = ctx->P;
+    const bool reuse = reuse_active(ctx);
     cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), st);
+    if (reuse) cudaMemsetAsync(ctx->maxshiftL, 0, sizeof(unsigned long long), st);
     if (ctx->fp32)
-        launch_drift32(P, ctx->Q, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, st);
+        launch_drift32(P, ctx->Q, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, st, reuse ? ctx->maxshiftL : nullptr);
     else
         launch_drift(P, ctx->S, ctx->Wm, ctx->maxshift, ctx->sms, st);
-    launch_decide(P, ctx->maxshift, ctx->dB, graph_cond, st);
+    launch_decide(P, ctx->maxshift, ctx->dB, graph_cond, st, reuse ? ctx->maxshiftL : nullptr);
+    if (reuse) {
+        launch_kept_trigger32(P, ctx->S, ctx->dB, ctx->n_fluid + ctx->n_solid, st);
+        launch_counts_list_kept(P, ctx->S, ctx->dB, st);
+    }
 }
+
+// kernels enqueue_head launches
+static long long head_launches(const dmph_ctx *ctx) { return reuse_active(ctx) ? 4 : 2; }
 
 // the pair passes (first part of a step's tail)
 void dmph::enqueue_passes(dmph_ctx *ctx, cudaStream_t st)
@@ -391,8 +415,8 @@ int dmph::step_once(dmph_ctx *ctx)
     phase_end(ctx, 0);
     CK(cudaMemcpyAsync(ctx->h_small, ctx->dB + B_NEED, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
-    ctx->launches += 2;
-    if (ctx->h_small[0]) {
+    ctx->launches += head_launches(ctx);
+    if (ctx->h_small[0] == 1) {
         phase_begin(ctx);
         enqueue_rebuild(ctx, false, ctx->st);
         phase_end(ctx, 1);
@@ -577,6 +601,17 @@ extern "C" int dmph_create(const dmph_params *p, int n, const int *type, const d
     AL(ctx->total, 4);
     AL(ctx->maxshift, 1);
     AL(ctx->dB, B_COUNT);
+    if (ctx->fp32 && (p->flags & DMPH_FLAG_LIST_REUSE)) {
+        ctx->list_reuse = true;
+        AL(S.xrefL4, N);
+        AL(ctx->maxshiftL, 1);
+    }
+    {
+        // the lists of the first build have the MARGIN skin
+        const int skin[2] = {10, 10};
+        CKC(cudaMemcpyAsync(ctx->dB + B_SKIN, skin, sizeof(skin), cudaMemcpyHostToDevice, ctx->st));
+        CKC(cudaStreamSynchronize(ctx->st));
+    }
     // upload: interleaved x,y,z rows -> component planes
     {
         std::vector<double> planes(N3);
@@ -738,6 +773,8 @@ __global__ void k_set_need(int *dB, int need)
 {
     dB[B_NEED] = need;
     dB[B_REBUILDS] += need;
+    dB[B_LIST_BUILDS] += need;
+    if (need) dB[B_SKIN_NEXT] = 10;  // lists with the MARGIN skin (no list reuse in split steps)
 }
 
 extern "C" int dmph_step_begin(dmph_ctx *ctx, double *max_shift2)
@@ -971,6 +1008,17 @@ extern "C" int dmph_get_params(dmph_ctx *ctx, dmph_params *out)
     return DMPH_OK;
 }
 
+extern "C" int dmph_get_rebuild_stats(dmph_ctx *ctx, int64_t *triggers, int64_t *list_builds)
+{
+    if (!ctx) return DMPH_EINVAL;
+    int b[B_COUNT];
+    const int rc = read_bounds(ctx, b);
+    if (rc) return rc;
+    if (triggers) *triggers = b[B_REBUILDS];
+    if (list_builds) *list_builds = b[B_LIST_BUILDS];
+    return DMPH_OK;
+}
+
 extern "C" int dmph_get_info(dmph_ctx *ctx, dmph_info *info)
 {
     if (!ctx || !info) return DMPH_EINVAL;
@@ -1000,8 +1048,8 @@ extern "C" int dmph_get_info(dmph_ctx *ctx, dmph_info *info)
     info->num_bodies = ctx->Bd.B;
     info->surface_tension = P.surface_tension;
     {
-        const long long graph_rebuilds = b[B_REBUILDS] - ctx->host_rebuilds;
-        info->kernel_launches = ctx->launches + ctx->graph_steps * (2 + tail_launches(ctx, true)) +
+        const long long graph_rebuilds = b[B_LIST_BUILDS] - ctx->host_rebuilds;
+        info->kernel_launches = ctx->launches + ctx->graph_steps * (head_launches(ctx) + tail_launches(ctx, true)) +
                                 graph_rebuilds * rebuild_launches(ctx, false);
     }
     return DMPH_OK;
@@ -1356,6 +1404,12 @@ extern "C" int dmph_set_pair_mode(dmph_ctx *ctx, int mode)
         if (ctx->fp32)
             launch_build_list32(ctx->P, ctx->Q, ctx->S, ctx->dB, ctx->Wm.moving ? 0 : 1, ctx->st, ctx->var_build);
         else launch_build_list64(ctx->P, ctx->S, ctx->dB, ctx->st);
+        if (ctx->list_reuse) {
+            // lists of the MARGIN skin, made away from a rebuild: the next
+            // trigger remakes them
+            const int ten = 10;
+            CK(cudaMemcpyAsync(ctx->dB + B_SKIN, &ten, sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+        }
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(ctx->st));
     }
@@ -1620,6 +1674,10 @@ extern "C" int dmph_ensemble_create(dmph_ctx *const *scenes, int nscenes, dmph_e
     for (int k = 0; k < nscenes; ++k) {
         dmph_ctx *c = scenes[k];
         if (!c || !c->fp32) return DMPH_EINVAL;  // the ensemble kernels are the FP32 split passes
+        if (c->list_reuse) {
+            c->err = "list reuse (DMPH_FLAG_LIST_REUSE) is not supported in an ensemble";
+            return DMPH_EINVAL;
+        }
         for (int j = 0; j < k; ++j)
             if (scenes[j] == c) return DMPH_EINVAL;
         if (dev < 0) dev = c->device;

@@ -46,6 +46,10 @@ struct dmph_ctx {
     unsigned long long *words2 = nullptr;
     int *flag = nullptr, *offs = nullptr, *bsums = nullptr, *total = nullptr;
     unsigned long long *maxshift = nullptr;
+    // list reuse (DMPH_FLAG_LIST_REUSE): largest displacement since the
+    // lists were built, and whether the flag was given
+    unsigned long long *maxshiftL = nullptr;
+    bool list_reuse = false;
     unsigned long long *stats = nullptr;      // dmph_get_list_stats counters
     double *sums = nullptr;                   // dmph_get_global_sums partials and result
     unsigned long long *h_maxshift = nullptr;  // pinned
@@ -121,6 +125,10 @@ int capture_rebuild_if(dmph_ctx *ctx, cudaGraphConditionalHandle cond, cudaStrea
 int check_finite(dmph_ctx *ctx);
 constexpr int kFiniteCheckEvery = 256;  // steps between two checks inside one dmph_step call
 void drop_graph(dmph_ctx *ctx);
+// list reuse in effect for the next steps: the flag, the FP32 build with
+// lists, walls at rest, the counting sort, no debris outside rigid bodies,
+// no neighbour counts kept for every particle
+bool reuse_active(const dmph_ctx *ctx);
 
 // surrogate (dmph_surrogate.cu)
 void surrogate_release(dmph_ctx *ctx);

@@ -23,6 +23,9 @@ namespace dmph {
 constexpr int kTypes = DMPH_TYPE_COUNT;
 constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xffffffffu;
+// list reuse: the widest list skin past MaxRadius, in hundredths of dx (the
+// cells are this much wider than MaxRadius + MARGIN)
+constexpr int kSkinMaxHundredths = 40;
 
 __host__ __device__ inline bool is_fluid(int t) { return DMPH_FLUID_BEGIN <= t && t < DMPH_FLUID_END; }
 __host__ __device__ inline bool is_solid(int t) { return DMPH_SOLID_BEGIN <= t && t < DMPH_SOLID_END; }
@@ -91,6 +94,12 @@ enum DevBound {
     B_LIST_OVF = 9, // a Verlet list of the last rebuild overflowed (FP32 list mode): stencil passes run
     B_LIST_SPLIT = 10, // the FP32 lists hold no wall-wall pairs (built with the walls at rest)
     B_NONFINITE = 11,  // a drift met a non-finite position or velocity (sticky; no rebuild runs while set)
+    // list reuse (FP32 lists kept across rebuild triggers): B_NEED = 1 for a
+    // full rebuild (sort and lists), 2 for a trigger that keeps the lists
+    B_SKIN = 12,        // skin of the current lists past MaxRadius, hundredths of dx (10 = MARGIN)
+    B_SKIN_NEXT = 13,   // skin of the lists the next build makes
+    B_GAP = 14,         // steps since the last rebuild trigger
+    B_LIST_BUILDS = 15, // full rebuilds (cell sort and lists) since creation, the first excluded
     B_COUNT = 16
 };
 

@@ -140,12 +140,49 @@ __device__ __forceinline__ void block_max_shift(float m2, unsigned long long *ma
     __syncthreads();
 }
 
-__global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm, unsigned long long *maxshift)
+// REUSE (list reuse): also the largest displacement since the lists were
+// built, into *maxshiftL
+template <bool REUSE>
+__global__ void k_drift32(DevParams P, DevParams32 Q, DevState S, WallMotion Wm, unsigned long long *maxshift,
+                          unsigned long long *maxshiftL)
 {
-    float m2 = 0.f;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.N; i += gridDim.x * blockDim.x)
+    float m2 = 0.f, mL = 0.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.N; i += gridDim.x * blockDim.x) {
         m2 = fmaxf(m2, drift32_slot(P, Q, S, Wm, i));
+        if (REUSE) {
+            const float4 p = S.p4[i], r = S.xrefL4[i];
+            const float dx = p.x - r.x, dy = p.y - r.y, dz = p.z - r.z;
+            mL = fmaxf(mL, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        }
+    }
     block_max_shift(m2, maxshift);
+    if (REUSE) block_max_shift(mL, maxshiftL);
+}
+
+// list reuse: a trigger that keeps the lists makes the current positions the
+// trigger positions, as a full rebuild does (k_permute32 writes xref and
+// xref4): the FP32 frame positions, and the FP64 ones (the fluid's from the
+// FP32 state as k_export32 forms them, the debris' FP64 masters)
+__global__ void k_kept_trigger32(DevParams P, DevState S, const int *dB, int n)
+{
+    if (dB[B_NEED] != 2) return;
+    const int N = P.N;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 p = S.p4[i];
+        S.xref4[i] = p;
+        const unsigned w = __float_as_uint(p.w);
+        if (is_fluid(unpack_type(w))) {
+            const int c[3] = {unpack_cx(w), unpack_cy(w), unpack_cz(w)};
+            const float pr[3] = {p.x, p.y, p.z};
+            for (int d = 0; d < 3; d++) {
+                const double a = P.dmin[d] + c[d] * P.cw[d] + (double)pr[d];
+                const double t = a - P.dmin[d];
+                S.xref[d * N + i] = (t - P.W[d] * floor(t / P.W[d])) + P.dmin[d];
+            }
+        } else {
+            for (int d = 0; d < 3; d++) S.xref[d * N + i] = S.pos[d * N + i];
+        }
+    }
 }
 
 // The drift of every scene of an ensemble in one launch (scenes whose walls
@@ -772,13 +809,21 @@ __device__ __forceinline__ void build_list32_chunk(const DevParams &P, const Dev
 
 // WPB warps per block, MINB resident blocks per SM requested from the
 // register allocator (the launch variants of dmph_autotune_list_build)
+// skin_from_dB (list reuse): the list radius is MaxRadius plus the skin
+// dB[B_SKIN_NEXT] (hundredths of dx, MARGIN at least), recorded in dB[B_SKIN]
 template <bool ST, int WPB, int MINB>
 __global__ void __launch_bounds__(WPB * kWarp, MINB) k_build_list32(DevParams P, DevParams32 Q, DevState S, int *dB,
-                                                                   float rc2, int split)
+                                                                   float rc2, int split, int skin_from_dB)
 {
     __shared__ TileL tiles[WPB];
     TileL &tl = tiles[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
+    if (skin_from_dB) {
+        const int h = dB[B_SKIN_NEXT] > 10 ? dB[B_SKIN_NEXT] : 10;
+        const float rl = (float)(sqrt(P.rc2) - 0.1 * P.dx + 0.01 * h * P.dx);
+        rc2 = rl * rl;
+        if (blockIdx.x == 0 && threadIdx.x == 0) dB[B_SKIN] = h;
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) dB[B_LIST_SPLIT] = split;
     FOR_EACH_CHUNK(dB, CR_WET, WPB, cidx)
     {
@@ -1267,7 +1312,8 @@ __global__ void k_permute32(DevParams P, int n, const unsigned long long *__rest
                             const int *__restrict__ pidx_in, float4 *__restrict__ p_out, float4 *__restrict__ v_out,
                             int *__restrict__ type_out, int *__restrict__ pidx_out, double *__restrict__ xref,
                             float4 *__restrict__ xref4, const int *__restrict__ bid_in, int *__restrict__ bid_out,
-                            const double *__restrict__ vabs, double *__restrict__ pos_out, double *__restrict__ vel_out)
+                            const double *__restrict__ vabs, double *__restrict__ pos_out, double *__restrict__ vel_out,
+                            float4 *__restrict__ xrefL4)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int N = P.N;
@@ -1291,6 +1337,7 @@ __global__ void k_permute32(DevParams P, int n, const unsigned long long *__rest
     const float4 p = make_float4(r[0], r[1], r[2], __uint_as_float(pack_cell(t, c[0], c[1], c[2])));
     p_out[i] = p;
     xref4[i] = p;
+    if (xrefL4) xrefL4[i] = p;
     v_out[i] = v_in[src];
     type_out[i] = t;
     pidx_out[i] = pidx_in[src];
@@ -1501,11 +1548,18 @@ DevParams32 make_params32(const DevParams &P)
 }
 
 void launch_drift32(const DevParams &P, const DevParams32 &Q, const DevState &S, const WallMotion &Wm,
-                    unsigned long long *maxshift, int sms, cudaStream_t st)
+                    unsigned long long *maxshift, int sms, cudaStream_t st, unsigned long long *maxshiftL)
 {
     int blocks = (P.N + 255) / 256;
     if (blocks > sms * 8) blocks = sms * 8;
-    k_drift32<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(P, Q, S, Wm, maxshift);
+    if (maxshiftL)
+        k_drift32<true><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(P, Q, S, Wm, maxshift, maxshiftL);
+    else
+        k_drift32<false><<<blocks > 0 ? blocks : 1, 256, 0, st>>>(P, Q, S, Wm, maxshift, nullptr);
+}
+void launch_kept_trigger32(const DevParams &P, const DevState &S, const int *dB, int n, cudaStream_t st)
+{
+    k_kept_trigger32<<<148 * 4, 256, 0, st>>>(P, S, dB, n);
 }
 // launch-parameter variants the autotuner chooses from: warps per block x
 // requested resident blocks per SM
@@ -1562,7 +1616,7 @@ void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S
 #define DMPH_BUILD_VARIANTS(X) X(0, 8, 3) X(1, 8, 4) X(2, 4, 8)
 
 void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, int split,
-                         cudaStream_t st, int variant)
+                         cudaStream_t st, int variant, int skin_from_dB)
 {
     cudaMemsetAsync(dB + B_LIST_OVF, 0, sizeof(int), st);
     cudaMemsetAsync(S.nbn, 0xFF, sizeof(int) * (size_t)P.N, st);
@@ -1570,10 +1624,12 @@ void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevStat
     case ID:                                                                                          \
         if (P.surface_tension) {                                                                      \
             static const int g = grid_for(k_build_list32<true, WPB, MINB>, WPB * kWarp);              \
-            k_build_list32<true, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2, split);   \
+            k_build_list32<true, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2, split,      \
+                                                                       skin_from_dB);                 \
         } else {                                                                                      \
             static const int g = grid_for(k_build_list32<false, WPB, MINB>, WPB * kWarp);             \
-            k_build_list32<false, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2, split);  \
+            k_build_list32<false, WPB, MINB><<<g, WPB * kWarp, 0, st>>>(P, Q, S, dB, (float)P.rc2, split,     \
+                                                                        skin_from_dB);                \
         }                                                                                             \
         break;
     switch (variant) {
@@ -1704,10 +1760,11 @@ void launch_import32(const DevParams &P, const DevState &S, const double *pos, c
 void launch_permute32(const DevParams &P, int n, const unsigned long long *words, const double *xabs,
                       const float4 *v_in, const int *type_in, const int *pidx_in, float4 *p_out, float4 *v_out,
                       int *type_out, int *pidx_out, double *xref, float4 *xref4, const int *bid_in, int *bid_out,
-                      const double *vabs, double *pos_out, double *vel_out, cudaStream_t st)
+                      const double *vabs, double *pos_out, double *vel_out, cudaStream_t st, float4 *xrefL4)
 {
     k_permute32<<<(n + 255) / 256, 256, 0, st>>>(P, n, words, xabs, v_in, type_in, pidx_in, p_out, v_out, type_out,
-                                                 pidx_out, xref, xref4, bid_in, bid_out, vabs, pos_out, vel_out);
+                                                 pidx_out, xref, xref4, bid_in, bid_out, vabs, pos_out, vel_out,
+                                                 xrefL4);
 }
 void launch_widen_f(const float *in, double *out, int n, cudaStream_t st)
 {

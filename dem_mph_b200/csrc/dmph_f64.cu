@@ -648,9 +648,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_counts(DevParams P, 
 // a thin shell past it); the reference's FP64 distance test on the
 // rebuild-time positions decides, as in k_counts, and i itself counts as
 // in the reference's list.  One warp per debris particle.
-__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_counts_list(DevParams P, DevState S, const int *dB)
+// need_gate: run only on a step whose B_NEED is that value (list reuse: a
+// trigger that keeps the lists); 0: always (inside a rebuild)
+__global__ void __launch_bounds__(kWarpsPerBlock * kWarp) k_counts_list(DevParams P, DevState S, const int *dB,
+                                                                      int need_gate)
 {
     if (dB[B_LIST_OVF]) return;
+    if (need_gate && dB[B_NEED] != need_gate) return;
     const int lane = threadIdx.x & 31;
     const int N = P.N;
     const long long ld = N;
@@ -946,9 +950,14 @@ void launch_counts(const DevParams &P, const DevState &S, const int *dB, int ran
 void launch_counts_list(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
 {
     static const int gl = persistent_grid((const void *)k_counts_list, kBlock);
-    k_counts_list<<<gl, kBlock, 0, st>>>(P, S, dB);
+    k_counts_list<<<gl, kBlock, 0, st>>>(P, S, dB, 0);
     static const int g = persistent_grid((const void *)k_counts, kBlock);
     k_counts<<<g, kBlock, 0, st>>>(P, S, dB, CR_SOLID, 1);
+}
+void launch_counts_list_kept(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st)
+{
+    static const int gl = persistent_grid((const void *)k_counts_list, kBlock);
+    k_counts_list<<<gl, kBlock, 0, st>>>(P, S, dB, 2);
 }
 void launch_neighbor_fill(const DevParams &P, const DevState &S, const int *dB, const long long *ptr, int *ind,
                           cudaStream_t st)

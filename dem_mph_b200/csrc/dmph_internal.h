@@ -39,8 +39,10 @@ void launch_widen(const int *in, long long *out, int n, cudaStream_t st);
 void launch_bounds(const DevParams &P, const int *start, const int *offs, const int *total, int *dB, cudaStream_t st);
 void launch_wet_partition(const DevParams &P, const unsigned long long *words, const int *start, Chunk *chunks,
                           Chunk *tmp, int *dB, int *flag, int *offs, int *block_sums, int *total, cudaStream_t st);
+// maxshiftL: largest displacement since the lists were built (list reuse),
+// null without list reuse
 void launch_decide(const DevParams &P, const unsigned long long *maxshift, int *dB, unsigned long long graph_cond,
-                   cudaStream_t st);
+                   cudaStream_t st, const unsigned long long *maxshiftL = nullptr);
 
 // dmph_f64.cu
 void launch_drift(const DevParams &P, const DevState &S, const WallMotion &Wm, unsigned long long *maxshift, int sms,
@@ -60,19 +62,30 @@ void launch_counts(const DevParams &P, const DevState &S, const int *dB, int ran
 // FP32 list mode, debris counts from the lists (with the stencil walk gated
 // on a list overflow): 2 kernels
 void launch_counts_list(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
+// list reuse: the same debris counts on a trigger that keeps the lists
+// (B_NEED = 2; 1 kernel, a no-op on other steps)
+void launch_counts_list_kept(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 void launch_neighbor_fill(const DevParams &P, const DevState &S, const int *dB, const long long *ptr, int *ind,
                           cudaStream_t st);
 
 // dmph_f32.cu
 DevParams32 make_params32(const DevParams &P);
+// maxshiftL (list reuse, else null): also the largest displacement since the
+// lists were built (from S.xrefL4)
 void launch_drift32(const DevParams &P, const DevParams32 &Q, const DevState &S, const WallMotion &Wm,
-                    unsigned long long *maxshift, int sms, cudaStream_t st);
+                    unsigned long long *maxshift, int sms, cudaStream_t st, unsigned long long *maxshiftL = nullptr);
+// list reuse, a trigger that keeps the lists (B_NEED = 2; a no-op on other
+// steps): the trigger positions of the first n slots (FP32 and FP64) become
+// the current ones
+void launch_kept_trigger32(const DevParams &P, const DevState &S, const int *dB, int n, cudaStream_t st);
 void launch_pass_a32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int range, int variant,
                      cudaStream_t st, int gate = 0);
 void launch_pass_b32(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
                      cudaStream_t st, int gate = 0);
+// skin_from_dB (list reuse): the list radius is MaxRadius + dB[B_SKIN_NEXT]
+// hundredths of dx (recorded in dB[B_SKIN]) instead of MaxRadius + MARGIN
 void launch_build_list32(const DevParams &P, const DevParams32 &Q, const DevState &S, int *dB, int split,
-                         cudaStream_t st, int variant = 0);
+                         cudaStream_t st, int variant = 0, int skin_from_dB = 0);
 constexpr int kBuildVariants = 3;  // launch variants of the FP32 list build
 void launch_list_wall_guard(int *dB, cudaStream_t st);
 void launch_pass_a32_list(const DevParams &P, const DevParams32 &Q, const DevState &S, const int *dB, int variant,
@@ -89,7 +102,8 @@ void launch_import32(const DevParams &P, const DevState &S, const double *pos, c
 void launch_permute32(const DevParams &P, int n, const unsigned long long *words, const double *xabs,
                       const float4 *v_in, const int *type_in, const int *pidx_in, float4 *p_out, float4 *v_out,
                       int *type_out, int *pidx_out, double *xref, float4 *xref4, const int *bid_in, int *bid_out,
-                      const double *vabs, double *pos_out, double *vel_out, cudaStream_t st);
+                      const double *vabs, double *pos_out, double *vel_out, cudaStream_t st,
+                      float4 *xrefL4 = nullptr);
 void launch_solid_force_to64(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 void launch_sync_solids32(const DevParams &P, const DevState &S, const int *dB, cudaStream_t st);
 double lattice_n0p32(const DevParams &P, const DevParams32 &Q, cudaStream_t st);

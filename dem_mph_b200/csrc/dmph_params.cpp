@@ -151,9 +151,16 @@ int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, con
         P.hW[d] = 0.5 * P.W[d];
         P.dmin[d] = p.domain_min[d];
     }
-    cc[0] = std::floor((p.domain_max[0] - p.domain_min[0]) / (maxR + margin));
-    cc[1] = std::floor((p.domain_max[1] - p.domain_min[1]) / (maxR + margin));
-    cc[2] = p.dim == 2 ? 1 : std::floor((p.domain_max[2] - p.domain_min[2]) / (maxR + margin));
+    // list reuse (FP32 build): cells wider by the widest list skin, so that
+    // the 3-cell stencil holds every pair within the list radius while the
+    // particles stay in the cells of the last sort
+    const double cell_r = maxR + margin +
+                          ((p.flags & DMPH_FLAG_LIST_REUSE) && p.precision == DMPH_PRECISION_FP32_SPLIT
+                               ? 0.01 * kSkinMaxHundredths * dx
+                               : 0.0);
+    cc[0] = std::floor((p.domain_max[0] - p.domain_min[0]) / cell_r);
+    cc[1] = std::floor((p.domain_max[1] - p.domain_min[1]) / cell_r);
+    cc[2] = p.dim == 2 ? 1 : std::floor((p.domain_max[2] - p.domain_min[2]) / cell_r);
     for (int d = 0; d < 3; d++)
         if (!(cc[d] >= 1.0) || cc[d] > 1.0e7) return *msg = "domain narrower than one neighbour cell", DMPH_EINVAL;
     const double tot = cc[0] * cc[1] * cc[2];
@@ -163,7 +170,7 @@ int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, con
     for (int d = 0; d < 3; d++) P.cw[d] = P.W[d] / P.cc[d];
     // the reference asserts a 3-cell stencil per axis (:1540-1543)
     for (int d = 0; d < (p.dim == 2 ? 2 : 3); d++)
-        if ((int)std::ceil((maxR + margin) / P.cw[d]) > 1) return *msg = "cell width below the neighbour radius", DMPH_EINVAL;
+        if ((int)std::ceil(cell_r / P.cw[d]) > 1) return *msg = "cell width below the neighbour radius", DMPH_EINVAL;
     P.rc2 = (maxR + margin) * (maxR + margin);
     P.RA2 = P.RA * P.RA;
     P.RG2 = P.RG * P.RG;

@@ -494,7 +494,19 @@ __global__ void k_copy_chunks(const Chunk *__restrict__ tmp, Chunk *__restrict__
 // velocity) sets the sticky B_NONFINITE flag, and no rebuild runs while it is
 // set: positions become cell indices only in the rebuild, so every index the
 // other kernels use stays the last finite rebuild's.
-__device__ __forceinline__ int decide(const unsigned long long *maxshift, double threshold, int *dB)
+// The reference's trigger (:1264-1286) on the largest displacement since the
+// last rebuild.  Without list reuse (maxshiftL null) every trigger is a full
+// rebuild (returns 1).  With it, a trigger keeps the lists (returns 2: the
+// trigger positions and neighbour counts are refreshed, no sort) while every
+// particle has moved less than S/2 - MARGIN/2 since the lists were built
+// (S: their skin past MaxRadius): until the next trigger, which comes before
+// any particle moves MARGIN/2 further, every pair within MaxRadius + MARGIN
+// then stays within MaxRadius + S of the list-time positions.  A full rebuild
+// picks the skin of its lists from the steps since the previous trigger
+// (0.4 dx when triggers come every step or two, 0.2 dx up to every fourth
+// step, MARGIN otherwise), MARGIN after a list overflow.
+__device__ __forceinline__ int decide(const unsigned long long *maxshift, double threshold, int *dB,
+                                     const unsigned long long *maxshiftL = nullptr, double dx = 0.0)
 {
     const unsigned long long bits = *maxshift;
     if (bits >= 0x7FF0000000000000ull || dB[B_NONFINITE]) {
@@ -503,21 +515,39 @@ __device__ __forceinline__ int decide(const unsigned long long *maxshift, double
         return 0;
     }
     const double m2 = __longlong_as_double((long long)bits);
-    const int need = m2 > threshold ? 1 : 0;
+    if (!(m2 > threshold)) {
+        dB[B_NEED] = 0;
+        dB[B_GAP] += 1;
+        return 0;
+    }
+    int need = 1;
+    const int gap = dB[B_GAP] + 1;
+    dB[B_GAP] = 0;
+    if (maxshiftL) {
+        const double mL = __longlong_as_double((long long)*maxshiftL);
+        const int h = dB[B_SKIN] > 10 ? dB[B_SKIN] : 10;
+        // the FP32 displacements carry a few 1e-7 dx of rounding: 1e-3 dx of slack
+        const double lim = (0.005 * h - 0.05 - 0.001) * dx;
+        if (!dB[B_LIST_OVF] && lim > 0.0 && mL < lim * lim) need = 2;
+        if (need == 1) dB[B_SKIN_NEXT] = dB[B_LIST_OVF] ? 10 : gap <= 2 ? kSkinMaxHundredths : gap <= 4 ? 20 : 10;
+    }
     dB[B_NEED] = need;
-    dB[B_REBUILDS] += need;
+    dB[B_REBUILDS] += 1;
+    if (need == 1) dB[B_LIST_BUILDS] += 1;
     return need;
 }
-__global__ void k_decide(const unsigned long long *maxshift, double threshold, int *dB)
+__global__ void k_decide(const unsigned long long *maxshift, double threshold, int *dB,
+                         const unsigned long long *maxshiftL, double dx)
 {
-    decide(maxshift, threshold, dB);
+    decide(maxshift, threshold, dB, maxshiftL, dx);
 }
-// same, inside a CUDA graph: also sets the condition of the graph's rebuild node
+// same, inside a CUDA graph: also sets the condition of the graph's rebuild
+// node (the full rebuild)
 __global__ void k_decide_graph(const unsigned long long *maxshift, double threshold, int *dB,
-                               cudaGraphConditionalHandle cond)
+                               cudaGraphConditionalHandle cond, const unsigned long long *maxshiftL, double dx)
 {
-    const int need = decide(maxshift, threshold, dB);
-    cudaGraphSetConditional(cond, need ? 1u : 0u);
+    const int need = decide(maxshift, threshold, dB, maxshiftL, dx);
+    cudaGraphSetConditional(cond, need == 1 ? 1u : 0u);
 }
 
 // The decisions of every scene of an ensemble (thread k: scene k), with the
@@ -540,14 +570,14 @@ void launch_ens_decide(const EnsScene *tab, int ns, const unsigned long long *ha
 }
 
 void launch_decide(const DevParams &P, const unsigned long long *maxshift, int *dB, unsigned long long graph_cond,
-                   cudaStream_t st)
+                   cudaStream_t st, const unsigned long long *maxshiftL)
 {
     const double margin = (0.1 * P.dx);
     const double thr = 0.5 * margin * 0.5 * margin;  // :1278
     if (graph_cond)
-        k_decide_graph<<<1, 1, 0, st>>>(maxshift, thr, dB, (cudaGraphConditionalHandle)graph_cond);
+        k_decide_graph<<<1, 1, 0, st>>>(maxshift, thr, dB, (cudaGraphConditionalHandle)graph_cond, maxshiftL, P.dx);
     else
-        k_decide<<<1, 1, 0, st>>>(maxshift, thr, dB);
+        k_decide<<<1, 1, 0, st>>>(maxshift, thr, dB, maxshiftL, P.dx);
 }
 
 void launch_bounds(const DevParams &P, const int *start, const int *offs, const int *total, int *dB, cudaStream_t st)

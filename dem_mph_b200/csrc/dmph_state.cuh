@@ -42,6 +42,8 @@ struct DevState {
     // the pressure of the last pass A (0 for solids and for walls without
     // fluid in reach), read by pass B together with the velocity
     float4 *p4, *v4, *f4, *xref4, *gc4;
+    // list reuse: positions (FP32 frame) when the current lists were built
+    float4 *xrefL4;
     float *pres32, *vsp32, *div32, *densA32, *pA32;
     float *alpha32, *dragC32;
     // rigid clumps (DMPH_FLAG_RIGID_CLUMPS): body of each slot (-1: none) and

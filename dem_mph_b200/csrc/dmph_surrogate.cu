@@ -949,6 +949,10 @@ extern "C" int dmph_surrogate_enable(dmph_ctx *ctx, const dmph_surrogate_params 
         ctx->err = "the surrogate runs on the FP32 split build";
         return DMPH_EINVAL;
     }
+    if (ctx->list_reuse) {
+        ctx->err = "the surrogate does not run with list reuse (DMPH_FLAG_LIST_REUSE)";
+        return DMPH_EINVAL;
+    }
     if (prm->substeps < 1 || prm->check_interval < 1 || prm->batch < 8192 || prm->batch % 8192 ||
         prm->pool_rows < prm->batch || !(prm->tolerance > 0) || prm->fallback_blocks < 1) {
         ctx->err = "surrogate parameters out of range (batch a multiple of 8192, pool >= batch)";

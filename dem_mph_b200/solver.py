@@ -49,6 +49,7 @@ def lib():
         L.dmph_get_global_sums.argtypes = [vp, vp]
         L.dmph_get_list_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
         L.dmph_set_bodies.argtypes = [vp, C.c_int, vp, vp]
+        L.dmph_get_rebuild_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.dmph_checkpoint_write.argtypes = [vp, C.c_char_p, vp, C.c_int]
         L.dmph_checkpoint_open.argtypes = [C.c_char_p, C.POINTER(vp), vp, C.c_int, C.POINTER(C.c_int)]
         L.dmph_get_bodies.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
@@ -259,6 +260,13 @@ class Solver:
         inf = Info()
         self._check(lib().dmph_get_info(self._h, C.byref(inf)))
         return inf
+
+    def rebuild_stats(self):
+        """(rebuild triggers, full rebuilds with cell sort and lists) since
+        creation (dmph_get_rebuild_stats; equal without list reuse)"""
+        a, b = C.c_int64(), C.c_int64()
+        self._check(lib().dmph_get_rebuild_stats(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def neighbor_list(self):
         ptr = np.empty(self.n + 1, np.int64)

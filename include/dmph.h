@@ -63,6 +63,10 @@ extern "C" {
 #define DMPH_FLAG_WALL_DEM_COEFFS (1u << 2) /* also compute the (output-only) DEM constants of wall particles */
 #define DMPH_FLAG_RIGID_CLUMPS (1u << 3)    /* debris bodies move as rigid clumps (no reference counterpart) */
 #define DMPH_FLAG_ALL_NEIGHBOR_COUNTS (1u << 4) /* keep NeighborCount for every particle (VTK "neighbor") */
+/* FP32 split build, Verlet lists: keep the lists across the reference's
+ * rebuild triggers while they stay valid (no reference counterpart; see
+ * dmph_get_rebuild_stats) */
+#define DMPH_FLAG_LIST_REUSE (1u << 5)
 
 /*
  * Simulation parameters: the keywords of dem.data
@@ -314,6 +318,28 @@ int dmph_get_global_sums(dmph_ctx *ctx, double sums[DMPH_SUM_COUNT]);
  * pointer may be NULL; all read 0 in stencil mode.
  */
 int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64_t *entries_pass_b, int32_t *overflowed);
+
+/*
+ * List reuse (DMPH_FLAG_LIST_REUSE, FP32 split build with Verlet lists, walls
+ * at rest, debris as rigid bodies or none, without
+ * DMPH_FLAG_ALL_NEIGHBOR_COUNTS; otherwise the flag only widens the cells).  The reference rebuilds at every
+ * trigger of its displacement test (neighborCalculation :1264-1286): cell
+ * sort, NeighborInd, and the neighbour counts the drag terms read.  With the
+ * flag, the cells are 0.4 dx wider than MaxRadius + MARGIN and each list is
+ * built with a skin S of 0.1, 0.2 or 0.4 dx past MaxRadius (chosen on the
+ * device from how many steps lay between the last two triggers: a wide skin
+ * when the triggers come every step or two).  Every trigger still resets the
+ * trigger positions and recounts NeighborCount and SolidNeighborCount within
+ * MaxRadius + MARGIN (from the lists, on the FP64 positions); the cell sort
+ * and the lists are remade only when some particle has moved more than
+ * S/2 - MARGIN/2 since the lists were built, so that until the next trigger
+ * (which comes before any particle moves MARGIN/2 further) every pair within
+ * MaxRadius + MARGIN is in the lists.  The physics is the reference's; the
+ * order of a cell's particles, and so the order of the neighbour sums, is
+ * that of the last sort.  *triggers counts the reference's rebuilds (as
+ * dmph_info.rebuilds), *list_builds the cell sorts and list builds among them.
+ */
+int dmph_get_rebuild_stats(dmph_ctx *ctx, int64_t *triggers, int64_t *list_builds);
 
 /*
  * Rigid debris bodies (no counterpart in the reference, whose debris particles
