@@ -216,8 +216,12 @@ def reference_rate(res, n, steps, rebuild_fraction):
 # list-mode kernels on config 2, FP32 split, late in the flow (after 6,000
 # steps), from ncu captures of the bench's own command
 TRAFFIC_CONFIG2_FP32 = {"pass_a": 765.5e6, "pass_b": 690.9e6, "list_build": 824.2e6}
-# the same with list reuse (lists with a skin of up to 0.4 dx); empty until captured
-TRAFFIC_CONFIG2_FP32_REUSE = {}
+# DRAM bytes per launch of the ensemble's shared pass launches on config 3
+# (one launch each, after the bench's settle steps); empty until captured
+TRAFFIC_CONFIG3 = {}
+TRAFFIC_SOURCE_CONFIG3 = "ncu capture of one launch of each ensemble pass kernel on config 3"
+# the same with list reuse (lists with a skin of up to 0.4 dx, cells 3.5 dx)
+TRAFFIC_CONFIG2_FP32_REUSE = {"pass_a": 959.6e6, "pass_b": 868.4e6, "list_build": 1064.7e6}
 TRAFFIC_SOURCE = "ncu capture of one launch of the same kernel and workload in the late flow"
 
 
@@ -628,6 +632,31 @@ def run_ensemble(args, rank, world):
     peaks, peak_src = load_peaks()
     bpp = algorithmic_bytes("fp32")
     achieved = n * bpp / (ms_max / args.steps / 1e3) / 1e9
+    # per-kernel device times of the two shared pass launches (events around
+    # each, no graph replay) over the next steps
+    prof_steps = min(args.steps, 50)
+    ens.set_profiling(True)
+    ens.step(prof_steps)
+    ph = ens.phase_times()
+    ens.set_profiling(False)
+    n_fs = int(sum(s.counts()["fluid"] + s.counts()["solid"] for s in sc))
+    kern, top = kernel_table(ph, "fp32", n, n_fs, 0, prof_steps, 0)
+    ens_names = {"pass_a": "k_ens_pass_list<false>", "pass_b": "k_ens_pass_list<true>"}
+    if top is not None:
+        k = kern[top]
+        ach_k = k["bytes"] / (k["launch_ms"] / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": ens_names[top], "achieved": ach_k, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": ach_k / peaks["hbm_gbs"], "traffic": TRAFFIC_CONFIG3.get(top),
+                "traffic_source": TRAFFIC_SOURCE_CONFIG3 if TRAFFIC_CONFIG3.get(top) else None,
+                "peak_source": peak_src, "launch_ms": k["launch_ms"], "algorithmic_bytes_per_launch": k["bytes"],
+                "kernels": {name: {"kernel": ens_names[name], "launch_ms": v["launch_ms"],
+                                   "achieved_gbs": v["bytes"] / (v["launch_ms"] / 1e3) / 1e9,
+                                   "traffic": TRAFFIC_CONFIG3.get(name)} for name, v in kern.items()},
+                "whole_step": {"achieved_gbs": achieved, "frac": achieved / peaks["hbm_gbs"],
+                               "algorithmic_bytes_per_step": n * bpp}}
+    else:
+        roof = {"bound": "hbm", "kernel": "whole ensemble step", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peak_src}
     # end to end: per step, upload every scene's state from pinned host memory,
     # one ensemble step, read every scene's state back
     host = []
@@ -663,9 +692,7 @@ def run_ensemble(args, rank, world):
                    "parallelism": "replicas x%d" % world,
                    "l2": "inputs larger than L2 (particle state alone %.0f MB)" % (n * 60 / 1e6)},
         "clocks": clk.summary(),
-        "roofline": {"bound": "hbm", "kernel": "whole ensemble step", "achieved": achieved,
-                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                     "traffic": None, "peak_source": peak_src},
+        "roofline": roof,
         "cpu_baseline": None,
         "e2e": {"value": n * world * e2e_steps / e2e_max, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": int(n * 48), "d2h_bytes_per_step": int(n * 56), "steps": e2e_steps},

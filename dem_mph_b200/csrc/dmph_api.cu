@@ -1626,6 +1626,11 @@ struct dmph_ensemble {
     int total_bodies = 0;
     int *bpre = nullptr;                    // device: prefix of the scenes' body counts
     unsigned long long *handles = nullptr;  // device: the IF-node conditions of the recorded step
+    // per-phase timing of the ensemble passes (dmph_ensemble_set_profiling)
+    bool prof = false;
+    cudaEvent_t pe0 = nullptr, pe1 = nullptr;
+    double phase_ms[DMPH_PHASE_COUNT] = {0};
+    long long phase_n[DMPH_PHASE_COUNT] = {0};
 };
 
 #define EK(call)                                                                          \
@@ -1658,10 +1663,12 @@ static void ens_release(dmph_ensemble *e)
     if (e->join) cudaEventDestroy(e->join);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->pe0) cudaEventDestroy(e->pe0);
+    if (e->pe1) cudaEventDestroy(e->pe1);
     if (e->st) cudaStreamDestroy(e->st);
     e->tab = nullptr;
     e->fork.clear();
-    e->join = e->ev0 = e->ev1 = nullptr;
+    e->join = e->ev0 = e->ev1 = e->pe0 = e->pe1 = nullptr;
     e->st = nullptr;
 }
 
@@ -1703,6 +1710,8 @@ extern "C" int dmph_ensemble_create(dmph_ctx *const *scenes, int nscenes, dmph_e
     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking);
     if (ce == cudaSuccess) ce = cudaEventCreate(&e->ev0);
     if (ce == cudaSuccess) ce = cudaEventCreate(&e->ev1);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e->pe0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e->pe1);
     if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->join, cudaEventDisableTiming);
     e->fork.assign(nscenes, nullptr);
     for (int k = 0; ce == cudaSuccess && k < nscenes; ++k)
@@ -1747,17 +1756,42 @@ extern "C" int dmph_ensemble_create(dmph_ctx *const *scenes, int nscenes, dmph_e
 }
 
 // the pair passes of all scenes: one persistent launch each
+// profiling (never inside a graph): events around a phase on the ensemble
+// stream, accumulated into phase k
+static void ens_phase_begin(dmph_ensemble *e)
+{
+    if (e->prof) cudaEventRecord(e->pe0, e->st);
+}
+static void ens_phase_end(dmph_ensemble *e, int k)
+{
+    if (!e->prof) return;
+    cudaEventRecord(e->pe1, e->st);
+    cudaEventSynchronize(e->pe1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e->pe0, e->pe1);
+    e->phase_ms[k] += ms;
+    e->phase_n[k] += 1;
+}
+
 static void ens_enqueue_passes(dmph_ensemble *e)
 {
     const int ns = (int)e->scenes.size();
     if (e->use_list) {
+        ens_phase_begin(e);
         launch_ens_pass_list(e->tab, ns, false, e->st);
         launch_ens_pass_a32(e->tab, ns, e->var_a, e->st, 1);
+        ens_phase_end(e, 2);
+        ens_phase_begin(e);
         launch_ens_pass_list(e->tab, ns, true, e->st);
         launch_ens_pass_b32(e->tab, ns, e->var_b, e->st, 1);
+        ens_phase_end(e, 3);
     } else {
+        ens_phase_begin(e);
         launch_ens_pass_a32(e->tab, ns, e->var_a, e->st);
+        ens_phase_end(e, 2);
+        ens_phase_begin(e);
         launch_ens_pass_b32(e->tab, ns, e->var_b, e->st);
+        ens_phase_end(e, 3);
     }
     launch_ens_fluid_accel32(e->tab, ns, e->st);
 }
@@ -1885,7 +1919,7 @@ static long long ens_step_launches(const dmph_ensemble *e)
 
 static bool ens_graph_usable(const dmph_ensemble *e)
 {
-    if (!e->use_graph) return false;
+    if (!e->use_graph || e->prof) return false;
     for (const dmph_ctx *c : e->scenes)
         if (c->prof || !(0.0 < c->time) || in_wall_window(c)) return false;
     return true;
@@ -2034,6 +2068,27 @@ extern "C" int dmph_ensemble_info(dmph_ensemble *e, int64_t *kernel_launches, in
 extern "C" const char *dmph_ensemble_last_error(dmph_ensemble *e)
 {
     return e ? e->err.c_str() : "null ensemble";
+}
+
+extern "C" int dmph_ensemble_set_profiling(dmph_ensemble *e, int enable)
+{
+    if (!e) return DMPH_EINVAL;
+    e->prof = enable != 0;
+    for (int k = 0; k < DMPH_PHASE_COUNT; k++) {
+        e->phase_ms[k] = 0.0;
+        e->phase_n[k] = 0;
+    }
+    return DMPH_OK;
+}
+
+extern "C" int dmph_ensemble_get_phase_times(dmph_ensemble *e, double *ms, int64_t *launches, int n)
+{
+    if (!e || n < 0) return DMPH_EINVAL;
+    for (int k = 0; k < n && k < DMPH_PHASE_COUNT; k++) {
+        if (ms) ms[k] = e->phase_ms[k];
+        if (launches) launches[k] = e->phase_n[k];
+    }
+    return DMPH_OK;
 }
 
 extern "C" int dmph_ensemble_destroy(dmph_ensemble *e)

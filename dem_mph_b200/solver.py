@@ -66,6 +66,8 @@ def lib():
         L.dmph_ensemble_autotune.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp, vp]
         L.dmph_ensemble_set_graph.argtypes = [vp, C.c_int]
         L.dmph_ensemble_info.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.dmph_ensemble_set_profiling.argtypes = [vp, C.c_int]
+        L.dmph_ensemble_get_phase_times.argtypes = [vp, vp, vp, C.c_int]
         L.dmph_ensemble_last_error.argtypes = [vp]
         L.dmph_ensemble_last_error.restype = C.c_char_p
         L.dmph_ensemble_destroy.argtypes = [vp]
@@ -468,6 +470,17 @@ class Ensemble:
 
     def set_graph(self, on=True):
         self._check(lib().dmph_ensemble_set_graph(self._h, 1 if on else 0))
+
+    def set_profiling(self, on=True):
+        """CUDA events around the ensemble passes (dmph_ensemble_set_profiling)"""
+        self._check(lib().dmph_ensemble_set_profiling(self._h, 1 if on else 0))
+
+    def phase_times(self):
+        """{phase: (total ms, launches)} of the timed phases (pass_a, pass_b)"""
+        ms = np.zeros(7)
+        n = np.zeros(7, np.int64)
+        self._check(lib().dmph_ensemble_get_phase_times(self._h, _ptr(ms), _ptr(n), 7))
+        return {name: (float(ms[k]), int(n[k])) for k, name in ((2, "pass_a"), (3, "pass_b")) if n[k] > 0}
 
     def info(self):
         n, s = C.c_int64(), C.c_int64()

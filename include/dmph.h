@@ -449,6 +449,11 @@ int dmph_ensemble_step_timed(dmph_ensemble *e, int nsteps, float *device_ms);
 int dmph_ensemble_autotune(dmph_ensemble *e, int *variant_a, int *variant_b, float *ms_a, float *ms_b);
 int dmph_ensemble_set_graph(dmph_ensemble *e, int enable);
 int dmph_ensemble_info(dmph_ensemble *e, int64_t *kernel_launches, int64_t *steps);
+/* Per-phase device timing of the ensemble's shared launches (no graph replay
+ * while on): phase 2 = pass A of all scenes, 3 = pass B of all scenes, in the
+ * indexing of dmph_get_phase_times; other phases read 0. */
+int dmph_ensemble_set_profiling(dmph_ensemble *e, int enable);
+int dmph_ensemble_get_phase_times(dmph_ensemble *e, double *ms, int64_t *launches, int n);
 const char *dmph_ensemble_last_error(dmph_ensemble *e);
 int dmph_ensemble_destroy(dmph_ensemble *e); /* NULL: nothing to do, returns 0 */
 

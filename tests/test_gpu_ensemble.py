@@ -138,3 +138,26 @@ def test_ensemble_rejects_fp64_and_duplicates():
         g.autotune()
     g.close()
     h.close()
+
+
+def test_ensemble_profiling_times_the_passes_and_changes_nothing():
+    """phase times of the shared pass launches, one pass A and one pass B
+    per step, and the same bits as graph replay"""
+    items = scene_list(RIGID)
+    a, b = make(items), make(items)
+    ea, eb = solver.Ensemble(a), solver.Ensemble(b)
+    ea.step(5)
+    eb.step(5)
+    ea.set_profiling(True)
+    ea.step(12)
+    eb.step(12)
+    ph = ea.phase_times()
+    assert set(ph) == {"pass_a", "pass_b"} and ph["pass_a"][1] == 12 and ph["pass_b"][1] == 12
+    assert ph["pass_a"][0] > 0 and ph["pass_b"][0] > 0
+    ea.set_profiling(False)
+    for x, y in zip(a, b):
+        assert same_state(x, y)
+    ea.close()
+    eb.close()
+    for g in a + b:
+        g.close()
