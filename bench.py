@@ -622,9 +622,13 @@ def run_ensemble(args, rank, world):
     barrier()
     torch.cuda.synchronize()
     l0 = ens.info()["kernel_launches"] + sum(g.info().kernel_launches for g in sv)
+    if args.profiler_range:
+        torch.cuda.profiler.start()
     with ClockSampler(torch.cuda.current_device()) as clk:
         ms = ens.step_timed(args.steps)
         torch.cuda.synchronize()
+    if args.profiler_range:
+        torch.cuda.profiler.stop()
     barrier()
     launches = ens.info()["kernel_launches"] + sum(g.info().kernel_launches for g in sv) - l0
     ms_max = max_over_ranks(ms, world, "cuda")
