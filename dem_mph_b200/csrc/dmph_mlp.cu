@@ -18,8 +18,16 @@
 //   EPI_BWD_RELU  gradient through ReLU (mask from the stored activation),
 //                 BF16 row-major and transposed
 //   EPI_WGRAD     split-K weight gradient, atomically added in FP32
+// The forward pass of a surrogate call runs instead as one fused kernel
+// (k_mlp_fwd): persistent CTAs keep all four weight matrices in shared memory,
+// the feature tiles arrive by TMA (cp.async.bulk.tensor, double-buffered, the
+// next tile's copy in flight while the current one is computed), and each
+// layer's tcgen05 accumulator goes through TMEM into shared memory as the
+// next layer's operand, so no activation touches HBM.
 // No CPU fallback exists; the host side is in dmph_surrogate.cu.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include "dmph_internal.h"
 #include "dmph_mlp.h"
@@ -263,6 +271,220 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tn(GemmArgs g)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
 }
 
+
+// ------------------------------------------------------------ fused forward
+namespace {
+
+// shared memory of k_mlp_fwd (bytes from a 1024-aligned base).  Weights in
+// the canonical no-swizzle K-major layout of stage_chunk over their whole K
+// (core matrices 128 B apart along K, 8-row groups K*16 B apart); the
+// feature tiles and the activations in the layout the TMA box {8 columns,
+// 128 rows} writes: K-slice s (8 columns) at s*2048, row r at
+// (r/8)*128 + (r%8)*16 inside it (core matrices 2048 B apart along K, 8-row
+// groups 128 B apart)
+constexpr int kFwdThreads = 128;
+constexpr int kW1 = 0;                        // 128 x 64
+constexpr int kW2 = kW1 + 128 * 64 * 2;       // 128 x 128
+constexpr int kW3 = kW2 + 128 * 128 * 2;      // 128 x 128
+constexpr int kW4 = kW3 + 128 * 128 * 2;      // 16 x 128
+constexpr int kX0 = kW4 + 16 * 128 * 2;       // two 128 x 64 feature tiles
+constexpr int kXBytes = 128 * 64 * 2;
+constexpr int kHa = kX0 + 2 * kXBytes;        // 128 x 128 activations
+constexpr int kBias = kHa + 128 * 128 * 2;    // 3 x 128 + 16 biases
+constexpr int kBiasCount = 3 * 128 + 16;
+constexpr int kBarOff = kBias + kBiasCount * 4;  // full[2], mma
+constexpr int kFwdSmem = kBarOff + 64;
+static_assert(kX0 % 128 == 0 && kHa % 128 == 0 && kBarOff % 8 == 0, "alignment of the fused MLP's buffers");
+
+struct FwdArgs {
+    const __nv_bfloat16 *w[kMlpLayers];  // [out][in], BF16
+    const float *b[kMlpLayers];
+    float *Y;  // [n][kMlpOut]
+    long long n;
+    int *err;
+};
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// one box {8 columns, 128 rows} of the feature matrix at column x (a
+// multiple of 8: 16-byte aligned) and row y into shared memory
+__device__ __forceinline__ void tma_box(uint32_t dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(dst),
+        "l"((unsigned long long)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// feature tile t (rows t*128 .. t*128+127, zero past n) into buffer b
+__device__ __forceinline__ void issue_tile(uint8_t *smem, const CUtensorMap *map, long long t, int b, uint64_t *full)
+{
+    mbar_expect_tx(&full[b], kXBytes);
+    const uint32_t dst = smem_u32(smem + kX0 + b * kXBytes);
+    for (int sl = 0; sl < kMlpIn / 8; ++sl) tma_box(dst + sl * 2048, map, sl * 8, (int)(t * 128), &full[b]);
+}
+
+// hidden-layer epilogue: bias and ReLU of this thread's row of the
+// accumulator, BF16 into the activation buffer (the next layer's A operand)
+__device__ __forceinline__ void epi_hidden(uint32_t tmem, int warp, int lane, const float *bias, uint8_t *H)
+{
+    const int r = warp * 32 + lane;
+    uint8_t *row = H + (r >> 3) * 128 + (r & 7) * 16;
+    for (int c0 = 0; c0 < kMlpHidden; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+        __align__(16) __nv_bfloat16 hb[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) hb[i] = __float2bfloat16_rn(fmaxf(v[i] + bias[c0 + i], 0.f));
+        *reinterpret_cast<uint4 *>(row + (c0 >> 3) * 2048) = reinterpret_cast<const uint4 *>(hb)[0];
+        *reinterpret_cast<uint4 *>(row + ((c0 >> 3) + 1) * 2048) = reinterpret_cast<const uint4 *>(hb)[1];
+    }
+}
+
+}  // namespace
+
+// Y = MLP(X) for n rows: persistent CTAs over 128-row tiles.  Thread 0
+// issues the TMA copies and the MMAs; all four warps run the epilogues (warp
+// w reads TMEM lanes 32w..32w+31, its tile rows).  Every wait is bounded; on
+// a time-out the kernel sets *err, waits (bounded) for its copies and MMAs in
+// flight, frees its TMEM and returns.
+__global__ void __launch_bounds__(kFwdThreads, 1) k_mlp_fwd(const __grid_constant__ CUtensorMap map, FwdArgs a)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + kBarOff);
+    uint64_t *mbar = full + 2;
+    float *bias = reinterpret_cast<float *>(smem + kBias);
+    __shared__ uint32_t tmem_base_s;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long tiles = (a.n + 127) / 128;
+    if ((long long)blockIdx.x >= tiles) return;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                     "r"(128));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // weights and biases, once per CTA
+    stage_chunk(smem + kW1, a.w[0], kMlpIn, 0, kMlpHidden, kMlpHidden, 0, kMlpIn, kMlpIn);
+    stage_chunk(smem + kW2, a.w[1], kMlpHidden, 0, kMlpHidden, kMlpHidden, 0, kMlpHidden, kMlpHidden);
+    stage_chunk(smem + kW3, a.w[2], kMlpHidden, 0, kMlpHidden, kMlpHidden, 0, kMlpHidden, kMlpHidden);
+    stage_chunk(smem + kW4, a.w[3], kMlpHidden, 0, kMlpOut, kMlpOut, 0, kMlpHidden, kMlpHidden);
+    for (int i = threadIdx.x; i < kBiasCount; i += blockDim.x)
+        bias[i] = i < 384 ? a.b[i >> 7][i & 127] : a.b[3][i - 384];
+    fence_async_smem();
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = tmem_base_s;
+    const uint32_t id_h = instr_desc(128, kMlpHidden), id_o = instr_desc(128, kMlpOut);
+    const uint32_t w1 = smem_u32(smem + kW1), w2 = smem_u32(smem + kW2), w3 = smem_u32(smem + kW3),
+                   w4 = smem_u32(smem + kW4), ha = smem_u32(smem + kHa);
+    uint32_t ph_full[2] = {0u, 0u}, ph_mma = 0u;
+    bool pend_full[2] = {false, false}, pend_mma = false;  // thread 0: copies / MMAs in flight
+    bool ok = true;
+    long long t = blockIdx.x;
+    if (threadIdx.x == 0) {
+        issue_tile(smem, &map, t, 0, full);
+        pend_full[0] = true;
+    }
+    // one layer: MMAs over K (16 per instruction) from A (activation layout,
+    // or the feature tile) and B (weights), then every thread waits for them
+    auto layer = [&](uint32_t a_addr, uint32_t b_addr, int K, uint32_t idesc) -> bool {
+        if (threadIdx.x == 0) {
+            fence_after_sync();
+            for (int j = 0; j < K / 16; ++j) {
+                const uint64_t da = smem_desc(a_addr + j * 4096, 2048, 128);
+                const uint64_t db = smem_desc(b_addr + j * 256, 128, K * 16);
+                mma_bf16(tmem, da, db, idesc, j > 0 ? 1u : 0u);
+            }
+            mma_commit(mbar);
+            pend_mma = true;
+        }
+        const bool done = __syncthreads_and(mbar_wait(mbar, ph_mma)) != 0;
+        ph_mma ^= 1u;
+        if (done && threadIdx.x == 0) pend_mma = false;
+        fence_after_sync();
+        return done;
+    };
+    for (int i = 0; t < tiles; ++i, t += gridDim.x) {
+        const int b = i & 1;
+        const long long tn = t + gridDim.x;
+        // the other buffer was read by the previous tile's first layer, whose
+        // MMAs have completed
+        if (threadIdx.x == 0 && tn < tiles) {
+            issue_tile(smem, &map, tn, b ^ 1, full);
+            pend_full[b ^ 1] = true;
+        }
+        // (only thread 0 waits on the copies; its parities advance on success)
+        bool got = true;
+        if (threadIdx.x == 0) {
+            got = mbar_wait(&full[b], ph_full[b]);
+            if (got) {
+                pend_full[b] = false;
+                ph_full[b] ^= 1u;
+            }
+        }
+        ok = __syncthreads_and(got) != 0;
+        if (!ok) break;
+        ok = layer(smem_u32(smem + kX0 + b * kXBytes), w1, kMlpIn, id_h);
+        if (!ok) break;
+        epi_hidden(tmem, warp, lane, bias, smem + kHa);
+        fence_async_smem();
+        fence_before_sync();
+        __syncthreads();
+        ok = layer(ha, w2, kMlpHidden, id_h);
+        if (!ok) break;
+        epi_hidden(tmem, warp, lane, bias + 128, smem + kHa);
+        fence_async_smem();
+        fence_before_sync();
+        __syncthreads();
+        ok = layer(ha, w3, kMlpHidden, id_h);
+        if (!ok) break;
+        epi_hidden(tmem, warp, lane, bias + 256, smem + kHa);
+        fence_async_smem();
+        fence_before_sync();
+        __syncthreads();
+        ok = layer(ha, w4, kMlpHidden, id_o);
+        if (!ok) break;
+        {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), v);
+            const long long row = t * 128 + warp * 32 + lane;
+            if (row < a.n) {
+                float4 *dst = reinterpret_cast<float4 *>(a.Y + row * kMlpOut);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    dst[q] = make_float4(v[4 * q] + bias[384 + 4 * q], v[4 * q + 1] + bias[385 + 4 * q],
+                                         v[4 * q + 2] + bias[386 + 4 * q], v[4 * q + 3] + bias[387 + 4 * q]);
+            }
+        }
+        // the accumulator is read before the next tile's first MMA
+        fence_before_sync();
+        __syncthreads();
+    }
+    if (!ok && threadIdx.x == 0) {
+        // bounded waits for the copies and MMAs still in flight (the MMA
+        // parity advanced past the wait that gave up)
+        atomicExch(a.err, 1);
+        for (int q = 0; q < 2; ++q)
+            if (pend_full[q]) mbar_wait(&full[q], ph_full[q]);
+        if (pend_mma) mbar_wait(mbar, ph_mma ^ 1u);
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+}
+
 // column sums of a transposed BF16 matrix (one row per block): bias gradients
 __global__ void k_row_sums(const __nv_bfloat16 *__restrict__ T, long long ld, int cols, float *__restrict__ out)
 {
@@ -321,6 +543,59 @@ void launch_gemm(const GemmArgs &g, int ksplit, cudaStream_t st)
     const long long tiles = (g.M + 127) / 128;
     dim3 grid((unsigned)tiles, 1, (unsigned)(ksplit > 0 ? ksplit : 1));
     k_gemm_tn<<<grid, kThreads, kSmemBytes, st>>>(g);
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    return fn;
+}
+
+int launch_mlp_forward(const MlpParamsDev &M, const __nv_bfloat16 *X, long long n, float *Y, int *err, int sms,
+                       cudaStream_t st)
+{
+    if (n <= 0) return 0;
+    if (n > (1ll << 30) || (reinterpret_cast<uintptr_t>(X) & 15) != 0) return -1;
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+    if (!encode) return -2;
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {(cuuint64_t)kMlpIn, (cuuint64_t)n};
+    const cuuint64_t strides[1] = {(cuuint64_t)kMlpIn * sizeof(__nv_bfloat16)};
+    const cuuint32_t box[2] = {8u, 128u};
+    const cuuint32_t estr[2] = {1u, 1u};
+    if (encode(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(X), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return -3;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdSmem);
+        attr = true;
+    }
+    FwdArgs a;
+    for (int l = 0; l < kMlpLayers; ++l) {
+        a.w[l] = M.wb[l];
+        a.b[l] = M.w + M.boff[l];
+    }
+    a.Y = Y;
+    a.n = n;
+    a.err = err;
+    const long long tiles = (n + 127) / 128;
+    const int grid = (int)(tiles < sms ? tiles : sms);
+    k_mlp_fwd<<<grid, kFwdThreads, kFwdSmem, st>>>(map, a);
+    return 0;
 }
 
 void launch_row_sums(const __nv_bfloat16 *T, long long ld, int rows, int cols, float *out, cudaStream_t st)

@@ -54,6 +54,12 @@ struct MlpParamsDev {
 };
 
 void launch_gemm(const GemmArgs &g, int ksplit, cudaStream_t st);
+// Y[n][kMlpOut] = MLP(X[n][kMlpIn]) in one fused kernel (TMA-fed feature
+// tiles, weights resident in shared memory); X 16-byte aligned.  Nonzero
+// when the launch could not be prepared (the tensor map); *err is set on
+// the device when a bounded wait ran out.
+int launch_mlp_forward(const MlpParamsDev &M, const __nv_bfloat16 *X, long long n, float *Y, int *err, int sms,
+                       cudaStream_t st);
 void launch_row_sums(const __nv_bfloat16 *T, long long ld, int rows, int cols, float *out, cudaStream_t st);
 void launch_adam(const MlpParamsDev &M, float lr, int t, cudaStream_t st);
 void launch_weights_to_bf16(const MlpParamsDev &M, cudaStream_t st);

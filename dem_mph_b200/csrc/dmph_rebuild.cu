@@ -502,9 +502,10 @@ __global__ void k_copy_chunks(const Chunk *__restrict__ tmp, Chunk *__restrict__
 // (S: their skin past MaxRadius): until the next trigger, which comes before
 // any particle moves MARGIN/2 further, every pair within MaxRadius + MARGIN
 // then stays within MaxRadius + S of the list-time positions.  A full rebuild
-// picks the skin of its lists from the steps since the previous trigger
-// (0.4 dx when triggers come every step or two, 0.2 dx up to every fourth
-// step, MARGIN otherwise), MARGIN after a list overflow.
+// picks the skin of its lists from the steps since the previous trigger:
+// 0.4 dx when triggers come at most four steps apart (the longer lists then
+// cost less than the full rebuilds they save), MARGIN otherwise and after a
+// list overflow.
 __device__ __forceinline__ int decide(const unsigned long long *maxshift, double threshold, int *dB,
                                      const unsigned long long *maxshiftL = nullptr, double dx = 0.0)
 {
@@ -529,7 +530,7 @@ __device__ __forceinline__ int decide(const unsigned long long *maxshift, double
         // the FP32 displacements carry a few 1e-7 dx of rounding: 1e-3 dx of slack
         const double lim = (0.005 * h - 0.05 - 0.001) * dx;
         if (!dB[B_LIST_OVF] && lim > 0.0 && mL < lim * lim) need = 2;
-        if (need == 1) dB[B_SKIN_NEXT] = dB[B_LIST_OVF] ? 10 : gap <= 2 ? kSkinMaxHundredths : gap <= 4 ? 20 : 10;
+        if (need == 1) dB[B_SKIN_NEXT] = dB[B_LIST_OVF] ? 10 : gap <= 4 ? kSkinMaxHundredths : 10;
     }
     dB[B_NEED] = need;
     dB[B_REBUILDS] += 1;

@@ -579,8 +579,21 @@ GemmArgs gemm(const __nv_bfloat16 *A, long long lda, const __nv_bfloat16 *B, lon
     return g;
 }
 
-// forward over rows [0, n) of X (row-major [n][64]) into Y [n][16]
-void mlp_forward(Surrogate *s, const __nv_bfloat16 *X, long long n, float *Y, cudaStream_t st)
+// forward over rows [0, n) of X (row-major [n][64]) into Y [n][16]: the
+// fused kernel (dmph_mlp.cu, k_mlp_fwd)
+int mlp_forward(dmph_ctx *ctx, Surrogate *s, const __nv_bfloat16 *X, long long n, float *Y, cudaStream_t st)
+{
+    const int rc = launch_mlp_forward(s->M, X, n, Y, s->d_err, ctx->sms, st);
+    if (rc) {
+        ctx->err = "surrogate: the fused MLP's tensor map could not be made (" + std::to_string(rc) + ")";
+        return DMPH_ECUDA;
+    }
+    return DMPH_OK;
+}
+
+// the same through one GEMM per layer (the training path's forward kernels;
+// dmph_mlp_forward_layers compares the two)
+void mlp_forward_layers(Surrogate *s, const __nv_bfloat16 *X, long long n, float *Y, cudaStream_t st)
 {
     const MlpParamsDev &M = s->M;
     const __nv_bfloat16 *in = X;
@@ -735,7 +748,10 @@ int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev)
     enqueue_features(ctx, s, nullptr, st);
     const int gs = grid_slots(ctx);
     k_record_start<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->v0, s->a0, s->x0, s->orig);
-    if (judge) mlp_forward(s, s->X, s->n_rows, s->Y, st);
+    if (judge) {
+        const int rc = mlp_forward(ctx, s, s->X, s->n_rows, s->Y, st);
+        if (rc) return rc;
+    }
     CK(cudaGetLastError());
     for (int k = 0; k < s->prm.substeps; ++k) {
         const int rc = step_once(ctx);
@@ -850,7 +866,10 @@ int surrogate_block(dmph_ctx *ctx, Surrogate *s)
 {
     cudaStream_t st = ctx->st;
     enqueue_features(ctx, s, nullptr, st);
-    mlp_forward(s, s->X, s->n_fluid, s->Y, st);
+    {
+        const int rc = mlp_forward(ctx, s, s->X, s->n_fluid, s->Y, st);
+        if (rc) return rc;
+    }
     CK(cudaMemsetAsync(s->d_bad, 0, sizeof(int), st));
     const int gs = grid_slots(ctx);
     k_check_finite<<<gs, 256, 0, st>>>(ctx->dB, s->Y, 0, s->d_bad);
@@ -1146,7 +1165,8 @@ extern "C" int dmph_surrogate_set_weights(dmph_ctx *ctx, const float *w, int cou
 }
 
 // MLP on host rows (n x 64 features, FP32) -> n x 16 outputs
-extern "C" int dmph_mlp_forward(dmph_ctx *ctx, const float *X, int n, float *Y)
+// layers: through one GEMM per layer instead of the fused kernel
+static int mlp_forward_host(dmph_ctx *ctx, const float *X, int n, float *Y, bool layers)
 {
     using namespace dmph;
     Surrogate *s = need_sg(ctx);
@@ -1155,11 +1175,26 @@ extern "C" int dmph_mlp_forward(dmph_ctx *ctx, const float *X, int n, float *Y)
     std::vector<__nv_bfloat16> xb((size_t)n * kMlpIn);
     for (size_t i = 0; i < xb.size(); ++i) xb[i] = __float2bfloat16_rn(X[i]);
     CK(cudaMemcpyAsync(s->X, xb.data(), xb.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, ctx->st));
-    mlp_forward(s, s->X, n, s->Y, ctx->st);
+    if (layers) {
+        mlp_forward_layers(s, s->X, n, s->Y, ctx->st);
+    } else {
+        const int rc = mlp_forward(ctx, s, s->X, n, s->Y, ctx->st);
+        if (rc) return rc;
+    }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(Y, s->Y, sizeof(float) * (size_t)n * kMlpOut, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     return check_err(ctx, s);
+}
+
+extern "C" int dmph_mlp_forward(dmph_ctx *ctx, const float *X, int n, float *Y)
+{
+    return mlp_forward_host(ctx, X, n, Y, false);
+}
+
+extern "C" int dmph_mlp_forward_layers(dmph_ctx *ctx, const float *X, int n, float *Y)
+{
+    return mlp_forward_host(ctx, X, n, Y, true);
 }
 
 // loss and parameter gradient of one batch of host rows (n = the batch size)

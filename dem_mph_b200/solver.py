@@ -80,6 +80,7 @@ def lib():
         L.dmph_surrogate_get_weights.argtypes = [vp, vp, C.c_int]
         L.dmph_surrogate_set_weights.argtypes = [vp, vp, C.c_int]
         L.dmph_mlp_forward.argtypes = [vp, vp, C.c_int, vp]
+        L.dmph_mlp_forward_layers.argtypes = [vp, vp, C.c_int, vp]
         L.dmph_mlp_gradient.argtypes = [vp, vp, vp, C.c_int, vp, C.POINTER(C.c_float)]
         L.dmph_surrogate_features.argtypes = [vp, vp, C.POINTER(C.c_int)]
         L.dmph_write_bodies_file.argtypes = [C.c_char_p, C.c_int, C.c_int, vp, vp]
@@ -382,10 +383,13 @@ class Solver:
         w = np.ascontiguousarray(w, dtype=np.float32)
         self._check(lib().dmph_surrogate_set_weights(self._h, _ptr(w), len(w)))
 
-    def mlp_forward(self, X):
+    def mlp_forward(self, X, layers=False):
+        """the surrogate network on host rows (dmph_mlp_forward: the fused
+        kernel; layers=True: one GEMM per layer, dmph_mlp_forward_layers)"""
         X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, abi.MLP_IN)
         Y = np.zeros((len(X), abi.MLP_OUT), np.float32)
-        self._check(lib().dmph_mlp_forward(self._h, _ptr(X), len(X), _ptr(Y)))
+        fn = lib().dmph_mlp_forward_layers if layers else lib().dmph_mlp_forward
+        self._check(fn(self._h, _ptr(X), len(X), _ptr(Y)))
         return Y
 
     def mlp_gradient(self, X, T):

@@ -326,9 +326,9 @@ int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64_t *entries
  * trigger of its displacement test (neighborCalculation :1264-1286): cell
  * sort, NeighborInd, and the neighbour counts the drag terms read.  With the
  * flag, the cells are 0.4 dx wider than MaxRadius + MARGIN and each list is
- * built with a skin S of 0.1, 0.2 or 0.4 dx past MaxRadius (chosen on the
- * device from how many steps lay between the last two triggers: a wide skin
- * when the triggers come every step or two).  Every trigger still resets the
+ * built with a skin S of 0.1 or 0.4 dx past MaxRadius (chosen on the device
+ * from how many steps lay between the last two triggers: the wide skin when
+ * they come at most four steps apart).  Every trigger still resets the
  * trigger positions and recounts NeighborCount and SolidNeighborCount within
  * MaxRadius + MARGIN (from the lists, on the FP64 positions); the cell sort
  * and the lists are remade only when some particle has moved more than
@@ -517,8 +517,12 @@ int dmph_surrogate_get_stats(dmph_ctx *ctx, dmph_surrogate_stats *out);
 int dmph_surrogate_get_weights(dmph_ctx *ctx, float *w, int count);
 int dmph_surrogate_set_weights(dmph_ctx *ctx, const float *w, int count);
 /* the network on host rows: X n x 64 (FP32, rounded to BF16 on upload),
- * Y n x 16 FP32 (first 6 meaningful); n <= particle count */
+ * Y n x 16 FP32 (first 6 meaningful); n <= particle count.  The fused
+ * forward kernel of the surrogate calls (weights resident in shared memory,
+ * TMA-fed feature tiles, activations kept on chip); _layers runs the same
+ * network through one GEMM launch per layer, as training does. */
 int dmph_mlp_forward(dmph_ctx *ctx, const float *X, int n, float *Y);
+int dmph_mlp_forward_layers(dmph_ctx *ctx, const float *X, int n, float *Y);
 /* mean squared error over the first 6 outputs and the parameter gradient of
  * one batch of host rows (n = the training batch) */
 int dmph_mlp_gradient(dmph_ctx *ctx, const float *X, const float *T, int n, float *grad, float *loss);

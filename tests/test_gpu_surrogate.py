@@ -52,8 +52,41 @@ def test_mlp_forward_matches_oracle():
     g.close()
 
 
+@pytest.mark.parametrize("n", [1, 127, 3000, 30000])
+def test_fused_forward_equals_the_layer_gemms(n):
+    """the fused forward kernel (TMA-fed tiles, weights in shared memory,
+    activations through TMEM and shared memory) gives the bits of the four
+    per-layer GEMMs: the same MMAs in the same K order, the same epilogues"""
+    if n > 7000:  # more tiles than SMs: each CTA loops over several, double-buffered
+        sc = scenes.small(dx=0.01)
+        p = sc.params.copy()
+        p.precision = PRECISION_FP32_SPLIT
+        g = solver.Solver(p, sc.type, sc.x, sc.v)
+        g.enable_surrogate(batch=8192, pool_rows=1 << 17, check_interval=5)
+        assert g.n >= n
+    else:
+        g = make()
+    w = g.surrogate_weights()
+    rng = np.random.default_rng(5)
+    g.set_surrogate_weights((w + 0.05 * rng.normal(size=w.shape)).astype(np.float32))
+    X = random_rows(n, 2)
+    a = g.mlp_forward(X)
+    b = g.mlp_forward(X, layers=True)
+    assert np.array_equal(a, b), np.abs(a - b).max()
+    assert np.abs(a[:, :6]).max() > 0.05
+    g.close()
+
+
 def test_mlp_gradient_matches_oracle():
-    g = make()
+    if n > 7000:  # more tiles than SMs: each CTA loops over several, double-buffered
+        sc = scenes.small(dx=0.01)
+        p = sc.params.copy()
+        p.precision = PRECISION_FP32_SPLIT
+        g = solver.Solver(p, sc.type, sc.x, sc.v)
+        g.enable_surrogate(batch=8192, pool_rows=1 << 17, check_interval=5)
+        assert g.n >= n
+    else:
+        g = make()
     w = g.surrogate_weights()
     rng = np.random.default_rng(5)
     w = (w + 0.05 * rng.normal(size=w.shape)).astype(np.float32)
