@@ -581,8 +581,33 @@ def run_surrogate(args, rank, world):
         "surrogate_stats": st, "cpu_baseline": None, "roofline": None, "e2e": None,
         "timing": "wall clock around synchronised calls",
     }
+    # the surrogate network's forward pass alone (device time): on the rows of
+    # this run's calls, and on config 2's 1.23 M fluid and debris rows
+    peaks, peak_src = load_peaks()
+    flop_row = 2 * (64 * 128 + 128 * 128 + 128 * 128 + 128 * 16)
+    inf_b = b.info()
+
+    def mlp_line(g, rows):
+        fused = g.mlp_forward_ms(rows, reps=20)
+        layers = g.mlp_forward_ms(rows, reps=20, layers=True)
+        tf = rows * flop_row / (fused / 1e3) / 1e12
+        return {"rows": rows, "fused_ms": fused, "per_layer_gemms_ms": layers,
+                "fused_tflops": tf, "frac_of_bf16_peak": tf / (peaks["bf16_tflops"]),
+                "flop_per_row": flop_row}
+    mlp = {"workload_rows": mlp_line(b, inf_b.n_fluid + inf_b.n_solid)}
     a.close()
     b.close()
+    big = make_scene("config2", rank)
+    p2 = big.params.copy()
+    p2.precision = PRECISION_FP32_SPLIT
+    g2 = solver.Solver(p2, big.type, big.x, big.v)
+    g2.set_bodies(big.body, big.body_density)
+    g2.enable_surrogate(substeps=K)
+    inf2 = g2.info()
+    mlp["config2_rows"] = mlp_line(g2, inf2.n_fluid + inf2.n_solid)
+    g2.close()
+    mlp["peak_source"] = peak_src
+    out["mlp_forward"] = mlp
     if rank == 0:
         print(json.dumps(out))
 

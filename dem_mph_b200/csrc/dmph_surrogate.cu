@@ -1197,6 +1197,34 @@ extern "C" int dmph_mlp_forward_layers(dmph_ctx *ctx, const float *X, int n, flo
     return mlp_forward_host(ctx, X, n, Y, true);
 }
 
+// device time of the forward pass over the first n rows of the features the
+// surrogate holds (the last call's or judge's), averaged over reps runs
+extern "C" int dmph_mlp_forward_timed(dmph_ctx *ctx, int n, int reps, int layers, float *ms)
+{
+    using namespace dmph;
+    Surrogate *s = need_sg(ctx);
+    if (!s || !ms || n <= 0 || reps <= 0) return DMPH_EINVAL;
+    if (n > ctx->P.N) return DMPH_ERANGE;
+    auto run = [&]() -> int {
+        if (layers) {
+            mlp_forward_layers(s, s->X, n, s->Y, ctx->st);
+            return DMPH_OK;
+        }
+        return mlp_forward(ctx, s, s->X, n, s->Y, ctx->st);
+    };
+    int rc = run();  // warm-up
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev0, ctx->st));
+    for (int r = 0; r < reps && !rc; ++r) rc = run();
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    CK(cudaEventSynchronize(ctx->ev1));
+    if (rc) return rc;
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, ctx->ev0, ctx->ev1));
+    *ms = t / (float)reps;
+    return check_err(ctx, s);
+}
+
 // loss and parameter gradient of one batch of host rows (n = the batch size)
 extern "C" int dmph_mlp_gradient(dmph_ctx *ctx, const float *X, const float *T, int n, float *grad, float *loss)
 {

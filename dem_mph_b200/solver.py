@@ -81,6 +81,7 @@ def lib():
         L.dmph_surrogate_set_weights.argtypes = [vp, vp, C.c_int]
         L.dmph_mlp_forward.argtypes = [vp, vp, C.c_int, vp]
         L.dmph_mlp_forward_layers.argtypes = [vp, vp, C.c_int, vp]
+        L.dmph_mlp_forward_timed.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float)]
         L.dmph_mlp_gradient.argtypes = [vp, vp, vp, C.c_int, vp, C.POINTER(C.c_float)]
         L.dmph_surrogate_features.argtypes = [vp, vp, C.POINTER(C.c_int)]
         L.dmph_write_bodies_file.argtypes = [C.c_char_p, C.c_int, C.c_int, vp, vp]
@@ -391,6 +392,13 @@ class Solver:
         fn = lib().dmph_mlp_forward_layers if layers else lib().dmph_mlp_forward
         self._check(fn(self._h, _ptr(X), len(X), _ptr(Y)))
         return Y
+
+    def mlp_forward_ms(self, n, reps=20, layers=False):
+        """device ms of one forward pass over n rows of the surrogate's
+        current features (dmph_mlp_forward_timed)"""
+        ms = C.c_float()
+        self._check(lib().dmph_mlp_forward_timed(self._h, n, reps, 1 if layers else 0, C.byref(ms)))
+        return ms.value
 
     def mlp_gradient(self, X, T):
         X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, abi.MLP_IN)

@@ -523,6 +523,10 @@ int dmph_surrogate_set_weights(dmph_ctx *ctx, const float *w, int count);
  * network through one GEMM launch per layer, as training does. */
 int dmph_mlp_forward(dmph_ctx *ctx, const float *X, int n, float *Y);
 int dmph_mlp_forward_layers(dmph_ctx *ctx, const float *X, int n, float *Y);
+/* device milliseconds of one forward pass over the first n rows of the
+ * features the surrogate holds, averaged over reps (layers: the per-layer
+ * GEMMs instead of the fused kernel) */
+int dmph_mlp_forward_timed(dmph_ctx *ctx, int n, int reps, int layers, float *ms);
 /* mean squared error over the first 6 outputs and the parameter gradient of
  * one batch of host rows (n = the training batch) */
 int dmph_mlp_gradient(dmph_ctx *ctx, const float *X, const float *T, int n, float *grad, float *loss);
