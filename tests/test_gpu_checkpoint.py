@@ -14,7 +14,7 @@ import pytest
 
 from helpers import load_scene
 from dem_mph_b200 import files, scenes, solver
-from dem_mph_b200.abi import PRECISION_FP32_SPLIT
+from dem_mph_b200.abi import FLAG_LIST_REUSE, PRECISION_FP32_SPLIT
 
 pytestmark = pytest.mark.gpu
 
@@ -34,11 +34,18 @@ def _same_state(a, b):
 
 
 @pytest.mark.parametrize("build,debris", [("fp64", "free"), ("fp64", "rigid"), ("fp32", "free"),
-                                          ("fp32", "rigid"), ("fp32-graph", "rigid")])
+                                          ("fp32", "rigid"), ("fp32-graph", "rigid"), ("fp32-reuse", "rigid")])
 def test_resume_is_exact(build, debris, tmp_path):
     p, typ, x, v = load_scene("small3d")
     if build.startswith("fp32"):
         p.precision = PRECISION_FP32_SPLIT
+    if build == "fp32-reuse":
+        # list reuse, in a shear flow whose triggers come every step or two
+        p.flags |= FLAG_LIST_REUSE
+        v = np.array(v, dtype=np.float64).reshape(-1, 3).copy()
+        fl = np.asarray(typ) < 2
+        xx = np.asarray(x, dtype=np.float64).reshape(-1, 3)
+        v[fl, 0] = 1.5 + 2.0 * (xx[fl, 1] / 0.12)
     a = solver.Solver(p, typ, x, v)
     if debris == "rigid":
         s = scenes.small()
@@ -60,6 +67,10 @@ def test_resume_is_exact(build, debris, tmp_path):
         assert _same_state(a, b), k
     assert a.info().rebuilds > r0  # rebuilds after the resume are covered
     assert a.info().rebuilds == b.info().rebuilds
+    assert a.rebuild_stats() == b.rebuild_stats()
+    if build == "fp32-reuse":
+        t, l = a.rebuild_stats()
+        assert l < t  # triggers that kept their lists are covered
     if debris == "rigid":
         ba, bb = a.bodies(), b.bodies()
         for key in ("X", "V", "L", "q"):
