@@ -1080,6 +1080,68 @@ extern "C" int dmph_surrogate_collect(dmph_ctx *ctx, int nblocks)
     return DMPH_OK;
 }
 
+// the training pool's rows (features as recorded, BF16 widened to FP32;
+// targets), oldest first once the ring has wrapped
+extern "C" int dmph_surrogate_get_samples(dmph_ctx *ctx, float *X, float *T, int capacity, int *rows)
+{
+    using namespace dmph;
+    Surrogate *s = need_sg(ctx);
+    if (!s || capacity < 0 || (capacity > 0 && (!X || !T))) return DMPH_EINVAL;
+    unsigned long long cur = 0;
+    CK(cudaMemcpyAsync(&cur, s->d_cursor, sizeof(cur), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    const long long count = std::min<long long>((long long)cur, s->pool_cap);
+    const long long n = std::min<long long>(count, capacity);
+    // the ring's oldest row is at cur % cap once it has wrapped
+    const long long start = (long long)cur > s->pool_cap ? (long long)(cur % (unsigned long long)s->pool_cap) : 0;
+    std::vector<__nv_bfloat16> xb((size_t)n * kMlpIn);
+    for (long long done = 0; done < n;) {
+        const long long r0 = (start + done) % s->pool_cap;
+        const long long len = std::min(n - done, s->pool_cap - r0);
+        CK(cudaMemcpyAsync(xb.data() + done * kMlpIn, s->poolX + r0 * kMlpIn, sizeof(__nv_bfloat16) * len * kMlpIn,
+                           cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(T + done * kMlpOut, s->poolT + r0 * kMlpOut, sizeof(float) * len * kMlpOut,
+                           cudaMemcpyDeviceToHost, ctx->st));
+        done += len;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    for (size_t i = 0; i < xb.size(); ++i) X[i] = __bfloat162float(xb[i]);
+    if (rows) *rows = (int)n;
+    return DMPH_OK;
+}
+
+// append rows to the training pool's ring (features rounded to BF16), as if
+// recorded: samples from other scenes for a training corpus
+extern "C" int dmph_surrogate_add_samples(dmph_ctx *ctx, const float *X, const float *T, int n)
+{
+    using namespace dmph;
+    Surrogate *s = need_sg(ctx);
+    if (!s || n < 0 || (n > 0 && (!X || !T))) return DMPH_EINVAL;
+    if (n == 0) return DMPH_OK;
+    unsigned long long cur = 0;
+    CK(cudaMemcpyAsync(&cur, s->d_cursor, sizeof(cur), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    std::vector<__nv_bfloat16> xb((size_t)n * kMlpIn);
+    for (size_t i = 0; i < xb.size(); ++i) xb[i] = __float2bfloat16_rn(X[i]);
+    // rows beyond the capacity only overwrite earlier ones: keep the last cap
+    const long long skip = n > s->pool_cap ? n - s->pool_cap : 0;
+    for (long long done = skip; done < n;) {
+        const long long r0 = (long long)((cur + (unsigned long long)done) % (unsigned long long)s->pool_cap);
+        const long long len = std::min(n - done, s->pool_cap - r0);
+        CK(cudaMemcpyAsync(s->poolX + r0 * kMlpIn, xb.data() + done * kMlpIn, sizeof(__nv_bfloat16) * len * kMlpIn,
+                           cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(s->poolT + r0 * kMlpOut, T + done * kMlpOut, sizeof(float) * len * kMlpOut,
+                           cudaMemcpyHostToDevice, ctx->st));
+        done += len;
+    }
+    cur += (unsigned long long)n;
+    CK(cudaMemcpyAsync(s->d_cursor, &cur, sizeof(cur), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    s->pool_count = std::min<long long>((long long)cur, s->pool_cap);
+    s->st.samples = (int64_t)cur;
+    return DMPH_OK;
+}
+
 extern "C" int dmph_surrogate_train(dmph_ctx *ctx, int iters, float *loss)
 {
     dmph::Surrogate *s = need_sg(ctx);

@@ -204,6 +204,23 @@ def config2(seed=1234, dx=0.005):
                      debris_x=(0.3, 0.95), yaw=True, seed=seed, name="config2_dambreak_3d_dx5mm")
 
 
+def config4(seed=1234, n_scenes=32, dx=0.0088):
+    """Config 4 (the surrogate's training corpus): 32 seeded dam breaks of the
+    config-1 type (1.6 x 0.6 x 0.6 m tank, 8 debris cuboids of 4 particles a
+    side) at 8.8 mm, about 250k particles each, with seeded column length
+    0.35-0.45 m, height 0.25-0.35 m and debris densities 400-900 kg/m^3."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_scenes):
+        Lc = float(rng.uniform(0.35, 0.45))
+        H = float(rng.uniform(0.25, 0.35))
+        sub = int(rng.integers(1 << 30))
+        out.append(dam_break(dx=dx, tank=(1.6, 0.6, 0.6), column=(Lc, H, 0.6), n_debris=8,
+                             debris_sides=((4, 4), (4, 4), (4, 4)), debris_density=(400.0, 900.0),
+                             yaw=True, seed=sub, name="config4_scene%02d" % k))
+    return out
+
+
 def config5(seed=1234, dx=0.0035):
     """Config 5 (the surrogate's production case): 3.2 x 1.0 x 1.0 m tank at
     3.5 mm, a 0.5 x 0.35 (H) x 1.0 m column (4.09 M fluid), 1000 debris

@@ -81,6 +81,8 @@ def lib():
         L.dmph_surrogate_set_weights.argtypes = [vp, vp, C.c_int]
         L.dmph_mlp_forward.argtypes = [vp, vp, C.c_int, vp]
         L.dmph_mlp_forward_layers.argtypes = [vp, vp, C.c_int, vp]
+        L.dmph_surrogate_get_samples.argtypes = [vp, vp, vp, C.c_int, C.POINTER(C.c_int)]
+        L.dmph_surrogate_add_samples.argtypes = [vp, vp, vp, C.c_int]
         L.dmph_mlp_forward_timed.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float)]
         L.dmph_mlp_gradient.argtypes = [vp, vp, vp, C.c_int, vp, C.POINTER(C.c_float)]
         L.dmph_surrogate_features.argtypes = [vp, vp, C.POINTER(C.c_int)]
@@ -392,6 +394,21 @@ class Solver:
         fn = lib().dmph_mlp_forward_layers if layers else lib().dmph_mlp_forward
         self._check(fn(self._h, _ptr(X), len(X), _ptr(Y)))
         return Y
+
+    def surrogate_samples(self, capacity):
+        """(X [rows, 64], T [rows, 16]) of the training pool, oldest first
+        (dmph_surrogate_get_samples)"""
+        X = np.zeros((capacity, abi.MLP_IN), np.float32)
+        T = np.zeros((capacity, abi.MLP_OUT), np.float32)
+        rows = C.c_int()
+        self._check(lib().dmph_surrogate_get_samples(self._h, _ptr(X), _ptr(T), capacity, C.byref(rows)))
+        return X[:rows.value], T[:rows.value]
+
+    def surrogate_add_samples(self, X, T):
+        """append rows to the training pool (dmph_surrogate_add_samples)"""
+        X = np.ascontiguousarray(X, dtype=np.float32).reshape(-1, abi.MLP_IN)
+        T = np.ascontiguousarray(T, dtype=np.float32).reshape(-1, abi.MLP_OUT)
+        self._check(lib().dmph_surrogate_add_samples(self._h, _ptr(X), _ptr(T), len(X)))
 
     def mlp_forward_ms(self, n, reps=20, layers=False):
         """device ms of one forward pass over n rows of the surrogate's

@@ -510,6 +510,13 @@ int dmph_surrogate_params_default(dmph_surrogate_params *p);
 int dmph_surrogate_enable(dmph_ctx *ctx, const dmph_surrogate_params *p);
 int dmph_surrogate_collect(dmph_ctx *ctx, int nblocks);
 int dmph_surrogate_train(dmph_ctx *ctx, int iters, float *loss);
+/* The training pool as host rows, and rows added to it (a corpus recorded on
+ * other scenes, dem_mph_b200/corpus.py): X capacity x 64 FP32 (features,
+ * BF16 in the pool), T capacity x 16 FP32 (targets, the first 6 meaningful);
+ * get copies min(pool rows, capacity) rows, oldest first, into *rows; add
+ * appends n rows to the pool's ring (the last pool_rows of them stay). */
+int dmph_surrogate_get_samples(dmph_ctx *ctx, float *X, float *T, int capacity, int *rows);
+int dmph_surrogate_add_samples(dmph_ctx *ctx, const float *X, const float *T, int n);
 int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks);
 int dmph_surrogate_get_stats(dmph_ctx *ctx, dmph_surrogate_stats *out);
 /* parameters: weights [out][in] then biases of each layer, FP32; with w NULL
