@@ -34,7 +34,7 @@ def test_corpus_roundtrip_and_training():
     w, losses = corpus.train(sc[0], X, T, iters=300, substeps=4, batch=8192, report_every=100)
     assert len(losses) == 3 and np.all(np.isfinite(losses))
     g = corpus._solver(sc[1], 4, 1 << 14)
-    m = min(len(X), 8000)
+    m = min(len(X), g.n)  # rows of one forward call: at most the particle count
 
     def mse(weights):
         g.set_surrogate_weights(weights)
