@@ -292,6 +292,10 @@ def main():
     ap.add_argument("--substeps", type=int, default=8, help="surrogate K")
     ap.add_argument("--corpus", action="store_true",
                     help="build the config-4 training corpus, train the surrogate on it, judge it held out")
+    ap.add_argument("--save-weights", default=None, help="--corpus: write the trained weights (.npy) here")
+    ap.add_argument("--weights", default=None, help="--surrogate: start from these weights (.npy)")
+    ap.add_argument("--pretrain-iters", type=int, default=None,
+                    help="--surrogate: Adam iterations on the run's own first blocks (default 2000, 0 with --weights)")
     ap.add_argument("--corpus-scenes", type=int, default=32)
     ap.add_argument("--corpus-steps", type=int, default=4000)
     ap.add_argument("--train-iters", type=int, default=20000)
@@ -516,8 +520,10 @@ def run_surrogate(args, rank, world):
 
     wl = "config1" if args.workload == "config2" and "--workload" not in sys.argv else args.workload
     scene = make_scene(wl, rank)
-    total = max(args.steps, 2000)
     K = args.substeps
+    settle = args.settle if "--settle" in sys.argv else SETTLE_DEFAULT.get(wl, 200)
+    # the surrogate's blocks follow the settle and collection steps
+    total = max(args.steps, 2000, settle + 480 + 100 * K)
 
     def make():
         p = scene.params.copy()
@@ -548,13 +554,16 @@ def run_surrogate(args, rank, world):
     b = make()
     b.enable_surrogate(substeps=K, check_interval=50, tolerance=args.sg_tolerance, fallback_blocks=20,
                        train_iters_per_block=20)
-    settle = args.settle if "--settle" in sys.argv else SETTLE_DEFAULT.get(wl, 200)
+    if args.weights:
+        # a network trained beforehand (bench.py --corpus --save-weights)
+        b.set_surrogate_weights(np.load(args.weights))
     b.step(settle)
     nb_collect = 480 // K
     b.surrogate_collect(nb_collect)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    losses = [b.surrogate_train(200) for _ in range(10)]
+    pre = args.pretrain_iters if args.pretrain_iters is not None else (0 if args.weights else 2000)
+    losses = [b.surrogate_train(200) for _ in range(pre // 200)]
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t1
     done = settle + nb_collect * K
@@ -580,11 +589,13 @@ def run_surrogate(args, rank, world):
         "data": "synthetic (seeded dam break with debris, dem_mph_b200.scenes)",
         "config": {"workload": scene.name, "n_particles": scene.n, "substeps_K": K, "check_interval": 50,
                    "tolerance": args.sg_tolerance, "settle_steps": settle, "collect_steps": nb_collect * K,
-                   "surrogate_blocks": nblocks, "dt": dt},
+                   "surrogate_blocks": nblocks, "dt": dt, "weights": args.weights or "trained on this run",
+                   "pretrain_iters": pre},
         "plain_sim_s_per_hour": plain_rate, "speedup_vs_plain": sg_rate / plain_rate,
         "front_error_rel_travel": front_err, "front_plain_m": fa, "front_surrogate_m": fb, "front_start_m": f0,
         "debris_centroid_error_max_m": cent_err, "debris_centroid_error_rel_tank": cent_err / L,
-        "train_seconds_before_advance": t_train, "train_loss_first_last": [losses[0], losses[-1]],
+        "train_seconds_before_advance": t_train,
+        "train_loss_first_last": [losses[0], losses[-1]] if losses else None,
         "surrogate_stats": st, "cpu_baseline": None, "roofline": None, "e2e": None,
         "timing": "wall clock around synchronised calls",
     }
@@ -637,6 +648,8 @@ def run_corpus(args, rank, world):
     t1 = time.perf_counter()
     w, losses = corpus.train(sc[0], X, T, iters=args.train_iters, substeps=K, batch=262144)
     t2 = time.perf_counter()
+    if args.save_weights and rank == 0:
+        np.save(args.save_weights, w)
     held = {"config1": scenes.config1(), "config4_unseen": scenes.config4(seed=999, n_scenes=1)[0]}
     ev = {}
     for name, s in held.items():
