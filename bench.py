@@ -50,6 +50,9 @@ WINDOW = {"config2": "late flow after 7,000 settle steps: a neighbour rebuild ev
 # cannot settle thousands of steps on the host, adds its own timed neighbour
 # rebuild at this cadence.  None: no rebuild added.
 WINDOW_REBUILD_FRACTION = {"config2": 1.0, "config1": None}
+# networks trained on the config-4 corpus (bench.py --corpus --save-weights),
+# by surrogate K
+CORPUS_WEIGHTS = {8: "dem_mph_b200/weights/surrogate_config4_k8.npy"}
 # the reference arm times at most this many steps (each config-2 step takes
 # seconds on the host); fewer than requested are reported as such
 REFERENCE_MAX_STEPS, REFERENCE_MAX_WARMUP = 30, 5
@@ -293,7 +296,10 @@ def main():
     ap.add_argument("--corpus", action="store_true",
                     help="build the config-4 training corpus, train the surrogate on it, judge it held out")
     ap.add_argument("--save-weights", default=None, help="--corpus: write the trained weights (.npy) here")
-    ap.add_argument("--weights", default=None, help="--surrogate: start from these weights (.npy)")
+    ap.add_argument("--weights", default=None,
+                    help="--surrogate: start from these weights (.npy; default for K = 8: the config-4 corpus network)")
+    ap.add_argument("--online-only", action="store_true",
+                    help="--surrogate: no corpus network, train on the run's own first blocks only")
     ap.add_argument("--pretrain-iters", type=int, default=None,
                     help="--surrogate: Adam iterations on the run's own first blocks (default 2000, 0 with --weights)")
     ap.add_argument("--corpus-scenes", type=int, default=32)
@@ -522,6 +528,9 @@ def run_surrogate(args, rank, world):
     scene = make_scene(wl, rank)
     K = args.substeps
     settle = args.settle if "--settle" in sys.argv else SETTLE_DEFAULT.get(wl, 200)
+    weights = args.weights
+    if weights is None and not args.online_only and K in CORPUS_WEIGHTS:
+        weights = os.path.join(ROOT, CORPUS_WEIGHTS[K])
     # the surrogate's blocks follow the settle and collection steps
     total = max(args.steps, 2000, settle + 480 + 100 * K)
 
@@ -554,15 +563,15 @@ def run_surrogate(args, rank, world):
     b = make()
     b.enable_surrogate(substeps=K, check_interval=50, tolerance=args.sg_tolerance, fallback_blocks=20,
                        train_iters_per_block=20)
-    if args.weights:
-        # a network trained beforehand (bench.py --corpus --save-weights)
-        b.set_surrogate_weights(np.load(args.weights))
+    if weights:
+        # a network trained beforehand on the config-4 corpus
+        b.set_surrogate_weights(np.load(weights))
     b.step(settle)
     nb_collect = 480 // K
     b.surrogate_collect(nb_collect)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    pre = args.pretrain_iters if args.pretrain_iters is not None else (0 if args.weights else 2000)
+    pre = args.pretrain_iters if args.pretrain_iters is not None else (0 if weights else 2000)
     losses = [b.surrogate_train(200) for _ in range(pre // 200)]
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t1
@@ -589,7 +598,8 @@ def run_surrogate(args, rank, world):
         "data": "synthetic (seeded dam break with debris, dem_mph_b200.scenes)",
         "config": {"workload": scene.name, "n_particles": scene.n, "substeps_K": K, "check_interval": 50,
                    "tolerance": args.sg_tolerance, "settle_steps": settle, "collect_steps": nb_collect * K,
-                   "surrogate_blocks": nblocks, "dt": dt, "weights": args.weights or "trained on this run",
+                   "surrogate_blocks": nblocks, "dt": dt,
+                   "weights": os.path.relpath(weights, ROOT) if weights else "trained on this run's first blocks",
                    "pretrain_iters": pre},
         "plain_sim_s_per_hour": plain_rate, "speedup_vs_plain": sg_rate / plain_rate,
         "front_error_rel_travel": front_err, "front_plain_m": fa, "front_surrogate_m": fb, "front_start_m": f0,

@@ -44,3 +44,15 @@ def test_corpus_roundtrip_and_training():
     print("corpus MSE before %.4f after %.4f, losses %s" % (before, after, losses))
     assert after < 0.8 * before
     g.close()
+
+
+def test_committed_corpus_network_gains_on_an_unseen_scene():
+    """the network trained on the config-4 corpus (dem_mph_b200/weights,
+    made by bench.py --corpus --save-weights) on config 1, a scene outside
+    its corpus: its K = 8 velocity increments are closer to the solver's than
+    constant acceleration over the block"""
+    import os
+    w = np.load(os.path.join(os.path.dirname(corpus.__file__), "weights", "surrogate_config4_k8.npy"))
+    e_net, e_none = corpus.evaluate(scenes.config1(), w, substeps=8)
+    print("held-out config 1, K = 8: with the network %.4f, without %.4f" % (e_net, e_none))
+    assert e_net < 0.75 * e_none
