@@ -307,6 +307,9 @@ def main():
     ap.add_argument("--train-iters", type=int, default=20000)
     ap.add_argument("--sg-tolerance", type=float, default=0.02,
                     help="surrogate judge tolerance on the velocity-increment error")
+    ap.add_argument("--front-tolerance", type=float, default=0.0,
+                    help="surrogate judge on the surge front: fall back above this fraction of its travel "
+                         "(alone unless --sg-tolerance is given too)")
     ap.add_argument("--no-bodies", action="store_true",
                     help="move debris particles individually (reference DEM) instead of as rigid bodies")
     ap.add_argument("--no-list-reuse", action="store_true",
@@ -561,8 +564,10 @@ def run_surrogate(args, rank, world):
     dt = scene.params.dt
 
     b = make()
-    b.enable_surrogate(substeps=K, check_interval=50, tolerance=args.sg_tolerance, fallback_blocks=20,
-                       train_iters_per_block=20)
+    # --front-tolerance alone judges the surge front only
+    vtol = args.sg_tolerance if (args.front_tolerance <= 0 or "--sg-tolerance" in sys.argv) else 0.0
+    b.enable_surrogate(substeps=K, check_interval=50, tolerance=vtol, front_tolerance=args.front_tolerance,
+                       fallback_blocks=20, train_iters_per_block=20)
     if weights:
         # a network trained beforehand on the config-4 corpus
         b.set_surrogate_weights(np.load(weights))
@@ -597,7 +602,8 @@ def run_surrogate(args, rank, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 MLP + f32/f64 solver",
         "data": "synthetic (seeded dam break with debris, dem_mph_b200.scenes)",
         "config": {"workload": scene.name, "n_particles": scene.n, "substeps_K": K, "check_interval": 50,
-                   "tolerance": args.sg_tolerance, "settle_steps": settle, "collect_steps": nb_collect * K,
+                   "tolerance": vtol, "front_tolerance": args.front_tolerance,
+                   "settle_steps": settle, "collect_steps": nb_collect * K,
                    "surrogate_blocks": nblocks, "dt": dt,
                    "weights": os.path.relpath(weights, ROOT) if weights else "trained on this run's first blocks",
                    "pretrain_iters": pre},

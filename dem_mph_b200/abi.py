@@ -127,6 +127,7 @@ class SurrogateParams(C.Structure):
         ("learning_rate", C.c_float),
         ("seed", C.c_uint64),
         ("residual", C.c_int32),
+        ("front_tolerance", C.c_double),
     ]
 
 
@@ -144,6 +145,8 @@ class SurrogateStats(C.Structure):
         ("last_error", C.c_double),
         ("last_error_v", C.c_double),
         ("last_loss", C.c_double),
+        ("last_front_dev", C.c_double),
+        ("front_estimate", C.c_double),
     ]
 
     def as_dict(self):

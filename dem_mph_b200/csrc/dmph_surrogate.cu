@@ -38,6 +38,8 @@
 
 namespace dmph {
 
+constexpr int kFrontBins = 4096;  // surge-front histograms over the domain's x extent
+
 struct FeatScales {
     float inv_vs, inv_as, inv_Ps, inv_W0, inv_dx;
     float vs, as;
@@ -81,6 +83,13 @@ struct Surrogate {
     dmph_surrogate_stats st{};
     int fallback_left = 0;
     int since_check = 0;
+    // surge-front judge: histograms of fluid x (predicted, solver), the two
+    // fronts, the front at the first call, the accumulated squared deviation
+    unsigned *d_hist = nullptr;
+    double *d_front = nullptr;
+    double front_start = 0.0;
+    bool front_start_set = false;
+    double front_est2 = 0.0;
     unsigned long long block_seed = 0;
     // the tail of a surrogate call as one graph: apply the prediction, the
     // debris substeps, the rebuild decision with the rebuild as an IF node
@@ -415,8 +424,18 @@ __global__ void k_record_end(DevParams P, DevState S, const int *dB, FeatScales 
 
 // judge: prediction of the block (outputs Y of the start features) against
 // what the solver did; speed-weighted sums of squares over fluid rows
+// bin of an x position among kFrontBins over the domain's x extent (clamped)
+__device__ __forceinline__ int front_bin(const DevParams &P, double x)
+{
+    const int b = (int)floor((x - P.dmin[0]) / P.W[0] * kFrontBins);
+    return b < 0 ? 0 : (b >= kFrontBins ? kFrontBins - 1 : b);
+}
+
+// hist (kFrontBins each): x of the fluid as the network predicted the block
+// (from its start, block-start slots) and as the solver ended it
 __global__ void k_judge(DevParams P, DevState S, const int *dB, FeatScales F, const float4 *v0, const float4 *a0,
-                        const double *x0, const int *orig, const int *inv, const float *Y, double *acc)
+                        const double *x0, const int *orig, const int *inv, const float *Y, double *acc,
+                        unsigned *hist)
 {
     double e[4] = {0.0, 0.0, 0.0, 0.0};  // |dx err|^2, |dx|^2, |dv err|^2, |dv|^2
     FOR_EACH_SLOT(dB, -1, B_FE, s)
@@ -436,6 +455,10 @@ __global__ void k_judge(DevParams P, DevState S, const int *dB, FeatScales F, co
             e[1] += wgt * dx[d] * dx[d];
             e[2] += wgt * (pdv - dv[d]) * (pdv - dv[d]);
             e[3] += wgt * dv[d] * dv[d];
+            if (d == 0 && hist) {
+                atomicAdd(hist + front_bin(P, x0[3 * (long long)s] + pdx), 1u);
+                atomicAdd(hist + kFrontBins + front_bin(P, x0[3 * (long long)s] + dx[0]), 1u);
+            }
         }
     }
     for (int k = 0; k < 4; ++k) {
@@ -443,6 +466,36 @@ __global__ void k_judge(DevParams P, DevState S, const int *dB, FeatScales F, co
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
         if ((threadIdx.x & 31) == 0) atomicAdd(acc + k, v);
     }
+}
+
+// x of the current fluid positions into hist
+__global__ void k_front_now(DevParams P, DevState S, const int *dB, unsigned *hist)
+{
+    FOR_EACH_SLOT(dB, -1, B_FE, s)
+    {
+        double x[3];
+        abs_pos(P, S.p4[s], x);
+        atomicAdd(hist + front_bin(P, x[0]), 1u);
+    }
+}
+
+// the surge front of each of nh histograms: the upper edge of the bin below
+// which 99% of the counted fluid lies
+__global__ void k_front_quantiles(const DevParams P, const unsigned *hist, int nh, double *front)
+{
+    const int h = threadIdx.x;
+    if (h >= nh) return;
+    const unsigned *c = hist + (long long)h * kFrontBins;
+    unsigned long long total = 0;
+    for (int b = 0; b < kFrontBins; ++b) total += c[b];
+    const unsigned long long beyond = total / 100;  // the 1% furthest downstream
+    unsigned long long acc = 0;
+    int b = kFrontBins - 1;
+    for (; b > 0; --b) {
+        acc += c[b];
+        if (acc > beyond) break;
+    }
+    front[h] = P.dmin[0] + (double)(b + 1) * P.W[0] / kFrontBins;
 }
 
 // every prediction of the rows that will be applied is finite
@@ -742,7 +795,7 @@ int check_err(dmph_ctx *ctx, Surrogate *s)
 
 // one block of K plain steps that records samples (and, with judge, scores
 // the network's prediction of the same block)
-int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev)
+int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev, double *fronts = nullptr)
 {
     cudaStream_t st = ctx->st;
     enqueue_features(ctx, s, nullptr, st);
@@ -760,8 +813,10 @@ int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev)
     k_inverse_perm<<<gs, 256, 0, st>>>(ctx->P, ctx->S, s->inv);
     if (judge) {
         CK(cudaMemsetAsync(s->d_acc, 0, 4 * sizeof(double), st));
+        CK(cudaMemsetAsync(s->d_hist, 0, 2 * kFrontBins * sizeof(unsigned), st));
         k_judge<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->v0, s->a0, s->x0, s->orig, s->inv, s->Y,
-                                    s->d_acc);
+                                    s->d_acc, s->d_hist);
+        k_front_quantiles<<<1, 32, 0, st>>>(ctx->P, s->d_hist, 2, s->d_front);
     }
     // keep about pool/16 rows of every block
     const double keep = std::min(1.0, (double)s->pool_cap / 16.0 / std::max(1, s->n_fluid));
@@ -773,7 +828,11 @@ int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev)
     unsigned long long cur = 0;
     double acc[4] = {0, 0, 0, 0};
     CK(cudaMemcpyAsync(&cur, s->d_cursor, sizeof(cur), cudaMemcpyDeviceToHost, st));
-    if (judge) CK(cudaMemcpyAsync(acc, s->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, st));
+    double fr[2] = {0.0, 0.0};
+    if (judge) {
+        CK(cudaMemcpyAsync(acc, s->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(fr, s->d_front, sizeof(fr), cudaMemcpyDeviceToHost, st));
+    }
     CK(cudaStreamSynchronize(st));
     s->pool_count = std::min<long long>((long long)cur, s->pool_cap);
     s->st.samples = (int64_t)cur;
@@ -781,6 +840,10 @@ int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev)
     if (judge) {
         *ex = std::sqrt(acc[0] / std::max(acc[1], 1e-300));
         *ev = std::sqrt(acc[2] / std::max(acc[3], 1e-300));
+        if (fronts) {
+            fronts[0] = fr[0];  // the network's prediction of the block
+            fronts[1] = fr[1];  // the solver's
+        }
     }
     return check_err(ctx, s);
 }
@@ -957,6 +1020,7 @@ extern "C" int dmph_surrogate_params_default(dmph_surrogate_params *p)
     p->learning_rate = 1e-3f;
     p->seed = 1234;
     p->residual = 1;
+    p->front_tolerance = 0.0;
     return DMPH_OK;
 }
 
@@ -973,7 +1037,8 @@ extern "C" int dmph_surrogate_enable(dmph_ctx *ctx, const dmph_surrogate_params 
         return DMPH_EINVAL;
     }
     if (prm->substeps < 1 || prm->check_interval < 1 || prm->batch < 8192 || prm->batch % 8192 ||
-        prm->pool_rows < prm->batch || !(prm->tolerance > 0) || prm->fallback_blocks < 1) {
+        prm->pool_rows < prm->batch || !(prm->tolerance > 0 || prm->front_tolerance > 0) ||
+        !(prm->front_tolerance >= 0) || prm->fallback_blocks < 1) {
         ctx->err = "surrogate parameters out of range (batch a multiple of 8192, pool >= batch)";
         return DMPH_ERANGE;
     }
@@ -1055,6 +1120,8 @@ extern "C" int dmph_surrogate_enable(dmph_ctx *ctx, const dmph_surrogate_params 
     SA(s->d_err, 1);
     SA(s->d_bad, 1);
     SA(s->d_acc, 4);
+    SA(s->d_hist, 2 * kFrontBins);
+    SA(s->d_front, 2);
     CK(cudaMallocHost(&s->h_bad, sizeof(int)));
     feat_scales(ctx, s);
     CK(cudaStreamSynchronize(ctx->st));
@@ -1156,6 +1223,15 @@ extern "C" int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks)
     if (!s) return DMPH_EINVAL;
     drop_tail(s);  // recorded again with the context's current settings
     drop_graph(ctx);
+    if (s->prm.front_tolerance > 0 && !s->front_start_set) {
+        // the front the travel is measured from: at the first call
+        CK(cudaMemsetAsync(s->d_hist, 0, kFrontBins * sizeof(unsigned), ctx->st));
+        k_front_now<<<grid_slots(ctx), 256, 0, ctx->st>>>(ctx->P, ctx->S, ctx->dB, s->d_hist);
+        k_front_quantiles<<<1, 32, 0, ctx->st>>>(ctx->P, s->d_hist, 1, s->d_front);
+        CK(cudaMemcpyAsync(&s->front_start, s->d_front, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        s->front_start_set = true;
+    }
     for (int k = 0; k < nblocks; ++k) {
         int rc = DMPH_OK;
         if (s->fallback_left > 0 || !surrogate_allowed(ctx, s)) {
@@ -1167,17 +1243,30 @@ extern "C" int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks)
                     rc = train(ctx, s, s->prm.train_iters_per_block, nullptr);
             }
         } else if (s->since_check >= s->prm.check_interval) {
-            double ex = 0, ev = 0;
-            rc = plain_block(ctx, s, true, &ex, &ev);
+            double ex = 0, ev = 0, fr[2] = {0.0, 0.0};
+            const int calls = s->since_check;
+            rc = plain_block(ctx, s, true, &ex, &ev, fr);
             s->since_check = 0;
             s->st.judged++;
             s->st.last_error = ex;
             s->st.last_error_v = ev;
             // the velocity increments carry the dynamics; the displacements are
             // mostly the known drift K dt v0 and would hide their error
-            if (!rc && !(ev <= s->prm.tolerance)) {
+            bool fall = s->prm.tolerance > 0 && !(ev <= s->prm.tolerance);
+            if (s->prm.front_tolerance > 0) {
+                // the front deviation of one block, taken as that of every
+                // call since the last judged block, adding as a random walk
+                const double d = std::fabs(fr[0] - fr[1]);
+                s->front_est2 += d * d * std::max(1, calls);
+                const double travel = std::max(fr[1] - s->front_start, 10.0 * ctx->P.dx);
+                s->st.last_front_dev = d;
+                s->st.front_estimate = std::sqrt(s->front_est2) / travel;
+                if (!(s->st.front_estimate <= s->prm.front_tolerance)) fall = true;
+            }
+            if (!rc && fall) {
                 s->st.fallbacks++;
                 s->fallback_left = s->prm.fallback_blocks;
+                s->front_est2 = 0.0;
             }
         } else {
             rc = surrogate_block(ctx, s);

@@ -490,6 +490,14 @@ typedef struct dmph_surrogate_params {
     float learning_rate;       /* Adam (1e-3) */
     unsigned long long seed;   /* initial weights */
     int residual;              /* 1: learn dv - K dt a0 (a0 = acceleration at the block start), 0: dv (1) */
+    /* surge-front judge (0: off, the default): fall back when the estimated
+     * deviation of the surge front (the x below which 99% of the fluid lies)
+     * exceeds this fraction of the front's travel since the first call.  At
+     * every judged block the front of the network's prediction of that block
+     * is compared with the plain solver's; the deviations of the calls since
+     * the previous judged block add as a random walk (sqrt(sum d^2 n)).
+     * tolerance <= 0 switches the velocity-increment judge off. */
+    double front_tolerance;
 } dmph_surrogate_params;
 
 typedef struct dmph_surrogate_stats {
@@ -504,6 +512,8 @@ typedef struct dmph_surrogate_stats {
     double last_error;    /* last judged relative L2 error of the displacements */
     double last_error_v;  /* same for the velocity increments (the fallback criterion) */
     double last_loss;     /* mean squared error of the last training batch */
+    double last_front_dev;   /* surge-front deviation of the last judged block (m) */
+    double front_estimate;   /* the front judge's estimate, as a fraction of the front's travel */
 } dmph_surrogate_stats;
 
 int dmph_surrogate_params_default(dmph_surrogate_params *p);

@@ -56,3 +56,17 @@ def test_checkpoint_open_rejects_foreign_files_without_gpu_work(tmp_path):
         with pytest.raises(solver.DmphError) as e:
             solver.Solver.open_checkpoint(str(path))
         assert e.value.code == -4, str(e.value)
+
+
+def test_surrogate_params_layout_matches_the_header():
+    """dmph_surrogate_params_default fills the ctypes mirror field by field
+    (no GPU): every default lands in its field, the last one included"""
+    import ctypes as C
+    from dem_mph_b200 import abi
+    sp = abi.SurrogateParams()
+    sp.front_tolerance = -7.0
+    assert solver.lib().dmph_surrogate_params_default(C.byref(sp)) == 0
+    assert (sp.substeps, sp.check_interval, sp.fallback_blocks, sp.batch, sp.pool_rows, sp.residual) == \
+        (8, 50, 50, 65536, 1 << 22, 1)
+    assert abs(sp.tolerance - 0.02) < 1e-15 and abs(sp.learning_rate - 1e-3) < 1e-9 and sp.seed == 1234
+    assert sp.front_tolerance == 0.0

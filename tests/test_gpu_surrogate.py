@@ -144,6 +144,28 @@ def test_fallback_on_large_error_and_none_on_loose_tolerance():
     h.close()
 
 
+def test_front_judge():
+    """the surge-front judge alone (velocity-increment judge off): a tolerance
+    no prediction meets falls back at the judged block, a loose one never;
+    the estimate and the last block's deviation are reported"""
+    g = make(tolerance=0.0, front_tolerance=1e-9, fallback_blocks=3, check_interval=2)
+    g.step(20)
+    g.surrogate_collect(4)
+    g.surrogate_advance(3)  # 2 surrogate calls, then a judged block
+    st = g.surrogate_stats()
+    assert st["judged"] == 1 and st["fallbacks"] == 1 and st["in_fallback"] == 1
+    assert np.isfinite(st["front_estimate"]) and st["last_front_dev"] >= 0
+    g.close()
+    h = make(tolerance=0.0, front_tolerance=1e9, check_interval=2)
+    h.step(20)
+    h.surrogate_collect(4)
+    h.surrogate_advance(6)
+    st = h.surrogate_stats()
+    assert st["judged"] == 2 and st["fallbacks"] == 0 and st["calls"] == 4
+    assert 0 <= st["front_estimate"] < 1e9
+    h.close()
+
+
 def test_list_features_match_stencil_features():
     """the features computed over the Verlet lists (the default) and over the
     27-cell stencil are the same sums up to FP32 summation order"""
