@@ -148,13 +148,18 @@ def test_front_judge():
     """the surge-front judge alone (velocity-increment judge off): a tolerance
     no prediction meets falls back at the judged block, a loose one never;
     the estimate and the last block's deviation are reported"""
-    g = make(tolerance=0.0, front_tolerance=1e-9, fallback_blocks=3, check_interval=2)
+    g = make(tolerance=0.0, front_tolerance=1e-6, fallback_blocks=3, check_interval=2)
+    # a network that predicts a strong push along x (output bias of dv_x),
+    # so that its front runs ahead of the solver's by several histogram bins
+    w = g.surrogate_weights()
+    w[-16] = 2000.0
+    g.set_surrogate_weights(w)
     g.step(20)
     g.surrogate_collect(4)
     g.surrogate_advance(3)  # 2 surrogate calls, then a judged block
     st = g.surrogate_stats()
     assert st["judged"] == 1 and st["fallbacks"] == 1 and st["in_fallback"] == 1
-    assert np.isfinite(st["front_estimate"]) and st["last_front_dev"] >= 0
+    assert st["front_estimate"] > 1e-6 and st["last_front_dev"] > 0
     g.close()
     h = make(tolerance=0.0, front_tolerance=1e9, check_interval=2)
     h.step(20)
