@@ -38,7 +38,10 @@
 
 namespace dmph {
 
-constexpr int kFrontBins = 4096;  // surge-front histograms over the domain's x extent
+// surge-front histograms over the domain's x extent: 65,536 bins (0.05 mm
+// on a 3.3 m domain), finer than the front moves in one block
+constexpr int kFrontBins = 1 << 16;
+constexpr int kFrontThreads = 1024;
 
 struct FeatScales {
     float inv_vs, inv_as, inv_Ps, inv_W0, inv_dx;
@@ -479,23 +482,33 @@ __global__ void k_front_now(DevParams P, DevState S, const int *dB, unsigned *hi
     }
 }
 
-// the surge front of each of nh histograms: the upper edge of the bin below
-// which 99% of the counted fluid lies
-__global__ void k_front_quantiles(const DevParams P, const unsigned *hist, int nh, double *front)
+// the surge front of histogram blockIdx.x: the upper edge of the bin below
+// which 99% of the counted fluid lies (each thread sums a run of bins, one
+// thread walks the run sums from the top, then the run that holds the
+// quantile bin by bin)
+__global__ void __launch_bounds__(kFrontThreads) k_front_quantiles(const DevParams P, const unsigned *hist,
+                                                                  double *front)
 {
-    const int h = threadIdx.x;
-    if (h >= nh) return;
-    const unsigned *c = hist + (long long)h * kFrontBins;
+    constexpr int kRun = kFrontBins / kFrontThreads;
+    __shared__ unsigned long long run[kFrontThreads];
+    const unsigned *c = hist + (long long)blockIdx.x * kFrontBins;
+    unsigned long long sum = 0;
+    for (int b = 0; b < kRun; ++b) sum += c[threadIdx.x * kRun + b];
+    run[threadIdx.x] = sum;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
     unsigned long long total = 0;
-    for (int b = 0; b < kFrontBins; ++b) total += c[b];
+    for (int r = 0; r < kFrontThreads; ++r) total += run[r];
     const unsigned long long beyond = total / 100;  // the 1% furthest downstream
     unsigned long long acc = 0;
-    int b = kFrontBins - 1;
-    for (; b > 0; --b) {
+    int r = kFrontThreads - 1;
+    for (; r > 0 && acc + run[r] <= beyond; --r) acc += run[r];
+    int b = (r + 1) * kRun - 1;
+    for (; b > r * kRun; --b) {
         acc += c[b];
         if (acc > beyond) break;
     }
-    front[h] = P.dmin[0] + (double)(b + 1) * P.W[0] / kFrontBins;
+    front[blockIdx.x] = P.dmin[0] + (double)(b + 1) * P.W[0] / kFrontBins;
 }
 
 // every prediction of the rows that will be applied is finite
@@ -816,7 +829,7 @@ int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev,
         CK(cudaMemsetAsync(s->d_hist, 0, 2 * kFrontBins * sizeof(unsigned), st));
         k_judge<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->v0, s->a0, s->x0, s->orig, s->inv, s->Y,
                                     s->d_acc, s->d_hist);
-        k_front_quantiles<<<1, 32, 0, st>>>(ctx->P, s->d_hist, 2, s->d_front);
+        k_front_quantiles<<<2, kFrontThreads, 0, st>>>(ctx->P, s->d_hist, s->d_front);
     }
     // keep about pool/16 rows of every block
     const double keep = std::min(1.0, (double)s->pool_cap / 16.0 / std::max(1, s->n_fluid));
@@ -1227,7 +1240,7 @@ extern "C" int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks)
         // the front the travel is measured from: at the first call
         CK(cudaMemsetAsync(s->d_hist, 0, kFrontBins * sizeof(unsigned), ctx->st));
         k_front_now<<<grid_slots(ctx), 256, 0, ctx->st>>>(ctx->P, ctx->S, ctx->dB, s->d_hist);
-        k_front_quantiles<<<1, 32, 0, ctx->st>>>(ctx->P, s->d_hist, 1, s->d_front);
+        k_front_quantiles<<<1, kFrontThreads, 0, ctx->st>>>(ctx->P, s->d_hist, s->d_front);
         CK(cudaMemcpyAsync(&s->front_start, s->d_front, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
         s->front_start_set = true;
