@@ -87,12 +87,13 @@ struct Surrogate {
     int fallback_left = 0;
     int since_check = 0;
     // surge-front judge: histograms of fluid x (predicted, solver), the two
-    // fronts, the front at the first call, the accumulated squared deviation
+    // fronts, the front at the first call, the accumulated deviation estimate
     unsigned *d_hist = nullptr;
+    float *d_histv = nullptr;  // predicted minus solver x-velocity, summed per bin of the solver's positions
     double *d_front = nullptr;
     double front_start = 0.0;
     bool front_start_set = false;
-    double front_est2 = 0.0;
+    double front_est = 0.0;
     unsigned long long block_seed = 0;
     // the tail of a surrogate call as one graph: apply the prediction, the
     // debris substeps, the rebuild decision with the rebuild as an IF node
@@ -435,10 +436,12 @@ __device__ __forceinline__ int front_bin(const DevParams &P, double x)
 }
 
 // hist (kFrontBins each): x of the fluid as the network predicted the block
-// (from its start, block-start slots) and as the solver ended it
+// (from its start, block-start slots) and as the solver ended it; histv: the
+// predicted minus the solver's x-velocity at the block's end, by the bin of
+// the solver's position
 __global__ void k_judge(DevParams P, DevState S, const int *dB, FeatScales F, const float4 *v0, const float4 *a0,
                         const double *x0, const int *orig, const int *inv, const float *Y, double *acc,
-                        unsigned *hist)
+                        unsigned *hist, float *histv)
 {
     double e[4] = {0.0, 0.0, 0.0, 0.0};  // |dx err|^2, |dx|^2, |dv err|^2, |dv|^2
     FOR_EACH_SLOT(dB, -1, B_FE, s)
@@ -459,8 +462,10 @@ __global__ void k_judge(DevParams P, DevState S, const int *dB, FeatScales F, co
             e[2] += wgt * (pdv - dv[d]) * (pdv - dv[d]);
             e[3] += wgt * dv[d] * dv[d];
             if (d == 0 && hist) {
+                const int bs = front_bin(P, x0[3 * (long long)s] + dx[0]);
                 atomicAdd(hist + front_bin(P, x0[3 * (long long)s] + pdx), 1u);
-                atomicAdd(hist + kFrontBins + front_bin(P, x0[3 * (long long)s] + dx[0]), 1u);
+                atomicAdd(hist + kFrontBins + bs, 1u);
+                atomicAdd(histv + bs, (float)(pdv - dv[0]));
             }
         }
     }
@@ -485,16 +490,24 @@ __global__ void k_front_now(DevParams P, DevState S, const int *dB, unsigned *hi
 // the surge front of histogram blockIdx.x: the upper edge of the bin below
 // which 99% of the counted fluid lies (each thread sums a run of bins, one
 // thread walks the run sums from the top, then the run that holds the
-// quantile bin by bin)
+// quantile bin by bin).  With histv (the second histogram only): front[2] =
+// the mean of histv over the front's 1% (bins from the quantile bin up)
 __global__ void __launch_bounds__(kFrontThreads) k_front_quantiles(const DevParams P, const unsigned *hist,
-                                                                  double *front)
+                                                                  double *front, const float *histv)
 {
     constexpr int kRun = kFrontBins / kFrontThreads;
     __shared__ unsigned long long run[kFrontThreads];
+    __shared__ double runv[kFrontThreads];
     const unsigned *c = hist + (long long)blockIdx.x * kFrontBins;
+    const bool vel = histv && blockIdx.x == 1;
     unsigned long long sum = 0;
-    for (int b = 0; b < kRun; ++b) sum += c[threadIdx.x * kRun + b];
+    double sv = 0.0;
+    for (int b = 0; b < kRun; ++b) {
+        sum += c[threadIdx.x * kRun + b];
+        if (vel) sv += histv[threadIdx.x * kRun + b];
+    }
     run[threadIdx.x] = sum;
+    runv[threadIdx.x] = sv;
     __syncthreads();
     if (threadIdx.x != 0) return;
     unsigned long long total = 0;
@@ -502,13 +515,23 @@ __global__ void __launch_bounds__(kFrontThreads) k_front_quantiles(const DevPara
     const unsigned long long beyond = total / 100;  // the 1% furthest downstream
     unsigned long long acc = 0;
     int r = kFrontThreads - 1;
-    for (; r > 0 && acc + run[r] <= beyond; --r) acc += run[r];
+    double accv = 0.0;
+    for (; r > 0 && acc + run[r] <= beyond; --r) {
+        acc += run[r];
+        accv += runv[r];
+    }
     int b = (r + 1) * kRun - 1;
     for (; b > r * kRun; --b) {
         acc += c[b];
+        if (vel) accv += histv[b];
         if (acc > beyond) break;
     }
+    if (b == r * kRun) {  // the run's lowest bin holds the quantile
+        acc += c[b];
+        if (vel) accv += histv[b];
+    }
     front[blockIdx.x] = P.dmin[0] + (double)(b + 1) * P.W[0] / kFrontBins;
+    if (vel) front[2] = acc > 0 ? accv / (double)acc : 0.0;
 }
 
 // every prediction of the rows that will be applied is finite
@@ -827,9 +850,10 @@ int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev,
     if (judge) {
         CK(cudaMemsetAsync(s->d_acc, 0, 4 * sizeof(double), st));
         CK(cudaMemsetAsync(s->d_hist, 0, 2 * kFrontBins * sizeof(unsigned), st));
+        CK(cudaMemsetAsync(s->d_histv, 0, kFrontBins * sizeof(float), st));
         k_judge<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->v0, s->a0, s->x0, s->orig, s->inv, s->Y,
-                                    s->d_acc, s->d_hist);
-        k_front_quantiles<<<2, kFrontThreads, 0, st>>>(ctx->P, s->d_hist, s->d_front);
+                                    s->d_acc, s->d_hist, s->d_histv);
+        k_front_quantiles<<<2, kFrontThreads, 0, st>>>(ctx->P, s->d_hist, s->d_front, s->d_histv);
     }
     // keep about pool/16 rows of every block
     const double keep = std::min(1.0, (double)s->pool_cap / 16.0 / std::max(1, s->n_fluid));
@@ -841,7 +865,7 @@ int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev,
     unsigned long long cur = 0;
     double acc[4] = {0, 0, 0, 0};
     CK(cudaMemcpyAsync(&cur, s->d_cursor, sizeof(cur), cudaMemcpyDeviceToHost, st));
-    double fr[2] = {0.0, 0.0};
+    double fr[3] = {0.0, 0.0, 0.0};
     if (judge) {
         CK(cudaMemcpyAsync(acc, s->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(fr, s->d_front, sizeof(fr), cudaMemcpyDeviceToHost, st));
@@ -854,8 +878,9 @@ int plain_block(dmph_ctx *ctx, Surrogate *s, bool judge, double *ex, double *ev,
         *ex = std::sqrt(acc[0] / std::max(acc[1], 1e-300));
         *ev = std::sqrt(acc[2] / std::max(acc[3], 1e-300));
         if (fronts) {
-            fronts[0] = fr[0];  // the network's prediction of the block
+            fronts[0] = fr[0];  // front of the network's prediction of the block
             fronts[1] = fr[1];  // the solver's
+            fronts[2] = fr[2];  // mean x-velocity error of the front's fluid
         }
     }
     return check_err(ctx, s);
@@ -1134,7 +1159,8 @@ extern "C" int dmph_surrogate_enable(dmph_ctx *ctx, const dmph_surrogate_params 
     SA(s->d_bad, 1);
     SA(s->d_acc, 4);
     SA(s->d_hist, 2 * kFrontBins);
-    SA(s->d_front, 2);
+    SA(s->d_histv, kFrontBins);
+    SA(s->d_front, 4);
     CK(cudaMallocHost(&s->h_bad, sizeof(int)));
     feat_scales(ctx, s);
     CK(cudaStreamSynchronize(ctx->st));
@@ -1240,7 +1266,7 @@ extern "C" int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks)
         // the front the travel is measured from: at the first call
         CK(cudaMemsetAsync(s->d_hist, 0, kFrontBins * sizeof(unsigned), ctx->st));
         k_front_now<<<grid_slots(ctx), 256, 0, ctx->st>>>(ctx->P, ctx->S, ctx->dB, s->d_hist);
-        k_front_quantiles<<<1, kFrontThreads, 0, ctx->st>>>(ctx->P, s->d_hist, s->d_front);
+        k_front_quantiles<<<1, kFrontThreads, 0, ctx->st>>>(ctx->P, s->d_hist, s->d_front, nullptr);
         CK(cudaMemcpyAsync(&s->front_start, s->d_front, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
         s->front_start_set = true;
@@ -1256,7 +1282,7 @@ extern "C" int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks)
                     rc = train(ctx, s, s->prm.train_iters_per_block, nullptr);
             }
         } else if (s->since_check >= s->prm.check_interval) {
-            double ex = 0, ev = 0, fr[2] = {0.0, 0.0};
+            double ex = 0, ev = 0, fr[3] = {0.0, 0.0, 0.0};
             const int calls = s->since_check;
             rc = plain_block(ctx, s, true, &ex, &ev, fr);
             s->since_check = 0;
@@ -1267,19 +1293,23 @@ extern "C" int dmph_surrogate_advance(dmph_ctx *ctx, int nblocks)
             // mostly the known drift K dt v0 and would hide their error
             bool fall = s->prm.tolerance > 0 && !(ev <= s->prm.tolerance);
             if (s->prm.front_tolerance > 0) {
-                // the front deviation of one block, taken as that of every
-                // call since the last judged block, adding as a random walk
-                const double d = std::fabs(fr[0] - fr[1]);
-                s->front_est2 += d * d * std::max(1, calls);
+                // the deviation a call makes in the front: its position error
+                // within the block, and the error of the front fluid's
+                // velocity, which persists and moves the front over the calls
+                // that follow; those since the last judged block each taken
+                // to have made it, added up
+                const double kdt = (double)s->prm.substeps * ctx->P.dt;
+                const double d = std::fabs(fr[0] - fr[1]) + std::fabs(fr[2]) * kdt * std::max(1, calls) * 0.5;
+                s->front_est += d * std::max(1, calls);
                 const double travel = std::max(fr[1] - s->front_start, 10.0 * ctx->P.dx);
                 s->st.last_front_dev = d;
-                s->st.front_estimate = std::sqrt(s->front_est2) / travel;
+                s->st.front_estimate = s->front_est / travel;
                 if (!(s->st.front_estimate <= s->prm.front_tolerance)) fall = true;
             }
             if (!rc && fall) {
                 s->st.fallbacks++;
                 s->fallback_left = s->prm.fallback_blocks;
-                s->front_est2 = 0.0;
+                s->front_est = 0.0;
             }
         } else {
             rc = surrogate_block(ctx, s);

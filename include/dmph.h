@@ -493,9 +493,12 @@ typedef struct dmph_surrogate_params {
     /* surge-front judge (0: off, the default): fall back when the estimated
      * deviation of the surge front (the x below which 99% of the fluid lies)
      * exceeds this fraction of the front's travel since the first call.  At
-     * every judged block the front of the network's prediction of that block
-     * is compared with the plain solver's; the deviations of the calls since
-     * the previous judged block add as a random walk (sqrt(sum d^2 n)).
+     * every judged block the network's prediction of that block is compared
+     * with the plain solver's: the front's position, and the x-velocity of
+     * the fluid in the front's 1%, whose error persists into the calls that
+     * follow; each of the n calls since the previous judged block is taken
+     * to have made the position error plus the velocity error times
+     * n K Dt / 2, and the estimate adds them up (reset at a fallback).
      * tolerance <= 0 switches the velocity-increment judge off. */
     double front_tolerance;
 } dmph_surrogate_params;
