@@ -305,11 +305,12 @@ def main():
     ap.add_argument("--corpus-scenes", type=int, default=32)
     ap.add_argument("--corpus-steps", type=int, default=4000)
     ap.add_argument("--train-iters", type=int, default=20000)
-    ap.add_argument("--sg-tolerance", type=float, default=0.02,
-                    help="surrogate judge tolerance on the velocity-increment error")
-    ap.add_argument("--front-tolerance", type=float, default=0.0,
-                    help="surrogate judge on the surge front: fall back above this fraction of its travel "
-                         "(alone unless --sg-tolerance is given too)")
+    ap.add_argument("--sg-tolerance", type=float, default=0.5,
+                    help="surrogate judge tolerance on the velocity-increment error of a judged block (a guard "
+                         "against a network that has lost the flow)")
+    ap.add_argument("--front-tolerance", type=float, default=0.02,
+                    help="surrogate judge on the surge front: fall back when its estimated deviation exceeds "
+                         "this fraction of its travel (0: off)")
     ap.add_argument("--no-bodies", action="store_true",
                     help="move debris particles individually (reference DEM) instead of as rigid bodies")
     ap.add_argument("--no-list-reuse", action="store_true",
@@ -564,8 +565,7 @@ def run_surrogate(args, rank, world):
     dt = scene.params.dt
 
     b = make()
-    # --front-tolerance alone judges the surge front only
-    vtol = args.sg_tolerance if (args.front_tolerance <= 0 or "--sg-tolerance" in sys.argv) else 0.0
+    vtol = args.sg_tolerance
     b.enable_surrogate(substeps=K, check_interval=50, tolerance=vtol, front_tolerance=args.front_tolerance,
                        fallback_blocks=20, train_iters_per_block=20)
     if weights:
