@@ -281,6 +281,35 @@ void dmph::enqueue_dem(dmph_ctx *ctx, cudaStream_t st)
     phase_end(ctx, ctx->Bd.B > 0 ? 5 : 4);
 }
 
+// The DEM substeps of `steps` steps with the fluid force held (the surrogate's
+// block).  With rigid bodies in the FP32 build the fluid force goes to the
+// FP64 planes once and the FP32 copies of the debris are refreshed once, at
+// the end (the contact forces have planes of their own and the substeps read
+// the FP64 masters); otherwise the steps' DEM phases one after the other.
+void dmph::enqueue_dem_block(dmph_ctx *ctx, int steps, cudaStream_t st)
+{
+    if (!(ctx->fp32 && ctx->Bd.B > 0)) {
+        for (int k = 0; k < steps; ++k) enqueue_dem(ctx, st);
+        return;
+    }
+    const DevParams &P = ctx->P;
+    DevState &S = ctx->S;
+    phase_begin(ctx);
+    launch_solid_force_to64(P, S, ctx->dB, st);
+    for (int k = 0; k < steps * ctx->demSteps; ++k) {
+        launch_clump_dem(P, S, ctx->dB, ctx->use_list, st);
+        launch_body_step(P, S, ctx->Bd, true, st);
+    }
+    launch_sync_solids32(P, S, ctx->dB, st);
+    phase_end(ctx, 5);
+}
+
+long long dmph::dem_block_launches(const dmph_ctx *ctx, int steps)
+{
+    if (!(ctx->fp32 && ctx->Bd.B > 0)) return steps * dem_launches(ctx);
+    return 2 + (long long)steps * ctx->demSteps * (ctx->use_list ? 3 : 2);
+}
+
 // the force passes and the DEM substeps (second part of a step)
 static void enqueue_tail(dmph_ctx *ctx, cudaStream_t st)
 {

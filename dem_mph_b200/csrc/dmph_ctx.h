@@ -112,6 +112,9 @@ void enqueue_head(dmph_ctx *ctx, unsigned long long graph_cond, cudaStream_t st)
 void enqueue_passes(dmph_ctx *ctx, cudaStream_t st);
 void enqueue_pair_passes32(dmph_ctx *ctx, cudaStream_t st);
 void enqueue_dem(dmph_ctx *ctx, cudaStream_t st);
+// the DEM substeps of `steps` steps with the fluid force held (surrogate block)
+void enqueue_dem_block(dmph_ctx *ctx, int steps, cudaStream_t st);
+long long dem_block_launches(const dmph_ctx *ctx, int steps);
 long long dem_launches(const dmph_ctx *ctx);
 long long tail_launches(const dmph_ctx *ctx, bool graph = false);
 void advance_host_clock(dmph_ctx *ctx);

@@ -930,8 +930,7 @@ void enqueue_tail_ops(dmph_ctx *ctx, Surrogate *s, unsigned long long cond, cuda
 {
     const int gs = grid_slots(ctx);
     k_apply32<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->dB, s->fs, s->Y, 0, s->d_bad);
-    if (s->n_rows > s->n_fluid)
-        for (int k = 0; k < s->prm.substeps; ++k) enqueue_dem(ctx, st);
+    if (s->n_rows > s->n_fluid) enqueue_dem_block(ctx, s->prm.substeps, st);
     cudaMemsetAsync(ctx->S.f4, 0, sizeof(float4) * (size_t)ctx->P.N, st);
     cudaMemsetAsync(ctx->maxshift, 0, sizeof(unsigned long long), st);
     k_maxshift32<<<gs, 256, 0, st>>>(ctx->P, ctx->S, ctx->maxshift);
@@ -1000,7 +999,7 @@ int surrogate_block(dmph_ctx *ctx, Surrogate *s)
     // pair passes (list mode: 5, stencil: 2), features (list mode: 2), 4
     // GEMMs, check, apply, maxshift, decide; the rebuilds the graph runs are
     // counted by the device's rebuild counter
-    ctx->launches += (ctx->use_list ? 15 : 11) + (s->n_rows > s->n_fluid ? s->prm.substeps * dem_launches(ctx) : 0);
+    ctx->launches += (ctx->use_list ? 15 : 11) + (s->n_rows > s->n_fluid ? dem_block_launches(ctx, s->prm.substeps) : 0);
     for (int k = 0; k < s->prm.substeps; ++k) advance_host_clock(ctx);
     s->st.calls++;
     return DMPH_OK;
