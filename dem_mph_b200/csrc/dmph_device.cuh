@@ -24,7 +24,7 @@ constexpr int kTypes = DMPH_TYPE_COUNT;
 constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xffffffffu;
 // list reuse: the widest list skin past MaxRadius, in hundredths of dx (the
-// cells are this much wider than MaxRadius + MARGIN)
+// cells are MaxRadius + this wide)
 constexpr int kSkinMaxHundredths = 40;
 
 __host__ __device__ inline bool is_fluid(int t) { return DMPH_FLUID_BEGIN <= t && t < DMPH_FLUID_END; }

@@ -151,13 +151,13 @@ int derive_params(const dmph_params &p, int n, DevParams &P, WallMotion &Wm, con
         P.hW[d] = 0.5 * P.W[d];
         P.dmin[d] = p.domain_min[d];
     }
-    // list reuse (FP32 build): cells wider by the widest list skin, so that
-    // the 3-cell stencil holds every pair within the list radius while the
-    // particles stay in the cells of the last sort
-    const double cell_r = maxR + margin +
-                          ((p.flags & DMPH_FLAG_LIST_REUSE) && p.precision == DMPH_PRECISION_FP32_SPLIT
-                               ? 0.01 * kSkinMaxHundredths * dx
-                               : 0.0);
+    // list reuse (FP32 build): cells of MaxRadius + the widest list skin
+    // (instead of + MARGIN): the 3-cell stencil then holds every pair within
+    // the widest list radius at a rebuild, and every pair within
+    // MaxRadius + MARGIN of particles up to (skin - MARGIN) / 2 from the
+    // positions of the last sort (the neighbour counts between rebuilds)
+    const bool reuse = (p.flags & DMPH_FLAG_LIST_REUSE) && p.precision == DMPH_PRECISION_FP32_SPLIT;
+    const double cell_r = reuse ? maxR + 0.01 * kSkinMaxHundredths * dx : maxR + margin;
     cc[0] = std::floor((p.domain_max[0] - p.domain_min[0]) / cell_r);
     cc[1] = std::floor((p.domain_max[1] - p.domain_min[1]) / cell_r);
     cc[2] = p.dim == 2 ? 1 : std::floor((p.domain_max[2] - p.domain_min[2]) / cell_r);

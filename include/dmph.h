@@ -325,7 +325,8 @@ int dmph_get_list_stats(dmph_ctx *ctx, int64_t *entries_pass_a, int64_t *entries
  * DMPH_FLAG_ALL_NEIGHBOR_COUNTS; otherwise the flag only widens the cells).  The reference rebuilds at every
  * trigger of its displacement test (neighborCalculation :1264-1286): cell
  * sort, NeighborInd, and the neighbour counts the drag terms read.  With the
- * flag, the cells are 0.4 dx wider than MaxRadius + MARGIN and each list is
+ * flag, the cells are MaxRadius + 0.4 dx wide (instead of MaxRadius + MARGIN)
+ * and each list is
  * built with a skin S of 0.1 or 0.4 dx past MaxRadius (chosen on the device
  * from how many steps lay between the last two triggers: the wide skin when
  * they come at most four steps apart).  Every trigger still resets the
